@@ -1,0 +1,165 @@
+"""Test infrastructure (oracle only): ctypes bindings for the two CPU oracles.
+
+* ``ref()``  -> oracle/_ref/libref_oracle.so: the reference's own device-math headers compiled for
+  the host (built from the reference sources by oracle/Makefile; the built file travels with the
+  repository).  ``None`` when it was never built.
+* ``orc()``  -> oracle/liboracle.so: the oracle restatement (FP32 bit-identical to ``ref()``, FP64
+  instantiations, CPU path tracer).
+
+Only tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` use this module;
+the product never imports it.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SO = os.path.join(HERE, "_ref", "libref_oracle.so")
+ORC_SO = os.path.join(HERE, "liboracle.so")
+
+_ref = None
+_orc = None
+
+F = ctypes.c_float
+D = ctypes.c_double
+U = ctypes.c_uint
+L = ctypes.c_long
+I = ctypes.c_int
+P = ctypes.c_void_p
+
+
+def fp(a):
+    """Pointer to a contiguous numpy array's data."""
+    assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
+    return a.ctypes.data_as(P)
+
+
+def build():
+    """Build both oracle libraries (the reference one only where the reference sources exist)."""
+    import subprocess
+
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+
+
+def _sig(lib, name, res, args):
+    f = getattr(lib, name)
+    f.restype = res
+    f.argtypes = args
+    return f
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        if not os.path.exists(REF_SO):
+            return None
+        lib = ctypes.CDLL(REF_SO)
+        _sig(lib, "ref_tea16", U, [U, U])
+        _sig(lib, "ref_rnd_tea_stream", U, [U, P, L])
+        _sig(lib, "ref_rnd_lcg_stream", U, [U, P, L])
+        _sig(lib, "ref_rnd_md5_stream", None, [P, P, P, L])
+        _sig(lib, "ref_md5_u2", None, [U, U, U, P])
+        _sig(lib, "ref_erfinv", D, [D])
+        _sig(lib, "ref_bsdf_queries", None, [L, L, L, P, P, F, P, P, P, P])
+        _sig(lib, "ref_sample_visible_normal", None, [P, P, F, F, F, F, U, P])
+        _sig(lib, "ref_eval_visible_normal", F, [P, P, P, F, F, U])
+        _sig(lib, "ref_sample_normal", None, [P, F, F, F, U, P])
+        _sig(lib, "ref_masking_G1", F, [P, P, P, F, U])
+        _sig(lib, "ref_masking_G1_aniso", F, [P, P, P, F, F, U])
+        _sig(lib, "ref_eval_bsdf", F, [P, P, P, F, F, U])
+        _sig(lib, "ref_fresnel_R_vec", F, [P, P, F])
+        _sig(lib, "ref_fresnel_complex", None, [P, P, P, P])
+        _sig(lib, "ref_complex_recip", None, [P, P])
+        _sig(lib, "ref_ms_dielectric_eval", F, [P, P, P, F, F, F, P, U, U])
+        _sig(lib, "ref_ms_dielectric_sample", None, [P, P, F, F, F, P, P, U, P])
+        _sig(lib, "ref_ms_conductor_eval", None, [P, P, P, P, F, F, P, U, U, P])
+        _sig(lib, "ref_ms_conductor_sample", None, [P, P, P, F, F, P, P, U, P, P])
+        _sig(lib, "ref_ms_diffuse_eval", None, [P, P, P, F, F, P, U, P, U, P])
+        _sig(lib, "ref_ms_diffuse_sample", None, [P, P, F, F, P, P, P, U, P, P])
+        _sig(lib, "ref_sample_cosine_weighted", None, [P, P, P])
+        _sig(lib, "ref_sample_barycentric", None, [P, P])
+        _sig(lib, "ref_create_onb", None, [P, P, P])
+        _sig(lib, "ref_set_light_buffers", None, [P, L, P, L])
+        _sig(lib, "ref_direct_illumination", None, [P, L, P, P, P, P])
+        _sig(lib, "ref_set_envmap", None, [P, I, I, P, P, P, P])
+        _sig(lib, "ref_env_lookup", None, [P, P])
+        _sig(lib, "ref_sample_environment", None, [P, P, P, P])
+        _sig(lib, "ref_set_scattering_properties", None, [P, L])
+        _sig(lib, "ref_dipole_bssrdf", None, [F, P])
+        _sig(lib, "ref_dirpole_bssrdf", None, [P, P, P, P, P, P])
+        _sig(lib, "ref_C_phi", F, [F])
+        _sig(lib, "ref_C_E", F, [F])
+        _sig(lib, "ref_sizeof", I, [ctypes.c_char_p])
+        _sig(lib, "ref_oob_reads", ctypes.c_ulonglong, [])
+        _ref = lib
+    return _ref
+
+
+def orc():
+    global _orc
+    if _orc is None:
+        if not os.path.exists(ORC_SO):
+            raise RuntimeError("oracle/liboracle.so is not built (run oracle/Makefile)")
+        lib = ctypes.CDLL(ORC_SO)
+        _sig(lib, "orc_tea16", U, [U, U])
+        _sig(lib, "orc_rnd_tea_stream", U, [U, P, L])
+        _sig(lib, "orc_rnd_lcg_stream", U, [U, P, L])
+        _sig(lib, "orc_rnd_md5_stream", None, [P, P, P, L])
+        _sig(lib, "orc_md5_u2", None, [U, U, P])
+        _sig(lib, "orc_erfinv", D, [D])
+        _sig(lib, "orc_bsdf_queries_f", None, [L, L, L, P, P, F, P, P, P, P, I])
+        _sig(lib, "orc_bsdf_queries_d", None, [L, L, L, P, P, F, P, P, P, P, I])
+        _sig(lib, "orc_c1_make_inputs", None, [L, L, P, P])
+        _sig(lib, "orc_sample_visible_normal_f", None, [P, P, F, F, F, F, U, P])
+        _sig(lib, "orc_sample_visible_normal_d", None, [P, P, F, F, F, F, U, P])
+        _sig(lib, "orc_eval_visible_normal_f", F, [P, P, P, F, F, U])
+        _sig(lib, "orc_sample_normal_f", None, [P, F, F, F, U, P])
+        _sig(lib, "orc_masking_G1_f", F, [P, P, P, F, U])
+        _sig(lib, "orc_masking_G1_aniso_f", F, [P, P, P, F, F, U])
+        _sig(lib, "orc_eval_bsdf_f", F, [P, P, P, F, F, U])
+        _sig(lib, "orc_eval_bsdf_d", D, [P, P, P, F, F, U])
+        _sig(lib, "orc_fresnel_R_vec_f", F, [P, P, F])
+        _sig(lib, "orc_fresnel_complex_f", None, [P, P, P, P])
+        _sig(lib, "orc_fresnel_complex_d", None, [P, P, P, P])
+        _sig(lib, "orc_complex_recip_f", None, [P, P])
+        _sig(lib, "orc_ms_dielectric_eval_f", F, [P, P, P, F, F, F, P, U, U])
+        _sig(lib, "orc_ms_dielectric_eval_d", D, [P, P, P, F, F, F, P, U, U])
+        _sig(lib, "orc_ms_dielectric_sample_f", None, [P, P, F, F, F, P, P, U, P])
+        _sig(lib, "orc_ms_conductor_eval_f", None, [P, P, P, P, F, F, P, U, U, P])
+        _sig(lib, "orc_ms_conductor_sample_f", None, [P, P, P, F, F, P, P, U, P, P])
+        _sig(lib, "orc_ms_diffuse_eval_f", None, [P, P, P, F, F, P, U, P, U, P])
+        _sig(lib, "orc_ms_diffuse_sample_f", None, [P, P, F, F, P, P, P, U, P, P])
+        _sig(lib, "orc_sample_cosine_weighted_f", None, [P, P, P])
+        _sig(lib, "orc_sample_barycentric_f", None, [P, P])
+        _sig(lib, "orc_create_onb_f", None, [P, P, P])
+        _sig(lib, "orc_direct_illumination_f", None, [P, P, L, P, L, L, P, P, P, P])
+        _sig(lib, "orc_C_phi_f", F, [F])
+        _sig(lib, "orc_C_E_f", F, [F])
+        _orc = lib
+    return _orc
+
+
+def c1_inputs(n, first=0):
+    """Synthetic BSDF-query inputs (SoA wo[3][n], alpha[n]) from the oracle's generator."""
+    wo = np.empty((3, n), np.float32)
+    alpha = np.empty(n, np.float32)
+    orc().orc_c1_make_inputs(n, first, fp(wo), fp(alpha))
+    return wo, alpha
+
+
+def bsdf_queries(n, first, n_ggx_below, wo, alpha, eta=1.0 / 1.5, fp64=False, threads=1, which="orc"):
+    """Run the config-1 query batch on the CPU: returns (wi[3][n], f, pdf, F)."""
+    dt = np.float64 if fp64 else np.float32
+    wi = np.empty((3, n), dt)
+    f = np.empty(n, dt)
+    pdf = np.empty(n, dt)
+    F_ = np.empty(n, dt)
+    if which == "ref":
+        assert not fp64
+        ref().ref_bsdf_queries(n, first, n_ggx_below, fp(wo), fp(alpha), eta, fp(wi), fp(f), fp(pdf), fp(F_))
+    elif fp64:
+        orc().orc_bsdf_queries_d(n, first, n_ggx_below, fp(wo), fp(alpha), eta, fp(wi), fp(f), fp(pdf), fp(F_), threads)
+    else:
+        orc().orc_bsdf_queries_f(n, first, n_ggx_below, fp(wo), fp(alpha), eta, fp(wi), fp(f), fp(pdf), fp(F_), threads)
+    return wi, f, pdf, F_
