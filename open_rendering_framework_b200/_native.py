@@ -1,0 +1,90 @@
+"""ctypes binding of the C ABI in include/orf_b200.h (library: libpt_b200.so in this package).
+
+This is the binding a Python caller of the reference-facing boundary uses; it is also what the
+tests and the benchmark call.  There is no fallback: if the compiled library is missing the
+import of any entry point raises ``NativeLibraryMissing``.
+"""
+import ctypes
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpt_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "orf_b200.h")
+
+P = ctypes.c_void_p
+U32 = ctypes.c_uint32
+U64 = ctypes.c_uint64
+I32 = ctypes.c_int
+F32 = ctypes.c_float
+
+STATUS_NAMES = {
+    0: "PT_OK",
+    1: "PT_INVALID_ARG",
+    2: "PT_OOM",
+    3: "PT_CUDA_ERROR",
+    4: "PT_DEVICE_TIMEOUT",
+    5: "PT_CAP_EXCEEDED",
+    6: "PT_NOT_READY",
+}
+
+
+class NativeLibraryMissing(RuntimeError):
+    pass
+
+
+class PtError(RuntimeError):
+    def __init__(self, status, where, message):
+        self.status = status
+        super().__init__("%s failed: %s (%s)" % (where, STATUS_NAMES.get(status, status), message))
+
+
+# name -> (restype, argtypes).  Every function declared in include/orf_b200.h appears here; the
+# CPU test suite checks both directions.
+SIGNATURES = {
+    "pt_last_error_message": (ctypes.c_char_p, []),
+    "pt_version": (I32, []),
+    "pt_kernel_launch_count": (U64, []),
+    "pt_bsdf_queries": (I32, [P, P, U64, U64, U64, F32, P, P, P, P, P]),
+    "pt_bsdf_queries_host": (I32, [P, P, U64, U64, U64, F32, P, P, P, P]),
+    "pt_c1_make_inputs": (I32, [U64, U64, P, P]),
+    "pt_rng_streams": (I32, [I32, P, U64, U32, P, P]),
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded C-ABI library (raises NativeLibraryMissing if it was never built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise NativeLibraryMissing(
+                "%s is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'`" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status, where):
+    """Raise PtError unless status is PT_OK."""
+    if status != 0:
+        msg = lib().pt_last_error_message()
+        raise PtError(status, where, msg.decode() if msg else "")
+    return status
+
+
+def call(name, *args):
+    """Call an entry point by name and raise on a non-OK status."""
+    return check(getattr(lib(), name)(*args), name)
+
+
+def declared_functions():
+    """Names of the functions declared in include/orf_b200.h."""
+    text = open(HEADER_PATH).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pt_[a-z0-9_]+)\s*\(", text)))

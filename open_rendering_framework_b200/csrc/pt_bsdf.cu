@@ -1,0 +1,138 @@
+// Config-1 kernel: batched microfacet BSDF queries (sample visible normal, Walter BSDF value,
+// sampling pdf, Fresnel term) and the RNG-stream kernels used for bit-exact stream parity.
+//
+// Layout: structure-of-arrays, 16 B read (wo.xyz + alpha) and 24 B written (wi.xyz, f, pdf, F) per
+// query, all coalesced.  The kernel is ALU-bound (16-round TEA, transcendentals, the Beckmann
+// Newton loop in double/float), so it runs a grid-stride loop over a grid sized to a multiple of the
+// SM count; queries are ordered GGX-then-Beckmann, so warps never mix distributions except at the
+// single boundary warp.
+#include <vector>
+
+#include "pt_common.cuh"
+#include "pt_math.cuh"
+
+namespace pt {
+
+__device__ unsigned long long g_bsdf_capped = 0;
+
+__global__ void __launch_bounds__(256) k_bsdf_queries(const float* __restrict__ wo_soa, const float* __restrict__ alpha, uint64_t n,
+                                                      uint64_t first, uint64_t n_ggx_below, float eta, float* __restrict__ wi_soa,
+                                                      float* __restrict__ f_out, float* __restrict__ pdf_out, float* __restrict__ F_out)
+{
+  const float3 nrm = f3(0.0f, 0.0f, 1.0f);
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t i = first + k;
+    uint32_t s = tea16((uint32_t)i, 0u);
+    float u1 = rnd_tea(s);
+    float u2 = rnd_tea(s);
+    uint32_t dist = (i < n_ggx_below) ? GGX : BECKMANN;
+    float3 wo = f3(__ldg(wo_soa + k), __ldg(wo_soa + n + k), __ldg(wo_soa + 2 * n + k));
+    float a = __ldg(alpha + k);
+    int capped = 0;
+    float3 m = sample_visible_normal(dist, wo, nrm, a, a, u1, u2, &capped);
+    float3 wi = reflect(-wo, m);
+    f_out[k] = walter_bsdf(dist, wo, wi, nrm, a, eta);
+    pdf_out[k] = eval_visible_normal(dist, wo, m, nrm, a, a) / (4.0f * fabsf(dot(wo, m)));
+    F_out[k] = fresnel_R(wo, m, eta);
+    wi_soa[k] = wi.x;
+    wi_soa[n + k] = wi.y;
+    wi_soa[2 * n + k] = wi.z;
+    if (capped) atomicAdd(&g_bsdf_capped, 1ull);
+  }
+}
+
+__global__ void k_rng_streams(int kind, uint32_t* seeds, uint64_t n, uint32_t draws, float* out)
+{
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
+    float* o = out + k * draws;
+    if (kind == 2) {
+      uint2 s = make_uint2(seeds[2 * k], seeds[2 * k + 1]);
+      for (uint32_t j = 0; j < draws; ++j) o[j] = rnd_md5(s);
+      seeds[2 * k] = s.x;
+      seeds[2 * k + 1] = s.y;
+    } else {
+      uint32_t s = seeds[k];
+      if (kind == 0)
+        for (uint32_t j = 0; j < draws; ++j) o[j] = rnd_tea(s);
+      else
+        for (uint32_t j = 0; j < draws; ++j) o[j] = rnd_lcg(s);
+      seeds[k] = s;
+    }
+  }
+}
+
+}  // namespace pt
+
+using namespace pt;
+
+extern "C" {
+
+pt_status pt_bsdf_queries(const float* d_wo_soa, const float* d_alpha, uint64_t n, uint64_t first_index, uint64_t n_ggx_below, float eta,
+                          float* d_wi_soa, float* d_f, float* d_pdf, float* d_F, void* stream)
+{
+  if (n == 0) return PT_OK;
+  if (!d_wo_soa || !d_alpha || !d_wi_soa || !d_f || !d_pdf || !d_F) return fail(PT_INVALID_ARG, "pt_bsdf_queries: null pointer");
+  if (!(eta > 0.0f)) return fail(PT_INVALID_ARG, "pt_bsdf_queries: eta must be > 0");
+  const int block = 256;
+  int grid = grid_for(n, block, 8);
+  k_bsdf_queries<<<grid, block, 0, (cudaStream_t)stream>>>(d_wo_soa, d_alpha, n, first_index, n_ggx_below, eta, d_wi_soa, d_f, d_pdf, d_F);
+  count_launch();
+  PT_CHECK_CUDA(cudaGetLastError(), "pt_bsdf_queries launch");
+  return PT_OK;
+}
+
+pt_status pt_bsdf_queries_host(const float* wo_soa, const float* alpha, uint64_t n, uint64_t first_index, uint64_t n_ggx_below, float eta,
+                               float* wi_soa, float* f, float* pdf, float* F)
+{
+  if (n == 0) return PT_OK;
+  if (!wo_soa || !alpha || !wi_soa || !f || !pdf || !F) return fail(PT_INVALID_ARG, "pt_bsdf_queries_host: null pointer");
+  float* d = nullptr;
+  size_t bytes = (size_t)n * 10 * sizeof(float);
+  PT_CHECK_CUDA(cudaMalloc(&d, bytes), "pt_bsdf_queries_host cudaMalloc");
+  float *d_wo = d, *d_a = d + 3 * n, *d_wi = d + 4 * n, *d_f = d + 7 * n, *d_pdf = d + 8 * n, *d_F = d + 9 * n;
+  pt_status st = PT_OK;
+  cudaError_t e = cudaMemcpy(d_wo, wo_soa, 3 * n * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_a, alpha, n * sizeof(float), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) st = cuda_status(e, "pt_bsdf_queries_host H2D");
+  if (st == PT_OK) st = pt_bsdf_queries(d_wo, d_a, n, first_index, n_ggx_below, eta, d_wi, d_f, d_pdf, d_F, nullptr);
+  if (st == PT_OK) {
+    e = cudaMemcpy(wi_soa, d_wi, 3 * n * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(f, d_f, n * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(pdf, d_pdf, n * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(F, d_F, n * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) st = cuda_status(e, "pt_bsdf_queries_host D2H");
+  }
+  cudaFree(d);
+  return st;
+}
+
+pt_status pt_c1_make_inputs(uint64_t n, uint64_t first_index, float* wo_soa, float* alpha)
+{
+  if (n && (!wo_soa || !alpha)) return fail(PT_INVALID_ARG, "pt_c1_make_inputs: null pointer");
+  for (uint64_t k = 0; k < n; ++k) {
+    uint32_t s = tea16((uint32_t)(first_index + k), 1u);
+    float a = 0.05f + 0.95f * rnd_tea(s);
+    float ct = 0.01f + 0.99f * rnd_tea(s);
+    float phi = 2.0f * kPi * rnd_tea(s);
+    float st = sqrtf(1.0f - ct * ct);
+    alpha[k] = a;
+    wo_soa[k] = st * cosf(phi);
+    wo_soa[n + k] = st * sinf(phi);
+    wo_soa[2 * n + k] = ct;
+  }
+  return PT_OK;
+}
+
+pt_status pt_rng_streams(int kind, uint32_t* d_seeds, uint64_t n, uint32_t draws, float* d_out, void* stream)
+{
+  if (kind < 0 || kind > 2) return fail(PT_INVALID_ARG, "pt_rng_streams: kind must be 0, 1 or 2");
+  if (n == 0) return PT_OK;
+  if (!d_seeds || !d_out) return fail(PT_INVALID_ARG, "pt_rng_streams: null pointer");
+  int grid = grid_for(n, 256, 8);
+  k_rng_streams<<<grid, 256, 0, (cudaStream_t)stream>>>(kind, d_seeds, n, draws, d_out);
+  count_launch();
+  PT_CHECK_CUDA(cudaGetLastError(), "pt_rng_streams launch");
+  return PT_OK;
+}
+
+}  // extern "C"

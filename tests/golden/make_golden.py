@@ -1,0 +1,123 @@
+"""Generate the golden vectors in tests/golden/ref_math.npz from the reference itself.
+
+The reference has no tests or fixtures of its own, so its own device-math headers, compiled for
+the host from the reference sources (oracle/_ref/libref_oracle.so, built by oracle/Makefile),
+produce the vectors.  Inputs are seeded numpy draws; every output is whatever the reference code
+returns for them.  Run from the repository root:  python tests/golden/make_golden.py
+"""
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from oracle import oracle_ctypes as oc  # noqa: E402
+
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_math.npz")
+
+
+def unit_vectors(rng, n, upper=True):
+    v = rng.normal(size=(n, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    if upper:
+        v[:, 2] = np.abs(v[:, 2]) + 1e-3
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+    return v.astype(np.float32)
+
+
+def main():
+    R = oc.ref()
+    if R is None:
+        raise SystemExit("oracle/_ref/libref_oracle.so is not built (needs the reference sources)")
+    rng = np.random.default_rng(20261203)
+    g = {}
+
+    # RNG streams (random.h): 64 seeds x 32 draws each.
+    seeds = rng.integers(0, 2**32, size=64, dtype=np.uint64).astype(np.uint32)
+    g["rng_seeds"] = seeds
+    for kind, fn in (("tea", R.ref_rnd_tea_stream), ("lcg", R.ref_rnd_lcg_stream)):
+        out = np.empty((64, 32), np.float32)
+        fin = np.empty(64, np.uint32)
+        for k, s in enumerate(seeds):
+            row = np.empty(32, np.float32)
+            fin[k] = fn(int(s), oc.fp(row), 32)
+            out[k] = row
+        g["rng_%s" % kind] = out
+        g["rng_%s_final" % kind] = fin
+    md5 = np.empty((64, 32), np.float32)
+    md5_final = np.empty((64, 2), np.uint32)
+    for k in range(64):
+        x = ctypes.c_uint(int(seeds[k]))
+        y = ctypes.c_uint(int(seeds[(k + 1) % 64]))
+        row = np.empty(32, np.float32)
+        R.ref_rnd_md5_stream(ctypes.byref(x), ctypes.byref(y), oc.fp(row), 32)
+        md5[k] = row
+        md5_final[k] = (x.value, y.value)
+    g["rng_md5"] = md5
+    g["rng_md5_final"] = md5_final
+    tea_ab = rng.integers(0, 2**32, size=(256, 2), dtype=np.uint64).astype(np.uint32)
+    g["tea16_in"] = tea_ab
+    g["tea16_out"] = np.array([R.ref_tea16(int(a), int(b)) for a, b in tea_ab], np.uint32)
+
+    # Config-1 BSDF queries: 4096 queries, first half GGX, from the synthetic generator.
+    n = 4096
+    wo, alpha = oc.c1_inputs(n)
+    wi, f, pdf, F = oc.bsdf_queries(n, 0, n // 2, wo, alpha, which="ref")
+    g.update(c1_wo=wo, c1_alpha=alpha, c1_wi=wi, c1_f=f, c1_pdf=pdf, c1_F=F)
+
+    # Multiscattering walks (Microfacet.h:95-177), shading normal +z, both distributions.
+    m = 256
+    nrm = np.array([0, 0, 1], np.float32)
+    ms_wi = unit_vectors(rng, m)
+    ms_wo = unit_vectors(rng, m, upper=False)
+    ms_alpha = rng.uniform(0.05, 1.0, m).astype(np.float32)
+    ms_seed = rng.integers(0, 2**32, size=m, dtype=np.uint64).astype(np.uint32)
+    ms_dist = (np.arange(m) % 2).astype(np.uint32)
+    eta6 = np.array([0.2, 3.9, 0.55, 3.15, 0.9, 2.4], np.float64)
+    inv = np.empty(6, np.float64)
+    R.ref_complex_recip(oc.fp(eta6), oc.fp(inv))
+    g.update(ms_wi=ms_wi, ms_wo=ms_wo, ms_alpha=ms_alpha, ms_seed=ms_seed, ms_dist=ms_dist, cond_ior=eta6, cond_eta=inv)
+    diel = np.empty(m, np.float32)
+    diel_seed = np.empty(m, np.uint32)
+    cond = np.empty((m, 3), np.float32)
+    cond_seed = np.empty(m, np.uint32)
+    diff = np.empty((m, 3), np.float32)
+    diff_seed = np.empty(m, np.uint32)
+    rho = np.array([0.7, 0.5, 0.3], np.float32)
+    for k in range(m):
+        s = ctypes.c_uint(int(ms_seed[k]))
+        diel[k] = R.ref_ms_dielectric_eval(oc.fp(ms_wi[k]), oc.fp(ms_wo[k]), oc.fp(nrm), 1.0 / 1.5, ms_alpha[k], ms_alpha[k],
+                                           ctypes.byref(s), 0, int(ms_dist[k]))
+        diel_seed[k] = s.value
+        s = ctypes.c_uint(int(ms_seed[k]))
+        out = np.empty(3, np.float32)
+        R.ref_ms_conductor_eval(oc.fp(ms_wi[k]), oc.fp(np.abs(ms_wo[k]).astype(np.float32)), oc.fp(nrm), oc.fp(inv), ms_alpha[k], ms_alpha[k],
+                                ctypes.byref(s), 0, int(ms_dist[k]), oc.fp(out))
+        cond[k] = out
+        cond_seed[k] = s.value
+        s = ctypes.c_uint(int(ms_seed[k]))
+        R.ref_ms_diffuse_eval(oc.fp(ms_wi[k]), oc.fp(np.abs(ms_wo[k]).astype(np.float32)), oc.fp(nrm), ms_alpha[k], ms_alpha[k],
+                              ctypes.byref(s), 0, oc.fp(rho), int(ms_dist[k]), oc.fp(out))
+        diff[k] = out
+        diff_seed[k] = s.value
+    g.update(ms_diel=diel, ms_diel_seed=diel_seed, ms_cond=cond, ms_cond_seed=cond_seed, ms_diff=diff, ms_diff_seed=diff_seed,
+             ms_rho=rho)
+
+    # Conductor Fresnel with complex IOR (Fresnel.h:78-91).
+    fw = unit_vectors(rng, m)
+    fm = unit_vectors(rng, m)
+    fc = np.empty((m, 3), np.float32)
+    for k in range(m):
+        out = np.empty(3, np.float32)
+        R.ref_fresnel_complex(oc.fp(fw[k]), oc.fp(fm[k]), oc.fp(inv), oc.fp(out))
+        fc[k] = out
+    g.update(fc_wi=fw, fc_m=fm, fc_out=fc)
+
+    np.savez_compressed(OUT, **g)
+    print("wrote", OUT, os.path.getsize(OUT), "bytes")
+
+
+if __name__ == "__main__":
+    main()

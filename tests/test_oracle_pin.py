@@ -1,0 +1,145 @@
+"""Pins the oracle restatement (oracle/liboracle.so) to the reference.
+
+Every check is bit-exact in FP32: the restatement keeps the reference's operation order and its
+float/double promotions, and both are built with g++ without contraction.  The vectors in
+tests/golden/ref_math.npz were produced by the reference's own headers compiled for the host
+(tests/golden/make_golden.py); where that compiled reference is present it is also checked
+directly on fresh inputs.
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle_ctypes as oc
+
+GOLD = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_math.npz"))
+
+
+def bits_equal(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    same = a.view(np.uint32) == b.view(np.uint32)
+    return bool(np.all(same | (np.isnan(a) & np.isnan(b))))
+
+
+def test_tea16_golden():
+    O = oc.orc()
+    got = np.array([O.orc_tea16(int(a), int(b)) for a, b in GOLD["tea16_in"]], np.uint32)
+    assert np.array_equal(got, GOLD["tea16_out"])
+    assert O.orc_tea16(12345, 0) == 0x5DF0BA3F
+
+
+@pytest.mark.parametrize("kind", ["tea", "lcg"])
+def test_rng_stream_golden(kind):
+    O = oc.orc()
+    fn = O.orc_rnd_tea_stream if kind == "tea" else O.orc_rnd_lcg_stream
+    for k, s in enumerate(GOLD["rng_seeds"]):
+        row = np.empty(32, np.float32)
+        fin = fn(int(s), oc.fp(row), 32)
+        assert fin == GOLD["rng_%s_final" % kind][k]
+        assert bits_equal(row, GOLD["rng_%s" % kind][k])
+
+
+def test_md5_stream_golden():
+    O = oc.orc()
+    seeds = GOLD["rng_seeds"]
+    for k in range(64):
+        x = ctypes.c_uint(int(seeds[k]))
+        y = ctypes.c_uint(int(seeds[(k + 1) % 64]))
+        row = np.empty(32, np.float32)
+        O.orc_rnd_md5_stream(ctypes.byref(x), ctypes.byref(y), oc.fp(row), 32)
+        assert bits_equal(row, GOLD["rng_md5"][k])
+        assert (x.value, y.value) == tuple(GOLD["rng_md5_final"][k])
+
+
+def test_c1_inputs_and_queries_golden():
+    n = GOLD["c1_alpha"].size
+    wo, alpha = oc.c1_inputs(n)
+    assert bits_equal(wo, GOLD["c1_wo"]) and bits_equal(alpha, GOLD["c1_alpha"])
+    wi, f, pdf, F = oc.bsdf_queries(n, 0, n // 2, wo, alpha)
+    assert bits_equal(wi, GOLD["c1_wi"])
+    assert bits_equal(f, GOLD["c1_f"])
+    assert bits_equal(pdf, GOLD["c1_pdf"])
+    assert bits_equal(F, GOLD["c1_F"])
+
+
+def test_multiscatter_golden():
+    O = oc.orc()
+    nrm = np.array([0, 0, 1], np.float32)
+    inv = GOLD["cond_eta"]
+    rho = GOLD["ms_rho"]
+    for k in range(GOLD["ms_alpha"].size):
+        wi, wo, a, d = GOLD["ms_wi"][k], GOLD["ms_wo"][k], float(GOLD["ms_alpha"][k]), int(GOLD["ms_dist"][k])
+        s = ctypes.c_uint(int(GOLD["ms_seed"][k]))
+        v = O.orc_ms_dielectric_eval_f(oc.fp(wi), oc.fp(wo), oc.fp(nrm), 1.0 / 1.5, a, a, ctypes.byref(s), 0, d)
+        assert bits_equal(np.float32(v), GOLD["ms_diel"][k]) and s.value == GOLD["ms_diel_seed"][k], k
+        wo_up = np.abs(wo).astype(np.float32)
+        s = ctypes.c_uint(int(GOLD["ms_seed"][k]))
+        out = np.empty(3, np.float32)
+        O.orc_ms_conductor_eval_f(oc.fp(wi), oc.fp(wo_up), oc.fp(nrm), oc.fp(inv), a, a, ctypes.byref(s), 0, d, oc.fp(out))
+        assert bits_equal(out, GOLD["ms_cond"][k]) and s.value == GOLD["ms_cond_seed"][k], k
+        s = ctypes.c_uint(int(GOLD["ms_seed"][k]))
+        O.orc_ms_diffuse_eval_f(oc.fp(wi), oc.fp(wo_up), oc.fp(nrm), a, a, ctypes.byref(s), 0, oc.fp(rho), d, oc.fp(out))
+        assert bits_equal(out, GOLD["ms_diff"][k]) and s.value == GOLD["ms_diff_seed"][k], k
+
+
+def test_conductor_fresnel_golden():
+    O = oc.orc()
+    inv = np.empty(6, np.float64)
+    O.orc_complex_recip_f(oc.fp(GOLD["cond_ior"]), oc.fp(inv))
+    assert np.array_equal(inv, GOLD["cond_eta"])
+    for k in range(GOLD["fc_wi"].shape[0]):
+        out = np.empty(3, np.float32)
+        O.orc_fresnel_complex_f(oc.fp(GOLD["fc_wi"][k]), oc.fp(GOLD["fc_m"][k]), oc.fp(inv), oc.fp(out))
+        assert bits_equal(out, GOLD["fc_out"][k]), k
+
+
+@pytest.mark.skipif(oc.ref() is None, reason="compiled reference (oracle/_ref) not built")
+def test_fresh_queries_against_compiled_reference():
+    n = 1 << 15
+    wo, alpha = oc.c1_inputs(n, first=12345)
+    for n_ggx in (n, 0):
+        a = oc.bsdf_queries(n, 12345, 12345 + n_ggx, wo, alpha, which="ref")
+        b = oc.bsdf_queries(n, 12345, 12345 + n_ggx, wo, alpha)
+        for x, y in zip(a, b):
+            assert bits_equal(x, y)
+
+
+@pytest.mark.skipif(oc.ref() is None, reason="compiled reference (oracle/_ref) not built")
+def test_fresh_pieces_against_compiled_reference():
+    R, O = oc.ref(), oc.orc()
+    rng = np.random.default_rng(7)
+    for _ in range(2000):
+        n = rng.normal(size=3).astype(np.float32)
+        n /= np.linalg.norm(n)
+        n = n.astype(np.float32)
+        v = rng.normal(size=3).astype(np.float32)
+        v = (v / np.linalg.norm(v)).astype(np.float32)
+        m = rng.normal(size=3).astype(np.float32)
+        m = (m / np.linalg.norm(m)).astype(np.float32)
+        a = np.float32(rng.uniform(0.02, 1.0))
+        z1, z2 = np.float32(rng.uniform()), np.float32(rng.uniform())
+        for d in (0, 1):
+            o1, o2 = np.empty(3, np.float32), np.empty(3, np.float32)
+            R.ref_sample_normal(oc.fp(n), z1, z2, a, d, oc.fp(o1))
+            O.orc_sample_normal_f(oc.fp(n), z1, z2, a, d, oc.fp(o2))
+            assert bits_equal(o1, o2)
+            R.ref_sample_visible_normal(oc.fp(v), oc.fp(n), a, a, z1, z2, d, oc.fp(o1))
+            O.orc_sample_visible_normal_f(oc.fp(v), oc.fp(n), a, a, z1, z2, d, oc.fp(o2))
+            assert bits_equal(o1, o2)
+            assert bits_equal(np.float32(R.ref_masking_G1(oc.fp(v), oc.fp(m), oc.fp(n), a, d)),
+                              np.float32(O.orc_masking_G1_f(oc.fp(v), oc.fp(m), oc.fp(n), a, d)))
+            assert bits_equal(np.float32(R.ref_masking_G1_aniso(oc.fp(v), oc.fp(m), oc.fp(n), a, a, d)),
+                              np.float32(O.orc_masking_G1_aniso_f(oc.fp(v), oc.fp(m), oc.fp(n), a, a, d)))
+            assert bits_equal(np.float32(R.ref_eval_visible_normal(oc.fp(v), oc.fp(m), oc.fp(n), a, a, d)),
+                              np.float32(O.orc_eval_visible_normal_f(oc.fp(v), oc.fp(m), oc.fp(n), a, a, d)))
+            assert bits_equal(np.float32(R.ref_eval_bsdf(oc.fp(v), oc.fp(m), oc.fp(n), a, np.float32(1 / 1.5), d)),
+                              np.float32(O.orc_eval_bsdf_f(oc.fp(v), oc.fp(m), oc.fp(n), a, np.float32(1 / 1.5), d)))
+        s1 = ctypes.c_uint(int(rng.integers(0, 2**32)))
+        s2 = ctypes.c_uint(s1.value)
+        o1, o2 = np.empty(3, np.float32), np.empty(3, np.float32)
+        R.ref_sample_cosine_weighted(oc.fp(n), ctypes.byref(s1), oc.fp(o1))
+        O.orc_sample_cosine_weighted_f(oc.fp(n), ctypes.byref(s2), oc.fp(o2))
+        assert bits_equal(o1, o2) and s1.value == s2.value
