@@ -73,6 +73,117 @@ pt_status pt_c1_make_inputs(uint64_t n, uint64_t first_index, float* wo_soa, flo
  * (random.h:134-142; seeds are uint2 pairs, so d_seeds holds 2*n words). */
 pt_status pt_rng_streams(int kind, uint32_t* d_seeds, uint64_t n, uint32_t draws, float* d_out, void* stream);
 
+
+/* ---------------------------------------------------------------- scene objects and rendering
+ * One pt_ctx per scene: it owns every device buffer (geometry, BVH, materials, lights, the float4
+ * accumulation buffer, the wavefront queues) and one CUDA stream. */
+typedef struct pt_ctx pt_ctx;
+
+/* Material types: the values of MaterialType (structs.h:209-225) for the shaders this path
+ * implements, plus the emitter material that TriangleAreaLight attaches (arealight_shader.cu). */
+enum {
+  PT_DIFFUSE_SHADER = 0,           /* diffuse_shader.cu            */
+  PT_ROUGH_TRANSPARENT_SHADER = 3, /* rough_transparent_shader.cu  */
+  PT_METALLIC_SHADER = 4,          /* metallic_shader.cu           */
+  PT_AREA_LIGHT_MATERIAL = 100     /* arealight_shader.cu          */
+};
+/* Microfacet model / normal distribution enums: structs.h:242-261. */
+enum { PT_WALTER_MODEL = 0, PT_VISIBLE_NORMALS_MODEL = 1, PT_MULTISCATTERING_MODEL = 2 };
+enum { PT_BECKMANN_DISTRIBUTION = 0, PT_GGX_DISTRIBUTION = 1 };
+
+/* mtl["diffuse_color"] (DiffuseMaterial.cpp:16). */
+typedef struct pt_diffuse_params { float diffuse_color[3]; } pt_diffuse_params;
+/* mtl["ior"] as MyComplex3 (re, im) per RGB, mtl["roughness"] float2, mtl["microfacet_model"],
+ * mtl["normal_distribution"] (MetallicMaterial.cpp:19-25).  The shader uses eta = 1 / ior. */
+typedef struct pt_metallic_params {
+  double ior[6];
+  float roughness[2];
+  uint32_t microfacet_model;
+  uint32_t normal_distribution;
+} pt_metallic_params;
+/* mtl["ior"], mtl["roughness"], mtl["glass_absorption"], mtl["microfacet_model"],
+ * mtl["normal_distribution"] (RoughTransparentMaterial.cpp:20-28). */
+typedef struct pt_rough_transparent_params {
+  float ior;
+  float roughness;
+  float glass_absorption[3];
+  uint32_t microfacet_model;
+  uint32_t normal_distribution;
+} pt_rough_transparent_params;
+/* gi["radiance"] of a TriangleAreaLight's geometry (Light.cpp:242). */
+typedef struct pt_area_light_params { float radiance[3]; } pt_area_light_params;
+
+/* Counters of the most recent pt_render_frames call. */
+typedef struct pt_render_stats {
+  uint64_t path_samples;    /* camera samples traced (pixels in the patch x frames)           */
+  uint64_t segments;        /* radiance rays traced (closest-hit queries)                     */
+  uint64_t shadow_rays;     /* shadow rays traced (any-hit queries)                           */
+  uint64_t capped_walks;    /* random walks / Newton loops stopped by their iteration cap     */
+  uint64_t clamped_indices; /* light / triangle indices clamped from size to size-1           */
+  float gpu_ms;             /* device time of the call (CUDA events on the context stream)    */
+  float extend_ms;          /* device time spent in the closest-hit (extend) kernel           */
+  uint32_t extend_launches; /* number of extend launches                                      */
+  uint32_t kernel_launches; /* all kernels launched by the call                               */
+} pt_render_stats;
+
+/* Create / destroy a context on CUDA device `device`. */
+pt_status pt_context_create(int device, pt_ctx** out);
+pt_status pt_context_destroy(pt_ctx* ctx);
+/* The context's CUDA stream (cudaStream_t). */
+void* pt_context_stream(pt_ctx* ctx);
+
+/* PathTracer parameters: context["max_depth"], ["scene_epsilon"], ["exception_color"]
+ * (Integrator.cpp:77-93).  rr_start_depth: the diffuse shader's Russian roulette (p = mean albedo,
+ * diffuse_shader.cu:165-184) applies from this depth on; 0 is the reference's behaviour. */
+pt_status pt_set_integrator(pt_ctx* ctx, uint32_t max_depth, float scene_epsilon, const float exception_color[3],
+                            uint32_t rr_start_depth);
+/* PinholeCamera variables eye, U, V, W, patch_origin, patch_dims (Camera.cpp:83-103) and the
+ * launch size; the accumulation buffer is (re)allocated to width x height and cleared. */
+pt_status pt_set_camera(pt_ctx* ctx, const float eye[3], const float U[3], const float V[3], const float W[3], uint32_t width,
+                        uint32_t height, const uint32_t patch_origin[2], const uint32_t patch_dims[2]);
+/* ConstantBackground: context["background_color"] (Background.cpp:13). */
+pt_status pt_set_background_constant(pt_ctx* ctx, const float color[3]);
+/* Create a material of the given type from its parameter struct; returns its id. */
+pt_status pt_material_create(pt_ctx* ctx, uint32_t type, const void* params, size_t params_size, uint32_t* out_id);
+/* Replace the parameters of an existing material (same type); takes effect at the next render. */
+pt_status pt_material_update(pt_ctx* ctx, uint32_t id, const void* params, size_t params_size);
+/* Add a triangle mesh in world space: positions (3 floats per vertex), position indices (3 int32 per
+ * triangle), optional normals (3 floats each) and normal indices (3 int32 per triangle, -1 = none),
+ * one material id for all its triangles (ObjLoader.cpp:278-373 buffers).  Returns the global index
+ * of the mesh's first triangle. */
+pt_status pt_mesh_add(pt_ctx* ctx, const float* positions, uint32_t n_vertices, const int32_t* vindex, uint32_t n_triangles,
+                      const float* normals, uint32_t n_normals, const int32_t* nindex, uint32_t material_id,
+                      uint32_t* out_first_triangle);
+/* light_buffer (LightStruct[], 40 B each) and triangle_light_buffer (TriangleLight[], 92 B each) in
+ * the reference's byte layout (structs.h:42-103, OptixSceneLoader.cpp:284-347). */
+pt_status pt_lights_upload(pt_ctx* ctx, const void* lights, uint32_t n_lights, const void* triangle_lights, uint32_t n_triangle_lights);
+/* Build the BVH over all meshes (binned SAH, BVH2 with child-pair nodes) and upload the scene. */
+pt_status pt_build(pt_ctx* ctx);
+/* Render frames first_frame .. first_frame+n_frames-1 (one camera sample per pixel and frame, seeded
+ * with tea<16>(pixel, frame) as path_tracer.cu:48-51) and fold each into the running mean exactly as
+ * path_tracer.cu:64-68 does, in frame order.  Replaces the integrator_pass launch of
+ * OptixScene::renderScene (OptixScene.cpp:159); asynchronous on the context stream. */
+pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames);
+/* Copy the float4 accumulation buffer (width*height*4 floats, row-major, y up) to host memory. */
+pt_status pt_readback(pt_ctx* ctx, float* host_rgba);
+/* Copy the float4 accumulation buffer into caller-owned device memory (width*height*4 floats). */
+pt_status pt_readback_device(pt_ctx* ctx, float* d_rgba);
+/* Wait for the context's work; returns the first device-side error, if any. */
+pt_status pt_sync(pt_ctx* ctx);
+/* Counters and timings of the last pt_render_frames (synchronizes). */
+pt_status pt_get_render_stats(pt_ctx* ctx, pt_render_stats* out);
+/* Upper bound on paths kept in flight by one wavefront pass (frames are grouped to fit). */
+pt_status pt_set_max_paths_in_flight(pt_ctx* ctx, uint64_t max_paths);
+
+/* ---------------------------------------------------------------- ray queries (BVH parity)
+ * Closest-hit / any-hit queries against the built scene for n rays given as d_orig_tmin
+ * (float4: origin.xyz, tmin) and d_dir_tmax (float4: direction.xyz, tmax).  Closest hit writes the
+ * original triangle index (-1 for a miss), t and the barycentrics (beta, gamma) of the hit; ties in t
+ * go to the lower triangle index.  Any hit writes 1 if some triangle has tmin < t < tmax, else 0. */
+pt_status pt_trace_closest(pt_ctx* ctx, const float* d_orig_tmin, const float* d_dir_tmax, uint32_t n, int32_t* d_prim,
+                           float* d_t, float* d_bary);
+pt_status pt_trace_any(pt_ctx* ctx, const float* d_orig_tmin, const float* d_dir_tmax, uint32_t n, int32_t* d_hit);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

@@ -17,6 +17,7 @@ U32 = ctypes.c_uint32
 U64 = ctypes.c_uint64
 I32 = ctypes.c_int
 F32 = ctypes.c_float
+SZ = ctypes.c_size_t
 
 STATUS_NAMES = {
     0: "PT_OK",
@@ -49,6 +50,25 @@ SIGNATURES = {
     "pt_bsdf_queries_host": (I32, [P, P, U64, U64, U64, F32, P, P, P, P]),
     "pt_c1_make_inputs": (I32, [U64, U64, P, P]),
     "pt_rng_streams": (I32, [I32, P, U64, U32, P, P]),
+    "pt_context_create": (I32, [I32, P]),
+    "pt_context_destroy": (I32, [P]),
+    "pt_context_stream": (P, [P]),
+    "pt_set_integrator": (I32, [P, U32, F32, P, U32]),
+    "pt_set_camera": (I32, [P, P, P, P, P, U32, U32, P, P]),
+    "pt_set_background_constant": (I32, [P, P]),
+    "pt_material_create": (I32, [P, U32, P, SZ, P]),
+    "pt_material_update": (I32, [P, U32, P, SZ]),
+    "pt_mesh_add": (I32, [P, P, U32, P, U32, P, U32, P, U32, P]),
+    "pt_lights_upload": (I32, [P, P, U32, P, U32]),
+    "pt_build": (I32, [P]),
+    "pt_render_frames": (I32, [P, U32, U32]),
+    "pt_readback": (I32, [P, P]),
+    "pt_readback_device": (I32, [P, P]),
+    "pt_sync": (I32, [P]),
+    "pt_get_render_stats": (I32, [P, P]),
+    "pt_set_max_paths_in_flight": (I32, [P, U64]),
+    "pt_trace_closest": (I32, [P, P, P, U32, P, P, P]),
+    "pt_trace_any": (I32, [P, P, P, U32, P]),
 }
 
 _lib = None

@@ -1,0 +1,276 @@
+// BVH construction (host): binned-SAH BVH2 flattened into child-pair nodes with parent links, and
+// triangles reordered into leaf order as Moller-Trumbore records (see pt_scene.cuh for the layout).
+//
+// The reference relies on OptiX's Trbvh/Sbvh builders (OptixSceneLoader.cpp:136,
+// ObjLoader.cpp:387-399), which are not available; this builder only has to produce a valid BVH,
+// because hit results are decided by the triangle test alone (closest t, ties to the lower
+// triangle index), so any valid tree gives the same hits as a brute-force loop.
+//
+// Build: 32 centroid bins per axis, SAH with traversal cost 1.2 and intersection cost 1 per
+// triangle, leaves of at most 8 triangles (15 when forced), object-median splits below depth 48 so
+// the depth stays below the traversal's 64-level trail.  Subtrees with more than 32k triangles are
+// built on separate host threads.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <future>
+#include <memory>
+#include <thread>
+#include <vector>
+
+#include "pt_bvh.h"
+
+namespace pt {
+namespace {
+
+struct Box {
+  float lo[3] = {INFINITY, INFINITY, INFINITY};
+  float hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  void grow(const float* p)
+  {
+    for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], p[k]); hi[k] = std::max(hi[k], p[k]); }
+  }
+  void grow(const Box& b)
+  {
+    for (int k = 0; k < 3; ++k) { lo[k] = std::min(lo[k], b.lo[k]); hi[k] = std::max(hi[k], b.hi[k]); }
+  }
+  float area() const
+  {
+    float d[3];
+    for (int k = 0; k < 3; ++k) d[k] = std::max(0.0f, hi[k] - lo[k]);
+    return 2.0f * (d[0] * d[1] + d[1] * d[2] + d[2] * d[0]);
+  }
+};
+
+struct TriRef {
+  Box box;
+  float c[3];
+};
+
+struct TmpNode {
+  Box box[2];
+  int child_kind[2];  // 0 = internal (node ptr), 1 = leaf
+  std::unique_ptr<TmpNode> node[2];
+  uint32_t first[2], count[2];
+};
+
+constexpr int kBins = 32;
+constexpr int kMaxLeaf = 8;
+constexpr int kForcedMaxLeaf = 15;
+constexpr int kMedianDepth = 48;
+constexpr float kTravCost = 1.2f;
+
+struct Builder {
+  const std::vector<TriRef>& refs;
+  std::vector<uint32_t>& idx;
+  std::atomic<int> max_depth{0};
+  Builder(const std::vector<TriRef>& r, std::vector<uint32_t>& i) : refs(r), idx(i) {}
+
+  Box bounds(uint32_t b, uint32_t e, Box* cbox) const
+  {
+    Box bb, cb;
+    for (uint32_t i = b; i < e; ++i) {
+      const TriRef& t = refs[idx[i]];
+      bb.grow(t.box);
+      cb.grow(t.c);
+    }
+    if (cbox) *cbox = cb;
+    return bb;
+  }
+
+  // Returns the split position (b < mid < e) for [b, e).
+  uint32_t split(uint32_t b, uint32_t e, const Box& cb, int depth, bool& make_leaf)
+  {
+    uint32_t n = e - b;
+    make_leaf = false;
+    int axis = 0;
+    float ext[3];
+    for (int k = 0; k < 3; ++k) ext[k] = cb.hi[k] - cb.lo[k];
+    if (ext[1] > ext[axis]) axis = 1;
+    if (ext[2] > ext[axis]) axis = 2;
+    if (!(ext[axis] > 0.0f)) {  // all centroids coincide: any partition is as good
+      if (n <= (uint32_t)kForcedMaxLeaf) { make_leaf = true; return e; }
+      return b + n / 2;
+    }
+    if (depth >= kMedianDepth) {
+      uint32_t mid = b + n / 2;
+      std::nth_element(idx.begin() + b, idx.begin() + mid, idx.begin() + e,
+                       [&](uint32_t x, uint32_t y) { return refs[x].c[axis] < refs[y].c[axis]; });
+      return mid;
+    }
+    float best_cost = INFINITY;
+    int best_axis = -1, best_bin = -1;
+    for (int a = 0; a < 3; ++a) {
+      if (!(ext[a] > 0.0f)) continue;
+      Box bin_box[kBins];
+      uint32_t bin_cnt[kBins] = {0};
+      float scale = (float)kBins / ext[a];
+      for (uint32_t i = b; i < e; ++i) {
+        const TriRef& t = refs[idx[i]];
+        int bi = std::min(kBins - 1, std::max(0, (int)((t.c[a] - cb.lo[a]) * scale)));
+        bin_cnt[bi]++;
+        bin_box[bi].grow(t.box);
+      }
+      float right_area[kBins];
+      uint32_t right_cnt[kBins];
+      Box acc;
+      uint32_t cnt = 0;
+      for (int i = kBins - 1; i > 0; --i) {
+        acc.grow(bin_box[i]);
+        cnt += bin_cnt[i];
+        right_area[i] = acc.area();
+        right_cnt[i] = cnt;
+      }
+      acc = Box();
+      cnt = 0;
+      for (int i = 0; i < kBins - 1; ++i) {
+        acc.grow(bin_box[i]);
+        cnt += bin_cnt[i];
+        if (cnt == 0 || right_cnt[i + 1] == 0) continue;
+        float cost = acc.area() * (float)cnt + right_area[i + 1] * (float)right_cnt[i + 1];
+        if (cost < best_cost) { best_cost = cost; best_axis = a; best_bin = i; }
+      }
+    }
+    Box all;
+    for (uint32_t i = b; i < e; ++i) all.grow(refs[idx[i]].box);
+    float parent_area = all.area();
+    float leaf_cost = (float)n;
+    float split_cost = parent_area > 0.0f ? kTravCost + best_cost / parent_area : INFINITY;
+    if (best_axis < 0) {
+      if (n <= (uint32_t)kForcedMaxLeaf) { make_leaf = true; return e; }
+      return b + n / 2;
+    }
+    if (n <= (uint32_t)kMaxLeaf && split_cost >= leaf_cost) { make_leaf = true; return e; }
+    float scale = (float)kBins / ext[best_axis];
+    auto it = std::partition(idx.begin() + b, idx.begin() + e, [&](uint32_t x) {
+      int bi = std::min(kBins - 1, std::max(0, (int)((refs[x].c[best_axis] - cb.lo[best_axis]) * scale)));
+      return bi <= best_bin;
+    });
+    uint32_t mid = (uint32_t)(it - idx.begin());
+    if (mid == b || mid == e) mid = b + n / 2;
+    return mid;
+  }
+
+  // Builds the subtree over [b, e) into `slot` of `parent` (child k).
+  void build_child(TmpNode* parent, int k, uint32_t b, uint32_t e, int depth)
+  {
+    Box cb;
+    parent->box[k] = bounds(b, e, &cb);
+    int d = depth;
+    int cur = max_depth.load();
+    while (d > cur && !max_depth.compare_exchange_weak(cur, d)) {}
+    uint32_t n = e - b;
+    bool leaf = false;
+    uint32_t mid = e;
+    if (n <= 1) leaf = true;
+    else mid = split(b, e, cb, depth, leaf);
+    if (leaf) {
+      parent->child_kind[k] = 1;
+      parent->first[k] = b;
+      parent->count[k] = n;
+      return;
+    }
+    parent->child_kind[k] = 0;
+    parent->node[k].reset(new TmpNode());
+    TmpNode* node = parent->node[k].get();
+    if (n > 32768 && depth < 8) {
+      auto fut = std::async(std::launch::async, [=] { build_child(node, 0, b, mid, depth + 1); });
+      build_child(node, 1, mid, e, depth + 1);
+      fut.get();
+    } else {
+      build_child(node, 0, b, mid, depth + 1);
+      build_child(node, 1, mid, e, depth + 1);
+    }
+  }
+};
+
+void flatten(const TmpNode* n, int parent, std::vector<float4>& out, int& index_out)
+{
+  int me = (int)(out.size() / 4);
+  index_out = me;
+  out.resize(out.size() + 4);
+  int child_ref[2];
+  for (int k = 0; k < 2; ++k) {
+    if (n->child_kind[k] == 1) {
+      child_ref[k] = (int)(0x80000000u | (n->first[k] << 4) | n->count[k]);
+    } else {
+      int ci;
+      flatten(n->node[k].get(), me, out, ci);
+      child_ref[k] = ci;
+    }
+  }
+  float4* nd = out.data() + 4 * me;
+  auto box_or_far = [](const Box& b, int k, bool lo) {
+    if (!(b.lo[0] <= b.hi[0])) return 1e30f;  // empty child: a point far outside any ray's reach
+    return lo ? b.lo[k] : b.hi[k];
+  };
+  nd[0] = make_float4(box_or_far(n->box[0], 0, true), box_or_far(n->box[0], 0, false), box_or_far(n->box[0], 1, true),
+                      box_or_far(n->box[0], 1, false));
+  nd[1] = make_float4(box_or_far(n->box[1], 0, true), box_or_far(n->box[1], 0, false), box_or_far(n->box[1], 1, true),
+                      box_or_far(n->box[1], 1, false));
+  nd[2] = make_float4(box_or_far(n->box[0], 2, true), box_or_far(n->box[0], 2, false), box_or_far(n->box[1], 2, true),
+                      box_or_far(n->box[1], 2, false));
+  int4 n3 = make_int4(child_ref[0], child_ref[1], parent, 0);
+  memcpy(&nd[3], &n3, sizeof(n3));
+}
+
+}  // namespace
+
+bool build_bvh(const float* tri_pos, uint32_t n_tris, BvhHost& out)
+{
+  out = BvhHost();
+  if (n_tris >= (1u << 27)) return false;
+  std::vector<TriRef> refs(n_tris);
+  for (uint32_t i = 0; i < n_tris; ++i) {
+    const float* p = tri_pos + 9 * (size_t)i;
+    TriRef& r = refs[i];
+    r.box.grow(p);
+    r.box.grow(p + 3);
+    r.box.grow(p + 6);
+    for (int k = 0; k < 3; ++k) r.c[k] = 0.5f * (r.box.lo[k] + r.box.hi[k]);
+  }
+  std::vector<uint32_t> idx(n_tris);
+  for (uint32_t i = 0; i < n_tris; ++i) idx[i] = i;
+  Builder B(refs, idx);
+  // Root: an internal node whose two children split the triangles; with fewer than two triangles
+  // the second child is an empty leaf.
+  TmpNode root;
+  if (n_tris <= 1) {
+    root.child_kind[0] = 1;
+    root.first[0] = 0;
+    root.count[0] = n_tris;
+    if (n_tris) root.box[0] = B.bounds(0, n_tris, nullptr);
+    root.child_kind[1] = 1;
+    root.first[1] = 0;
+    root.count[1] = 0;
+  } else {
+    Box cb;
+    B.bounds(0, n_tris, &cb);
+    bool leaf = false;
+    uint32_t mid = B.split(0, n_tris, cb, 0, leaf);
+    if (leaf || mid == 0 || mid >= n_tris) mid = n_tris / 2;
+    B.build_child(&root, 0, 0, mid, 1);
+    B.build_child(&root, 1, mid, n_tris, 1);
+  }
+  int root_index = 0;
+  flatten(&root, -1, out.nodes, root_index);
+  out.depth = B.max_depth.load() + 1;
+  out.tri_v0.resize(n_tris);
+  out.tri_e1.resize(n_tris);
+  out.tri_e2.resize(n_tris);
+  out.order = idx;
+  for (uint32_t j = 0; j < n_tris; ++j) {
+    uint32_t i = idx[j];
+    const float* p = tri_pos + 9 * (size_t)i;
+    int orig = (int)i;
+    float w;
+    memcpy(&w, &orig, 4);
+    out.tri_v0[j] = make_float4(p[0], p[1], p[2], w);
+    out.tri_e1[j] = make_float4(p[3] - p[0], p[4] - p[1], p[5] - p[2], 0.0f);
+    out.tri_e2[j] = make_float4(p[6] - p[0], p[7] - p[1], p[8] - p[2], 0.0f);
+  }
+  return out.depth < 64;
+}
+
+}  // namespace pt

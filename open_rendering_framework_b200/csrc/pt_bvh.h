@@ -1,0 +1,21 @@
+// Host BVH builder interface (implementation in pt_bvh.cu; layout documented in pt_scene.cuh).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+namespace pt {
+
+struct BvhHost {
+  std::vector<float4> nodes;                 // 4 float4 per node, root = node 0
+  std::vector<float4> tri_v0, tri_e1, tri_e2;  // leaf order
+  std::vector<uint32_t> order;               // leaf position -> original triangle index
+  int depth = 0;                             // levels including the leaves
+};
+
+// tri_pos: 9 floats per triangle (v0, v1, v2).  Returns false if the scene is too large for the
+// node encoding (2^27 triangles) or the tree is deeper than the traversal trail allows.
+bool build_bvh(const float* tri_pos, uint32_t n_tris, BvhHost& out);
+
+}  // namespace pt

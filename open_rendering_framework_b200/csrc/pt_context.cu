@@ -1,0 +1,418 @@
+// C ABI: context lifetime, scene objects (integrator, camera, background, materials, meshes,
+// lights), BVH build and upload, readback, and the closest/any-hit query kernels.
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "pt_bvh.h"
+#include "pt_context.h"
+
+namespace pt {
+
+SceneDev Context::view() const
+{
+  SceneDev s;
+  s.nodes = d_nodes.as<float4>();
+  s.tri_v0 = d_v0.as<float4>();
+  s.tri_e1 = d_e1.as<float4>();
+  s.tri_e2 = d_e2.as<float4>();
+  s.tri_info = d_info.as<int4>();
+  s.normals = d_normals.as<float4>();
+  s.mats = d_mats.as<MatDev>();
+  s.lights = d_lights.as<LightRaw>();
+  s.tri_lights = d_tri_lights.as<TriLightRaw>();
+  s.n_lights = (int)lights.size();
+  s.n_tri_lights = (int)tri_lights.size();
+  s.n_tris = n_tris;
+  s.bg_color = bg_color;
+  s.cam = cam;
+  s.integ = integ;
+  return s;
+}
+
+// 1.0f / MyComplex in the reference's arithmetic (MyComplex.h:155-160 with :18-23): the squared
+// magnitude is powf(float |c|, 2) and the quotient is formed in double.
+static Cx host_recip(const Cx& b)
+{
+  float r = (float)b.re, i = (float)b.im;
+  float ab = sqrtf(r * r + i * i);
+  double den = (double)powf(ab, 2.0f);
+  double s = 1.0 / den;
+  return Cx{((double)1.0f * b.re) * s, ((double)1.0f * -b.im) * s};
+}
+
+static bool finite_nonneg3(const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]) && v[0] >= 0 && v[1] >= 0 && v[2] >= 0; }
+
+static pt_status make_material(uint32_t type, const void* params, size_t size, MatDev& m)
+{
+  memset(&m, 0, sizeof(m));
+  m.type = type;
+  if (!params) return fail(PT_INVALID_ARG, "material: null parameters");
+  switch (type) {
+    case PT_DIFFUSE_SHADER: {
+      if (size != sizeof(pt_diffuse_params)) return fail(PT_INVALID_ARG, "diffuse material: wrong parameter size");
+      const pt_diffuse_params* p = (const pt_diffuse_params*)params;
+      if (!finite_nonneg3(p->diffuse_color)) return fail(PT_INVALID_ARG, "diffuse material: diffuse_color must be finite and >= 0");
+      m.a = make_float4(p->diffuse_color[0], p->diffuse_color[1], p->diffuse_color[2], 0.0f);
+      return PT_OK;
+    }
+    case PT_METALLIC_SHADER: {
+      if (size != sizeof(pt_metallic_params)) return fail(PT_INVALID_ARG, "metallic material: wrong parameter size");
+      const pt_metallic_params* p = (const pt_metallic_params*)params;
+      if (!(p->roughness[0] > 0.0f && p->roughness[1] > 0.0f && std::isfinite(p->roughness[0]) && std::isfinite(p->roughness[1])))
+        return fail(PT_INVALID_ARG, "metallic material: roughness must be finite and > 0");
+      if (p->microfacet_model > PT_MULTISCATTERING_MODEL || p->normal_distribution > PT_GGX_DISTRIBUTION)
+        return fail(PT_INVALID_ARG, "metallic material: bad microfacet_model or normal_distribution");
+      for (int k = 0; k < 6; ++k)
+        if (!std::isfinite(p->ior[k])) return fail(PT_INVALID_ARG, "metallic material: ior must be finite");
+      m.model = p->microfacet_model;
+      m.dist = p->normal_distribution;
+      m.a = make_float4(p->roughness[0], p->roughness[1], 0.0f, 0.0f);
+      for (int c = 0; c < 3; ++c) {
+        Cx ior{p->ior[2 * c], p->ior[2 * c + 1]};
+        if (ior.re == 0.0 && ior.im == 0.0) return fail(PT_INVALID_ARG, "metallic material: ior must be non-zero");
+        m.eta.c[c] = host_recip(ior);
+        m.inv_eta.c[c] = host_recip(m.eta.c[c]);
+      }
+      return PT_OK;
+    }
+    case PT_ROUGH_TRANSPARENT_SHADER: {
+      if (size != sizeof(pt_rough_transparent_params)) return fail(PT_INVALID_ARG, "rough transparent material: wrong parameter size");
+      const pt_rough_transparent_params* p = (const pt_rough_transparent_params*)params;
+      if (!(p->ior > 0.0f && std::isfinite(p->ior))) return fail(PT_INVALID_ARG, "rough transparent material: ior must be > 0");
+      if (!(p->roughness > 0.0f && std::isfinite(p->roughness))) return fail(PT_INVALID_ARG, "rough transparent material: roughness must be > 0");
+      if (!finite_nonneg3(p->glass_absorption)) return fail(PT_INVALID_ARG, "rough transparent material: glass_absorption must be finite and >= 0");
+      if (p->microfacet_model > PT_MULTISCATTERING_MODEL || p->normal_distribution > PT_GGX_DISTRIBUTION)
+        return fail(PT_INVALID_ARG, "rough transparent material: bad microfacet_model or normal_distribution");
+      m.model = p->microfacet_model;
+      m.dist = p->normal_distribution;
+      m.a = make_float4(p->ior, p->roughness, 0.0f, 0.0f);
+      m.b = make_float4(p->glass_absorption[0], p->glass_absorption[1], p->glass_absorption[2], 0.0f);
+      return PT_OK;
+    }
+    case PT_AREA_LIGHT_MATERIAL: {
+      if (size != sizeof(pt_area_light_params)) return fail(PT_INVALID_ARG, "area light material: wrong parameter size");
+      const pt_area_light_params* p = (const pt_area_light_params*)params;
+      if (!finite_nonneg3(p->radiance)) return fail(PT_INVALID_ARG, "area light material: radiance must be finite and >= 0");
+      m.a = make_float4(p->radiance[0], p->radiance[1], p->radiance[2], 0.0f);
+      return PT_OK;
+    }
+    default:
+      return fail(PT_INVALID_ARG, "material: unsupported type " + std::to_string(type));
+  }
+}
+
+template <class T> static pt_status upload(DevBuf& buf, const std::vector<T>& v, cudaStream_t s, const char* what)
+{
+  size_t bytes = v.size() * sizeof(T);
+  pt_status st = buf.reserve(bytes ? bytes : 16, what);
+  if (st != PT_OK) return st;
+  if (bytes) PT_CHECK_CUDA(cudaMemcpyAsync(buf.p, v.data(), bytes, cudaMemcpyHostToDevice, s), what);
+  return PT_OK;
+}
+
+// ------------------------------------------------------------------ query kernels
+__global__ void k_trace_closest(SceneDev S, const float4* ot, const float4* dt, uint32_t n, int32_t* prim, float* tout, float* bary)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float4 a = ot[i], b = dt[i];
+    Hit h = trace_closest(S, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), a.w, b.w);
+    prim[i] = h.prim;
+    tout[i] = h.prim >= 0 ? h.t : -1.0f;
+    bary[2 * i] = h.u;
+    bary[2 * i + 1] = h.v;
+  }
+}
+__global__ void k_trace_any(SceneDev S, const float4* ot, const float4* dt, uint32_t n, int32_t* hit)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float4 a = ot[i], b = dt[i];
+    hit[i] = trace_any(S, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), a.w, b.w) ? 1 : 0;
+  }
+}
+
+}  // namespace pt
+
+using namespace pt;
+
+#define CTX_CHECK(ctx)                                                          \
+  do {                                                                          \
+    if (!(ctx)) return fail(PT_INVALID_ARG, "null context");                    \
+    PT_CHECK_CUDA(cudaSetDevice((ctx)->c.device), "cudaSetDevice");             \
+  } while (0)
+
+extern "C" {
+
+pt_status pt_context_create(int device, pt_ctx** out)
+{
+  if (!out) return fail(PT_INVALID_ARG, "pt_context_create: null output");
+  *out = nullptr;
+  int n = 0;
+  PT_CHECK_CUDA(cudaGetDeviceCount(&n), "cudaGetDeviceCount");
+  if (device < 0 || device >= n) return fail(PT_INVALID_ARG, "pt_context_create: no such device");
+  PT_CHECK_CUDA(cudaSetDevice(device), "cudaSetDevice");
+  pt_ctx* ctx = new (std::nothrow) pt_ctx();
+  if (!ctx) return fail(PT_OOM, "pt_context_create: host allocation");
+  ctx->c.device = device;
+  cudaError_t e = cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->c.ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->c.ev1);
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->c.ext0);
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->c.ext1);
+  if (e != cudaSuccess) {
+    pt_context_destroy(ctx);
+    return cuda_status(e, "pt_context_create");
+  }
+  *out = ctx;
+  return PT_OK;
+}
+
+pt_status pt_context_destroy(pt_ctx* ctx)
+{
+  if (!ctx) return PT_OK;
+  cudaSetDevice(ctx->c.device);
+  if (ctx->c.stream) cudaStreamSynchronize(ctx->c.stream);
+  Context& c = ctx->c;
+  for (cudaEvent_t ev : {c.ev0, c.ev1, c.ext0, c.ext1})
+    if (ev) cudaEventDestroy(ev);
+  cudaStream_t s = c.stream;
+  delete ctx;  // frees device buffers
+  if (s) cudaStreamDestroy(s);
+  return PT_OK;
+}
+
+void* pt_context_stream(pt_ctx* ctx) { return ctx ? (void*)ctx->c.stream : nullptr; }
+
+pt_status pt_set_integrator(pt_ctx* ctx, uint32_t max_depth, float scene_epsilon, const float exception_color[3], uint32_t rr_start_depth)
+{
+  if (!ctx) return fail(PT_INVALID_ARG, "null context");
+  if (max_depth > 1000) return fail(PT_INVALID_ARG, "pt_set_integrator: max_depth must be <= 1000");
+  if (!(scene_epsilon >= 0.0f) || !std::isfinite(scene_epsilon)) return fail(PT_INVALID_ARG, "pt_set_integrator: scene_epsilon must be finite and >= 0");
+  ctx->c.integ.max_depth = (int)max_depth;
+  ctx->c.integ.scene_epsilon = scene_epsilon;
+  ctx->c.integ.rr_start = (int)rr_start_depth;
+  if (exception_color) ctx->c.integ.exception_color = make_float3(exception_color[0], exception_color[1], exception_color[2]);
+  return PT_OK;
+}
+
+pt_status pt_set_camera(pt_ctx* ctx, const float eye[3], const float U[3], const float V[3], const float W[3], uint32_t width,
+                        uint32_t height, const uint32_t patch_origin[2], const uint32_t patch_dims[2])
+{
+  CTX_CHECK(ctx);
+  if (!eye || !U || !V || !W) return fail(PT_INVALID_ARG, "pt_set_camera: null vector");
+  if (width == 0 || height == 0 || (uint64_t)width * height > (1ull << 28)) return fail(PT_INVALID_ARG, "pt_set_camera: bad image size");
+  for (int k = 0; k < 3; ++k)
+    if (!std::isfinite(eye[k]) || !std::isfinite(U[k]) || !std::isfinite(V[k]) || !std::isfinite(W[k]))
+      return fail(PT_INVALID_ARG, "pt_set_camera: non-finite camera vector");
+  Context& c = ctx->c;
+  c.cam.eye = make_float3(eye[0], eye[1], eye[2]);
+  c.cam.U = make_float3(U[0], U[1], U[2]);
+  c.cam.V = make_float3(V[0], V[1], V[2]);
+  c.cam.W = make_float3(W[0], W[1], W[2]);
+  c.cam.patch_origin = patch_origin ? make_uint2(patch_origin[0], patch_origin[1]) : make_uint2(0, 0);
+  c.cam.patch_dims = patch_dims ? make_uint2(patch_dims[0], patch_dims[1]) : make_uint2(width, height);
+  bool resized = c.cam.width != width || c.cam.height != height || !c.d_accum.p;
+  c.cam.width = width;
+  c.cam.height = height;
+  c.camera_set = true;
+  if (resized) {
+    pt_status st = c.d_accum.reserve((size_t)width * height * sizeof(float4), "accumulation buffer");
+    if (st != PT_OK) return st;
+    PT_CHECK_CUDA(cudaMemsetAsync(c.d_accum.p, 0, (size_t)width * height * sizeof(float4), c.stream), "clear accumulation");
+  }
+  return PT_OK;
+}
+
+pt_status pt_set_background_constant(pt_ctx* ctx, const float color[3])
+{
+  if (!ctx || !color) return fail(PT_INVALID_ARG, "pt_set_background_constant: null argument");
+  if (!std::isfinite(color[0]) || !std::isfinite(color[1]) || !std::isfinite(color[2]))
+    return fail(PT_INVALID_ARG, "pt_set_background_constant: non-finite color");
+  ctx->c.bg_color = make_float3(color[0], color[1], color[2]);
+  return PT_OK;
+}
+
+pt_status pt_material_create(pt_ctx* ctx, uint32_t type, const void* params, size_t params_size, uint32_t* out_id)
+{
+  if (!ctx || !out_id) return fail(PT_INVALID_ARG, "pt_material_create: null argument");
+  MatDev m;
+  pt_status st = make_material(type, params, params_size, m);
+  if (st != PT_OK) return st;
+  if (ctx->c.mats.size() >= (1u << 20)) return fail(PT_CAP_EXCEEDED, "pt_material_create: too many materials");
+  *out_id = (uint32_t)ctx->c.mats.size();
+  ctx->c.mats.push_back(m);
+  ctx->c.dirty_materials = true;
+  return PT_OK;
+}
+
+pt_status pt_material_update(pt_ctx* ctx, uint32_t id, const void* params, size_t params_size)
+{
+  if (!ctx) return fail(PT_INVALID_ARG, "null context");
+  if (id >= ctx->c.mats.size()) return fail(PT_INVALID_ARG, "pt_material_update: no such material");
+  MatDev m;
+  pt_status st = make_material(ctx->c.mats[id].type, params, params_size, m);
+  if (st != PT_OK) return st;
+  ctx->c.mats[id] = m;
+  ctx->c.dirty_materials = true;
+  return PT_OK;
+}
+
+pt_status pt_mesh_add(pt_ctx* ctx, const float* positions, uint32_t n_vertices, const int32_t* vindex, uint32_t n_triangles,
+                      const float* normals, uint32_t n_normals, const int32_t* nindex, uint32_t material_id,
+                      uint32_t* out_first_triangle)
+{
+  if (!ctx) return fail(PT_INVALID_ARG, "null context");
+  Context& c = ctx->c;
+  if (n_triangles == 0) return fail(PT_INVALID_ARG, "pt_mesh_add: empty mesh");
+  if (!positions || !vindex) return fail(PT_INVALID_ARG, "pt_mesh_add: null positions or indices");
+  if (material_id >= c.mats.size()) return fail(PT_INVALID_ARG, "pt_mesh_add: unknown material id");
+  if ((uint64_t)c.n_tris + n_triangles >= (1ull << 27)) return fail(PT_CAP_EXCEEDED, "pt_mesh_add: scene exceeds 2^27 triangles");
+  if (n_normals && (!normals || !nindex)) return fail(PT_INVALID_ARG, "pt_mesh_add: normals without normal indices");
+  for (uint64_t k = 0; k < 3ull * n_vertices; ++k)
+    if (!std::isfinite(positions[k])) return fail(PT_INVALID_ARG, "pt_mesh_add: non-finite vertex position");
+  for (uint64_t k = 0; k < 3ull * n_triangles; ++k) {
+    if (vindex[k] < 0 || (uint32_t)vindex[k] >= n_vertices) return fail(PT_INVALID_ARG, "pt_mesh_add: vertex index out of range");
+    if (n_normals && (nindex[k] >= (int32_t)n_normals)) return fail(PT_INVALID_ARG, "pt_mesh_add: normal index out of range");
+  }
+  uint32_t normal_base = (uint32_t)c.normals.size();
+  for (uint32_t k = 0; k < n_normals; ++k)
+    c.normals.push_back(make_float4(normals[3 * k], normals[3 * k + 1], normals[3 * k + 2], 0.0f));
+  if (out_first_triangle) *out_first_triangle = c.n_tris;
+  for (uint32_t t = 0; t < n_triangles; ++t) {
+    for (int k = 0; k < 3; ++k) {
+      const float* p = positions + 3 * (size_t)vindex[3 * t + k];
+      c.tri_pos.push_back(p[0]);
+      c.tri_pos.push_back(p[1]);
+      c.tri_pos.push_back(p[2]);
+    }
+    int4 info = make_int4(-1, -1, -1, (int)material_id);
+    if (n_normals && nindex[3 * t] >= 0 && nindex[3 * t + 1] >= 0 && nindex[3 * t + 2] >= 0) {
+      info.x = (int)normal_base + nindex[3 * t];
+      info.y = (int)normal_base + nindex[3 * t + 1];
+      info.z = (int)normal_base + nindex[3 * t + 2];
+    }
+    c.tri_info.push_back(info);
+  }
+  c.n_tris += n_triangles;
+  c.built = false;
+  return PT_OK;
+}
+
+pt_status pt_lights_upload(pt_ctx* ctx, const void* lights, uint32_t n_lights, const void* triangle_lights, uint32_t n_triangle_lights)
+{
+  if (!ctx) return fail(PT_INVALID_ARG, "null context");
+  if ((n_lights && !lights) || (n_triangle_lights && !triangle_lights)) return fail(PT_INVALID_ARG, "pt_lights_upload: null buffer");
+  Context& c = ctx->c;
+  c.lights.assign((const LightRaw*)lights, (const LightRaw*)lights + n_lights);
+  c.tri_lights.assign((const TriLightRaw*)triangle_lights, (const TriLightRaw*)triangle_lights + n_triangle_lights);
+  for (const LightRaw& l : c.lights) {
+    if (l.type > SPHERICAL_LIGHT) return fail(PT_INVALID_ARG, "pt_lights_upload: unknown light_type");
+    if (l.type == TRIANGLES_AREA_LIGHT) {
+      float cnt, start;
+      memcpy(&cnt, &l.p[0], 4);
+      memcpy(&start, &l.p[1], 4);
+      if (!(cnt >= 1.0f) || !(start >= 0.0f) || (uint64_t)(start + cnt) > n_triangle_lights)
+        return fail(PT_INVALID_ARG, "pt_lights_upload: triangle range of a TrianglesAreaLight is outside triangle_light_buffer");
+    }
+  }
+  PT_CHECK_CUDA(cudaSetDevice(c.device), "cudaSetDevice");
+  pt_status st = upload(c.d_lights, c.lights, c.stream, "light buffer");
+  if (st == PT_OK) st = upload(c.d_tri_lights, c.tri_lights, c.stream, "triangle light buffer");
+  return st;
+}
+
+pt_status pt_build(pt_ctx* ctx)
+{
+  CTX_CHECK(ctx);
+  Context& c = ctx->c;
+  if (c.n_tris == 0) return fail(PT_NOT_READY, "pt_build: no meshes");
+  BvhHost bvh;
+  if (!build_bvh(c.tri_pos.data(), c.n_tris, bvh)) return fail(PT_CAP_EXCEEDED, "pt_build: scene too large or BVH too deep");
+  c.bvh_depth = bvh.depth;
+  pt_status st = upload(c.d_nodes, bvh.nodes, c.stream, "BVH nodes");
+  if (st == PT_OK) st = upload(c.d_v0, bvh.tri_v0, c.stream, "triangles");
+  if (st == PT_OK) st = upload(c.d_e1, bvh.tri_e1, c.stream, "triangles");
+  if (st == PT_OK) st = upload(c.d_e2, bvh.tri_e2, c.stream, "triangles");
+  if (st == PT_OK) st = upload(c.d_info, c.tri_info, c.stream, "triangle info");
+  if (st == PT_OK) st = upload(c.d_normals, c.normals, c.stream, "normals");
+  if (st == PT_OK) st = upload(c.d_mats, c.mats, c.stream, "materials");
+  if (st != PT_OK) return st;
+  if (c.lights.empty()) {
+    // light_buffer of size 0 is legal; keep a valid pointer for the kernels
+    st = c.d_lights.reserve(sizeof(LightRaw), "light buffer");
+    if (st == PT_OK) st = c.d_tri_lights.reserve(sizeof(TriLightRaw), "triangle light buffer");
+    if (st != PT_OK) return st;
+  }
+  PT_CHECK_CUDA(cudaStreamSynchronize(c.stream), "pt_build upload");
+  c.dirty_materials = false;
+  c.geo_stale = true;
+  c.built = true;
+  return PT_OK;
+}
+
+pt_status pt_readback(pt_ctx* ctx, float* host_rgba)
+{
+  CTX_CHECK(ctx);
+  Context& c = ctx->c;
+  if (!host_rgba) return fail(PT_INVALID_ARG, "pt_readback: null buffer");
+  if (!c.camera_set) return fail(PT_NOT_READY, "pt_readback: camera not set");
+  PT_CHECK_CUDA(cudaMemcpyAsync(host_rgba, c.d_accum.p, (size_t)c.cam.width * c.cam.height * sizeof(float4), cudaMemcpyDeviceToHost, c.stream),
+                "pt_readback");
+  PT_CHECK_CUDA(cudaStreamSynchronize(c.stream), "pt_readback");
+  return PT_OK;
+}
+
+pt_status pt_readback_device(pt_ctx* ctx, float* d_rgba)
+{
+  CTX_CHECK(ctx);
+  Context& c = ctx->c;
+  if (!d_rgba) return fail(PT_INVALID_ARG, "pt_readback_device: null buffer");
+  if (!c.camera_set) return fail(PT_NOT_READY, "pt_readback_device: camera not set");
+  PT_CHECK_CUDA(cudaMemcpyAsync(d_rgba, c.d_accum.p, (size_t)c.cam.width * c.cam.height * sizeof(float4), cudaMemcpyDeviceToDevice, c.stream),
+                "pt_readback_device");
+  return PT_OK;
+}
+
+pt_status pt_sync(pt_ctx* ctx)
+{
+  CTX_CHECK(ctx);
+  PT_CHECK_CUDA(cudaStreamSynchronize(ctx->c.stream), "pt_sync");
+  return PT_OK;
+}
+
+pt_status pt_set_max_paths_in_flight(pt_ctx* ctx, uint64_t max_paths)
+{
+  if (!ctx) return fail(PT_INVALID_ARG, "null context");
+  if (max_paths < 1024 || max_paths > (1ull << 30)) return fail(PT_INVALID_ARG, "pt_set_max_paths_in_flight: must be in [1024, 2^30]");
+  ctx->c.max_paths = max_paths;
+  return PT_OK;
+}
+
+pt_status pt_trace_closest(pt_ctx* ctx, const float* d_orig_tmin, const float* d_dir_tmax, uint32_t n, int32_t* d_prim, float* d_t, float* d_bary)
+{
+  CTX_CHECK(ctx);
+  Context& c = ctx->c;
+  if (!c.built) return fail(PT_NOT_READY, "pt_trace_closest: call pt_build first");
+  if (n == 0) return PT_OK;
+  if (!d_orig_tmin || !d_dir_tmax || !d_prim || !d_t || !d_bary) return fail(PT_INVALID_ARG, "pt_trace_closest: null pointer");
+  k_trace_closest<<<grid_for(n, 128, 16), 128, 0, c.stream>>>(c.view(), (const float4*)d_orig_tmin, (const float4*)d_dir_tmax, n, d_prim, d_t, d_bary);
+  count_launch();
+  PT_CHECK_CUDA(cudaGetLastError(), "pt_trace_closest launch");
+  return PT_OK;
+}
+
+pt_status pt_trace_any(pt_ctx* ctx, const float* d_orig_tmin, const float* d_dir_tmax, uint32_t n, int32_t* d_hit)
+{
+  CTX_CHECK(ctx);
+  Context& c = ctx->c;
+  if (!c.built) return fail(PT_NOT_READY, "pt_trace_any: call pt_build first");
+  if (n == 0) return PT_OK;
+  if (!d_orig_tmin || !d_dir_tmax || !d_hit) return fail(PT_INVALID_ARG, "pt_trace_any: null pointer");
+  k_trace_any<<<grid_for(n, 128, 16), 128, 0, c.stream>>>(c.view(), (const float4*)d_orig_tmin, (const float4*)d_dir_tmax, n, d_hit);
+  count_launch();
+  PT_CHECK_CUDA(cudaGetLastError(), "pt_trace_any launch");
+  return PT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,113 @@
+// Host-side context behind the opaque pt_ctx handle of the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "pt_common.cuh"
+#include "pt_scene.cuh"
+
+namespace pt {
+
+// Owning device allocation (cudaMalloc / cudaFree), reused when large enough.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release()
+  {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  // Ensures capacity >= n bytes (contents are not preserved when it grows).
+  pt_status reserve(size_t n, const char* what)
+  {
+    if (n <= bytes && p) return PT_OK;
+    release();
+    if (n == 0) return PT_OK;
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return cuda_status(e, what);
+    }
+    bytes = n;
+    return PT_OK;
+  }
+  template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+// Wavefront buffers, sized for `cap` paths in flight.
+struct Wavefront {
+  uint64_t cap = 0;
+  DevBuf ray_o, ray_d, thr, rad, rng, hit;   // per path
+  DevBuf q_a, q_b;                            // active queues (path ids)
+  DevBuf q_mat;                               // per-material-class queues, kQueues x cap
+  DevBuf sh_o, sh_d, sh_c, sh_pid;            // shadow-ray queue
+  DevBuf counters;                            // kCounters uint32
+};
+
+// Counter slots in Wavefront::counters.
+enum CounterSlot {
+  CNT_ACTIVE_A = 0,
+  CNT_ACTIVE_B = 1,
+  CNT_Q_MISS = 2,
+  CNT_Q_LIGHT = 3,
+  CNT_Q_DIFFUSE = 4,
+  CNT_Q_METAL = 5,
+  CNT_Q_GLASS = 6,
+  CNT_SHADOW = 7,
+  CNT_SEGMENTS_LO = 8,   // 64-bit totals as two words each (atomicAdd on unsigned long long)
+  CNT_SHADOW_TOTAL = 10,
+  CNT_CAPPED = 12,
+  CNT_CLAMPED = 14,
+  CNT_ERROR = 16,
+  kCounters = 32
+};
+enum QueueClass { QC_MISS = 0, QC_LIGHT = 1, QC_DIFFUSE = 2, QC_METAL = 3, QC_GLASS = 4, kQueues = 5 };
+
+struct Context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ext0 = nullptr, ext1 = nullptr;
+
+  IntegratorDev integ{50, 1e-4f, 0, {1.0f, 0.0f, 0.0f}};  // PathTracer defaults (Integrator.cpp:6-24)
+  CameraDev cam{};
+  bool camera_set = false;
+  float3 bg_color{1.0f, 1.0f, 1.0f};                      // ConstantBackground default (Background.cpp:10)
+
+  std::vector<MatDev> mats;
+  // meshes as added (host copies until pt_build)
+  std::vector<float> tri_pos;       // 9 floats per triangle
+  std::vector<int4> tri_info;       // (n0, n1, n2, material)
+  std::vector<float4> normals;
+  std::vector<LightRaw> lights;
+  std::vector<TriLightRaw> tri_lights;
+  bool built = false;
+  bool dirty_materials = true;
+  int bvh_depth = 0;
+  uint32_t n_tris = 0;
+
+  DevBuf d_nodes, d_v0, d_e1, d_e2, d_info, d_normals, d_mats, d_lights, d_tri_lights;
+  DevBuf d_accum;  // float4 per pixel
+  DevBuf d_normals_geo;  // float4 per original triangle: cross(v1-v0, v2-v0)
+  bool geo_stale = true;
+  Wavefront wf;
+  uint64_t max_paths = 1ull << 24;
+
+  pt_render_stats stats{};
+  bool stats_pending = false;
+  uint64_t launches_at_start = 0;
+
+  SceneDev view() const;
+};
+
+}  // namespace pt
+
+struct pt_ctx {
+  pt::Context c;
+};

@@ -1,0 +1,299 @@
+// Device-side scene layout and the stackless BVH traversal.
+//
+// HBM layout (all 16-byte aligned, loaded as float4 / int4):
+//   nodes    : BVH2 with child-pair nodes, 4 x float4 = 64 B per node
+//              n0 = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)   n1 = same for child 1
+//              n2 = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)   n3 = (child0, child1, parent, 0) as int
+//              child >= 0: internal node index; child < 0: leaf, bits = 0x80000000 | first<<4 | count
+//   tri_v0/e1/e2 : Moller-Trumbore triangles in leaf order, 3 x float4 = 48 B per triangle
+//              (v0.xyz, original index), (v1-v0, 0), (v2-v0, 0)
+//   tri_info : per ORIGINAL triangle, int4 (normal index 0,1,2 or -1, material id)
+//   normals  : float4 per shading normal (xyz, 0)
+// A radiance or shadow query reads one node (64 B) per visited node, 48 B per tested triangle;
+// the BVH of the single-scene configuration (~100k triangles, ~7 MB of nodes and triangles) stays
+// resident in the 126 MB L2.
+#pragma once
+#include <string.h>
+
+#include "pt_math.cuh"
+
+// Loads through the read-only path on the device; plain loads when the traversal is compiled for the
+// host (the CPU check of the traversal in tests/ builds it that way).
+#ifdef __CUDA_ARCH__
+#define PT_LDG(p) __ldg(p)
+#else
+#define PT_LDG(p) (*(p))
+#endif
+
+namespace pt {
+
+PT_HD float as_float(int i)
+{
+#ifdef __CUDA_ARCH__
+  return __int_as_float(i);
+#else
+  float f;
+  memcpy(&f, &i, 4);
+  return f;
+#endif
+}
+PT_HD int as_int(float f)
+{
+#ifdef __CUDA_ARCH__
+  return __float_as_int(f);
+#else
+  int i;
+  memcpy(&i, &f, 4);
+  return i;
+#endif
+}
+
+constexpr uint32_t kLeafFlag = 0x80000000u;
+constexpr int kMaxDepth = 62;  // depth bound of the build; the traversal trail has 64 bits
+
+enum MatType : uint32_t { MAT_DIFFUSE = 0, MAT_ROUGH_GLASS = 3, MAT_METAL = 4, MAT_LIGHT = 100 };
+
+// Material record, 16-byte aligned (128 B).
+struct __align__(16) MatDev {
+  uint32_t type, model, dist, pad;
+  float4 a;   // diffuse: color.xyz | metal: roughness.xy | glass: ior, roughness | light: radiance.xyz
+  float4 b;   // glass: absorption.xyz
+  Cx3 eta;    // metal: 1 / ior (metallic_shader.cu:61), computed on the host
+  Cx3 inv_eta;// metal: 1 / eta (the walk's inside branch)
+};
+
+struct LightRaw { uint32_t type; float emitted[3]; float p[3]; float pad[3]; };  // structs.h:42-48 (40 B)
+struct TriLightRaw { float v0[3], v1[3], v2[3], n0[3], n1[3], n2[3]; uint32_t has_normals; float emission[3]; float area; };  // :96-103
+static_assert(sizeof(LightRaw) == 40, "LightStruct layout");
+static_assert(sizeof(TriLightRaw) == 92, "TriangleLight layout");
+enum LightType : uint32_t { POINT_LIGHT = 0, DIRECTIONAL_LIGHT = 1, TRIANGLES_AREA_LIGHT = 2, DISK_LIGHT = 3, SPHERICAL_LIGHT = 4 };
+
+struct CameraDev {
+  float3 eye, U, V, W;
+  uint32_t width, height;
+  uint2 patch_origin, patch_dims;
+};
+struct IntegratorDev {
+  int max_depth;
+  float scene_epsilon;
+  int rr_start;
+  float3 exception_color;
+};
+
+struct SceneDev {
+  const float4* nodes;
+  const float4* tri_v0;
+  const float4* tri_e1;
+  const float4* tri_e2;
+  const int4* tri_info;
+  const float4* normals;
+  const MatDev* mats;
+  const LightRaw* lights;
+  const TriLightRaw* tri_lights;
+  int n_lights, n_tri_lights;
+  uint32_t n_tris;
+  float3 bg_color;
+  CameraDev cam;
+  IntegratorDev integ;
+};
+
+struct Ray {
+  float3 o, d;
+  float tmin, tmax;
+};
+struct Hit {
+  float t, u, v;
+  int prim;  // original triangle index, -1 = miss
+};
+
+// ------------------------------------------------------------------ intersection primitives
+struct RayPre {
+  float3 inv;
+};
+PT_HD RayPre ray_pre(const float3& o, const float3& d)
+{
+  RayPre r;
+  float dx = fabsf(d.x) > 1e-20f ? d.x : copysignf(1e-20f, d.x);
+  float dy = fabsf(d.y) > 1e-20f ? d.y : copysignf(1e-20f, d.y);
+  float dz = fabsf(d.z) > 1e-20f ? d.z : copysignf(1e-20f, d.z);
+  r.inv = f3(1.0f / dx, 1.0f / dy, 1.0f / dz);
+  return r;
+}
+// Slab test of one child box; returns the entry distance, or +inf on a miss.  Each slab distance is
+// (plane - origin) * (1/d): two correctly rounded operations, so its relative error is at most
+// 2 ulp plus the 1 ulp of the reciprocal, and the exit distance is widened by kSlack (>> 3 ulp)
+// before the comparison (the robust slab test of T. Ize, "Robust BVH Ray Traversal", JCGT 2013).
+// The triangle test alone decides hits; boxes only prune, so the widening costs a little culling.
+constexpr float kSlack = 1.00001f;
+PT_HD float slab(float lox, float hix, float loy, float hiy, float loz, float hiz, const float3& o, const RayPre& r, float tmin, float tmax)
+{
+  float tx0 = (lox - o.x) * r.inv.x, tx1 = (hix - o.x) * r.inv.x;
+  float ty0 = (loy - o.y) * r.inv.y, ty1 = (hiy - o.y) * r.inv.y;
+  float tz0 = (loz - o.z) * r.inv.z, tz1 = (hiz - o.z) * r.inv.z;
+  float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tmin));
+  float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax * kSlack));
+  return tn <= tf * kSlack ? tn : as_float(0x7f800000);
+}
+// Moller-Trumbore (T. Moller, B. Trumbore, "Fast, minimum storage ray-triangle intersection",
+// JGT 1997) on (v0, e1 = v1-v0, e2 = v2-v0).  u weights v1, v weights v2.  Plain IEEE single
+// operations in a fixed order (no contraction), mirrored by the CPU oracle.
+PT_HD bool tri_mt(const float3& o, const float3& d, const float3& v0, const float3& e1, const float3& e2, float& t, float& u, float& v)
+{
+  float3 p = cross(d, e2);
+  float det = dot(e1, p);
+  if (det == 0.0f) return false;
+  float inv = 1.0f / det;
+  float3 tv = o - v0;
+  u = dot(tv, p) * inv;
+  if (!(u >= 0.0f && u <= 1.0f)) return false;
+  float3 q = cross(tv, e1);
+  v = dot(d, q) * inv;
+  if (!(v >= 0.0f && u + v <= 1.0f)) return false;
+  t = dot(e2, q) * inv;
+  return true;
+}
+
+PT_HD float3 ld3(const float4& a) { return f3(a.x, a.y, a.z); }
+
+// Intersect the triangles of leaf `code` and keep the closest hit (ties -> lower original index).
+PT_HD void leaf_closest(const SceneDev& S, uint32_t code, const float3& o, const float3& d, float tmin, Hit& h)
+{
+  uint32_t first = (code & 0x7fffffffu) >> 4, count = code & 15u;
+  for (uint32_t j = first; j < first + count; ++j) {
+    float4 a = PT_LDG(S.tri_v0 + j), b = PT_LDG(S.tri_e1 + j), c = PT_LDG(S.tri_e2 + j);
+    float t, u, v;
+    if (!tri_mt(o, d, ld3(a), ld3(b), ld3(c), t, u, v)) continue;
+    int prim = as_int(a.w);
+    if (t > tmin && (t < h.t || (t == h.t && h.prim >= 0 && prim < h.prim))) {
+      h.t = t;
+      h.u = u;
+      h.v = v;
+      h.prim = prim;
+    }
+  }
+}
+PT_HD bool leaf_any(const SceneDev& S, uint32_t code, const float3& o, const float3& d, float tmin, float tmax)
+{
+  uint32_t first = (code & 0x7fffffffu) >> 4, count = code & 15u;
+  for (uint32_t j = first; j < first + count; ++j) {
+    float4 a = PT_LDG(S.tri_v0 + j), b = PT_LDG(S.tri_e1 + j), c = PT_LDG(S.tri_e2 + j);
+    float t, u, v;
+    if (tri_mt(o, d, ld3(a), ld3(b), ld3(c), t, u, v) && t > tmin && t < tmax) return true;
+  }
+  return false;
+}
+
+// Stackless closest-hit traversal.  A 64-bit trail marks, per depth, whether the far child of the
+// node at that depth is still pending, and a second 64-bit word records which child it is; the way
+// back up follows the parent index stored in each node.  When a pending far child is resumed its box
+// is re-tested against the current closest distance.  No per-ray stack lives in local memory.
+PT_HD Hit trace_closest(const SceneDev& S, const float3& o, const float3& d, float tmin, float tmax)
+{
+  Hit h;
+  h.t = tmax;
+  h.u = h.v = 0.0f;
+  h.prim = -1;
+  RayPre rp = ray_pre(o, d);
+  int cur = 0, depth = 0;
+  unsigned long long pend = 0ull, farc1 = 0ull;
+  for (;;) {
+    const float4* nd = S.nodes + 4 * (size_t)cur;
+    float4 n0 = PT_LDG(nd), n1 = PT_LDG(nd + 1), n2 = PT_LDG(nd + 2);
+    int4 n3 = PT_LDG(reinterpret_cast<const int4*>(nd + 3));
+    float t0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, rp, tmin, h.t);
+    float t1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, rp, tmin, h.t);
+    bool h0 = t0 != as_float(0x7f800000), h1 = t1 != as_float(0x7f800000);
+    if (h0 && n3.x < 0) { leaf_closest(S, (uint32_t)n3.x, o, d, tmin, h); h0 = false; }
+    if (h1 && n3.y < 0) { leaf_closest(S, (uint32_t)n3.y, o, d, tmin, h); h1 = false; }
+    h0 = h0 && t0 <= h.t * kSlack;
+    h1 = h1 && t1 <= h.t * kSlack;
+    if (h0 && h1) {
+      bool near1 = t1 < t0;
+      pend |= 1ull << depth;
+      if (near1) farc1 &= ~(1ull << depth); else farc1 |= 1ull << depth;
+      cur = near1 ? n3.y : n3.x;
+      ++depth;
+      continue;
+    }
+    if (h0 || h1) {
+      cur = h0 ? n3.x : n3.y;
+      ++depth;
+      continue;
+    }
+    // backtrack to the deepest pending far child
+    for (;;) {
+      if (depth == 0) return h;
+      int parent = PT_LDG(reinterpret_cast<const int*>(S.nodes + 4 * (size_t)cur + 3) + 2);
+      --depth;
+      unsigned long long bit = 1ull << depth;
+      if (pend & bit) {
+        pend &= ~bit;
+        const float4* pn = S.nodes + 4 * (size_t)parent;
+        int4 p3 = PT_LDG(reinterpret_cast<const int4*>(pn + 3));
+        float tf;
+        int far;
+        if (farc1 & bit) {
+          float4 b1 = PT_LDG(pn + 1), b2 = PT_LDG(pn + 2);
+          tf = slab(b1.x, b1.y, b1.z, b1.w, b2.z, b2.w, o, rp, tmin, h.t);
+          far = p3.y;
+        } else {
+          float4 b0 = PT_LDG(pn), b2 = PT_LDG(pn + 2);
+          tf = slab(b0.x, b0.y, b0.z, b0.w, b2.x, b2.y, o, rp, tmin, h.t);
+          far = p3.x;
+        }
+        if (tf <= h.t * kSlack) {
+          cur = far;
+          ++depth;
+          break;
+        }
+      }
+      cur = parent;
+    }
+  }
+}
+
+// Stackless any-hit traversal (shadow rays): same trail, children visited in fixed order, stops at
+// the first triangle with tmin < t < tmax.
+PT_HD bool trace_any(const SceneDev& S, const float3& o, const float3& d, float tmin, float tmax)
+{
+  RayPre rp = ray_pre(o, d);
+  int cur = 0, depth = 0;
+  unsigned long long pend = 0ull;
+  for (;;) {
+    const float4* nd = S.nodes + 4 * (size_t)cur;
+    float4 n0 = PT_LDG(nd), n1 = PT_LDG(nd + 1), n2 = PT_LDG(nd + 2);
+    int4 n3 = PT_LDG(reinterpret_cast<const int4*>(nd + 3));
+    float t0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, rp, tmin, tmax);
+    float t1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, rp, tmin, tmax);
+    bool h0 = t0 != as_float(0x7f800000), h1 = t1 != as_float(0x7f800000);
+    if (h0 && n3.x < 0) { if (leaf_any(S, (uint32_t)n3.x, o, d, tmin, tmax)) return true; h0 = false; }
+    if (h1 && n3.y < 0) { if (leaf_any(S, (uint32_t)n3.y, o, d, tmin, tmax)) return true; h1 = false; }
+    if (h0 && h1) {
+      pend |= 1ull << depth;  // child 1 pending
+      cur = n3.x;
+      ++depth;
+      continue;
+    }
+    if (h0 || h1) {
+      cur = h0 ? n3.x : n3.y;
+      ++depth;
+      continue;
+    }
+    for (;;) {
+      if (depth == 0) return false;
+      int parent = PT_LDG(reinterpret_cast<const int*>(S.nodes + 4 * (size_t)cur + 3) + 2);
+      --depth;
+      unsigned long long bit = 1ull << depth;
+      if (pend & bit) {
+        pend &= ~bit;
+        int4 p3 = PT_LDG(reinterpret_cast<const int4*>(S.nodes + 4 * (size_t)parent + 3));
+        cur = p3.y;
+        ++depth;
+        break;
+      }
+      cur = parent;
+    }
+  }
+}
+
+}  // namespace pt

@@ -1,0 +1,427 @@
+"""Scene-object API of the reference, over the C ABI.
+
+The reference's host classes write OptiX variables; these write the same parameters through
+include/orf_b200.h.  Class and setter names follow the reference (Integrator.h, Camera.h,
+Background.h, Light.h, Material.h); ``Renderer`` plays the part of OptixScene (OptixScene.h) and
+its ``renderScene`` mirrors OptixScene::renderScene (OptixScene.cpp:139-168): one frame per call,
+`frame` incremented, the result folded into the running mean.
+
+Invalid parameters raise ``PtError`` (status PT_INVALID_ARG) from the native library, which checks
+every value before any device work.
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import _native as nat
+
+# ---------------------------------------------------------------- enums (structs.h)
+DIFFUSE_SHADER = 0
+ROUGH_TRANSPARENT_SHADER = 3
+METALLIC_SHADER = 4
+AREA_LIGHT_MATERIAL = 100
+WALTER_MODEL, VISIBLE_NORMALS_MODEL, MULTISCATTERING_MODEL = 0, 1, 2
+BECKMANN_DISTRIBUTION, GGX_DISTRIBUTION = 0, 1
+POINT_LIGHT, DIRECTIONAL_LIGHT, TRIANGLES_AREA_LIGHT, DISK_LIGHT, SPHERICAL_LIGHT = 0, 1, 2, 3, 4
+
+
+class DiffuseParams(ctypes.Structure):
+    _fields_ = [("diffuse_color", ctypes.c_float * 3)]
+
+
+class MetallicParams(ctypes.Structure):
+    _fields_ = [("ior", ctypes.c_double * 6), ("roughness", ctypes.c_float * 2), ("microfacet_model", ctypes.c_uint32),
+                ("normal_distribution", ctypes.c_uint32)]
+
+
+class RoughTransparentParams(ctypes.Structure):
+    _fields_ = [("ior", ctypes.c_float), ("roughness", ctypes.c_float), ("glass_absorption", ctypes.c_float * 3),
+                ("microfacet_model", ctypes.c_uint32), ("normal_distribution", ctypes.c_uint32)]
+
+
+class AreaLightParams(ctypes.Structure):
+    _fields_ = [("radiance", ctypes.c_float * 3)]
+
+
+class RenderStats(ctypes.Structure):
+    _fields_ = [("path_samples", ctypes.c_uint64), ("segments", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
+                ("capped_walks", ctypes.c_uint64), ("clamped_indices", ctypes.c_uint64), ("gpu_ms", ctypes.c_float),
+                ("extend_ms", ctypes.c_float), ("extend_launches", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32)]
+
+
+# LightStruct (40 B) and TriangleLight (92 B), structs.h:42-103, as numpy record types.
+LIGHT_DTYPE = np.dtype([("light_type", "<u4"), ("emitted_radiance", "<f4", 3), ("p", "<f4", 3), ("padding", "<f4", 3)])
+TRIANGLE_LIGHT_DTYPE = np.dtype([("v0", "<f4", 3), ("v1", "<f4", 3), ("v2", "<f4", 3), ("n0", "<f4", 3), ("n1", "<f4", 3),
+                                 ("n2", "<f4", 3), ("has_normals", "<u4"), ("emission", "<f4", 3), ("area", "<f4")])
+assert LIGHT_DTYPE.itemsize == 40 and TRIANGLE_LIGHT_DTYPE.itemsize == 92
+
+
+def _f3(v):
+    return (ctypes.c_float * 3)(*[float(x) for x in v])
+
+
+# ---------------------------------------------------------------- Integrator.h
+class PathTracer:
+    """PathTracer (Integrator.cpp:6-24 defaults: max_depth 50, scene_epsilon 1e-4, red exception)."""
+
+    def __init__(self, max_depth=50, scene_epsilon=1e-4, exception_color=(1.0, 0.0, 0.0), rr_start_depth=0):
+        self.max_depth = int(max_depth)
+        self.scene_epsilon = float(scene_epsilon)
+        self.exception_color = tuple(exception_color)
+        self.rr_start_depth = int(rr_start_depth)
+
+    def setMaxDepth(self, d):
+        self.max_depth = int(d)
+
+    def setSceneEpsilon(self, e):
+        self.scene_epsilon = float(e)
+
+    def setExceptionColor(self, c):
+        self.exception_color = tuple(c)
+
+    def getMaxDepth(self):
+        return self.max_depth
+
+    def getSceneEpsilon(self):
+        return self.scene_epsilon
+
+
+# ---------------------------------------------------------------- Camera.h
+class PinholeCamera:
+    """PinholeCamera: eye / lookat / up / vfov -> U, V, W as PinholeCamera::calculateCameraVariables
+    (Camera.cpp:83-103): W = lookat - eye (not normalised), U = |W| tan(vfov/2) aspect * unit(W x up),
+    V = |W| tan(vfov/2) * unit(U x W)."""
+
+    def __init__(self, eye, lookat, up, vfov, width, height, patch_origin=(0, 0), patch_dims=None):
+        self.eye = np.asarray(eye, np.float32)
+        self.lookat = np.asarray(lookat, np.float32)
+        self.up = np.asarray(up, np.float32)
+        self.vfov = float(vfov)
+        self.width = int(width)
+        self.height = int(height)
+        self.patch_origin = tuple(int(x) for x in patch_origin)
+        self.patch_dims = tuple(int(x) for x in (patch_dims or (width, height)))
+        self.calculateCameraVariables()
+
+    def calculateCameraVariables(self):
+        W = (self.lookat - self.eye).astype(np.float32)
+        wlen = np.float32(np.linalg.norm(W.astype(np.float64)))
+        U = np.cross(W.astype(np.float64), self.up.astype(np.float64))
+        U = (U / np.linalg.norm(U)).astype(np.float32)
+        V = np.cross(U.astype(np.float64), W.astype(np.float64))
+        V = (V / np.linalg.norm(V)).astype(np.float32)
+        vlen = np.float32(wlen * np.float32(math.tan(0.5 * self.vfov * math.pi / 180.0)))
+        V = (V * vlen).astype(np.float32)
+        ulen = np.float32(vlen * np.float32(self.width / self.height))
+        U = (U * ulen).astype(np.float32)
+        self.U, self.V, self.W = U, V, W
+
+    def setEye(self, e):
+        self.eye = np.asarray(e, np.float32)
+        self.calculateCameraVariables()
+
+    def setLookat(self, l):
+        self.lookat = np.asarray(l, np.float32)
+        self.calculateCameraVariables()
+
+    def setUp(self, u):
+        self.up = np.asarray(u, np.float32)
+        self.calculateCameraVariables()
+
+    def setFov(self, f):
+        self.vfov = float(f)
+        self.calculateCameraVariables()
+
+    def resizeCamera(self, width, height):
+        self.width, self.height = int(width), int(height)
+        self.patch_dims = (self.width, self.height)
+        self.calculateCameraVariables()
+
+
+# ---------------------------------------------------------------- Background.h
+class ConstantBackground:
+    def __init__(self, background_color=(1.0, 1.0, 1.0)):
+        self.background_color = tuple(background_color)
+
+    def setBackgroundColor(self, c):
+        self.background_color = tuple(c)
+
+
+# ---------------------------------------------------------------- Material.h
+class DiffuseMaterial:
+    type = DIFFUSE_SHADER
+
+    def __init__(self, color=(0.8, 0.8, 0.8)):
+        self.color = tuple(color)
+
+    def params(self):
+        return DiffuseParams(_f3(self.color))
+
+    def setColor(self, c):
+        self.color = tuple(c)
+
+
+class MetallicMaterial:
+    """Conductor with complex IOR per RGB (MyComplex3); defaults of MetallicMaterial.cpp:7-26
+    (gold, roughness 0.1, Walter model, Beckmann distribution)."""
+    type = METALLIC_SHADER
+    GOLD = ((0.170265, 3.01893), (0.511516, 2.44734), (1.47544, 1.87263))  # Material.h:328
+
+    def __init__(self, ior=GOLD, roughness=(0.1, 0.1), microfacet_model=WALTER_MODEL, normal_distribution=BECKMANN_DISTRIBUTION):
+        self.ior = tuple(tuple(float(x) for x in c) for c in ior)
+        self.roughness = tuple(float(x) for x in roughness)
+        self.microfacet_model = int(microfacet_model)
+        self.normal_distribution = int(normal_distribution)
+
+    def params(self):
+        flat = [v for c in self.ior for v in c]
+        return MetallicParams((ctypes.c_double * 6)(*flat), (ctypes.c_float * 2)(*self.roughness), self.microfacet_model,
+                              self.normal_distribution)
+
+    def setIor(self, ior):
+        self.ior = tuple(tuple(float(x) for x in c) for c in ior)
+
+    def setRoughness(self, r):
+        self.roughness = tuple(float(x) for x in r)
+
+    def setMicrofacetModel(self, m):
+        self.microfacet_model = int(m)
+
+    def setNormalDistribution(self, d):
+        self.normal_distribution = int(d)
+
+
+class RoughTransparentMaterial:
+    """Rough dielectric; defaults of RoughTransparentMaterial.cpp:7-28 (ior 1.3, roughness 0.1,
+    no absorption, Walter model, Beckmann distribution)."""
+    type = ROUGH_TRANSPARENT_SHADER
+
+    def __init__(self, ior=1.3, roughness=0.1, glass_absorption=(0.0, 0.0, 0.0), microfacet_model=WALTER_MODEL,
+                 normal_distribution=BECKMANN_DISTRIBUTION):
+        self.ior = float(ior)
+        self.roughness = float(roughness)
+        self.glass_absorption = tuple(glass_absorption)
+        self.microfacet_model = int(microfacet_model)
+        self.normal_distribution = int(normal_distribution)
+
+    def params(self):
+        return RoughTransparentParams(self.ior, self.roughness, _f3(self.glass_absorption), self.microfacet_model,
+                                      self.normal_distribution)
+
+
+class AreaLightMaterial:
+    """The emitter program TriangleAreaLight attaches to its geometry (arealight_shader.cu)."""
+    type = AREA_LIGHT_MATERIAL
+
+    def __init__(self, radiance):
+        self.radiance = tuple(radiance)
+
+    def params(self):
+        return AreaLightParams(_f3(self.radiance))
+
+
+# ---------------------------------------------------------------- Light.h
+class TriangleAreaLight:
+    """TriangleAreaLight: an emitting triangle mesh.  Produces its LightStruct (triangle_count /
+    buffer_start_idx / buffer_end_idx stored as float, structs.h:66-74), its TriangleLight records
+    (area = 0.5 |(v1-v0) x (v2-v0)|, Light.cpp:286-297) and the emitter geometry."""
+
+    def __init__(self, positions, vindex, radiance):
+        self.positions = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        self.vindex = np.ascontiguousarray(vindex, np.int32).reshape(-1, 3)
+        self.radiance = tuple(float(x) for x in radiance)
+
+    def triangle_records(self):
+        recs = np.zeros(len(self.vindex), TRIANGLE_LIGHT_DTYPE)
+        for k, (a, b, c) in enumerate(self.vindex):
+            v0, v1, v2 = self.positions[a], self.positions[b], self.positions[c]
+            recs[k]["v0"], recs[k]["v1"], recs[k]["v2"] = v0, v1, v2
+            recs[k]["has_normals"] = 0
+            recs[k]["emission"] = self.radiance
+            perp = np.cross((v1 - v0).astype(np.float32), (v2 - v0).astype(np.float32)).astype(np.float32)
+            recs[k]["area"] = np.float32(0.5 * float(np.sqrt(np.float32(np.dot(perp, perp)))))
+        return recs
+
+
+class PointLight:
+    def __init__(self, position, radiance):
+        self.position, self.radiance = tuple(position), tuple(radiance)
+
+
+class DirectionalLight:
+    def __init__(self, direction, radiance):
+        self.direction, self.radiance = tuple(direction), tuple(radiance)
+
+
+def light_buffers(lights):
+    """light_buffer and triangle_light_buffer for a list of lights (OptixSceneLoader.cpp:284-347)."""
+    ls = np.zeros(len(lights), LIGHT_DTYPE)
+    tri_recs = []
+    start = 0
+    for k, L in enumerate(lights):
+        if isinstance(L, TriangleAreaLight):
+            recs = L.triangle_records()
+            ls[k]["light_type"] = TRIANGLES_AREA_LIGHT
+            ls[k]["emitted_radiance"] = L.radiance
+            ls[k]["p"] = (float(len(recs)), float(start), float(start + len(recs) - 1))
+            tri_recs.append(recs)
+            start += len(recs)
+        elif isinstance(L, PointLight):
+            ls[k]["light_type"] = POINT_LIGHT
+            ls[k]["emitted_radiance"] = L.radiance
+            ls[k]["p"] = L.position
+        elif isinstance(L, DirectionalLight):
+            ls[k]["light_type"] = DIRECTIONAL_LIGHT
+            ls[k]["emitted_radiance"] = L.radiance
+            d = np.asarray(L.direction, np.float32)
+            ls[k]["p"] = d / np.float32(np.linalg.norm(d))
+        else:
+            raise TypeError("unsupported light %r" % (L,))
+    tris = np.concatenate(tri_recs) if tri_recs else np.zeros(0, TRIANGLE_LIGHT_DTYPE)
+    return ls, tris
+
+
+class Mesh:
+    """A triangle mesh with one material (the OBJGeometry buffers of ObjLoader.cpp:278-373)."""
+
+    def __init__(self, positions, vindex, material, normals=None, nindex=None):
+        self.positions = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        self.vindex = np.ascontiguousarray(vindex, np.int32).reshape(-1, 3)
+        self.normals = None if normals is None else np.ascontiguousarray(normals, np.float32).reshape(-1, 3)
+        self.nindex = None if nindex is None else np.ascontiguousarray(nindex, np.int32).reshape(-1, 3)
+        self.material = material
+
+
+# ---------------------------------------------------------------- scene flattening
+class SceneData:
+    """Everything a render needs, flattened in one fixed order that the GPU context and the CPU
+    oracle both use: materials are numbered in order of first use (meshes first, then the emitter
+    materials of TriangleAreaLights); triangles follow mesh order, then the lights' emitter meshes."""
+
+    def __init__(self, integrator, camera, background, meshes, lights):
+        self.integrator, self.camera, self.background = integrator, camera, background
+        self.lights = list(lights)
+        self.meshes = list(meshes)
+        for L in self.lights:
+            if isinstance(L, TriangleAreaLight):
+                self.meshes.append(Mesh(L.positions, L.vindex, AreaLightMaterial(L.radiance)))
+        self.materials = []
+        index = {}
+        self.mesh_material = []
+        for m in self.meshes:
+            if id(m.material) not in index:
+                index[id(m.material)] = len(self.materials)
+                self.materials.append(m.material)
+            self.mesh_material.append(index[id(m.material)])
+        self.light_buffer, self.triangle_light_buffer = light_buffers(self.lights)
+
+    @property
+    def n_triangles(self):
+        return sum(len(m.vindex) for m in self.meshes)
+
+    def flat_triangles(self):
+        """(tri_pos [T,9] float32, tri_info [T,4] int32, normals [N,3] float32) as pt_mesh_add stores them."""
+        pos, info, nrm = [], [], []
+        nbase = 0
+        for m, mid in zip(self.meshes, self.mesh_material):
+            pos.append(m.positions[m.vindex].reshape(-1, 9))
+            inf = np.full((len(m.vindex), 4), -1, np.int32)
+            inf[:, 3] = mid
+            if m.normals is not None:
+                ok = np.all(m.nindex >= 0, axis=1)
+                inf[ok, :3] = m.nindex[ok] + nbase
+                nrm.append(m.normals)
+                nbase += len(m.normals)
+            info.append(inf)
+        normals = np.concatenate(nrm).astype(np.float32) if nrm else np.zeros((0, 3), np.float32)
+        return np.ascontiguousarray(np.concatenate(pos), np.float32), np.ascontiguousarray(np.concatenate(info)), normals
+
+
+# ---------------------------------------------------------------- OptixScene
+class Renderer:
+    """Owns a pt_ctx and plays the part of OptixScene: scene setup, build, renderScene()."""
+
+    def __init__(self, data, device=0, max_paths_in_flight=None):
+        self.data = data
+        self.integrator, self.camera, self.background = data.integrator, data.camera, data.background
+        self.frame = 0
+        ctx = ctypes.c_void_p()
+        nat.check(nat.lib().pt_context_create(device, ctypes.byref(ctx)), "pt_context_create")
+        self.ctx = ctx
+        if max_paths_in_flight:
+            nat.call("pt_set_max_paths_in_flight", self.ctx, int(max_paths_in_flight))
+        self.material_ids = {}
+        for k, mat in enumerate(data.materials):
+            mid = ctypes.c_uint32()
+            p = mat.params()
+            nat.call("pt_material_create", self.ctx, mat.type, ctypes.byref(p), ctypes.sizeof(p), ctypes.byref(mid))
+            assert mid.value == k
+            self.material_ids[id(mat)] = k
+        self.apply_integrator()
+        self.apply_camera()
+        self.apply_background()
+        for m, mid in zip(data.meshes, data.mesh_material):
+            nn = 0 if m.normals is None else len(m.normals)
+            first = ctypes.c_uint32()
+            nat.call("pt_mesh_add", self.ctx, m.positions.ctypes.data, len(m.positions), m.vindex.ctypes.data, len(m.vindex),
+                     None if m.normals is None else m.normals.ctypes.data, nn,
+                     None if m.nindex is None else m.nindex.ctypes.data, mid, ctypes.byref(first))
+        lb, tb = data.light_buffer, data.triangle_light_buffer
+        nat.call("pt_lights_upload", self.ctx, lb.ctypes.data if len(lb) else None, len(lb), tb.ctypes.data if len(tb) else None, len(tb))
+        nat.call("pt_build", self.ctx)
+
+    def update_material(self, mat):
+        """Push changed parameters of a material already in the scene."""
+        p = mat.params()
+        nat.call("pt_material_update", self.ctx, self.material_ids[id(mat)], ctypes.byref(p), ctypes.sizeof(p))
+
+    def apply_integrator(self):
+        I = self.integrator
+        nat.call("pt_set_integrator", self.ctx, I.max_depth, I.scene_epsilon, _f3(I.exception_color), I.rr_start_depth)
+
+    def apply_camera(self):
+        C = self.camera
+        nat.call("pt_set_camera", self.ctx, _f3(C.eye), _f3(C.U), _f3(C.V), _f3(C.W), C.width, C.height,
+                 (ctypes.c_uint32 * 2)(*C.patch_origin), (ctypes.c_uint32 * 2)(*C.patch_dims))
+        self.frame = 0
+
+    def apply_background(self):
+        nat.call("pt_set_background_constant", self.ctx, _f3(self.background.background_color))
+
+    def renderScene(self):
+        """One frame, as OptixScene::renderScene: frame++ and one integrator pass."""
+        nat.call("pt_render_frames", self.ctx, self.frame, 1)
+        self.frame += 1
+
+    def render(self, n_frames):
+        """n_frames more frames folded into the running mean (one wavefront launch group)."""
+        nat.call("pt_render_frames", self.ctx, self.frame, int(n_frames))
+        self.frame += int(n_frames)
+
+    def readback(self):
+        out = np.empty((self.camera.height, self.camera.width, 4), np.float32)
+        nat.call("pt_readback", self.ctx, out.ctypes.data)
+        return out
+
+    def stats(self):
+        s = RenderStats()
+        nat.call("pt_get_render_stats", self.ctx, ctypes.byref(s))
+        return s
+
+    def sync(self):
+        nat.call("pt_sync", self.ctx)
+
+    def stream(self):
+        return nat.lib().pt_context_stream(self.ctx)
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            nat.lib().pt_context_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

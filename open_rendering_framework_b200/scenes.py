@@ -1,0 +1,86 @@
+"""Procedural scenes of the benchmark configurations (synthetic stand-ins: the reference ships no
+benchmark scenes, and its demo scene depends on assets that are not in the repository).
+
+single_scene(): the single-scene render -- a closed box of 12 triangles (diffuse, albedo 0.7), an
+icosphere subdivided 6 times (81,920 triangles, radius 0.3) of GGX conductor with alpha 0.2 and
+complex IOR R = 0.2+3.9i, G = 0.55+3.15i, B = 0.9+2.4i (the (0.2,0.9)-(3.9,2.4) range read as
+red/blue endpoints, green in between), an icosphere subdivided 5 times (20,480 triangles, radius
+0.3) of rough dielectric (Beckmann, alpha 0.1, eta 1.5), and one 0.25 x 0.25 quad light of radiance
+15 under the ceiling; 512 x 512, max depth 8, Russian roulette from depth 3.  The placement is fixed:
+box [-1,1]^3, camera at (0, 0, 0.9) looking down -z with a 60 degree vertical field of view,
+conductor sphere at (-0.45, -0.7, -0.3), dielectric sphere at (0.45, -0.7, 0.1), light at y = 0.99.
+"""
+import numpy as np
+
+from . import scene as sc
+
+
+def icosphere(subdiv, radius=1.0, center=(0.0, 0.0, 0.0)):
+    """Icosahedron subdivided `subdiv` times (20 * 4^subdiv triangles), projected to the sphere,
+    with per-vertex normals (positions, vindex, normals, nindex)."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+             (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+             (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+             (8, 6, 7), (9, 8, 1)]
+    V = np.array(verts, np.float64)
+    V /= np.linalg.norm(V, axis=1, keepdims=True)
+    F = np.array(faces, np.int64)
+    for _ in range(subdiv):
+        edges = np.concatenate([F[:, [0, 1]], F[:, [1, 2]], F[:, [2, 0]]])
+        key = np.sort(edges, axis=1)
+        uniq, inv = np.unique(key, axis=0, return_inverse=True)
+        mids = V[uniq[:, 0]] + V[uniq[:, 1]]
+        mids /= np.linalg.norm(mids, axis=1, keepdims=True)
+        base = len(V)
+        V = np.concatenate([V, mids])
+        m = inv.reshape(3, -1).T + base  # midpoint of edges (0,1), (1,2), (2,0) per face
+        a, b, c = F[:, 0], F[:, 1], F[:, 2]
+        ab, bc, ca = m[:, 0], m[:, 1], m[:, 2]
+        F = np.concatenate([np.stack([a, ab, ca], 1), np.stack([b, bc, ab], 1), np.stack([c, ca, bc], 1), np.stack([ab, bc, ca], 1)])
+    normals = V.astype(np.float32)
+    pos = (V * radius + np.asarray(center, np.float64)).astype(np.float32)
+    vi = F.astype(np.int32)
+    return pos, vi, normals, vi.copy()
+
+
+def box(lo=(-1.0, -1.0, -1.0), hi=(1.0, 1.0, 1.0)):
+    """A closed box of 12 triangles (no vertex normals: the geometric normal is used)."""
+    x0, y0, z0 = lo
+    x1, y1, z1 = hi
+    P = np.array([(x0, y0, z0), (x1, y0, z0), (x1, y1, z0), (x0, y1, z0), (x0, y0, z1), (x1, y0, z1), (x1, y1, z1), (x0, y1, z1)], np.float32)
+    quads = [(0, 1, 2, 3), (5, 4, 7, 6), (4, 0, 3, 7), (1, 5, 6, 2), (4, 5, 1, 0), (3, 2, 6, 7)]
+    tris = []
+    for a, b, c, d in quads:
+        tris += [(a, b, c), (a, c, d)]
+    return P, np.array(tris, np.int32)
+
+
+def quad_light(center, size, y_down=True):
+    """A horizontal square of 2 triangles facing -y (the emitter test of arealight_shader.cu is
+    front-facing against the geometric normal cross(v1-v0, v2-v0))."""
+    cx, cy, cz = center
+    h = size / 2.0
+    P = np.array([(cx - h, cy, cz - h), (cx + h, cy, cz - h), (cx + h, cy, cz + h), (cx - h, cy, cz + h)], np.float32)
+    idx = np.array([(0, 1, 2), (0, 2, 3)], np.int32) if y_down else np.array([(0, 2, 1), (0, 3, 2)], np.int32)
+    return P, idx
+
+
+def single_scene(width=512, height=512, metal_subdiv=6, glass_subdiv=5, max_depth=8, rr_start_depth=3,
+                 metal_model=sc.WALTER_MODEL, glass_model=sc.WALTER_MODEL):
+    integrator = sc.PathTracer(max_depth=max_depth, scene_epsilon=1e-4, rr_start_depth=rr_start_depth)
+    camera = sc.PinholeCamera(eye=(0.0, 0.0, 0.9), lookat=(0.0, 0.0, -1.0), up=(0.0, 1.0, 0.0), vfov=60.0, width=width, height=height)
+    background = sc.ConstantBackground((0.0, 0.0, 0.0))
+    diffuse = sc.DiffuseMaterial((0.7, 0.7, 0.7))
+    metal = sc.MetallicMaterial(ior=((0.2, 3.9), (0.55, 3.15), (0.9, 2.4)), roughness=(0.2, 0.2), microfacet_model=metal_model,
+                                normal_distribution=sc.GGX_DISTRIBUTION)
+    glass = sc.RoughTransparentMaterial(ior=1.5, roughness=0.1, glass_absorption=(0.0, 0.0, 0.0), microfacet_model=glass_model,
+                                        normal_distribution=sc.BECKMANN_DISTRIBUTION)
+    bp, bi = box()
+    mp, mi, mn, mni = icosphere(metal_subdiv, 0.3, (-0.45, -0.7, -0.3))
+    gp, gi, gn, gni = icosphere(glass_subdiv, 0.3, (0.45, -0.7, 0.1))
+    meshes = [sc.Mesh(bp, bi, diffuse), sc.Mesh(mp, mi, metal, mn, mni), sc.Mesh(gp, gi, glass, gn, gni)]
+    lp, li = quad_light((0.0, 0.99, 0.0), 0.25)
+    lights = [sc.TriangleAreaLight(lp, li, (15.0, 15.0, 15.0))]
+    return sc.SceneData(integrator, camera, background, meshes, lights)

@@ -163,3 +163,96 @@ def bsdf_queries(n, first, n_ggx_below, wo, alpha, eta=1.0 / 1.5, fp64=False, th
     else:
         orc().orc_bsdf_queries_f(n, first, n_ggx_below, fp(wo), fp(alpha), eta, fp(wi), fp(f), fp(pdf), fp(F_), threads)
     return wi, f, pdf, F_
+
+
+# ---------------------------------------------------------------- CPU path tracer (orc_trace.cpp)
+def _trace_sigs(lib):
+    if getattr(lib, "_trace_bound", False):
+        return
+    _sig(lib, "orc_scene_create", P, [P, P, U, P, U, P, P, P, P, P, U, P, U, P, U, P, U, U, P, I, F, I, P])
+    _sig(lib, "orc_scene_destroy", None, [P])
+    _sig(lib, "orc_render", L, [P, U, U, U, U, P, P, I])
+    _sig(lib, "orc_capped", L, [P])
+    _sig(lib, "orc_trace_batch", None, [P, P, L, I, P, P, P, P])
+    lib._trace_bound = True
+
+
+class OracleScene:
+    """The CPU restatement of the reference's recursive path tracer over a SceneData
+    (open_rendering_framework_b200.scene) flattened exactly as the GPU context stores it."""
+
+    def __init__(self, data):
+        lib = orc()
+        _trace_sigs(lib)
+        self.lib = lib
+        self.data = data
+        tri_pos, tri_info, normals = data.flat_triangles()
+        n_m = len(data.materials)
+        mtype = np.zeros(n_m, np.uint32)
+        mmodel = np.zeros(n_m, np.uint32)
+        mdist = np.zeros(n_m, np.uint32)
+        mab = np.zeros((n_m, 8), np.float32)
+        mior = np.zeros((n_m, 6), np.float64)
+        for k, m in enumerate(data.materials):
+            mtype[k] = m.type
+            name = type(m).__name__
+            if name == "DiffuseMaterial":
+                mab[k, :3] = m.color
+            elif name == "MetallicMaterial":
+                mmodel[k], mdist[k] = m.microfacet_model, m.normal_distribution
+                mab[k, :2] = m.roughness
+                mior[k] = [v for c in m.ior for v in c]
+            elif name == "RoughTransparentMaterial":
+                mmodel[k], mdist[k] = m.microfacet_model, m.normal_distribution
+                mab[k, 0], mab[k, 1] = m.ior, m.roughness
+                mab[k, 4:7] = m.glass_absorption
+            elif name == "AreaLightMaterial":
+                mab[k, :3] = m.radiance
+            else:
+                raise TypeError(name)
+        C = data.camera
+        cam = np.concatenate([C.eye, C.U, C.V, C.W]).astype(np.float32)
+        patch = np.array(list(C.patch_origin) + list(C.patch_dims), np.uint32)
+        I_ = data.integrator
+        bg = np.asarray(data.background.background_color, np.float32)
+        # keep every buffer alive for the scene's lifetime
+        self._keep = [tri_pos, tri_info, normals, mtype, mmodel, mdist, mab, mior, cam, patch, bg,
+                      np.ascontiguousarray(data.light_buffer), np.ascontiguousarray(data.triangle_light_buffer)]
+        lb, tb = self._keep[-2], self._keep[-1]
+        self.h = lib.orc_scene_create(fp(tri_pos), fp(tri_info), len(tri_pos), fp(normals) if len(normals) else None, len(normals),
+                                      fp(mtype), fp(mmodel), fp(mdist), fp(mab), fp(mior), n_m,
+                                      fp(lb) if len(lb) else None, len(lb), fp(tb) if len(tb) else None, len(tb),
+                                      fp(cam), C.width, C.height, fp(patch), I_.max_depth, I_.scene_epsilon, I_.rr_start_depth, fp(bg))
+
+    def render(self, first_frame, n_frames, accum=None, p_begin=0, p_end=None, path_radiance=False, threads=1):
+        """Runs the CPU tracer; returns (accum [H,W,4] or None, per-path radiance [F,P,3] or None)."""
+        W, H = self.data.camera.width, self.data.camera.height
+        p_end = W * H if p_end is None else p_end
+        pr = np.zeros((n_frames, p_end - p_begin, 3), np.float32) if path_radiance else None
+        if accum is not None:
+            accum = np.ascontiguousarray(accum, np.float32)
+        self.lib.orc_render(self.h, first_frame, n_frames, p_begin, p_end, fp(pr) if pr is not None else None,
+                            fp(accum) if accum is not None else None, threads)
+        return accum, pr
+
+    def trace(self, rays8, brute=False):
+        """Closest and any hit for rays [n,8] = (origin, tmin, dir, tmax)."""
+        rays8 = np.ascontiguousarray(rays8, np.float32)
+        n = len(rays8)
+        prim = np.empty(n, np.int32)
+        t = np.empty(n, np.float32)
+        bary = np.empty((n, 2), np.float32)
+        anyh = np.empty(n, np.int32)
+        self.lib.orc_trace_batch(self.h, fp(rays8), n, 1 if brute else 0, fp(prim), fp(t), fp(bary), fp(anyh))
+        return prim, t, bary, anyh
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.orc_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,595 @@
+// Test infrastructure (oracle only): CPU restatement of the reference's recursive OptiX path
+// tracer -- the path_tracer.cu ray generation and accumulation, the closest-hit programs of
+// diffuse_shader.cu, metallic_shader.cu, rough_transparent_shader.cu and arealight_shader.cu, and
+// the constantbg.cu miss program -- with the random numbers consumed in exactly the reference's
+// order.  OptiX's traversal is replaced by a CPU BVH whose closest hit equals a brute-force loop over
+// all triangles with the same Moller-Trumbore test as the CUDA kernels (closest t, ties to the lower
+// triangle index); orc_trace_brute exposes that brute-force loop for BVH parity tests.
+//
+// Used by tests (image and per-path parity on small scenes) and as the CPU baseline of the
+// benchmark (multi-threaded over pixels).
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "orc_light.hpp"
+#include "orc_math.hpp"
+#include "orc_microfacet.hpp"
+
+using namespace orc;
+
+#define EXPORT extern "C" __attribute__((visibility("default")))
+
+namespace {
+
+typedef V3<float> F3;
+
+enum { MT_DIFFUSE = 0, MT_GLASS = 3, MT_METAL = 4, MT_LIGHT = 100 };
+
+struct Mat {
+  u32 type, model, dist;
+  float a[4], b[4];
+  Cx3 eta, inv_eta;
+};
+
+struct Tri {
+  F3 v0, e1, e2;
+};
+
+struct Scene {
+  std::vector<Tri> tris;
+  std::vector<int> info;       // 4 per triangle
+  std::vector<F3> normals;
+  std::vector<Mat> mats;
+  LightSet lights;
+  F3 eye, U, V, W;
+  u32 width, height, po_x, po_y, pd_x, pd_y;
+  int max_depth;
+  float eps;
+  int rr_start;
+  F3 bg;
+  // BVH
+  struct Node { float lo[3], hi[3]; int left, right, first, count; };
+  std::vector<Node> nodes;
+  std::vector<int> order;
+  std::atomic<long> capped{0};
+};
+
+// Moller-Trumbore in the same operation order as the CUDA kernel (pt_scene.cuh tri_mt).
+static inline bool tri_mt(const F3& o, const F3& d, const Tri& T, float& t, float& u, float& v)
+{
+  F3 p = cross(d, T.e2);
+  float det = dot(T.e1, p);
+  if (det == 0.0f) return false;
+  float inv = 1.0f / det;
+  F3 tv = o - T.v0;
+  u = dot(tv, p) * inv;
+  if (!(u >= 0.0f && u <= 1.0f)) return false;
+  F3 q = cross(tv, T.e1);
+  v = dot(d, q) * inv;
+  if (!(v >= 0.0f && u + v <= 1.0f)) return false;
+  t = dot(T.e2, q) * inv;
+  return true;
+}
+
+struct HitRec {
+  float t, u, v;
+  int prim;
+};
+
+static void build_bvh(Scene& S)
+{
+  size_t n = S.tris.size();
+  S.order.resize(n);
+  for (size_t i = 0; i < n; ++i) S.order[i] = (int)i;
+  std::vector<float> lo(3 * n), hi(3 * n), c(3 * n);
+  for (size_t i = 0; i < n; ++i) {
+    const Tri& T = S.tris[i];
+    F3 v1 = T.v0 + T.e1, v2 = T.v0 + T.e2;  // only for bounds; widened below
+    float p[3][3] = {{T.v0.x, T.v0.y, T.v0.z}, {v1.x, v1.y, v1.z}, {v2.x, v2.y, v2.z}};
+    for (int k = 0; k < 3; ++k) {
+      lo[3 * i + k] = std::min(p[0][k], std::min(p[1][k], p[2][k]));
+      hi[3 * i + k] = std::max(p[0][k], std::max(p[1][k], p[2][k]));
+      c[3 * i + k] = 0.5f * (lo[3 * i + k] + hi[3 * i + k]);
+    }
+  }
+  S.nodes.clear();
+  S.nodes.reserve(2 * n + 1);
+  struct Item { int node, b, e; };
+  std::vector<Item> work;
+  S.nodes.push_back(Scene::Node());
+  work.push_back({0, 0, (int)n});
+  while (!work.empty()) {
+    Item it = work.back();
+    work.pop_back();
+    Scene::Node nd;
+    for (int k = 0; k < 3; ++k) { nd.lo[k] = INFINITY; nd.hi[k] = -INFINITY; }
+    for (int i = it.b; i < it.e; ++i)
+      for (int k = 0; k < 3; ++k) {
+        nd.lo[k] = std::min(nd.lo[k], lo[3 * S.order[i] + k]);
+        nd.hi[k] = std::max(nd.hi[k], hi[3 * S.order[i] + k]);
+      }
+    // widen by a relative margin so the box test is conservative for the single-precision hits
+    for (int k = 0; k < 3; ++k) {
+      float m = 1e-5f * (std::fabs(nd.lo[k]) + std::fabs(nd.hi[k])) + 1e-6f;
+      nd.lo[k] -= m;
+      nd.hi[k] += m;
+    }
+    if (it.e - it.b <= 4) {
+      nd.left = nd.right = -1;
+      nd.first = it.b;
+      nd.count = it.e - it.b;
+      S.nodes[it.node] = nd;
+      continue;
+    }
+    int axis = 0;
+    float ext[3] = {nd.hi[0] - nd.lo[0], nd.hi[1] - nd.lo[1], nd.hi[2] - nd.lo[2]};
+    if (ext[1] > ext[axis]) axis = 1;
+    if (ext[2] > ext[axis]) axis = 2;
+    int mid = (it.b + it.e) / 2;
+    std::nth_element(S.order.begin() + it.b, S.order.begin() + mid, S.order.begin() + it.e,
+                     [&](int x, int y) { return c[3 * x + axis] < c[3 * y + axis]; });
+    nd.left = (int)S.nodes.size();
+    nd.right = nd.left + 1;
+    nd.first = nd.count = 0;
+    S.nodes[it.node] = nd;
+    S.nodes.push_back(Scene::Node());
+    S.nodes.push_back(Scene::Node());
+    work.push_back({nd.left, it.b, mid});
+    work.push_back({nd.right, mid, it.e});
+  }
+}
+
+static inline bool box_hit(const Scene::Node& n, const double* o, const double* inv, double tmin, double tmax)
+{
+  double t0 = tmin, t1 = tmax;
+  for (int k = 0; k < 3; ++k) {
+    double a = (n.lo[k] - o[k]) * inv[k], b = (n.hi[k] - o[k]) * inv[k];
+    if (a > b) std::swap(a, b);
+    t0 = std::max(t0, a);
+    t1 = std::min(t1, b);
+  }
+  return t0 <= t1 * (1.0 + 1e-9) + 1e-12;
+}
+
+static HitRec closest(const Scene& S, const F3& o, const F3& d, float tmin, float tmax)
+{
+  HitRec h = {tmax, 0.0f, 0.0f, -1};
+  double od[3] = {o.x, o.y, o.z};
+  double inv[3] = {1.0 / (d.x != 0 ? d.x : 1e-30), 1.0 / (d.y != 0 ? d.y : 1e-30), 1.0 / (d.z != 0 ? d.z : 1e-30)};
+  int stack[128];
+  int sp = 0;
+  stack[sp++] = 0;
+  while (sp) {
+    const Scene::Node& n = S.nodes[stack[--sp]];
+    if (!box_hit(n, od, inv, tmin, (double)h.t * (1.0 + 1e-6))) continue;
+    if (n.left < 0) {
+      for (int i = n.first; i < n.first + n.count; ++i) {
+        int prim = S.order[i];
+        float t, u, v;
+        if (!tri_mt(o, d, S.tris[prim], t, u, v)) continue;
+        if (t > tmin && (t < h.t || (t == h.t && h.prim >= 0 && prim < h.prim))) h = {t, u, v, prim};
+      }
+    } else {
+      stack[sp++] = n.left;
+      stack[sp++] = n.right;
+    }
+  }
+  return h;
+}
+
+static bool occluded(const Scene& S, const F3& o, const F3& d, float tmin, float tmax)
+{
+  double od[3] = {o.x, o.y, o.z};
+  double inv[3] = {1.0 / (d.x != 0 ? d.x : 1e-30), 1.0 / (d.y != 0 ? d.y : 1e-30), 1.0 / (d.z != 0 ? d.z : 1e-30)};
+  int stack[128];
+  int sp = 0;
+  stack[sp++] = 0;
+  while (sp) {
+    const Scene::Node& n = S.nodes[stack[--sp]];
+    if (!box_hit(n, od, inv, tmin, (double)tmax * (1.0 + 1e-6))) continue;
+    if (n.left < 0) {
+      for (int i = n.first; i < n.first + n.count; ++i) {
+        float t, u, v;
+        if (tri_mt(o, d, S.tris[S.order[i]], t, u, v) && t > tmin && t < tmax) return true;
+      }
+    } else {
+      stack[sp++] = n.left;
+      stack[sp++] = n.right;
+    }
+  }
+  return false;
+}
+
+// Shading normal: normalize(rtTransformNormal(normalize(n))) with the identity transform.
+static F3 shading_normal(const Scene& S, int prim, float u, float v)
+{
+  const int* in = &S.info[4 * (size_t)prim];
+  F3 n;
+  if (in[0] >= 0) {
+    const F3 &n0 = S.normals[in[0]], &n1 = S.normals[in[1]], &n2 = S.normals[in[2]];
+    n = normalize(n1 * u + n2 * v + n0 * (1.0f - u - v));
+  } else {
+    n = normalize(cross(S.tris[prim].e1, S.tris[prim].e2));
+  }
+  return normalize(n);
+}
+
+struct PRD {
+  F3 result;
+  int emit_light;
+  int depth;
+  u32 seed;
+  Seed64 seed64;
+};
+
+static void trace(Scene& S, const F3& o, const F3& d, PRD& prd, LightSet& ls);
+
+// diffuse_shader.cu:122-187
+static void shade_diffuse(Scene& S, const Mat& m, const F3& o, const F3& d, const HitRec& h, PRD& prd, LightSet& ls)
+{
+  if (prd.depth > S.max_depth) return;
+  F3 hit_pos = o + h.t * d;
+  F3 normal = shading_normal(S, h.prim, h.u, h.v);
+  F3 ffnormal = faceforward(normal, -d, normal);
+  const F3 dc = v3(m.a[0], m.a[1], m.a[2]);
+  u32& t = prd.seed;
+  F3 result = v3s(0.0f);
+  float draw = rnd_tea(t);
+  if (ls.n_lights > 0) {
+    u32 li = (u32)((float)ls.n_lights * draw);
+    if ((long)li >= ls.n_lights) { li = (u32)(ls.n_lights - 1); ++ls.oob; }
+    float light_pdf = 1.0f / (float)ls.n_lights;
+    F3 w_l = v3s(0.0f), radiance = v3s(0.0f);
+    float dist = 0.0f;
+    eval_direct<float>(hit_pos, ls.lights[li], ls, w_l, radiance, dist, t);
+    radiance = radiance / light_pdf;
+    float cos_theta = dot(ffnormal, w_l);
+    if (cos_theta > 0.0f) {
+      float V = occluded(S, hit_pos, w_l, S.eps, dist - S.eps) ? 0.0f : 1.0f;
+      F3 Li = V * radiance;
+      result = result + Li * K<float>::INV_PI * cos_theta * dc;
+      prd.emit_light = 0;
+    }
+  }
+  float prob = (dc.x + dc.y + dc.z) / 3.0f;
+  float xi = rnd_tea(t);
+  bool forced = prd.depth < S.rr_start;
+  if (forced) prob = 1.0f;
+  if (xi < prob || forced) {
+    F3 nd = sample_cosine_weighted<float>(ffnormal, t);
+    PRD child;
+    child.depth = prd.depth + 1;
+    child.seed = t;
+    child.seed64 = prd.seed64;
+    child.result = v3s(0.0f);
+    child.emit_light = prd.emit_light;
+    trace(S, hit_pos, nd, child, ls);
+    result = result + child.result * dc / prob;
+    prd.seed = child.seed;
+  }
+  prd.result = result;
+}
+
+// metallic_shader.cu:232-348
+static void shade_metal(Scene& S, const Mat& m, const F3& o, const F3& d, const HitRec& h, PRD& prd, LightSet& ls)
+{
+  if (prd.depth >= S.max_depth) { prd.result = v3s(0.0f); return; }
+  F3 result = v3s(0.0f);
+  F3 hit_point = o + h.t * d;
+  F3 normal = shading_normal(S, h.prim, h.u, h.v);
+  F3 ffnormal = faceforward(normal, -d, normal);
+  F3 w_i = -d;
+  u32& seed = prd.seed;
+  float a_x = m.a[0], a_y = m.a[1];
+  int capped = 0;
+  if (m.model == MULTISCATTERING) {
+    u32 order = 0;
+    F3 wm, weight;
+    F3 lwo = ms_conductor_sample<float>((int)m.dist, to_local(w_i, normal), wm, m.eta, m.inv_eta, a_x, a_y, seed, order, weight, 4096, &capped);
+    F3 w_o = to_world(lwo, normal);
+    PRD child;
+    child.depth = prd.depth + 1;
+    child.result = v3s(0.0f);
+    child.seed = seed;
+    child.seed64 = prd.seed64;
+    child.emit_light = 1;
+    trace(S, hit_point, w_o, child, ls);
+    result = result + child.result * weight;
+  } else {
+    float z1 = rnd_tea(seed), z2 = rnd_tea(seed);
+    F3 mn;
+    float G_i_m;
+    if (m.model == WALTER) {
+      mn = sample_normal<float>((int)m.dist, ffnormal, z1, z2, a_x);
+      G_i_m = masking_G1<float>((int)m.dist, w_i, mn, ffnormal, a_x);
+    } else {
+      mn = sample_visible_normal<float>((int)m.dist, w_i, ffnormal, a_x, a_y, z1, z2, &capped);
+      G_i_m = masking_G1_aniso<float>((int)m.dist, w_i, mn, ffnormal, a_x, a_y);
+    }
+    if (G_i_m <= 0.0f) { prd.result = result; S.capped += capped; return; }
+    F3 F = fresnel_complex<float>(w_i, mn, m.eta);
+    F3 w_o = -w_i + 2.0f * mn * dot(w_i, mn);
+    float abs_i_m = std::fabs(dot(w_i, mn)), abs_i_n = std::fabs(dot(w_i, ffnormal)), abs_n_m = std::fabs(dot(normal, mn));
+    PRD child;
+    child.depth = prd.depth + 1;
+    child.result = v3s(0.0f);
+    child.seed = seed;
+    child.seed64 = prd.seed64;
+    child.emit_light = 1;
+    F3 weight = F;
+    float G_o_m = (m.model == WALTER) ? masking_G1<float>((int)m.dist, w_o, mn, ffnormal, a_x) : masking_G1_aniso<float>((int)m.dist, w_o, mn, ffnormal, a_x, a_y);
+    if (G_o_m <= 0.0f) { prd.result = result; S.capped += capped; return; }
+    trace(S, hit_point, w_o, child, ls);
+    if (m.model == WALTER) weight = weight * (abs_i_m * G_i_m * G_o_m / (abs_i_n * abs_n_m));
+    else weight = weight * G_o_m;
+    prd.seed = child.seed;
+    result = result + child.result * weight;
+  }
+  S.capped += capped;
+  prd.result = result;
+}
+
+// rough_transparent_shader.cu:66-225
+static void shade_glass(Scene& S, const Mat& m, const F3& o, const F3& d, const HitRec& h, PRD& prd, LightSet& ls)
+{
+  if (prd.depth >= S.max_depth) { prd.result = v3s(0.0f); return; }
+  F3 result = v3s(0.0f);
+  F3 hit_point = o + h.t * d;
+  F3 normal = shading_normal(S, h.prim, h.u, h.v);
+  F3 ffnormal = faceforward(normal, -d, normal);
+  F3 w_i = -d;
+  u32& t = prd.seed;
+  const float ior = m.a[0], rough = m.a[1];
+  F3 beam_T = v3s(1.0f);
+  float cos_theta = dot(-d, normal);
+  if (cos_theta < 0.0f) {
+    beam_T = vexp((-h.t) * v3(m.b[0], m.b[1], m.b[2]));
+    float prob = (beam_T.x + beam_T.y + beam_T.z) / 3.0f;
+    if (rnd_tea(t) >= prob) return;
+    beam_T = beam_T / prob;
+  }
+  float z1 = rnd_tea(t), z2 = rnd_tea(t);
+  int capped = 0;
+  if (m.model == MULTISCATTERING) {
+    u32 order = 0;
+    F3 lwo = ms_dielectric_sample<float>((int)m.dist, to_local(w_i, normal), 1.0f / ior, rough, rough, t, order, 4096, &capped);
+    F3 w_o = to_world(lwo, normal);
+    PRD child;
+    child.depth = prd.depth + 1;
+    child.result = v3s(0.0f);
+    child.seed = t;
+    child.seed64 = prd.seed64;
+    child.emit_light = 1;
+    trace(S, hit_point, w_o, child, ls);
+    prd.seed = child.seed;
+    result = result + child.result;
+  } else {
+    F3 mn = (m.model == WALTER) ? sample_normal<float>((int)m.dist, ffnormal, z1, z2, rough)
+                                : sample_visible_normal<float>((int)m.dist, w_i, ffnormal, rough, rough, z1, z2, &capped);
+    float cos_in = dot(normal, w_i);
+    float eta = cos_in < 0.0f ? ior : 1.0f / ior;
+    float G_i_m = (m.model == WALTER) ? masking_G1<float>((int)m.dist, w_i, mn, ffnormal, rough) : masking_G1_aniso<float>((int)m.dist, w_i, mn, ffnormal, rough, rough);
+    if (G_i_m <= 0.0f) { prd.result = result; S.capped += capped; return; }
+    float ct = std::fabs(dot(mn, -d));
+    float st2 = eta * eta * (1.0f - ct * ct);
+    float ctt = std::sqrt(1.0f - st2);
+    float R = st2 < 1.0f ? fresnel_R(ct, ctt, eta) : 1.0f;
+    F3 refr = eta * d + mn * (eta * ct - ctt);
+    F3 refl = reflect(d, mn);
+    float abs_i_m = std::fabs(dot(w_i, mn)), abs_i_n = std::fabs(dot(w_i, ffnormal)), abs_n_m = std::fabs(dot(normal, mn));
+    float rr = rnd_tea(t);
+    PRD child;
+    child.depth = prd.depth + 1;
+    child.result = v3s(0.0f);
+    child.seed = t;
+    child.seed64 = prd.seed64;
+    child.emit_light = 1;
+    F3 w_o = rr > R ? refr : refl;
+    float G_o_m = (m.model == WALTER) ? masking_G1<float>((int)m.dist, w_o, mn, ffnormal, rough) : masking_G1_aniso<float>((int)m.dist, w_o, mn, ffnormal, rough, rough);
+    if (G_o_m <= 0.0f) { prd.result = result; S.capped += capped; return; }
+    trace(S, hit_point, w_o, child, ls);
+    float weight = (m.model == WALTER) ? abs_i_m * G_i_m * G_o_m / (abs_i_n * abs_n_m) : G_o_m;
+    prd.seed = child.seed;
+    result = result + child.result * weight;
+  }
+  S.capped += capped;
+  prd.result = result * beam_T;
+}
+
+static void trace(Scene& S, const F3& o, const F3& d, PRD& prd, LightSet& ls)
+{
+  HitRec h = closest(S, o, d, S.eps, DEFAULT_MAX);
+  if (h.prim < 0) {  // constantbg.cu:16-19
+    prd.result = S.bg;
+    return;
+  }
+  const Mat& m = S.mats[S.info[4 * (size_t)h.prim + 3]];
+  switch (m.type) {
+    case MT_LIGHT: {  // arealight_shader.cu:36-50
+      F3 normal = shading_normal(S, h.prim, h.u, h.v);
+      F3 result = v3s(0.0f);
+      if (dot(normal, -d) > 0.0f && prd.emit_light) result = v3(m.a[0], m.a[1], m.a[2]);
+      prd.result = result;
+      return;
+    }
+    case MT_DIFFUSE: shade_diffuse(S, m, o, d, h, prd, ls); return;
+    case MT_METAL: shade_metal(S, m, o, d, h, prd, ls); return;
+    case MT_GLASS: shade_glass(S, m, o, d, h, prd, ls); return;
+    default: prd.result = v3s(0.0f); return;
+  }
+}
+
+}  // namespace
+
+// Scene handle for the C interface.
+EXPORT void* orc_scene_create(const float* tri_pos, const int* tri_info, unsigned n_tris, const float* normals, unsigned n_normals,
+                              const unsigned* mat_type, const unsigned* mat_model, const unsigned* mat_dist, const float* mat_ab,
+                              const double* mat_ior, unsigned n_mats, const void* lights, unsigned n_lights, const void* tri_lights,
+                              unsigned n_tri_lights, const float* cam12, unsigned width, unsigned height, const unsigned* patch4,
+                              int max_depth, float eps, int rr_start, const float* bg3)
+{
+  Scene* S = new Scene();
+  S->tris.resize(n_tris);
+  for (unsigned i = 0; i < n_tris; ++i) {
+    const float* p = tri_pos + 9 * (size_t)i;
+    F3 v0 = v3(p[0], p[1], p[2]), v1 = v3(p[3], p[4], p[5]), v2 = v3(p[6], p[7], p[8]);
+    S->tris[i] = {v0, v1 - v0, v2 - v0};
+  }
+  S->info.assign(tri_info, tri_info + 4 * (size_t)n_tris);
+  for (unsigned k = 0; k < n_normals; ++k) S->normals.push_back(v3(normals[3 * k], normals[3 * k + 1], normals[3 * k + 2]));
+  for (unsigned k = 0; k < n_mats; ++k) {
+    Mat m;
+    memset(&m, 0, sizeof(m));
+    m.type = mat_type[k];
+    m.model = mat_model[k];
+    m.dist = mat_dist[k];
+    memcpy(m.a, mat_ab + 8 * (size_t)k, 16);
+    memcpy(m.b, mat_ab + 8 * (size_t)k + 4, 16);
+    if (m.type == MT_METAL) {
+      const double* io = mat_ior + 6 * (size_t)k;
+      Cx3 ior = {{io[0], io[1]}, {io[2], io[3]}, {io[4], io[5]}};
+      m.eta = crecip3<float>(ior);       // eta = n1 / ior, metallic_shader.cu:61
+      m.inv_eta = crecip3<float>(m.eta);
+    }
+    S->mats.push_back(m);
+  }
+  S->lights.lights = (const LightStructRaw*)lights;
+  S->lights.n_lights = n_lights;
+  S->lights.tris = (const TriangleLightRaw*)tri_lights;
+  S->lights.n_tris = n_tri_lights;
+  S->eye = v3(cam12[0], cam12[1], cam12[2]);
+  S->U = v3(cam12[3], cam12[4], cam12[5]);
+  S->V = v3(cam12[6], cam12[7], cam12[8]);
+  S->W = v3(cam12[9], cam12[10], cam12[11]);
+  S->width = width;
+  S->height = height;
+  S->po_x = patch4[0]; S->po_y = patch4[1]; S->pd_x = patch4[2]; S->pd_y = patch4[3];
+  S->max_depth = max_depth;
+  S->eps = eps;
+  S->rr_start = rr_start;
+  S->bg = v3(bg3[0], bg3[1], bg3[2]);
+  build_bvh(*S);
+  return S;
+}
+
+EXPORT void orc_scene_destroy(void* s) { delete (Scene*)s; }
+
+// Renders frames [first_frame, first_frame + n_frames) for pixels [p_begin, p_end) with `threads`
+// host threads.  path_rad (optional): radiance of every path, [frame][pixel][3] over the pixel
+// range.  accum (optional): the float4 running mean over the full image, updated in frame order as
+// path_tracer.cu:64-68.  The light arrays passed to orc_scene_create must outlive the scene.
+EXPORT long orc_render(void* scene, unsigned first_frame, unsigned n_frames, unsigned p_begin, unsigned p_end, float* path_rad, float* accum,
+                       int threads)
+{
+  Scene& S = *(Scene*)scene;
+  const unsigned W = S.width, H = S.height;
+  p_end = std::min(p_end, W * H);
+  if (p_begin >= p_end) return 0;
+  std::atomic<unsigned> next(p_begin);
+  std::atomic<long> oob(0);
+  auto worker = [&]() {
+    LightSet ls = S.lights;
+    ls.oob = 0;
+    for (;;) {
+      unsigned p0 = next.fetch_add(64);
+      if (p0 >= p_end) break;
+      unsigned p1 = std::min(p_end, p0 + 64);
+      for (unsigned p = p0; p < p1; ++p) {
+        unsigned x = p % W, y = p / W;
+        bool inside = !(x < S.po_x || x > S.po_x + S.pd_x || y < S.po_y || y > S.po_y + S.pd_y);
+        float out[4];
+        if (accum) memcpy(out, accum + 4 * (size_t)p, 16);
+        for (unsigned fl = 0; fl < n_frames; ++fl) {
+          unsigned frame = first_frame + fl;
+          F3 result = v3s(0.0f);
+          if (inside) {
+            PRD prd;
+            prd.emit_light = 1;
+            prd.depth = 0;
+            prd.seed = tea<16>(W * y + x, frame);
+            u32 s2 = tea<16>(W * y + x, frame);
+            prd.seed64 = {s2, s2};
+            float jx = rnd_tea(prd.seed), jy = rnd_tea(prd.seed);
+            float ipx = ((float)x + jx) / (float)W * 2.0f - 1.0f;
+            float ipy = ((float)y + jy) / (float)H * 2.0f - 1.0f;
+            F3 dir = normalize(ipx * S.U + ipy * S.V + S.W);
+            prd.result = v3s(0.0f);
+            trace(S, S.eye, dir, prd, ls);
+            result = result + prd.result;
+          }
+          if (path_rad) {
+            float* pr = path_rad + 3 * ((size_t)fl * (p_end - p_begin) + (p - p_begin));
+            pr[0] = result.x; pr[1] = result.y; pr[2] = result.z;
+          }
+          if (accum) {
+            if (!inside) {
+              out[0] = out[1] = out[2] = 0.0f;
+              out[3] = 1.0f;
+            } else if (std::isfinite(result.x) && std::isfinite(result.y) && std::isfinite(result.z)) {
+              float cur[4] = {0, 0, 0, 0};
+              if (frame != 0)
+                for (int k = 0; k < 4; ++k) cur[k] = out[k] * (float)frame;
+              float den = (float)(frame + 1);
+              out[0] = (result.x + cur[0]) / den;
+              out[1] = (result.y + cur[1]) / den;
+              out[2] = (result.z + cur[2]) / den;
+              out[3] = (1.0f + cur[3]) / den;
+            }
+          }
+        }
+        if (accum) memcpy(accum + 4 * (size_t)p, out, 16);
+      }
+    }
+    oob += ls.oob;
+  };
+  threads = std::max(1, threads);
+  std::vector<std::thread> th;
+  for (int i = 1; i < threads; ++i) th.emplace_back(worker);
+  worker();
+  for (auto& t : th) t.join();
+  return oob.load();
+}
+
+EXPORT long orc_capped(void* scene) { return ((Scene*)scene)->capped.load(); }
+
+// Closest / any hit for a batch of rays (origin.xyz, tmin, dir.xyz, tmax per 8 floats): BVH
+// result and brute-force result over all triangles.
+EXPORT void orc_trace_batch(void* scene, const float* rays8, long n, int brute, int* prim, float* t, float* bary, int* any)
+{
+  Scene& S = *(Scene*)scene;
+  for (long i = 0; i < n; ++i) {
+    const float* r = rays8 + 8 * i;
+    F3 o = v3(r[0], r[1], r[2]), d = v3(r[4], r[5], r[6]);
+    HitRec h;
+    if (brute) {
+      h = {r[7], 0.0f, 0.0f, -1};
+      for (size_t k = 0; k < S.tris.size(); ++k) {
+        float tt, u, v;
+        if (!tri_mt(o, d, S.tris[k], tt, u, v)) continue;
+        if (tt > r[3] && (tt < h.t || (tt == h.t && h.prim >= 0 && (int)k < h.prim))) h = {tt, u, v, (int)k};
+      }
+    } else {
+      h = closest(S, o, d, r[3], r[7]);
+    }
+    prim[i] = h.prim;
+    t[i] = h.prim >= 0 ? h.t : -1.0f;
+    bary[2 * i] = h.u;
+    bary[2 * i + 1] = h.v;
+    if (any) {
+      if (brute) {
+        int a = 0;
+        for (size_t k = 0; k < S.tris.size() && !a; ++k) {
+          float tt, u, v;
+          if (tri_mt(o, d, S.tris[k], tt, u, v) && tt > r[3] && tt < r[7]) a = 1;
+        }
+        any[i] = a;
+      } else {
+        any[i] = occluded(S, o, d, r[3], r[7]) ? 1 : 0;
+      }
+    }
+  }
+}

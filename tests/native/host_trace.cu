@@ -1,0 +1,45 @@
+// Test-only library: the product's BVH builder (pt_bvh.cu) and stackless traversal (pt_scene.cuh)
+// compiled for the HOST, so the traversal logic can be checked against brute force without a GPU.
+// Built by tests/conftest.py into tests/native/_build/libhost_trace.so; never part of the product.
+#include <vector>
+
+#include "../../open_rendering_framework_b200/csrc/pt_bvh.h"
+#include "../../open_rendering_framework_b200/csrc/pt_scene.cuh"
+
+using namespace pt;
+
+struct HostScene {
+  BvhHost bvh;
+  SceneDev S;
+};
+
+extern "C" __attribute__((visibility("default"))) void* ht_build(const float* tri_pos, unsigned n, int* depth_out)
+{
+  HostScene* h = new HostScene();
+  if (!build_bvh(tri_pos, n, h->bvh)) { delete h; return nullptr; }
+  memset(&h->S, 0, sizeof(h->S));
+  h->S.nodes = h->bvh.nodes.data();
+  h->S.tri_v0 = h->bvh.tri_v0.data();
+  h->S.tri_e1 = h->bvh.tri_e1.data();
+  h->S.tri_e2 = h->bvh.tri_e2.data();
+  h->S.n_tris = n;
+  if (depth_out) *depth_out = h->bvh.depth;
+  return h;
+}
+extern "C" __attribute__((visibility("default"))) void ht_free(void* h) { delete (HostScene*)h; }
+extern "C" __attribute__((visibility("default"))) unsigned ht_nodes(void* h) { return (unsigned)(((HostScene*)h)->bvh.nodes.size() / 4); }
+// rays: n x 8 floats (origin, tmin, dir, tmax)
+extern "C" __attribute__((visibility("default"))) void ht_trace(void* hp, const float* rays, long n, int* prim, float* t, float* bary, int* any)
+{
+  HostScene* h = (HostScene*)hp;
+  for (long i = 0; i < n; ++i) {
+    const float* r = rays + 8 * i;
+    float3 o = make_float3(r[0], r[1], r[2]), d = make_float3(r[4], r[5], r[6]);
+    Hit hh = trace_closest(h->S, o, d, r[3], r[7]);
+    prim[i] = hh.prim;
+    t[i] = hh.prim >= 0 ? hh.t : -1.0f;
+    bary[2 * i] = hh.u;
+    bary[2 * i + 1] = hh.v;
+    any[i] = trace_any(h->S, o, d, r[3], r[7]) ? 1 : 0;
+  }
+}

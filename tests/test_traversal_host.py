@@ -1,0 +1,83 @@
+"""The product's BVH builder and stackless traversal (pt_bvh.cu, pt_scene.cuh), compiled for the
+host by tests/native/host_trace.cu, against the brute-force oracle: closest-hit index, t and
+barycentrics and any-hit bit-identical, including rays aimed exactly at vertices and edges.  Runs
+without a GPU (the same code runs on the device in tests/test_render_gpu.py)."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import oracle_ctypes as oc
+from open_rendering_framework_b200 import scenes
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SO = os.path.join(HERE, "native", "_build", "libhost_trace.so")
+SRC = [os.path.join(HERE, "native", "host_trace.cu"),
+       os.path.join(HERE, "..", "open_rendering_framework_b200", "csrc", "pt_bvh.cu")]
+HDR = [os.path.join(HERE, "..", "open_rendering_framework_b200", "csrc", f) for f in ("pt_scene.cuh", "pt_math.cuh", "pt_bvh.h")]
+
+
+@pytest.fixture(scope="module")
+def host_lib():
+    newest = max(os.path.getmtime(p) for p in SRC + HDR)
+    if not os.path.exists(SO) or os.path.getmtime(SO) < newest:
+        os.makedirs(os.path.dirname(SO), exist_ok=True)
+        subprocess.run(["/usr/local/cuda/bin/nvcc", "-std=c++17", "-O2", "--fmad=false", "-Wno-deprecated-gpu-targets",
+                        "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-shared"] + SRC + ["-o", SO], check=True)
+    L = ctypes.CDLL(SO)
+    L.ht_build.restype = ctypes.c_void_p
+    L.ht_build.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p]
+    L.ht_free.argtypes = [ctypes.c_void_p]
+    L.ht_trace.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long] + [ctypes.c_void_p] * 4
+    return L
+
+
+def edge_and_random_rays(tp, n, seed):
+    rng = np.random.default_rng(seed)
+    pick = rng.integers(0, len(tp), n)
+    w = rng.dirichlet([1, 1, 1], n).astype(np.float32)
+    w[: n // 3] = np.array([1, 0, 0], np.float32)           # vertices
+    w[n // 3: 2 * n // 3] = np.array([0.5, 0.5, 0], np.float32)  # edge midpoints
+    targets = tp[pick, 0:3] * w[:, 0:1] + tp[pick, 3:6] * w[:, 1:2] + tp[pick, 6:9] * w[:, 2:3]
+    orig = rng.uniform(-0.9, 0.9, (n, 3)).astype(np.float32)
+    d = targets - orig
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    tmax = np.where(rng.uniform(size=n) < 0.7, 1e27, rng.uniform(0.05, 2.0, n))
+    return np.ascontiguousarray(np.concatenate([orig, np.full((n, 1), 1e-4), d, tmax[:, None]], 1).astype(np.float32))
+
+
+@pytest.mark.parametrize("subdiv", [(1, 0), (3, 2), (4, 3)])
+def test_host_traversal_matches_brute_force(host_lib, subdiv):
+    data = scenes.single_scene(width=8, height=8, metal_subdiv=subdiv[0], glass_subdiv=subdiv[1])
+    tp, _, _ = data.flat_triangles()
+    depth = ctypes.c_int()
+    h = host_lib.ht_build(oc.fp(tp), len(tp), ctypes.byref(depth))
+    assert h and 0 < depth.value < 64
+    rays = edge_and_random_rays(tp, 6000, 11)
+    n = len(rays)
+    prim, t = np.empty(n, np.int32), np.empty(n, np.float32)
+    bary, anyh = np.empty((n, 2), np.float32), np.empty(n, np.int32)
+    host_lib.ht_trace(h, oc.fp(rays), n, oc.fp(prim), oc.fp(t), oc.fp(bary), oc.fp(anyh))
+    host_lib.ht_free(h)
+    bp, bt, bb, ba = oc.OracleScene(data).trace(rays, brute=True)
+    assert np.array_equal(prim, bp)
+    assert np.array_equal(t.view(np.uint32), bt.view(np.uint32))
+    assert np.array_equal(bary.view(np.uint32), bb.view(np.uint32))
+    assert np.array_equal(anyh, ba)
+
+
+def test_single_triangle_and_degenerate_scenes(host_lib):
+    # one triangle (root with an empty second child), and many coincident triangles (no centroid split)
+    one = np.array([[0, 0, 0, 1, 0, 0, 0, 1, 0]], np.float32)
+    same = np.repeat(one, 40, axis=0)
+    for tp in (one, same):
+        h = host_lib.ht_build(oc.fp(tp), len(tp), None)
+        rays = np.array([[0.2, 0.2, 1, 1e-4, 0, 0, -1, 1e27], [2, 2, 1, 1e-4, 0, 0, -1, 1e27]], np.float32)
+        prim, t = np.empty(2, np.int32), np.empty(2, np.float32)
+        bary, anyh = np.empty((2, 2), np.float32), np.empty(2, np.int32)
+        host_lib.ht_trace(h, oc.fp(rays), 2, oc.fp(prim), oc.fp(t), oc.fp(bary), oc.fp(anyh))
+        host_lib.ht_free(h)
+        assert prim[0] == 0 and t[0] == 1.0 and anyh[0] == 1   # ties between coincident copies go to index 0
+        assert prim[1] == -1 and anyh[1] == 0
