@@ -1,0 +1,336 @@
+"""Benchmark: Mpath-samples/s of the single-scene wavefront render on one B200 (per GPU replica).
+
+Workload (one step): 512 x 512 pixels x 64 camera samples (frames) of the procedural single scene
+(box of 12 diffuse triangles, 81,920-triangle GGX conductor icosphere, 20,480-triangle Beckmann
+dielectric icosphere, 0.25 x 0.25 quad light of radiance 15), max depth 8, Russian roulette from
+depth 3 -- 16,777,216 path samples per step, traced as one wavefront launch group.
+
+Arms
+  --impl ours (default): the CUDA path through the C ABI.  `value` is device-timed (CUDA events
+      on the render stream, barrier + synchronize on both sides, max over ranks); `e2e` times the
+      public API with host buffers: per step a camera + material update (H2D), the render, and the
+      float4 image read back into pinned host memory (D2H).
+  --impl reference: the reference's path tracer has no CPU build (OptiX), so its CPU restatement
+      (oracle/orc/orc_trace.cpp: path_tracer.cu and the shaders, recursive, the reference's math)
+      runs on all host cores over a bounded sample of the same workload.
+
+Multi-GPU: the path shards by scene/frames with no exchange step, so N GPUs run N independent
+replicas (weak scaling); value = all ranks' path samples / max-over-ranks time.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mpath-samples/s plain vs batched vs fwd+adjoint on 1 B200 at equal image relMSE"
+UNIT = "Mpath-samples/s"
+WORKLOAD = ("single-scene render 512x512, 64 spp, max depth 8, Russian roulette from depth 3: 12-triangle diffuse box, "
+            "81,920-triangle GGX conductor icosphere, 20,480-triangle Beckmann rough-dielectric icosphere, quad light")
+EXTEND_BYTES_PER_SEGMENT = 56  # queue id 4 + ray 32 + hit record 16 + material-queue append 4
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--spp", type=int, default=64)
+    ap.add_argument("--width", type=int, default=512)
+    ap.add_argument("--height", type=int, default=512)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profile():
+    """Per-launch DRAM bytes of the extend kernel from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "k_extend_single_scene.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch_full_size:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "", 1).isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "", 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def cpu_baseline_sample(data, target_s=12.0, threads=None):
+    """Times the CPU restatement of the reference tracer on a bounded sample of the workload."""
+    from oracle import oracle_ctypes as oc
+
+    threads = threads or os.cpu_count() or 1
+    O = oc.OracleScene(data)
+    W = data.camera.width
+    # calibrate on a small band, then size the sample for ~target_s seconds
+    rows = 4
+    t0 = time.perf_counter()
+    O.render(0, 1, p_begin=W * 254, p_end=W * (254 + rows), threads=threads)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    rate = rows * W / dt
+    n_paths = int(min(max(rate * target_s, W), W * data.camera.height * 64))
+    frames = max(1, min(64, n_paths // (W * 32)))
+    band = max(1, min(data.camera.height, n_paths // (W * frames)))
+    p0 = W * max(0, (data.camera.height - band) // 2)
+    t0 = time.perf_counter()
+    O.render(0, frames, p_begin=p0, p_end=p0 + W * band, threads=threads)
+    dt = time.perf_counter() - t0
+    samples = W * band * frames
+    O.close()
+    return {"value": samples / dt / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "%d rows x %d px x %d spp (%d path samples) of the same scene, CPU restatement of the reference's "
+                      "recursive path tracer (path_tracer.cu + shaders, its own math), %d threads, %.1f s" % (
+                          band, W, frames, samples, threads, dt)}
+
+
+def run_reference(args, world, rank):
+    from open_rendering_framework_b200 import scenes
+
+    if rank != 0:
+        return
+    data = scenes.single_scene(width=args.width, height=args.height)
+    from oracle import oracle_ctypes as oc
+
+    threads = os.cpu_count() or 1
+    O = oc.OracleScene(data)
+    W, H = data.camera.width, data.camera.height
+    band = 16  # rows per step: each step is a bounded sample (16 x 512 px x 8 spp)
+    frames = 8
+    p0 = W * (H // 2 - band // 2)
+    for _ in range(max(0, args.warmup)):
+        O.render(0, 1, p_begin=p0, p_end=p0 + W * 2, threads=threads)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        O.render(k * frames, frames, p_begin=p0, p_end=p0 + W * band, threads=threads)
+    dt = time.perf_counter() - t0
+    samples = args.steps * W * band * frames
+    value = samples / dt / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(1, args.steps), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_per_step": "%d rows x %d px x %d spp" % (band, W, frames)},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": "%d rows x %d px x %d spp per step; the reference's OptiX tracer has no CPU build, so its "
+                                   "CPU restatement (path_tracer.cu + shaders, the reference's math) runs on all host cores" % (
+                                       band, W, frames)},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    O.close()
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    from open_rendering_framework_b200 import _native as nat
+    from open_rendering_framework_b200 import scene as sc
+    from open_rendering_framework_b200 import scenes
+
+    torch.cuda.set_device(local)
+    data = scenes.single_scene(width=args.width, height=args.height)
+    R = sc.Renderer(data, device=local)
+    stream = torch.cuda.ExternalStream(R.stream())
+    spp = args.spp
+    path_samples = args.width * args.height * spp
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    # ---- device-timed steps
+    for _ in range(args.warmup):
+        R.render(spp)
+    R.sync()
+    barrier()
+    torch.cuda.synchronize()
+    L = nat.lib()
+    launches0 = L.pt_kernel_launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            R.render(spp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = L.pt_kernel_launch_count() - launches0
+    ms = e0.elapsed_time(e1)
+    barrier()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps * path_samples / (ms_max * 1e-3) / 1e6
+
+    # ---- end-to-end through the public API with host buffers
+    img_host = torch.empty((args.height, args.width, 4), dtype=torch.float32, pin_memory=True)
+    mats = [m for m in data.materials]
+    h2d = sum(ctypes.sizeof(m.params()) for m in mats)
+    d2h = img_host.numel() * 4
+    for _ in range(2):
+        R.apply_camera()
+        for m in mats:
+            R.update_material(m)
+        R.render(spp)
+        nat.call("pt_readback", R.ctx, img_host.data_ptr())
+    barrier()
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        R.apply_camera()           # camera variables (and a cleared accumulation buffer)
+        for m in mats:             # material parameters, copied host -> device
+            R.update_material(m)
+        R.render(spp)
+        nat.call("pt_readback", R.ctx, img_host.data_ptr())  # float4 image -> pinned host memory
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.steps * path_samples / (float(t.item()) * 1e-3) / 1e6
+
+    # ---- roofline of the dominant kernel (closest-hit extend), from a separately profiled render
+    nat.call("pt_set_profiling", R.ctx, 1)
+    R.render(spp)
+    st = R.stats()
+    nat.call("pt_set_profiling", R.ctx, 0)
+    peak, peak_kind = load_peaks()
+    ext_bytes = st.segments * EXTEND_BYTES_PER_SEGMENT
+    achieved = ext_bytes / (st.extend_ms * 1e-3) / 1e9 if st.extend_ms > 0 else None
+    traffic = traffic_from_profile()
+    roofline = {"bound": "hbm", "kernel": "k_extend (closest-hit traversal + material binning)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                "peak_source": peak_kind,
+                "traffic": traffic, "extend_share_of_render": st.extend_ms / st.gpu_ms if st.gpu_ms else None,
+                "segments_per_path": st.segments / st.path_samples, "shadow_rays_per_path": st.shadow_rays / st.path_samples,
+                "algorithmic_bytes_per_segment": EXTEND_BYTES_PER_SEGMENT,
+                "giga_rays_per_s": (st.segments + st.shadow_rays) / (st.gpu_ms * 1e-3) / 1e9}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "path_samples_per_step": path_samples, "parallelism": "replicas (one independent render per GPU)",
+                   "l2": "inputs larger than L2: per-path wavefront state of %.1f GB per step" % (path_samples * 176 / 1e9)},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": roofline,
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+        "stats": {"capped_walks": st.capped_walks, "clamped_indices": st.clamped_indices},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(data)
+    R.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1 and args.impl == "ours":
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -172,6 +172,15 @@ pt_status pt_readback_device(pt_ctx* ctx, float* d_rgba);
 pt_status pt_sync(pt_ctx* ctx);
 /* Counters and timings of the last pt_render_frames (synchronizes). */
 pt_status pt_get_render_stats(pt_ctx* ctx, pt_render_stats* out);
+/* Launch options (the autotuner's search space):
+ *   "extend_mode"  0 = one ray per thread with block-aggregated queue appends,
+ *                  1 = persistent warps that refill finished lanes with new rays (default)
+ *   "refill"       persistent kernels refill a warp when at least this many lanes are idle (1..32, default 24) */
+pt_status pt_set_option(pt_ctx* ctx, const char* name, int64_t value);
+/* When enabled, CUDA events bracket every extend (closest-hit) launch and pt_get_render_stats
+ * reports their summed device time in extend_ms.  Off by default (the events serialise nothing
+ * but cost a few microseconds per bounce). */
+pt_status pt_set_profiling(pt_ctx* ctx, int enable);
 /* Upper bound on paths kept in flight by one wavefront pass (frames are grouped to fit). */
 pt_status pt_set_max_paths_in_flight(pt_ctx* ctx, uint64_t max_paths);
 

@@ -67,6 +67,8 @@ SIGNATURES = {
     "pt_sync": (I32, [P]),
     "pt_get_render_stats": (I32, [P, P]),
     "pt_set_max_paths_in_flight": (I32, [P, U64]),
+    "pt_set_profiling": (I32, [P, I32]),
+    "pt_set_option": (I32, [P, ctypes.c_char_p, ctypes.c_int64]),
     "pt_trace_closest": (I32, [P, P, P, U32, P, P, P]),
     "pt_trace_any": (I32, [P, P, P, U32, P]),
 }

@@ -176,6 +176,8 @@ pt_status pt_context_destroy(pt_ctx* ctx)
   Context& c = ctx->c;
   for (cudaEvent_t ev : {c.ev0, c.ev1, c.ext0, c.ext1})
     if (ev) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : c.prof_events)
+    if (ev) cudaEventDestroy(ev);
   cudaStream_t s = c.stream;
   delete ctx;  // frees device buffers
   if (s) cudaStreamDestroy(s);
@@ -384,8 +386,31 @@ pt_status pt_sync(pt_ctx* ctx)
 pt_status pt_set_max_paths_in_flight(pt_ctx* ctx, uint64_t max_paths)
 {
   if (!ctx) return fail(PT_INVALID_ARG, "null context");
-  if (max_paths < 1024 || max_paths > (1ull << 30)) return fail(PT_INVALID_ARG, "pt_set_max_paths_in_flight: must be in [1024, 2^30]");
+  if (max_paths < 1 || max_paths > (1ull << 30)) return fail(PT_INVALID_ARG, "pt_set_max_paths_in_flight: must be in [1, 2^30]");
   ctx->c.max_paths = max_paths;
+  return PT_OK;
+}
+
+pt_status pt_set_option(pt_ctx* ctx, const char* name, int64_t value)
+{
+  if (!ctx || !name) return fail(PT_INVALID_ARG, "pt_set_option: null argument");
+  std::string k(name);
+  if (k == "extend_mode") {
+    if (value != 0 && value != 1) return fail(PT_INVALID_ARG, "pt_set_option: extend_mode must be 0 or 1");
+    ctx->c.opt.extend_mode = (int)value;
+  } else if (k == "refill") {
+    if (value < 1 || value > 32) return fail(PT_INVALID_ARG, "pt_set_option: refill must be in [1, 32]");
+    ctx->c.opt.refill = (int)value;
+  } else {
+    return fail(PT_INVALID_ARG, "pt_set_option: unknown option " + k);
+  }
+  return PT_OK;
+}
+
+pt_status pt_set_profiling(pt_ctx* ctx, int enable)
+{
+  if (!ctx) return fail(PT_INVALID_ARG, "null context");
+  ctx->c.profile = enable != 0;
   return PT_OK;
 }
 

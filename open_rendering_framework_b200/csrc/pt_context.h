@@ -66,9 +66,17 @@ enum CounterSlot {
   CNT_CAPPED = 12,
   CNT_CLAMPED = 14,
   CNT_ERROR = 16,
+  CNT_FETCH_EXT = 18,
+  CNT_FETCH_SH = 19,
   kCounters = 32
 };
 enum QueueClass { QC_MISS = 0, QC_LIGHT = 1, QC_DIFFUSE = 2, QC_METAL = 3, QC_GLASS = 4, kQueues = 5 };
+
+// Tunable launch options (pt_set_option); the autotuner searches over these.
+struct Options {
+  int extend_mode = 1;  // 0: one ray per thread, block-aggregated appends; 1: persistent warps with ray refill
+  int refill = 24;      // persistent kernels: refill when at least this many lanes of a warp are idle (1..32)
+};
 
 struct Context {
   int device = 0;
@@ -99,6 +107,10 @@ struct Context {
   Wavefront wf;
   uint64_t max_paths = 1ull << 24;
 
+  Options opt;
+  bool profile = false;
+  std::vector<cudaEvent_t> prof_events;  // pairs around each extend launch when profiling
+  uint32_t prof_pairs = 0;
   pt_render_stats stats{};
   bool stats_pending = false;
   uint64_t launches_at_start = 0;

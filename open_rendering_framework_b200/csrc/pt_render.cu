@@ -291,6 +291,151 @@ __global__ void __launch_bounds__(kBlock) k_extend(SceneDev S, WfDev w)
   if (traced) atomicAdd(cnt64(w.cnt, CNT_SEGMENTS_LO), (unsigned long long)traced);
 }
 
+// Warp-aggregated multi-queue append (no block barrier): lanes with cls in [0, kQueues) get distinct
+// slots; one atomic per warp and class.  All lanes of the warp must call it.
+__device__ __forceinline__ uint32_t warp_slot_multi(int cls, uint32_t* counters)
+{
+  const unsigned lane = threadIdx.x & 31;
+  uint32_t slot = 0;
+#pragma unroll
+  for (int q = 0; q < kQueues; ++q) {
+    unsigned m = __ballot_sync(0xffffffffu, cls == q);
+    if (m) {
+      int leader = __ffs(m) - 1;
+      uint32_t base = 0;
+      if ((int)lane == leader) base = atomicAdd(counters + q, (uint32_t)__popc(m));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (cls == q) slot = base + __popc(m & lanemask_lt());
+    }
+  }
+  return slot;
+}
+
+// Persistent closest-hit kernel with dynamic ray fetch: every warp keeps 32 rays in flight and,
+// whenever at least `refill` of its lanes have finished (or the queue is drained and all have),
+// hands the finished ones to the material queues and fetches new rays for the idle lanes with one
+// atomic.  Traversal state (pt_scene.cuh TravState) is resumable, so lanes never wait for the
+// slowest ray of a whole block (T. Aila, S. Laine, "Understanding the efficiency of ray traversal
+// on GPUs", HPG 2009: persistent threads with ray replacement).
+__global__ void __launch_bounds__(kBlock) k_extend_persistent(SceneDev S, WfDev w, int refill)
+{
+  const uint32_t n = w.cnt[w.in_slot];
+  uint32_t* fetch = w.cnt + CNT_FETCH_EXT;
+  const float eps = S.integ.scene_epsilon;
+  const unsigned lane = threadIdx.x & 31;
+  bool has = false, done = false, drained = false;
+  uint32_t pid = 0, traced = 0;
+  float3 o = f3s(0.0f), d = f3s(0.0f);
+  RayPre rp;
+  rp.inv = f3s(0.0f);
+  Hit h;
+  h.t = 0.0f; h.u = h.v = 0.0f; h.prim = -1;
+  TravState st;
+  trav_init(st);
+  for (;;) {
+    unsigned idle = __ballot_sync(0xffffffffu, !has);
+    if (!drained && (__popc(idle) >= refill || idle == 0xffffffffu)) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(fetch, (uint32_t)__popc(idle));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base + __popc(idle) >= n) drained = true;
+      if (!has) {
+        uint32_t i = base + __popc(idle & lanemask_lt());
+        if (i < n) {
+          pid = w.q_in[i];
+          float4 o4 = w.ray_o[pid], d4 = w.ray_d[pid];
+          o = ld3(o4);
+          d = ld3(d4);
+          rp = ray_pre(o, d);
+          h.t = kDefaultMax;
+          h.u = h.v = 0.0f;
+          h.prim = -1;
+          trav_init(st);
+          has = true;
+          done = false;
+          ++traced;
+        }
+      }
+    }
+    if (__ballot_sync(0xffffffffu, has) == 0) break;
+    for (;;) {
+      if (has && !done) done = trav_step_closest(S, o, d, rp, eps, h, st);
+      unsigned fin = __ballot_sync(0xffffffffu, !has || done);
+      if (fin == 0xffffffffu || (!drained && __popc(fin) >= refill)) break;
+    }
+    int cls = -1;
+    if (has && done) {
+      w.hit[pid] = make_float4(h.t, h.u, h.v, as_float(h.prim));
+      cls = h.prim < 0 ? QC_MISS : class_of(__ldg(&S.mats[__ldg(&S.tri_info[h.prim].w)].type));
+    }
+    uint32_t slot = warp_slot_multi(cls, w.cnt + CNT_Q_MISS);
+    if (cls >= 0) w.q_mat[(size_t)cls * w.cap + slot] = pid;
+    if (has && done) has = false;
+  }
+  traced += __shfl_xor_sync(0xffffffffu, traced, 16);
+  traced += __shfl_xor_sync(0xffffffffu, traced, 8);
+  traced += __shfl_xor_sync(0xffffffffu, traced, 4);
+  traced += __shfl_xor_sync(0xffffffffu, traced, 2);
+  traced += __shfl_xor_sync(0xffffffffu, traced, 1);
+  if (lane == 0 && traced) atomicAdd(cnt64(w.cnt, CNT_SEGMENTS_LO), (unsigned long long)traced);
+}
+
+// Persistent any-hit kernel for the shadow queue (same ray replacement).
+__global__ void __launch_bounds__(kBlock) k_shadow_persistent(SceneDev S, WfDev w, int refill)
+{
+  const uint32_t n = w.cnt[CNT_SHADOW];
+  uint32_t* fetch = w.cnt + CNT_FETCH_SH;
+  const unsigned lane = threadIdx.x & 31;
+  bool has = false, drained = false;
+  int res = 0;
+  uint32_t slot = 0;
+  float3 o = f3s(0.0f), d = f3s(0.0f);
+  float tmin = 0.0f, tmax = 0.0f;
+  RayPre rp;
+  rp.inv = f3s(0.0f);
+  TravState st;
+  trav_init(st);
+  for (;;) {
+    unsigned idle = __ballot_sync(0xffffffffu, !has);
+    if (!drained && (__popc(idle) >= refill || idle == 0xffffffffu)) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(fetch, (uint32_t)__popc(idle));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (base + __popc(idle) >= n) drained = true;
+      if (!has) {
+        uint32_t i = base + __popc(idle & lanemask_lt());
+        if (i < n) {
+          slot = i;
+          float4 o4 = w.sh_o[i], d4 = w.sh_d[i];
+          o = ld3(o4);
+          d = ld3(d4);
+          tmin = o4.w;
+          tmax = d4.w;
+          rp = ray_pre(o, d);
+          trav_init(st);
+          has = true;
+          res = 0;
+        }
+      }
+    }
+    if (__ballot_sync(0xffffffffu, has) == 0) break;
+    for (;;) {
+      if (has && res == 0) res = trav_step_any(S, o, d, rp, tmin, tmax, st);
+      unsigned fin = __ballot_sync(0xffffffffu, !has || res != 0);
+      if (fin == 0xffffffffu || (!drained && __popc(fin) >= refill)) break;
+    }
+    if (has && res != 0) {
+      if (res < 0) {
+        uint32_t p = w.sh_pid[slot];
+        float4 c = w.sh_c[slot], r = w.rad[p];
+        w.rad[p] = make_float4(r.x + c.x, r.y + c.y, r.z + c.z, 0.0f);
+      }
+      has = false;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && n) atomicAdd(cnt64(w.cnt, CNT_SHADOW_TOTAL), (unsigned long long)n);
+}
+
 // constantbg.cu:16-19
 __global__ void __launch_bounds__(kBlock) k_shade_miss(SceneDev S, WfDev w)
 {
@@ -695,7 +840,12 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
   w.cap = wf.cap;
   const float4* geo_p = geo.as<float4>();
   const int grid_trace = sm_count() * 8, grid_shade = sm_count() * 8;
+  int occ_ext = 0, occ_sh = 0;
+  PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, k_extend_persistent, kBlock, 0), "occupancy");
+  PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, k_shadow_persistent, kBlock, 0), "occupancy");
+  const int grid_persist = sm_count() * std::max(1, std::min(occ_ext, occ_sh));
   PT_CHECK_CUDA(cudaMemsetAsync(w.cnt, 0, kCounters * 4, c.stream), "reset counters");
+  c.prof_pairs = 0;
   PT_CHECK_CUDA(cudaEventRecord(c.ev0, c.stream), "event");
   float extend_ms = 0.0f;
   uint32_t extend_launches = 0;
@@ -712,14 +862,33 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
     const int passes = c.integ.max_depth + 2;
     for (int b = 0; b < passes; ++b) {
       PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_Q_MISS, 0, 6 * 4, c.stream), "reset queues");
+      PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_FETCH_EXT, 0, 2 * 4, c.stream), "reset fetch counters");
       PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + w.out_slot, 0, 4, c.stream), "reset queues");
-      k_extend<<<grid_trace, kBlock, 0, c.stream>>>(S, w);
+      if (c.profile) {
+        while (c.prof_events.size() < 2 * (size_t)(c.prof_pairs + 1)) {
+          cudaEvent_t ev;
+          PT_CHECK_CUDA(cudaEventCreate(&ev), "profiling event");
+          c.prof_events.push_back(ev);
+        }
+        PT_CHECK_CUDA(cudaEventRecord(c.prof_events[2 * c.prof_pairs], c.stream), "profiling event");
+      }
+      if (c.opt.extend_mode == 1)
+        k_extend_persistent<<<grid_persist, kBlock, 0, c.stream>>>(S, w, c.opt.refill);
+      else
+        k_extend<<<grid_trace, kBlock, 0, c.stream>>>(S, w);
+      if (c.profile) {
+        PT_CHECK_CUDA(cudaEventRecord(c.prof_events[2 * c.prof_pairs + 1], c.stream), "profiling event");
+        ++c.prof_pairs;
+      }
       k_shade_miss<<<grid_shade, kBlock, 0, c.stream>>>(S, w);
       k_shade_light<<<grid_shade, kBlock, 0, c.stream>>>(S, w, geo_p);
       k_shade_diffuse<<<grid_shade, kBlock, 0, c.stream>>>(S, w, geo_p);
       k_shade_metal<<<grid_shade, kBlock, 0, c.stream>>>(S, w, geo_p);
       k_shade_glass<<<grid_shade, kBlock, 0, c.stream>>>(S, w, geo_p);
-      k_shadow<<<grid_trace, kBlock, 0, c.stream>>>(S, w);
+      if (c.opt.extend_mode == 1)
+        k_shadow_persistent<<<grid_persist, kBlock, 0, c.stream>>>(S, w, c.opt.refill);
+      else
+        k_shadow<<<grid_trace, kBlock, 0, c.stream>>>(S, w);
       count_launch(7);
       ++extend_launches;
       std::swap(w.q_in, w.q_out);
@@ -763,6 +932,13 @@ pt_status pt_get_render_stats(pt_ctx* ctx, pt_render_stats* out)
     float ms = 0.0f;
     PT_CHECK_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1), "event time");
     c.stats.gpu_ms = ms;
+    float ext = 0.0f;
+    for (uint32_t k = 0; k < c.prof_pairs; ++k) {
+      float e = 0.0f;
+      PT_CHECK_CUDA(cudaEventElapsedTime(&e, c.prof_events[2 * k], c.prof_events[2 * k + 1]), "event time");
+      ext += e;
+    }
+    c.stats.extend_ms = ext;
     c.stats_pending = false;
   }
   *out = c.stats;

@@ -183,10 +183,117 @@ PT_HD bool leaf_any(const SceneDev& S, uint32_t code, const float3& o, const flo
   return false;
 }
 
-// Stackless closest-hit traversal.  A 64-bit trail marks, per depth, whether the far child of the
-// node at that depth is still pending, and a second 64-bit word records which child it is; the way
-// back up follows the parent index stored in each node.  When a pending far child is resumed its box
-// is re-tested against the current closest distance.  No per-ray stack lives in local memory.
+// Stackless traversal state.  A 64-bit trail marks, per depth, whether the far child of the node at
+// that depth is still pending (`pend`), and a second 64-bit word records which child it is
+// (`farc1`); the way back up follows the parent index stored in each node.  No per-ray stack lives
+// in local memory.
+struct TravState {
+  int cur, depth;
+  unsigned long long pend, farc1;
+};
+PT_HD void trav_init(TravState& st)
+{
+  st.cur = 0;
+  st.depth = 0;
+  st.pend = 0ull;
+  st.farc1 = 0ull;
+}
+
+// Backtrack to the deepest pending child.  Closest-hit: the pending far child's box is re-tested
+// against the current closest distance when it is resumed.  Returns false when the root is done.
+PT_HD bool trav_backtrack(const SceneDev& S, const float3& o, const RayPre& rp, float tmin, float tlimit, TravState& st, bool retest)
+{
+  for (;;) {
+    if (st.depth == 0) return false;
+    int parent = PT_LDG(reinterpret_cast<const int*>(S.nodes + 4 * (size_t)st.cur + 3) + 2);
+    --st.depth;
+    unsigned long long bit = 1ull << st.depth;
+    if (st.pend & bit) {
+      st.pend &= ~bit;
+      const float4* pn = S.nodes + 4 * (size_t)parent;
+      int4 p3 = PT_LDG(reinterpret_cast<const int4*>(pn + 3));
+      int far = (st.farc1 & bit) ? p3.y : p3.x;
+      bool go = true;
+      if (retest) {
+        float tf;
+        if (st.farc1 & bit) {
+          float4 b1 = PT_LDG(pn + 1), b2 = PT_LDG(pn + 2);
+          tf = slab(b1.x, b1.y, b1.z, b1.w, b2.z, b2.w, o, rp, tmin, tlimit);
+        } else {
+          float4 b0 = PT_LDG(pn), b2 = PT_LDG(pn + 2);
+          tf = slab(b0.x, b0.y, b0.z, b0.w, b2.x, b2.y, o, rp, tmin, tlimit);
+        }
+        go = tf <= tlimit * kSlack;
+      }
+      if (go) {
+        st.cur = far;
+        ++st.depth;
+        return true;
+      }
+    }
+    st.cur = parent;
+  }
+}
+
+// One closest-hit step: visit node st.cur (test both child boxes, intersect leaf children, descend
+// near-first or backtrack).  Returns true when the traversal is finished.
+PT_HD bool trav_step_closest(const SceneDev& S, const float3& o, const float3& d, const RayPre& rp, float tmin, Hit& h, TravState& st)
+{
+  const float4* nd = S.nodes + 4 * (size_t)st.cur;
+  float4 n0 = PT_LDG(nd), n1 = PT_LDG(nd + 1), n2 = PT_LDG(nd + 2);
+  int4 n3 = PT_LDG(reinterpret_cast<const int4*>(nd + 3));
+  float t0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, rp, tmin, h.t);
+  float t1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, rp, tmin, h.t);
+  bool h0 = t0 != as_float(0x7f800000), h1 = t1 != as_float(0x7f800000);
+  if (h0 && n3.x < 0) { leaf_closest(S, (uint32_t)n3.x, o, d, tmin, h); h0 = false; }
+  if (h1 && n3.y < 0) { leaf_closest(S, (uint32_t)n3.y, o, d, tmin, h); h1 = false; }
+  h0 = h0 && t0 <= h.t * kSlack;
+  h1 = h1 && t1 <= h.t * kSlack;
+  if (h0 && h1) {
+    bool near1 = t1 < t0;
+    unsigned long long bit = 1ull << st.depth;
+    st.pend |= bit;
+    if (near1) st.farc1 &= ~bit; else st.farc1 |= bit;
+    st.cur = near1 ? n3.y : n3.x;
+    ++st.depth;
+    return false;
+  }
+  if (h0 || h1) {
+    st.cur = h0 ? n3.x : n3.y;
+    ++st.depth;
+    return false;
+  }
+  return !trav_backtrack(S, o, rp, tmin, h.t, st, true);
+}
+
+// One any-hit step (children in fixed order, child 1 pending when both are hit).  Returns 1 when a
+// triangle with tmin < t < tmax was found, -1 when the traversal finished without one, 0 otherwise.
+PT_HD int trav_step_any(const SceneDev& S, const float3& o, const float3& d, const RayPre& rp, float tmin, float tmax, TravState& st)
+{
+  const float4* nd = S.nodes + 4 * (size_t)st.cur;
+  float4 n0 = PT_LDG(nd), n1 = PT_LDG(nd + 1), n2 = PT_LDG(nd + 2);
+  int4 n3 = PT_LDG(reinterpret_cast<const int4*>(nd + 3));
+  float t0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, rp, tmin, tmax);
+  float t1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, rp, tmin, tmax);
+  bool h0 = t0 != as_float(0x7f800000), h1 = t1 != as_float(0x7f800000);
+  if (h0 && n3.x < 0) { if (leaf_any(S, (uint32_t)n3.x, o, d, tmin, tmax)) return 1; h0 = false; }
+  if (h1 && n3.y < 0) { if (leaf_any(S, (uint32_t)n3.y, o, d, tmin, tmax)) return 1; h1 = false; }
+  if (h0 && h1) {
+    unsigned long long bit = 1ull << st.depth;
+    st.pend |= bit;
+    st.farc1 |= bit;
+    st.cur = n3.x;
+    ++st.depth;
+    return 0;
+  }
+  if (h0 || h1) {
+    st.cur = h0 ? n3.x : n3.y;
+    ++st.depth;
+    return 0;
+  }
+  return trav_backtrack(S, o, rp, tmin, tmax, st, false) ? 0 : -1;
+}
+
 PT_HD Hit trace_closest(const SceneDev& S, const float3& o, const float3& d, float tmin, float tmax)
 {
   Hit h;
@@ -194,106 +301,20 @@ PT_HD Hit trace_closest(const SceneDev& S, const float3& o, const float3& d, flo
   h.u = h.v = 0.0f;
   h.prim = -1;
   RayPre rp = ray_pre(o, d);
-  int cur = 0, depth = 0;
-  unsigned long long pend = 0ull, farc1 = 0ull;
-  for (;;) {
-    const float4* nd = S.nodes + 4 * (size_t)cur;
-    float4 n0 = PT_LDG(nd), n1 = PT_LDG(nd + 1), n2 = PT_LDG(nd + 2);
-    int4 n3 = PT_LDG(reinterpret_cast<const int4*>(nd + 3));
-    float t0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, rp, tmin, h.t);
-    float t1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, rp, tmin, h.t);
-    bool h0 = t0 != as_float(0x7f800000), h1 = t1 != as_float(0x7f800000);
-    if (h0 && n3.x < 0) { leaf_closest(S, (uint32_t)n3.x, o, d, tmin, h); h0 = false; }
-    if (h1 && n3.y < 0) { leaf_closest(S, (uint32_t)n3.y, o, d, tmin, h); h1 = false; }
-    h0 = h0 && t0 <= h.t * kSlack;
-    h1 = h1 && t1 <= h.t * kSlack;
-    if (h0 && h1) {
-      bool near1 = t1 < t0;
-      pend |= 1ull << depth;
-      if (near1) farc1 &= ~(1ull << depth); else farc1 |= 1ull << depth;
-      cur = near1 ? n3.y : n3.x;
-      ++depth;
-      continue;
-    }
-    if (h0 || h1) {
-      cur = h0 ? n3.x : n3.y;
-      ++depth;
-      continue;
-    }
-    // backtrack to the deepest pending far child
-    for (;;) {
-      if (depth == 0) return h;
-      int parent = PT_LDG(reinterpret_cast<const int*>(S.nodes + 4 * (size_t)cur + 3) + 2);
-      --depth;
-      unsigned long long bit = 1ull << depth;
-      if (pend & bit) {
-        pend &= ~bit;
-        const float4* pn = S.nodes + 4 * (size_t)parent;
-        int4 p3 = PT_LDG(reinterpret_cast<const int4*>(pn + 3));
-        float tf;
-        int far;
-        if (farc1 & bit) {
-          float4 b1 = PT_LDG(pn + 1), b2 = PT_LDG(pn + 2);
-          tf = slab(b1.x, b1.y, b1.z, b1.w, b2.z, b2.w, o, rp, tmin, h.t);
-          far = p3.y;
-        } else {
-          float4 b0 = PT_LDG(pn), b2 = PT_LDG(pn + 2);
-          tf = slab(b0.x, b0.y, b0.z, b0.w, b2.x, b2.y, o, rp, tmin, h.t);
-          far = p3.x;
-        }
-        if (tf <= h.t * kSlack) {
-          cur = far;
-          ++depth;
-          break;
-        }
-      }
-      cur = parent;
-    }
-  }
+  TravState st;
+  trav_init(st);
+  while (!trav_step_closest(S, o, d, rp, tmin, h, st)) {}
+  return h;
 }
 
-// Stackless any-hit traversal (shadow rays): same trail, children visited in fixed order, stops at
-// the first triangle with tmin < t < tmax.
 PT_HD bool trace_any(const SceneDev& S, const float3& o, const float3& d, float tmin, float tmax)
 {
   RayPre rp = ray_pre(o, d);
-  int cur = 0, depth = 0;
-  unsigned long long pend = 0ull;
-  for (;;) {
-    const float4* nd = S.nodes + 4 * (size_t)cur;
-    float4 n0 = PT_LDG(nd), n1 = PT_LDG(nd + 1), n2 = PT_LDG(nd + 2);
-    int4 n3 = PT_LDG(reinterpret_cast<const int4*>(nd + 3));
-    float t0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, rp, tmin, tmax);
-    float t1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, rp, tmin, tmax);
-    bool h0 = t0 != as_float(0x7f800000), h1 = t1 != as_float(0x7f800000);
-    if (h0 && n3.x < 0) { if (leaf_any(S, (uint32_t)n3.x, o, d, tmin, tmax)) return true; h0 = false; }
-    if (h1 && n3.y < 0) { if (leaf_any(S, (uint32_t)n3.y, o, d, tmin, tmax)) return true; h1 = false; }
-    if (h0 && h1) {
-      pend |= 1ull << depth;  // child 1 pending
-      cur = n3.x;
-      ++depth;
-      continue;
-    }
-    if (h0 || h1) {
-      cur = h0 ? n3.x : n3.y;
-      ++depth;
-      continue;
-    }
-    for (;;) {
-      if (depth == 0) return false;
-      int parent = PT_LDG(reinterpret_cast<const int*>(S.nodes + 4 * (size_t)cur + 3) + 2);
-      --depth;
-      unsigned long long bit = 1ull << depth;
-      if (pend & bit) {
-        pend &= ~bit;
-        int4 p3 = PT_LDG(reinterpret_cast<const int4*>(S.nodes + 4 * (size_t)parent + 3));
-        cur = p3.y;
-        ++depth;
-        break;
-      }
-      cur = parent;
-    }
-  }
+  TravState st;
+  trav_init(st);
+  int r;
+  while ((r = trav_step_any(S, o, d, rp, tmin, tmax, st)) == 0) {}
+  return r > 0;
 }
 
 }  // namespace pt
