@@ -62,6 +62,20 @@ pt_status pt_bsdf_queries(const float* d_wo_soa, const float* d_alpha, uint64_t 
  * results back and synchronizes.  Device scratch is allocated per call. */
 pt_status pt_bsdf_queries_host(const float* wo_soa, const float* alpha, uint64_t n, uint64_t first_index,
                                uint64_t n_ggx_below, float eta, float* wi_soa, float* f, float* pdf, float* F);
+/* Same query batch through host buffers, without allocating any device memory.  This entry point
+ * has no counterpart in the reference.  It exists for callers that must not call cudaMalloc: a
+ * host application whose device memory is already handed out by its own allocator or pool (for
+ * example a renderer that reserved the GPU's memory for its scenes at start-up), and a real-time
+ * thread such as an editor's UI thread re-evaluating a material, where cudaMalloc/cudaFree would
+ * synchronise the device and stall the frame.  Instead of per-call staging buffers it uses one
+ * fixed device array of 65536 queries (2.5 MiB, held by every GPU that loads the library until the
+ * process exits); larger batches are rejected with PT_INVALID_ARG.  The first call on a device looks
+ * up that array's device address, so make the first call on each device before any stream capture.
+ * All calls share the one array: calls that overlap on the GPU (from several host threads) race, so
+ * serialise them.  The call is synchronous and allocates nothing; inputs and outputs are host
+ * pointers as in pt_bsdf_queries_host, and the results are identical to it. */
+pt_status pt_bsdf_queries_host_noalloc(const float* wo_soa, const float* alpha, uint64_t n, uint64_t first_index,
+                                       uint64_t n_ggx_below, float eta, float* wi_soa, float* f, float* pdf, float* F);
 /* The synthetic query inputs used by the benchmark (alpha in [0.05,1], cos(theta_o) in [0.01,1],
  * phi in [0,2pi) drawn with rnd_tea from tea<16>(i,1)), generated on the host. */
 pt_status pt_c1_make_inputs(uint64_t n, uint64_t first_index, float* wo_soa, float* alpha);

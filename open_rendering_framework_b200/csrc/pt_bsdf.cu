@@ -6,6 +6,7 @@
 // Newton loop in double/float), so it runs a grid-stride loop over a grid sized to a multiple of the
 // SM count; queries are ordered GGX-then-Beckmann, so warps never mix distributions except at the
 // single boundary warp.
+#include <mutex>
 #include <vector>
 
 #include "pt_common.cuh"
@@ -61,6 +62,33 @@ __global__ void k_rng_streams(int kind, uint32_t* seeds, uint64_t n, uint32_t dr
   }
 }
 
+// Staging area of pt_bsdf_queries_host_noalloc: room for kNoAllocMaxQueries queries, laid out as
+// wo (3n) | alpha (n) | wi (3n) | f (n) | pdf (n) | F (n).  Every GPU that loads this library holds
+// it (2.5 MiB) until the process exits.
+constexpr uint64_t kNoAllocMaxQueries = 65536;
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocMaxQueries * 10];
+
+// Device address of g_noalloc_scratch per device, looked up on the first call on that device.  The
+// symbol's name in host code only stands for the device array; its device address must come from
+// cudaGetSymbolAddress with that device current.
+static std::mutex g_noalloc_mu;
+static std::vector<float*> g_noalloc_ptr;
+
+static pt_status noalloc_scratch(float** out)
+{
+  int dev = 0;
+  PT_CHECK_CUDA(cudaGetDevice(&dev), "pt_bsdf_queries_host_noalloc cudaGetDevice");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if ((int)g_noalloc_ptr.size() <= dev) g_noalloc_ptr.resize(dev + 1, nullptr);
+  if (!g_noalloc_ptr[dev]) {
+    float* p = nullptr;
+    PT_CHECK_CUDA(cudaGetSymbolAddress((void**)&p, g_noalloc_scratch), "pt_bsdf_queries_host_noalloc cudaGetSymbolAddress");
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return PT_OK;
+}
+
 }  // namespace pt
 
 using namespace pt;
@@ -104,6 +132,33 @@ pt_status pt_bsdf_queries_host(const float* wo_soa, const float* alpha, uint64_t
   }
   cudaFree(d);
   return st;
+}
+
+pt_status pt_bsdf_queries_host_noalloc(const float* wo_soa, const float* alpha, uint64_t n, uint64_t first_index, uint64_t n_ggx_below,
+                                       float eta, float* wi_soa, float* f, float* pdf, float* F)
+{
+  if (n == 0) return PT_OK;
+  if (n > kNoAllocMaxQueries)
+    return fail(PT_INVALID_ARG, "pt_bsdf_queries_host_noalloc: at most 65536 queries per call (the staging area is a fixed 2.5 MiB "
+                                "device array); split the batch or use pt_bsdf_queries_host");
+  if (!wo_soa || !alpha || !wi_soa || !f || !pdf || !F) return fail(PT_INVALID_ARG, "pt_bsdf_queries_host_noalloc: null pointer");
+  float* d = nullptr;
+  pt_status st = noalloc_scratch(&d);
+  if (st != PT_OK) return st;
+  // Every output element k < n is written by the kernel, and the inputs are copied in before it
+  // runs, so nothing left over from an earlier call is read and nothing needs clearing.
+  float *d_wo = d, *d_a = d + 3 * n, *d_wi = d + 4 * n, *d_f = d + 7 * n, *d_pdf = d + 8 * n, *d_F = d + 9 * n;
+  cudaError_t e = cudaMemcpy(d_wo, wo_soa, 3 * n * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_a, alpha, n * sizeof(float), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_status(e, "pt_bsdf_queries_host_noalloc H2D");
+  st = pt_bsdf_queries(d_wo, d_a, n, first_index, n_ggx_below, eta, d_wi, d_f, d_pdf, d_F, nullptr);
+  if (st != PT_OK) return st;
+  e = cudaMemcpy(wi_soa, d_wi, 3 * n * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(f, d_f, n * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(pdf, d_pdf, n * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(F, d_F, n * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_status(e, "pt_bsdf_queries_host_noalloc D2H");
+  return PT_OK;
 }
 
 pt_status pt_c1_make_inputs(uint64_t n, uint64_t first_index, float* wo_soa, float* alpha)
