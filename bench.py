@@ -61,13 +61,14 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def traffic_from_profile():
-    """Per-launch DRAM bytes of the extend kernel from the committed ncu summary, if present."""
+def traffic_per_segment_from_profile():
+    """DRAM bytes per traced segment of the extend kernel, from the committed ncu summary (a small
+    capture of the same kernel; traffic grows in proportion to the rays a launch traces)."""
     path = os.path.join(ROOT, "profiles", "k_extend_single_scene.md")
     if not os.path.exists(path):
         return None
     for line in open(path):
-        if line.startswith("traffic_bytes_per_launch_full_size:"):
+        if line.startswith("traffic_bytes_per_segment:"):
             try:
                 return float(line.split(":", 1)[1].strip())
             except ValueError:
@@ -288,12 +289,16 @@ def run_ours(args, world, rank, local):
     nat.call("pt_set_profiling", R.ctx, 0)
     peak, peak_kind = load_peaks()
     ext_bytes = st.segments * EXTEND_BYTES_PER_SEGMENT
+    # per launch: algorithmic bytes of one launch / that launch's average duration == totals ratio
     achieved = ext_bytes / (st.extend_ms * 1e-3) / 1e9 if st.extend_ms > 0 else None
-    traffic = traffic_from_profile()
+    per_seg = traffic_per_segment_from_profile()
+    launches_ext = max(1, st.extend_launches)
+    traffic = per_seg * st.segments / launches_ext if per_seg else None
     roofline = {"bound": "hbm", "kernel": "k_extend (closest-hit traversal + material binning)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                 "peak_source": peak_kind,
-                "traffic": traffic, "extend_share_of_render": st.extend_ms / st.gpu_ms if st.gpu_ms else None,
+                "traffic": traffic, "traffic_unit": "bytes per launch (ncu small-case capture scaled by rays per launch)",
+                "extend_share_of_render": st.extend_ms / st.gpu_ms if st.gpu_ms else None,
                 "segments_per_path": st.segments / st.path_samples, "shadow_rays_per_path": st.shadow_rays / st.path_samples,
                 "algorithmic_bytes_per_segment": EXTEND_BYTES_PER_SEGMENT,
                 "giga_rays_per_s": (st.segments + st.shadow_rays) / (st.gpu_ms * 1e-3) / 1e9}

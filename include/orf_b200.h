@@ -157,6 +157,15 @@ pt_status pt_set_camera(pt_ctx* ctx, const float eye[3], const float U[3], const
                         uint32_t height, const uint32_t patch_origin[2], const uint32_t patch_dims[2]);
 /* ConstantBackground: context["background_color"] (Background.cpp:13). */
 pt_status pt_set_background_constant(pt_ctx* ctx, const float color[3]);
+/* EnvMapBackground (Background.cpp:57-69): float4 texels (width*height, row-major, row 0 = v 0),
+ * looked up bilinearly with REPEAT wrap on every miss (envmap_background.cu:20-23).  The marginal and
+ * conditional pdf/cdf tables of env_cameras.cu:23-75 are built on the device.  A LightStruct with
+ * light_type 5 (an extension: the environment map as a light, sampled by sample_environment,
+ * Envmap.h:66-98) makes the diffuse shader's next-event estimation sample it; misses after such an
+ * estimate then add nothing, as emitter hits do. */
+pt_status pt_set_envmap(pt_ctx* ctx, const float* rgba, uint32_t width, uint32_t height);
+/* Copy the environment tables to host memory (any pointer may be NULL). */
+pt_status pt_get_envmap_tables(pt_ctx* ctx, float* marginal_pdf, float* marginal_cdf, float* conditional_pdf, float* conditional_cdf);
 /* Create a material of the given type from its parameter struct; returns its id. */
 pt_status pt_material_create(pt_ctx* ctx, uint32_t type, const void* params, size_t params_size, uint32_t* out_id);
 /* Replace the parameters of an existing material (same type); takes effect at the next render. */

@@ -26,6 +26,17 @@ SceneDev Context::view() const
   s.n_tri_lights = (int)tri_lights.size();
   s.n_tris = n_tris;
   s.bg_color = bg_color;
+  s.env.tex = d_env_tex.as<float4>();
+  s.env.marginal_pdf = d_env_mpdf.as<float>();
+  s.env.marginal_cdf = d_env_mcdf.as<float>();
+  s.env.conditional_pdf = d_env_cpdf.as<float>();
+  s.env.conditional_cdf = d_env_ccdf.as<float>();
+  s.env.w = env_w;
+  s.env.h = env_h;
+  s.env.present = env_present ? 1 : 0;
+  s.env.is_light = 0;
+  for (const LightRaw& l : lights)
+    if (l.type == ENVMAP_LIGHT) s.env.is_light = 1;
   s.cam = cam;
   s.integ = integ;
   return s;
@@ -132,6 +143,54 @@ __global__ void k_trace_any(SceneDev S, const float4* ot, const float4* dt, uint
   }
 }
 
+// ------------------------------------------------------------------ environment CDFs (env_cameras.cu:23-75)
+// env_luminance_camera: luminance_NTSC(texel at the texel centre) * sin(theta).
+__global__ void k_env_luminance(EnvDev E, float* lum)
+{
+  size_t n = (size_t)E.w * E.h;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(k % E.w), j = (int)(k / E.w);
+    float u = ((float)i + 0.5f) / (float)E.w, v = ((float)j + 0.5f) / (float)E.h;
+    float theta = (1.0f - v) * kPi;
+    float3 t = env_tex(E, u, v);
+    lum[k] = (t.x * 0.2989f + t.y * 0.5866f + t.z * 0.1145f) * sinf(theta);
+  }
+}
+// env_marginal_camera and the conditional half of env_pdf_camera: per row, the sequential float sum
+// in the reference's order (every prefix is the sum the reference recomputes per texel).
+__global__ void k_env_rows(EnvDev E, const float* lum, float* mf, float* cpdf, float* ccdf)
+{
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < E.h; j += gridDim.x * blockDim.x) {
+    const float* row = lum + (size_t)j * E.w;
+    float s = 0.0f;
+    for (int i = 0; i < E.w; ++i) s += row[i];
+    float m = s / (float)E.w;
+    mf[j] = m;
+    float c = 0.0f;
+    for (int i = 0; i < E.w; ++i) {
+      c += row[i];
+      cpdf[(size_t)j * E.w + i] = row[i] / m;
+      ccdf[(size_t)j * E.w + i] = (c / (float)E.w) / m;
+    }
+  }
+}
+// The marginal half of env_pdf_camera (one sequential pass) and the two entries forced to 1.
+__global__ void k_env_marginal(EnvDev E, const float* mf, float* mpdf, float* mcdf, float* ccdf)
+{
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  float total = 0.0f;
+  for (int j = 0; j < E.h; ++j) total += mf[j];
+  float m = total / (float)E.h;
+  float c = 0.0f;
+  for (int j = 0; j < E.h; ++j) {
+    c += mf[j];
+    mpdf[j] = mf[j] / m;
+    mcdf[j] = (c / (float)E.h) / m;
+  }
+  mcdf[E.h - 1] = 1.0f;
+  ccdf[(size_t)(E.h - 1) * E.w + (E.w - 1)] = 1.0f;
+}
+
 }  // namespace pt
 
 using namespace pt;
@@ -235,6 +294,51 @@ pt_status pt_set_background_constant(pt_ctx* ctx, const float color[3])
   return PT_OK;
 }
 
+pt_status pt_set_envmap(pt_ctx* ctx, const float* rgba, uint32_t width, uint32_t height)
+{
+  CTX_CHECK(ctx);
+  Context& c = ctx->c;
+  if (!rgba) return fail(PT_INVALID_ARG, "pt_set_envmap: null texels");
+  if (width < 2 || height < 2 || (uint64_t)width * height > (1ull << 26)) return fail(PT_INVALID_ARG, "pt_set_envmap: bad size");
+  for (uint64_t k = 0; k < 4ull * width * height; ++k)
+    if (!std::isfinite(rgba[k]) || rgba[k] < 0.0f) return fail(PT_INVALID_ARG, "pt_set_envmap: texels must be finite and >= 0");
+  size_t n = (size_t)width * height;
+  pt_status st = c.d_env_tex.reserve(n * sizeof(float4), "env texture");
+  if (st == PT_OK) st = c.d_env_lum.reserve(n * 4, "env luminance");
+  if (st == PT_OK) st = c.d_env_cpdf.reserve(n * 4, "env conditional pdf");
+  if (st == PT_OK) st = c.d_env_ccdf.reserve(n * 4, "env conditional cdf");
+  if (st == PT_OK) st = c.d_env_mf.reserve((size_t)height * 4, "env marginal");
+  if (st == PT_OK) st = c.d_env_mpdf.reserve((size_t)height * 4, "env marginal pdf");
+  if (st == PT_OK) st = c.d_env_mcdf.reserve((size_t)height * 4, "env marginal cdf");
+  if (st != PT_OK) return st;
+  PT_CHECK_CUDA(cudaMemcpyAsync(c.d_env_tex.p, rgba, n * sizeof(float4), cudaMemcpyHostToDevice, c.stream), "env upload");
+  c.env_w = (int)width;
+  c.env_h = (int)height;
+  c.env_present = true;
+  EnvDev E = c.view().env;
+  k_env_luminance<<<grid_for(n, 256, 8), 256, 0, c.stream>>>(E, c.d_env_lum.as<float>());
+  k_env_rows<<<(height + 127) / 128, 128, 0, c.stream>>>(E, c.d_env_lum.as<float>(), c.d_env_mf.as<float>(), c.d_env_cpdf.as<float>(),
+                                                         c.d_env_ccdf.as<float>());
+  k_env_marginal<<<1, 32, 0, c.stream>>>(E, c.d_env_mf.as<float>(), c.d_env_mpdf.as<float>(), c.d_env_mcdf.as<float>(), c.d_env_ccdf.as<float>());
+  count_launch(3);
+  PT_CHECK_CUDA(cudaGetLastError(), "pt_set_envmap launch");
+  PT_CHECK_CUDA(cudaStreamSynchronize(c.stream), "pt_set_envmap");
+  return PT_OK;
+}
+
+pt_status pt_get_envmap_tables(pt_ctx* ctx, float* marginal_pdf, float* marginal_cdf, float* conditional_pdf, float* conditional_cdf)
+{
+  CTX_CHECK(ctx);
+  Context& c = ctx->c;
+  if (!c.env_present) return fail(PT_NOT_READY, "pt_get_envmap_tables: no environment map");
+  size_t n = (size_t)c.env_w * c.env_h;
+  if (marginal_pdf) PT_CHECK_CUDA(cudaMemcpy(marginal_pdf, c.d_env_mpdf.p, (size_t)c.env_h * 4, cudaMemcpyDeviceToHost), "env tables");
+  if (marginal_cdf) PT_CHECK_CUDA(cudaMemcpy(marginal_cdf, c.d_env_mcdf.p, (size_t)c.env_h * 4, cudaMemcpyDeviceToHost), "env tables");
+  if (conditional_pdf) PT_CHECK_CUDA(cudaMemcpy(conditional_pdf, c.d_env_cpdf.p, n * 4, cudaMemcpyDeviceToHost), "env tables");
+  if (conditional_cdf) PT_CHECK_CUDA(cudaMemcpy(conditional_cdf, c.d_env_ccdf.p, n * 4, cudaMemcpyDeviceToHost), "env tables");
+  return PT_OK;
+}
+
 pt_status pt_material_create(pt_ctx* ctx, uint32_t type, const void* params, size_t params_size, uint32_t* out_id)
 {
   if (!ctx || !out_id) return fail(PT_INVALID_ARG, "pt_material_create: null argument");
@@ -309,7 +413,7 @@ pt_status pt_lights_upload(pt_ctx* ctx, const void* lights, uint32_t n_lights, c
   c.lights.assign((const LightRaw*)lights, (const LightRaw*)lights + n_lights);
   c.tri_lights.assign((const TriLightRaw*)triangle_lights, (const TriLightRaw*)triangle_lights + n_triangle_lights);
   for (const LightRaw& l : c.lights) {
-    if (l.type > SPHERICAL_LIGHT) return fail(PT_INVALID_ARG, "pt_lights_upload: unknown light_type");
+    if (l.type > ENVMAP_LIGHT) return fail(PT_INVALID_ARG, "pt_lights_upload: unknown light_type");
     if (l.type == TRIANGLES_AREA_LIGHT) {
       float cnt, start;
       memcpy(&cnt, &l.p[0], 4);

@@ -102,6 +102,9 @@ struct Context {
 
   DevBuf d_nodes, d_v0, d_e1, d_e2, d_info, d_normals, d_mats, d_lights, d_tri_lights;
   DevBuf d_accum;  // float4 per pixel
+  DevBuf d_env_tex, d_env_mpdf, d_env_mcdf, d_env_cpdf, d_env_ccdf, d_env_lum, d_env_mf;
+  int env_w = 0, env_h = 0;
+  bool env_present = false;
   DevBuf d_normals_geo;  // float4 per original triangle: cross(v1-v0, v2-v0)
   bool geo_stale = true;
   Wavefront wf;

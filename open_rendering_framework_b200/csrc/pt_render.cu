@@ -209,6 +209,11 @@ __device__ void eval_direct(const SceneDev& S, const float3& pos, const LightRaw
       L = em * (cp / sq) / pdf;
       break;
     }
+    case ENVMAP_LIGHT: {  // the environment map as a light: sample_environment (Envmap.h:66-98)
+      sample_environment(S.env, dir, L, seed);
+      dist = kDefaultMax;
+      break;
+    }
     default:
       dir = f3s(0.0f);
       L = f3s(0.0f);
@@ -436,15 +441,21 @@ __global__ void __launch_bounds__(kBlock) k_shadow_persistent(SceneDev S, WfDev 
   if (blockIdx.x == 0 && threadIdx.x == 0 && n) atomicAdd(cnt64(w.cnt, CNT_SHADOW_TOTAL), (unsigned long long)n);
 }
 
-// constantbg.cu:16-19
+// constantbg.cu:16-19 / envmap_background.cu:20-23.  With the environment map registered as a light,
+// a miss after next-event estimation (emission disabled) adds nothing, as for area lights.
 __global__ void __launch_bounds__(kBlock) k_shade_miss(SceneDev S, WfDev w)
 {
   const uint32_t n = w.cnt[CNT_Q_MISS];
   const uint32_t* q = w.q_mat + (size_t)QC_MISS * w.cap;
   for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
     uint32_t pid = q[i];
+    float3 bg = S.bg_color;
+    if (S.env.present) {
+      if (S.env.is_light && !(w.rng[pid].w & META_EMIT)) continue;
+      bg = env_lookup(S.env, ld3(w.ray_d[pid]));
+    }
     float4 t = w.thr[pid], r = w.rad[pid];
-    float3 L = ld3(r) + ld3(t) * S.bg_color;
+    float3 L = ld3(r) + ld3(t) * bg;
     w.rad[pid] = make_float4(L.x, L.y, L.z, 0.0f);
   }
 }
@@ -800,6 +811,9 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
   if (!c.built) return fail(PT_NOT_READY, "pt_render_frames: call pt_build first");
   if (!c.camera_set) return fail(PT_NOT_READY, "pt_render_frames: camera not set");
   if (n_frames == 0) return PT_OK;
+  for (const LightRaw& l : c.lights)
+    if (l.type == ENVMAP_LIGHT && !c.env_present)
+      return fail(PT_NOT_READY, "pt_render_frames: an environment-map light needs pt_set_envmap");
   for (const MatDev& m : c.mats)
     if (m.type == MAT_DIFFUSE && c.lights.empty())
       return fail(PT_NOT_READY, "pt_render_frames: diffuse materials need at least one light (light_buffer is indexed unguarded by the diffuse shader)");

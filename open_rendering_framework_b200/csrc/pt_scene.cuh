@@ -66,7 +66,21 @@ struct LightRaw { uint32_t type; float emitted[3]; float p[3]; float pad[3]; }; 
 struct TriLightRaw { float v0[3], v1[3], v2[3], n0[3], n1[3], n2[3]; uint32_t has_normals; float emission[3]; float area; };  // :96-103
 static_assert(sizeof(LightRaw) == 40, "LightStruct layout");
 static_assert(sizeof(TriLightRaw) == 92, "TriangleLight layout");
-enum LightType : uint32_t { POINT_LIGHT = 0, DIRECTIONAL_LIGHT = 1, TRIANGLES_AREA_LIGHT = 2, DISK_LIGHT = 3, SPHERICAL_LIGHT = 4 };
+enum LightType : uint32_t { POINT_LIGHT = 0, DIRECTIONAL_LIGHT = 1, TRIANGLES_AREA_LIGHT = 2, DISK_LIGHT = 3, SPHERICAL_LIGHT = 4,
+                            ENVMAP_LIGHT = 5 /* the environment map as a light (sample_environment, Envmap.h:66-98) */ };
+
+// Environment map: float4 texels (row-major, row j = v), bilinear with REPEAT wrap, and the
+// marginal / conditional pdf and cdf tables of env_cameras.cu:23-75.
+struct EnvDev {
+  const float4* tex;
+  const float* marginal_pdf;
+  const float* marginal_cdf;
+  const float* conditional_pdf;
+  const float* conditional_cdf;
+  int w, h;
+  int present;   // EnvMapBackground set: misses return env_lookup(dir)
+  int is_light;  // an ENVMAP_LIGHT is in the light buffer: misses after next-event estimation return 0
+};
 
 struct CameraDev {
   float3 eye, U, V, W;
@@ -93,6 +107,7 @@ struct SceneDev {
   int n_lights, n_tri_lights;
   uint32_t n_tris;
   float3 bg_color;
+  EnvDev env;
   CameraDev cam;
   IntegratorDev integ;
 };
@@ -315,6 +330,73 @@ PT_HD bool trace_any(const SceneDev& S, const float3& o, const float3& d, float 
   int r;
   while ((r = trav_step_any(S, o, d, rp, tmin, tmax, st)) == 0) {}
   return r > 0;
+}
+
+// ------------------------------------------------------------------ environment map (Envmap.h)
+PT_HD int wrap_index(int i, int n) { int r = i % n; return r < 0 ? r + n : r; }
+// Software FP32 bilinear filtering with REPEAT wrap and normalised coordinates (the sampler state of
+// HDRLoader.cpp:232-236,286); the same weights as the oracle.
+PT_HD float3 env_tex(const EnvDev& E, float u, float v)
+{
+  float x = u * (float)E.w - 0.5f, y = v * (float)E.h - 0.5f;
+  float fx = floorf(x), fy = floorf(y);
+  float ax = x - fx, ay = y - fy;
+  int i0 = wrap_index((int)fx, E.w), j0 = wrap_index((int)fy, E.h), i1 = wrap_index((int)fx + 1, E.w), j1 = wrap_index((int)fy + 1, E.h);
+  float4 t00 = PT_LDG(E.tex + (size_t)j0 * E.w + i0), t10 = PT_LDG(E.tex + (size_t)j0 * E.w + i1);
+  float4 t01 = PT_LDG(E.tex + (size_t)j1 * E.w + i0), t11 = PT_LDG(E.tex + (size_t)j1 * E.w + i1);
+  float w00 = (1.0f - ax) * (1.0f - ay), w10 = ax * (1.0f - ay), w01 = (1.0f - ax) * ay, w11 = ax * ay;
+  return f3(t00.x * w00 + t10.x * w10 + t01.x * w01 + t11.x * w11, t00.y * w00 + t10.y * w10 + t01.y * w01 + t11.y * w11,
+            t00.z * w00 + t10.z * w10 + t01.z * w01 + t11.z * w11);
+}
+// env_lookup, Envmap.h:57-64.
+PT_D float3 env_lookup(const EnvDev& E, const float3& dir)
+{
+  float theta = acosf(dir.y);
+  float phi = atan2f(dir.x, dir.z);
+  float u = (phi + kPi) * 0.5f * kInvPi;
+  float v = (float)(1.0 - (double)(theta * kInvPi));
+  return env_tex(E, u, v);
+}
+// cdf_bsearch_marginal / cdf_bsearch_conditional, Envmap.h:23-55 (the read at middle-1 is skipped at
+// middle 0, which a power-of-two table size never reaches).
+PT_D unsigned cdf_bsearch(const float* cdf, unsigned size, float xi)
+{
+  unsigned ts = size >> 1;
+  unsigned middle = ts;
+  while (ts > 0) {
+    unsigned odd = ts & 1;
+    ts >>= 1;
+    unsigned tmp = ts + odd;
+    if (xi > PT_LDG(cdf + middle)) middle = middle + tmp;
+    else if (middle > 0 && xi < PT_LDG(cdf + middle - 1)) middle = middle - tmp;
+  }
+  return middle;
+}
+// sample_environment, Envmap.h:66-98.
+PT_D void sample_environment(const EnvDev& E, float3& dir, float3& L, uint32_t& t)
+{
+  const float M_2PIPI = 2.0f * kPi * kPi;
+  float xi1 = rnd_tea(t), xi2 = rnd_tea(t);
+  unsigned v_idx = cdf_bsearch(E.marginal_cdf, (unsigned)E.h, xi1);
+  float mc = PT_LDG(E.marginal_cdf + v_idx);
+  float dv = v_idx > 0 ? (xi1 - PT_LDG(E.marginal_cdf + v_idx - 1)) / (mc - PT_LDG(E.marginal_cdf + v_idx - 1)) : xi1 / mc;
+  float pdf_m = PT_LDG(E.marginal_pdf + v_idx);
+  float v = ((float)v_idx + dv) / (float)E.h;
+  const float* crow = E.conditional_cdf + (size_t)v_idx * E.w;
+  unsigned u_idx = cdf_bsearch(crow, (unsigned)E.w, xi2);
+  float cc = PT_LDG(crow + u_idx);
+  float du = u_idx > 0 ? (xi2 - PT_LDG(crow + u_idx - 1)) / (cc - PT_LDG(crow + u_idx - 1)) : xi2 / cc;
+  float pdf_c = PT_LDG(E.conditional_pdf + (size_t)v_idx * E.w + u_idx);
+  float u = ((float)u_idx + du) / (float)E.w;
+  float prob = pdf_m * pdf_c;
+  float theta = (1.0f - v) * kPi;
+  float phi = (2.0f * u - 1.0f) * kPi;
+  float st, ct, sp, cp;
+  sincosf(theta, &st, &ct);
+  sincosf(phi, &sp, &cp);
+  dir = f3(st * sp, ct, st * cp);
+  float3 em = env_tex(E, u, v);
+  L = em * st * M_2PIPI / prob;
 }
 
 }  // namespace pt

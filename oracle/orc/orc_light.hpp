@@ -4,6 +4,7 @@
 #pragma once
 #include "orc_math.hpp"
 #include <cstring>
+#include <vector>
 
 namespace orc {
 
@@ -120,6 +121,126 @@ template <class R> static inline void eval_direct(const V3<R>& pos, const LightS
     case SPHERICAL_LIGHT: eval_sphere_light(pos, ls, dir, L, dist, seed); break;
     default: break;
   }
+}
+
+}  // namespace orc
+
+namespace orc {
+
+// ------------------------------------------------------------------ environment map (Envmap.h)
+// float4 texels (row-major, j = v row), normalized coordinates, bilinear filtering with REPEAT wrap
+// (HDRLoader.cpp:232-236,286 sampler state); software FP32 weights, identical to the CUDA lookup.
+struct EnvMap {
+  const float* rgba = nullptr;
+  int w = 0, h = 0;
+  std::vector<float> marginal_pdf, marginal_cdf, conditional_pdf, conditional_cdf;
+};
+static inline int wrap_i(int i, int n) { int r = i % n; return r < 0 ? r + n : r; }
+static inline V3<float> env_tex(const EnvMap& E, float u, float v)
+{
+  float x = u * (float)E.w - 0.5f, y = v * (float)E.h - 0.5f;
+  float fx = std::floor(x), fy = std::floor(y);
+  float ax = x - fx, ay = y - fy;
+  int i0 = wrap_i((int)fx, E.w), j0 = wrap_i((int)fy, E.h), i1 = wrap_i((int)fx + 1, E.w), j1 = wrap_i((int)fy + 1, E.h);
+  const float* t00 = E.rgba + 4 * ((size_t)j0 * E.w + i0);
+  const float* t10 = E.rgba + 4 * ((size_t)j0 * E.w + i1);
+  const float* t01 = E.rgba + 4 * ((size_t)j1 * E.w + i0);
+  const float* t11 = E.rgba + 4 * ((size_t)j1 * E.w + i1);
+  float w00 = (1.0f - ax) * (1.0f - ay), w10 = ax * (1.0f - ay), w01 = (1.0f - ax) * ay, w11 = ax * ay;
+  float c[3];
+  for (int k = 0; k < 3; ++k) c[k] = t00[k] * w00 + t10[k] * w10 + t01[k] * w01 + t11[k] * w11;
+  return v3(c[0], c[1], c[2]);
+}
+// env_lookup, Envmap.h:57-64
+static inline V3<float> env_lookup(const EnvMap& E, const V3<float>& dir)
+{
+  float theta = std::acos(dir.y);
+  float phi = std::atan2(dir.x, dir.z);
+  float u = (phi + K<float>::PI) * 0.5f * K<float>::INV_PI;
+  float v = (float)(1.0 - (double)(theta * K<float>::INV_PI));
+  return env_tex(E, u, v);
+}
+// CDF construction of env_cameras.cu:23-75 (luminance x sin(theta), row marginal, conditional
+// pdf/cdf, marginal pdf/cdf; the last conditional entry of the last row and the last marginal entry
+// are set to 1).  Sums are accumulated sequentially in float in the reference's order.
+static inline void env_build_cdf(EnvMap& E)
+{
+  const int W = E.w, H = E.h;
+  std::vector<float> lum((size_t)W * H), mf(H);
+  for (int j = 0; j < H; ++j)
+    for (int i = 0; i < W; ++i) {
+      float u = ((float)i + 0.5f) / (float)W, v = ((float)j + 0.5f) / (float)H;
+      float theta = (1.0f - v) * K<float>::PI;
+      V3<float> t = env_tex(E, u, v);
+      lum[(size_t)j * W + i] = (t.x * 0.2989f + t.y * 0.5866f + t.z * 0.1145f) * std::sin(theta);
+    }
+  for (int j = 0; j < H; ++j) {
+    float s = 0.0f;
+    for (int i = 0; i < W; ++i) s += lum[(size_t)j * W + i];
+    mf[j] = s / (float)W;
+  }
+  E.conditional_pdf.assign((size_t)W * H, 0.0f);
+  E.conditional_cdf.assign((size_t)W * H, 0.0f);
+  for (int j = 0; j < H; ++j) {
+    float s = 0.0f;
+    for (int i = 0; i < W; ++i) {
+      s += lum[(size_t)j * W + i];
+      E.conditional_pdf[(size_t)j * W + i] = lum[(size_t)j * W + i] / mf[j];
+      E.conditional_cdf[(size_t)j * W + i] = (s / (float)W) / mf[j];
+    }
+  }
+  E.conditional_cdf[(size_t)(H - 1) * W + (W - 1)] = 1.0f;
+  E.marginal_pdf.assign(H, 0.0f);
+  E.marginal_cdf.assign(H, 0.0f);
+  float total = 0.0f;
+  for (int j = 0; j < H; ++j) total += mf[j];
+  float s = 0.0f;
+  for (int j = 0; j < H; ++j) {
+    s += mf[j];
+    float m = total / (float)H;
+    E.marginal_pdf[j] = mf[j] / m;
+    E.marginal_cdf[j] = (s / (float)H) / m;
+  }
+  E.marginal_cdf[H - 1] = 1.0f;
+}
+// cdf_bsearch_marginal / cdf_bsearch_conditional, Envmap.h:23-55 (the read at middle-1 is skipped
+// when middle is 0; for power-of-two sizes the search never reaches it).
+static inline unsigned cdf_bsearch(const float* cdf, unsigned size, float xi)
+{
+  unsigned ts = size;
+  unsigned middle = ts = ts >> 1;
+  while (ts > 0) {
+    unsigned odd = ts & 1;
+    ts = ts >> 1;
+    unsigned tmp = ts + odd;
+    if (xi > cdf[middle]) middle = middle + tmp;
+    else if (middle > 0 && xi < cdf[middle - 1]) middle = middle - tmp;
+  }
+  return middle;
+}
+// sample_environment, Envmap.h:66-98.
+static inline void sample_environment(const EnvMap& E, V3<float>& dir, V3<float>& L, u32& t)
+{
+  const float M_2PIPI = 2.0f * K<float>::PI * K<float>::PI;
+  float xi1 = rnd_tea(t), xi2 = rnd_tea(t);
+  unsigned v_idx = cdf_bsearch(E.marginal_cdf.data(), (unsigned)E.h, xi1);
+  float dv = v_idx > 0 ? (xi1 - E.marginal_cdf[v_idx - 1]) / (E.marginal_cdf[v_idx] - E.marginal_cdf[v_idx - 1]) : xi1 / E.marginal_cdf[v_idx];
+  float pdf_m = E.marginal_pdf[v_idx];
+  float v = ((float)v_idx + dv) / (float)E.h;
+  const float* crow = E.conditional_cdf.data() + (size_t)v_idx * E.w;
+  unsigned u_idx = cdf_bsearch(crow, (unsigned)E.w, xi2);
+  float du = u_idx > 0 ? (xi2 - crow[u_idx - 1]) / (crow[u_idx] - crow[u_idx - 1]) : xi2 / crow[u_idx];
+  float pdf_c = E.conditional_pdf[(size_t)v_idx * E.w + u_idx];
+  float u = ((float)u_idx + du) / (float)E.w;
+  float prob = pdf_m * pdf_c;
+  float theta = (1.0f - v) * K<float>::PI;
+  float phi = (2.0f * u - 1.0f) * K<float>::PI;
+  float st, ct, sp, cp;
+  ::sincosf(theta, &st, &ct);
+  ::sincosf(phi, &sp, &cp);
+  dir = v3(st * sp, ct, st * cp);
+  V3<float> em = env_tex(E, u, v);
+  L = em * st * M_2PIPI / prob;
 }
 
 }  // namespace orc
