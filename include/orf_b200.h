@@ -166,6 +166,11 @@ pt_status pt_set_background_constant(pt_ctx* ctx, const float color[3]);
 pt_status pt_set_envmap(pt_ctx* ctx, const float* rgba, uint32_t width, uint32_t height);
 /* Copy the environment tables to host memory (any pointer may be NULL). */
 pt_status pt_get_envmap_tables(pt_ctx* ctx, float* marginal_pdf, float* marginal_cdf, float* conditional_pdf, float* conditional_cdf);
+/* Environment queries (parity checks): env_lookup of n_dirs directions (3 floats each) into d_looked,
+ * and n_samples draws of sample_environment from the rnd_tea seeds in d_seeds (advanced in place)
+ * into d_sample_dirs / d_sample_L (3 floats each). */
+pt_status pt_env_query(pt_ctx* ctx, const float* d_dirs, uint32_t n_dirs, float* d_looked, uint32_t* d_seeds, uint32_t n_samples,
+                       float* d_sample_dirs, float* d_sample_L);
 /* Create a material of the given type from its parameter struct; returns its id. */
 pt_status pt_material_create(pt_ctx* ctx, uint32_t type, const void* params, size_t params_size, uint32_t* out_id);
 /* Replace the parameters of an existing material (same type); takes effect at the next render. */

@@ -59,6 +59,7 @@ SIGNATURES = {
     "pt_set_background_constant": (I32, [P, P]),
     "pt_set_envmap": (I32, [P, P, U32, U32]),
     "pt_get_envmap_tables": (I32, [P, P, P, P, P]),
+    "pt_env_query": (I32, [P, P, U32, P, P, U32, P, P]),
     "pt_material_create": (I32, [P, U32, P, SZ, P]),
     "pt_material_update": (I32, [P, U32, P, SZ]),
     "pt_mesh_add": (I32, [P, P, U32, P, U32, P, U32, P, U32, P]),

@@ -191,6 +191,26 @@ __global__ void k_env_marginal(EnvDev E, const float* mf, float* mpdf, float* mc
   ccdf[(size_t)(E.h - 1) * E.w + (E.w - 1)] = 1.0f;
 }
 
+__global__ void k_env_query(EnvDev E, const float* dirs, uint32_t n_dirs, float* looked, uint32_t* seeds, uint32_t n_samples, float* sdir, float* sL)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_dirs + n_samples; i += gridDim.x * blockDim.x) {
+    if (i < n_dirs) {
+      float3 r = env_lookup(E, f3(dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]));
+      looked[3 * i] = r.x;
+      looked[3 * i + 1] = r.y;
+      looked[3 * i + 2] = r.z;
+    } else {
+      uint32_t k = i - n_dirs;
+      uint32_t t = seeds[k];
+      float3 d, L;
+      sample_environment(E, d, L, t);
+      seeds[k] = t;
+      sdir[3 * k] = d.x; sdir[3 * k + 1] = d.y; sdir[3 * k + 2] = d.z;
+      sL[3 * k] = L.x; sL[3 * k + 1] = L.y; sL[3 * k + 2] = L.z;
+    }
+  }
+}
+
 }  // namespace pt
 
 using namespace pt;
@@ -336,6 +356,22 @@ pt_status pt_get_envmap_tables(pt_ctx* ctx, float* marginal_pdf, float* marginal
   if (marginal_cdf) PT_CHECK_CUDA(cudaMemcpy(marginal_cdf, c.d_env_mcdf.p, (size_t)c.env_h * 4, cudaMemcpyDeviceToHost), "env tables");
   if (conditional_pdf) PT_CHECK_CUDA(cudaMemcpy(conditional_pdf, c.d_env_cpdf.p, n * 4, cudaMemcpyDeviceToHost), "env tables");
   if (conditional_cdf) PT_CHECK_CUDA(cudaMemcpy(conditional_cdf, c.d_env_ccdf.p, n * 4, cudaMemcpyDeviceToHost), "env tables");
+  return PT_OK;
+}
+
+pt_status pt_env_query(pt_ctx* ctx, const float* d_dirs, uint32_t n_dirs, float* d_looked, uint32_t* d_seeds, uint32_t n_samples,
+                       float* d_sample_dirs, float* d_sample_L)
+{
+  CTX_CHECK(ctx);
+  Context& c = ctx->c;
+  if (!c.env_present) return fail(PT_NOT_READY, "pt_env_query: no environment map");
+  if ((n_dirs && (!d_dirs || !d_looked)) || (n_samples && (!d_seeds || !d_sample_dirs || !d_sample_L)))
+    return fail(PT_INVALID_ARG, "pt_env_query: null pointer");
+  if (n_dirs + (uint64_t)n_samples == 0) return PT_OK;
+  k_env_query<<<grid_for(n_dirs + (uint64_t)n_samples, 128, 8), 128, 0, c.stream>>>(c.view().env, d_dirs, n_dirs, d_looked, d_seeds, n_samples,
+                                                                                    d_sample_dirs, d_sample_L);
+  count_launch();
+  PT_CHECK_CUDA(cudaGetLastError(), "pt_env_query launch");
   return PT_OK;
 }
 

@@ -148,6 +148,19 @@ class ConstantBackground:
         self.background_color = tuple(c)
 
 
+class EnvMapBackground:
+    """EnvMapBackground (Background.cpp:57-69): float4 texels [H, W, 4], row 0 at v = 0."""
+
+    def __init__(self, rgba):
+        self.rgba = np.ascontiguousarray(rgba, np.float32)
+        assert self.rgba.ndim == 3 and self.rgba.shape[2] == 4
+
+
+class EnvMapLight:
+    """The environment map as a light in light_buffer (light_type 5, sampled with
+    sample_environment of Envmap.h:66-98): diffuse next-event estimation picks it like any light."""
+
+
 # ---------------------------------------------------------------- Material.h
 class DiffuseMaterial:
     type = DIFFUSE_SHADER
@@ -271,6 +284,9 @@ def light_buffers(lights):
             ls[k]["light_type"] = POINT_LIGHT
             ls[k]["emitted_radiance"] = L.radiance
             ls[k]["p"] = L.position
+        elif isinstance(L, EnvMapLight):
+            ls[k]["light_type"] = 5
+            ls[k]["emitted_radiance"] = (1.0, 1.0, 1.0)
         elif isinstance(L, DirectionalLight):
             ls[k]["light_type"] = DIRECTIONAL_LIGHT
             ls[k]["emitted_radiance"] = L.radiance
@@ -387,7 +403,17 @@ class Renderer:
         self.frame = 0
 
     def apply_background(self):
-        nat.call("pt_set_background_constant", self.ctx, _f3(self.background.background_color))
+        if isinstance(self.background, EnvMapBackground):
+            e = self.background.rgba
+            nat.call("pt_set_envmap", self.ctx, e.ctypes.data, e.shape[1], e.shape[0])
+        else:
+            nat.call("pt_set_background_constant", self.ctx, _f3(self.background.background_color))
+
+    def envmap_tables(self):
+        H, W = self.background.rgba.shape[:2]
+        out = [np.empty(H, np.float32), np.empty(H, np.float32), np.empty((H, W), np.float32), np.empty((H, W), np.float32)]
+        nat.call("pt_get_envmap_tables", self.ctx, *[o.ctypes.data for o in out])
+        return out
 
     def renderScene(self):
         """One frame, as OptixScene::renderScene: frame++ and one integrator pass."""

@@ -84,3 +84,45 @@ def single_scene(width=512, height=512, metal_subdiv=6, glass_subdiv=5, max_dept
     lp, li = quad_light((0.0, 0.99, 0.0), 0.25)
     lights = [sc.TriangleAreaLight(lp, li, (15.0, 15.0, 15.0))]
     return sc.SceneData(integrator, camera, background, meshes, lights)
+
+
+def sky_envmap(width=2048, height=1024, sun_dir=(0.35, 0.55, 0.45), sun_peak=5.0e4, sun_sigma_deg=1.0):
+    """Procedural equirectangular sky in the reference's mapping (envmap.h: u = (atan2(x, z) + pi) / 2pi,
+    v = 1 - acos(y) / pi): a vertical gradient from horizon to zenith, a darker ground, and a Gaussian sun
+    lobe of the given peak radiance and angular width.  float4 texels [H, W, 4], row 0 at v = 0."""
+    u = (np.arange(width, dtype=np.float64) + 0.5) / width
+    v = (np.arange(height, dtype=np.float64) + 0.5) / height
+    theta = (1.0 - v)[:, None] * np.pi
+    phi = (2.0 * u - 1.0)[None, :] * np.pi
+    d = np.stack([np.sin(theta) * np.sin(phi), np.cos(theta) * np.ones_like(phi), np.sin(theta) * np.cos(phi)], -1)
+    y = d[..., 1:2]
+    horizon = np.array([0.85, 0.9, 1.0])
+    zenith = np.array([0.15, 0.35, 0.85])
+    ground = np.array([0.25, 0.22, 0.2])
+    sky = np.where(y >= 0, horizon + (zenith - horizon) * np.sqrt(np.clip(y, 0, 1)), ground)
+    s = np.asarray(sun_dir, np.float64)
+    s /= np.linalg.norm(s)
+    ang = np.arccos(np.clip(np.tensordot(d, s, axes=([2], [0])), -1, 1))
+    sig = np.radians(sun_sigma_deg)
+    sun = sun_peak * np.exp(-0.5 * (ang / sig) ** 2)[..., None] * np.array([1.0, 0.95, 0.85])
+    rgb = sky + sun
+    out = np.concatenate([rgb, np.ones(rgb.shape[:2] + (1,))], -1).astype(np.float32)
+    return np.ascontiguousarray(out)
+
+
+def env_scene(width=256, height=256, env_w=256, env_h=128, metal_subdiv=3, glass_subdiv=2, env_as_light=True, max_depth=6):
+    """Open scene lit only by the procedural sky (no box): a diffuse floor quad, a conductor and a
+    dielectric sphere; the environment map is both the miss radiance and (optionally) a light."""
+    integrator = sc.PathTracer(max_depth=max_depth, scene_epsilon=1e-4)
+    camera = sc.PinholeCamera(eye=(0.0, 0.3, 2.2), lookat=(0.0, -0.3, 0.0), up=(0.0, 1.0, 0.0), vfov=45.0, width=width, height=height)
+    background = sc.EnvMapBackground(sky_envmap(env_w, env_h, sun_peak=5.0e4, sun_sigma_deg=4.0))
+    floor = sc.DiffuseMaterial((0.6, 0.6, 0.55))
+    metal = sc.MetallicMaterial(ior=((0.2, 3.9), (0.55, 3.15), (0.9, 2.4)), roughness=(0.2, 0.2), normal_distribution=sc.GGX_DISTRIBUTION)
+    glass = sc.RoughTransparentMaterial(ior=1.5, roughness=0.1, normal_distribution=sc.BECKMANN_DISTRIBUTION)
+    fp_ = np.array([(-3, -1, -3), (3, -1, -3), (3, -1, 3), (-3, -1, 3)], np.float32)
+    fi = np.array([(0, 2, 1), (0, 3, 2)], np.int32)
+    mp, mi, mn, mni = icosphere(metal_subdiv, 0.5, (-0.6, -0.5, 0.0))
+    gp, gi, gn, gni = icosphere(glass_subdiv, 0.5, (0.6, -0.5, 0.2))
+    meshes = [sc.Mesh(fp_, fi, floor), sc.Mesh(mp, mi, metal, mn, mni), sc.Mesh(gp, gi, glass, gn, gni)]
+    lights = [sc.EnvMapLight()] if env_as_light else []
+    return sc.SceneData(integrator, camera, background, meshes, lights)

@@ -174,6 +174,9 @@ def _trace_sigs(lib):
     _sig(lib, "orc_render", L, [P, U, U, U, U, P, P, I])
     _sig(lib, "orc_capped", L, [P])
     _sig(lib, "orc_trace_batch", None, [P, P, L, I, P, P, P, P])
+    _sig(lib, "orc_scene_set_env", None, [P, P, I, I])
+    _sig(lib, "orc_env_tables", None, [P, P, P, P, P])
+    _sig(lib, "orc_env_query", None, [P, P, L, P, P, L, P, P])
     lib._trace_bound = True
 
 
@@ -214,7 +217,7 @@ class OracleScene:
         cam = np.concatenate([C.eye, C.U, C.V, C.W]).astype(np.float32)
         patch = np.array(list(C.patch_origin) + list(C.patch_dims), np.uint32)
         I_ = data.integrator
-        bg = np.asarray(data.background.background_color, np.float32)
+        bg = np.asarray(getattr(data.background, "background_color", (0.0, 0.0, 0.0)), np.float32)
         # keep every buffer alive for the scene's lifetime
         self._keep = [tri_pos, tri_info, normals, mtype, mmodel, mdist, mab, mior, cam, patch, bg,
                       np.ascontiguousarray(data.light_buffer), np.ascontiguousarray(data.triangle_light_buffer)]
@@ -223,6 +226,11 @@ class OracleScene:
                                       fp(mtype), fp(mmodel), fp(mdist), fp(mab), fp(mior), n_m,
                                       fp(lb) if len(lb) else None, len(lb), fp(tb) if len(tb) else None, len(tb),
                                       fp(cam), C.width, C.height, fp(patch), I_.max_depth, I_.scene_epsilon, I_.rr_start_depth, fp(bg))
+        env = getattr(data.background, "rgba", None)
+        if env is not None:
+            env = np.ascontiguousarray(env, np.float32)
+            self._keep.append(env)
+            lib.orc_scene_set_env(self.h, fp(env), env.shape[1], env.shape[0])
 
     def render(self, first_frame, n_frames, accum=None, p_begin=0, p_end=None, path_radiance=False, threads=1):
         """Runs the CPU tracer; returns (accum [H,W,4] or None, per-path radiance [F,P,3] or None)."""
@@ -234,6 +242,22 @@ class OracleScene:
         self.lib.orc_render(self.h, first_frame, n_frames, p_begin, p_end, fp(pr) if pr is not None else None,
                             fp(accum) if accum is not None else None, threads)
         return accum, pr
+
+    def env_tables(self):
+        H, W = self.data.background.rgba.shape[:2]
+        mpdf, mcdf = np.empty(H, np.float32), np.empty(H, np.float32)
+        cpdf, ccdf = np.empty((H, W), np.float32), np.empty((H, W), np.float32)
+        self.lib.orc_env_tables(self.h, fp(mpdf), fp(mcdf), fp(cpdf), fp(ccdf))
+        return mpdf, mcdf, cpdf, ccdf
+
+    def env_query(self, dirs, seeds):
+        dirs = np.ascontiguousarray(dirs, np.float32)
+        seeds = np.ascontiguousarray(seeds, np.uint32).copy()
+        looked = np.empty_like(dirs)
+        sd = np.empty((len(seeds), 3), np.float32)
+        sL = np.empty((len(seeds), 3), np.float32)
+        self.lib.orc_env_query(self.h, fp(dirs), len(dirs), fp(looked), fp(seeds), len(seeds), fp(sd), fp(sL))
+        return looked, seeds, sd, sL
 
     def trace(self, rays8, brute=False):
         """Closest and any hit for rays [n,8] = (origin, tmin, dir, tmax)."""

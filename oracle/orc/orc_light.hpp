@@ -13,11 +13,13 @@ struct LightStructRaw { u32 light_type; float emitted[3]; float p[3]; float pad[
 struct TriangleLightRaw { float v0[3], v1[3], v2[3], n0[3], n1[3], n2[3]; u32 has_normals; float emission[3]; float area; };
 static_assert(sizeof(LightStructRaw) == 40, "LightStruct layout");
 static_assert(sizeof(TriangleLightRaw) == 92, "TriangleLight layout");
-enum { POINT_LIGHT = 0, DIRECTIONAL_LIGHT = 1, TRIANGLES_AREA_LIGHT = 2, DISK_LIGHT = 3, SPHERICAL_LIGHT = 4 };
+enum { POINT_LIGHT = 0, DIRECTIONAL_LIGHT = 1, TRIANGLES_AREA_LIGHT = 2, DISK_LIGHT = 3, SPHERICAL_LIGHT = 4, ENVMAP_LIGHT = 5 };
 
 template <class R> static inline V3<R> ldv(const float* p) { return v3((R)p[0], (R)p[1], (R)p[2]); }
 
+struct EnvMap;
 struct LightSet {
+  const EnvMap* env = nullptr;  // ENVMAP_LIGHT (type 5): the environment map as a light
   const LightStructRaw* lights = nullptr;
   long n_lights = 0;
   const TriangleLightRaw* tris = nullptr;
@@ -109,20 +111,6 @@ template <class R> static inline void eval_sphere_light(const V3<R>& pos, const 
   R cp = std::fmax(dot(nrm, -dir), R(0));
   L = ldv<R>(ls.emitted) * (cp / sq) / pdf;
 }
-// evaluate_direct_illumination dispatch, LightSampler.h:143-166.
-template <class R> static inline void eval_direct(const V3<R>& pos, const LightStructRaw& ls, LightSet& set, V3<R>& dir, V3<R>& L,
-                                                  R& dist, u32& seed)
-{
-  switch (ls.light_type) {
-    case POINT_LIGHT: eval_point_light(pos, ls, dir, L, dist); break;
-    case DIRECTIONAL_LIGHT: eval_directional_light(ls, dir, L, dist); break;
-    case TRIANGLES_AREA_LIGHT: eval_triangle_area_light(pos, ls, set, dir, L, dist, seed); break;
-    case DISK_LIGHT: eval_disk_light(pos, ls, dir, L, dist, seed); break;
-    case SPHERICAL_LIGHT: eval_sphere_light(pos, ls, dir, L, dist, seed); break;
-    default: break;
-  }
-}
-
 }  // namespace orc
 
 namespace orc {
@@ -241,6 +229,33 @@ static inline void sample_environment(const EnvMap& E, V3<float>& dir, V3<float>
   dir = v3(st * sp, ct, st * cp);
   V3<float> em = env_tex(E, u, v);
   L = em * st * M_2PIPI / prob;
+}
+
+}  // namespace orc
+
+namespace orc {
+
+// evaluate_direct_illumination dispatch, LightSampler.h:143-166.
+template <class R> static inline void eval_direct(const V3<R>& pos, const LightStructRaw& ls, LightSet& set, V3<R>& dir, V3<R>& L,
+                                                  R& dist, u32& seed)
+{
+  switch (ls.light_type) {
+    case POINT_LIGHT: eval_point_light(pos, ls, dir, L, dist); break;
+    case DIRECTIONAL_LIGHT: eval_directional_light(ls, dir, L, dist); break;
+    case TRIANGLES_AREA_LIGHT: eval_triangle_area_light(pos, ls, set, dir, L, dist, seed); break;
+    case DISK_LIGHT: eval_disk_light(pos, ls, dir, L, dist, seed); break;
+    case SPHERICAL_LIGHT: eval_sphere_light(pos, ls, dir, L, dist, seed); break;
+    case ENVMAP_LIGHT:
+      if (set.env) {
+        V3<float> d3, L3;
+        sample_environment(*set.env, d3, L3, seed);
+        dir = cvt<R>(d3);
+        L = cvt<R>(L3);
+        dist = (R)DEFAULT_MAX;
+      }
+      break;
+    default: break;
+  }
 }
 
 }  // namespace orc

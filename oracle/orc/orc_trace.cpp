@@ -51,6 +51,9 @@ struct Scene {
   float eps;
   int rr_start;
   F3 bg;
+  EnvMap env;
+  std::vector<float> env_texels;
+  bool env_present = false, env_is_light = false;
   // BVH
   struct Node { float lo[3], hi[3]; int left, right, first, count; };
   std::vector<Node> nodes;
@@ -403,8 +406,13 @@ static void shade_glass(Scene& S, const Mat& m, const F3& o, const F3& d, const 
 static void trace(Scene& S, const F3& o, const F3& d, PRD& prd, LightSet& ls)
 {
   HitRec h = closest(S, o, d, S.eps, DEFAULT_MAX);
-  if (h.prim < 0) {  // constantbg.cu:16-19
-    prd.result = S.bg;
+  if (h.prim < 0) {  // constantbg.cu:16-19 / envmap_background.cu:20-23
+    if (S.env_present) {
+      if (S.env_is_light && !prd.emit_light) prd.result = v3s(0.0f);
+      else prd.result = env_lookup(S.env, d);
+    } else {
+      prd.result = S.bg;
+    }
     return;
   }
   const Mat& m = S.mats[S.info[4 * (size_t)h.prim + 3]];
@@ -478,6 +486,46 @@ EXPORT void* orc_scene_create(const float* tri_pos, const int* tri_info, unsigne
 
 EXPORT void orc_scene_destroy(void* s) { delete (Scene*)s; }
 
+// EnvMapBackground for the scene: copies the float4 texels and builds the CDF tables.
+EXPORT void orc_scene_set_env(void* s, const float* rgba, int w, int h)
+{
+  Scene& S = *(Scene*)s;
+  S.env_texels.assign(rgba, rgba + 4 * (size_t)w * h);
+  S.env.rgba = S.env_texels.data();
+  S.env.w = w;
+  S.env.h = h;
+  env_build_cdf(S.env);
+  S.env_present = true;
+  S.env_is_light = false;
+  for (long k = 0; k < S.lights.n_lights; ++k)
+    if (S.lights.lights[k].light_type == ENVMAP_LIGHT) S.env_is_light = true;
+}
+EXPORT void orc_env_tables(void* s, float* mpdf, float* mcdf, float* cpdf, float* ccdf)
+{
+  const EnvMap& E = ((Scene*)s)->env;
+  memcpy(mpdf, E.marginal_pdf.data(), 4 * (size_t)E.h);
+  memcpy(mcdf, E.marginal_cdf.data(), 4 * (size_t)E.h);
+  memcpy(cpdf, E.conditional_pdf.data(), 4 * (size_t)E.w * E.h);
+  memcpy(ccdf, E.conditional_cdf.data(), 4 * (size_t)E.w * E.h);
+}
+// Batch env queries: lookups of dirs3[n] and importance samples from seeds[n] (seeds advanced).
+EXPORT void orc_env_query(void* s, const float* dirs3, long n_dirs, float* looked3, unsigned* seeds, long n_samples, float* sdir3, float* sL3)
+{
+  const EnvMap& E = ((Scene*)s)->env;
+  for (long i = 0; i < n_dirs; ++i) {
+    F3 r = env_lookup(E, v3(dirs3[3 * i], dirs3[3 * i + 1], dirs3[3 * i + 2]));
+    looked3[3 * i] = r.x; looked3[3 * i + 1] = r.y; looked3[3 * i + 2] = r.z;
+  }
+  for (long i = 0; i < n_samples; ++i) {
+    u32 t = seeds[i];
+    F3 d, L;
+    sample_environment(E, d, L, t);
+    seeds[i] = t;
+    sdir3[3 * i] = d.x; sdir3[3 * i + 1] = d.y; sdir3[3 * i + 2] = d.z;
+    sL3[3 * i] = L.x; sL3[3 * i + 1] = L.y; sL3[3 * i + 2] = L.z;
+  }
+}
+
 // Renders frames [first_frame, first_frame + n_frames) for pixels [p_begin, p_end) with `threads`
 // host threads.  path_rad (optional): radiance of every path, [frame][pixel][3] over the pixel
 // range.  accum (optional): the float4 running mean over the full image, updated in frame order as
@@ -493,6 +541,7 @@ EXPORT long orc_render(void* scene, unsigned first_frame, unsigned n_frames, uns
   std::atomic<long> oob(0);
   auto worker = [&]() {
     LightSet ls = S.lights;
+    ls.env = S.env_present ? &S.env : nullptr;
     ls.oob = 0;
     for (;;) {
       unsigned p0 = next.fetch_add(64);

@@ -115,6 +115,32 @@ def main():
         fc[k] = out
     g.update(fc_wi=fw, fc_m=fm, fc_out=fc)
 
+    # Environment map lookup and importance sampling (Envmap.h:57-98) on a small procedural map, with
+    # the CDF tables built by the oracle restatement of env_cameras.cu (that program is not compiled by
+    # the reference build, so its restatement is checked for self-consistency in the tests instead).
+    from open_rendering_framework_b200 import scenes
+
+    env = scenes.sky_envmap(64, 32, sun_peak=5.0e4, sun_sigma_deg=8.0)
+    data = scenes.env_scene(8, 8, env_w=64, env_h=32)
+    data.background.rgba = env
+    O = oc.OracleScene(data)
+    mp, mc, cp, cc = O.env_tables()
+    R.ref_set_envmap(oc.fp(env), env.shape[1], env.shape[0], oc.fp(mp), oc.fp(mc), oc.fp(cp), oc.fp(cc))
+    dirs = unit_vectors(rng, 256, upper=False)
+    seeds = rng.integers(0, 2**32, size=256, dtype=np.uint64).astype(np.uint32)
+    looked = np.empty((256, 3), np.float32)
+    sdir = np.empty((256, 3), np.float32)
+    sL = np.empty((256, 3), np.float32)
+    sfin = np.empty(256, np.uint32)
+    pos = np.zeros(3, np.float32)
+    for k in range(256):
+        R.ref_env_lookup(oc.fp(dirs[k]), oc.fp(looked[k]))
+        s_ = ctypes.c_uint(int(seeds[k]))
+        R.ref_sample_environment(oc.fp(pos), ctypes.byref(s_), oc.fp(sdir[k]), oc.fp(sL[k]))
+        sfin[k] = s_.value
+    g.update(env_map=env, env_mpdf=mp, env_mcdf=mc, env_cpdf=cp, env_ccdf=cc, env_dirs=dirs, env_looked=looked, env_seeds=seeds,
+             env_sdir=sdir, env_sL=sL, env_sfin=sfin)
+
     np.savez_compressed(OUT, **g)
     print("wrote", OUT, os.path.getsize(OUT), "bytes")
 

@@ -1,0 +1,76 @@
+"""GPU parity of the environment map: CDF tables built on the device (env_cameras.cu), the bilinear
+lookup (envmap_background.cu / Envmap.h env_lookup), importance sampling (Envmap.h
+sample_environment), and renders lit by the map, against the oracle.
+
+The device tables use CUDA's sinf where the oracle uses glibc's, so table entries agree to a few ulp,
+not bit for bit: bars are 1e-5 relative for the tables, 1e-4 for lookups, and for samples 99.5% of
+directions within 1e-4 (a draw within a few ulp of a CDF step may pick the neighbouring texel).
+Random-number consumption is identical (two draws per sample).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle_ctypes as oc
+from open_rendering_framework_b200 import _native as nat
+from open_rendering_framework_b200 import scene as sc
+from open_rendering_framework_b200 import scenes
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b, floor=1e-12):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.abs(a - b) / np.maximum(np.abs(b), floor)
+
+
+@pytest.mark.parametrize("size", [(256, 128), (2048, 1024)])
+def test_env_tables_lookup_and_sampling(size):
+    w, h = size
+    data = scenes.env_scene(16, 16, env_w=w, env_h=h)
+    R = sc.Renderer(data)
+    O = oc.OracleScene(data)
+    g_tables = R.envmap_tables()
+    o_tables = O.env_tables()
+    for g, o in zip(g_tables, o_tables):
+        assert np.mean(rel(g, o, 1e-20) <= 1e-5) >= 0.9999
+    assert g_tables[1][-1] == 1.0 and g_tables[3][-1, -1] == 1.0
+    rng = np.random.default_rng(3)
+    n = 20000
+    dirs = rng.normal(size=(n, 3))
+    dirs = (dirs / np.linalg.norm(dirs, axis=1, keepdims=True)).astype(np.float32)
+    seeds = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    d_dirs = torch.from_numpy(dirs).cuda()
+    d_look = torch.empty_like(d_dirs)
+    d_seeds = torch.from_numpy(seeds.view(np.int32).copy()).cuda()
+    d_sd = torch.empty((n, 3), dtype=torch.float32, device="cuda")
+    d_sl = torch.empty((n, 3), dtype=torch.float32, device="cuda")
+    nat.call("pt_env_query", R.ctx, d_dirs.data_ptr(), n, d_look.data_ptr(), d_seeds.data_ptr(), n, d_sd.data_ptr(), d_sl.data_ptr())
+    R.sync()
+    looked, fin, sdir, sL = O.env_query(dirs, seeds)
+    assert np.mean(np.all(rel(d_look.cpu().numpy(), looked, 1e-6) <= 1e-4, axis=1)) >= 0.999
+    assert np.array_equal(d_seeds.cpu().numpy().view(np.uint32), fin)
+    ddir = np.linalg.norm(d_sd.cpu().numpy() - sdir, axis=1)
+    assert np.mean(ddir <= 1e-4) >= 0.995
+    ok = ddir <= 1e-4
+    assert np.mean(np.all(rel(d_sl.cpu().numpy()[ok], sL[ok], 1e-6) <= 1e-3, axis=1)) >= 0.995
+    R.close()
+
+
+@pytest.mark.parametrize("as_light", [True, False])
+def test_env_lit_render_matches_cpu_restatement(as_light):
+    w = h = 32
+    data = scenes.env_scene(w, h, env_w=256, env_h=128, env_as_light=as_light)
+    R = sc.Renderer(data)
+    R.render(4)
+    got = R.readback()
+    O = oc.OracleScene(data)
+    ref, _ = O.render(0, 4, accum=np.zeros((h, w, 4), np.float32), threads=8)
+    r = rel(got[..., :3], ref[..., :3], 1e-3)
+    pix_ok = np.mean(np.all(r <= 1e-3, axis=-1))
+    rmse = float(np.mean((got[..., :3].astype(np.float64) - ref[..., :3]) ** 2 / (ref[..., :3].astype(np.float64) ** 2 + 1e-2)))
+    print("env as light", as_light, "pixels within 1e-3:", pix_ok, "relMSE", rmse)
+    assert np.all(np.isfinite(got))
+    assert pix_ok >= 0.95
+    assert rmse < 1e-2
+    R.close()

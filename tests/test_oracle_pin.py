@@ -143,3 +143,31 @@ def test_fresh_pieces_against_compiled_reference():
         R.ref_sample_cosine_weighted(oc.fp(n), ctypes.byref(s1), oc.fp(o1))
         O.orc_sample_cosine_weighted_f(oc.fp(n), ctypes.byref(s2), oc.fp(o2))
         assert bits_equal(o1, o2) and s1.value == s2.value
+
+
+def test_env_lookup_and_sampling_golden():
+    from open_rendering_framework_b200 import scenes
+
+    data = scenes.env_scene(8, 8, env_w=64, env_h=32)
+    data.background.rgba = GOLD["env_map"]
+    O = oc.OracleScene(data)
+    mp, mc, cp, cc = O.env_tables()
+    # the oracle's CDF build is the one the golden sampling vectors were made with
+    for a, b in ((mp, "env_mpdf"), (mc, "env_mcdf"), (cp, "env_cpdf"), (cc, "env_ccdf")):
+        assert bits_equal(a, GOLD[b])
+    looked, fin, sdir, sL = O.env_query(GOLD["env_dirs"], GOLD["env_seeds"])
+    assert bits_equal(looked, GOLD["env_looked"])
+    assert bits_equal(sdir, GOLD["env_sdir"]) and bits_equal(sL, GOLD["env_sL"])
+    assert np.array_equal(fin, GOLD["env_sfin"])
+
+
+def test_env_tables_are_valid_distributions():
+    from open_rendering_framework_b200 import scenes
+
+    data = scenes.env_scene(8, 8, env_w=128, env_h=64)
+    mp, mc, cp, cc = oc.OracleScene(data).env_tables()
+    assert mc[-1] == 1.0 and cc[-1, -1] == 1.0
+    assert np.all(np.diff(mc) >= 0) and np.all(np.diff(cc, axis=1) >= -1e-6)
+    # marginal pdf integrates to 1 over rows, each conditional pdf to 1 over its row
+    assert abs(mp.mean() - 1.0) < 1e-4
+    assert np.allclose(cp.mean(axis=1), 1.0, atol=1e-4)
