@@ -99,6 +99,7 @@ enum {
   PT_DIFFUSE_SHADER = 0,           /* diffuse_shader.cu            */
   PT_ROUGH_TRANSPARENT_SHADER = 3, /* rough_transparent_shader.cu  */
   PT_METALLIC_SHADER = 4,          /* metallic_shader.cu           */
+  PT_TRANSLUCENT_SHADER = 5,       /* subsurface_scattering_shader.cu */
   PT_AREA_LIGHT_MATERIAL = 100     /* arealight_shader.cu          */
 };
 /* Microfacet model / normal distribution enums: structs.h:242-261. */
@@ -124,6 +125,21 @@ typedef struct pt_rough_transparent_params {
   uint32_t microfacet_model;
   uint32_t normal_distribution;
 } pt_rough_transparent_params;
+/* TranslucentMaterial (TranslucentMaterial.cpp:7-30): scattering and absorption coefficients per
+ * RGB channel in 1/mm, the mean cosine of the phase function, the relative index of refraction and
+ * the scene-unit scale applied to the coefficients (default 100), plus mtl["dipole_model"]
+ * (structs.h:311-316, TranslucentMaterial.cpp:15).  The library derives
+ * mtl["scattering_properties"] from them as TranslucentMaterial::computeCoefficients does
+ * (TranslucentMaterial.cpp:303-330, ior_outside = 1). */
+enum { PT_STANDARD_DIPOLE = 0, PT_DIRECTIONAL_DIPOLE = 1 };
+typedef struct pt_translucent_params {
+  float scattering[3];
+  float absorption[3];
+  float meancosine[3];
+  float ior;
+  float scale;
+  uint32_t dipole_model;
+} pt_translucent_params;
 /* gi["radiance"] of a TriangleAreaLight's geometry (Light.cpp:242). */
 typedef struct pt_area_light_params { float radiance[3]; } pt_area_light_params;
 
@@ -138,6 +154,9 @@ typedef struct pt_render_stats {
   float extend_ms;          /* device time spent in the closest-hit (extend) kernel           */
   uint32_t extend_launches; /* number of extend launches                                      */
   uint32_t kernel_launches; /* all kernels launched by the call                               */
+  uint64_t dipole_gathers;  /* dipole gathers evaluated (camera paths entering translucent objects) */
+  uint64_t dipole_pairs;    /* (gather, probe) pairs visited by those gathers                 */
+  uint64_t gather_overflows;/* gathers dropped because a path's gather stack was full (0)     */
 } pt_render_stats;
 
 /* Create / destroy a context on CUDA device `device`. */
@@ -209,6 +228,18 @@ pt_status pt_set_option(pt_ctx* ctx, const char* name, int64_t value);
  * reports their summed device time in extend_ms.  Off by default (the events serialise nothing
  * but cost a few microseconds per bounce). */
 pt_status pt_set_profiling(pt_ctx* ctx, int enable);
+/* Probe points per translucent object and frame: context["samples"] (SAMPLES_FRAME = 500,
+ * OptixSceneLoader.cpp:11-17).  Every frame first runs the probe pass of sample_camera.cu over each
+ * translucent object (OptixScene.cpp:146-157), then the camera paths. */
+pt_status pt_set_probe_count(pt_ctx* ctx, uint32_t samples);
+/* The probe records (PositionSample, structs.h:105-114, 80 bytes each: pos, dir, normal, L,
+ * transmitted, weight as float3 plus 8 bytes of padding) of the last frame rendered, object-major
+ * (samples_output_buffer, translucent object k at [k*samples, (k+1)*samples)).  Writes at most
+ * `capacity` records and the total count to *n_out.  The dir field of probes lit by an indirect path
+ * is zero (the reference leaves it unset). */
+pt_status pt_get_probes(pt_ctx* ctx, void* out, uint64_t capacity, uint64_t* n_out);
+/* The 260-byte ScatteringMaterialProperties (structs.h:116-144) derived for a translucent material. */
+pt_status pt_get_scattering_properties(pt_ctx* ctx, uint32_t material_id, void* out260);
 /* Upper bound on paths kept in flight by one wavefront pass (frames are grouped to fit). */
 pt_status pt_set_max_paths_in_flight(pt_ctx* ctx, uint64_t max_paths);
 

@@ -71,6 +71,9 @@ SIGNATURES = {
     "pt_sync": (I32, [P]),
     "pt_get_render_stats": (I32, [P, P]),
     "pt_set_max_paths_in_flight": (I32, [P, U64]),
+    "pt_set_probe_count": (I32, [P, U32]),
+    "pt_get_probes": (I32, [P, P, U64, P]),
+    "pt_get_scattering_properties": (I32, [P, U32, P]),
     "pt_set_profiling": (I32, [P, I32]),
     "pt_set_option": (I32, [P, ctypes.c_char_p, ctypes.c_int64]),
     "pt_trace_closest": (I32, [P, P, P, U32, P, P, P]),

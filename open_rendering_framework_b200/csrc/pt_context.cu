@@ -20,6 +20,7 @@ SceneDev Context::view() const
   s.tri_info = d_info.as<int4>();
   s.normals = d_normals.as<float4>();
   s.mats = d_mats.as<MatDev>();
+  s.scat = d_scat.as<ScatDev>();
   s.lights = d_lights.as<LightRaw>();
   s.tri_lights = d_tri_lights.as<TriLightRaw>();
   s.n_lights = (int)lights.size();
@@ -55,9 +56,68 @@ static Cx host_recip(const Cx& b)
 
 static bool finite_nonneg3(const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]) && v[0] >= 0 && v[1] >= 0 && v[2] >= 0; }
 
-static pt_status make_material(uint32_t type, const void* params, size_t size, MatDev& m)
+// The boundary polynomials of Fresnel.h:93-124 (two_C1, three_C2, C_phi, C_E).
+static float two_C1(float n)
+{
+  if (n >= 1.0f) return -9.23372f + n * (22.2272f + n * (-20.9292f + n * (10.2291f + n * (-2.54396f + n * 0.254913f))));
+  return 0.919317f + n * (-3.4793f + n * (6.75335f + n * (-7.80989f + n * (4.98554f - n * 1.36881f))));
+}
+static float three_C2(float n)
+{
+  float r;
+  if (n >= 1.0f) {
+    r = -1641.1f + n * (1213.67f + n * (-568.556f + n * (164.798f + n * (-27.0181f + n * 1.91826f))));
+    r += (((135.926f / n) - 656.175f) / n + 1376.53f) / n;
+  } else {
+    r = 0.828421f + n * (-2.62051f + n * (3.36231f + n * (-1.95284f + n * (0.236494f + n * 0.145787f))));
+  }
+  return r;
+}
+static float C_phi(float n) { return 0.25f * (1.0f - two_C1(n)); }
+static float C_E(float n) { return 0.5f * (1.0f - three_C2(n)); }
+
+// TranslucentMaterial::computeCoefficients (TranslucentMaterial.cpp:303-330) with ior_outside = 1,
+// evaluated in FP32 on the host in the same order.
+static ScatDev compute_coefficients(const pt_translucent_params& q)
+{
+  ScatDev p;
+  memset(&p, 0, sizeof(p));
+  const float3 one = f3s(1.0f);
+  const float3 ior_outside = one;
+  p.absorption = f3(q.absorption[0], q.absorption[1], q.absorption[2]) * q.scale;
+  p.scattering = f3(q.scattering[0], q.scattering[1], q.scattering[2]) * q.scale;
+  p.meancosine = f3(q.meancosine[0], q.meancosine[1], q.meancosine[2]);
+  p.relative_ior = q.ior;
+  p.ior_real = f3s(q.ior);
+  float3 ior_rgb = p.ior_real / ior_outside;
+  float3 reducedScattering = p.scattering * (1.0f - p.meancosine);
+  p.relative_ior /= (ior_outside.x + ior_outside.y + ior_outside.z) / 3.0f;
+  p.ior_real = ior_rgb;
+  p.extinction = p.scattering + p.absorption;
+  p.reducedExtinction = reducedScattering + p.absorption;
+  p.deltaEddExtinction = p.scattering * (1.0f - p.meancosine * p.meancosine) + p.absorption;
+  p.D = one / (3.0f * p.reducedExtinction);
+  float3 aD = p.absorption / p.D;
+  p.transport = f3(sqrtf(aD.x), sqrtf(aD.y), sqrtf(aD.z));
+  p.C_phi = f3(C_phi(ior_rgb.x), C_phi(ior_rgb.y), C_phi(ior_rgb.z));
+  p.C_phi_inv = f3(C_phi(1.0f / ior_rgb.x), C_phi(1.0f / ior_rgb.y), C_phi(1.0f / ior_rgb.z));
+  p.C_E = f3(C_E(ior_rgb.x), C_E(ior_rgb.y), C_E(ior_rgb.z));
+  p.albedo = p.scattering / p.extinction;
+  p.reducedAlbedo = reducedScattering / p.reducedExtinction;
+  p.de = 2.131f * p.D / f3(sqrtf(p.reducedAlbedo.x), sqrtf(p.reducedAlbedo.y), sqrtf(p.reducedAlbedo.z));
+  p.A = (1.0f - p.C_E) / (2.0f * p.C_phi);
+  p.three_D = 3.0f * p.D;
+  p.two_A_de = 2.0f * p.A * p.de;
+  p.global_coeff = one / (4.0f * p.C_phi_inv) * 1.0f / (4.0f * kPi * kPi);
+  p.one_over_three_ext = one / (3.0f * p.extinction);
+  p.mean_transport = (p.transport.x + p.transport.y + p.transport.z) / 3.0f;
+  return p;
+}
+
+static pt_status make_material(uint32_t type, const void* params, size_t size, MatDev& m, ScatDev& sc)
 {
   memset(&m, 0, sizeof(m));
+  memset(&sc, 0, sizeof(sc));
   m.type = type;
   if (!params) return fail(PT_INVALID_ARG, "material: null parameters");
   switch (type) {
@@ -100,6 +160,23 @@ static pt_status make_material(uint32_t type, const void* params, size_t size, M
       m.dist = p->normal_distribution;
       m.a = make_float4(p->ior, p->roughness, 0.0f, 0.0f);
       m.b = make_float4(p->glass_absorption[0], p->glass_absorption[1], p->glass_absorption[2], 0.0f);
+      return PT_OK;
+    }
+    case PT_TRANSLUCENT_SHADER: {
+      if (size != sizeof(pt_translucent_params)) return fail(PT_INVALID_ARG, "translucent material: wrong parameter size");
+      const pt_translucent_params* p = (const pt_translucent_params*)params;
+      if (!finite_nonneg3(p->absorption) || !finite_nonneg3(p->scattering))
+        return fail(PT_INVALID_ARG, "translucent material: absorption and scattering must be finite and >= 0");
+      for (int k = 0; k < 3; ++k) {
+        if (!(p->meancosine[k] > -1.0f && p->meancosine[k] < 1.0f)) return fail(PT_INVALID_ARG, "translucent material: meancosine must be in (-1, 1)");
+        if (!(p->absorption[k] + p->scattering[k] * (1.0f - p->meancosine[k]) > 0.0f))
+          return fail(PT_INVALID_ARG, "translucent material: the reduced extinction must be > 0");
+      }
+      if (!(p->ior > 0.0f && std::isfinite(p->ior))) return fail(PT_INVALID_ARG, "translucent material: ior must be > 0");
+      if (!(p->scale > 0.0f && std::isfinite(p->scale))) return fail(PT_INVALID_ARG, "translucent material: scale must be > 0");
+      if (p->dipole_model > PT_DIRECTIONAL_DIPOLE) return fail(PT_INVALID_ARG, "translucent material: bad dipole_model");
+      m.model = p->dipole_model;
+      sc = compute_coefficients(*p);
       return PT_OK;
     }
     case PT_AREA_LIGHT_MATERIAL: {
@@ -379,11 +456,13 @@ pt_status pt_material_create(pt_ctx* ctx, uint32_t type, const void* params, siz
 {
   if (!ctx || !out_id) return fail(PT_INVALID_ARG, "pt_material_create: null argument");
   MatDev m;
-  pt_status st = make_material(type, params, params_size, m);
+  ScatDev sc;
+  pt_status st = make_material(type, params, params_size, m, sc);
   if (st != PT_OK) return st;
   if (ctx->c.mats.size() >= (1u << 20)) return fail(PT_CAP_EXCEEDED, "pt_material_create: too many materials");
   *out_id = (uint32_t)ctx->c.mats.size();
   ctx->c.mats.push_back(m);
+  ctx->c.scat.push_back(sc);
   ctx->c.dirty_materials = true;
   return PT_OK;
 }
@@ -393,9 +472,12 @@ pt_status pt_material_update(pt_ctx* ctx, uint32_t id, const void* params, size_
   if (!ctx) return fail(PT_INVALID_ARG, "null context");
   if (id >= ctx->c.mats.size()) return fail(PT_INVALID_ARG, "pt_material_update: no such material");
   MatDev m;
-  pt_status st = make_material(ctx->c.mats[id].type, params, params_size, m);
+  ScatDev sc;
+  pt_status st = make_material(ctx->c.mats[id].type, params, params_size, m, sc);
   if (st != PT_OK) return st;
+  m.aux = ctx->c.mats[id].aux;  // translucent_index stays with the material
   ctx->c.mats[id] = m;
+  ctx->c.scat[id] = sc;
   ctx->c.dirty_materials = true;
   return PT_OK;
 }
@@ -435,6 +517,15 @@ pt_status pt_mesh_add(pt_ctx* ctx, const float* positions, uint32_t n_vertices, 
       info.z = (int)normal_base + nindex[3 * t + 2];
     }
     c.tri_info.push_back(info);
+  }
+  if (c.mats[material_id].type == PT_TRANSLUCENT_SHADER) {
+    // a translucent object with its own probe set; the material's translucent_index is the last
+    // object registered with it (OptixSceneLoader.cpp:509-510)
+    if (c.trans_objs.size() >= 1024) return fail(PT_CAP_EXCEEDED, "pt_mesh_add: at most 1024 translucent objects");
+    c.trans_objs.push_back(make_uint4(material_id, c.n_tris, n_triangles, (uint32_t)(c.trans_pos.size() / 9)));
+    c.trans_pos.insert(c.trans_pos.end(), c.tri_pos.end() - 9 * (size_t)n_triangles, c.tri_pos.end());
+    c.mats[material_id].aux = (uint32_t)c.trans_objs.size() - 1;
+    c.dirty_materials = true;
   }
   c.n_tris += n_triangles;
   c.built = false;
@@ -479,6 +570,9 @@ pt_status pt_build(pt_ctx* ctx)
   if (st == PT_OK) st = upload(c.d_info, c.tri_info, c.stream, "triangle info");
   if (st == PT_OK) st = upload(c.d_normals, c.normals, c.stream, "normals");
   if (st == PT_OK) st = upload(c.d_mats, c.mats, c.stream, "materials");
+  if (st == PT_OK) st = upload(c.d_scat, c.scat, c.stream, "scattering properties");
+  if (st == PT_OK) st = upload(c.d_trans_objs, c.trans_objs, c.stream, "translucent objects");
+  if (st == PT_OK) st = upload(c.d_trans_pos, c.trans_pos, c.stream, "translucent triangles");
   if (st != PT_OK) return st;
   if (c.lights.empty()) {
     // light_buffer of size 0 is legal; keep a valid pointer for the kernels
@@ -520,6 +614,23 @@ pt_status pt_sync(pt_ctx* ctx)
 {
   CTX_CHECK(ctx);
   PT_CHECK_CUDA(cudaStreamSynchronize(ctx->c.stream), "pt_sync");
+  return PT_OK;
+}
+
+pt_status pt_set_probe_count(pt_ctx* ctx, uint32_t samples)
+{
+  if (!ctx) return fail(PT_INVALID_ARG, "null context");
+  if (samples < 1 || samples > (1u << 24)) return fail(PT_INVALID_ARG, "pt_set_probe_count: must be in [1, 2^24]");
+  ctx->c.probe_samples = samples;
+  return PT_OK;
+}
+
+pt_status pt_get_scattering_properties(pt_ctx* ctx, uint32_t material_id, void* out260)
+{
+  if (!ctx || !out260) return fail(PT_INVALID_ARG, "pt_get_scattering_properties: null argument");
+  if (material_id >= ctx->c.mats.size()) return fail(PT_INVALID_ARG, "pt_get_scattering_properties: no such material");
+  if (ctx->c.mats[material_id].type != PT_TRANSLUCENT_SHADER) return fail(PT_INVALID_ARG, "pt_get_scattering_properties: not a translucent material");
+  memcpy(out260, &ctx->c.scat[material_id], sizeof(ScatDev));
   return PT_OK;
 }
 

@@ -49,28 +49,39 @@ struct Wavefront {
   DevBuf q_mat;                               // per-material-class queues, kQueues x cap
   DevBuf sh_o, sh_d, sh_c, sh_pid;            // shadow-ray queue
   DevBuf counters;                            // kCounters uint32
+  // translucent objects: the per-path stack of pending dipole gathers ([slot][path]) and the probes
+  uint32_t gather_slots = 0;
+  uint64_t gather_cap = 0;
+  DevBuf g_a, g_b, g_c;
+  uint64_t probe_cap = 0;                     // PositionSample records held
+  DevBuf probes;                              // PositionSample (80 B) per probe, [frame][object][sample]
+  DevBuf pc_pos, pc_wl, pc_nrm, pc_tr, pc_cnt;// probes with L != 0, compacted in order per (frame, object)
 };
 
 // Counter slots in Wavefront::counters.
 enum CounterSlot {
   CNT_ACTIVE_A = 0,
   CNT_ACTIVE_B = 1,
-  CNT_Q_MISS = 2,
+  CNT_Q_MISS = 2,        // kQueues consecutive material-queue counts
   CNT_Q_LIGHT = 3,
   CNT_Q_DIFFUSE = 4,
   CNT_Q_METAL = 5,
   CNT_Q_GLASS = 6,
-  CNT_SHADOW = 7,
-  CNT_SEGMENTS_LO = 8,   // 64-bit totals as two words each (atomicAdd on unsigned long long)
-  CNT_SHADOW_TOTAL = 10,
-  CNT_CAPPED = 12,
-  CNT_CLAMPED = 14,
-  CNT_ERROR = 16,
-  CNT_FETCH_EXT = 18,
-  CNT_FETCH_SH = 19,
+  CNT_Q_TRANS = 7,
+  CNT_SHADOW = 8,
+  CNT_FETCH_EXT = 9,
+  CNT_FETCH_SH = 10,
+  CNT_GATHER = 11,
+  CNT_SEGMENTS_LO = 12,  // 64-bit totals as two words each (atomicAdd on unsigned long long)
+  CNT_SHADOW_TOTAL = 14,
+  CNT_CAPPED = 16,
+  CNT_CLAMPED = 18,
+  CNT_ERROR = 20,
+  CNT_PAIRS = 22,        // probe evaluations of the dipole gathers
+  CNT_GATHERS = 24,      // dipole gathers evaluated
   kCounters = 32
 };
-enum QueueClass { QC_MISS = 0, QC_LIGHT = 1, QC_DIFFUSE = 2, QC_METAL = 3, QC_GLASS = 4, kQueues = 5 };
+enum QueueClass { QC_MISS = 0, QC_LIGHT = 1, QC_DIFFUSE = 2, QC_METAL = 3, QC_GLASS = 4, QC_TRANS = 5, kQueues = 6 };
 
 // Tunable launch options (pt_set_option); the autotuner searches over these.
 struct Options {
@@ -89,6 +100,13 @@ struct Context {
   float3 bg_color{1.0f, 1.0f, 1.0f};                      // ConstantBackground default (Background.cpp:10)
 
   std::vector<MatDev> mats;
+  std::vector<ScatDev> scat;        // per material; the scattering properties of translucent ones
+  // translucent objects (OptixSceneLoader::computeTranslucentGeometries, OptixSceneLoader.cpp:482-524):
+  // (material, first triangle, triangle count, offset into trans_pos) per translucent mesh
+  std::vector<uint4> trans_objs;
+  std::vector<float> trans_pos;     // their vertex positions, 9 floats per triangle, as given
+  uint32_t probe_samples = 500;     // context["samples"] (OptixSceneLoader.cpp:11-17)
+  uint32_t probe_last_frames = 0;   // frames whose probes the probe buffer holds (the last one is read back)
   // meshes as added (host copies until pt_build)
   std::vector<float> tri_pos;       // 9 floats per triangle
   std::vector<int4> tri_info;       // (n0, n1, n2, material)
@@ -101,6 +119,7 @@ struct Context {
   uint32_t n_tris = 0;
 
   DevBuf d_nodes, d_v0, d_e1, d_e2, d_info, d_normals, d_mats, d_lights, d_tri_lights;
+  DevBuf d_scat, d_trans_objs, d_trans_pos;
   DevBuf d_accum;  // float4 per pixel
   DevBuf d_env_tex, d_env_mpdf, d_env_mcdf, d_env_cpdf, d_env_ccdf, d_env_lum, d_env_mf;
   int env_w = 0, env_h = 0;

@@ -4,7 +4,7 @@
 // One call of pt_render_frames traces every (pixel, frame) camera sample of a group of frames at
 // once.  Per bounce:
 //   extend   closest hit through the stackless BVH; each path id is appended to the queue of its
-//            hit's material class (miss, emitter, diffuse, conductor, rough dielectric) -- the sort
+//            hit's material class (miss, emitter, diffuse, conductor, rough dielectric, translucent) -- the sort
 //            by material key -- with block-aggregated appends (warp ballots + shared-memory prefix,
 //            one global atomic per block and class)
 //   shade    one kernel per material class, following diffuse_shader.cu, metallic_shader.cu,
@@ -12,7 +12,13 @@
 //            appended to the next active queue and diffuse next-event estimation to the shadow queue
 //   shadow   any-hit through the same BVH; unoccluded contributions are added to the path radiance
 // and finally `accumulate` folds the frames into the float4 running mean in frame order
-// (path_tracer.cu:64-68).  Each path keeps one tea stream and one MD5 stream exactly as the
+// (path_tracer.cu:64-68).
+//
+// Scenes with translucent objects first run the probe pass of every frame (sample_camera.cu): one
+// PositionSample per (object, sample), lit by a shadowed light sample or by an indirect path that
+// goes through the same wavefront.  The probes with L != 0 are compacted in order, and the dipole
+// gathers that camera paths owe on entering a translucent object are evaluated after the paths end
+// (see k_shade_translucent).  Each path keeps one tea stream and one MD5 stream exactly as the
 // reference's recursion passes prd.seed down the path, so paths consume identical random numbers.
 //
 // The reference's recursion result is result = own + child * weight; here the equivalent iterative
@@ -24,6 +30,7 @@
 #include <cstring>
 
 #include "pt_context.h"
+#include "pt_dipole.cuh"
 
 namespace pt {
 
@@ -34,6 +41,9 @@ constexpr int kWarps = kBlock / 32;
 constexpr uint32_t META_DEPTH = 0xffffu;
 constexpr uint32_t META_EMIT = 1u << 16;
 constexpr uint32_t META_OUTSIDE = 1u << 17;
+constexpr uint32_t META_PROBE = 1u << 18;  // a probe's indirect path (sample_camera.cu:168-206)
+constexpr int META_GSHIFT = 24;            // pending dipole gathers on the path's stack (8 bits)
+constexpr uint32_t META_KEEP = ~(META_DEPTH | META_EMIT);
 
 struct WfDev {
   float4* ray_o;
@@ -52,6 +62,24 @@ struct WfDev {
   uint32_t* cnt;
   uint64_t cap;
   int in_slot, out_slot;
+  // pending dipole gathers, [slot * cap + path]: (xo, throughput.x), (no, throughput.y), (throughput.z, material)
+  float4* g_a;
+  float4* g_b;
+  float2* g_c;
+  uint32_t g_slots;
+};
+
+// Translucent objects and their probes.
+struct SssDev {
+  const uint4* objs;   // (material, first triangle, triangle count, offset into pos9)
+  const float* pos9;   // vertex positions of the objects' triangles, as given
+  uint32_t n_obj, samples;
+  float4* probes;      // 5 float4 per PositionSample
+  float4* pc_pos;      // compacted probes with L != 0 per (frame, object): pos
+  float4* pc_wl;       //   weight * L
+  float4* pc_nrm;      //   normal
+  float4* pc_tr;       //   transmitted
+  uint32_t* pc_cnt;    //   count per (frame, object)
 };
 
 __device__ __forceinline__ unsigned lanemask_lt() { return (1u << (threadIdx.x & 31)) - 1u; }
@@ -266,6 +294,7 @@ __device__ __forceinline__ int class_of(uint32_t type)
     case MAT_DIFFUSE: return QC_DIFFUSE;
     case MAT_METAL: return QC_METAL;
     case MAT_ROUGH_GLASS: return QC_GLASS;
+    case MAT_TRANSLUCENT: return QC_TRANS;
     case MAT_LIGHT: return QC_LIGHT;
     default: return -1;
   }
@@ -542,7 +571,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_diffuse(SceneDev S, WfDev w, c
           w.thr[pid] = make_float4(nt.x, nt.y, nt.z, 0.0f);
           cont = true;
         }
-        w.rng[pid] = make_uint4(t, rg.y, rg.z, (uint32_t)(depth + 1) | (emit ? META_EMIT : 0u));
+        w.rng[pid] = make_uint4(t, rg.y, rg.z, (rg.w & META_KEEP) | (uint32_t)(depth + 1) | (emit ? META_EMIT : 0u));
       }
     }
     uint32_t s_slot = block_slot(shadow, w.cnt + CNT_SHADOW, sm);
@@ -622,7 +651,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_metal(SceneDev S, WfDev w, con
           w.thr[pid] = make_float4(nt.x, nt.y, nt.z, 0.0f);
           cont = true;
         }
-        w.rng[pid] = make_uint4(seed, rg.y, rg.z, (uint32_t)(depth + 1) | META_EMIT);
+        w.rng[pid] = make_uint4(seed, rg.y, rg.z, (rg.w & META_KEEP) | (uint32_t)(depth + 1) | META_EMIT);
       }
     }
     uint32_t c_slot = block_slot(cont, w.cnt + w.out_slot, sm);
@@ -710,13 +739,351 @@ __global__ void __launch_bounds__(kBlock) k_shade_glass(SceneDev S, WfDev w, con
           w.thr[pid] = make_float4(nt.x, nt.y, nt.z, 0.0f);
           cont = true;
         }
-        w.rng[pid] = make_uint4(t, rg.y, rg.z, (uint32_t)(depth + 1) | META_EMIT);
+        w.rng[pid] = make_uint4(t, rg.y, rg.z, (rg.w & META_KEEP) | (uint32_t)(depth + 1) | META_EMIT);
       }
     }
     uint32_t c_slot = block_slot(cont, w.cnt + w.out_slot, sm);
     if (cont) w.q_out[c_slot] = pid;
   }
   if (capped_total) atomicAdd(cnt64(w.cnt, CNT_CAPPED), (unsigned long long)capped_total);
+}
+
+// ------------------------------------------------------------------ translucent objects
+// subsurface_scattering_shader.cu:55-201 with REFLECT, TRANSMIT and RND_64 defined: the Fresnel
+// choice between the reflected and the refracted ray (one MD5 draw), and inside the object Beer
+// transmittance over the segment with Russian roulette on its mean (extinction, or the
+// delta-Eddington extinction for the directional dipole).  A camera path refracted into the object
+// from outside also owes the dipole gather over the frame's probes (:126-173).  The reference
+// evaluates it after the refracted subtree has returned, so its MD5 draws follow every draw of that
+// subtree; the vertex (position, normal, throughput, material) is therefore pushed on the path's
+// gather stack and evaluated in last-in first-out order when the path has ended (k_gather).  A
+// probe's indirect path does not gather: in the reference it would read the probe buffer that its
+// own launch is writing.
+__global__ void __launch_bounds__(kBlock) k_shade_translucent(SceneDev S, WfDev w, const float4* geo)
+{
+  __shared__ uint32_t sm[kWarps + 1];
+  const uint32_t n = w.cnt[CNT_Q_TRANS];
+  const uint32_t* q = w.q_mat + (size_t)QC_TRANS * w.cap;
+  uint32_t overflow = 0;
+  for (uint32_t base = blockIdx.x * kBlock; base < n; base += gridDim.x * kBlock) {
+    uint32_t i = base + threadIdx.x;
+    bool cont = false;
+    uint32_t pid = 0;
+    if (i < n) {
+      pid = q[i];
+      uint4 rg = w.rng[pid];
+      int depth = (int)(rg.w & META_DEPTH);
+      if (depth <= S.integ.max_depth) {
+        float4 h = w.hit[pid], o = w.ray_o[pid], d4 = w.ray_d[pid];
+        int prim = __float_as_int(h.w);
+        int4 info = __ldg(S.tri_info + prim);
+        const MatDev& m = S.mats[info.w];
+        const ScatDev& P = S.scat[info.w];
+        float3 d = ld3(d4);
+        float3 no = shading_normal(S, geo, info, h.y, h.z, prim);
+        float3 xo = ld3(o) + h.x * d;
+        float3 wo = -d;
+        float recip_ior = 1.0f / P.relative_ior;
+        float3 beam_T = f3s(1.0f);
+        uint2 t64 = make_uint2(rg.y, rg.z);
+        float reflect_xi = rnd_md5(t64);
+        float cos_o = dot(wo, no);
+        bool inside = cos_o < 0.0f;
+        bool alive = true;
+        if (inside) {
+          float3 ext = m.model == DIRECTIONAL_DIPOLE ? P.deltaEddExtinction : P.extinction;
+          beam_T = expf3((-h.x) * ext);
+          float prob = (beam_T.x + beam_T.y + beam_T.z) / 3.0f;
+          if (rnd_md5(t64) >= prob) {
+            alive = false;
+          } else {
+            beam_T = beam_T / prob;
+            recip_ior = P.relative_ior;
+            no = -no;
+            cos_o = -cos_o;
+          }
+        }
+        uint32_t meta = rg.w & META_KEEP;
+        if (alive) {
+          float st2 = recip_ior * recip_ior * (1.0f - cos_o * cos_o);
+          float cos_t = 1.0f, R = 1.0f;
+          if (st2 < 1.0f) {
+            cos_t = sqrtf(1.0f - st2);
+            R = fresnel_R(cos_o, cos_t, recip_ior);
+          }
+          float4 t4 = w.thr[pid];
+          float3 nd;
+          if (reflect_xi >= R) {
+            nd = recip_ior * (cos_o * no - wo) - no * cos_t;
+            if (!inside && !(rg.w & META_PROBE)) {
+              uint32_t slot = meta >> META_GSHIFT;
+              if (slot < w.g_slots) {
+                size_t at = (size_t)slot * w.cap + pid;
+                w.g_a[at] = make_float4(xo.x, xo.y, xo.z, t4.x);
+                w.g_b[at] = make_float4(no.x, no.y, no.z, t4.y);
+                w.g_c[at] = make_float2(t4.z, __int_as_float(info.w));
+                meta += 1u << META_GSHIFT;
+              } else {
+                ++overflow;
+              }
+            }
+          } else {
+            nd = 2.0f * cos_o * no - wo;
+          }
+          float3 nt = ld3(t4) * beam_T;
+          w.ray_o[pid] = make_float4(xo.x, xo.y, xo.z, 0.0f);
+          w.ray_d[pid] = make_float4(nd.x, nd.y, nd.z, 0.0f);
+          w.thr[pid] = make_float4(nt.x, nt.y, nt.z, 0.0f);
+          cont = true;
+        }
+        w.rng[pid] = make_uint4(rg.x, t64.x, t64.y, meta | (uint32_t)(depth + 1) | META_EMIT);
+      }
+    }
+    uint32_t c_slot = block_slot(cont, w.cnt + w.out_slot, sm);
+    if (cont) w.q_out[c_slot] = pid;
+  }
+  if (overflow) atomicAdd(cnt64(w.cnt, CNT_ERROR), (unsigned long long)overflow);
+}
+
+// Paths with pending dipole gathers, appended to `out` (warp-aggregated).
+__global__ void __launch_bounds__(kBlock) k_gather_collect(WfDev w, uint64_t n_paths, uint32_t* out)
+{
+  for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < n_paths; base += (uint64_t)gridDim.x * kBlock) {
+    uint64_t pid = base + threadIdx.x;
+    bool want = pid < n_paths && (w.rng[pid].w >> META_GSHIFT) != 0;
+    unsigned m = __ballot_sync(0xffffffffu, want);
+    if (m) {
+      int leader = __ffs(m) - 1;
+      uint32_t b = 0;
+      if ((int)(threadIdx.x & 31) == leader) b = atomicAdd(w.cnt + CNT_GATHER, (uint32_t)__popc(m));
+      b = __shfl_sync(0xffffffffu, b, leader);
+      if (want) out[b + __popc(m & lanemask_lt())] = (uint32_t)pid;
+    }
+  }
+}
+
+// The dipole gathers of subsurface_scattering_shader.cu:126-173, evaluated for each path in the
+// reverse order of their vertices (the post-order of the reference's recursion).  Per probe with
+// L != 0 of the path's frame and object: distance Russian roulette with p = exp(-dist * min sigma_tr)
+// on one MD5 draw, and on acceptance T12 * L * S(probe, xo) / p with the standard or directional
+// dipole.  The sum times global_coeff / samples is added to the path's radiance, weighted by the
+// throughput at the vertex.  One thread per path: the MD5 stream is one sequential chain.
+__global__ void __launch_bounds__(kBlock) k_gather(SceneDev S, WfDev w, SssDev g, const uint32_t* list, uint32_t pixels)
+{
+  const uint32_t n = w.cnt[CNT_GATHER];
+  unsigned long long pairs = 0, gathers = 0;
+  for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+    uint32_t pid = list[i];
+    uint4 rg = w.rng[pid];
+    uint2 t64 = make_uint2(rg.y, rg.z);
+    uint32_t fl = pid / pixels;
+    float4 r4 = w.rad[pid];
+    float3 L = ld3(r4);
+    for (int slot = (int)(rg.w >> META_GSHIFT) - 1; slot >= 0; --slot) {
+      size_t at = (size_t)slot * w.cap + pid;
+      float4 a = w.g_a[at], b = w.g_b[at];
+      float2 c = w.g_c[at];
+      const float3 xo = ld3(a), no = ld3(b), thr = f3(a.w, b.w, c.x);
+      const int mat = __float_as_int(c.y);
+      const MatDev& m = S.mats[mat];
+      const ScatDev& P = S.scat[mat];
+      const uint32_t set = fl * g.n_obj + m.aux;
+      const size_t pb = (size_t)set * g.samples;
+      const uint32_t nc = g.pc_cnt[set];
+      const float chosen = fminf(P.transport.x, fminf(P.transport.y, P.transport.z));
+      float3 acc = f3s(0.0f);
+      if (m.model == DIRECTIONAL_DIPOLE) {
+        for (uint32_t k = 0; k < nc; ++k) {
+          float3 pos = ld3(__ldg(g.pc_pos + pb + k));
+          float dist = length(xo - pos);
+          float exp_term = expf(-dist * chosen);
+          if (rnd_md5(t64) < exp_term) {
+            float3 wl = ld3(__ldg(g.pc_wl + pb + k));
+            float3 pn = ld3(__ldg(g.pc_nrm + pb + k)), pt = ld3(__ldg(g.pc_tr + pb + k));
+            acc = acc + wl * dirpole_bssrdf(pos, pn, pt, xo, no, P) / exp_term;
+          }
+        }
+      } else {
+        const StdDipole sd = std_dipole_terms(P);
+        for (uint32_t k = 0; k < nc; ++k) {
+          float3 pos = ld3(__ldg(g.pc_pos + pb + k));
+          float dist = length(xo - pos);
+          float exp_term = expf(-dist * chosen);
+          if (rnd_md5(t64) < exp_term) {
+            float3 wl = ld3(__ldg(g.pc_wl + pb + k));
+            acc = acc + wl * dipole_bssrdf(dist, sd) / exp_term;
+          }
+        }
+      }
+      float3 contrib = acc * P.global_coeff / (float)g.samples;
+      L = L + thr * contrib;
+      pairs += nc;
+      ++gathers;
+    }
+    w.rad[pid] = make_float4(L.x, L.y, L.z, r4.w);
+    w.rng[pid] = make_uint4(rg.x, t64.x, t64.y, rg.w);
+  }
+  if (pairs) atomicAdd(cnt64(w.cnt, CNT_PAIRS), pairs);
+  if (gathers) atomicAdd(cnt64(w.cnt, CNT_GATHERS), gathers);
+}
+
+// sample_camera.cu:48-268 for a smooth translucent object, with GLOBAL and RND_64 defined: probe j of
+// the group (frame-major, then object, then sample; path id j - j0).  The triangle is picked with an
+// MD5 draw, the point uniformly on it, and with probability 1/2 (one LCG draw) the probe is lit by a
+// light sample with a shadow ray (written to the path's radiance here), else by an indirect path
+// started into the wavefront from the point (depth 0, emission on).  The record keeps pos, dir (of the
+// light sample), normal, transmitted direction and T12; pad = (triangles * area, indirect flag) until
+// k_probe_finish forms L.
+__global__ void __launch_bounds__(kBlock) k_probe_gen(SceneDev S, WfDev w, SssDev g, uint32_t first_frame, uint64_t j0, uint64_t n)
+{
+  __shared__ uint32_t sm[kWarps + 1];
+  const uint64_t per_frame = (uint64_t)g.n_obj * g.samples;
+  uint32_t clamped = 0;
+  for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < n; base += (uint64_t)gridDim.x * kBlock) {
+    uint64_t pid = base + threadIdx.x;
+    bool indirect = false;
+    if (pid < n) {
+      uint64_t j = j0 + pid;
+      uint32_t fl = (uint32_t)(j / per_frame);
+      uint32_t idx = (uint32_t)(j % per_frame);  // launch_index + current_translucent_obj * samples
+      uint32_t k = idx / g.samples;
+      uint32_t frame = first_frame + fl;
+      uint4 ob = g.objs[k];
+      const uint32_t triangles = ob.z;
+      const ScatDev& P = S.scat[ob.x];
+      uint32_t t = tea16(idx, frame);
+      uint32_t s2 = tea16(idx, frame);
+      uint2 t64 = make_uint2(s2, s2);
+      uint32_t tid = (uint32_t)(int)(rnd_md5(t64) * (float)triangles);
+      if (tid >= triangles) { tid = triangles - 1; ++clamped; }
+      const float* v = g.pos9 + 9 * ((size_t)ob.w + tid);
+      float3 v0 = f3(v[0], v[1], v[2]), v1 = f3(v[3], v[4], v[5]), v2 = f3(v[6], v[7], v[8]);
+      float3 perp = cross(v1 - v0, v2 - v0);
+      float area = 0.5f * length(perp);
+      float xi1 = sqrtf(rnd_md5(t64));
+      float xi2 = rnd_md5(t64);
+      float u = 1.0f - xi1, vv = (1.0f - xi2) * xi1, ww = xi1 * xi2;
+      float3 pos = u * v0 + vv * v1 + ww * v2;
+      int4 info = __ldg(S.tri_info + ob.y + tid);
+      float3 nrm;
+      if (info.x >= 0) {
+        float3 n0 = ld3(__ldg(S.normals + info.x)), n1 = ld3(__ldg(S.normals + info.y)), n2 = ld3(__ldg(S.normals + info.z));
+        nrm = normalize(u * n0 + vv * n1 + ww * n2);
+        nrm = normalize(nrm);
+      } else {
+        nrm = normalize(perp);
+      }
+      const float recip_ior = 1.0f / P.relative_ior;
+      float3 Le, w_i, dir = f3s(0.0f);
+      if (rnd_lcg(t) < 0.5f) {
+        uint32_t li = (uint32_t)((float)S.n_lights * rnd_md5(t64));
+        if (li >= (uint32_t)S.n_lights) { li = (uint32_t)S.n_lights - 1; ++clamped; }
+        float light_pdf = 1.0f / (float)S.n_lights;
+        LightRaw ls = S.lights[li];
+        float r = 0.0f;
+        eval_direct(S, pos, ls, w_i, Le, r, t, clamped);
+        dir = w_i;
+        float cos_i = fmaxf(dot(w_i, nrm), 0.0f);
+        if (cos_i > 0.0f) {
+          float att = trace_any(S, pos, w_i, S.integ.scene_epsilon, r) ? 0.0f : 1.0f;
+          Le = Le * (att * cos_i / light_pdf);
+        } else {
+          Le = f3s(0.0f);
+        }
+        w.rad[pid] = make_float4(Le.x, Le.y, Le.z, 0.0f);
+      } else {
+        w_i = sample_cosine_weighted(nrm, t);
+        w.ray_o[pid] = make_float4(pos.x, pos.y, pos.z, 0.0f);
+        w.ray_d[pid] = make_float4(w_i.x, w_i.y, w_i.z, 0.0f);
+        w.thr[pid] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        w.rad[pid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        w.rng[pid] = make_uint4(t, t64.x, t64.y, META_EMIT | META_PROBE);
+        indirect = true;
+      }
+      float cos_i = fmaxf(dot(w_i, nrm), 0.0f);
+      float cos_i2 = cos_i * cos_i;
+      float st2 = recip_ior * recip_ior * (1.0f - cos_i2);
+      float cos_t = sqrtf(1.0f - st2);
+      float3 tr = recip_ior * (cos_i * nrm - w_i) - nrm * cos_t;
+      float T12 = 1.0f - fresnel_R(cos_i, cos_t, recip_ior);
+      float4* rec = g.probes + 5 * j;
+      rec[0] = make_float4(pos.x, pos.y, pos.z, dir.x);
+      rec[1] = make_float4(dir.y, dir.z, nrm.x, nrm.y);
+      rec[2] = make_float4(nrm.z, 0.0f, 0.0f, 0.0f);
+      rec[3] = make_float4(tr.x, tr.y, tr.z, T12);
+      rec[4] = make_float4(T12, T12, (float)triangles * area, indirect ? 1.0f : 0.0f);
+    }
+    uint32_t slot = block_slot(indirect, w.cnt + w.in_slot, sm);
+    if (indirect) w.q_in[slot] = (uint32_t)pid;
+  }
+  if (clamped) atomicAdd(cnt64(w.cnt, CNT_CLAMPED), (unsigned long long)clamped);
+}
+
+// sample_camera.cu:207 and :230: Le = (light sample, or the indirect path's radiance times pi) / 0.5,
+// L = Le * (triangles * area).
+__global__ void __launch_bounds__(kBlock) k_probe_finish(WfDev w, SssDev g, uint64_t j0, uint64_t n)
+{
+  for (uint64_t pid = (uint64_t)blockIdx.x * kBlock + threadIdx.x; pid < n; pid += (uint64_t)gridDim.x * kBlock) {
+    float4* rec = g.probes + 5 * (j0 + pid);
+    float4 r4 = rec[4];
+    float3 Le = ld3(w.rad[pid]);
+    if (r4.w != 0.0f) Le = Le * kPi;
+    Le = Le / 0.5f;
+    float3 L = Le * r4.z;
+    float4 r2 = rec[2];
+    rec[2] = make_float4(r2.x, L.x, L.y, L.z);
+    rec[4] = make_float4(r4.x, r4.y, 0.0f, 0.0f);
+  }
+}
+
+// The probes with dot(L, L) > 0 of one (frame, object) set, compacted in order: one block per set.
+__global__ void __launch_bounds__(256) k_probe_compact(SssDev g)
+{
+  __shared__ uint32_t warp_off[8];
+  __shared__ uint32_t total;
+  const uint32_t set = blockIdx.x;
+  const size_t b = (size_t)set * g.samples;
+  if (threadIdx.x == 0) total = 0;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t c0 = 0; c0 < g.samples; c0 += 256) {
+    uint32_t i = c0 + threadIdx.x;
+    bool keep = false;
+    float3 pos, nrm, L, tr, wt;
+    if (i < g.samples) {
+      const float4* rec = g.probes + 5 * (b + i);
+      float4 r0 = rec[0], r1 = rec[1], r2 = rec[2], r3 = rec[3], r4 = rec[4];
+      pos = ld3(r0);
+      nrm = f3(r1.z, r1.w, r2.x);
+      L = f3(r2.y, r2.z, r2.w);
+      tr = ld3(r3);
+      wt = f3(r3.w, r4.x, r4.y);
+      keep = dot(L, L) > 0.0f;
+    }
+    unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) warp_off[warp] = __popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t run = total;
+      for (int k = 0; k < 8; ++k) {
+        uint32_t cnt = warp_off[k];
+        warp_off[k] = run;
+        run += cnt;
+      }
+      total = run;
+    }
+    __syncthreads();
+    if (keep) {
+      size_t o = b + warp_off[warp] + __popc(m & lanemask_lt());
+      float3 wl = wt * L;
+      g.pc_pos[o] = make_float4(pos.x, pos.y, pos.z, 0.0f);
+      g.pc_wl[o] = make_float4(wl.x, wl.y, wl.z, 0.0f);
+      g.pc_nrm[o] = make_float4(nrm.x, nrm.y, nrm.z, 0.0f);
+      g.pc_tr[o] = make_float4(tr.x, tr.y, tr.z, 0.0f);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) g.pc_cnt[set] = total;
 }
 
 // Shadow rays of diffuse_shader.cu:149-161 (every material's any-hit program is opaque).
@@ -797,6 +1164,39 @@ static pt_status ensure_wavefront(Context& c, uint64_t cap)
   return PT_OK;
 }
 
+// Gather stacks for `cap` paths with `slots` entries each, and probe storage for `records` probes.
+static pt_status ensure_sss(Context& c, uint64_t cap, uint32_t slots, uint64_t records, uint64_t sets)
+{
+  Wavefront& wf = c.wf;
+  pt_status st = PT_OK;
+  if (wf.gather_cap < cap || wf.gather_slots < slots || !wf.g_a.p) {
+    const size_t n = (size_t)cap * slots;
+    st = wf.g_a.reserve(n * sizeof(float4), "dipole gather stack");
+    if (st == PT_OK) st = wf.g_b.reserve(n * sizeof(float4), "dipole gather stack");
+    if (st == PT_OK) st = wf.g_c.reserve(n * sizeof(float2), "dipole gather stack");
+    if (st != PT_OK) {
+      wf.gather_cap = 0;
+      wf.gather_slots = 0;
+      return st;
+    }
+    wf.gather_cap = cap;
+    wf.gather_slots = slots;
+  }
+  if (wf.probe_cap < records || !wf.probes.p) {
+    st = wf.probes.reserve(records * 80, "probe records");
+    if (st == PT_OK) st = wf.pc_pos.reserve(records * sizeof(float4), "compacted probes");
+    if (st == PT_OK) st = wf.pc_wl.reserve(records * sizeof(float4), "compacted probes");
+    if (st == PT_OK) st = wf.pc_nrm.reserve(records * sizeof(float4), "compacted probes");
+    if (st == PT_OK) st = wf.pc_tr.reserve(records * sizeof(float4), "compacted probes");
+    if (st != PT_OK) {
+      wf.probe_cap = 0;
+      return st;
+    }
+    wf.probe_cap = records;
+  }
+  return wf.pc_cnt.reserve(sets * 4, "probe counts");
+}
+
 }  // namespace pt
 
 using namespace pt;
@@ -817,15 +1217,36 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
   for (const MatDev& m : c.mats)
     if (m.type == MAT_DIFFUSE && c.lights.empty())
       return fail(PT_NOT_READY, "pt_render_frames: diffuse materials need at least one light (light_buffer is indexed unguarded by the diffuse shader)");
+  const bool sss = !c.trans_objs.empty();
+  if (sss && c.lights.empty())
+    return fail(PT_NOT_READY, "pt_render_frames: translucent objects need at least one light (the probe pass samples light_buffer)");
+  if (sss && c.integ.max_depth > 254)
+    return fail(PT_CAP_EXCEEDED, "pt_render_frames: translucent objects support max_depth <= 254 (the gather stack holds 255 entries)");
   if (c.dirty_materials) {
     PT_CHECK_CUDA(cudaMemcpyAsync(c.d_mats.p, c.mats.data(), c.mats.size() * sizeof(MatDev), cudaMemcpyHostToDevice, c.stream), "material upload");
+    PT_CHECK_CUDA(cudaMemcpyAsync(c.d_scat.p, c.scat.data(), c.scat.size() * sizeof(ScatDev), cudaMemcpyHostToDevice, c.stream),
+                  "scattering properties upload");
     c.dirty_materials = false;
   }
   const uint32_t pixels = c.cam.width * c.cam.height;
-  uint32_t frames_per_pass = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(n_frames, c.max_paths / pixels));
+  const uint32_t n_obj = (uint32_t)c.trans_objs.size();
+  const uint64_t per_frame_probes = (uint64_t)n_obj * c.probe_samples;
+  const uint32_t g_slots = sss ? (uint32_t)c.integ.max_depth + 1 : 0;
+  uint64_t max_paths = c.max_paths;
+  if (sss) {
+    // keep the gather stacks within 4 GiB by grouping fewer frames
+    uint64_t per_path = (uint64_t)g_slots * 40;
+    max_paths = std::min<uint64_t>(max_paths, std::max<uint64_t>(pixels, (4ull << 30) / per_path));
+  }
+  uint32_t frames_per_pass = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(n_frames, max_paths / pixels));
   uint64_t cap = (uint64_t)frames_per_pass * pixels;
   pt_status st = ensure_wavefront(c, cap);
   if (st != PT_OK) return st;
+  if (sss) {
+    // the stacks are indexed with the wavefront's capacity, which may exceed this call's `cap`
+    st = ensure_sss(c, c.wf.cap, g_slots, (uint64_t)frames_per_pass * per_frame_probes, (uint64_t)frames_per_pass * n_obj);
+    if (st != PT_OK) return st;
+  }
   // per-context geometric normals (computed once per build)
   DevBuf& geo = c.d_normals_geo;
   if (!geo.p || geo.bytes < (size_t)c.n_tris * sizeof(float4) || c.geo_stale) {
@@ -852,6 +1273,24 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
   w.sh_pid = wf.sh_pid.as<uint32_t>();
   w.cnt = wf.counters.as<uint32_t>();
   w.cap = wf.cap;
+  w.g_a = sss ? wf.g_a.as<float4>() : nullptr;
+  w.g_b = sss ? wf.g_b.as<float4>() : nullptr;
+  w.g_c = sss ? wf.g_c.as<float2>() : nullptr;
+  w.g_slots = sss ? g_slots : 0;
+  SssDev g;
+  memset(&g, 0, sizeof(g));
+  if (sss) {
+    g.objs = c.d_trans_objs.as<uint4>();
+    g.pos9 = c.d_trans_pos.as<float>();
+    g.n_obj = n_obj;
+    g.samples = c.probe_samples;
+    g.probes = wf.probes.as<float4>();
+    g.pc_pos = wf.pc_pos.as<float4>();
+    g.pc_wl = wf.pc_wl.as<float4>();
+    g.pc_nrm = wf.pc_nrm.as<float4>();
+    g.pc_tr = wf.pc_tr.as<float4>();
+    g.pc_cnt = wf.pc_cnt.as<uint32_t>();
+  }
   const float4* geo_p = geo.as<float4>();
   const int grid_trace = sm_count() * 8, grid_shade = sm_count() * 8;
   int occ_ext = 0, occ_sh = 0;
@@ -861,22 +1300,20 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
   PT_CHECK_CUDA(cudaMemsetAsync(w.cnt, 0, kCounters * 4, c.stream), "reset counters");
   c.prof_pairs = 0;
   PT_CHECK_CUDA(cudaEventRecord(c.ev0, c.stream), "event");
-  float extend_ms = 0.0f;
   uint32_t extend_launches = 0;
-  for (uint32_t f0 = 0; f0 < n_frames; f0 += frames_per_pass) {
-    uint32_t nf = std::min(frames_per_pass, n_frames - f0);
-    uint64_t n_paths = (uint64_t)nf * pixels;
+  auto reset_queues = [&]() -> pt_status {
     w.q_in = wf.q_a.as<uint32_t>();
     w.q_out = wf.q_b.as<uint32_t>();
     w.in_slot = CNT_ACTIVE_A;
     w.out_slot = CNT_ACTIVE_B;
-    PT_CHECK_CUDA(cudaMemsetAsync(w.cnt, 0, 8 * 4, c.stream), "reset queues");
-    k_raygen<<<grid_for(n_paths, kBlock, 16), kBlock, 0, c.stream>>>(S, w, first_frame + f0, n_paths, pixels);
-    count_launch();
+    PT_CHECK_CUDA(cudaMemsetAsync(w.cnt, 0, (CNT_FETCH_SH + 1) * 4, c.stream), "reset queues");
+    return PT_OK;
+  };
+  // max_depth + 2 bounces: every path has ended by then (each shader stops at max_depth).
+  auto bounces = [&]() -> pt_status {
     const int passes = c.integ.max_depth + 2;
     for (int b = 0; b < passes; ++b) {
-      PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_Q_MISS, 0, 6 * 4, c.stream), "reset queues");
-      PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_FETCH_EXT, 0, 2 * 4, c.stream), "reset fetch counters");
+      PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_Q_MISS, 0, (CNT_FETCH_SH - CNT_Q_MISS + 1) * 4, c.stream), "reset queues");
       PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + w.out_slot, 0, 4, c.stream), "reset queues");
       if (c.profile) {
         while (c.prof_events.size() < 2 * (size_t)(c.prof_pairs + 1)) {
@@ -899,17 +1336,54 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
       k_shade_diffuse<<<grid_shade, kBlock, 0, c.stream>>>(S, w, geo_p);
       k_shade_metal<<<grid_shade, kBlock, 0, c.stream>>>(S, w, geo_p);
       k_shade_glass<<<grid_shade, kBlock, 0, c.stream>>>(S, w, geo_p);
+      count_launch(6);
+      if (sss) {
+        k_shade_translucent<<<grid_shade, kBlock, 0, c.stream>>>(S, w, geo_p);
+        count_launch();
+      }
       if (c.opt.extend_mode == 1)
         k_shadow_persistent<<<grid_persist, kBlock, 0, c.stream>>>(S, w, c.opt.refill);
       else
         k_shadow<<<grid_trace, kBlock, 0, c.stream>>>(S, w);
-      count_launch(7);
+      count_launch();
       ++extend_launches;
       std::swap(w.q_in, w.q_out);
       std::swap(w.in_slot, w.out_slot);
     }
+    return PT_OK;
+  };
+  for (uint32_t f0 = 0; f0 < n_frames; f0 += frames_per_pass) {
+    uint32_t nf = std::min(frames_per_pass, n_frames - f0);
+    uint64_t n_paths = (uint64_t)nf * pixels;
+    if (sss) {
+      // probe pass of frames first_frame+f0 .. +nf-1, in groups of at most `cap` probes
+      const uint64_t n_probes = (uint64_t)nf * per_frame_probes;
+      for (uint64_t j0 = 0; j0 < n_probes; j0 += cap) {
+        uint64_t nj = std::min<uint64_t>(cap, n_probes - j0);
+        if ((st = reset_queues()) != PT_OK) return st;
+        k_probe_gen<<<grid_for(nj, kBlock, 16), kBlock, 0, c.stream>>>(S, w, g, first_frame + f0, j0, nj);
+        count_launch();
+        if ((st = bounces()) != PT_OK) return st;
+        k_probe_finish<<<grid_for(nj, kBlock, 16), kBlock, 0, c.stream>>>(w, g, j0, nj);
+        count_launch();
+      }
+      k_probe_compact<<<nf * n_obj, 256, 0, c.stream>>>(g);
+      count_launch();
+    }
+    if ((st = reset_queues()) != PT_OK) return st;
+    k_raygen<<<grid_for(n_paths, kBlock, 16), kBlock, 0, c.stream>>>(S, w, first_frame + f0, n_paths, pixels);
+    count_launch();
+    if ((st = bounces()) != PT_OK) return st;
+    if (sss) {
+      PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_GATHER, 0, 4, c.stream), "reset gather list");
+      uint32_t* list = wf.q_a.as<uint32_t>();
+      k_gather_collect<<<grid_for(n_paths, kBlock, 16), kBlock, 0, c.stream>>>(w, n_paths, list);
+      k_gather<<<grid_shade, kBlock, 0, c.stream>>>(S, w, g, list, pixels);
+      count_launch(2);
+    }
     k_accumulate<<<grid_for(pixels, kBlock, 16), kBlock, 0, c.stream>>>(S, w, c.d_accum.as<float4>(), first_frame + f0, nf, pixels);
     count_launch();
+    c.probe_last_frames = nf;
   }
   PT_CHECK_CUDA(cudaEventRecord(c.ev1, c.stream), "event");
   PT_CHECK_CUDA(cudaGetLastError(), "pt_render_frames launch");
@@ -924,8 +1398,26 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
   }
   c.stats.extend_launches = extend_launches;
   c.stats.kernel_launches = (uint32_t)(pt_kernel_launch_count() - launches0);
-  c.stats.extend_ms = extend_ms;
   c.stats_pending = true;
+  return PT_OK;
+}
+
+pt_status pt_get_probes(pt_ctx* ctx, void* out, uint64_t capacity, uint64_t* n_out)
+{
+  if (!ctx || !n_out) return fail(PT_INVALID_ARG, "pt_get_probes: null argument");
+  Context& c = ctx->c;
+  PT_CHECK_CUDA(cudaSetDevice(c.device), "cudaSetDevice");
+  const uint64_t per_frame = (uint64_t)c.trans_objs.size() * c.probe_samples;
+  if (c.probe_last_frames == 0 || per_frame == 0 || !c.wf.probes.p) {
+    *n_out = 0;
+    return PT_OK;
+  }
+  *n_out = per_frame;
+  uint64_t n = std::min(capacity, per_frame);
+  if (n && !out) return fail(PT_INVALID_ARG, "pt_get_probes: null output buffer");
+  const char* src = (const char*)c.wf.probes.p + (size_t)(c.probe_last_frames - 1) * per_frame * 80;
+  if (n) PT_CHECK_CUDA(cudaMemcpyAsync(out, src, (size_t)n * 80, cudaMemcpyDeviceToHost, c.stream), "pt_get_probes");
+  PT_CHECK_CUDA(cudaStreamSynchronize(c.stream), "pt_get_probes");
   return PT_OK;
 }
 
@@ -943,6 +1435,9 @@ pt_status pt_get_render_stats(pt_ctx* ctx, pt_render_stats* out)
     c.stats.shadow_rays = rd64(CNT_SHADOW_TOTAL);
     c.stats.capped_walks = rd64(CNT_CAPPED);
     c.stats.clamped_indices = rd64(CNT_CLAMPED);
+    c.stats.dipole_gathers = rd64(CNT_GATHERS);
+    c.stats.dipole_pairs = rd64(CNT_PAIRS);
+    c.stats.gather_overflows = rd64(CNT_ERROR);
     float ms = 0.0f;
     PT_CHECK_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1), "event time");
     c.stats.gpu_ms = ms;

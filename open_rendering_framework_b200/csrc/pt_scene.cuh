@@ -51,16 +51,27 @@ PT_HD int as_int(float f)
 constexpr uint32_t kLeafFlag = 0x80000000u;
 constexpr int kMaxDepth = 62;  // depth bound of the build; the traversal trail has 64 bits
 
-enum MatType : uint32_t { MAT_DIFFUSE = 0, MAT_ROUGH_GLASS = 3, MAT_METAL = 4, MAT_LIGHT = 100 };
+enum MatType : uint32_t { MAT_DIFFUSE = 0, MAT_ROUGH_GLASS = 3, MAT_METAL = 4, MAT_TRANSLUCENT = 5, MAT_LIGHT = 100 };
+enum DipoleModel : uint32_t { STANDARD_DIPOLE = 0, DIRECTIONAL_DIPOLE = 1 };
 
 // Material record, 16-byte aligned (128 B).
 struct __align__(16) MatDev {
-  uint32_t type, model, dist, pad;
+  uint32_t type, model, dist, aux;  // translucent: model = dipole_model, aux = translucent_index
   float4 a;   // diffuse: color.xyz | metal: roughness.xy | glass: ior, roughness | light: radiance.xyz
   float4 b;   // glass: absorption.xyz
   Cx3 eta;    // metal: 1 / ior (metallic_shader.cu:61), computed on the host
   Cx3 inv_eta;// metal: 1 / eta (the walk's inside branch)
 };
+
+// ScatteringMaterialProperties, structs.h:116-144 (260 bytes), one per material id (filled for
+// translucent materials).
+struct ScatDev {
+  float relative_ior;
+  float3 ior_real, ior_imag, absorption, scattering, meancosine, extinction, reducedExtinction, deltaEddExtinction, D, transport, C_phi,
+      C_phi_inv, C_E, A, albedo, reducedAlbedo, de, three_D, two_A_de, global_coeff, one_over_three_ext;
+  float mean_transport;
+};
+static_assert(sizeof(ScatDev) == 260, "ScatteringMaterialProperties layout");
 
 struct LightRaw { uint32_t type; float emitted[3]; float p[3]; float pad[3]; };  // structs.h:42-48 (40 B)
 struct TriLightRaw { float v0[3], v1[3], v2[3], n0[3], n1[3], n2[3]; uint32_t has_normals; float emission[3]; float area; };  // :96-103
@@ -102,6 +113,7 @@ struct SceneDev {
   const int4* tri_info;
   const float4* normals;
   const MatDev* mats;
+  const ScatDev* scat;  // per material id
   const LightRaw* lights;
   const TriLightRaw* tri_lights;
   int n_lights, n_tri_lights;

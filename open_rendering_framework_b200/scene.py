@@ -20,7 +20,9 @@ from . import _native as nat
 DIFFUSE_SHADER = 0
 ROUGH_TRANSPARENT_SHADER = 3
 METALLIC_SHADER = 4
+TRANSLUCENT_SHADER = 5
 AREA_LIGHT_MATERIAL = 100
+STANDARD_DIPOLE, DIRECTIONAL_DIPOLE = 0, 1
 WALTER_MODEL, VISIBLE_NORMALS_MODEL, MULTISCATTERING_MODEL = 0, 1, 2
 BECKMANN_DISTRIBUTION, GGX_DISTRIBUTION = 0, 1
 POINT_LIGHT, DIRECTIONAL_LIGHT, TRIANGLES_AREA_LIGHT, DISK_LIGHT, SPHERICAL_LIGHT = 0, 1, 2, 3, 4
@@ -44,10 +46,27 @@ class AreaLightParams(ctypes.Structure):
     _fields_ = [("radiance", ctypes.c_float * 3)]
 
 
+class TranslucentParams(ctypes.Structure):
+    _fields_ = [("scattering", ctypes.c_float * 3), ("absorption", ctypes.c_float * 3), ("meancosine", ctypes.c_float * 3),
+                ("ior", ctypes.c_float), ("scale", ctypes.c_float), ("dipole_model", ctypes.c_uint32)]
+
+
+# ScatteringMaterialProperties (structs.h:116-144, 260 bytes) and PositionSample (:105-114, 80 bytes).
+SCATTERING_PROPERTIES_DTYPE = np.dtype([(name, "<f4", 3) if name not in ("relative_ior", "mean_transport") else (name, "<f4")
+                                        for name in ("relative_ior", "ior_real", "ior_imag", "absorption", "scattering", "meancosine",
+                                                     "extinction", "reducedExtinction", "deltaEddExtinction", "D", "transport", "C_phi",
+                                                     "C_phi_inv", "C_E", "A", "albedo", "reducedAlbedo", "de", "three_D", "two_A_de",
+                                                     "global_coeff", "one_over_three_ext", "mean_transport")])
+POSITION_SAMPLE_DTYPE = np.dtype([("pos", "<f4", 3), ("dir", "<f4", 3), ("normal", "<f4", 3), ("L", "<f4", 3), ("transmitted", "<f4", 3),
+                                  ("weight", "<f4", 3), ("padding", "<f4", 2)])
+assert SCATTERING_PROPERTIES_DTYPE.itemsize == 260 and POSITION_SAMPLE_DTYPE.itemsize == 80
+
+
 class RenderStats(ctypes.Structure):
     _fields_ = [("path_samples", ctypes.c_uint64), ("segments", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
                 ("capped_walks", ctypes.c_uint64), ("clamped_indices", ctypes.c_uint64), ("gpu_ms", ctypes.c_float),
-                ("extend_ms", ctypes.c_float), ("extend_launches", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32)]
+                ("extend_ms", ctypes.c_float), ("extend_launches", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32),
+                ("dipole_gathers", ctypes.c_uint64), ("dipole_pairs", ctypes.c_uint64), ("gather_overflows", ctypes.c_uint64)]
 
 
 # LightStruct (40 B) and TriangleLight (92 B), structs.h:42-103, as numpy record types.
@@ -223,6 +242,44 @@ class RoughTransparentMaterial:
                                       self.normal_distribution)
 
 
+class TranslucentMaterial:
+    """Smooth translucent surface with the dipole BSSRDF (TranslucentMaterial.cpp, shader
+    subsurface_scattering_shader.cu).  Coefficients per RGB channel in 1/mm, scaled by `scale` to
+    scene units; defaults: the "Apple" entry of getDefaultMaterial (TranslucentMaterial.cpp:245-250),
+    scale 100, standard dipole (:7-19)."""
+    type = TRANSLUCENT_SHADER
+
+    def __init__(self, scattering=(2.29, 2.39, 1.97), absorption=(0.0030, 0.0034, 0.0046), meancosine=(0.0, 0.0, 0.0), ior=1.3,
+                 scale=100.0, dipole_model=STANDARD_DIPOLE):
+        self.scattering = tuple(float(x) for x in scattering)
+        self.absorption = tuple(float(x) for x in absorption)
+        self.meancosine = tuple(float(x) for x in meancosine)
+        self.ior = float(ior)
+        self.scale = float(scale)
+        self.dipole_model = int(dipole_model)
+
+    def params(self):
+        return TranslucentParams(_f3(self.scattering), _f3(self.absorption), _f3(self.meancosine), self.ior, self.scale, self.dipole_model)
+
+    def setIor(self, i):
+        self.ior = float(i)
+
+    def setScale(self, s):
+        self.scale = float(s)
+
+    def setAbsorption(self, a):
+        self.absorption = tuple(float(x) for x in a)
+
+    def setScattering(self, s):
+        self.scattering = tuple(float(x) for x in s)
+
+    def setMeanCosine(self, m):
+        self.meancosine = tuple(float(x) for x in m)
+
+    def setDipoleModel(self, m):
+        self.dipole_model = int(m)
+
+
 class AreaLightMaterial:
     """The emitter program TriangleAreaLight attaches to its geometry (arealight_shader.cu)."""
     type = AREA_LIGHT_MATERIAL
@@ -315,8 +372,9 @@ class SceneData:
     oracle both use: materials are numbered in order of first use (meshes first, then the emitter
     materials of TriangleAreaLights); triangles follow mesh order, then the lights' emitter meshes."""
 
-    def __init__(self, integrator, camera, background, meshes, lights):
+    def __init__(self, integrator, camera, background, meshes, lights, probe_samples=500):
         self.integrator, self.camera, self.background = integrator, camera, background
+        self.probe_samples = int(probe_samples)  # context["samples"] (OptixSceneLoader.cpp:11-17)
         self.lights = list(lights)
         self.meshes = list(meshes)
         for L in self.lights:
@@ -331,6 +389,16 @@ class SceneData:
                 self.materials.append(m.material)
             self.mesh_material.append(index[id(m.material)])
         self.light_buffer, self.triangle_light_buffer = light_buffers(self.lights)
+
+    def translucent_objects(self):
+        """(material index, first triangle, triangle count) of every mesh with a translucent material,
+        in mesh order (OptixSceneLoader::computeTranslucentGeometries)."""
+        out, first = [], 0
+        for m, mid in zip(self.meshes, self.mesh_material):
+            if getattr(m.material, "type", None) == TRANSLUCENT_SHADER:
+                out.append((mid, first, len(m.vindex)))
+            first += len(m.vindex)
+        return out
 
     @property
     def n_triangles(self):
@@ -377,6 +445,7 @@ class Renderer:
         self.apply_integrator()
         self.apply_camera()
         self.apply_background()
+        nat.call("pt_set_probe_count", self.ctx, data.probe_samples)
         for m, mid in zip(data.meshes, data.mesh_material):
             nn = 0 if m.normals is None else len(m.normals)
             first = ctypes.c_uint32()
@@ -414,6 +483,20 @@ class Renderer:
         out = [np.empty(H, np.float32), np.empty(H, np.float32), np.empty((H, W), np.float32), np.empty((H, W), np.float32)]
         nat.call("pt_get_envmap_tables", self.ctx, *[o.ctypes.data for o in out])
         return out
+
+    def probes(self):
+        """The PositionSample records of the last frame rendered (object-major)."""
+        n = ctypes.c_uint64()
+        nat.call("pt_get_probes", self.ctx, None, 0, ctypes.byref(n))
+        out = np.zeros(n.value, POSITION_SAMPLE_DTYPE)
+        if n.value:
+            nat.call("pt_get_probes", self.ctx, out.ctypes.data, n.value, ctypes.byref(n))
+        return out
+
+    def scattering_properties(self, mat):
+        out = np.zeros(1, SCATTERING_PROPERTIES_DTYPE)
+        nat.call("pt_get_scattering_properties", self.ctx, self.material_ids[id(mat)], out.ctypes.data)
+        return out[0]
 
     def renderScene(self):
         """One frame, as OptixScene::renderScene: frame++ and one integrator pass."""

@@ -126,3 +126,83 @@ def env_scene(width=256, height=256, env_w=256, env_h=128, metal_subdiv=3, glass
     meshes = [sc.Mesh(fp_, fi, floor), sc.Mesh(mp, mi, metal, mn, mni), sc.Mesh(gp, gi, glass, gn, gni)]
     lights = [sc.EnvMapLight()] if env_as_light else []
     return sc.SceneData(integrator, camera, background, meshes, lights)
+
+
+def value_noise3(p, seed, cells=4.0):
+    """Seeded 3-D value noise in [-1, 1]: random values on an integer lattice (cells per unit),
+    trilinearly interpolated with a smoothstep fade.  p: [N, 3]."""
+    rng = np.random.default_rng(seed)
+    n = 64
+    table = rng.uniform(-1.0, 1.0, size=(n, n, n))
+    q = (np.asarray(p, np.float64) + 8.0) * cells
+    i0 = np.floor(q).astype(np.int64)
+    f = q - i0
+    f = f * f * (3.0 - 2.0 * f)
+    out = np.zeros(len(q))
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                w = (f[:, 0] if dx else 1 - f[:, 0]) * (f[:, 1] if dy else 1 - f[:, 1]) * (f[:, 2] if dz else 1 - f[:, 2])
+                out += w * table[(i0[:, 0] + dx) % n, (i0[:, 1] + dy) % n, (i0[:, 2] + dz) % n]
+    return out
+
+
+def jittered_icosphere(subdiv, radius=1.0, center=(0.0, 0.0, 0.0), amplitude=0.02, seed=0):
+    """icosphere() with every vertex moved along its radius by value noise of the given relative
+    amplitude (2% of the radius by default); vertex normals are the area-weighted face normals."""
+    pos, vi, _, _ = icosphere(subdiv, 1.0)
+    d = pos.astype(np.float64)
+    r = 1.0 + amplitude * value_noise3(d, seed)
+    P = d * r[:, None] * radius + np.asarray(center, np.float64)
+    fn = np.cross(P[vi[:, 1]] - P[vi[:, 0]], P[vi[:, 2]] - P[vi[:, 0]])
+    N = np.zeros_like(P)
+    for k in range(3):
+        np.add.at(N, vi[:, k], fn)
+    N /= np.linalg.norm(N, axis=1, keepdims=True)
+    return P.astype(np.float32), vi, N.astype(np.float32), vi.copy()
+
+
+def dipole_coefficients(seed):
+    """Per-RGB reduced scattering sigma_s' ~ U[0.5, 3] /mm and absorption sigma_a ~ U[0.001, 0.05] /mm
+    (mean cosine 0, so sigma_s = sigma_s')."""
+    rng = np.random.default_rng(seed)
+    return tuple(rng.uniform(0.5, 3.0, 3)), tuple(rng.uniform(0.001, 0.05, 3))
+
+
+def subsurface_scene(width=1024, height=1024, subdiv=7, probe_samples=4096, env_w=2048, env_h=1024, seed=3, dipole_model=sc.STANDARD_DIPOLE,
+                     max_depth=8, scale=100.0):
+    """The subsurface configuration: a translucent icosphere subdivided `subdiv` times (7: 327,680
+    triangles), radius 0.5, vertices jittered by 2% value noise, dipole BSSRDF with seeded
+    coefficients in 1/mm and eta 1.3, scaled by `scale` (100: one scene unit is 100 mm, so the sphere
+    is 10 cm across), `probe_samples` probe points per frame; lit by the procedural sky (gradient
+    plus a Gaussian sun lobe of peak 5e4) as background and as the only light."""
+    integrator = sc.PathTracer(max_depth=max_depth, scene_epsilon=1e-4)
+    camera = sc.PinholeCamera(eye=(0.0, 0.35, 2.0), lookat=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0), vfov=36.0, width=width, height=height)
+    background = sc.EnvMapBackground(sky_envmap(env_w, env_h, sun_peak=5.0e4, sun_sigma_deg=1.0 if env_w >= 1024 else 6.0))
+    sigma_s, sigma_a = dipole_coefficients(seed)
+    mat = sc.TranslucentMaterial(scattering=sigma_s, absorption=sigma_a, meancosine=(0.0, 0.0, 0.0), ior=1.3, scale=scale,
+                                 dipole_model=dipole_model)
+    p, i, n, ni = jittered_icosphere(subdiv, 0.5, (0.0, 0.0, 0.0), 0.02, seed)
+    meshes = [sc.Mesh(p, i, mat, n, ni)]
+    return sc.SceneData(integrator, camera, background, meshes, [sc.EnvMapLight()], probe_samples=probe_samples)
+
+
+def translucent_box_scene(width=64, height=64, subdiv=3, probe_samples=64, dipole_model=sc.STANDARD_DIPOLE, max_depth=6, two_objects=False):
+    """A small closed scene for parity checks: the diffuse box, a translucent icosphere (and
+    optionally a second translucent object with its own material), a quad light."""
+    integrator = sc.PathTracer(max_depth=max_depth, scene_epsilon=1e-4)
+    camera = sc.PinholeCamera(eye=(0.0, 0.0, 0.9), lookat=(0.0, 0.0, -1.0), up=(0.0, 1.0, 0.0), vfov=60.0, width=width, height=height)
+    background = sc.ConstantBackground((0.0, 0.0, 0.0))
+    diffuse = sc.DiffuseMaterial((0.7, 0.7, 0.7))
+    skin = sc.TranslucentMaterial(scattering=(0.74, 0.88, 1.01), absorption=(0.032, 0.17, 0.48), ior=1.3, scale=10.0, dipole_model=dipole_model)
+    bp, bi = box()
+    p, i, n, ni = jittered_icosphere(subdiv, 0.35, (-0.2, -0.6, -0.2), 0.02, 1)
+    meshes = [sc.Mesh(bp, bi, diffuse), sc.Mesh(p, i, skin, n, ni)]
+    if two_objects:
+        marble = sc.TranslucentMaterial(scattering=(2.19, 2.62, 3.00), absorption=(0.0021, 0.0041, 0.0071), ior=1.5, scale=10.0,
+                                        dipole_model=dipole_model)
+        q, j, m, mj = icosphere(max(1, subdiv - 1), 0.25, (0.45, -0.7, 0.1))
+        meshes.append(sc.Mesh(q, j, marble, m, mj))
+    lp, li = quad_light((0.0, 0.99, 0.0), 0.5)
+    lights = [sc.TriangleAreaLight(lp, li, (15.0, 15.0, 15.0))]
+    return sc.SceneData(integrator, camera, background, meshes, lights, probe_samples=probe_samples)

@@ -177,7 +177,53 @@ def _trace_sigs(lib):
     _sig(lib, "orc_scene_set_env", None, [P, P, I, I])
     _sig(lib, "orc_env_tables", None, [P, P, P, P, P])
     _sig(lib, "orc_env_query", None, [P, P, L, P, P, L, P, P])
+    _sig(lib, "orc_scene_set_translucent", None, [P, U, P, U])
+    _sig(lib, "orc_scene_add_translucent_object", None, [P, U, U, U])
+    _sig(lib, "orc_scene_set_samples", None, [P, U])
+    _sig(lib, "orc_scene_probes", L, [P, P])
+    _sig(lib, "orc_compute_coefficients", None, [P, P, P, F, F, P])
+    _sig(lib, "orc_dipole_bssrdf", None, [P, F, P])
+    _sig(lib, "orc_dirpole_bssrdf", None, [P, P, P, P, P, P, P])
     lib._trace_bound = True
+
+
+def compute_coefficients(mat):
+    """TranslucentMaterial::computeCoefficients restated (260-byte ScatteringMaterialProperties)."""
+    lib = orc()
+    _trace_sigs(lib)
+    out = np.zeros(65, np.float32)
+    a = np.asarray(mat.absorption, np.float32)
+    s = np.asarray(mat.scattering, np.float32)
+    g = np.asarray(mat.meancosine, np.float32)
+    lib.orc_compute_coefficients(fp(a), fp(s), fp(g), mat.ior, mat.scale, fp(out))
+    return out
+
+
+def dipole_bssrdf(props, dist, which="orc"):
+    out = np.empty(3, np.float32)
+    props = np.ascontiguousarray(props, np.float32)
+    if which == "ref":
+        ref().ref_set_scattering_properties(fp(props), 260)
+        ref().ref_dipole_bssrdf(dist, fp(out))
+    else:
+        lib = orc()
+        _trace_sigs(lib)
+        lib.orc_dipole_bssrdf(fp(props), dist, fp(out))
+    return out
+
+
+def dirpole_bssrdf(props, xi, ni, w12, xo, no, which="orc"):
+    out = np.empty(3, np.float32)
+    props = np.ascontiguousarray(props, np.float32)
+    args = [np.ascontiguousarray(v, np.float32) for v in (xi, ni, w12, xo, no)]
+    if which == "ref":
+        ref().ref_set_scattering_properties(fp(props), 260)
+        ref().ref_dirpole_bssrdf(*[fp(a) for a in args], fp(out))
+    else:
+        lib = orc()
+        _trace_sigs(lib)
+        lib.orc_dirpole_bssrdf(fp(props), *[fp(a) for a in args], fp(out))
+    return out
 
 
 class OracleScene:
@@ -211,6 +257,8 @@ class OracleScene:
                 mab[k, 4:7] = m.glass_absorption
             elif name == "AreaLightMaterial":
                 mab[k, :3] = m.radiance
+            elif name == "TranslucentMaterial":
+                pass
             else:
                 raise TypeError(name)
         C = data.camera
@@ -226,6 +274,14 @@ class OracleScene:
                                       fp(mtype), fp(mmodel), fp(mdist), fp(mab), fp(mior), n_m,
                                       fp(lb) if len(lb) else None, len(lb), fp(tb) if len(tb) else None, len(tb),
                                       fp(cam), C.width, C.height, fp(patch), I_.max_depth, I_.scene_epsilon, I_.rr_start_depth, fp(bg))
+        for k, m in enumerate(data.materials):
+            if type(m).__name__ == "TranslucentMaterial":
+                props = compute_coefficients(m)
+                self._keep.append(props)
+                lib.orc_scene_set_translucent(self.h, k, fp(props), m.dipole_model)
+        for mid, first, n in data.translucent_objects():
+            lib.orc_scene_add_translucent_object(self.h, mid, first, n)
+        lib.orc_scene_set_samples(self.h, getattr(data, "probe_samples", 500))
         env = getattr(data.background, "rgba", None)
         if env is not None:
             env = np.ascontiguousarray(env, np.float32)
@@ -242,6 +298,14 @@ class OracleScene:
         self.lib.orc_render(self.h, first_frame, n_frames, p_begin, p_end, fp(pr) if pr is not None else None,
                             fp(accum) if accum is not None else None, threads)
         return accum, pr
+
+    def probes(self):
+        """PositionSample records of the last frame rendered, as raw float32 [n, 20]."""
+        n = self.lib.orc_scene_probes(self.h, None)
+        out = np.zeros((n, 20), np.float32)
+        if n:
+            self.lib.orc_scene_probes(self.h, fp(out))
+        return out
 
     def env_tables(self):
         H, W = self.data.background.rgba.shape[:2]

@@ -15,6 +15,7 @@
 #include <thread>
 #include <vector>
 
+#include "orc_dipole.hpp"
 #include "orc_light.hpp"
 #include "orc_math.hpp"
 #include "orc_microfacet.hpp"
@@ -27,12 +28,28 @@ namespace {
 
 typedef V3<float> F3;
 
-enum { MT_DIFFUSE = 0, MT_GLASS = 3, MT_METAL = 4, MT_LIGHT = 100 };
+enum { MT_DIFFUSE = 0, MT_GLASS = 3, MT_METAL = 4, MT_TRANSLUCENT = 5, MT_LIGHT = 100 };
+enum { STANDARD_DIPOLE = 0, DIRECTIONAL_DIPOLE = 1 };
 
 struct Mat {
   u32 type, model, dist;
   float a[4], b[4];
   Cx3 eta, inv_eta;
+  ScatProps props;       // translucent: scattering_properties
+  u32 dipole_model = 0;  // translucent: dipole_model
+  int translucent_index = -1;
+};
+
+// PositionSample, structs.h:105-114 (80 bytes).
+struct Probe {
+  F3 pos, dir, normal, L, transmitted, weight;
+  float pad[2];
+};
+static_assert(sizeof(Probe) == 80, "PositionSample layout");
+
+struct TranslucentObject {
+  int material;
+  unsigned first_tri, n_tris;
 };
 
 struct Tri {
@@ -41,6 +58,7 @@ struct Tri {
 
 struct Scene {
   std::vector<Tri> tris;
+  std::vector<float> pos9;     // vertex positions as given, 9 per triangle (the probe pass reads these)
   std::vector<int> info;       // 4 per triangle
   std::vector<F3> normals;
   std::vector<Mat> mats;
@@ -53,6 +71,10 @@ struct Scene {
   F3 bg;
   EnvMap env;
   std::vector<float> env_texels;
+  std::vector<TranslucentObject> translucent;
+  unsigned samples = 500;                // context["samples"] (OptixSceneLoader.cpp:11,17)
+  std::vector<Probe> probes;             // samples_output_buffer of the current frame
+  unsigned probe_frame = 0xffffffffu;
   bool env_present = false, env_is_light = false;
   // BVH
   struct Node { float lo[3], hi[3]; int left, right, first, count; };
@@ -227,6 +249,7 @@ struct PRD {
   int depth;
   u32 seed;
   Seed64 seed64;
+  bool probe_path = false;  // traced by the probe pass: translucent hits do not gather
 };
 
 static void trace(Scene& S, const F3& o, const F3& d, PRD& prd, LightSet& ls);
@@ -265,6 +288,7 @@ static void shade_diffuse(Scene& S, const Mat& m, const F3& o, const F3& d, cons
   if (xi < prob || forced) {
     F3 nd = sample_cosine_weighted<float>(ffnormal, t);
     PRD child;
+    child.probe_path = prd.probe_path;
     child.depth = prd.depth + 1;
     child.seed = t;
     child.seed64 = prd.seed64;
@@ -295,6 +319,7 @@ static void shade_metal(Scene& S, const Mat& m, const F3& o, const F3& d, const 
     F3 lwo = ms_conductor_sample<float>((int)m.dist, to_local(w_i, normal), wm, m.eta, m.inv_eta, a_x, a_y, seed, order, weight, 4096, &capped);
     F3 w_o = to_world(lwo, normal);
     PRD child;
+    child.probe_path = prd.probe_path;
     child.depth = prd.depth + 1;
     child.result = v3s(0.0f);
     child.seed = seed;
@@ -318,6 +343,7 @@ static void shade_metal(Scene& S, const Mat& m, const F3& o, const F3& d, const 
     F3 w_o = -w_i + 2.0f * mn * dot(w_i, mn);
     float abs_i_m = std::fabs(dot(w_i, mn)), abs_i_n = std::fabs(dot(w_i, ffnormal)), abs_n_m = std::fabs(dot(normal, mn));
     PRD child;
+    child.probe_path = prd.probe_path;
     child.depth = prd.depth + 1;
     child.result = v3s(0.0f);
     child.seed = seed;
@@ -362,6 +388,7 @@ static void shade_glass(Scene& S, const Mat& m, const F3& o, const F3& d, const 
     F3 lwo = ms_dielectric_sample<float>((int)m.dist, to_local(w_i, normal), 1.0f / ior, rough, rough, t, order, 4096, &capped);
     F3 w_o = to_world(lwo, normal);
     PRD child;
+    child.probe_path = prd.probe_path;
     child.depth = prd.depth + 1;
     child.result = v3s(0.0f);
     child.seed = t;
@@ -386,6 +413,7 @@ static void shade_glass(Scene& S, const Mat& m, const F3& o, const F3& d, const 
     float abs_i_m = std::fabs(dot(w_i, mn)), abs_i_n = std::fabs(dot(w_i, ffnormal)), abs_n_m = std::fabs(dot(normal, mn));
     float rr = rnd_tea(t);
     PRD child;
+    child.probe_path = prd.probe_path;
     child.depth = prd.depth + 1;
     child.result = v3s(0.0f);
     child.seed = t;
@@ -401,6 +429,167 @@ static void shade_glass(Scene& S, const Mat& m, const F3& o, const F3& d, const 
   }
   S.capped += capped;
   prd.result = result * beam_T;
+}
+
+// subsurface_scattering_shader.cu:324-470 (REFLECT, TRANSMIT and RND_64 defined).
+static void shade_translucent(Scene& S, const Mat& m, const F3& o, const F3& d, const HitRec& h, PRD& prd, LightSet& ls)
+{
+  prd.result = v3s(0.0f);
+  if (prd.depth > S.max_depth) return;
+  F3 no = shading_normal(S, h.prim, h.u, h.v);
+  F3 xo = o + h.t * d;
+  F3 wo = -d;
+  const ScatProps& P = m.props;
+  float recip_ior = 1.0f / P.relative_ior;
+  F3 beam_T = v3s(1.0f);
+  u32& t = prd.seed;
+  Seed64& t64 = prd.seed64;
+  float reflect_xi = rnd_accurate(t64);
+  float cos_theta_o = dot(wo, no);
+  bool inside = cos_theta_o < 0.0f;
+  if (inside) {
+    const F3& ext = (m.dipole_model == DIRECTIONAL_DIPOLE) ? P.deltaEddExtinction : P.extinction;
+    beam_T = vexp((-h.t) * ext);
+    float prob = (beam_T.x + beam_T.y + beam_T.z) / 3.0f;
+    if (rnd_accurate(t64) >= prob) return;
+    beam_T = beam_T / prob;
+    recip_ior = P.relative_ior;
+    no = -no;
+    cos_theta_o = -cos_theta_o;
+  }
+  float sin_theta_t_sqr = recip_ior * recip_ior * (1.0f - cos_theta_o * cos_theta_o);
+  float cos_theta_t = 1.0f, R = 1.0f;
+  if (sin_theta_t_sqr < 1.0f) {
+    cos_theta_t = std::sqrt(1.0f - sin_theta_t_sqr);
+    R = fresnel_R(cos_theta_o, cos_theta_t, recip_ior);
+  }
+  if (reflect_xi >= R) {
+    F3 wt = recip_ior * (cos_theta_o * no - wo) - no * cos_theta_t;
+    PRD child;
+    child.depth = prd.depth + 1;
+    child.seed64 = t64;
+    child.seed = t;
+    child.result = v3s(0.0f);
+    child.emit_light = 1;
+    child.probe_path = prd.probe_path;
+    trace(S, xo, wt, child, ls);
+    prd.result = prd.result + child.result;
+    t = child.seed;
+    t64 = child.seed64;
+    if (!inside && !prd.probe_path) {
+      float chosen = std::fmin(P.transport.x, std::fmin(P.transport.y, P.transport.z));
+      F3 acc = v3s(0.0f);
+      unsigned N = S.samples;
+      const Probe* pr = S.probes.data() + (size_t)m.translucent_index * N;
+      for (unsigned i = 0; i < N; ++i) {
+        const Probe& sm = pr[i];
+        if (dot(sm.L, sm.L) > 0.0f) {
+          float dist = length(xo - sm.pos);
+          float exp_term = std::exp(-dist * chosen);
+          float rnd_number = rnd_accurate(t64);
+          if (rnd_number < exp_term) {
+            if (m.dipole_model == DIRECTIONAL_DIPOLE)
+              acc = acc + sm.weight * sm.L * dirpole_bssrdf(sm.pos, sm.normal, sm.transmitted, xo, no, P) / exp_term;
+            else
+              acc = acc + sm.weight * sm.L * dipole_bssrdf(dist, P) / exp_term;
+          }
+        }
+      }
+      prd.result = prd.result + acc * P.global_coeff / (float)N;
+    }
+  }
+  if (reflect_xi < R) {
+    F3 wr = 2.0f * cos_theta_o * no - wo;
+    PRD child;
+    child.depth = prd.depth + 1;
+    child.seed = t;
+    child.seed64 = t64;
+    child.result = v3s(0.0f);
+    child.emit_light = 1;
+    child.probe_path = prd.probe_path;
+    trace(S, xo, wr, child, ls);
+    prd.result = prd.result + child.result;
+    t = child.seed;
+    t64 = child.seed64;
+  }
+  prd.result = prd.result * beam_T;
+}
+
+// sample_camera.cu:48-268 for a smooth translucent object (GLOBAL and RND_64 defined): one
+// PositionSample per launch index of the probe pass of translucent object k.
+static Probe make_probe(Scene& S, unsigned k, unsigned i, unsigned frame, LightSet& ls)
+{
+  const TranslucentObject& T = S.translucent[k];
+  const Mat& m = S.mats[T.material];
+  unsigned idx = i + k * S.samples;
+  Probe sm;
+  memset(&sm, 0, sizeof(sm));
+  u32 triangles = T.n_tris;
+  u32 t = tea<16>(idx, frame);
+  u32 s2 = tea<16>(idx, frame);
+  Seed64 t64 = {s2, s2};
+  u32 tid = (u32)(int)(rnd_accurate(t64) * (float)triangles);
+  if (tid >= triangles) { tid = triangles - 1; ++ls.oob; }
+  unsigned prim = T.first_tri + tid;
+  const float* pv = &S.pos9[9 * (size_t)prim];
+  F3 v0 = v3(pv[0], pv[1], pv[2]), v1 = v3(pv[3], pv[4], pv[5]), v2 = v3(pv[6], pv[7], pv[8]);
+  F3 perp = cross(v1 - v0, v2 - v0);
+  float area = 0.5f * length(perp);
+  float xi1 = std::sqrt(rnd_accurate(t64));
+  float xi2 = rnd_accurate(t64);
+  float u = 1.0f - xi1, v = (1.0f - xi2) * xi1, w = xi1 * xi2;
+  sm.pos = u * v0 + v * v1 + w * v2;
+  const int* in = &S.info[4 * (size_t)prim];
+  F3 n;
+  if (in[0] >= 0) {
+    n = normalize(u * S.normals[in[0]] + v * S.normals[in[1]] + w * S.normals[in[2]]);
+    n = normalize(n);
+  } else {
+    n = normalize(perp);
+  }
+  sm.normal = n;
+  float recip_ior = 1.0f / m.props.relative_ior;
+  F3 Le, w_i;
+  if (rnd(t) < 0.5f) {
+    u32 li = (u32)((float)ls.n_lights * rnd_accurate(t64));
+    if ((long)li >= ls.n_lights) { li = (u32)(ls.n_lights - 1); ++ls.oob; }
+    float light_pdf = 1.0f / (float)ls.n_lights;
+    float r = 0.0f;
+    Le = v3s(0.0f);
+    w_i = v3s(0.0f);
+    eval_direct<float>(sm.pos, ls.lights[li], ls, w_i, Le, r, t);
+    sm.dir = w_i;
+    float cos_theta_i = std::fmax(dot(w_i, n), 0.0f);
+    if (cos_theta_i > 0.0f) {
+      float att = occluded(S, sm.pos, w_i, S.eps, r) ? 0.0f : 1.0f;
+      Le = Le * (att * cos_theta_i / light_pdf);
+    } else {
+      Le = v3s(0.0f);
+    }
+  } else {
+    w_i = sample_cosine_weighted<float>(n, t);
+    PRD pn;
+    pn.depth = 0;
+    pn.seed = t;
+    pn.seed64 = t64;
+    pn.result = v3s(0.0f);
+    pn.emit_light = 1;
+    pn.probe_path = true;
+    trace(S, sm.pos, w_i, pn, ls);
+    t = pn.seed;
+    t64 = pn.seed64;
+    Le = pn.result * K<float>::PI;
+  }
+  Le = Le / 0.5f;
+  float cos_theta_i = std::fmax(dot(w_i, sm.normal), 0.0f);
+  float cos_i2 = cos_theta_i * cos_theta_i;
+  float sin_t2 = recip_ior * recip_ior * (1.0f - cos_i2);
+  float cos_t = std::sqrt(1.0f - sin_t2);
+  sm.transmitted = recip_ior * (cos_theta_i * sm.normal - w_i) - sm.normal * cos_t;
+  float T12 = 1.0f - fresnel_R(cos_theta_i, cos_t, recip_ior);
+  sm.weight = v3s(T12);
+  sm.L = Le * ((float)triangles * area);
+  return sm;
 }
 
 static void trace(Scene& S, const F3& o, const F3& d, PRD& prd, LightSet& ls)
@@ -427,6 +616,7 @@ static void trace(Scene& S, const F3& o, const F3& d, PRD& prd, LightSet& ls)
     case MT_DIFFUSE: shade_diffuse(S, m, o, d, h, prd, ls); return;
     case MT_METAL: shade_metal(S, m, o, d, h, prd, ls); return;
     case MT_GLASS: shade_glass(S, m, o, d, h, prd, ls); return;
+    case MT_TRANSLUCENT: shade_translucent(S, m, o, d, h, prd, ls); return;
     default: prd.result = v3s(0.0f); return;
   }
 }
@@ -441,6 +631,7 @@ EXPORT void* orc_scene_create(const float* tri_pos, const int* tri_info, unsigne
                               int max_depth, float eps, int rr_start, const float* bg3)
 {
   Scene* S = new Scene();
+  S->pos9.assign(tri_pos, tri_pos + 9 * (size_t)n_tris);
   S->tris.resize(n_tris);
   for (unsigned i = 0; i < n_tris; ++i) {
     const float* p = tri_pos + 9 * (size_t)i;
@@ -450,8 +641,7 @@ EXPORT void* orc_scene_create(const float* tri_pos, const int* tri_info, unsigne
   S->info.assign(tri_info, tri_info + 4 * (size_t)n_tris);
   for (unsigned k = 0; k < n_normals; ++k) S->normals.push_back(v3(normals[3 * k], normals[3 * k + 1], normals[3 * k + 2]));
   for (unsigned k = 0; k < n_mats; ++k) {
-    Mat m;
-    memset(&m, 0, sizeof(m));
+    Mat m = Mat();  // zero-initialised, then the member defaults
     m.type = mat_type[k];
     m.model = mat_model[k];
     m.dist = mat_dist[k];
@@ -527,9 +717,11 @@ EXPORT void orc_env_query(void* s, const float* dirs3, long n_dirs, float* looke
 }
 
 // Renders frames [first_frame, first_frame + n_frames) for pixels [p_begin, p_end) with `threads`
-// host threads.  path_rad (optional): radiance of every path, [frame][pixel][3] over the pixel
-// range.  accum (optional): the float4 running mean over the full image, updated in frame order as
-// path_tracer.cu:64-68.  The light arrays passed to orc_scene_create must outlive the scene.
+// host threads, frame by frame: the probe pass of every translucent object (sample_camera.cu) and
+// then the integrator pass (path_tracer.cu), as OptixScene::renderScene launches them
+// (OptixScene.cpp:146-159).  path_rad (optional): radiance of every path, [frame][pixel][3] over the
+// pixel range.  accum (optional): the float4 running mean over the full image (path_tracer.cu:64-68).
+// The light arrays passed to orc_scene_create must outlive the scene.
 EXPORT long orc_render(void* scene, unsigned first_frame, unsigned n_frames, unsigned p_begin, unsigned p_end, float* path_rad, float* accum,
                        int threads)
 {
@@ -537,70 +729,123 @@ EXPORT long orc_render(void* scene, unsigned first_frame, unsigned n_frames, uns
   const unsigned W = S.width, H = S.height;
   p_end = std::min(p_end, W * H);
   if (p_begin >= p_end) return 0;
-  std::atomic<unsigned> next(p_begin);
-  std::atomic<long> oob(0);
-  auto worker = [&]() {
-    LightSet ls = S.lights;
-    ls.env = S.env_present ? &S.env : nullptr;
-    ls.oob = 0;
-    for (;;) {
-      unsigned p0 = next.fetch_add(64);
-      if (p0 >= p_end) break;
-      unsigned p1 = std::min(p_end, p0 + 64);
-      for (unsigned p = p0; p < p1; ++p) {
-        unsigned x = p % W, y = p / W;
-        bool inside = !(x < S.po_x || x > S.po_x + S.pd_x || y < S.po_y || y > S.po_y + S.pd_y);
-        float out[4];
-        if (accum) memcpy(out, accum + 4 * (size_t)p, 16);
-        for (unsigned fl = 0; fl < n_frames; ++fl) {
-          unsigned frame = first_frame + fl;
-          F3 result = v3s(0.0f);
-          if (inside) {
-            PRD prd;
-            prd.emit_light = 1;
-            prd.depth = 0;
-            prd.seed = tea<16>(W * y + x, frame);
-            u32 s2 = tea<16>(W * y + x, frame);
-            prd.seed64 = {s2, s2};
-            float jx = rnd_tea(prd.seed), jy = rnd_tea(prd.seed);
-            float ipx = ((float)x + jx) / (float)W * 2.0f - 1.0f;
-            float ipy = ((float)y + jy) / (float)H * 2.0f - 1.0f;
-            F3 dir = normalize(ipx * S.U + ipy * S.V + S.W);
-            prd.result = v3s(0.0f);
-            trace(S, S.eye, dir, prd, ls);
-            result = result + prd.result;
-          }
-          if (path_rad) {
-            float* pr = path_rad + 3 * ((size_t)fl * (p_end - p_begin) + (p - p_begin));
-            pr[0] = result.x; pr[1] = result.y; pr[2] = result.z;
-          }
-          if (accum) {
-            if (!inside) {
-              out[0] = out[1] = out[2] = 0.0f;
-              out[3] = 1.0f;
-            } else if (std::isfinite(result.x) && std::isfinite(result.y) && std::isfinite(result.z)) {
-              float cur[4] = {0, 0, 0, 0};
-              if (frame != 0)
-                for (int k = 0; k < 4; ++k) cur[k] = out[k] * (float)frame;
-              float den = (float)(frame + 1);
-              out[0] = (result.x + cur[0]) / den;
-              out[1] = (result.y + cur[1]) / den;
-              out[2] = (result.z + cur[2]) / den;
-              out[3] = (1.0f + cur[3]) / den;
-            }
-          }
-        }
-        if (accum) memcpy(accum + 4 * (size_t)p, out, 16);
-      }
-    }
-    oob += ls.oob;
-  };
   threads = std::max(1, threads);
-  std::vector<std::thread> th;
-  for (int i = 1; i < threads; ++i) th.emplace_back(worker);
-  worker();
-  for (auto& t : th) t.join();
+  std::atomic<long> oob(0);
+  auto parallel = [&](unsigned count, unsigned chunk, auto&& body) {
+    std::atomic<unsigned> next(0);
+    auto worker = [&]() {
+      LightSet ls = S.lights;
+      ls.env = S.env_present ? &S.env : nullptr;
+      ls.oob = 0;
+      for (;;) {
+        unsigned b = next.fetch_add(chunk);
+        if (b >= count) break;
+        unsigned e = std::min(count, b + chunk);
+        for (unsigned k = b; k < e; ++k) body(k, ls);
+      }
+      oob += ls.oob;
+    };
+    std::vector<std::thread> th;
+    for (int i = 1; i < threads; ++i) th.emplace_back(worker);
+    worker();
+    for (auto& x : th) x.join();
+  };
+  for (unsigned fl = 0; fl < n_frames; ++fl) {
+    const unsigned frame = first_frame + fl;
+    if (!S.translucent.empty()) {
+      S.probes.assign((size_t)S.samples * S.translucent.size(), Probe());
+      unsigned total = S.samples * (unsigned)S.translucent.size();
+      parallel(total, 16, [&](unsigned j, LightSet& ls) { S.probes[j] = make_probe(S, j / S.samples, j % S.samples, frame, ls); });
+      S.probe_frame = frame;
+    }
+    parallel(p_end - p_begin, 64, [&](unsigned k, LightSet& ls) {
+      unsigned p = p_begin + k;
+      unsigned x = p % W, y = p / W;
+      bool inside = !(x < S.po_x || x > S.po_x + S.pd_x || y < S.po_y || y > S.po_y + S.pd_y);
+      F3 result = v3s(0.0f);
+      if (inside) {
+        PRD prd;
+        prd.emit_light = 1;
+        prd.depth = 0;
+        prd.seed = tea<16>(W * y + x, frame);
+        u32 s2 = tea<16>(W * y + x, frame);
+        prd.seed64 = {s2, s2};
+        float jx = rnd_tea(prd.seed), jy = rnd_tea(prd.seed);
+        float ipx = ((float)x + jx) / (float)W * 2.0f - 1.0f;
+        float ipy = ((float)y + jy) / (float)H * 2.0f - 1.0f;
+        F3 dir = normalize(ipx * S.U + ipy * S.V + S.W);
+        prd.result = v3s(0.0f);
+        trace(S, S.eye, dir, prd, ls);
+        result = result + prd.result;
+      }
+      if (path_rad) {
+        float* pr = path_rad + 3 * ((size_t)fl * (p_end - p_begin) + k);
+        pr[0] = result.x; pr[1] = result.y; pr[2] = result.z;
+      }
+      if (accum) {
+        float* out = accum + 4 * (size_t)p;
+        if (!inside) {
+          out[0] = out[1] = out[2] = 0.0f;
+          out[3] = 1.0f;
+        } else if (std::isfinite(result.x) && std::isfinite(result.y) && std::isfinite(result.z)) {
+          float cur[4] = {0, 0, 0, 0};
+          if (frame != 0)
+            for (int q = 0; q < 4; ++q) cur[q] = out[q] * (float)frame;
+          float den = (float)(frame + 1);
+          out[0] = (result.x + cur[0]) / den;
+          out[1] = (result.y + cur[1]) / den;
+          out[2] = (result.z + cur[2]) / den;
+          out[3] = (1.0f + cur[3]) / den;
+        }
+      }
+    });
+  }
   return oob.load();
+}
+
+// Translucent material `mat` (scattering_properties as the 260-byte ScatteringMaterialProperties and
+// dipole_model) and the translucent objects: meshes [first_tri, first_tri + n_tris) with their probe
+// sets in object order (translucent_index).
+EXPORT void orc_scene_set_translucent(void* s, unsigned mat, const void* props260, unsigned dipole_model)
+{
+  Scene& S = *(Scene*)s;
+  memcpy(&S.mats[mat].props, props260, sizeof(ScatProps));
+  S.mats[mat].dipole_model = dipole_model;
+}
+EXPORT void orc_scene_add_translucent_object(void* s, unsigned mat, unsigned first_tri, unsigned n_tris)
+{
+  Scene& S = *(Scene*)s;
+  S.mats[mat].translucent_index = (int)S.translucent.size();
+  S.translucent.push_back({(int)mat, first_tri, n_tris});
+}
+EXPORT void orc_scene_set_samples(void* s, unsigned n) { ((Scene*)s)->samples = n; }
+// The probes of the most recent frame rendered (PositionSample records, 80 bytes each).
+EXPORT long orc_scene_probes(void* s, void* out)
+{
+  Scene& S = *(Scene*)s;
+  if (out) memcpy(out, S.probes.data(), S.probes.size() * sizeof(Probe));
+  return (long)S.probes.size();
+}
+EXPORT void orc_compute_coefficients(const float* absorption, const float* scattering, const float* meancosine, float ior, float scale,
+                                     void* out260)
+{
+  ScatProps p = compute_coefficients(absorption, scattering, meancosine, ior, scale);
+  memcpy(out260, &p, sizeof(p));
+}
+EXPORT void orc_dipole_bssrdf(const void* props260, float dist, float* out3)
+{
+  ScatProps P;
+  memcpy(&P, props260, sizeof(P));
+  F3 r = dipole_bssrdf(dist, P);
+  out3[0] = r.x; out3[1] = r.y; out3[2] = r.z;
+}
+EXPORT void orc_dirpole_bssrdf(const void* props260, const float* xi, const float* ni, const float* w12, const float* xo, const float* no, float* out3)
+{
+  ScatProps P;
+  memcpy(&P, props260, sizeof(P));
+  F3 r = dirpole_bssrdf(v3(xi[0], xi[1], xi[2]), v3(ni[0], ni[1], ni[2]), v3(w12[0], w12[1], w12[2]), v3(xo[0], xo[1], xo[2]),
+                        v3(no[0], no[1], no[2]), P);
+  out3[0] = r.x; out3[1] = r.y; out3[2] = r.z;
 }
 
 EXPORT long orc_capped(void* scene) { return ((Scene*)scene)->capped.load(); }

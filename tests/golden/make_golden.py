@@ -141,6 +141,32 @@ def main():
     g.update(env_map=env, env_mpdf=mp, env_mcdf=mc, env_cpdf=cp, env_ccdf=cc, env_dirs=dirs, env_looked=looked, env_seeds=seeds,
              env_sdir=sdir, env_sL=sL, env_sfin=sfin)
 
+    # Dipole BSSRDFs (dipoles/standard_dipole.h, dipoles/directional_dipole.h) on scattering
+    # properties from the restatement of TranslucentMaterial::computeCoefficients (that file needs Qt
+    # and is not compiled; the derived properties are pinned by the dipoles' outputs).
+    from open_rendering_framework_b200 import scene as sc
+
+    r2 = np.random.default_rng(20261204)
+    props = []
+    for seed in range(4):
+        s_, a_ = scenes.dipole_coefficients(seed)
+        props.append(oc.compute_coefficients(sc.TranslucentMaterial(scattering=s_, absorption=a_, ior=1.3 + 0.1 * seed, scale=100.0)))
+    props = np.stack(props)
+    nd = 256
+    dist = r2.uniform(0.0, 0.5, nd).astype(np.float32)
+    dist[:8] = 0.0
+    dp = np.empty((4, nd, 3), np.float32)
+    xi = (r2.normal(size=(nd, 3)) * 0.3).astype(np.float32)
+    xo = (r2.normal(size=(nd, 3)) * 0.3).astype(np.float32)
+    xo[:4] = xi[:4]
+    ni, no, w12 = unit_vectors(r2, nd, False), unit_vectors(r2, nd, False), unit_vectors(r2, nd, False)
+    dd = np.empty((4, nd, 3), np.float32)
+    for k in range(4):
+        for j in range(nd):
+            dp[k, j] = oc.dipole_bssrdf(props[k], dist[j], which="ref")
+            dd[k, j] = oc.dirpole_bssrdf(props[k], xi[j], ni[j], w12[j], xo[j], no[j], which="ref")
+    g.update(dip_props=props, dip_dist=dist, dip_std=dp, dip_xi=xi, dip_xo=xo, dip_ni=ni, dip_no=no, dip_w12=w12, dip_dir=dd)
+
     np.savez_compressed(OUT, **g)
     print("wrote", OUT, os.path.getsize(OUT), "bytes")
 

@@ -171,3 +171,65 @@ def test_env_tables_are_valid_distributions():
     # marginal pdf integrates to 1 over rows, each conditional pdf to 1 over its row
     assert abs(mp.mean() - 1.0) < 1e-4
     assert np.allclose(cp.mean(axis=1), 1.0, atol=1e-4)
+
+
+def test_dipoles_golden():
+    """Standard and directional dipole of the restatement against the reference's outputs."""
+    P = GOLD["dip_props"]
+    for k in range(P.shape[0]):
+        for j in range(GOLD["dip_dist"].size):
+            assert bits_equal(oc.dipole_bssrdf(P[k], GOLD["dip_dist"][j]), GOLD["dip_std"][k, j]), (k, j)
+            got = oc.dirpole_bssrdf(P[k], GOLD["dip_xi"][j], GOLD["dip_ni"][j], GOLD["dip_w12"][j], GOLD["dip_xo"][j], GOLD["dip_no"][j])
+            assert bits_equal(got, GOLD["dip_dir"][k, j]), (k, j)
+
+
+def test_scattering_properties_derivation():
+    """computeCoefficients restated: the fixture's properties are reproduced bit for bit and obey
+    the definitions (D = 1/(3 sigma_t'), sigma_tr = sqrt(sigma_a / D), A = (1 - C_E) / (2 C_phi))."""
+    from open_rendering_framework_b200 import scene as sc, scenes
+
+    for seed in range(4):
+        s_, a_ = scenes.dipole_coefficients(seed)
+        p = oc.compute_coefficients(sc.TranslucentMaterial(scattering=s_, absorption=a_, ior=1.3 + 0.1 * seed, scale=100.0))
+        assert bits_equal(p, GOLD["dip_props"][seed])
+        rec = p.view(sc.SCATTERING_PROPERTIES_DTYPE)[0]
+        np.testing.assert_allclose(rec["D"], 1.0 / (3.0 * rec["reducedExtinction"]), rtol=1e-6)
+        np.testing.assert_allclose(rec["transport"], np.sqrt(rec["absorption"] / rec["D"]), rtol=1e-6)
+        np.testing.assert_allclose(rec["A"], (1.0 - rec["C_E"]) / (2.0 * rec["C_phi"]), rtol=1e-6)
+        np.testing.assert_allclose(rec["absorption"], np.float32(a_) * np.float32(100.0), rtol=1e-7)
+
+
+@pytest.mark.skipif(oc.ref() is None, reason="compiled reference (oracle/_ref) not built")
+def test_fresh_dipoles_against_compiled_reference():
+    from open_rendering_framework_b200 import scene as sc, scenes
+
+    rng = np.random.default_rng(11)
+    for seed in (5, 6):
+        s_, a_ = scenes.dipole_coefficients(seed)
+        P = oc.compute_coefficients(sc.TranslucentMaterial(scattering=s_, absorption=a_, meancosine=(0.3, 0.2, 0.1), ior=1.4, scale=30.0))
+        for _ in range(500):
+            d = np.float32(rng.uniform(0.0, 1.0))
+            assert bits_equal(oc.dipole_bssrdf(P, d), oc.dipole_bssrdf(P, d, which="ref"))
+            v = [rng.normal(size=3).astype(np.float32) for _ in range(5)]
+            args = (v[0] * 0.2, v[1] / np.linalg.norm(v[1]), v[2] / np.linalg.norm(v[2]), v[3] * 0.2, v[4] / np.linalg.norm(v[4]))
+            assert bits_equal(oc.dirpole_bssrdf(P, *args), oc.dirpole_bssrdf(P, *args, which="ref"))
+
+
+def test_translucent_oracle_is_deterministic_and_well_formed():
+    """The CPU restatement's probe pass and gathers give the same probes and image whatever the
+    thread count (probe paths never read the probe set being built), and the probes are sane:
+    unit normals, 0 <= T12 <= 1, L >= 0."""
+    from open_rendering_framework_b200 import scenes
+
+    data = scenes.translucent_box_scene(24, 24, subdiv=2, probe_samples=48, two_objects=True)
+    out = []
+    for threads in (1, 6):
+        O = oc.OracleScene(data)
+        acc, _ = O.render(0, 2, accum=np.zeros((24, 24, 4), np.float32), threads=threads)
+        out.append((acc, O.probes()))
+    assert bits_equal(out[0][0], out[1][0]) and bits_equal(out[0][1], out[1][1])
+    pr = out[0][1]
+    assert pr.shape == (96, 20)
+    np.testing.assert_allclose(np.linalg.norm(pr[:, 6:9], axis=1), 1.0, atol=1e-5)
+    assert np.all((pr[:, 15:18] >= 0) & (pr[:, 15:18] <= 1)) and np.all(pr[:, 9:12] >= 0)
+    assert np.any(pr[:, 9:12] > 0)
