@@ -1,9 +1,17 @@
 """Benchmark: Mpath-samples/s of the single-scene wavefront render on one B200 (per GPU replica).
 
-Workload (one step): 512 x 512 pixels x 64 camera samples (frames) of the procedural single scene
-(box of 12 diffuse triangles, 81,920-triangle GGX conductor icosphere, 20,480-triangle Beckmann
-dielectric icosphere, 0.25 x 0.25 quad light of radiance 15), max depth 8, Russian roulette from
-depth 3 -- 16,777,216 path samples per step, traced as one wavefront launch group.
+Workload (one step, default --workload single_scene): 512 x 512 pixels x 64 camera samples (frames)
+of the procedural single scene (box of 12 diffuse triangles, 81,920-triangle GGX conductor
+icosphere, 20,480-triangle Beckmann dielectric icosphere, 0.25 x 0.25 quad light of radiance 15),
+max depth 8, Russian roulette from depth 3 -- 16,777,216 path samples per step, traced as one
+wavefront launch group.
+
+--workload subsurface: 1024 x 1024 pixels x 256 frames (--spp) of the translucent scene: a
+327,680-triangle jittered icosphere with the dipole BSSRDF (standard; --dipole directional), 4,096
+probes per frame (2^20 over the 256 frames), lit by a 2048 x 1024 procedural sky with a sun lobe of
+peak 5e4 as background and light.  Its dominant kernel is the dipole gather, which is bound by
+integer issue (one MD5 hash per (gather, probe) pair), so its line reports pair evaluations per
+second instead of a memory roofline.
 
 Arms
   --impl ours (default): the CUDA path through the C ABI.  `value` is device-timed (CUDA events
@@ -37,6 +45,7 @@ UNIT = "Mpath-samples/s"
 WORKLOAD = ("single-scene render 512x512, 64 spp, max depth 8, Russian roulette from depth 3: 12-triangle diffuse box, "
             "81,920-triangle GGX conductor icosphere, 20,480-triangle Beckmann rough-dielectric icosphere, quad light")
 EXTEND_BYTES_PER_SEGMENT = 56  # queue id 4 + ray 32 + hit record 16 + material-queue append 4
+GATHER_INSTR_PER_PAIR = 256    # thread instructions per (gather, probe) pair of k_gather, from its ncu capture
 
 
 def parse():
@@ -45,11 +54,36 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--spp", type=int, default=64)
-    ap.add_argument("--width", type=int, default=512)
-    ap.add_argument("--height", type=int, default=512)
+    ap.add_argument("--workload", default="single_scene", choices=["single_scene", "subsurface"])
+    ap.add_argument("--spp", type=int, default=None, help="frames per step (default 64, subsurface 256)")
+    ap.add_argument("--width", type=int, default=None)
+    ap.add_argument("--height", type=int, default=None)
+    ap.add_argument("--dipole", default="standard", choices=["standard", "directional"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
+
+
+SUBSURFACE = ("subsurface render 1024x1024, 256 spp, max depth 8: 327,680-triangle icosphere jittered by 2%% value noise, %s dipole "
+              "BSSRDF with seeded sigma_s' ~ U[0.5,3]/mm and sigma_a ~ U[0.001,0.05]/mm per RGB, eta 1.3, 4,096 probes per frame "
+              "(2^20 over 256 frames); 2048x1024 procedural sky + Gaussian sun lobe (peak 5e4) as background and importance-sampled light")
+
+
+def workload(args):
+    """(scene data, frames per step, description) of the selected workload."""
+    from open_rendering_framework_b200 import scene as sc
+    from open_rendering_framework_b200 import scenes
+
+    if args.workload == "subsurface":
+        w, h = args.width or 1024, args.height or 1024
+        model = sc.DIRECTIONAL_DIPOLE if args.dipole == "directional" else sc.STANDARD_DIPOLE
+        data = scenes.subsurface_scene(w, h, subdiv=7, probe_samples=4096, env_w=2048, env_h=1024, dipole_model=model)
+        desc = SUBSURFACE % args.dipole
+        if (w, h) != (1024, 1024):
+            desc += " (resized to %dx%d)" % (w, h)
+        return data, args.spp or 256, desc
+    w, h = args.width or 512, args.height or 512
+    desc = WORKLOAD if (w, h) == (512, 512) else WORKLOAD + " (resized to %dx%d)" % (w, h)
+    return scenes.single_scene(width=w, height=h), args.spp or 64, desc
 
 
 def load_peaks():
@@ -147,12 +181,15 @@ def cpu_baseline_sample(data, target_s=12.0, threads=None):
     W = data.camera.width
     # calibrate on a small band, then size the sample for ~target_s seconds
     rows = 4
+    mid = data.camera.height // 2 - rows // 2
     t0 = time.perf_counter()
-    O.render(0, 1, p_begin=W * 254, p_end=W * (254 + rows), threads=threads)
+    O.render(0, 1, p_begin=W * mid, p_end=W * (mid + rows), threads=threads)
     dt = max(time.perf_counter() - t0, 1e-3)
     rate = rows * W / dt
     n_paths = int(min(max(rate * target_s, W), W * data.camera.height * 64))
     frames = max(1, min(64, n_paths // (W * 32)))
+    if data.translucent_objects():
+        frames = max(1, min(4, frames))  # every frame also runs the probe pass
     band = max(1, min(data.camera.height, n_paths // (W * frames)))
     p0 = W * max(0, (data.camera.height - band) // 2)
     t0 = time.perf_counter()
@@ -162,7 +199,7 @@ def cpu_baseline_sample(data, target_s=12.0, threads=None):
     O.close()
     return {"value": samples / dt / 1e6, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": "%d rows x %d px x %d spp (%d path samples) of the same scene, CPU restatement of the reference's "
-                      "recursive path tracer (path_tracer.cu + shaders, its own math), %d threads, %.1f s" % (
+                      "recursive path tracer (path_tracer.cu + shaders, its own math; probe pass included), %d threads, %.1f s" % (
                           band, W, frames, samples, threads, dt)}
 
 
@@ -171,14 +208,14 @@ def run_reference(args, world, rank):
 
     if rank != 0:
         return
-    data = scenes.single_scene(width=args.width, height=args.height)
+    data, _, desc = workload(args)
     from oracle import oracle_ctypes as oc
 
     threads = os.cpu_count() or 1
     O = oc.OracleScene(data)
     W, H = data.camera.width, data.camera.height
-    band = 16  # rows per step: each step is a bounded sample (16 x 512 px x 8 spp)
-    frames = 8
+    band = 16  # rows per step: each step is a bounded sample (16 rows x 8 spp; 1 spp for the subsurface scene)
+    frames = 8 if args.workload == "single_scene" else 1
     p0 = W * (H // 2 - band // 2)
     for _ in range(max(0, args.warmup)):
         O.render(0, 1, p_begin=p0, p_end=p0 + W * 2, threads=threads)
@@ -192,7 +229,7 @@ def run_reference(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(1, args.steps), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_per_step": "%d rows x %d px x %d spp" % (band, W, frames)},
+        "config": {"workload": desc, "sample_per_step": "%d rows x %d px x %d spp" % (band, W, frames)},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": "%d rows x %d px x %d spp per step; the reference's OptiX tracer has no CPU build, so its "
                                    "CPU restatement (path_tracer.cu + shaders, the reference's math) runs on all host cores" % (
@@ -211,11 +248,11 @@ def run_ours(args, world, rank, local):
     from open_rendering_framework_b200 import scenes
 
     torch.cuda.set_device(local)
-    data = scenes.single_scene(width=args.width, height=args.height)
+    data, spp, desc = workload(args)
     R = sc.Renderer(data, device=local)
     stream = torch.cuda.ExternalStream(R.stream())
-    spp = args.spp
-    path_samples = args.width * args.height * spp
+    width, height = data.camera.width, data.camera.height
+    path_samples = width * height * spp
 
     def barrier():
         if world > 1:
@@ -251,7 +288,7 @@ def run_ours(args, world, rank, local):
     value = world * args.steps * path_samples / (ms_max * 1e-3) / 1e6
 
     # ---- end-to-end through the public API with host buffers
-    img_host = torch.empty((args.height, args.width, 4), dtype=torch.float32, pin_memory=True)
+    img_host = torch.empty((height, width, 4), dtype=torch.float32, pin_memory=True)
     mats = [m for m in data.materials]
     h2d = sum(ctypes.sizeof(m.params()) for m in mats)
     d2h = img_host.numel() * 4
@@ -302,18 +339,35 @@ def run_ours(args, world, rank, local):
                 "segments_per_path": st.segments / st.path_samples, "shadow_rays_per_path": st.shadow_rays / st.path_samples,
                 "algorithmic_bytes_per_segment": EXTEND_BYTES_PER_SEGMENT,
                 "giga_rays_per_s": (st.segments + st.shadow_rays) / (st.gpu_ms * 1e-3) / 1e9}
+    if args.workload == "subsurface":
+        roofline["traffic"] = None  # the committed traffic figure is the single-scene kernel's
+        # integer-issue bound: 64 INT32 lanes per clock per SM at the sampled SM clock, divided by the
+        # thread instructions one pair takes (ncu capture of k_gather)
+        sm_mhz = clocks.summary().get("sm_mhz") or 1965.0
+        alu_peak = torch.cuda.get_device_properties(local).multi_processor_count * 64 * sm_mhz * 1e6 / GATHER_INSTR_PER_PAIR / 1e9
+        achieved_g = st.dipole_pairs / (st.gather_ms * 1e-3) / 1e9 if st.gather_ms else None
+        roofline = {"bound": "alu", "kernel": "k_gather (dipole gathers: one MD5 draw per (gather, probe) pair)",
+                    "achieved": achieved_g, "unit": "Gpair/s", "peak": alu_peak,
+                    "peak_source": "INT32 pipe: 64 lanes/clk/SM x SMs x median SM clock / %d thread instructions per pair (ncu)" %
+                                   GATHER_INSTR_PER_PAIR,
+                    "frac": achieved_g / alu_peak if achieved_g else None, "traffic": None,
+                    "gather_share_of_render": st.gather_ms / st.gpu_ms if st.gpu_ms else None,
+                    "pairs_per_gather": st.dipole_pairs / max(1, st.dipole_gathers),
+                    "gathers_per_path": st.dipole_gathers / st.path_samples,
+                    "probe_bytes_per_pair": 16, "extend": roofline}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "path_samples_per_step": path_samples, "parallelism": "replicas (one independent render per GPU)",
+        "config": {"workload": desc, "path_samples_per_step": path_samples, "parallelism": "replicas (one independent render per GPU)",
                    "l2": "inputs larger than L2: per-path wavefront state of %.1f GB per step" % (path_samples * 176 / 1e9)},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": roofline,
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
-        "stats": {"capped_walks": st.capped_walks, "clamped_indices": st.clamped_indices},
+        "stats": {"capped_walks": st.capped_walks, "clamped_indices": st.clamped_indices, "dipole_gathers": st.dipole_gathers,
+                  "dipole_pairs": st.dipole_pairs},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(data)

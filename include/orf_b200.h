@@ -157,6 +157,7 @@ typedef struct pt_render_stats {
   uint64_t dipole_gathers;  /* dipole gathers evaluated (camera paths entering translucent objects) */
   uint64_t dipole_pairs;    /* (gather, probe) pairs visited by those gathers                 */
   uint64_t gather_overflows;/* gathers dropped because a path's gather stack was full (0)     */
+  float gather_ms;          /* device time of the dipole gather kernel (when profiling)       */
 } pt_render_stats;
 
 /* Create / destroy a context on CUDA device `device`. */
@@ -224,8 +225,8 @@ pt_status pt_get_render_stats(pt_ctx* ctx, pt_render_stats* out);
  *                  1 = persistent warps that refill finished lanes with new rays (default)
  *   "refill"       persistent kernels refill a warp when at least this many lanes are idle (1..32, default 24) */
 pt_status pt_set_option(pt_ctx* ctx, const char* name, int64_t value);
-/* When enabled, CUDA events bracket every extend (closest-hit) launch and pt_get_render_stats
- * reports their summed device time in extend_ms.  Off by default (the events serialise nothing
+/* When enabled, CUDA events bracket every extend (closest-hit) and dipole-gather launch and
+ * pt_get_render_stats reports their summed device times in extend_ms and gather_ms.  Off by default (the events serialise nothing
  * but cost a few microseconds per bounce). */
 pt_status pt_set_profiling(pt_ctx* ctx, int enable);
 /* Probe points per translucent object and frame: context["samples"] (SAMPLES_FRAME = 500,

@@ -83,6 +83,8 @@ enum CounterSlot {
 };
 enum QueueClass { QC_MISS = 0, QC_LIGHT = 1, QC_DIFFUSE = 2, QC_METAL = 3, QC_GLASS = 4, QC_TRANS = 5, kQueues = 6 };
 
+enum ProfKind { PROF_EXTEND = 0, PROF_GATHER = 1 };
+
 // Tunable launch options (pt_set_option); the autotuner searches over these.
 struct Options {
   int extend_mode = 1;  // 0: one ray per thread, block-aggregated appends; 1: persistent warps with ray refill
@@ -131,7 +133,8 @@ struct Context {
 
   Options opt;
   bool profile = false;
-  std::vector<cudaEvent_t> prof_events;  // pairs around each extend launch when profiling
+  std::vector<cudaEvent_t> prof_events;  // pairs around each extend and gather launch when profiling
+  std::vector<int> prof_kind;            // PROF_EXTEND or PROF_GATHER per pair
   uint32_t prof_pairs = 0;
   pt_render_stats stats{};
   bool stats_pending = false;

@@ -127,14 +127,18 @@ PT_HD void md5_u2(uint32_t x, uint32_t y, uint32_t& h0, uint32_t& h1)
 }
 // rnd_accurate, random.h:134-142: the seed becomes the low 64 bits of the digest; the draw is
 // (digest & 0x7FFF...) / 2^63 in double, rounded to float.
+PT_HD float md5_draw(uint32_t h0, uint32_t h1)
+{
+  unsigned long long l = (((unsigned long long)h1 << 32) | h0) & 0x7FFFFFFFFFFFFFFFull;
+  return (float)((double)l / 9223372036854775808.0);
+}
 PT_HD float rnd_md5(uint2& s)
 {
   uint32_t h0, h1;
   md5_u2(s.x, s.y, h0, h1);
   s.x = h0;
   s.y = h1;
-  unsigned long long l = (((unsigned long long)h1 << 32) | h0) & 0x7FFFFFFFFFFFFFFFull;
-  return (float)((double)l / 9223372036854775808.0);
+  return md5_draw(h0, h1);
 }
 
 // ------------------------------------------------------------------ helpers.h

@@ -1309,28 +1309,37 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
     PT_CHECK_CUDA(cudaMemsetAsync(w.cnt, 0, (CNT_FETCH_SH + 1) * 4, c.stream), "reset queues");
     return PT_OK;
   };
+  // CUDA events around the launches whose device time the stats report (when profiling is on)
+  auto prof_begin = [&](int kind) -> pt_status {
+    if (!c.profile) return PT_OK;
+    while (c.prof_events.size() < 2 * (size_t)(c.prof_pairs + 1)) {
+      cudaEvent_t ev;
+      PT_CHECK_CUDA(cudaEventCreate(&ev), "profiling event");
+      c.prof_events.push_back(ev);
+    }
+    if (c.prof_kind.size() < (size_t)c.prof_pairs + 1) c.prof_kind.resize(c.prof_pairs + 1);
+    c.prof_kind[c.prof_pairs] = kind;
+    PT_CHECK_CUDA(cudaEventRecord(c.prof_events[2 * c.prof_pairs], c.stream), "profiling event");
+    return PT_OK;
+  };
+  auto prof_end = [&]() -> pt_status {
+    if (!c.profile) return PT_OK;
+    PT_CHECK_CUDA(cudaEventRecord(c.prof_events[2 * c.prof_pairs + 1], c.stream), "profiling event");
+    ++c.prof_pairs;
+    return PT_OK;
+  };
   // max_depth + 2 bounces: every path has ended by then (each shader stops at max_depth).
   auto bounces = [&]() -> pt_status {
     const int passes = c.integ.max_depth + 2;
     for (int b = 0; b < passes; ++b) {
       PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_Q_MISS, 0, (CNT_FETCH_SH - CNT_Q_MISS + 1) * 4, c.stream), "reset queues");
       PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + w.out_slot, 0, 4, c.stream), "reset queues");
-      if (c.profile) {
-        while (c.prof_events.size() < 2 * (size_t)(c.prof_pairs + 1)) {
-          cudaEvent_t ev;
-          PT_CHECK_CUDA(cudaEventCreate(&ev), "profiling event");
-          c.prof_events.push_back(ev);
-        }
-        PT_CHECK_CUDA(cudaEventRecord(c.prof_events[2 * c.prof_pairs], c.stream), "profiling event");
-      }
+      if ((st = prof_begin(PROF_EXTEND)) != PT_OK) return st;
       if (c.opt.extend_mode == 1)
         k_extend_persistent<<<grid_persist, kBlock, 0, c.stream>>>(S, w, c.opt.refill);
       else
         k_extend<<<grid_trace, kBlock, 0, c.stream>>>(S, w);
-      if (c.profile) {
-        PT_CHECK_CUDA(cudaEventRecord(c.prof_events[2 * c.prof_pairs + 1], c.stream), "profiling event");
-        ++c.prof_pairs;
-      }
+      if ((st = prof_end()) != PT_OK) return st;
       k_shade_miss<<<grid_shade, kBlock, 0, c.stream>>>(S, w);
       k_shade_light<<<grid_shade, kBlock, 0, c.stream>>>(S, w, geo_p);
       k_shade_diffuse<<<grid_shade, kBlock, 0, c.stream>>>(S, w, geo_p);
@@ -1378,7 +1387,9 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
       PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_GATHER, 0, 4, c.stream), "reset gather list");
       uint32_t* list = wf.q_a.as<uint32_t>();
       k_gather_collect<<<grid_for(n_paths, kBlock, 16), kBlock, 0, c.stream>>>(w, n_paths, list);
+      if ((st = prof_begin(PROF_GATHER)) != PT_OK) return st;
       k_gather<<<grid_shade, kBlock, 0, c.stream>>>(S, w, g, list, pixels);
+      if ((st = prof_end()) != PT_OK) return st;
       count_launch(2);
     }
     k_accumulate<<<grid_for(pixels, kBlock, 16), kBlock, 0, c.stream>>>(S, w, c.d_accum.as<float4>(), first_frame + f0, nf, pixels);
@@ -1441,13 +1452,14 @@ pt_status pt_get_render_stats(pt_ctx* ctx, pt_render_stats* out)
     float ms = 0.0f;
     PT_CHECK_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1), "event time");
     c.stats.gpu_ms = ms;
-    float ext = 0.0f;
+    float ext = 0.0f, gat = 0.0f;
     for (uint32_t k = 0; k < c.prof_pairs; ++k) {
       float e = 0.0f;
       PT_CHECK_CUDA(cudaEventElapsedTime(&e, c.prof_events[2 * k], c.prof_events[2 * k + 1]), "event time");
-      ext += e;
+      (c.prof_kind[k] == PROF_GATHER ? gat : ext) += e;
     }
     c.stats.extend_ms = ext;
+    c.stats.gather_ms = gat;
     c.stats_pending = false;
   }
   *out = c.stats;

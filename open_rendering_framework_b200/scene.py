@@ -66,7 +66,8 @@ class RenderStats(ctypes.Structure):
     _fields_ = [("path_samples", ctypes.c_uint64), ("segments", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
                 ("capped_walks", ctypes.c_uint64), ("clamped_indices", ctypes.c_uint64), ("gpu_ms", ctypes.c_float),
                 ("extend_ms", ctypes.c_float), ("extend_launches", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32),
-                ("dipole_gathers", ctypes.c_uint64), ("dipole_pairs", ctypes.c_uint64), ("gather_overflows", ctypes.c_uint64)]
+                ("dipole_gathers", ctypes.c_uint64), ("dipole_pairs", ctypes.c_uint64), ("gather_overflows", ctypes.c_uint64),
+                ("gather_ms", ctypes.c_float)]
 
 
 # LightStruct (40 B) and TriangleLight (92 B), structs.h:42-103, as numpy record types.
