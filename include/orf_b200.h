@@ -244,6 +244,47 @@ pt_status pt_get_scattering_properties(pt_ctx* ctx, uint32_t material_id, void* 
 /* Upper bound on paths kept in flight by one wavefront pass (frames are grouped to fit). */
 pt_status pt_set_max_paths_in_flight(pt_ctx* ctx, uint64_t max_paths);
 
+/* Frame the next batch render of this scene starts at (advanced by pt_render_frames and by batch
+ * renders; reset to 0 by pt_set_camera). */
+pt_status pt_get_next_frame(pt_ctx* ctx, uint32_t* next_frame);
+
+/* ---------------------------------------------------------------- batches of scenes
+ * No counterpart in the reference (one OptiX launch per scene).  A batch renders several scenes
+ * (built contexts on one device) in one wavefront pass: every scene's frames become items of one
+ * path-id space, so small scenes fill the GPU together, and the pass's whole launch sequence is
+ * captured once into a CUDA graph and replayed on later renders.  Each scene keeps the semantics of
+ * pt_render_frames: a batch render of frames [f, f+n) leaves exactly the image that
+ * pt_render_frames(ctx, f, n) would.  The batch works on its own stream; read-backs on a scene's
+ * context are ordered after it. */
+typedef struct pt_batch pt_batch;
+typedef struct pt_tune_result {
+  int32_t extend_mode;          /* chosen "extend_mode"                                  */
+  int32_t refill;               /* chosen "refill" (rays a warp fetches per refill, 1..32) */
+  uint64_t max_paths_in_flight; /* chosen paths per wavefront chunk                     */
+  float best_mpaths_per_s;      /* calibration throughput of the winner                 */
+  uint32_t trials;              /* configurations timed                                 */
+} pt_tune_result;
+pt_status pt_batch_create(int device, pt_batch** out);
+pt_status pt_batch_destroy(pt_batch* batch);
+/* The batch's CUDA stream (cudaStream_t). */
+void* pt_batch_stream(pt_batch* batch);
+/* Adds a built scene; each batch render traces frames_per_render frames of it. */
+pt_status pt_batch_add(pt_batch* batch, pt_ctx* scene, uint32_t frames_per_render);
+/* Options of the batch engine: "extend_mode", "refill" (as pt_set_option), "max_paths_in_flight",
+ * "use_graph" (1 = capture and replay the launch sequence, the default). */
+pt_status pt_batch_set_option(pt_batch* batch, const char* name, int64_t value);
+/* Renders the next frames_per_render frames of every scene (starting at each scene's next frame). */
+pt_status pt_batch_render(pt_batch* batch);
+/* The same frames rendered scene after scene, each by its own single-scene pass (the plain path), on
+ * the batch's buffers: the baseline the batched pass is compared with. */
+pt_status pt_batch_render_sequential(pt_batch* batch);
+/* Counters and device time of the last batch render (synchronizes). */
+pt_status pt_batch_get_stats(pt_batch* batch, pt_render_stats* out);
+/* Times short renders (min(frames_per_render, frames_per_trial) frames of every scene) over the
+ * engine options -- extend kernel, warp refill threshold, paths per wavefront chunk -- and keeps the
+ * fastest.  The trials render from frame 0, so every scene's accumulation restarts at frame 0. */
+pt_status pt_batch_autotune(pt_batch* batch, uint32_t frames_per_trial, pt_tune_result* out);
+
 /* ---------------------------------------------------------------- ray queries (BVH parity)
  * Closest-hit / any-hit queries against the built scene for n rays given as d_orig_tmin
  * (float4: origin.xyz, tmin) and d_dir_tmax (float4: direction.xyz, tmax).  Closest hit writes the

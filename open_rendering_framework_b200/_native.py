@@ -72,6 +72,16 @@ SIGNATURES = {
     "pt_get_render_stats": (I32, [P, P]),
     "pt_set_max_paths_in_flight": (I32, [P, U64]),
     "pt_set_probe_count": (I32, [P, U32]),
+    "pt_get_next_frame": (I32, [P, P]),
+    "pt_batch_create": (I32, [ctypes.c_int, P]),
+    "pt_batch_destroy": (I32, [P]),
+    "pt_batch_stream": (P, [P]),
+    "pt_batch_add": (I32, [P, P, U32]),
+    "pt_batch_set_option": (I32, [P, ctypes.c_char_p, ctypes.c_int64]),
+    "pt_batch_render": (I32, [P]),
+    "pt_batch_render_sequential": (I32, [P]),
+    "pt_batch_get_stats": (I32, [P, P]),
+    "pt_batch_autotune": (I32, [P, U32, P]),
     "pt_get_probes": (I32, [P, P, U64, P]),
     "pt_get_scattering_properties": (I32, [P, U32, P]),
     "pt_set_profiling": (I32, [P, I32]),

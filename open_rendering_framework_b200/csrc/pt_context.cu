@@ -21,6 +21,12 @@ SceneDev Context::view() const
   s.normals = d_normals.as<float4>();
   s.mats = d_mats.as<MatDev>();
   s.scat = d_scat.as<ScatDev>();
+  s.geo = d_normals_geo.as<float4>();
+  s.accum = d_accum.as<float4>();
+  s.trans_objs = d_trans_objs.as<uint4>();
+  s.trans_pos = d_trans_pos.as<float>();
+  s.n_trans = (uint32_t)trans_objs.size();
+  s.probe_samples = probe_samples;
   s.lights = d_lights.as<LightRaw>();
   s.tri_lights = d_tri_lights.as<TriLightRaw>();
   s.n_lights = (int)lights.size();
@@ -374,6 +380,7 @@ pt_status pt_set_camera(pt_ctx* ctx, const float eye[3], const float U[3], const
   c.cam.width = width;
   c.cam.height = height;
   c.camera_set = true;
+  c.next_frame = 0;
   if (resized) {
     pt_status st = c.d_accum.reserve((size_t)width * height * sizeof(float4), "accumulation buffer");
     if (st != PT_OK) return st;

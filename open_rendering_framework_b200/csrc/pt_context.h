@@ -45,6 +45,7 @@ struct DevBuf {
 struct Wavefront {
   uint64_t cap = 0;
   DevBuf ray_o, ray_d, thr, rad, rng, hit;   // per path
+  DevBuf path_item;                           // per path: its item of the pass (uint16)
   DevBuf q_a, q_b;                            // active queues (path ids)
   DevBuf q_mat;                               // per-material-class queues, kQueues x cap
   DevBuf sh_o, sh_d, sh_c, sh_pid;            // shadow-ray queue
@@ -82,6 +83,41 @@ enum CounterSlot {
   kCounters = 32
 };
 enum QueueClass { QC_MISS = 0, QC_LIGHT = 1, QC_DIFFUSE = 2, QC_METAL = 3, QC_GLASS = 4, QC_TRANS = 5, kQueues = 6 };
+
+// One (scene, frame range) of a wavefront pass.  The camera paths, probes, accumulated pixels and probe
+// sets of a pass are numbered item after item; every path records its item.
+struct ItemDev {
+  uint32_t scene;        // index into the pass's scene table
+  uint32_t first_frame;
+  uint32_t n_frames;
+  uint32_t pixels;       // width * height of the scene
+  uint64_t path_begin;   // first camera path id: path = path_begin + frame_in_item * pixels + pixel
+  uint64_t probe_begin;  // first probe id: probe = probe_begin + (frame_in_item * n_trans + object) * samples + sample
+  uint64_t pix_begin;    // first accumulation id: pix_begin + pixel
+  uint32_t set_begin;    // first probe set: set_begin + frame_in_item * n_trans + object
+  uint32_t pad;
+};
+
+// What the pass planner needs to know of a scene.
+struct SceneFacts {
+  uint32_t pixels = 1, n_trans = 0, samples = 0;
+  int max_depth = 0;
+};
+// A request: frames [first_frame, first_frame + n_frames) of scene `scene`.
+struct ItemReq {
+  uint32_t scene, first_frame, n_frames;
+};
+// A planned pass: chunks of whole frames, each at most max_paths camera paths, items chunk after chunk.
+struct PassLayout {
+  std::vector<ItemDev> items;
+  std::vector<uint32_t> chunk_item_begin;
+  std::vector<uint64_t> chunk_paths, chunk_probes, chunk_pixels;
+  std::vector<uint32_t> chunk_sets;
+  uint64_t cap_paths = 0, cap_probes = 0, cap_sets = 0;
+  int passes = 0;
+  bool sss = false;
+  uint32_t g_slots = 0;
+};
 
 enum ProfKind { PROF_EXTEND = 0, PROF_GATHER = 1 };
 
@@ -122,6 +158,8 @@ struct Context {
 
   DevBuf d_nodes, d_v0, d_e1, d_e2, d_info, d_normals, d_mats, d_lights, d_tri_lights;
   DevBuf d_scat, d_trans_objs, d_trans_pos;
+  DevBuf d_scene_tab, d_item_tab;  // scene and item tables of the current pass (this context as the engine)
+  uint32_t next_frame = 0;         // first frame of the next render that does not name one (batches)
   DevBuf d_accum;  // float4 per pixel
   DevBuf d_env_tex, d_env_mpdf, d_env_mcdf, d_env_cpdf, d_env_ccdf, d_env_lum, d_env_mf;
   int env_w = 0, env_h = 0;
@@ -142,6 +180,13 @@ struct Context {
 
   SceneDev view() const;
 };
+
+struct Context;
+pt_status prepare_scene(Context& c, const char* who);
+uint64_t scene_path_samples(const Context& c, uint32_t n_frames);
+PassLayout plan_pass(const std::vector<SceneFacts>& facts, const std::vector<ItemReq>& reqs, uint64_t max_paths);
+pt_status pass_resources(Context& E, const PassLayout& L, const std::vector<SceneDev>& scenes);
+pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool multi, bool allow_events);
 
 }  // namespace pt
 

@@ -67,20 +67,36 @@ struct WfDev {
   float4* g_b;
   float2* g_c;
   uint32_t g_slots;
+  // the scenes and items of the pass; each path's item
+  const SceneDev* scenes;
+  const ItemDev* items;
+  uint32_t n_items;
+  uint16_t* path_item;
 };
 
-// Translucent objects and their probes.
+// Probe storage of a pass, indexed by probe id (item after item, then frame, object, sample).
 struct SssDev {
-  const uint4* objs;   // (material, first triangle, triangle count, offset into pos9)
-  const float* pos9;   // vertex positions of the objects' triangles, as given
-  uint32_t n_obj, samples;
   float4* probes;      // 5 float4 per PositionSample
-  float4* pc_pos;      // compacted probes with L != 0 per (frame, object): pos
+  float4* pc_pos;      // compacted probes with L != 0 per (frame, object) set, at the set's first probe id: pos
   float4* pc_wl;       //   weight * L
   float4* pc_nrm;      //   normal
   float4* pc_tr;       //   transmitted
-  uint32_t* pc_cnt;    //   count per (frame, object)
+  uint32_t* pc_cnt;    //   count per set
 };
+
+// Index of the last item whose begin field is <= key (every begin field increases item after item).
+template <class F>
+__device__ __forceinline__ uint32_t find_item(const ItemDev* items, uint32_t n, uint64_t key, F begin)
+{
+  uint32_t lo = 0, hi = n;
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if ((uint64_t)begin(items[mid]) <= key) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+__device__ __forceinline__ const SceneDev& scene_of(const WfDev& w, uint32_t pid) { return w.scenes[w.items[w.path_item[pid]].scene]; }
 
 __device__ __forceinline__ unsigned lanemask_lt() { return (1u << (threadIdx.x & 31)) - 1u; }
 __device__ __forceinline__ unsigned long long* cnt64(uint32_t* cnt, int slot) { return reinterpret_cast<unsigned long long*>(cnt + slot); }
@@ -139,14 +155,14 @@ __device__ __forceinline__ uint32_t block_slot_multi(int cls, uint32_t* counters
 // Shading normal of a hit: normalize(rtTransformNormal(normalize(n))) with the identity transform,
 // where n is the interpolated vertex normal or the geometric normal (triangle_mesh.cu:63-70,
 // diffuse_shader.cu:48).
-__device__ __forceinline__ float3 shading_normal(const SceneDev& S, const float4* geo, const int4& info, float u, float v, int prim)
+__device__ __forceinline__ float3 shading_normal(const SceneDev& S, const int4& info, float u, float v, int prim)
 {
   float3 n;
   if (info.x >= 0) {
     float3 n0 = ld3(__ldg(S.normals + info.x)), n1 = ld3(__ldg(S.normals + info.y)), n2 = ld3(__ldg(S.normals + info.z));
     n = normalize(n1 * u + n2 * v + n0 * (1.0f - u - v));
   } else {
-    n = normalize(ld3(__ldg(geo + prim)));
+    n = normalize(ld3(__ldg(S.geo + prim)));
   }
   return normalize(n);
 }
@@ -252,18 +268,22 @@ __device__ void eval_direct(const SceneDev& S, const float3& pos, const LightRaw
 
 // ------------------------------------------------------------------ kernels
 // path_tracer.cu:32-60: seed, jitter, pinhole direction; paths outside the patch are flagged.
-__global__ void __launch_bounds__(kBlock) k_raygen(SceneDev S, WfDev w, uint32_t first_frame, uint64_t n_paths, uint32_t pixels)
+__global__ void __launch_bounds__(kBlock) k_raygen(WfDev w, uint64_t n_paths)
 {
   __shared__ uint32_t sm[kWarps + 1];
-  const CameraDev& C = S.cam;
   for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < n_paths; base += (uint64_t)gridDim.x * kBlock) {
     uint64_t pid = base + threadIdx.x;
     bool valid = pid < n_paths;
     bool inside = false;
     if (valid) {
-      uint32_t fl = (uint32_t)(pid / pixels), p = (uint32_t)(pid % pixels);
+      uint32_t k = find_item(w.items, w.n_items, pid, [](const ItemDev& it) { return it.path_begin; });
+      const ItemDev& it = w.items[k];
+      const CameraDev& C = w.scenes[it.scene].cam;
+      w.path_item[pid] = (uint16_t)k;
+      uint64_t local = pid - it.path_begin;
+      uint32_t fl = (uint32_t)(local / it.pixels), p = (uint32_t)(local % it.pixels);
       uint32_t x = p % C.width, y = p / C.width;
-      uint32_t frame = first_frame + fl;
+      uint32_t frame = it.first_frame + fl;
       inside = !(x < C.patch_origin.x || x > C.patch_origin.x + C.patch_dims.x || y < C.patch_origin.y || y > C.patch_origin.y + C.patch_dims.y);
       if (inside) {
         uint32_t seed = tea16(C.width * y + x, frame);
@@ -300,11 +320,10 @@ __device__ __forceinline__ int class_of(uint32_t type)
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_extend(SceneDev S, WfDev w)
+__global__ void __launch_bounds__(kBlock) k_extend(WfDev w)
 {
   __shared__ uint32_t sm[kWarps * kQueues + kQueues];
   const uint32_t n = w.cnt[w.in_slot];
-  const float eps = S.integ.scene_epsilon;
   uint32_t traced = 0;
   for (uint32_t base = blockIdx.x * kBlock; base < n; base += gridDim.x * kBlock) {
     uint32_t i = base + threadIdx.x;
@@ -312,8 +331,9 @@ __global__ void __launch_bounds__(kBlock) k_extend(SceneDev S, WfDev w)
     uint32_t pid = 0;
     if (i < n) {
       pid = w.q_in[i];
+      const SceneDev& S = scene_of(w, pid);
       float4 o = w.ray_o[pid], d = w.ray_d[pid];
-      Hit h = trace_closest(S, ld3(o), ld3(d), eps, kDefaultMax);
+      Hit h = trace_closest(trav_geom(S), ld3(o), ld3(d), S.integ.scene_epsilon, kDefaultMax);
       w.hit[pid] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
       if (h.prim < 0) cls = QC_MISS;
       else cls = class_of(__ldg(&S.mats[__ldg(&S.tri_info[h.prim].w)].type));
@@ -351,11 +371,17 @@ __device__ __forceinline__ uint32_t warp_slot_multi(int cls, uint32_t* counters)
 // atomic.  Traversal state (pt_scene.cuh TravState) is resumable, so lanes never wait for the
 // slowest ray of a whole block (T. Aila, S. Laine, "Understanding the efficiency of ray traversal
 // on GPUs", HPG 2009: persistent threads with ray replacement).
-__global__ void __launch_bounds__(kBlock) k_extend_persistent(SceneDev S, WfDev w, int refill)
+// kMulti: the rays belong to several scenes (a batch); each lane keeps its ray's scene view in
+// registers.  Otherwise the single scene is the kernel parameter S0.
+template <bool kMulti>
+__global__ void __launch_bounds__(kBlock) k_extend_persistent(SceneDev S0, WfDev w, int refill)
 {
   const uint32_t n = w.cnt[w.in_slot];
   uint32_t* fetch = w.cnt + CNT_FETCH_EXT;
-  const float eps = S.integ.scene_epsilon;
+  TravGeom g = trav_geom(S0);
+  float eps = S0.integ.scene_epsilon;
+  const MatDev* mats = S0.mats;
+  const int4* tinfo = S0.tri_info;
   const unsigned lane = threadIdx.x & 31;
   bool has = false, done = false, drained = false;
   uint32_t pid = 0, traced = 0;
@@ -377,6 +403,13 @@ __global__ void __launch_bounds__(kBlock) k_extend_persistent(SceneDev S, WfDev 
         uint32_t i = base + __popc(idle & lanemask_lt());
         if (i < n) {
           pid = w.q_in[i];
+          if constexpr (kMulti) {
+            const SceneDev& S = scene_of(w, pid);
+            g = trav_geom(S);
+            eps = S.integ.scene_epsilon;
+            mats = S.mats;
+            tinfo = S.tri_info;
+          }
           float4 o4 = w.ray_o[pid], d4 = w.ray_d[pid];
           o = ld3(o4);
           d = ld3(d4);
@@ -393,14 +426,14 @@ __global__ void __launch_bounds__(kBlock) k_extend_persistent(SceneDev S, WfDev 
     }
     if (__ballot_sync(0xffffffffu, has) == 0) break;
     for (;;) {
-      if (has && !done) done = trav_step_closest(S, o, d, rp, eps, h, st);
+      if (has && !done) done = trav_step_closest(g, o, d, rp, eps, h, st);
       unsigned fin = __ballot_sync(0xffffffffu, !has || done);
       if (fin == 0xffffffffu || (!drained && __popc(fin) >= refill)) break;
     }
     int cls = -1;
     if (has && done) {
       w.hit[pid] = make_float4(h.t, h.u, h.v, as_float(h.prim));
-      cls = h.prim < 0 ? QC_MISS : class_of(__ldg(&S.mats[__ldg(&S.tri_info[h.prim].w)].type));
+      cls = h.prim < 0 ? QC_MISS : class_of(__ldg(&mats[__ldg(&tinfo[h.prim].w)].type));
     }
     uint32_t slot = warp_slot_multi(cls, w.cnt + CNT_Q_MISS);
     if (cls >= 0) w.q_mat[(size_t)cls * w.cap + slot] = pid;
@@ -415,10 +448,12 @@ __global__ void __launch_bounds__(kBlock) k_extend_persistent(SceneDev S, WfDev 
 }
 
 // Persistent any-hit kernel for the shadow queue (same ray replacement).
-__global__ void __launch_bounds__(kBlock) k_shadow_persistent(SceneDev S, WfDev w, int refill)
+template <bool kMulti>
+__global__ void __launch_bounds__(kBlock) k_shadow_persistent(SceneDev S0, WfDev w, int refill)
 {
   const uint32_t n = w.cnt[CNT_SHADOW];
   uint32_t* fetch = w.cnt + CNT_FETCH_SH;
+  TravGeom g = trav_geom(S0);
   const unsigned lane = threadIdx.x & 31;
   bool has = false, drained = false;
   int res = 0;
@@ -440,6 +475,7 @@ __global__ void __launch_bounds__(kBlock) k_shadow_persistent(SceneDev S, WfDev 
         uint32_t i = base + __popc(idle & lanemask_lt());
         if (i < n) {
           slot = i;
+          if constexpr (kMulti) g = trav_geom(scene_of(w, w.sh_pid[i]));
           float4 o4 = w.sh_o[i], d4 = w.sh_d[i];
           o = ld3(o4);
           d = ld3(d4);
@@ -454,7 +490,7 @@ __global__ void __launch_bounds__(kBlock) k_shadow_persistent(SceneDev S, WfDev 
     }
     if (__ballot_sync(0xffffffffu, has) == 0) break;
     for (;;) {
-      if (has && res == 0) res = trav_step_any(S, o, d, rp, tmin, tmax, st);
+      if (has && res == 0) res = trav_step_any(g, o, d, rp, tmin, tmax, st);
       unsigned fin = __ballot_sync(0xffffffffu, !has || res != 0);
       if (fin == 0xffffffffu || (!drained && __popc(fin) >= refill)) break;
     }
@@ -472,12 +508,13 @@ __global__ void __launch_bounds__(kBlock) k_shadow_persistent(SceneDev S, WfDev 
 
 // constantbg.cu:16-19 / envmap_background.cu:20-23.  With the environment map registered as a light,
 // a miss after next-event estimation (emission disabled) adds nothing, as for area lights.
-__global__ void __launch_bounds__(kBlock) k_shade_miss(SceneDev S, WfDev w)
+__global__ void __launch_bounds__(kBlock) k_shade_miss(WfDev w)
 {
   const uint32_t n = w.cnt[CNT_Q_MISS];
   const uint32_t* q = w.q_mat + (size_t)QC_MISS * w.cap;
   for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
     uint32_t pid = q[i];
+    const SceneDev& S = scene_of(w, pid);
     float3 bg = S.bg_color;
     if (S.env.present) {
       if (S.env.is_light && !(w.rng[pid].w & META_EMIT)) continue;
@@ -490,17 +527,18 @@ __global__ void __launch_bounds__(kBlock) k_shade_miss(SceneDev S, WfDev w)
 }
 
 // arealight_shader.cu:36-50: emitted radiance if the hit is front-facing and emission is enabled.
-__global__ void __launch_bounds__(kBlock) k_shade_light(SceneDev S, WfDev w, const float4* geo)
+__global__ void __launch_bounds__(kBlock) k_shade_light(WfDev w)
 {
   const uint32_t n = w.cnt[CNT_Q_LIGHT];
   const uint32_t* q = w.q_mat + (size_t)QC_LIGHT * w.cap;
   for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
     uint32_t pid = q[i];
+    const SceneDev& S = scene_of(w, pid);
     if (!(w.rng[pid].w & META_EMIT)) continue;
     float4 h = w.hit[pid], d = w.ray_d[pid];
     int prim = __float_as_int(h.w);
     int4 info = __ldg(S.tri_info + prim);
-    float3 normal = shading_normal(S, geo, info, h.y, h.z, prim);
+    float3 normal = shading_normal(S, info, h.y, h.z, prim);
     if (dot(normal, -ld3(d)) > 0.0f) {
       const MatDev& m = S.mats[info.w];
       float4 t = w.thr[pid], r = w.rad[pid];
@@ -511,21 +549,22 @@ __global__ void __launch_bounds__(kBlock) k_shade_light(SceneDev S, WfDev w, con
 }
 
 // diffuse_shader.cu:122-187
-__global__ void __launch_bounds__(kBlock) k_shade_diffuse(SceneDev S, WfDev w, const float4* geo)
+__global__ void __launch_bounds__(kBlock) k_shade_diffuse(WfDev w)
 {
   __shared__ uint32_t sm[kWarps + 1];
   const uint32_t n = w.cnt[CNT_Q_DIFFUSE];
   const uint32_t* q = w.q_mat + (size_t)QC_DIFFUSE * w.cap;
-  const float eps = S.integ.scene_epsilon;
   uint32_t clamped = 0;
   for (uint32_t base = blockIdx.x * kBlock; base < n; base += gridDim.x * kBlock) {
     uint32_t i = base + threadIdx.x;
     bool shadow = false, cont = false;
     uint32_t pid = 0;
     float3 hit_pos, w_l, sh_contrib;
-    float sh_tmax = 0.0f;
+    float sh_tmax = 0.0f, eps = 0.0f;
     if (i < n) {
       pid = q[i];
+      const SceneDev& S = scene_of(w, pid);
+      eps = S.integ.scene_epsilon;
       uint4 rg = w.rng[pid];
       int depth = (int)(rg.w & META_DEPTH);
       if (depth <= S.integ.max_depth) {
@@ -536,7 +575,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_diffuse(SceneDev S, WfDev w, c
         const float3 dc = f3(m.a.x, m.a.y, m.a.z);
         float3 d = ld3(d4);
         hit_pos = ld3(o) + h.x * d;
-        float3 normal = shading_normal(S, geo, info, h.y, h.z, prim);
+        float3 normal = shading_normal(S, info, h.y, h.z, prim);
         float3 ffnormal = faceforward(normal, -d, normal);
         uint32_t t = rg.x;
         bool emit = (rg.w & META_EMIT) != 0;
@@ -588,7 +627,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_diffuse(SceneDev S, WfDev w, c
 }
 
 // metallic_shader.cu:232-348
-__global__ void __launch_bounds__(kBlock) k_shade_metal(SceneDev S, WfDev w, const float4* geo)
+__global__ void __launch_bounds__(kBlock) k_shade_metal(WfDev w)
 {
   __shared__ uint32_t sm[kWarps + 1];
   const uint32_t n = w.cnt[CNT_Q_METAL];
@@ -600,6 +639,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_metal(SceneDev S, WfDev w, con
     uint32_t pid = 0;
     if (i < n) {
       pid = q[i];
+      const SceneDev& S = scene_of(w, pid);
       uint4 rg = w.rng[pid];
       int depth = (int)(rg.w & META_DEPTH);
       if (depth < S.integ.max_depth) {
@@ -609,7 +649,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_metal(SceneDev S, WfDev w, con
         const MatDev& m = S.mats[info.w];
         float3 d = ld3(d4);
         float3 hit_point = ld3(o) + h.x * d;
-        float3 normal = shading_normal(S, geo, info, h.y, h.z, prim);
+        float3 normal = shading_normal(S, info, h.y, h.z, prim);
         float3 ffnormal = faceforward(normal, -d, normal);
         float3 w_i = -d;
         uint32_t seed = rg.x;
@@ -661,7 +701,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_metal(SceneDev S, WfDev w, con
 }
 
 // rough_transparent_shader.cu:66-225
-__global__ void __launch_bounds__(kBlock) k_shade_glass(SceneDev S, WfDev w, const float4* geo)
+__global__ void __launch_bounds__(kBlock) k_shade_glass(WfDev w)
 {
   __shared__ uint32_t sm[kWarps + 1];
   const uint32_t n = w.cnt[CNT_Q_GLASS];
@@ -673,6 +713,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_glass(SceneDev S, WfDev w, con
     uint32_t pid = 0;
     if (i < n) {
       pid = q[i];
+      const SceneDev& S = scene_of(w, pid);
       uint4 rg = w.rng[pid];
       int depth = (int)(rg.w & META_DEPTH);
       if (depth < S.integ.max_depth) {
@@ -683,7 +724,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_glass(SceneDev S, WfDev w, con
         const float ior = m.a.x, rough = m.a.y;
         float3 d = ld3(d4);
         float3 hit_point = ld3(o) + h.x * d;
-        float3 normal = shading_normal(S, geo, info, h.y, h.z, prim);
+        float3 normal = shading_normal(S, info, h.y, h.z, prim);
         float3 ffnormal = faceforward(normal, -d, normal);
         float3 w_i = -d;
         uint32_t t = rg.x;
@@ -759,7 +800,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_glass(SceneDev S, WfDev w, con
 // gather stack and evaluated in last-in first-out order when the path has ended (k_gather).  A
 // probe's indirect path does not gather: in the reference it would read the probe buffer that its
 // own launch is writing.
-__global__ void __launch_bounds__(kBlock) k_shade_translucent(SceneDev S, WfDev w, const float4* geo)
+__global__ void __launch_bounds__(kBlock) k_shade_translucent(WfDev w)
 {
   __shared__ uint32_t sm[kWarps + 1];
   const uint32_t n = w.cnt[CNT_Q_TRANS];
@@ -771,6 +812,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_translucent(SceneDev S, WfDev 
     uint32_t pid = 0;
     if (i < n) {
       pid = q[i];
+      const SceneDev& S = scene_of(w, pid);
       uint4 rg = w.rng[pid];
       int depth = (int)(rg.w & META_DEPTH);
       if (depth <= S.integ.max_depth) {
@@ -780,7 +822,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_translucent(SceneDev S, WfDev 
         const MatDev& m = S.mats[info.w];
         const ScatDev& P = S.scat[info.w];
         float3 d = ld3(d4);
-        float3 no = shading_normal(S, geo, info, h.y, h.z, prim);
+        float3 no = shading_normal(S, info, h.y, h.z, prim);
         float3 xo = ld3(o) + h.x * d;
         float3 wo = -d;
         float recip_ior = 1.0f / P.relative_ior;
@@ -868,15 +910,17 @@ __global__ void __launch_bounds__(kBlock) k_gather_collect(WfDev w, uint64_t n_p
 // on one MD5 draw, and on acceptance T12 * L * S(probe, xo) / p with the standard or directional
 // dipole.  The sum times global_coeff / samples is added to the path's radiance, weighted by the
 // throughput at the vertex.  One thread per path: the MD5 stream is one sequential chain.
-__global__ void __launch_bounds__(kBlock) k_gather(SceneDev S, WfDev w, SssDev g, const uint32_t* list, uint32_t pixels)
+__global__ void __launch_bounds__(kBlock) k_gather(WfDev w, SssDev g, const uint32_t* list)
 {
   const uint32_t n = w.cnt[CNT_GATHER];
   unsigned long long pairs = 0, gathers = 0;
   for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
     uint32_t pid = list[i];
+    const ItemDev& it = w.items[w.path_item[pid]];
+    const SceneDev& S = w.scenes[it.scene];
     uint4 rg = w.rng[pid];
     uint2 t64 = make_uint2(rg.y, rg.z);
-    uint32_t fl = pid / pixels;
+    uint32_t fl = (uint32_t)((pid - it.path_begin) / it.pixels);
     float4 r4 = w.rad[pid];
     float3 L = ld3(r4);
     for (int slot = (int)(rg.w >> META_GSHIFT) - 1; slot >= 0; --slot) {
@@ -887,9 +931,9 @@ __global__ void __launch_bounds__(kBlock) k_gather(SceneDev S, WfDev w, SssDev g
       const int mat = __float_as_int(c.y);
       const MatDev& m = S.mats[mat];
       const ScatDev& P = S.scat[mat];
-      const uint32_t set = fl * g.n_obj + m.aux;
-      const size_t pb = (size_t)set * g.samples;
-      const uint32_t nc = g.pc_cnt[set];
+      const uint32_t set_in_item = fl * S.n_trans + m.aux;
+      const size_t pb = it.probe_begin + (size_t)set_in_item * S.probe_samples;
+      const uint32_t nc = g.pc_cnt[it.set_begin + set_in_item];
       const float chosen = fminf(P.transport.x, fminf(P.transport.y, P.transport.z));
       float3 acc = f3s(0.0f);
       if (m.model == DIRECTIONAL_DIPOLE) {
@@ -915,7 +959,7 @@ __global__ void __launch_bounds__(kBlock) k_gather(SceneDev S, WfDev w, SssDev g
           }
         }
       }
-      float3 contrib = acc * P.global_coeff / (float)g.samples;
+      float3 contrib = acc * P.global_coeff / (float)S.probe_samples;
       L = L + thr * contrib;
       pairs += nc;
       ++gathers;
@@ -934,21 +978,24 @@ __global__ void __launch_bounds__(kBlock) k_gather(SceneDev S, WfDev w, SssDev g
 // started into the wavefront from the point (depth 0, emission on).  The record keeps pos, dir (of the
 // light sample), normal, transmitted direction and T12; pad = (triangles * area, indirect flag) until
 // k_probe_finish forms L.
-__global__ void __launch_bounds__(kBlock) k_probe_gen(SceneDev S, WfDev w, SssDev g, uint32_t first_frame, uint64_t j0, uint64_t n)
+__global__ void __launch_bounds__(kBlock) k_probe_gen(WfDev w, SssDev g, uint64_t j0, uint64_t n)
 {
   __shared__ uint32_t sm[kWarps + 1];
-  const uint64_t per_frame = (uint64_t)g.n_obj * g.samples;
   uint32_t clamped = 0;
   for (uint64_t base = (uint64_t)blockIdx.x * kBlock; base < n; base += (uint64_t)gridDim.x * kBlock) {
     uint64_t pid = base + threadIdx.x;
     bool indirect = false;
     if (pid < n) {
       uint64_t j = j0 + pid;
-      uint32_t fl = (uint32_t)(j / per_frame);
-      uint32_t idx = (uint32_t)(j % per_frame);  // launch_index + current_translucent_obj * samples
-      uint32_t k = idx / g.samples;
-      uint32_t frame = first_frame + fl;
-      uint4 ob = g.objs[k];
+      uint32_t item = find_item(w.items, w.n_items, j, [](const ItemDev& x) { return x.probe_begin; });
+      const ItemDev& it = w.items[item];
+      const SceneDev& S = w.scenes[it.scene];
+      const uint64_t per_frame = (uint64_t)S.n_trans * S.probe_samples;
+      uint32_t fl = (uint32_t)((j - it.probe_begin) / per_frame);
+      uint32_t idx = (uint32_t)((j - it.probe_begin) % per_frame);  // launch_index + current_translucent_obj * samples
+      uint32_t k = idx / S.probe_samples;
+      uint32_t frame = it.first_frame + fl;
+      uint4 ob = S.trans_objs[k];
       const uint32_t triangles = ob.z;
       const ScatDev& P = S.scat[ob.x];
       uint32_t t = tea16(idx, frame);
@@ -956,7 +1003,7 @@ __global__ void __launch_bounds__(kBlock) k_probe_gen(SceneDev S, WfDev w, SssDe
       uint2 t64 = make_uint2(s2, s2);
       uint32_t tid = (uint32_t)(int)(rnd_md5(t64) * (float)triangles);
       if (tid >= triangles) { tid = triangles - 1; ++clamped; }
-      const float* v = g.pos9 + 9 * ((size_t)ob.w + tid);
+      const float* v = S.trans_pos + 9 * ((size_t)ob.w + tid);
       float3 v0 = f3(v[0], v[1], v[2]), v1 = f3(v[3], v[4], v[5]), v2 = f3(v[6], v[7], v[8]);
       float3 perp = cross(v1 - v0, v2 - v0);
       float area = 0.5f * length(perp);
@@ -998,6 +1045,7 @@ __global__ void __launch_bounds__(kBlock) k_probe_gen(SceneDev S, WfDev w, SssDe
         w.thr[pid] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
         w.rad[pid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         w.rng[pid] = make_uint4(t, t64.x, t64.y, META_EMIT | META_PROBE);
+        w.path_item[pid] = (uint16_t)item;
         indirect = true;
       }
       float cos_i = fmaxf(dot(w_i, nrm), 0.0f);
@@ -1037,20 +1085,22 @@ __global__ void __launch_bounds__(kBlock) k_probe_finish(WfDev w, SssDev g, uint
 }
 
 // The probes with dot(L, L) > 0 of one (frame, object) set, compacted in order: one block per set.
-__global__ void __launch_bounds__(256) k_probe_compact(SssDev g)
+__global__ void __launch_bounds__(256) k_probe_compact(WfDev w, SssDev g)
 {
   __shared__ uint32_t warp_off[8];
   __shared__ uint32_t total;
   const uint32_t set = blockIdx.x;
-  const size_t b = (size_t)set * g.samples;
+  const ItemDev& it = w.items[find_item(w.items, w.n_items, set, [](const ItemDev& x) { return x.set_begin; })];
+  const uint32_t samples = w.scenes[it.scene].probe_samples;
+  const size_t b = it.probe_begin + (size_t)(set - it.set_begin) * samples;
   if (threadIdx.x == 0) total = 0;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (uint32_t c0 = 0; c0 < g.samples; c0 += 256) {
+  for (uint32_t c0 = 0; c0 < samples; c0 += 256) {
     uint32_t i = c0 + threadIdx.x;
     bool keep = false;
     float3 pos, nrm, L, tr, wt;
-    if (i < g.samples) {
+    if (i < samples) {
       const float4* rec = g.probes + 5 * (b + i);
       float4 r0 = rec[0], r1 = rec[1], r2 = rec[2], r3 = rec[3], r4 = rec[4];
       pos = ld3(r0);
@@ -1087,13 +1137,13 @@ __global__ void __launch_bounds__(256) k_probe_compact(SssDev g)
 }
 
 // Shadow rays of diffuse_shader.cu:149-161 (every material's any-hit program is opaque).
-__global__ void __launch_bounds__(kBlock) k_shadow(SceneDev S, WfDev w)
+__global__ void __launch_bounds__(kBlock) k_shadow(WfDev w)
 {
   const uint32_t n = w.cnt[CNT_SHADOW];
   for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
     float4 o = w.sh_o[i], d = w.sh_d[i];
-    if (!trace_any(S, ld3(o), ld3(d), o.w, d.w)) {
-      uint32_t pid = w.sh_pid[i];
+    uint32_t pid = w.sh_pid[i];
+    if (!trace_any(trav_geom(scene_of(w, pid)), ld3(o), ld3(d), o.w, d.w)) {
       float4 c = w.sh_c[i], r = w.rad[pid];
       w.rad[pid] = make_float4(r.x + c.x, r.y + c.y, r.z + c.z, 0.0f);
     }
@@ -1102,13 +1152,17 @@ __global__ void __launch_bounds__(kBlock) k_shadow(SceneDev S, WfDev w)
 }
 
 // path_tracer.cu:36-43 and :64-68, frame by frame in order.
-__global__ void __launch_bounds__(kBlock) k_accumulate(SceneDev S, WfDev w, float4* accum, uint32_t first_frame, uint32_t n_frames, uint32_t pixels)
+// One thread per (item, pixel): the item's frames are folded into the scene's running mean in order.
+__global__ void __launch_bounds__(kBlock) k_accumulate(WfDev w, uint64_t n_pix)
 {
-  for (uint32_t p = blockIdx.x * kBlock + threadIdx.x; p < pixels; p += gridDim.x * kBlock) {
+  for (uint64_t q = (uint64_t)blockIdx.x * kBlock + threadIdx.x; q < n_pix; q += (uint64_t)gridDim.x * kBlock) {
+    const ItemDev& it = w.items[find_item(w.items, w.n_items, q, [](const ItemDev& x) { return x.pix_begin; })];
+    const uint32_t p = (uint32_t)(q - it.pix_begin);
+    float4* accum = w.scenes[it.scene].accum;
     float4 out = accum[p];
-    for (uint32_t fl = 0; fl < n_frames; ++fl) {
-      uint64_t pid = (uint64_t)fl * pixels + p;
-      uint32_t frame = first_frame + fl;
+    for (uint32_t fl = 0; fl < it.n_frames; ++fl) {
+      uint64_t pid = it.path_begin + (uint64_t)fl * it.pixels + p;
+      uint32_t frame = it.first_frame + fl;
       if (w.rng[pid].w & META_OUTSIDE) {
         out = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
         continue;
@@ -1148,6 +1202,7 @@ static pt_status ensure_wavefront(Context& c, uint64_t cap)
   if (st == PT_OK) st = wf.rad.reserve(cap * f4, "wavefront radiance");
   if (st == PT_OK) st = wf.rng.reserve(cap * u4, "wavefront rng");
   if (st == PT_OK) st = wf.hit.reserve(cap * f4, "wavefront hits");
+  if (st == PT_OK) st = wf.path_item.reserve(cap * 2, "wavefront path items");
   if (st == PT_OK) st = wf.q_a.reserve(cap * 4, "queue");
   if (st == PT_OK) st = wf.q_b.reserve(cap * 4, "queue");
   if (st == PT_OK) st = wf.q_mat.reserve(cap * 4 * kQueues, "material queues");
@@ -1194,70 +1249,138 @@ static pt_status ensure_sss(Context& c, uint64_t cap, uint32_t slots, uint64_t r
     }
     wf.probe_cap = records;
   }
-  return wf.pc_cnt.reserve(sets * 4, "probe counts");
+  return wf.pc_cnt.reserve(std::max<uint64_t>(sets, 1) * 4, "probe counts");
 }
 
-}  // namespace pt
-
-using namespace pt;
-
-extern "C" {
-
-pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
+// Checks a scene before it is rendered and brings its device state up to date on its own stream:
+// changed materials, and the geometric normals (once per build).
+pt_status prepare_scene(Context& c, const char* who)
 {
-  if (!ctx) return fail(PT_INVALID_ARG, "null context");
-  Context& c = ctx->c;
   PT_CHECK_CUDA(cudaSetDevice(c.device), "cudaSetDevice");
-  if (!c.built) return fail(PT_NOT_READY, "pt_render_frames: call pt_build first");
-  if (!c.camera_set) return fail(PT_NOT_READY, "pt_render_frames: camera not set");
-  if (n_frames == 0) return PT_OK;
+  if (!c.built) return fail(PT_NOT_READY, std::string(who) + ": call pt_build first");
+  if (!c.camera_set) return fail(PT_NOT_READY, std::string(who) + ": camera not set");
   for (const LightRaw& l : c.lights)
-    if (l.type == ENVMAP_LIGHT && !c.env_present)
-      return fail(PT_NOT_READY, "pt_render_frames: an environment-map light needs pt_set_envmap");
+    if (l.type == ENVMAP_LIGHT && !c.env_present) return fail(PT_NOT_READY, std::string(who) + ": an environment-map light needs pt_set_envmap");
   for (const MatDev& m : c.mats)
     if (m.type == MAT_DIFFUSE && c.lights.empty())
-      return fail(PT_NOT_READY, "pt_render_frames: diffuse materials need at least one light (light_buffer is indexed unguarded by the diffuse shader)");
+      return fail(PT_NOT_READY, std::string(who) +
+                                    ": diffuse materials need at least one light (light_buffer is indexed unguarded by the diffuse shader)");
   const bool sss = !c.trans_objs.empty();
   if (sss && c.lights.empty())
-    return fail(PT_NOT_READY, "pt_render_frames: translucent objects need at least one light (the probe pass samples light_buffer)");
+    return fail(PT_NOT_READY, std::string(who) + ": translucent objects need at least one light (the probe pass samples light_buffer)");
   if (sss && c.integ.max_depth > 254)
-    return fail(PT_CAP_EXCEEDED, "pt_render_frames: translucent objects support max_depth <= 254 (the gather stack holds 255 entries)");
+    return fail(PT_CAP_EXCEEDED, std::string(who) + ": translucent objects support max_depth <= 254 (the gather stack holds 255 entries)");
   if (c.dirty_materials) {
     PT_CHECK_CUDA(cudaMemcpyAsync(c.d_mats.p, c.mats.data(), c.mats.size() * sizeof(MatDev), cudaMemcpyHostToDevice, c.stream), "material upload");
     PT_CHECK_CUDA(cudaMemcpyAsync(c.d_scat.p, c.scat.data(), c.scat.size() * sizeof(ScatDev), cudaMemcpyHostToDevice, c.stream),
                   "scattering properties upload");
     c.dirty_materials = false;
   }
-  const uint32_t pixels = c.cam.width * c.cam.height;
-  const uint32_t n_obj = (uint32_t)c.trans_objs.size();
-  const uint64_t per_frame_probes = (uint64_t)n_obj * c.probe_samples;
-  const uint32_t g_slots = sss ? (uint32_t)c.integ.max_depth + 1 : 0;
-  uint64_t max_paths = c.max_paths;
-  if (sss) {
-    // keep the gather stacks within 4 GiB by grouping fewer frames
-    uint64_t per_path = (uint64_t)g_slots * 40;
-    max_paths = std::min<uint64_t>(max_paths, std::max<uint64_t>(pixels, (4ull << 30) / per_path));
-  }
-  uint32_t frames_per_pass = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(n_frames, max_paths / pixels));
-  uint64_t cap = (uint64_t)frames_per_pass * pixels;
-  pt_status st = ensure_wavefront(c, cap);
-  if (st != PT_OK) return st;
-  if (sss) {
-    // the stacks are indexed with the wavefront's capacity, which may exceed this call's `cap`
-    st = ensure_sss(c, c.wf.cap, g_slots, (uint64_t)frames_per_pass * per_frame_probes, (uint64_t)frames_per_pass * n_obj);
-    if (st != PT_OK) return st;
-  }
-  // per-context geometric normals (computed once per build)
   DevBuf& geo = c.d_normals_geo;
   if (!geo.p || geo.bytes < (size_t)c.n_tris * sizeof(float4) || c.geo_stale) {
-    st = geo.reserve((size_t)c.n_tris * sizeof(float4), "geometric normals");
+    pt_status st = geo.reserve((size_t)c.n_tris * sizeof(float4), "geometric normals");
     if (st != PT_OK) return st;
     k_geo_normals<<<grid_for(c.n_tris, 256, 8), 256, 0, c.stream>>>(c.view(), geo.as<float4>());
     count_launch();
     c.geo_stale = false;
   }
-  uint64_t launches0 = pt_kernel_launch_count();
-  SceneDev S = c.view();
+  return PT_OK;
+}
+
+// Camera samples a render of `n_frames` frames of this scene traces (pixels inside the patch).
+uint64_t scene_path_samples(const Context& c, uint32_t n_frames)
+{
+  uint64_t inside_w = (uint64_t)std::min<uint32_t>(c.cam.width, c.cam.patch_origin.x + c.cam.patch_dims.x + 1) -
+                      std::min<uint32_t>(c.cam.width, c.cam.patch_origin.x);
+  uint64_t inside_h = (uint64_t)std::min<uint32_t>(c.cam.height, c.cam.patch_origin.y + c.cam.patch_dims.y + 1) -
+                      std::min<uint32_t>(c.cam.height, c.cam.patch_origin.y);
+  return inside_w * inside_h * n_frames;
+}
+
+PassLayout plan_pass(const std::vector<SceneFacts>& facts, const std::vector<ItemReq>& reqs, uint64_t max_paths)
+{
+  PassLayout L;
+  uint32_t max_pixels = 1;
+  for (const SceneFacts& f : facts) {
+    L.passes = std::max(L.passes, f.max_depth + 2);
+    max_pixels = std::max(max_pixels, f.pixels);
+    if (f.n_trans) {
+      L.sss = true;
+      L.g_slots = std::max<uint32_t>(L.g_slots, (uint32_t)f.max_depth + 1);
+    }
+  }
+  if (L.sss) max_paths = std::min<uint64_t>(max_paths, std::max<uint64_t>(max_pixels, (4ull << 30) / ((uint64_t)L.g_slots * 40)));
+  uint64_t paths = 0, probes = 0, pix = 0;
+  uint32_t sets = 0;
+  auto close_chunk = [&]() {
+    if (L.chunk_item_begin.size() && L.chunk_item_begin.back() == (uint32_t)L.items.size()) return;
+    L.chunk_paths.push_back(paths);
+    L.chunk_probes.push_back(probes);
+    L.chunk_pixels.push_back(pix);
+    L.chunk_sets.push_back(sets);
+    L.cap_paths = std::max(L.cap_paths, paths);
+    L.cap_probes = std::max(L.cap_probes, probes);
+    L.cap_sets = std::max<uint64_t>(L.cap_sets, sets);
+    L.chunk_item_begin.push_back((uint32_t)L.items.size());
+    paths = probes = pix = 0;
+    sets = 0;
+  };
+  L.chunk_item_begin.push_back(0);
+  for (const ItemReq& r : reqs) {
+    const SceneFacts& f = facts[r.scene];
+    uint32_t done = 0;
+    while (done < r.n_frames) {
+      uint64_t room = max_paths > paths ? max_paths - paths : 0;
+      uint64_t fit = room / f.pixels;
+      if ((fit == 0 && paths > 0) || L.items.size() - L.chunk_item_begin.back() >= 65535) {
+        close_chunk();
+        continue;
+      }
+      uint32_t take = (uint32_t)std::min<uint64_t>(r.n_frames - done, std::max<uint64_t>(1, fit));
+      ItemDev it;
+      it.scene = r.scene;
+      it.first_frame = r.first_frame + done;
+      it.n_frames = take;
+      it.pixels = f.pixels;
+      it.path_begin = paths;
+      it.probe_begin = probes;
+      it.pix_begin = pix;
+      it.set_begin = sets;
+      it.pad = 0;
+      L.items.push_back(it);
+      paths += (uint64_t)take * f.pixels;
+      probes += (uint64_t)take * f.n_trans * f.samples;
+      pix += f.pixels;
+      sets += take * f.n_trans;
+      done += take;
+    }
+  }
+  close_chunk();
+  L.chunk_item_begin.pop_back();  // one begin per chunk
+  return L;
+}
+
+// Allocates what a pass needs in the engine context E and uploads its scene and item tables (on
+// E's stream).  Nothing here may run while E's stream is being captured.
+pt_status pass_resources(Context& E, const PassLayout& L, const std::vector<SceneDev>& scenes)
+{
+  pt_status st = ensure_wavefront(E, L.cap_paths);
+  if (st == PT_OK && L.sss) st = ensure_sss(E, E.wf.cap, L.g_slots, L.cap_probes, L.cap_sets);
+  if (st == PT_OK) st = E.d_scene_tab.reserve(scenes.size() * sizeof(SceneDev), "scene table");
+  if (st == PT_OK) st = E.d_item_tab.reserve(std::max<size_t>(L.items.size(), 1) * sizeof(ItemDev), "item table");
+  if (st != PT_OK) return st;
+  PT_CHECK_CUDA(cudaMemcpyAsync(E.d_scene_tab.p, scenes.data(), scenes.size() * sizeof(SceneDev), cudaMemcpyHostToDevice, E.stream), "scene table");
+  PT_CHECK_CUDA(cudaMemcpyAsync(E.d_item_tab.p, L.items.data(), L.items.size() * sizeof(ItemDev), cudaMemcpyHostToDevice, E.stream), "item table");
+  return PT_OK;
+}
+
+// Launches a planned pass on E's stream: per chunk, the probe pass (chunks with translucent objects),
+// the camera paths, the deferred gathers and the accumulation.  Only kernel launches and memsets of
+// device state: the whole sequence can be captured into a CUDA graph.  multi: the pass spans
+// several scenes (the traversal kernels then read each ray's scene from the table; otherwise S0).
+pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool multi, bool allow_events)
+{
+  Context& c = E;
   WfDev w;
   Wavefront& wf = c.wf;
   w.ray_o = wf.ray_o.as<float4>();
@@ -1273,17 +1396,15 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
   w.sh_pid = wf.sh_pid.as<uint32_t>();
   w.cnt = wf.counters.as<uint32_t>();
   w.cap = wf.cap;
-  w.g_a = sss ? wf.g_a.as<float4>() : nullptr;
-  w.g_b = sss ? wf.g_b.as<float4>() : nullptr;
-  w.g_c = sss ? wf.g_c.as<float2>() : nullptr;
-  w.g_slots = sss ? g_slots : 0;
+  w.g_a = L.sss ? wf.g_a.as<float4>() : nullptr;
+  w.g_b = L.sss ? wf.g_b.as<float4>() : nullptr;
+  w.g_c = L.sss ? wf.g_c.as<float2>() : nullptr;
+  w.g_slots = L.sss ? wf.gather_slots : 0;
+  w.scenes = c.d_scene_tab.as<SceneDev>();
+  w.path_item = wf.path_item.as<uint16_t>();
   SssDev g;
   memset(&g, 0, sizeof(g));
-  if (sss) {
-    g.objs = c.d_trans_objs.as<uint4>();
-    g.pos9 = c.d_trans_pos.as<float>();
-    g.n_obj = n_obj;
-    g.samples = c.probe_samples;
+  if (L.sss) {
     g.probes = wf.probes.as<float4>();
     g.pc_pos = wf.pc_pos.as<float4>();
     g.pc_wl = wf.pc_wl.as<float4>();
@@ -1291,27 +1412,23 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
     g.pc_tr = wf.pc_tr.as<float4>();
     g.pc_cnt = wf.pc_cnt.as<uint32_t>();
   }
-  const float4* geo_p = geo.as<float4>();
   const int grid_trace = sm_count() * 8, grid_shade = sm_count() * 8;
   int occ_ext = 0, occ_sh = 0;
-  PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, k_extend_persistent, kBlock, 0), "occupancy");
-  PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, k_shadow_persistent, kBlock, 0), "occupancy");
+  if (multi) {
+    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, k_extend_persistent<true>, kBlock, 0), "occupancy");
+    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, k_shadow_persistent<true>, kBlock, 0), "occupancy");
+  } else {
+    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, k_extend_persistent<false>, kBlock, 0), "occupancy");
+    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, k_shadow_persistent<false>, kBlock, 0), "occupancy");
+  }
   const int grid_persist = sm_count() * std::max(1, std::min(occ_ext, occ_sh));
+  const bool prof = c.profile && allow_events;
   PT_CHECK_CUDA(cudaMemsetAsync(w.cnt, 0, kCounters * 4, c.stream), "reset counters");
   c.prof_pairs = 0;
-  PT_CHECK_CUDA(cudaEventRecord(c.ev0, c.stream), "event");
-  uint32_t extend_launches = 0;
-  auto reset_queues = [&]() -> pt_status {
-    w.q_in = wf.q_a.as<uint32_t>();
-    w.q_out = wf.q_b.as<uint32_t>();
-    w.in_slot = CNT_ACTIVE_A;
-    w.out_slot = CNT_ACTIVE_B;
-    PT_CHECK_CUDA(cudaMemsetAsync(w.cnt, 0, (CNT_FETCH_SH + 1) * 4, c.stream), "reset queues");
-    return PT_OK;
-  };
+  pt_status st = PT_OK;
   // CUDA events around the launches whose device time the stats report (when profiling is on)
   auto prof_begin = [&](int kind) -> pt_status {
-    if (!c.profile) return PT_OK;
+    if (!prof) return PT_OK;
     while (c.prof_events.size() < 2 * (size_t)(c.prof_pairs + 1)) {
       cudaEvent_t ev;
       PT_CHECK_CUDA(cudaEventCreate(&ev), "profiling event");
@@ -1323,93 +1440,128 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
     return PT_OK;
   };
   auto prof_end = [&]() -> pt_status {
-    if (!c.profile) return PT_OK;
+    if (!prof) return PT_OK;
     PT_CHECK_CUDA(cudaEventRecord(c.prof_events[2 * c.prof_pairs + 1], c.stream), "profiling event");
     ++c.prof_pairs;
     return PT_OK;
   };
-  // max_depth + 2 bounces: every path has ended by then (each shader stops at max_depth).
+  auto reset_queues = [&]() -> pt_status {
+    w.q_in = wf.q_a.as<uint32_t>();
+    w.q_out = wf.q_b.as<uint32_t>();
+    w.in_slot = CNT_ACTIVE_A;
+    w.out_slot = CNT_ACTIVE_B;
+    PT_CHECK_CUDA(cudaMemsetAsync(w.cnt, 0, (CNT_FETCH_SH + 1) * 4, c.stream), "reset queues");
+    return PT_OK;
+  };
+  // L.passes = max_depth + 2 bounces: every path has ended by then (each shader stops at max_depth).
   auto bounces = [&]() -> pt_status {
-    const int passes = c.integ.max_depth + 2;
-    for (int b = 0; b < passes; ++b) {
+    for (int b = 0; b < L.passes; ++b) {
       PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_Q_MISS, 0, (CNT_FETCH_SH - CNT_Q_MISS + 1) * 4, c.stream), "reset queues");
       PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + w.out_slot, 0, 4, c.stream), "reset queues");
       if ((st = prof_begin(PROF_EXTEND)) != PT_OK) return st;
-      if (c.opt.extend_mode == 1)
-        k_extend_persistent<<<grid_persist, kBlock, 0, c.stream>>>(S, w, c.opt.refill);
-      else
-        k_extend<<<grid_trace, kBlock, 0, c.stream>>>(S, w);
+      if (c.opt.extend_mode == 1) {
+        if (multi) k_extend_persistent<true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+        else k_extend_persistent<false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+      } else {
+        k_extend<<<grid_trace, kBlock, 0, c.stream>>>(w);
+      }
       if ((st = prof_end()) != PT_OK) return st;
-      k_shade_miss<<<grid_shade, kBlock, 0, c.stream>>>(S, w);
-      k_shade_light<<<grid_shade, kBlock, 0, c.stream>>>(S, w, geo_p);
-      k_shade_diffuse<<<grid_shade, kBlock, 0, c.stream>>>(S, w, geo_p);
-      k_shade_metal<<<grid_shade, kBlock, 0, c.stream>>>(S, w, geo_p);
-      k_shade_glass<<<grid_shade, kBlock, 0, c.stream>>>(S, w, geo_p);
+      k_shade_miss<<<grid_shade, kBlock, 0, c.stream>>>(w);
+      k_shade_light<<<grid_shade, kBlock, 0, c.stream>>>(w);
+      k_shade_diffuse<<<grid_shade, kBlock, 0, c.stream>>>(w);
+      k_shade_metal<<<grid_shade, kBlock, 0, c.stream>>>(w);
+      k_shade_glass<<<grid_shade, kBlock, 0, c.stream>>>(w);
       count_launch(6);
-      if (sss) {
-        k_shade_translucent<<<grid_shade, kBlock, 0, c.stream>>>(S, w, geo_p);
+      if (L.sss) {
+        k_shade_translucent<<<grid_shade, kBlock, 0, c.stream>>>(w);
         count_launch();
       }
-      if (c.opt.extend_mode == 1)
-        k_shadow_persistent<<<grid_persist, kBlock, 0, c.stream>>>(S, w, c.opt.refill);
-      else
-        k_shadow<<<grid_trace, kBlock, 0, c.stream>>>(S, w);
+      if (c.opt.extend_mode == 1) {
+        if (multi) k_shadow_persistent<true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+        else k_shadow_persistent<false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+      } else {
+        k_shadow<<<grid_trace, kBlock, 0, c.stream>>>(w);
+      }
       count_launch();
-      ++extend_launches;
+      ++c.stats.extend_launches;
       std::swap(w.q_in, w.q_out);
       std::swap(w.in_slot, w.out_slot);
     }
     return PT_OK;
   };
-  for (uint32_t f0 = 0; f0 < n_frames; f0 += frames_per_pass) {
-    uint32_t nf = std::min(frames_per_pass, n_frames - f0);
-    uint64_t n_paths = (uint64_t)nf * pixels;
-    if (sss) {
-      // probe pass of frames first_frame+f0 .. +nf-1, in groups of at most `cap` probes
-      const uint64_t n_probes = (uint64_t)nf * per_frame_probes;
-      for (uint64_t j0 = 0; j0 < n_probes; j0 += cap) {
-        uint64_t nj = std::min<uint64_t>(cap, n_probes - j0);
+  const ItemDev* items = c.d_item_tab.as<ItemDev>();
+  const size_t n_chunks = L.chunk_paths.size();
+  for (size_t k = 0; k < n_chunks; ++k) {
+    const uint32_t ib = L.chunk_item_begin[k];
+    const uint32_t ie = k + 1 < n_chunks ? L.chunk_item_begin[k + 1] : (uint32_t)L.items.size();
+    w.items = items + ib;
+    w.n_items = ie - ib;
+    const uint64_t n_paths = L.chunk_paths[k], n_probes = L.chunk_probes[k];
+    if (n_probes) {
+      for (uint64_t j0 = 0; j0 < n_probes; j0 += w.cap) {
+        uint64_t nj = std::min<uint64_t>(w.cap, n_probes - j0);
         if ((st = reset_queues()) != PT_OK) return st;
-        k_probe_gen<<<grid_for(nj, kBlock, 16), kBlock, 0, c.stream>>>(S, w, g, first_frame + f0, j0, nj);
+        k_probe_gen<<<grid_for(nj, kBlock, 16), kBlock, 0, c.stream>>>(w, g, j0, nj);
         count_launch();
         if ((st = bounces()) != PT_OK) return st;
         k_probe_finish<<<grid_for(nj, kBlock, 16), kBlock, 0, c.stream>>>(w, g, j0, nj);
         count_launch();
       }
-      k_probe_compact<<<nf * n_obj, 256, 0, c.stream>>>(g);
+      k_probe_compact<<<L.chunk_sets[k], 256, 0, c.stream>>>(w, g);
       count_launch();
     }
     if ((st = reset_queues()) != PT_OK) return st;
-    k_raygen<<<grid_for(n_paths, kBlock, 16), kBlock, 0, c.stream>>>(S, w, first_frame + f0, n_paths, pixels);
+    k_raygen<<<grid_for(n_paths, kBlock, 16), kBlock, 0, c.stream>>>(w, n_paths);
     count_launch();
     if ((st = bounces()) != PT_OK) return st;
-    if (sss) {
+    if (n_probes) {
       PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_GATHER, 0, 4, c.stream), "reset gather list");
       uint32_t* list = wf.q_a.as<uint32_t>();
       k_gather_collect<<<grid_for(n_paths, kBlock, 16), kBlock, 0, c.stream>>>(w, n_paths, list);
       if ((st = prof_begin(PROF_GATHER)) != PT_OK) return st;
-      k_gather<<<grid_shade, kBlock, 0, c.stream>>>(S, w, g, list, pixels);
+      k_gather<<<grid_shade, kBlock, 0, c.stream>>>(w, g, list);
       if ((st = prof_end()) != PT_OK) return st;
       count_launch(2);
     }
-    k_accumulate<<<grid_for(pixels, kBlock, 16), kBlock, 0, c.stream>>>(S, w, c.d_accum.as<float4>(), first_frame + f0, nf, pixels);
+    k_accumulate<<<grid_for(L.chunk_pixels[k], kBlock, 16), kBlock, 0, c.stream>>>(w, L.chunk_pixels[k]);
     count_launch();
-    c.probe_last_frames = nf;
   }
-  PT_CHECK_CUDA(cudaEventRecord(c.ev1, c.stream), "event");
-  PT_CHECK_CUDA(cudaGetLastError(), "pt_render_frames launch");
+  PT_CHECK_CUDA(cudaGetLastError(), "render launch");
+  return PT_OK;
+}
+
+}  // namespace pt
+
+using namespace pt;
+
+extern "C" {
+
+pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
+{
+  if (!ctx) return fail(PT_INVALID_ARG, "null context");
+  Context& c = ctx->c;
+  pt_status st = prepare_scene(c, "pt_render_frames");
+  if (st != PT_OK) return st;
+  if (n_frames == 0) return PT_OK;
+  SceneFacts f;
+  f.pixels = c.cam.width * c.cam.height;
+  f.n_trans = (uint32_t)c.trans_objs.size();
+  f.samples = c.probe_samples;
+  f.max_depth = c.integ.max_depth;
+  PassLayout L = plan_pass({f}, {ItemReq{0, first_frame, n_frames}}, c.max_paths);
+  std::vector<SceneDev> scenes{c.view()};
+  if ((st = pass_resources(c, L, scenes)) != PT_OK) return st;
+  uint64_t launches0 = pt_kernel_launch_count();
   memset(&c.stats, 0, sizeof(c.stats));
-  c.stats.path_samples = 0;
-  {
-    uint64_t inside_w = (uint64_t)std::min<uint32_t>(c.cam.width, c.cam.patch_origin.x + c.cam.patch_dims.x + 1) -
-                        std::min<uint32_t>(c.cam.width, c.cam.patch_origin.x);
-    uint64_t inside_h = (uint64_t)std::min<uint32_t>(c.cam.height, c.cam.patch_origin.y + c.cam.patch_dims.y + 1) -
-                        std::min<uint32_t>(c.cam.height, c.cam.patch_origin.y);
-    c.stats.path_samples = inside_w * inside_h * n_frames;
-  }
-  c.stats.extend_launches = extend_launches;
+  PT_CHECK_CUDA(cudaEventRecord(c.ev0, c.stream), "event");
+  if ((st = launch_pass(c, L, scenes[0], false, true)) != PT_OK) return st;
+  PT_CHECK_CUDA(cudaEventRecord(c.ev1, c.stream), "event");
+  c.stats.path_samples = scene_path_samples(c, n_frames);
   c.stats.kernel_launches = (uint32_t)(pt_kernel_launch_count() - launches0);
   c.stats_pending = true;
+  // the probe buffer of the last chunk holds the last frames of this scene
+  c.probe_last_frames = L.items.empty() ? 0 : L.items.back().n_frames;
+  c.next_frame = first_frame + n_frames;
   return PT_OK;
 }
 

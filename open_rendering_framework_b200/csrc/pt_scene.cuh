@@ -112,6 +112,7 @@ struct SceneDev {
   const float4* tri_e2;
   const int4* tri_info;
   const float4* normals;
+  const float4* geo;    // per original triangle: cross(v1 - v0, v2 - v0), unnormalised
   const MatDev* mats;
   const ScatDev* scat;  // per material id
   const LightRaw* lights;
@@ -122,7 +123,22 @@ struct SceneDev {
   EnvDev env;
   CameraDev cam;
   IntegratorDev integ;
+  float4* accum;        // the running mean, width * height
+  // translucent objects: (material, first triangle, triangle count, offset into trans_pos) and their
+  // vertex positions as given (9 floats per triangle)
+  const uint4* trans_objs;
+  const float* trans_pos;
+  uint32_t n_trans, probe_samples;
 };
+// The traversal's view of a scene (the four arrays it reads), held in registers by kernels that
+// trace rays of several scenes.
+struct TravGeom {
+  const float4* nodes;
+  const float4* tri_v0;
+  const float4* tri_e1;
+  const float4* tri_e2;
+};
+PT_HD TravGeom trav_geom(const SceneDev& S) { return TravGeom{S.nodes, S.tri_v0, S.tri_e1, S.tri_e2}; }
 
 struct Ray {
   float3 o, d;
@@ -183,7 +199,7 @@ PT_HD bool tri_mt(const float3& o, const float3& d, const float3& v0, const floa
 PT_HD float3 ld3(const float4& a) { return f3(a.x, a.y, a.z); }
 
 // Intersect the triangles of leaf `code` and keep the closest hit (ties -> lower original index).
-PT_HD void leaf_closest(const SceneDev& S, uint32_t code, const float3& o, const float3& d, float tmin, Hit& h)
+template <class G> PT_HD void leaf_closest(const G& S, uint32_t code, const float3& o, const float3& d, float tmin, Hit& h)
 {
   uint32_t first = (code & 0x7fffffffu) >> 4, count = code & 15u;
   for (uint32_t j = first; j < first + count; ++j) {
@@ -199,7 +215,7 @@ PT_HD void leaf_closest(const SceneDev& S, uint32_t code, const float3& o, const
     }
   }
 }
-PT_HD bool leaf_any(const SceneDev& S, uint32_t code, const float3& o, const float3& d, float tmin, float tmax)
+template <class G> PT_HD bool leaf_any(const G& S, uint32_t code, const float3& o, const float3& d, float tmin, float tmax)
 {
   uint32_t first = (code & 0x7fffffffu) >> 4, count = code & 15u;
   for (uint32_t j = first; j < first + count; ++j) {
@@ -228,7 +244,7 @@ PT_HD void trav_init(TravState& st)
 
 // Backtrack to the deepest pending child.  Closest-hit: the pending far child's box is re-tested
 // against the current closest distance when it is resumed.  Returns false when the root is done.
-PT_HD bool trav_backtrack(const SceneDev& S, const float3& o, const RayPre& rp, float tmin, float tlimit, TravState& st, bool retest)
+template <class G> PT_HD bool trav_backtrack(const G& S, const float3& o, const RayPre& rp, float tmin, float tlimit, TravState& st, bool retest)
 {
   for (;;) {
     if (st.depth == 0) return false;
@@ -264,7 +280,7 @@ PT_HD bool trav_backtrack(const SceneDev& S, const float3& o, const RayPre& rp, 
 
 // One closest-hit step: visit node st.cur (test both child boxes, intersect leaf children, descend
 // near-first or backtrack).  Returns true when the traversal is finished.
-PT_HD bool trav_step_closest(const SceneDev& S, const float3& o, const float3& d, const RayPre& rp, float tmin, Hit& h, TravState& st)
+template <class G> PT_HD bool trav_step_closest(const G& S, const float3& o, const float3& d, const RayPre& rp, float tmin, Hit& h, TravState& st)
 {
   const float4* nd = S.nodes + 4 * (size_t)st.cur;
   float4 n0 = PT_LDG(nd), n1 = PT_LDG(nd + 1), n2 = PT_LDG(nd + 2);
@@ -295,7 +311,7 @@ PT_HD bool trav_step_closest(const SceneDev& S, const float3& o, const float3& d
 
 // One any-hit step (children in fixed order, child 1 pending when both are hit).  Returns 1 when a
 // triangle with tmin < t < tmax was found, -1 when the traversal finished without one, 0 otherwise.
-PT_HD int trav_step_any(const SceneDev& S, const float3& o, const float3& d, const RayPre& rp, float tmin, float tmax, TravState& st)
+template <class G> PT_HD int trav_step_any(const G& S, const float3& o, const float3& d, const RayPre& rp, float tmin, float tmax, TravState& st)
 {
   const float4* nd = S.nodes + 4 * (size_t)st.cur;
   float4 n0 = PT_LDG(nd), n1 = PT_LDG(nd + 1), n2 = PT_LDG(nd + 2);
@@ -321,7 +337,7 @@ PT_HD int trav_step_any(const SceneDev& S, const float3& o, const float3& d, con
   return trav_backtrack(S, o, rp, tmin, tmax, st, false) ? 0 : -1;
 }
 
-PT_HD Hit trace_closest(const SceneDev& S, const float3& o, const float3& d, float tmin, float tmax)
+template <class G> PT_HD Hit trace_closest(const G& S, const float3& o, const float3& d, float tmin, float tmax)
 {
   Hit h;
   h.t = tmax;
@@ -334,7 +350,7 @@ PT_HD Hit trace_closest(const SceneDev& S, const float3& o, const float3& d, flo
   return h;
 }
 
-PT_HD bool trace_any(const SceneDev& S, const float3& o, const float3& d, float tmin, float tmax)
+template <class G> PT_HD bool trace_any(const G& S, const float3& o, const float3& d, float tmin, float tmax)
 {
   RayPre rp = ray_pre(o, d);
   TravState st;

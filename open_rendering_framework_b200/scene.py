@@ -535,3 +535,65 @@ class Renderer:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------- batches (no counterpart in the reference)
+class TuneResult(ctypes.Structure):
+    _fields_ = [("extend_mode", ctypes.c_int32), ("refill", ctypes.c_int32), ("max_paths_in_flight", ctypes.c_uint64),
+                ("best_mpaths_per_s", ctypes.c_float), ("trials", ctypes.c_uint32)]
+
+
+class Batch:
+    """Several Renderers rendered by one wavefront pass (pt_batch_*): each render traces the next
+    `frames` frames of every scene; the launch sequence is captured once in a CUDA graph."""
+
+    def __init__(self, renderers, frames, device=0):
+        b = ctypes.c_void_p()
+        nat.call("pt_batch_create", device, ctypes.byref(b))
+        self.b = b
+        self.renderers = list(renderers)
+        self.frames = [int(f) for f in frames]
+        for R, f in zip(self.renderers, self.frames):
+            nat.call("pt_batch_add", self.b, R.ctx, f)
+
+    def set_option(self, name, value):
+        nat.call("pt_batch_set_option", self.b, name.encode(), int(value))
+
+    def _sync_frames(self):
+        for R in self.renderers:
+            n = ctypes.c_uint32()
+            nat.call("pt_get_next_frame", R.ctx, ctypes.byref(n))
+            R.frame = n.value
+
+    def render(self):
+        nat.call("pt_batch_render", self.b)
+        self._sync_frames()
+
+    def render_sequential(self):
+        nat.call("pt_batch_render_sequential", self.b)
+        self._sync_frames()
+
+    def autotune(self, frames_per_trial=1):
+        r = TuneResult()
+        nat.call("pt_batch_autotune", self.b, int(frames_per_trial), ctypes.byref(r))
+        self._sync_frames()
+        return r
+
+    def stats(self):
+        s = RenderStats()
+        nat.call("pt_batch_get_stats", self.b, ctypes.byref(s))
+        return s
+
+    def stream(self):
+        return nat.lib().pt_batch_stream(self.b)
+
+    def close(self):
+        if getattr(self, "b", None):
+            nat.lib().pt_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -206,3 +206,75 @@ def translucent_box_scene(width=64, height=64, subdiv=3, probe_samples=64, dipol
     lp, li = quad_light((0.0, 0.99, 0.0), 0.5)
     lights = [sc.TriangleAreaLight(lp, li, (15.0, 15.0, 15.0))]
     return sc.SceneData(integrator, camera, background, meshes, lights, probe_samples=probe_samples)
+
+
+def heightfield(n, extent=1.2, height=0.15, y0=-0.35, seed=0):
+    """An n x n grid of quads (2 n^2 triangles) over [-extent/2, extent/2]^2 at y0 + height * value
+    noise, with per-vertex normals from central differences."""
+    t = np.linspace(-extent / 2, extent / 2, n + 1)
+    X, Z = np.meshgrid(t, t, indexing="ij")
+    P = np.stack([X.ravel(), np.zeros(X.size), Z.ravel()], 1)
+    H = height * value_noise3(P * 1.5, seed, cells=2.0).reshape(n + 1, n + 1)
+    Y = y0 + H
+    dx = np.gradient(Y, t, axis=0)
+    dz = np.gradient(Y, t, axis=1)
+    N = np.stack([-dx, np.ones_like(Y), -dz], -1)
+    N /= np.linalg.norm(N, axis=-1, keepdims=True)
+    pos = np.stack([X, Y, Z], -1).reshape(-1, 3).astype(np.float32)
+    idx = np.arange((n + 1) * (n + 1)).reshape(n + 1, n + 1)
+    a, b, c, d = idx[:-1, :-1].ravel(), idx[1:, :-1].ravel(), idx[1:, 1:].ravel(), idx[:-1, 1:].ravel()
+    tris = np.concatenate([np.stack([a, c, b], 1), np.stack([a, d, c], 1)]).astype(np.int32)
+    return pos, tris, N.reshape(-1, 3).astype(np.float32), tris.copy()
+
+
+BATCH_MATERIALS = ("diffuse", "ggx", "beckmann", "rough_dielectric", "dipole")
+
+
+def batch_scene(k, seed=0, size_scale=1.0, spp_scale=1.0, env_w=128, env_h=64, probe_samples=1024):
+    """Scene k of the batched configuration: a seeded mesh (an icosphere at the subdivision nearest a
+    log-uniform [1e3, 5e5] triangle count, or a heightfield grid of that size), a material drawn
+    uniformly from diffuse / GGX conductor / Beckmann conductor / rough dielectric / dipole, a
+    resolution from {128, 256, 512, 1024}^2 and a log-uniform spp in [4, 256]; lit by a procedural sky
+    (background and light).  size_scale / spp_scale shrink the resolution and spp (tests)."""
+    rng = np.random.default_rng([seed, k])
+    tris = float(np.exp(rng.uniform(np.log(1e3), np.log(5e5))))
+    res = int(rng.choice([128, 256, 512, 1024]))
+    spp = int(round(np.exp(rng.uniform(np.log(4), np.log(256)))))
+    kind = BATCH_MATERIALS[int(rng.integers(0, 5))]
+    use_grid = bool(rng.integers(0, 2))
+    res = max(8, int(res * size_scale))
+    spp = max(1, int(round(spp * spp_scale)))
+    if kind == "diffuse":
+        mat = sc.DiffuseMaterial(tuple(rng.uniform(0.3, 0.9, 3)))
+    elif kind == "ggx":
+        mat = sc.MetallicMaterial(ior=((0.2, 3.9), (0.55, 3.15), (0.9, 2.4)), roughness=(0.2, 0.2), microfacet_model=sc.VISIBLE_NORMALS_MODEL,
+                                  normal_distribution=sc.GGX_DISTRIBUTION)
+    elif kind == "beckmann":
+        mat = sc.MetallicMaterial(roughness=(0.15, 0.15), microfacet_model=sc.WALTER_MODEL, normal_distribution=sc.BECKMANN_DISTRIBUTION)
+    elif kind == "rough_dielectric":
+        mat = sc.RoughTransparentMaterial(ior=1.5, roughness=0.1, microfacet_model=sc.WALTER_MODEL, normal_distribution=sc.BECKMANN_DISTRIBUTION)
+    else:
+        s_, a_ = dipole_coefficients(seed * 1000 + k)
+        mat = sc.TranslucentMaterial(scattering=s_, absorption=a_, ior=1.3, scale=100.0)
+    if use_grid:
+        n = max(4, int(round((tris / 2) ** 0.5)))
+        p, i, nn, ni = heightfield(n, seed=seed * 1000 + k)
+    else:
+        sub = int(np.clip(round(np.log(tris / 20.0) / np.log(4.0)), 2, 7))
+        p, i, nn, ni = jittered_icosphere(sub, 0.4, (0.0, 0.0, 0.0), 0.02, seed * 1000 + k)
+    floor = sc.DiffuseMaterial((0.5, 0.5, 0.5))
+    fp_ = np.array([(-4, -0.45, -4), (4, -0.45, -4), (4, -0.45, 4), (-4, -0.45, 4)], np.float32)
+    fi = np.array([(0, 2, 1), (0, 3, 2)], np.int32)
+    az = rng.uniform(0, 2 * np.pi)
+    eye = (2.0 * np.sin(az), 0.8, 2.0 * np.cos(az))
+    camera = sc.PinholeCamera(eye=eye, lookat=(0.0, -0.1, 0.0), up=(0.0, 1.0, 0.0), vfov=40.0, width=res, height=res)
+    background = sc.EnvMapBackground(sky_envmap(env_w, env_h, sun_peak=5.0e4 if env_w >= 1024 else 2.0e3, sun_sigma_deg=6.0))
+    integrator = sc.PathTracer(max_depth=8, scene_epsilon=1e-4, rr_start_depth=3)
+    meshes = [sc.Mesh(p, i, mat, nn, ni), sc.Mesh(fp_, fi, floor)]
+    data = sc.SceneData(integrator, camera, background, meshes, [sc.EnvMapLight()], probe_samples=probe_samples)
+    return data, spp, {"triangles": int(len(i)), "mesh": "grid" if use_grid else "icosphere", "material": kind, "resolution": res, "spp": spp}
+
+
+def batch_scenes(n=64, seed=0, size_scale=1.0, spp_scale=1.0, **kw):
+    """The n scenes of the batched configuration: [(SceneData, spp, description)]."""
+    return [batch_scene(k, seed, size_scale, spp_scale, **kw) for k in range(n)]
