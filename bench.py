@@ -6,6 +6,12 @@ icosphere, 20,480-triangle Beckmann dielectric icosphere, 0.25 x 0.25 quad light
 max depth 8, Russian roulette from depth 3 -- 16,777,216 path samples per step, traced as one
 wavefront launch group.
 
+--workload batched: 64 seeded procedural scenes (icospheres or heightfields of 1e3-5e5 triangles,
+diffuse / GGX / Beckmann / rough-dielectric / dipole materials, 128^2-1024^2 pixels, 4-256 spp,
+procedural sky light) rendered as one batch: one step = one batch render of every scene's spp, one
+CUDA-graph launch, with the engine options from the autotuner.  The same frames rendered scene after
+scene through single-scene passes (the plain path) are timed beside it (`plain`).
+
 --workload subsurface: 1024 x 1024 pixels x 256 frames (--spp) of the translucent scene: a
 327,680-triangle jittered icosphere with the dipole BSSRDF (standard; --dipole directional), 4,096
 probes per frame (2^20 over the 256 frames), lit by a 2048 x 1024 procedural sky with a sun lobe of
@@ -54,7 +60,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="single_scene", choices=["single_scene", "subsurface"])
+    ap.add_argument("--workload", default="single_scene", choices=["single_scene", "subsurface", "batched"])
+    ap.add_argument("--scenes", type=int, default=64, help="batched workload: number of scenes")
     ap.add_argument("--spp", type=int, default=None, help="frames per step (default 64, subsurface 256)")
     ap.add_argument("--width", type=int, default=None)
     ap.add_argument("--height", type=int, default=None)
@@ -203,11 +210,49 @@ def cpu_baseline_sample(data, target_s=12.0, threads=None):
                           band, W, frames, samples, threads, dt)}
 
 
+def run_reference_batched(args):
+    """Reference arm of the batched workload: the CPU restatement on a bounded sample of each step's
+    work -- step k renders 8 rows through the middle of scene k mod n at one sample per pixel."""
+    from oracle import oracle_ctypes as oc
+    from open_rendering_framework_b200 import scenes
+
+    S = scenes.batch_scenes(args.scenes, seed=0)
+    threads = os.cpu_count() or 1
+    band = 8
+    total, samples = 0.0, 0
+    for k in range(args.warmup + args.steps):
+        data = S[k % len(S)][0]
+        O = oc.OracleScene(data)
+        W, H = data.camera.width, data.camera.height
+        p0 = W * max(0, H // 2 - band // 2)
+        t0 = time.perf_counter()
+        O.render(0, 1, p_begin=p0, p_end=p0 + W * band, threads=threads)
+        dt = time.perf_counter() - t0
+        O.close()
+        if k >= args.warmup:
+            total += dt
+            samples += W * band
+    value = samples / total / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total * 1e3 / max(1, args.steps), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": BATCHED % len(S), "sample_per_step": "8 rows x 1 spp of scene (step mod %d)" % len(S)},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": "8 rows x 1 spp of one scene per step, scenes in order; CPU restatement of the reference's "
+                                   "recursive tracer (probe pass included), all host cores"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, world, rank):
     from open_rendering_framework_b200 import scenes
 
     if rank != 0:
         return
+    if args.workload == "batched":
+        return run_reference_batched(args)
     data, _, desc = workload(args)
     from oracle import oracle_ctypes as oc
 
@@ -238,6 +283,133 @@ def run_reference(args, world, rank):
     }
     print(json.dumps(line), flush=True)
     O.close()
+
+
+BATCHED = ("batched render of %d seeded procedural scenes in one pass (CUDA graph): meshes log-uniform over 1e3-5e5 triangles "
+           "(jittered icospheres or value-noise heightfields) on a diffuse floor, materials uniform over diffuse / GGX conductor / "
+           "Beckmann conductor / Beckmann rough dielectric / dipole (500 probes per frame, the reference's default), resolutions from {128,256,512,1024}^2, "
+           "spp log-uniform over 4-256, 128x64 procedural sky as background and light, max depth 8, Russian roulette from depth 3")
+
+
+def run_batched(args, world, rank, local):
+    import torch
+
+    from open_rendering_framework_b200 import _native as nat
+    from open_rendering_framework_b200 import scene as sc
+    from open_rendering_framework_b200 import scenes
+
+    torch.cuda.set_device(local)
+    # each rank renders its own batch (replicas): scene seeds differ by rank only through nothing -- the
+    # same batch, so the per-rank work is fixed (weak scaling)
+    S = scenes.batch_scenes(args.scenes, seed=0)
+    Rs = [sc.Renderer(d, device=local) for d, _, _ in S]
+    spp = [p for _, p, _ in S]
+    B = sc.Batch(Rs, spp, device=local)
+    stream = torch.cuda.ExternalStream(B.stream())
+    path_samples = sum(d.camera.width * d.camera.height * p for d, p, _ in S)
+    tune = B.autotune(frames_per_trial=1)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        B.render()
+    torch.cuda.synchronize()
+    barrier()
+    L = nat.lib()
+    launches0 = L.pt_kernel_launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            B.render()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = L.pt_kernel_launch_count() - launches0
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps * path_samples / (ms_max * 1e-3) / 1e6
+    # the plain path: the same frames, scene after scene, each by its own single-scene pass
+    B.render_sequential()
+    torch.cuda.synchronize()
+    p0 = torch.cuda.Event(enable_timing=True)
+    p1 = torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    B.render_sequential()
+    p1.record(stream)
+    torch.cuda.synchronize()
+    plain = path_samples / (p0.elapsed_time(p1) * 1e-3) / 1e6
+    # end to end: per step every scene's camera and materials set from the host, the batch render, and
+    # every image read back into pinned host memory
+    imgs = [torch.empty((d.camera.height, d.camera.width, 4), dtype=torch.float32, pin_memory=True) for d, _, _ in S]
+    h2d = sum(ctypes.sizeof(m.params()) for d, _, _ in S for m in d.materials) + 12 * 4 * len(S)
+    d2h = sum(im.numel() * 4 for im in imgs)
+
+    def e2e_step():
+        for R in Rs:
+            R.apply_camera()
+            for m in R.data.materials:
+                R.update_material(m)
+        B.render()
+        for R, im in zip(Rs, imgs):
+            nat.call("pt_readback", R.ctx, im.data_ptr())
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    t = torch.tensor([f0.elapsed_time(f1)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.steps * path_samples / (float(t.item()) * 1e-3) / 1e6
+    st = B.stats()
+    peak, peak_kind = load_peaks()
+    kinds = {}
+    for _, p, info in S:
+        kinds[info["material"]] = kinds.get(info["material"], 0) + 1
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": BATCHED % len(S), "path_samples_per_step": path_samples, "scenes": len(S), "materials": kinds,
+                   "parallelism": "replicas (one independent batch per GPU)",
+                   "l2": "inputs larger than L2: %.1f GB of path state per chunk" % (tune.max_paths_in_flight * 178 / 1e9)},
+        "plain": {"value": plain, "unit": UNIT, "what": "the same frames rendered scene after scene by single-scene passes"},
+        "batched_over_plain": value / plain,
+        "autotune": {"extend_mode": tune.extend_mode, "refill": tune.refill, "max_paths_in_flight": tune.max_paths_in_flight,
+                     "trials": tune.trials, "best_calibration_mpaths_per_s": tune.best_mpaths_per_s},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "kernel": "k_extend_persistent", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
+                     "peak_source": peak_kind, "traffic": None,
+                     "note": "the batch runs from a CUDA graph without per-kernel events; the extend kernel's roofline is "
+                             "reported by the single-scene workload"},
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+        "stats": {"segments_per_path": st.segments / max(1, st.path_samples), "dipole_gathers": st.dipole_gathers,
+                  "dipole_pairs": st.dipole_pairs},
+    }
+    B.close()
+    for R in Rs:
+        R.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def run_ours(args, world, rank, local):
@@ -382,6 +554,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.workload == "batched":
+            run_batched(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -220,7 +220,8 @@ pt_status pt_readback_device(pt_ctx* ctx, float* d_rgba);
 pt_status pt_sync(pt_ctx* ctx);
 /* Counters and timings of the last pt_render_frames (synchronizes). */
 pt_status pt_get_render_stats(pt_ctx* ctx, pt_render_stats* out);
-/* Launch options (the autotuner's search space):
+/* Launch options (the autotuner's search space) and modes:
+ *   "differentiable" 1 = renders keep the forward state pt_render_adjoint needs (default 0)
  *   "extend_mode"  0 = one ray per thread with block-aggregated queue appends,
  *                  1 = persistent warps that refill finished lanes with new rays (default)
  *   "refill"       persistent kernels refill a warp when at least this many lanes are idle (1..32, default 24) */
@@ -229,6 +230,36 @@ pt_status pt_set_option(pt_ctx* ctx, const char* name, int64_t value);
  * pt_get_render_stats reports their summed device times in extend_ms and gather_ms.  Off by default (the events serialise nothing
  * but cost a few microseconds per bounce). */
 pt_status pt_set_profiling(pt_ctx* ctx, int enable);
+/* Textures (no counterpart in the reference's shaders, which read constant material parameters; they
+ * carry the per-texel parameters of differentiable renders).  A texture is width x height texels of 1
+ * or 3 float channels, texel (x, y) channel c at [(y*width + x)*channels + c].  pt_texture_create
+ * copies host data into library-owned device memory; pt_texture_bind points a texture at caller-owned
+ * device memory of the same shape (not copied: it must stay valid while renders read it);
+ * pt_texture_bind_grad gives the device buffer (same layout) that pt_render_adjoint accumulates the
+ * texture's gradient into (NULL: none). */
+pt_status pt_texture_create(pt_ctx* ctx, const float* host_data, uint32_t width, uint32_t height, uint32_t channels, uint32_t* out_id);
+pt_status pt_texture_bind(pt_ctx* ctx, uint32_t texture_id, const float* d_data);
+pt_status pt_texture_bind_grad(pt_ctx* ctx, uint32_t texture_id, float* d_grad);
+/* A diffuse material's diffuse_color (3-channel texture) or a metallic material's isotropic roughness
+ * (1-channel texture; Walter or visible-normal model) read at the nearest texel of a cube map around
+ * `center`: the largest component of (hit - center) picks one of six faces, laid out 3 x 2 in the
+ * texture, and the other two components divided by it give the face coordinates. */
+pt_status pt_material_set_texture(pt_ctx* ctx, uint32_t material_id, uint32_t texture_id, const float center[3]);
+/* Gradient buffer (6 device floats: d/d sigma_a RGB, d/d sigma_s' RGB, in the units of
+ * pt_translucent_params, sigma_s' = scattering * (1 - meancosine)) of a translucent material
+ * (standard dipole) for pt_render_adjoint; NULL to unbind. */
+pt_status pt_material_bind_sigma_grad(pt_ctx* ctx, uint32_t material_id, float* d_grad6);
+/* Adjoint (path replay backprop; no counterpart in the reference): with the option "differentiable"
+ * set, pt_render_frames keeps per camera path its radiance and the value of each dipole gather.
+ * pt_render_adjoint then replays the same paths (same random numbers, nothing else stored) and adds
+ * to the bound gradient buffers the gradient of a loss whose gradient with respect to the
+ * accumulation buffer is d_dimage (device, width*height*4 floats, the w channel ignored).  The
+ * differentiated estimator keeps the forward render's sampling fixed (directions, Russian roulette
+ * and dipole acceptance with their probabilities); albedo textures enter through next-event
+ * estimates and bounce weights, GGX roughness textures through the bounce weights, and sigma_a /
+ * sigma_s' through the Beer transmittance inside and the dipole gathers.  Probes are part of the
+ * sampling.  Frames must be those of the last differentiable forward render. */
+pt_status pt_render_adjoint(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames, const float* d_dimage);
 /* Probe points per translucent object and frame: context["samples"] (SAMPLES_FRAME = 500,
  * OptixSceneLoader.cpp:11-17).  Every frame first runs the probe pass of sample_camera.cu over each
  * translucent object (OptixScene.cpp:146-157), then the camera paths. */

@@ -72,6 +72,12 @@ SIGNATURES = {
     "pt_get_render_stats": (I32, [P, P]),
     "pt_set_max_paths_in_flight": (I32, [P, U64]),
     "pt_set_probe_count": (I32, [P, U32]),
+    "pt_texture_create": (I32, [P, P, U32, U32, U32, P]),
+    "pt_texture_bind": (I32, [P, U32, P]),
+    "pt_texture_bind_grad": (I32, [P, U32, P]),
+    "pt_material_set_texture": (I32, [P, U32, U32, P]),
+    "pt_material_bind_sigma_grad": (I32, [P, U32, P]),
+    "pt_render_adjoint": (I32, [P, U32, U32, P]),
     "pt_get_next_frame": (I32, [P, P]),
     "pt_batch_create": (I32, [ctypes.c_int, P]),
     "pt_batch_destroy": (I32, [P]),

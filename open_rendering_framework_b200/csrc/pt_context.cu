@@ -21,12 +21,22 @@ SceneDev Context::view() const
   s.normals = d_normals.as<float4>();
   s.mats = d_mats.as<MatDev>();
   s.scat = d_scat.as<ScatDev>();
+  s.tex = d_tex.as<TexDev>();
   s.geo = d_normals_geo.as<float4>();
   s.accum = d_accum.as<float4>();
   s.trans_objs = d_trans_objs.as<uint4>();
   s.trans_pos = d_trans_pos.as<float>();
   s.n_trans = (uint32_t)trans_objs.size();
   s.probe_samples = probe_samples;
+  const bool adj = differentiable && d_adj_L.p;
+  s.adj_L = adj ? d_adj_L.as<float4>() : nullptr;
+  s.adj_G = adj && adj_slots ? d_adj_G.as<float4>() : nullptr;
+  s.adj_first = adj_first;
+  s.adj_frames = adj_frames;
+  s.adj_slots = adj_slots;
+  s.adj_dimg = adj_dimg;
+  s.adj_dscale = adj_dscale;
+  s.mat_grad = d_mat_grad.as<float*>();
   s.lights = d_lights.as<LightRaw>();
   s.tri_lights = d_tri_lights.as<TriLightRaw>();
   s.n_lights = (int)lights.size();
@@ -61,6 +71,13 @@ static Cx host_recip(const Cx& b)
 }
 
 static bool finite_nonneg3(const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]) && v[0] >= 0 && v[1] >= 0 && v[2] >= 0; }
+
+static float __int_as_float_host(int i)
+{
+  float f;
+  memcpy(&f, &i, 4);
+  return f;
+}
 
 // The boundary polynomials of Fresnel.h:93-124 (two_C1, three_C2, C_phi, C_E).
 static float two_C1(float n)
@@ -125,6 +142,7 @@ static pt_status make_material(uint32_t type, const void* params, size_t size, M
   memset(&m, 0, sizeof(m));
   memset(&sc, 0, sizeof(sc));
   m.type = type;
+  m.tmap = make_float4(0.0f, 0.0f, 0.0f, __int_as_float_host(-1));
   if (!params) return fail(PT_INVALID_ARG, "material: null parameters");
   switch (type) {
     case PT_DIFFUSE_SHADER: {
@@ -182,6 +200,7 @@ static pt_status make_material(uint32_t type, const void* params, size_t size, M
       if (!(p->scale > 0.0f && std::isfinite(p->scale))) return fail(PT_INVALID_ARG, "translucent material: scale must be > 0");
       if (p->dipole_model > PT_DIRECTIONAL_DIPOLE) return fail(PT_INVALID_ARG, "translucent material: bad dipole_model");
       m.model = p->dipole_model;
+      m.a = make_float4(p->scale, 0.0f, 0.0f, 0.0f);  // scale: d extinction / d sigma (adjoint renders)
       sc = compute_coefficients(*p);
       return PT_OK;
     }
@@ -482,7 +501,8 @@ pt_status pt_material_update(pt_ctx* ctx, uint32_t id, const void* params, size_
   ScatDev sc;
   pt_status st = make_material(ctx->c.mats[id].type, params, params_size, m, sc);
   if (st != PT_OK) return st;
-  m.aux = ctx->c.mats[id].aux;  // translucent_index stays with the material
+  m.aux = ctx->c.mats[id].aux;    // translucent_index stays with the material
+  m.tmap = ctx->c.mats[id].tmap;  // and so does its texture
   ctx->c.mats[id] = m;
   ctx->c.scat[id] = sc;
   ctx->c.dirty_materials = true;
@@ -624,6 +644,87 @@ pt_status pt_sync(pt_ctx* ctx)
   return PT_OK;
 }
 
+pt_status pt_texture_create(pt_ctx* ctx, const float* host_data, uint32_t width, uint32_t height, uint32_t channels, uint32_t* out_id)
+{
+  if (!ctx || !host_data || !out_id) return fail(PT_INVALID_ARG, "pt_texture_create: null argument");
+  Context& c = ctx->c;
+  if (width < 3 || height < 2 || (channels != 1 && channels != 3)) return fail(PT_INVALID_ARG, "pt_texture_create: need width >= 3, height >= 2, 1 or 3 channels");
+  if ((uint64_t)width * height * channels > (1ull << 30)) return fail(PT_CAP_EXCEEDED, "pt_texture_create: texture too large");
+  const size_t n = (size_t)width * height * channels;
+  for (size_t k = 0; k < n; ++k)
+    if (!std::isfinite(host_data[k])) return fail(PT_INVALID_ARG, "pt_texture_create: non-finite texel");
+  PT_CHECK_CUDA(cudaSetDevice(c.device), "cudaSetDevice");
+  c.tex_own.emplace_back(new DevBuf());
+  pt_status st = c.tex_own.back()->reserve(n * 4, "texture");
+  if (st != PT_OK) return st;
+  PT_CHECK_CUDA(cudaMemcpyAsync(c.tex_own.back()->p, host_data, n * 4, cudaMemcpyHostToDevice, c.stream), "texture upload");
+  TexDev t;
+  memset(&t, 0, sizeof(t));
+  t.data = c.tex_own.back()->as<float>();
+  t.w = width;
+  t.h = height;
+  t.ch = channels;
+  *out_id = (uint32_t)c.textures.size();
+  c.textures.push_back(t);
+  c.dirty_textures = true;
+  return PT_OK;
+}
+
+pt_status pt_texture_bind(pt_ctx* ctx, uint32_t id, const float* d_data)
+{
+  if (!ctx || !d_data) return fail(PT_INVALID_ARG, "pt_texture_bind: null argument");
+  if (id >= ctx->c.textures.size()) return fail(PT_INVALID_ARG, "pt_texture_bind: no such texture");
+  ctx->c.textures[id].data = d_data;
+  ctx->c.dirty_textures = true;
+  return PT_OK;
+}
+
+pt_status pt_texture_bind_grad(pt_ctx* ctx, uint32_t id, float* d_grad)
+{
+  if (!ctx) return fail(PT_INVALID_ARG, "pt_texture_bind_grad: null context");
+  if (id >= ctx->c.textures.size()) return fail(PT_INVALID_ARG, "pt_texture_bind_grad: no such texture");
+  ctx->c.textures[id].grad = d_grad;
+  ctx->c.dirty_textures = true;
+  return PT_OK;
+}
+
+pt_status pt_material_set_texture(pt_ctx* ctx, uint32_t material_id, uint32_t tex_id, const float center[3])
+{
+  if (!ctx || !center) return fail(PT_INVALID_ARG, "pt_material_set_texture: null argument");
+  Context& c = ctx->c;
+  if (material_id >= c.mats.size()) return fail(PT_INVALID_ARG, "pt_material_set_texture: no such material");
+  if (tex_id >= c.textures.size()) return fail(PT_INVALID_ARG, "pt_material_set_texture: no such texture");
+  MatDev& m = c.mats[material_id];
+  const TexDev& t = c.textures[tex_id];
+  if (m.type == PT_DIFFUSE_SHADER) {
+    if (t.ch != 3) return fail(PT_INVALID_ARG, "pt_material_set_texture: a diffuse albedo texture has 3 channels");
+  } else if (m.type == PT_METALLIC_SHADER) {
+    if (t.ch != 1) return fail(PT_INVALID_ARG, "pt_material_set_texture: a roughness texture has 1 channel");
+    if (m.model == PT_MULTISCATTERING_MODEL) return fail(PT_INVALID_ARG, "pt_material_set_texture: textured roughness supports the Walter and visible-normal models");
+  } else {
+    return fail(PT_INVALID_ARG, "pt_material_set_texture: only diffuse and metallic materials take a texture");
+  }
+  for (int k = 0; k < 3; ++k)
+    if (!std::isfinite(center[k])) return fail(PT_INVALID_ARG, "pt_material_set_texture: non-finite center");
+  m.tmap = make_float4(center[0], center[1], center[2], __int_as_float_host((int)tex_id));
+  c.dirty_materials = true;
+  return PT_OK;
+}
+
+pt_status pt_material_bind_sigma_grad(pt_ctx* ctx, uint32_t material_id, float* d_grad6)
+{
+  if (!ctx) return fail(PT_INVALID_ARG, "pt_material_bind_sigma_grad: null context");
+  Context& c = ctx->c;
+  if (material_id >= c.mats.size()) return fail(PT_INVALID_ARG, "pt_material_bind_sigma_grad: no such material");
+  if (c.mats[material_id].type != PT_TRANSLUCENT_SHADER) return fail(PT_INVALID_ARG, "pt_material_bind_sigma_grad: not a translucent material");
+  if (d_grad6 && c.mats[material_id].model != PT_STANDARD_DIPOLE)
+    return fail(PT_INVALID_ARG, "pt_material_bind_sigma_grad: gradients are implemented for the standard dipole");
+  c.mat_grad.resize(c.mats.size(), nullptr);
+  c.mat_grad[material_id] = d_grad6;
+  c.dirty_mat_grad = true;
+  return PT_OK;
+}
+
 pt_status pt_set_probe_count(pt_ctx* ctx, uint32_t samples)
 {
   if (!ctx) return fail(PT_INVALID_ARG, "null context");
@@ -653,6 +754,12 @@ pt_status pt_set_option(pt_ctx* ctx, const char* name, int64_t value)
 {
   if (!ctx || !name) return fail(PT_INVALID_ARG, "pt_set_option: null argument");
   std::string k(name);
+  if (k == "differentiable") {
+    if (value != 0 && value != 1) return fail(PT_INVALID_ARG, "pt_set_option: differentiable must be 0 or 1");
+    ctx->c.differentiable = value != 0;
+    ctx->c.adj_valid = false;
+    return PT_OK;
+  }
   if (k == "extend_mode") {
     if (value != 0 && value != 1) return fail(PT_INVALID_ARG, "pt_set_option: extend_mode must be 0 or 1");
     ctx->c.opt.extend_mode = (int)value;

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <memory>
 #include <vector>
 
 #include "pt_common.cuh"
@@ -46,6 +47,7 @@ struct Wavefront {
   uint64_t cap = 0;
   DevBuf ray_o, ray_d, thr, rad, rng, hit;   // per path
   DevBuf path_item;                           // per path: its item of the pass (uint16)
+  DevBuf adj_a, adj_b;                        // adjoint renders: per path image gradient and pending gradient
   DevBuf q_a, q_b;                            // active queues (path ids)
   DevBuf q_mat;                               // per-material-class queues, kQueues x cap
   DevBuf sh_o, sh_d, sh_c, sh_pid;            // shadow-ray queue
@@ -159,6 +161,20 @@ struct Context {
   DevBuf d_nodes, d_v0, d_e1, d_e2, d_info, d_normals, d_mats, d_lights, d_tri_lights;
   DevBuf d_scat, d_trans_objs, d_trans_pos;
   DevBuf d_scene_tab, d_item_tab;  // scene and item tables of the current pass (this context as the engine)
+  // differentiable renders: the forward state of the last render of frames [adj_first, +adj_frames)
+  bool differentiable = false;
+  DevBuf d_adj_L, d_adj_G;
+  uint32_t adj_first = 0, adj_frames = 0, adj_slots = 0;
+  bool adj_valid = false;
+  const float4* adj_dimg = nullptr;  // set while an adjoint render is being launched
+  float adj_dscale = 0.0f;
+  std::vector<float*> mat_grad;     // per material: sigma gradient buffer (6 floats) or null
+  DevBuf d_mat_grad;
+  bool dirty_mat_grad = true;
+  std::vector<TexDev> textures;     // bound textures (data in tex_own or caller-owned device memory)
+  std::vector<std::unique_ptr<DevBuf>> tex_own;
+  DevBuf d_tex;
+  bool dirty_textures = false;
   uint32_t next_frame = 0;         // first frame of the next render that does not name one (batches)
   DevBuf d_accum;  // float4 per pixel
   DevBuf d_env_tex, d_env_mpdf, d_env_mcdf, d_env_cpdf, d_env_ccdf, d_env_lum, d_env_mf;
@@ -186,7 +202,7 @@ pt_status prepare_scene(Context& c, const char* who);
 uint64_t scene_path_samples(const Context& c, uint32_t n_frames);
 PassLayout plan_pass(const std::vector<SceneFacts>& facts, const std::vector<ItemReq>& reqs, uint64_t max_paths);
 pt_status pass_resources(Context& E, const PassLayout& L, const std::vector<SceneDev>& scenes);
-pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool multi, bool allow_events);
+pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool multi, bool allow_events, bool adjoint = false);
 
 }  // namespace pt
 

@@ -67,6 +67,9 @@ struct WfDev {
   float4* g_b;
   float2* g_c;
   uint32_t g_slots;
+  // adjoint renders: per path (image gradient of the path, pending kind) and (pending d w / w, index)
+  float4* adj_a;
+  float4* adj_b;
   // the scenes and items of the pass; each path's item
   const SceneDev* scenes;
   const ItemDev* items;
@@ -266,8 +269,160 @@ __device__ void eval_direct(const SceneDev& S, const float3& pos, const LightRaw
   }
 }
 
+
+// ------------------------------------------------------------------ MD5 stream across vertices
+// The diffuse, conductor and rough-dielectric shaders hand their child ray only the tea seed
+// (diffuse_shader.cu:94-104, metallic_shader.cu:76-156, rough_transparent_shader.cu:114-220): their own
+// MD5 state is never updated from the child, so after such a vertex returns, the dipole gathers of the
+// translucent vertices above it draw from the MD5 state the vertex was entered with (the oracle passes
+// that state down to the child, which the reference leaves uninitialised).  The wavefront keeps one
+// running MD5 state per path and evaluates the gathers at the end, newest first; a vertex of those
+// shaders with gathers pending above it therefore pushes a reset marker holding its entry state,
+// which the gather evaluation restores when it reaches the marker.
+__device__ __forceinline__ uint32_t push_md5_reset(const WfDev& w, uint32_t pid, uint32_t meta, uint32_t s64x, uint32_t s64y, uint32_t& overflow)
+{
+  if (!(meta & META_PROBE) && (meta >> META_GSHIFT) != 0) {
+    const uint32_t slot = meta >> META_GSHIFT;
+    if (slot < w.g_slots) {
+      size_t at = (size_t)slot * w.cap + pid;
+      w.g_a[at] = make_float4(__uint_as_float(s64x), __uint_as_float(s64y), 0.0f, 0.0f);
+      w.g_b[at] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      w.g_c[at] = make_float2(0.0f, __int_as_float(-1));
+      meta += 1u << META_GSHIFT;
+    } else {
+      ++overflow;
+    }
+  }
+  return meta;
+}
+
+// ------------------------------------------------------------------ path replay backprop
+// The adjoint render replays every camera path with the same random numbers (same kernels, same
+// decisions) and differentiates the path's contribution with respect to the scene parameters,
+// with sampling detached: directions, Russian-roulette and acceptance decisions and their
+// probabilities are those of the forward render; only the weights and emissions that the parameters
+// enter are differentiated (M. Vicini, S. Speierer, W. Jakob, "Path replay backpropagation",
+// SIGGRAPH 2021).  With T_k the throughput at vertex k, w_k its weight and E_k what vertex k adds
+// to the path radiance L = sum_k T_k E_k:
+//   dL/dtheta = sum_k T_k dE_k/dtheta + (dw_k/dtheta / w_k) R_{k+1},   R_{k+1} = sum_{m>k} T_m E_m.
+// R starts as the forward render's L of the path and loses T_k E_k as the replay passes vertex k, so
+// nothing of the path is stored: a vertex leaves (dw/w, parameter) pending in the path state, and the
+// next kernel that handles the path -- after the shadow ray of the vertex has been resolved -- adds it
+// times the current R.  Each gradient is weighted by the path's image gradient dLoss/dL.
+enum PendingKind : uint32_t { PEND_NONE = 0, PEND_ALBEDO = 1, PEND_ROUGH = 2, PEND_SIGMA = 3 };
+constexpr uint32_t kNoTexel = 0xffffffffu;
+
+__device__ __forceinline__ void set_pending(const WfDev& w, uint32_t pid, uint32_t kind, uint32_t id, uint32_t index, const float3& d)
+{
+  float4 a = w.adj_a[pid];
+  w.adj_a[pid] = make_float4(a.x, a.y, a.z, __uint_as_float(kind | (id << 8)));
+  w.adj_b[pid] = make_float4(d.x, d.y, d.z, __uint_as_float(index));
+}
+
+// Adds the pending gradient of the path's previous vertex (R is the radiance collected beyond it).
+__device__ __forceinline__ void apply_pending(const SceneDev& S, const WfDev& w, uint32_t pid)
+{
+  float4 a = w.adj_a[pid];
+  const uint32_t kind = __float_as_uint(a.w);
+  if ((kind & 0xffu) == PEND_NONE) return;
+  const float4 b = w.adj_b[pid];
+  const float3 R = ld3(w.rad[pid]);
+  const uint32_t id = kind >> 8, idx = __float_as_uint(b.w);
+  switch (kind & 0xffu) {
+    case PEND_ALBEDO: {
+      float* g = S.tex[id].grad;
+      if (g) {
+        atomicAdd(g + 3 * idx, a.x * b.x * R.x);
+        atomicAdd(g + 3 * idx + 1, a.y * b.y * R.y);
+        atomicAdd(g + 3 * idx + 2, a.z * b.z * R.z);
+      }
+      break;
+    }
+    case PEND_ROUGH: {
+      float* g = S.tex[id].grad;
+      if (g) atomicAdd(g + idx, (a.x * R.x + a.y * R.y + a.z * R.z) * b.x);
+      break;
+    }
+    case PEND_SIGMA: {
+      float* g = S.mat_grad[id];
+      if (g) {
+        // b = d w / d sigma_a / w per channel; sigma_s' enters the extinction divided by (1 - g)
+        // (standard dipole) or times (1 + g) (delta-Eddington, directional dipole)
+        const float3 mc = S.scat[id].meancosine;
+        const bool dir = S.mats[id].model == DIRECTIONAL_DIPOLE;
+        const float3 k = dir ? f3(1.0f + mc.x, 1.0f + mc.y, 1.0f + mc.z) : f3(1.0f / (1.0f - mc.x), 1.0f / (1.0f - mc.y), 1.0f / (1.0f - mc.z));
+        const float3 ga = f3(a.x * b.x * R.x, a.y * b.y * R.y, a.z * b.z * R.z);
+        atomicAdd(g + 0, ga.x);
+        atomicAdd(g + 1, ga.y);
+        atomicAdd(g + 2, ga.z);
+        atomicAdd(g + 3, ga.x * k.x);
+        atomicAdd(g + 4, ga.y * k.y);
+        atomicAdd(g + 5, ga.z * k.z);
+      }
+      break;
+    }
+    default:
+      break;
+  }
+  w.adj_a[pid] = make_float4(a.x, a.y, a.z, __uint_as_float(PEND_NONE));
+}
+
+// d ln D / d alpha of the GGX distribution at microfacet normal m (ggx_distribution):
+// D = alpha^2 / (pi cos^4 (alpha^2 + tan^2)^2).
+__device__ __forceinline__ float ggx_dlnD(const float3& m, const float3& n, float alpha)
+{
+  float c = dot(m, n);
+  if (!(c > 0.0f)) return 0.0f;
+  float c2 = c * c, t2 = (1.0f - c2) / c2, a2 = alpha * alpha;
+  return 2.0f / alpha - 4.0f * alpha / (a2 + t2);
+}
+// d ln G1 / d alpha of the GGX Smith masking (ggx_G1_cos): G1 = 2 / (1 + sqrt(1 + alpha^2 tan^2)).
+__device__ __forceinline__ float ggx_dlnG1(const float3& v, const float3& n, float alpha)
+{
+  float c = dot(v, n);
+  float c2 = c * c, t2 = (1.0f - c2) / c2;
+  float q = sqrtf(1.0f + alpha * alpha * t2);
+  return -(alpha * t2 / q) / (1.0f + q);
+}
+
+// A value with its derivatives with respect to (sigma_a, sigma_s') of one channel.
+struct Dual2 {
+  float v, da, ds;
+};
+// The standard dipole of one channel (standard_dipole.h:8-29) and its derivatives with respect to the
+// channel's sigma_a and sigma_s' (before the material's scale; A depends on the ior only):
+// ln S_r = ln 3D + ln(1 + tr d_r) - tr d_r - 3 ln d_r, and likewise for the virtual source.
+__device__ __forceinline__ Dual2 dipole_channel_grad(float dist, float sa, float red_ext, float A, float scale)
+{
+  const float x = red_ext;             // sigma_t' (scaled)
+  const float D = 1.0f / (3.0f * x);
+  const float dD = -D / x * scale;     // d D / d sigma (either), sigma_t' = (sigma_s' + sigma_a) * scale
+  const float three_D = 3.0f * D, d3D = 3.0f * dD;
+  const float tr = sqrtf(sa / D);      // sqrt(3 sigma_a sigma_t')
+  const float dtr_a = 3.0f * scale * (x + sa) / (2.0f * tr), dtr_s = 3.0f * sa * scale / (2.0f * tr);
+  const float ext = 4.0f * A * D, dext = 4.0f * A * dD;
+  const float r2 = dist * dist;
+  const float dr2 = r2 + three_D * three_D, dr = sqrtf(dr2), ddr = three_D * d3D / dr;
+  const float dv2 = r2 + ext * ext, dv = sqrtf(dv2), ddv = ext * dext / dv;
+  const float cmf = three_D + ext, dcmf = d3D + dext;
+  const float trr = tr * dr, trv = tr * dv;
+  const float Sr = three_D * (1.0f + trr) / (dr2 * dr) * expf(-trr);
+  const float Sv = cmf * (1.0f + trv) / (dv2 * dv) * expf(-trv);
+  // d(tr d) for each of the two parameters
+  const float dtrr_a = dtr_a * dr + tr * ddr, dtrr_s = dtr_s * dr + tr * ddr;
+  const float dtrv_a = dtr_a * dv + tr * ddv, dtrv_s = dtr_s * dv + tr * ddv;
+  const float kr_a = d3D / three_D + dtrr_a / (1.0f + trr) - dtrr_a - 3.0f * ddr / dr;
+  const float kr_s = d3D / three_D + dtrr_s / (1.0f + trr) - dtrr_s - 3.0f * ddr / dr;
+  const float kv_a = dcmf / cmf + dtrv_a / (1.0f + trv) - dtrv_a - 3.0f * ddv / dv;
+  const float kv_s = dcmf / cmf + dtrv_s / (1.0f + trv) - dtrv_s - 3.0f * ddv / dv;
+  return Dual2{Sr + Sv, Sr * kr_a + Sv * kv_a, Sr * kr_s + Sv * kv_s};
+}
+
 // ------------------------------------------------------------------ kernels
 // path_tracer.cu:32-60: seed, jitter, pinhole direction; paths outside the patch are flagged.
+// kAdj: the adjoint replay; the path's radiance slot carries R (the forward radiance of the path, not
+// yet passed by the replay) and adj_a its image gradient.
+template <bool kAdj>
 __global__ void __launch_bounds__(kBlock) k_raygen(WfDev w, uint64_t n_paths)
 {
   __shared__ uint32_t sm[kWarps + 1];
@@ -278,7 +433,8 @@ __global__ void __launch_bounds__(kBlock) k_raygen(WfDev w, uint64_t n_paths)
     if (valid) {
       uint32_t k = find_item(w.items, w.n_items, pid, [](const ItemDev& it) { return it.path_begin; });
       const ItemDev& it = w.items[k];
-      const CameraDev& C = w.scenes[it.scene].cam;
+      const SceneDev& S = w.scenes[it.scene];
+      const CameraDev& C = S.cam;
       w.path_item[pid] = (uint16_t)k;
       uint64_t local = pid - it.path_begin;
       uint32_t fl = (uint32_t)(local / it.pixels), p = (uint32_t)(local % it.pixels);
@@ -296,7 +452,18 @@ __global__ void __launch_bounds__(kBlock) k_raygen(WfDev w, uint64_t n_paths)
         w.ray_o[pid] = make_float4(C.eye.x, C.eye.y, C.eye.z, 0.0f);
         w.ray_d[pid] = make_float4(dir.x, dir.y, dir.z, 0.0f);
         w.thr[pid] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-        w.rad[pid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if constexpr (kAdj) {
+          const uint64_t gp = (uint64_t)(frame - S.adj_first) * it.pixels + p;
+          const float4 L = S.adj_L[gp];
+          const float4 di = S.adj_dimg[p];
+          // the running mean skips non-finite samples (path_tracer.cu:64-68): no gradient through them
+          const bool fin = isfinite(L.x) && isfinite(L.y) && isfinite(L.z);
+          const float sc = fin ? S.adj_dscale : 0.0f;
+          w.rad[pid] = make_float4(L.x, L.y, L.z, 0.0f);
+          w.adj_a[pid] = make_float4(di.x * sc, di.y * sc, di.z * sc, __uint_as_float(PEND_NONE));
+        } else {
+          w.rad[pid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
         w.rng[pid] = make_uint4(seed, s64.x, s64.y, META_EMIT);
       } else {
         w.rad[pid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -447,8 +614,33 @@ __global__ void __launch_bounds__(kBlock) k_extend_persistent(SceneDev S0, WfDev
   if (lane == 0 && traced) atomicAdd(cnt64(w.cnt, CNT_SEGMENTS_LO), (unsigned long long)traced);
 }
 
+// Adds an unoccluded next-event estimate to the path (kAdj: takes it off R, and adds the albedo
+// texel's gradient: the estimate is linear in the albedo).
+template <bool kAdj>
+__device__ __forceinline__ void shadow_unoccluded(const SceneDev& S, const WfDev& w, uint32_t slot)
+{
+  const uint32_t p = w.sh_pid[slot];
+  const float4 c = w.sh_c[slot], r = w.rad[p];
+  if constexpr (kAdj) {
+    w.rad[p] = make_float4(r.x - c.x, r.y - c.y, r.z - c.z, 0.0f);
+    const uint32_t code = __float_as_uint(c.w);
+    if (code != kNoTexel) {
+      const TexDev& T = S.tex[code >> 24];
+      const uint32_t tx = code & 0xffffffu;
+      if (T.grad) {
+        const float4 a = w.adj_a[p];
+        atomicAdd(T.grad + 3 * tx, a.x * c.x / __ldg(T.data + 3 * tx));
+        atomicAdd(T.grad + 3 * tx + 1, a.y * c.y / __ldg(T.data + 3 * tx + 1));
+        atomicAdd(T.grad + 3 * tx + 2, a.z * c.z / __ldg(T.data + 3 * tx + 2));
+      }
+    }
+  } else {
+    w.rad[p] = make_float4(r.x + c.x, r.y + c.y, r.z + c.z, 0.0f);
+  }
+}
+
 // Persistent any-hit kernel for the shadow queue (same ray replacement).
-template <bool kMulti>
+template <bool kMulti, bool kAdj>
 __global__ void __launch_bounds__(kBlock) k_shadow_persistent(SceneDev S0, WfDev w, int refill)
 {
   const uint32_t n = w.cnt[CNT_SHADOW];
@@ -496,9 +688,8 @@ __global__ void __launch_bounds__(kBlock) k_shadow_persistent(SceneDev S0, WfDev
     }
     if (has && res != 0) {
       if (res < 0) {
-        uint32_t p = w.sh_pid[slot];
-        float4 c = w.sh_c[slot], r = w.rad[p];
-        w.rad[p] = make_float4(r.x + c.x, r.y + c.y, r.z + c.z, 0.0f);
+        if constexpr (kMulti) shadow_unoccluded<kAdj>(scene_of(w, w.sh_pid[slot]), w, slot);
+        else shadow_unoccluded<kAdj>(S0, w, slot);
       }
       has = false;
     }
@@ -508,6 +699,9 @@ __global__ void __launch_bounds__(kBlock) k_shadow_persistent(SceneDev S0, WfDev
 
 // constantbg.cu:16-19 / envmap_background.cu:20-23.  With the environment map registered as a light,
 // a miss after next-event estimation (emission disabled) adds nothing, as for area lights.
+// kAdj (all shade kernels): the adjoint replay; the first thing done for a path is adding the pending
+// gradient of its previous vertex, and what the forward adds to the path radiance is taken off R.
+template <bool kAdj>
 __global__ void __launch_bounds__(kBlock) k_shade_miss(WfDev w)
 {
   const uint32_t n = w.cnt[CNT_Q_MISS];
@@ -515,18 +709,20 @@ __global__ void __launch_bounds__(kBlock) k_shade_miss(WfDev w)
   for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
     uint32_t pid = q[i];
     const SceneDev& S = scene_of(w, pid);
+    if constexpr (kAdj) apply_pending(S, w, pid);
     float3 bg = S.bg_color;
     if (S.env.present) {
       if (S.env.is_light && !(w.rng[pid].w & META_EMIT)) continue;
       bg = env_lookup(S.env, ld3(w.ray_d[pid]));
     }
     float4 t = w.thr[pid], r = w.rad[pid];
-    float3 L = ld3(r) + ld3(t) * bg;
+    float3 L = kAdj ? ld3(r) - ld3(t) * bg : ld3(r) + ld3(t) * bg;
     w.rad[pid] = make_float4(L.x, L.y, L.z, 0.0f);
   }
 }
 
 // arealight_shader.cu:36-50: emitted radiance if the hit is front-facing and emission is enabled.
+template <bool kAdj>
 __global__ void __launch_bounds__(kBlock) k_shade_light(WfDev w)
 {
   const uint32_t n = w.cnt[CNT_Q_LIGHT];
@@ -534,6 +730,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_light(WfDev w)
   for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
     uint32_t pid = q[i];
     const SceneDev& S = scene_of(w, pid);
+    if constexpr (kAdj) apply_pending(S, w, pid);
     if (!(w.rng[pid].w & META_EMIT)) continue;
     float4 h = w.hit[pid], d = w.ray_d[pid];
     int prim = __float_as_int(h.w);
@@ -542,28 +739,33 @@ __global__ void __launch_bounds__(kBlock) k_shade_light(WfDev w)
     if (dot(normal, -ld3(d)) > 0.0f) {
       const MatDev& m = S.mats[info.w];
       float4 t = w.thr[pid], r = w.rad[pid];
-      float3 L = ld3(r) + ld3(t) * f3(m.a.x, m.a.y, m.a.z);
+      float3 L = kAdj ? ld3(r) - ld3(t) * f3(m.a.x, m.a.y, m.a.z) : ld3(r) + ld3(t) * f3(m.a.x, m.a.y, m.a.z);
       w.rad[pid] = make_float4(L.x, L.y, L.z, 0.0f);
     }
   }
 }
 
-// diffuse_shader.cu:122-187
+// diffuse_shader.cu:122-187.  Adjoint: an albedo texel's gradient through the next-event estimate
+// (resolved with the shadow ray) and through the bounce weight albedo / p (pending).
+template <bool kAdj>
 __global__ void __launch_bounds__(kBlock) k_shade_diffuse(WfDev w)
 {
   __shared__ uint32_t sm[kWarps + 1];
   const uint32_t n = w.cnt[CNT_Q_DIFFUSE];
   const uint32_t* q = w.q_mat + (size_t)QC_DIFFUSE * w.cap;
   uint32_t clamped = 0;
+  uint32_t overflow = 0;
   for (uint32_t base = blockIdx.x * kBlock; base < n; base += gridDim.x * kBlock) {
     uint32_t i = base + threadIdx.x;
     bool shadow = false, cont = false;
     uint32_t pid = 0;
     float3 hit_pos, w_l, sh_contrib;
     float sh_tmax = 0.0f, eps = 0.0f;
+    uint32_t texel_code = kNoTexel;
     if (i < n) {
       pid = q[i];
       const SceneDev& S = scene_of(w, pid);
+      if constexpr (kAdj) apply_pending(S, w, pid);
       eps = S.integ.scene_epsilon;
       uint4 rg = w.rng[pid];
       int depth = (int)(rg.w & META_DEPTH);
@@ -572,9 +774,16 @@ __global__ void __launch_bounds__(kBlock) k_shade_diffuse(WfDev w)
         int prim = __float_as_int(h.w);
         int4 info = __ldg(S.tri_info + prim);
         const MatDev& m = S.mats[info.w];
-        const float3 dc = f3(m.a.x, m.a.y, m.a.z);
         float3 d = ld3(d4);
         hit_pos = ld3(o) + h.x * d;
+        float3 dc = f3(m.a.x, m.a.y, m.a.z);
+        const int tid = __float_as_int(m.tmap.w);
+        if (tid >= 0) {  // albedo texture (nearest texel of the cube map)
+          const TexDev& T = S.tex[tid];
+          const uint32_t tx = cube_texel(hit_pos, ld3(m.tmap), T.w, T.h);
+          dc = f3(__ldg(T.data + 3 * tx), __ldg(T.data + 3 * tx + 1), __ldg(T.data + 3 * tx + 2));
+          texel_code = ((uint32_t)tid << 24) | tx;
+        }
         float3 normal = shading_normal(S, info, h.y, h.z, prim);
         float3 ffnormal = faceforward(normal, -d, normal);
         uint32_t t = rg.x;
@@ -609,30 +818,39 @@ __global__ void __launch_bounds__(kBlock) k_shade_diffuse(WfDev w)
           w.ray_d[pid] = make_float4(nd.x, nd.y, nd.z, 0.0f);
           w.thr[pid] = make_float4(nt.x, nt.y, nt.z, 0.0f);
           cont = true;
+          // weight albedo / p with p detached: d w / w = 1 / albedo per channel
+          if (kAdj && texel_code != kNoTexel)
+            set_pending(w, pid, PEND_ALBEDO, (uint32_t)tid, texel_code & 0xffffffu, f3(1.0f / dc.x, 1.0f / dc.y, 1.0f / dc.z));
         }
-        w.rng[pid] = make_uint4(t, rg.y, rg.z, (rg.w & META_KEEP) | (uint32_t)(depth + 1) | (emit ? META_EMIT : 0u));
+        const uint32_t meta = push_md5_reset(w, pid, rg.w & META_KEEP, rg.y, rg.z, overflow);
+        w.rng[pid] = make_uint4(t, rg.y, rg.z, meta | (uint32_t)(depth + 1) | (emit ? META_EMIT : 0u));
       }
     }
     uint32_t s_slot = block_slot(shadow, w.cnt + CNT_SHADOW, sm);
     if (shadow) {
       w.sh_o[s_slot] = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, eps);
       w.sh_d[s_slot] = make_float4(w_l.x, w_l.y, w_l.z, sh_tmax);
-      w.sh_c[s_slot] = make_float4(sh_contrib.x, sh_contrib.y, sh_contrib.z, 0.0f);
+      w.sh_c[s_slot] = make_float4(sh_contrib.x, sh_contrib.y, sh_contrib.z, __uint_as_float(texel_code));
       w.sh_pid[s_slot] = pid;
     }
     uint32_t c_slot = block_slot(cont, w.cnt + w.out_slot, sm);
     if (cont) w.q_out[c_slot] = pid;
   }
   if (clamped) atomicAdd(cnt64(w.cnt, CNT_CLAMPED), (unsigned long long)clamped);
+  if (overflow) atomicAdd(cnt64(w.cnt, CNT_ERROR), (unsigned long long)overflow);
 }
 
-// metallic_shader.cu:232-348
+// metallic_shader.cu:232-348.  Adjoint: a GGX roughness texel's gradient through the weight, with
+// the microfacet normal's sampling detached: d ln w / d alpha = d ln D(m) + d ln G1(wi) + d ln G1(wo)
+// for the Walter and the visible-normal models alike.
+template <bool kAdj>
 __global__ void __launch_bounds__(kBlock) k_shade_metal(WfDev w)
 {
   __shared__ uint32_t sm[kWarps + 1];
   const uint32_t n = w.cnt[CNT_Q_METAL];
   const uint32_t* q = w.q_mat + (size_t)QC_METAL * w.cap;
   uint32_t capped_total = 0;
+  uint32_t overflow = 0;
   for (uint32_t base = blockIdx.x * kBlock; base < n; base += gridDim.x * kBlock) {
     uint32_t i = base + threadIdx.x;
     bool cont = false;
@@ -640,6 +858,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_metal(WfDev w)
     if (i < n) {
       pid = q[i];
       const SceneDev& S = scene_of(w, pid);
+      if constexpr (kAdj) apply_pending(S, w, pid);
       uint4 rg = w.rng[pid];
       int depth = (int)(rg.w & META_DEPTH);
       if (depth < S.integ.max_depth) {
@@ -649,11 +868,19 @@ __global__ void __launch_bounds__(kBlock) k_shade_metal(WfDev w)
         const MatDev& m = S.mats[info.w];
         float3 d = ld3(d4);
         float3 hit_point = ld3(o) + h.x * d;
+        uint32_t rtexel = kNoTexel;
+        float3 mn_used = f3s(0.0f);
         float3 normal = shading_normal(S, info, h.y, h.z, prim);
         float3 ffnormal = faceforward(normal, -d, normal);
         float3 w_i = -d;
         uint32_t seed = rg.x;
         float a_x = m.a.x, a_y = m.a.y;
+        const int tid = __float_as_int(m.tmap.w);
+        if (tid >= 0) {  // isotropic roughness texture (nearest texel of the cube map)
+          const TexDev& T = S.tex[tid];
+          rtexel = cube_texel(hit_point, ld3(m.tmap), T.w, T.h);
+          a_x = a_y = __ldg(T.data + rtexel);
+        }
         int capped = 0;
         float3 w_o, weight;
         bool go = true;
@@ -680,6 +907,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_metal(WfDev w)
             G_o_m = (m.model == WALTER) ? masking_G1(m.dist, w_o, mn, ffnormal, a_x) : masking_G1_aniso(m.dist, w_o, mn, ffnormal, a_x, a_y);
             go = G_o_m > 0.0f;
             weight = (m.model == WALTER) ? F * (abs_i_m * G_i_m * G_o_m / (abs_i_n * abs_n_m)) : F * G_o_m;
+            mn_used = mn;
           }
         }
         capped_total += capped;
@@ -690,23 +918,32 @@ __global__ void __launch_bounds__(kBlock) k_shade_metal(WfDev w)
           w.ray_d[pid] = make_float4(w_o.x, w_o.y, w_o.z, 0.0f);
           w.thr[pid] = make_float4(nt.x, nt.y, nt.z, 0.0f);
           cont = true;
+          if (kAdj && rtexel != kNoTexel && m.model != MULTISCATTERING && m.dist == GGX) {
+            const float dl = ggx_dlnD(mn_used, ffnormal, a_x) + ggx_dlnG1(w_i, ffnormal, a_x) + ggx_dlnG1(w_o, ffnormal, a_x);
+            set_pending(w, pid, PEND_ROUGH, (uint32_t)tid, rtexel, f3s(dl));
+          }
         }
-        w.rng[pid] = make_uint4(seed, rg.y, rg.z, (rg.w & META_KEEP) | (uint32_t)(depth + 1) | META_EMIT);
+        const uint32_t meta = push_md5_reset(w, pid, rg.w & META_KEEP, rg.y, rg.z, overflow);
+        w.rng[pid] = make_uint4(seed, rg.y, rg.z, meta | (uint32_t)(depth + 1) | META_EMIT);
       }
     }
     uint32_t c_slot = block_slot(cont, w.cnt + w.out_slot, sm);
     if (cont) w.q_out[c_slot] = pid;
   }
   if (capped_total) atomicAdd(cnt64(w.cnt, CNT_CAPPED), (unsigned long long)capped_total);
+  if (overflow) atomicAdd(cnt64(w.cnt, CNT_ERROR), (unsigned long long)overflow);
 }
 
-// rough_transparent_shader.cu:66-225
+// rough_transparent_shader.cu:66-225 (no parameters to differentiate: the adjoint only settles the
+// pending gradient of the previous vertex)
+template <bool kAdj>
 __global__ void __launch_bounds__(kBlock) k_shade_glass(WfDev w)
 {
   __shared__ uint32_t sm[kWarps + 1];
   const uint32_t n = w.cnt[CNT_Q_GLASS];
   const uint32_t* q = w.q_mat + (size_t)QC_GLASS * w.cap;
   uint32_t capped_total = 0;
+  uint32_t overflow = 0;
   for (uint32_t base = blockIdx.x * kBlock; base < n; base += gridDim.x * kBlock) {
     uint32_t i = base + threadIdx.x;
     bool cont = false;
@@ -714,6 +951,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_glass(WfDev w)
     if (i < n) {
       pid = q[i];
       const SceneDev& S = scene_of(w, pid);
+      if constexpr (kAdj) apply_pending(S, w, pid);
       uint4 rg = w.rng[pid];
       int depth = (int)(rg.w & META_DEPTH);
       if (depth < S.integ.max_depth) {
@@ -780,13 +1018,15 @@ __global__ void __launch_bounds__(kBlock) k_shade_glass(WfDev w)
           w.thr[pid] = make_float4(nt.x, nt.y, nt.z, 0.0f);
           cont = true;
         }
-        w.rng[pid] = make_uint4(t, rg.y, rg.z, (rg.w & META_KEEP) | (uint32_t)(depth + 1) | META_EMIT);
+        const uint32_t meta = push_md5_reset(w, pid, rg.w & META_KEEP, rg.y, rg.z, overflow);
+        w.rng[pid] = make_uint4(t, rg.y, rg.z, meta | (uint32_t)(depth + 1) | META_EMIT);
       }
     }
     uint32_t c_slot = block_slot(cont, w.cnt + w.out_slot, sm);
     if (cont) w.q_out[c_slot] = pid;
   }
   if (capped_total) atomicAdd(cnt64(w.cnt, CNT_CAPPED), (unsigned long long)capped_total);
+  if (overflow) atomicAdd(cnt64(w.cnt, CNT_ERROR), (unsigned long long)overflow);
 }
 
 // ------------------------------------------------------------------ translucent objects
@@ -800,6 +1040,11 @@ __global__ void __launch_bounds__(kBlock) k_shade_glass(WfDev w)
 // gather stack and evaluated in last-in first-out order when the path has ended (k_gather).  A
 // probe's indirect path does not gather: in the reference it would read the probe buffer that its
 // own launch is writing.
+//
+// Adjoint: the gather a camera path owes at an entry vertex is taken off R there (its forward value
+// was stored with the path); its gradient is added at the end (k_gather_adj).  Inside, the weight
+// beam_T / p has p detached: d w / d sigma_a / w = -t * scale per channel.
+template <bool kAdj>
 __global__ void __launch_bounds__(kBlock) k_shade_translucent(WfDev w)
 {
   __shared__ uint32_t sm[kWarps + 1];
@@ -813,6 +1058,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_translucent(WfDev w)
     if (i < n) {
       pid = q[i];
       const SceneDev& S = scene_of(w, pid);
+      if constexpr (kAdj) apply_pending(S, w, pid);
       uint4 rg = w.rng[pid];
       int depth = (int)(rg.w & META_DEPTH);
       if (depth <= S.integ.max_depth) {
@@ -864,6 +1110,14 @@ __global__ void __launch_bounds__(kBlock) k_shade_translucent(WfDev w)
                 w.g_a[at] = make_float4(xo.x, xo.y, xo.z, t4.x);
                 w.g_b[at] = make_float4(no.x, no.y, no.z, t4.y);
                 w.g_c[at] = make_float2(t4.z, __int_as_float(info.w));
+                if constexpr (kAdj) {
+                  const ItemDev& it = w.items[w.path_item[pid]];
+                  const uint64_t local = pid - it.path_begin;
+                  const uint64_t gp = (uint64_t)(it.first_frame + (uint32_t)(local / it.pixels) - S.adj_first) * it.pixels + local % it.pixels;
+                  const float4 G = S.adj_G[gp * S.adj_slots + slot];
+                  const float4 r = w.rad[pid];
+                  w.rad[pid] = make_float4(r.x - t4.x * G.x, r.y - t4.y * G.y, r.z - t4.z * G.z, 0.0f);
+                }
                 meta += 1u << META_GSHIFT;
               } else {
                 ++overflow;
@@ -877,6 +1131,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_translucent(WfDev w)
           w.ray_d[pid] = make_float4(nd.x, nd.y, nd.z, 0.0f);
           w.thr[pid] = make_float4(nt.x, nt.y, nt.z, 0.0f);
           cont = true;
+          if (kAdj && inside) set_pending(w, pid, PEND_SIGMA, (uint32_t)info.w, 0u, f3s(-h.x * m.a.x));
         }
         w.rng[pid] = make_uint4(rg.x, t64.x, t64.y, meta | (uint32_t)(depth + 1) | META_EMIT);
       }
@@ -910,6 +1165,11 @@ __global__ void __launch_bounds__(kBlock) k_gather_collect(WfDev w, uint64_t n_p
 // on one MD5 draw, and on acceptance T12 * L * S(probe, xo) / p with the standard or directional
 // dipole.  The sum times global_coeff / samples is added to the path's radiance, weighted by the
 // throughput at the vertex.  One thread per path: the MD5 stream is one sequential chain.
+//
+// A differentiable forward render also stores each gather's value with the path (adj_G).  kAdj: the
+// same gathers replayed (same MD5 chain) for the gradient of the standard dipole with respect to the
+// material's sigma_a and sigma_s' per channel; the acceptance probability exp_term is detached.
+template <bool kAdj>
 __global__ void __launch_bounds__(kBlock) k_gather(WfDev w, SssDev g, const uint32_t* list)
 {
   const uint32_t n = w.cnt[CNT_GATHER];
@@ -923,12 +1183,19 @@ __global__ void __launch_bounds__(kBlock) k_gather(WfDev w, SssDev g, const uint
     uint32_t fl = (uint32_t)((pid - it.path_begin) / it.pixels);
     float4 r4 = w.rad[pid];
     float3 L = ld3(r4);
+    const uint64_t gp = S.adj_G ? (uint64_t)(it.first_frame + fl - S.adj_first) * it.pixels + (pid - it.path_begin) % it.pixels : 0;
+    float3 dl = f3s(0.0f);
+    if constexpr (kAdj) dl = ld3(w.adj_a[pid]);
     for (int slot = (int)(rg.w >> META_GSHIFT) - 1; slot >= 0; --slot) {
       size_t at = (size_t)slot * w.cap + pid;
       float4 a = w.g_a[at], b = w.g_b[at];
       float2 c = w.g_c[at];
-      const float3 xo = ld3(a), no = ld3(b), thr = f3(a.w, b.w, c.x);
       const int mat = __float_as_int(c.y);
+      if (mat < 0) {  // reset marker: the MD5 state the vertex below was entered with
+        t64 = make_uint2(__float_as_uint(a.x), __float_as_uint(a.y));
+        continue;
+      }
+      const float3 xo = ld3(a), no = ld3(b), thr = f3(a.w, b.w, c.x);
       const MatDev& m = S.mats[mat];
       const ScatDev& P = S.scat[mat];
       const uint32_t set_in_item = fl * S.n_trans + m.aux;
@@ -936,7 +1203,35 @@ __global__ void __launch_bounds__(kBlock) k_gather(WfDev w, SssDev g, const uint
       const uint32_t nc = g.pc_cnt[it.set_begin + set_in_item];
       const float chosen = fminf(P.transport.x, fminf(P.transport.y, P.transport.z));
       float3 acc = f3s(0.0f);
-      if (m.model == DIRECTIONAL_DIPOLE) {
+      if constexpr (kAdj) {
+        // standard dipole only (pt_render_adjoint rejects the directional one)
+        float* gr = S.mat_grad[mat];
+        float3 ga = f3s(0.0f), gs = f3s(0.0f);
+        const float scale = m.a.x;
+        const float3 sa = P.absorption, rx = P.reducedExtinction, A = P.A;
+        for (uint32_t k = 0; k < nc; ++k) {
+          float3 pos = ld3(__ldg(g.pc_pos + pb + k));
+          float dist = length(xo - pos);
+          float exp_term = expf(-dist * chosen);
+          if (rnd_md5(t64) < exp_term) {
+            float3 wl = ld3(__ldg(g.pc_wl + pb + k));
+            Dual2 sx = dipole_channel_grad(dist, sa.x, rx.x, A.x, scale);
+            Dual2 sy = dipole_channel_grad(dist, sa.y, rx.y, A.y, scale);
+            Dual2 sz = dipole_channel_grad(dist, sa.z, rx.z, A.z, scale);
+            ga = ga + wl * f3(sx.da, sy.da, sz.da) / exp_term;
+            gs = gs + wl * f3(sx.ds, sy.ds, sz.ds) / exp_term;
+          }
+        }
+        if (gr) {
+          const float3 f = dl * thr * P.global_coeff / (float)S.probe_samples;
+          atomicAdd(gr + 0, f.x * ga.x);
+          atomicAdd(gr + 1, f.y * ga.y);
+          atomicAdd(gr + 2, f.z * ga.z);
+          atomicAdd(gr + 3, f.x * gs.x);
+          atomicAdd(gr + 4, f.y * gs.y);
+          atomicAdd(gr + 5, f.z * gs.z);
+        }
+      } else if (m.model == DIRECTIONAL_DIPOLE) {
         for (uint32_t k = 0; k < nc; ++k) {
           float3 pos = ld3(__ldg(g.pc_pos + pb + k));
           float dist = length(xo - pos);
@@ -959,12 +1254,15 @@ __global__ void __launch_bounds__(kBlock) k_gather(WfDev w, SssDev g, const uint
           }
         }
       }
-      float3 contrib = acc * P.global_coeff / (float)S.probe_samples;
-      L = L + thr * contrib;
+      if constexpr (!kAdj) {
+        float3 contrib = acc * P.global_coeff / (float)S.probe_samples;
+        L = L + thr * contrib;
+        if (S.adj_G) S.adj_G[gp * S.adj_slots + slot] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+      }
       pairs += nc;
       ++gathers;
     }
-    w.rad[pid] = make_float4(L.x, L.y, L.z, r4.w);
+    if constexpr (!kAdj) w.rad[pid] = make_float4(L.x, L.y, L.z, r4.w);
     w.rng[pid] = make_uint4(rg.x, t64.x, t64.y, rg.w);
   }
   if (pairs) atomicAdd(cnt64(w.cnt, CNT_PAIRS), pairs);
@@ -1137,16 +1435,15 @@ __global__ void __launch_bounds__(256) k_probe_compact(WfDev w, SssDev g)
 }
 
 // Shadow rays of diffuse_shader.cu:149-161 (every material's any-hit program is opaque).
+template <bool kAdj>
 __global__ void __launch_bounds__(kBlock) k_shadow(WfDev w)
 {
   const uint32_t n = w.cnt[CNT_SHADOW];
   for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
     float4 o = w.sh_o[i], d = w.sh_d[i];
     uint32_t pid = w.sh_pid[i];
-    if (!trace_any(trav_geom(scene_of(w, pid)), ld3(o), ld3(d), o.w, d.w)) {
-      float4 c = w.sh_c[i], r = w.rad[pid];
-      w.rad[pid] = make_float4(r.x + c.x, r.y + c.y, r.z + c.z, 0.0f);
-    }
+    const SceneDev& S = scene_of(w, pid);
+    if (!trace_any(trav_geom(S), ld3(o), ld3(d), o.w, d.w)) shadow_unoccluded<kAdj>(S, w, i);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && n) atomicAdd(cnt64(w.cnt, CNT_SHADOW_TOTAL), (unsigned long long)n);
 }
@@ -1158,11 +1455,13 @@ __global__ void __launch_bounds__(kBlock) k_accumulate(WfDev w, uint64_t n_pix)
   for (uint64_t q = (uint64_t)blockIdx.x * kBlock + threadIdx.x; q < n_pix; q += (uint64_t)gridDim.x * kBlock) {
     const ItemDev& it = w.items[find_item(w.items, w.n_items, q, [](const ItemDev& x) { return x.pix_begin; })];
     const uint32_t p = (uint32_t)(q - it.pix_begin);
-    float4* accum = w.scenes[it.scene].accum;
+    const SceneDev& S = w.scenes[it.scene];
+    float4* accum = S.accum;
     float4 out = accum[p];
     for (uint32_t fl = 0; fl < it.n_frames; ++fl) {
       uint64_t pid = it.path_begin + (uint64_t)fl * it.pixels + p;
       uint32_t frame = it.first_frame + fl;
+      if (S.adj_L) S.adj_L[(uint64_t)(frame - S.adj_first) * it.pixels + p] = w.rad[pid];
       if (w.rng[pid].w & META_OUTSIDE) {
         out = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
         continue;
@@ -1252,6 +1551,13 @@ static pt_status ensure_sss(Context& c, uint64_t cap, uint32_t slots, uint64_t r
   return wf.pc_cnt.reserve(std::max<uint64_t>(sets, 1) * 4, "probe counts");
 }
 
+static int __float_as_int_host(float f)
+{
+  int i;
+  memcpy(&i, &f, 4);
+  return i;
+}
+
 // Checks a scene before it is rendered and brings its device state up to date on its own stream:
 // changed materials, and the geometric normals (once per build).
 pt_status prepare_scene(Context& c, const char* who)
@@ -1270,6 +1576,23 @@ pt_status prepare_scene(Context& c, const char* who)
     return fail(PT_NOT_READY, std::string(who) + ": translucent objects need at least one light (the probe pass samples light_buffer)");
   if (sss && c.integ.max_depth > 254)
     return fail(PT_CAP_EXCEEDED, std::string(who) + ": translucent objects support max_depth <= 254 (the gather stack holds 255 entries)");
+  if (c.dirty_mat_grad || c.mat_grad.size() != c.mats.size()) {
+    c.mat_grad.resize(c.mats.size(), nullptr);
+    pt_status st = c.d_mat_grad.reserve(std::max<size_t>(c.mats.size(), 1) * sizeof(float*), "gradient table");
+    if (st != PT_OK) return st;
+    if (!c.mat_grad.empty())
+      PT_CHECK_CUDA(cudaMemcpyAsync(c.d_mat_grad.p, c.mat_grad.data(), c.mat_grad.size() * sizeof(float*), cudaMemcpyHostToDevice, c.stream),
+                    "gradient table");
+    c.dirty_mat_grad = false;
+  }
+  if (c.dirty_textures) {
+    pt_status st = c.d_tex.reserve(std::max<size_t>(c.textures.size(), 1) * sizeof(TexDev), "texture table");
+    if (st != PT_OK) return st;
+    if (!c.textures.empty())
+      PT_CHECK_CUDA(cudaMemcpyAsync(c.d_tex.p, c.textures.data(), c.textures.size() * sizeof(TexDev), cudaMemcpyHostToDevice, c.stream),
+                    "texture table");
+    c.dirty_textures = false;
+  }
   if (c.dirty_materials) {
     PT_CHECK_CUDA(cudaMemcpyAsync(c.d_mats.p, c.mats.data(), c.mats.size() * sizeof(MatDev), cudaMemcpyHostToDevice, c.stream), "material upload");
     PT_CHECK_CUDA(cudaMemcpyAsync(c.d_scat.p, c.scat.data(), c.scat.size() * sizeof(ScatDev), cudaMemcpyHostToDevice, c.stream),
@@ -1378,7 +1701,7 @@ pt_status pass_resources(Context& E, const PassLayout& L, const std::vector<Scen
 // the camera paths, the deferred gathers and the accumulation.  Only kernel launches and memsets of
 // device state: the whole sequence can be captured into a CUDA graph.  multi: the pass spans
 // several scenes (the traversal kernels then read each ray's scene from the table; otherwise S0).
-pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool multi, bool allow_events)
+pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool multi, bool allow_events, bool adjoint)
 {
   Context& c = E;
   WfDev w;
@@ -1402,6 +1725,8 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
   w.g_slots = L.sss ? wf.gather_slots : 0;
   w.scenes = c.d_scene_tab.as<SceneDev>();
   w.path_item = wf.path_item.as<uint16_t>();
+  w.adj_a = adjoint ? wf.adj_a.as<float4>() : nullptr;
+  w.adj_b = adjoint ? wf.adj_b.as<float4>() : nullptr;
   SssDev g;
   memset(&g, 0, sizeof(g));
   if (L.sss) {
@@ -1416,10 +1741,10 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
   int occ_ext = 0, occ_sh = 0;
   if (multi) {
     PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, k_extend_persistent<true>, kBlock, 0), "occupancy");
-    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, k_shadow_persistent<true>, kBlock, 0), "occupancy");
+    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, k_shadow_persistent<true, false>, kBlock, 0), "occupancy");
   } else {
     PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, k_extend_persistent<false>, kBlock, 0), "occupancy");
-    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, k_shadow_persistent<false>, kBlock, 0), "occupancy");
+    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, k_shadow_persistent<false, false>, kBlock, 0), "occupancy");
   }
   const int grid_persist = sm_count() * std::max(1, std::min(occ_ext, occ_sh));
   const bool prof = c.profile && allow_events;
@@ -1454,7 +1779,8 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
     return PT_OK;
   };
   // L.passes = max_depth + 2 bounces: every path has ended by then (each shader stops at max_depth).
-  auto bounces = [&]() -> pt_status {
+  auto bounces = [&](bool adj_pass) -> pt_status {
+    const bool adjoint = adj_pass;
     for (int b = 0; b < L.passes; ++b) {
       PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_Q_MISS, 0, (CNT_FETCH_SH - CNT_Q_MISS + 1) * 4, c.stream), "reset queues");
       PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + w.out_slot, 0, 4, c.stream), "reset queues");
@@ -1466,21 +1792,33 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
         k_extend<<<grid_trace, kBlock, 0, c.stream>>>(w);
       }
       if ((st = prof_end()) != PT_OK) return st;
-      k_shade_miss<<<grid_shade, kBlock, 0, c.stream>>>(w);
-      k_shade_light<<<grid_shade, kBlock, 0, c.stream>>>(w);
-      k_shade_diffuse<<<grid_shade, kBlock, 0, c.stream>>>(w);
-      k_shade_metal<<<grid_shade, kBlock, 0, c.stream>>>(w);
-      k_shade_glass<<<grid_shade, kBlock, 0, c.stream>>>(w);
+      if (adjoint) {
+        k_shade_miss<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
+        k_shade_light<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
+        k_shade_diffuse<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
+        k_shade_metal<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
+        k_shade_glass<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
+      } else {
+        k_shade_miss<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
+        k_shade_light<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
+        k_shade_diffuse<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
+        k_shade_metal<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
+        k_shade_glass<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
+      }
       count_launch(6);
       if (L.sss) {
-        k_shade_translucent<<<grid_shade, kBlock, 0, c.stream>>>(w);
+        if (adjoint) k_shade_translucent<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
+        else k_shade_translucent<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
         count_launch();
       }
       if (c.opt.extend_mode == 1) {
-        if (multi) k_shadow_persistent<true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-        else k_shadow_persistent<false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+        if (multi && adjoint) k_shadow_persistent<true, true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+        else if (multi) k_shadow_persistent<true, false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+        else if (adjoint) k_shadow_persistent<false, true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+        else k_shadow_persistent<false, false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
       } else {
-        k_shadow<<<grid_trace, kBlock, 0, c.stream>>>(w);
+        if (adjoint) k_shadow<true><<<grid_trace, kBlock, 0, c.stream>>>(w);
+        else k_shadow<false><<<grid_trace, kBlock, 0, c.stream>>>(w);
       }
       count_launch();
       ++c.stats.extend_launches;
@@ -1503,7 +1841,7 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
         if ((st = reset_queues()) != PT_OK) return st;
         k_probe_gen<<<grid_for(nj, kBlock, 16), kBlock, 0, c.stream>>>(w, g, j0, nj);
         count_launch();
-        if ((st = bounces()) != PT_OK) return st;
+        if ((st = bounces(false)) != PT_OK) return st;
         k_probe_finish<<<grid_for(nj, kBlock, 16), kBlock, 0, c.stream>>>(w, g, j0, nj);
         count_launch();
       }
@@ -1511,20 +1849,24 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
       count_launch();
     }
     if ((st = reset_queues()) != PT_OK) return st;
-    k_raygen<<<grid_for(n_paths, kBlock, 16), kBlock, 0, c.stream>>>(w, n_paths);
+    if (adjoint) k_raygen<true><<<grid_for(n_paths, kBlock, 16), kBlock, 0, c.stream>>>(w, n_paths);
+    else k_raygen<false><<<grid_for(n_paths, kBlock, 16), kBlock, 0, c.stream>>>(w, n_paths);
     count_launch();
-    if ((st = bounces()) != PT_OK) return st;
+    if ((st = bounces(adjoint)) != PT_OK) return st;
     if (n_probes) {
       PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_GATHER, 0, 4, c.stream), "reset gather list");
       uint32_t* list = wf.q_a.as<uint32_t>();
       k_gather_collect<<<grid_for(n_paths, kBlock, 16), kBlock, 0, c.stream>>>(w, n_paths, list);
       if ((st = prof_begin(PROF_GATHER)) != PT_OK) return st;
-      k_gather<<<grid_shade, kBlock, 0, c.stream>>>(w, g, list);
+      if (adjoint) k_gather<true><<<grid_shade, kBlock, 0, c.stream>>>(w, g, list);
+      else k_gather<false><<<grid_shade, kBlock, 0, c.stream>>>(w, g, list);
       if ((st = prof_end()) != PT_OK) return st;
       count_launch(2);
     }
-    k_accumulate<<<grid_for(L.chunk_pixels[k], kBlock, 16), kBlock, 0, c.stream>>>(w, L.chunk_pixels[k]);
-    count_launch();
+    if (!adjoint) {
+      k_accumulate<<<grid_for(L.chunk_pixels[k], kBlock, 16), kBlock, 0, c.stream>>>(w, L.chunk_pixels[k]);
+      count_launch();
+    }
   }
   PT_CHECK_CUDA(cudaGetLastError(), "render launch");
   return PT_OK;
@@ -1548,6 +1890,18 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
   f.n_trans = (uint32_t)c.trans_objs.size();
   f.samples = c.probe_samples;
   f.max_depth = c.integ.max_depth;
+  if (c.differentiable) {
+    // keep what the adjoint needs: each path's radiance and the value of each of its gathers
+    const uint64_t n = (uint64_t)n_frames * f.pixels;
+    const uint32_t slots = f.n_trans ? (uint32_t)f.max_depth + 1 : 0;
+    if (n * (1 + slots) * sizeof(float4) > (16ull << 30)) return fail(PT_CAP_EXCEEDED, "pt_render_frames: differentiable state above 16 GiB");
+    if ((st = c.d_adj_L.reserve(n * sizeof(float4), "adjoint path radiance")) != PT_OK) return st;
+    if (slots && (st = c.d_adj_G.reserve(n * slots * sizeof(float4), "adjoint gather values")) != PT_OK) return st;
+    c.adj_first = first_frame;
+    c.adj_frames = n_frames;
+    c.adj_slots = slots;
+    c.adj_valid = true;
+  }
   PassLayout L = plan_pass({f}, {ItemReq{0, first_frame, n_frames}}, c.max_paths);
   std::vector<SceneDev> scenes{c.view()};
   if ((st = pass_resources(c, L, scenes)) != PT_OK) return st;
@@ -1562,6 +1916,43 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
   // the probe buffer of the last chunk holds the last frames of this scene
   c.probe_last_frames = L.items.empty() ? 0 : L.items.back().n_frames;
   c.next_frame = first_frame + n_frames;
+  return PT_OK;
+}
+
+pt_status pt_render_adjoint(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames, const float* d_dimage)
+{
+  if (!ctx || !d_dimage) return fail(PT_INVALID_ARG, "pt_render_adjoint: null argument");
+  Context& c = ctx->c;
+  if (!c.differentiable || !c.adj_valid) return fail(PT_NOT_READY, "pt_render_adjoint: needs a forward pt_render_frames with the differentiable option on");
+  if (first_frame != c.adj_first || n_frames != c.adj_frames)
+    return fail(PT_INVALID_ARG, "pt_render_adjoint: frames differ from the last differentiable forward render");
+  for (const MatDev& m : c.mats)
+    if (m.type == PT_METALLIC_SHADER && __float_as_int_host(m.tmap.w) >= 0 && m.dist != PT_GGX_DISTRIBUTION)
+      return fail(PT_INVALID_ARG, "pt_render_adjoint: roughness gradients are implemented for the GGX distribution");
+  pt_status st = prepare_scene(c, "pt_render_adjoint");
+  if (st != PT_OK) return st;
+  SceneFacts f;
+  f.pixels = c.cam.width * c.cam.height;
+  f.n_trans = (uint32_t)c.trans_objs.size();
+  f.samples = c.probe_samples;
+  f.max_depth = c.integ.max_depth;
+  PassLayout L = plan_pass({f}, {ItemReq{0, first_frame, n_frames}}, c.max_paths);
+  c.adj_dimg = (const float4*)d_dimage;
+  c.adj_dscale = 1.0f / (float)((uint64_t)first_frame + n_frames);
+  std::vector<SceneDev> scenes{c.view()};
+  c.adj_dimg = nullptr;
+  c.adj_dscale = 0.0f;
+  if ((st = pass_resources(c, L, scenes)) != PT_OK) return st;
+  if ((st = c.wf.adj_a.reserve(c.wf.cap * sizeof(float4), "adjoint path state")) != PT_OK) return st;
+  if ((st = c.wf.adj_b.reserve(c.wf.cap * sizeof(float4), "adjoint path state")) != PT_OK) return st;
+  uint64_t launches0 = pt_kernel_launch_count();
+  memset(&c.stats, 0, sizeof(c.stats));
+  PT_CHECK_CUDA(cudaEventRecord(c.ev0, c.stream), "event");
+  if ((st = launch_pass(c, L, scenes[0], false, true, true)) != PT_OK) return st;
+  PT_CHECK_CUDA(cudaEventRecord(c.ev1, c.stream), "event");
+  c.stats.path_samples = scene_path_samples(c, n_frames);
+  c.stats.kernel_launches = (uint32_t)(pt_kernel_launch_count() - launches0);
+  c.stats_pending = true;
   return PT_OK;
 }
 

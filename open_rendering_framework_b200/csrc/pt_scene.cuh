@@ -61,7 +61,41 @@ struct __align__(16) MatDev {
   float4 b;   // glass: absorption.xyz
   Cx3 eta;    // metal: 1 / ior (metallic_shader.cu:61), computed on the host
   Cx3 inv_eta;// metal: 1 / eta (the walk's inside branch)
+  float4 tmap;// texture: cube-map center xyz, texture id in w (int bits, -1 = none)
 };
+
+// A float texture (1 or 3 channels), texel (x, y) channel c at data[(y * w + x) * ch + c], and the
+// buffer its gradient accumulates into (adjoint renders; may be null).
+struct TexDev {
+  const float* data;
+  float* grad;
+  uint32_t w, h, ch, pad;
+};
+
+// Nearest texel of a cube map around c, the six faces laid out 3 x 2 in the texture: the largest
+// component of p - c picks the face, the other two divided by it give the face coordinates.
+// Divisions, comparisons and truncations only, so host and device pick the same texel.
+PT_HD uint32_t cube_texel(const float3& p, const float3& c, uint32_t w, uint32_t h)
+{
+  float3 d = p - c;
+  float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+  uint32_t face;
+  float s, t, m;
+  if (ax >= ay && ax >= az) { face = d.x >= 0.0f ? 0u : 1u; m = ax; s = d.z; t = d.y; }
+  else if (ay >= az) { face = d.y >= 0.0f ? 2u : 3u; m = ay; s = d.x; t = d.z; }
+  else { face = d.z >= 0.0f ? 4u : 5u; m = az; s = d.x; t = d.y; }
+  float u = 0.5f, v = 0.5f;
+  if (m > 0.0f) {
+    u = 0.5f * (s / m + 1.0f);
+    v = 0.5f * (t / m + 1.0f);
+  }
+  const uint32_t fw = w / 3u, fh = h / 2u;
+  float fu = u * (float)fw, fv = v * (float)fh;
+  uint32_t x = fu > 0.0f ? (uint32_t)fu : 0u, y = fv > 0.0f ? (uint32_t)fv : 0u;
+  if (x >= fw) x = fw - 1u;
+  if (y >= fh) y = fh - 1u;
+  return ((face / 3u) * fh + y) * w + (face % 3u) * fw + x;
+}
 
 // ScatteringMaterialProperties, structs.h:116-144 (260 bytes), one per material id (filled for
 // translucent materials).
@@ -115,6 +149,7 @@ struct SceneDev {
   const float4* geo;    // per original triangle: cross(v1 - v0, v2 - v0), unnormalised
   const MatDev* mats;
   const ScatDev* scat;  // per material id
+  const TexDev* tex;    // textures (diffuse albedo, conductor roughness)
   const LightRaw* lights;
   const TriLightRaw* tri_lights;
   int n_lights, n_tri_lights;
@@ -129,6 +164,17 @@ struct SceneDev {
   const uint4* trans_objs;
   const float* trans_pos;
   uint32_t n_trans, probe_samples;
+  // differentiable renders: per camera path of frames [adj_first, adj_first + adj_frames), its radiance
+  // (adj_L) and the value of each of its dipole gathers (adj_G, adj_slots per path), written by the
+  // forward render and read by the adjoint; the image gradient dLoss/d(running mean) and its factor
+  // d(running mean)/d(path radiance); per material, the buffer of 6 floats that the gradient of a
+  // translucent material's (sigma_a, sigma_s') per RGB channel accumulates into (or null)
+  float4* adj_L;
+  float4* adj_G;
+  uint32_t adj_first, adj_frames, adj_slots;
+  const float4* adj_dimg;
+  float adj_dscale;
+  float* const* mat_grad;
 };
 // The traversal's view of a scene (the four arrays it reads), held in registers by kernels that
 // trace rays of several scenes.

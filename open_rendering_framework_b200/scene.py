@@ -182,7 +182,19 @@ class EnvMapLight:
 
 
 # ---------------------------------------------------------------- Material.h
-class DiffuseMaterial:
+class _Textured:
+    """Optional per-texel parameter: a texture [H, W, C] read at the nearest texel of a cube map around
+    `texture_center` (pt_material_set_texture)."""
+    texture = None
+    texture_center = (0.0, 0.0, 0.0)
+
+    def setTexture(self, texture, center=(0.0, 0.0, 0.0)):
+        self.texture = None if texture is None else np.ascontiguousarray(texture, np.float32)
+        self.texture_center = tuple(float(x) for x in center)
+
+
+class DiffuseMaterial(_Textured):
+    """diffuse_color; setTexture(albedo [H, W, 3], center) makes it per texel."""
     type = DIFFUSE_SHADER
 
     def __init__(self, color=(0.8, 0.8, 0.8)):
@@ -195,9 +207,10 @@ class DiffuseMaterial:
         self.color = tuple(c)
 
 
-class MetallicMaterial:
+class MetallicMaterial(_Textured):
     """Conductor with complex IOR per RGB (MyComplex3); defaults of MetallicMaterial.cpp:7-26
-    (gold, roughness 0.1, Walter model, Beckmann distribution)."""
+    (gold, roughness 0.1, Walter model, Beckmann distribution).  setTexture(roughness [H, W], center)
+    makes the (isotropic) roughness per texel."""
     type = METALLIC_SHADER
     GOLD = ((0.170265, 3.01893), (0.511516, 2.44734), (1.47544, 1.87263))  # Material.h:328
 
@@ -447,6 +460,15 @@ class Renderer:
         self.apply_camera()
         self.apply_background()
         nat.call("pt_set_probe_count", self.ctx, data.probe_samples)
+        self.texture_ids = {}
+        for k, mat in enumerate(data.materials):
+            tex = getattr(mat, "texture", None)
+            if tex is not None:
+                ch = 1 if tex.ndim == 2 else tex.shape[2]
+                tid = ctypes.c_uint32()
+                nat.call("pt_texture_create", self.ctx, tex.ctypes.data, tex.shape[1], tex.shape[0], ch, ctypes.byref(tid))
+                nat.call("pt_material_set_texture", self.ctx, k, tid.value, _f3(mat.texture_center))
+                self.texture_ids[id(mat)] = tid.value
         for m, mid in zip(data.meshes, data.mesh_material):
             nn = 0 if m.normals is None else len(m.normals)
             first = ctypes.c_uint32()

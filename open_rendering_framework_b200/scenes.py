@@ -230,12 +230,14 @@ def heightfield(n, extent=1.2, height=0.15, y0=-0.35, seed=0):
 BATCH_MATERIALS = ("diffuse", "ggx", "beckmann", "rough_dielectric", "dipole")
 
 
-def batch_scene(k, seed=0, size_scale=1.0, spp_scale=1.0, env_w=128, env_h=64, probe_samples=1024):
+def batch_scene(k, seed=0, size_scale=1.0, spp_scale=1.0, env_w=128, env_h=64, probe_samples=500):
     """Scene k of the batched configuration: a seeded mesh (an icosphere at the subdivision nearest a
     log-uniform [1e3, 5e5] triangle count, or a heightfield grid of that size), a material drawn
     uniformly from diffuse / GGX conductor / Beckmann conductor / rough dielectric / dipole, a
     resolution from {128, 256, 512, 1024}^2 and a log-uniform spp in [4, 256]; lit by a procedural sky
-    (background and light).  size_scale / spp_scale shrink the resolution and spp (tests)."""
+    (background and light).  Dipole scenes use the reference's default of 500 probes per frame
+    (SAMPLES_FRAME, OptixSceneLoader.cpp:11).  size_scale / spp_scale shrink the resolution and spp
+    (tests)."""
     rng = np.random.default_rng([seed, k])
     tris = float(np.exp(rng.uniform(np.log(1e3), np.log(5e5))))
     res = int(rng.choice([128, 256, 512, 1024]))
@@ -278,3 +280,32 @@ def batch_scene(k, seed=0, size_scale=1.0, spp_scale=1.0, env_w=128, env_h=64, p
 def batch_scenes(n=64, seed=0, size_scale=1.0, spp_scale=1.0, **kw):
     """The n scenes of the batched configuration: [(SceneData, spp, description)]."""
     return [batch_scene(k, seed, size_scale, spp_scale, **kw) for k in range(n)]
+
+
+def inverse_scene(width=256, height=256, subdiv=5, tex_res=256, seed=0, max_depth=6, probe_samples=500, scale=10.0):
+    """The differentiable configuration: the single-scene geometry with both icospheres at `subdiv`
+    subdivisions -- the diffuse box carries an albedo texture (tex_res^2 x 3, cube map around the box
+    center), the GGX conductor sphere a roughness texture (tex_res^2, cube map around its center), and
+    the second sphere is a translucent material (standard dipole) whose sigma_a and sigma_s' per RGB
+    (1/mm, scaled by `scale` to scene units) are parameters; max depth 6, Russian roulette from depth 3.
+    Every parameter is drawn from a seeded U[0.1, 0.9]."""
+    rng = np.random.default_rng(seed)
+    integrator = sc.PathTracer(max_depth=max_depth, scene_epsilon=1e-4, rr_start_depth=3)
+    camera = sc.PinholeCamera(eye=(0.0, 0.0, 0.9), lookat=(0.0, 0.0, -1.0), up=(0.0, 1.0, 0.0), vfov=60.0, width=width, height=height)
+    background = sc.ConstantBackground((0.0, 0.0, 0.0))
+    diffuse = sc.DiffuseMaterial((0.7, 0.7, 0.7))
+    diffuse.setTexture(rng.uniform(0.1, 0.9, (tex_res, tex_res, 3)).astype(np.float32), (0.0, 0.0, 0.0))
+    metal_center = (-0.45, -0.7, -0.3)
+    metal = sc.MetallicMaterial(ior=((0.2, 3.9), (0.55, 3.15), (0.9, 2.4)), roughness=(0.2, 0.2), microfacet_model=sc.WALTER_MODEL,
+                                normal_distribution=sc.GGX_DISTRIBUTION)
+    metal.setTexture(rng.uniform(0.1, 0.9, (tex_res, tex_res)).astype(np.float32), metal_center)
+    sig = rng.uniform(0.1, 0.9, 6)
+    trans = sc.TranslucentMaterial(scattering=tuple(sig[3:]), absorption=tuple(sig[:3]), meancosine=(0.0, 0.0, 0.0), ior=1.3, scale=scale)
+    bp, bi = box()
+    mp, mi, mn, mni = icosphere(subdiv, 0.3, metal_center)
+    tp, ti, tn, tni = icosphere(subdiv, 0.3, (0.45, -0.7, 0.1))
+    meshes = [sc.Mesh(bp, bi, diffuse), sc.Mesh(mp, mi, metal, mn, mni), sc.Mesh(tp, ti, trans, tn, tni)]
+    lp, li = quad_light((0.0, 0.99, 0.0), 0.25)
+    lights = [sc.TriangleAreaLight(lp, li, (15.0, 15.0, 15.0))]
+    data = sc.SceneData(integrator, camera, background, meshes, lights, probe_samples=probe_samples)
+    return data, (diffuse, metal, trans)

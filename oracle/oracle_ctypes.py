@@ -180,6 +180,12 @@ def _trace_sigs(lib):
     _sig(lib, "orc_scene_set_translucent", None, [P, U, P, U])
     _sig(lib, "orc_scene_add_translucent_object", None, [P, U, U, U])
     _sig(lib, "orc_scene_set_samples", None, [P, U])
+    _sig(lib, "orc_scene_set_texture", None, [P, U, P, U, U, U, P])
+    _sig(lib, "orc_cube_texel", U, [P, P, U, U])
+    _sig(lib, "orc_scene_record", None, [P, I])
+    _sig(lib, "orc_scene_set_translucent_raw", None, [P, U, P, P, P, D, D])
+    _sig(lib, "orc_tape_stats", None, [P, P])
+    _sig(lib, "orc_tape_eval", None, [P, P, P, P, P, P, P, I])
     _sig(lib, "orc_scene_probes", L, [P, P])
     _sig(lib, "orc_compute_coefficients", None, [P, P, P, F, F, P])
     _sig(lib, "orc_dipole_bssrdf", None, [P, F, P])
@@ -274,11 +280,25 @@ class OracleScene:
                                       fp(mtype), fp(mmodel), fp(mdist), fp(mab), fp(mior), n_m,
                                       fp(lb) if len(lb) else None, len(lb), fp(tb) if len(tb) else None, len(tb),
                                       fp(cam), C.width, C.height, fp(patch), I_.max_depth, I_.scene_epsilon, I_.rr_start_depth, fp(bg))
+        self.tex_of_material = {}
         for k, m in enumerate(data.materials):
             if type(m).__name__ == "TranslucentMaterial":
                 props = compute_coefficients(m)
                 self._keep.append(props)
                 lib.orc_scene_set_translucent(self.h, k, fp(props), m.dipole_model)
+                g = np.asarray(m.meancosine, np.float64)
+                sa = np.asarray(m.absorption, np.float32).astype(np.float64)
+                ssr = np.asarray(m.scattering, np.float32).astype(np.float64) * (1.0 - g)
+                lib.orc_scene_set_translucent_raw(self.h, k, fp(sa), fp(ssr), fp(g), float(np.float32(m.ior)), float(np.float32(m.scale)))
+        for k, m in enumerate(data.materials):
+            tex = getattr(m, "texture", None)
+            if tex is not None:
+                tex = np.ascontiguousarray(tex, np.float32)
+                center = np.asarray(m.texture_center, np.float32)
+                self._keep += [tex, center]
+                ch = 1 if tex.ndim == 2 else tex.shape[2]
+                self.tex_of_material[k] = len(self.tex_of_material)
+                lib.orc_scene_set_texture(self.h, k, fp(tex), tex.shape[1], tex.shape[0], ch, fp(center))
         for mid, first, n in data.translucent_objects():
             lib.orc_scene_add_translucent_object(self.h, mid, first, n)
         lib.orc_scene_set_samples(self.h, getattr(data, "probe_samples", 500))
@@ -297,7 +317,51 @@ class OracleScene:
             accum = np.ascontiguousarray(accum, np.float32)
         self.lib.orc_render(self.h, first_frame, n_frames, p_begin, p_end, fp(pr) if pr is not None else None,
                             fp(accum) if accum is not None else None, threads)
+        self._tape_range = (p_begin, p_end)
         return accum, pr
+
+    # ---- path tapes (FP64 re-evaluation of the recorded paths; adjoint checks)
+    def record(self, on=True):
+        self.lib.orc_scene_record(self.h, 1 if on else 0)
+
+    def tape_stats(self):
+        out = np.zeros(3, np.int64)
+        self.lib.orc_tape_stats(self.h, fp(out))
+        return tuple(int(x) for x in out)
+
+    def param_layout(self, materials):
+        """(offsets per texture id, offsets per material, size) for parameters of the given materials:
+        a textured material contributes its texture, a translucent one its 6 sigmas."""
+        n_tex = len(self.tex_of_material)
+        tex_off = np.full(max(1, n_tex), -1, np.int64)
+        mat_off = np.full(max(1, len(self.data.materials)), -1, np.int64)
+        off = 0
+        for m in materials:
+            k = self.data.materials.index(m)
+            if k in self.tex_of_material:
+                tex_off[self.tex_of_material[k]] = off
+                off += m.texture.size
+            else:
+                mat_off[k] = off
+                off += 6
+        return tex_off, mat_off, off
+
+    def tape_eval(self, P, tex_off, mat_off, dimg=None, threads=8):
+        """FP64 image [npix, 3] of the recorded paths at parameters P; with dimg, also the FP64
+        gradient of the loss whose image gradient is dimg ([npix, 3])."""
+        P = np.ascontiguousarray(P, np.float64)
+        npix = self._tape_npix()
+        img = np.zeros((npix, 3), np.float64)
+        grad = None
+        if dimg is not None:
+            dimg = np.ascontiguousarray(dimg, np.float64)
+            grad = np.zeros_like(P)
+        self.lib.orc_tape_eval(self.h, fp(P), fp(tex_off), fp(mat_off), fp(img), fp(dimg) if dimg is not None else None,
+                               fp(grad) if grad is not None else None, threads)
+        return img, grad
+
+    def _tape_npix(self):
+        return self._tape_range[1] - self._tape_range[0]
 
     def probes(self):
         """PositionSample records of the last frame rendered, as raw float32 [n, 20]."""

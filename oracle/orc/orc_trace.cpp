@@ -38,7 +38,40 @@ struct Mat {
   ScatProps props;       // translucent: scattering_properties
   u32 dipole_model = 0;  // translucent: dipole_model
   int translucent_index = -1;
+  int tex = -1;          // texture (diffuse albedo / conductor roughness), -1 = none
+  F3 tcenter;            // its cube-map center
+  // translucent: the parameters the scattering properties were derived from (FP64 tape evaluation)
+  double sig_a[3] = {0, 0, 0}, sig_sr[3] = {0, 0, 0}, mcos[3] = {0, 0, 0}, ior = 1.0, scale = 1.0;
 };
+
+struct Tex {
+  unsigned w, h, ch;
+  std::vector<float> data;
+};
+
+// Nearest texel of a cube map around c, faces laid out 3 x 2 (the device's cube_texel): face by the
+// largest component of p - c, face coordinates from the other two divided by it.
+static unsigned cube_texel(const F3& p, const F3& c, unsigned w, unsigned h)
+{
+  F3 d = p - c;
+  float ax = std::fabs(d.x), ay = std::fabs(d.y), az = std::fabs(d.z);
+  unsigned face;
+  float s, t, m;
+  if (ax >= ay && ax >= az) { face = d.x >= 0.0f ? 0u : 1u; m = ax; s = d.z; t = d.y; }
+  else if (ay >= az) { face = d.y >= 0.0f ? 2u : 3u; m = ay; s = d.x; t = d.z; }
+  else { face = d.z >= 0.0f ? 4u : 5u; m = az; s = d.x; t = d.y; }
+  float u = 0.5f, v = 0.5f;
+  if (m > 0.0f) {
+    u = 0.5f * (s / m + 1.0f);
+    v = 0.5f * (t / m + 1.0f);
+  }
+  const unsigned fw = w / 3u, fh = h / 2u;
+  float fu = u * (float)fw, fv = v * (float)fh;
+  unsigned x = fu > 0.0f ? (unsigned)fu : 0u, y = fv > 0.0f ? (unsigned)fv : 0u;
+  if (x >= fw) x = fw - 1u;
+  if (y >= fh) y = fh - 1u;
+  return ((face / 3u) * fh + y) * w + (face % 3u) * fw + x;
+}
 
 // PositionSample, structs.h:105-114 (80 bytes).
 struct Probe {
@@ -54,6 +87,27 @@ struct TranslucentObject {
 
 struct Tri {
   F3 v0, e1, e2;
+};
+
+// Path tape (test infrastructure for the adjoint): what each vertex of a camera path adds to the path
+// radiance and what it multiplies the rest of the path by, with every sampled quantity (directions,
+// Russian-roulette and acceptance decisions and probabilities) frozen, so that the path's radiance
+// can be re-evaluated in FP64 for other parameter values (see orc_tape_*).
+enum TapeType { TAPE_EMIT = 0, TAPE_CONST_W = 1, TAPE_NEE = 2, TAPE_DIFF_W = 3, TAPE_METAL_W = 4, TAPE_BEER = 5, TAPE_GATHER = 6 };
+struct TapeRec {
+  int type = TAPE_EMIT;
+  int tex = -1, texel = -1, mat = -1;
+  float v[3] = {0.0f, 0.0f, 0.0f};     // emission | constant weight | NEE factor (albedo excluded) | metal weight at alpha0
+  float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};  // diffuse: prob0 | metal: cos(m,n), cos(wi,n), cos(wo,n), alpha0 | beer: t, prob0
+  int g_begin = 0, g_count = 0;       // gather: accepted probes
+};
+struct TapeProbe {
+  float dist, wl[3], exp0;
+};
+struct Tape {
+  std::vector<TapeRec> recs;
+  std::vector<TapeProbe> probes;
+  bool valid = true;
 };
 
 struct Scene {
@@ -72,6 +126,11 @@ struct Scene {
   EnvMap env;
   std::vector<float> env_texels;
   std::vector<TranslucentObject> translucent;
+  std::vector<Tex> textures;
+  // path tapes of the last recorded render: [frame][pixel] over its pixel range
+  bool record = false;
+  std::vector<Tape> tapes;
+  unsigned tape_first = 0, tape_frames = 0, tape_p0 = 0, tape_p1 = 0;
   unsigned samples = 500;                // context["samples"] (OptixSceneLoader.cpp:11,17)
   std::vector<Probe> probes;             // samples_output_buffer of the current frame
   unsigned probe_frame = 0xffffffffu;
@@ -250,7 +309,30 @@ struct PRD {
   u32 seed;
   Seed64 seed64;
   bool probe_path = false;  // traced by the probe pass: translucent hits do not gather
+  Tape* tape = nullptr;     // camera path being recorded
 };
+
+static inline int tape_add(PRD& prd, const TapeRec& r)
+{
+  if (!prd.tape) return -1;
+  prd.tape->recs.push_back(r);
+  return (int)prd.tape->recs.size() - 1;
+}
+static inline void tape_emit(PRD& prd, const F3& e)
+{
+  if (!prd.tape || (e.x == 0.0f && e.y == 0.0f && e.z == 0.0f)) return;
+  TapeRec r;
+  r.type = TAPE_EMIT;
+  r.v[0] = e.x; r.v[1] = e.y; r.v[2] = e.z;
+  prd.tape->recs.push_back(r);
+}
+static inline void tape_const_w(PRD& prd, int slot, const F3& w)
+{
+  if (!prd.tape || slot < 0) return;
+  TapeRec& r = prd.tape->recs[slot];
+  r.type = TAPE_CONST_W;
+  r.v[0] = w.x; r.v[1] = w.y; r.v[2] = w.z;
+}
 
 static void trace(Scene& S, const F3& o, const F3& d, PRD& prd, LightSet& ls);
 
@@ -261,7 +343,14 @@ static void shade_diffuse(Scene& S, const Mat& m, const F3& o, const F3& d, cons
   F3 hit_pos = o + h.t * d;
   F3 normal = shading_normal(S, h.prim, h.u, h.v);
   F3 ffnormal = faceforward(normal, -d, normal);
-  const F3 dc = v3(m.a[0], m.a[1], m.a[2]);
+  F3 dc = v3(m.a[0], m.a[1], m.a[2]);
+  int texel = -1;
+  if (m.tex >= 0) {
+    const Tex& T = S.textures[m.tex];
+    unsigned tx = cube_texel(hit_pos, m.tcenter, T.w, T.h);
+    dc = v3(T.data[3 * tx], T.data[3 * tx + 1], T.data[3 * tx + 2]);
+    texel = (int)tx;
+  }
   u32& t = prd.seed;
   F3 result = v3s(0.0f);
   float draw = rnd_tea(t);
@@ -279,6 +368,19 @@ static void shade_diffuse(Scene& S, const Mat& m, const F3& o, const F3& d, cons
       F3 Li = V * radiance;
       result = result + Li * K<float>::INV_PI * cos_theta * dc;
       prd.emit_light = 0;
+      if (prd.tape && V != 0.0f) {
+        if (texel >= 0) {
+          TapeRec r;
+          r.type = TAPE_NEE;
+          r.tex = m.tex;
+          r.texel = texel;
+          F3 f = Li * K<float>::INV_PI * cos_theta;
+          r.v[0] = f.x; r.v[1] = f.y; r.v[2] = f.z;
+          tape_add(prd, r);
+        } else {
+          tape_emit(prd, Li * K<float>::INV_PI * cos_theta * dc);
+        }
+      }
     }
   }
   float prob = (dc.x + dc.y + dc.z) / 3.0f;
@@ -286,9 +388,24 @@ static void shade_diffuse(Scene& S, const Mat& m, const F3& o, const F3& d, cons
   bool forced = prd.depth < S.rr_start;
   if (forced) prob = 1.0f;
   if (xi < prob || forced) {
+    if (prd.tape) {
+      TapeRec r;
+      if (texel >= 0) {
+        r.type = TAPE_DIFF_W;
+        r.tex = m.tex;
+        r.texel = texel;
+        r.c[0] = prob;
+      } else {
+        r.type = TAPE_CONST_W;
+        F3 wgt = dc / prob;
+        r.v[0] = wgt.x; r.v[1] = wgt.y; r.v[2] = wgt.z;
+      }
+      tape_add(prd, r);
+    }
     F3 nd = sample_cosine_weighted<float>(ffnormal, t);
     PRD child;
     child.probe_path = prd.probe_path;
+    child.tape = prd.tape;
     child.depth = prd.depth + 1;
     child.seed = t;
     child.seed64 = prd.seed64;
@@ -312,6 +429,12 @@ static void shade_metal(Scene& S, const Mat& m, const F3& o, const F3& d, const 
   F3 w_i = -d;
   u32& seed = prd.seed;
   float a_x = m.a[0], a_y = m.a[1];
+  int rtexel = -1;
+  if (m.tex >= 0) {
+    const Tex& T = S.textures[m.tex];
+    rtexel = (int)cube_texel(hit_point, m.tcenter, T.w, T.h);
+    a_x = a_y = T.data[rtexel];
+  }
   int capped = 0;
   if (m.model == MULTISCATTERING) {
     u32 order = 0;
@@ -320,11 +443,13 @@ static void shade_metal(Scene& S, const Mat& m, const F3& o, const F3& d, const 
     F3 w_o = to_world(lwo, normal);
     PRD child;
     child.probe_path = prd.probe_path;
+    child.tape = prd.tape;
     child.depth = prd.depth + 1;
     child.result = v3s(0.0f);
     child.seed = seed;
     child.seed64 = prd.seed64;
     child.emit_light = 1;
+    tape_const_w(prd, tape_add(prd, TapeRec()), weight);
     trace(S, hit_point, w_o, child, ls);
     result = result + child.result * weight;
   } else {
@@ -344,6 +469,7 @@ static void shade_metal(Scene& S, const Mat& m, const F3& o, const F3& d, const 
     float abs_i_m = std::fabs(dot(w_i, mn)), abs_i_n = std::fabs(dot(w_i, ffnormal)), abs_n_m = std::fabs(dot(normal, mn));
     PRD child;
     child.probe_path = prd.probe_path;
+    child.tape = prd.tape;
     child.depth = prd.depth + 1;
     child.result = v3s(0.0f);
     child.seed = seed;
@@ -352,9 +478,23 @@ static void shade_metal(Scene& S, const Mat& m, const F3& o, const F3& d, const 
     F3 weight = F;
     float G_o_m = (m.model == WALTER) ? masking_G1<float>((int)m.dist, w_o, mn, ffnormal, a_x) : masking_G1_aniso<float>((int)m.dist, w_o, mn, ffnormal, a_x, a_y);
     if (G_o_m <= 0.0f) { prd.result = result; S.capped += capped; return; }
+    const int slot = tape_add(prd, TapeRec());
     trace(S, hit_point, w_o, child, ls);
     if (m.model == WALTER) weight = weight * (abs_i_m * G_i_m * G_o_m / (abs_i_n * abs_n_m));
     else weight = weight * G_o_m;
+    if (slot >= 0) {
+      tape_const_w(prd, slot, weight);
+      if (rtexel >= 0 && m.dist == GGX) {
+        TapeRec& r = prd.tape->recs[slot];
+        r.type = TAPE_METAL_W;
+        r.tex = m.tex;
+        r.texel = rtexel;
+        r.c[0] = dot(mn, ffnormal);
+        r.c[1] = dot(w_i, ffnormal);
+        r.c[2] = dot(w_o, ffnormal);
+        r.c[3] = a_x;
+      }
+    }
     prd.seed = child.seed;
     result = result + child.result * weight;
   }
@@ -389,11 +529,13 @@ static void shade_glass(Scene& S, const Mat& m, const F3& o, const F3& d, const 
     F3 w_o = to_world(lwo, normal);
     PRD child;
     child.probe_path = prd.probe_path;
+    child.tape = prd.tape;
     child.depth = prd.depth + 1;
     child.result = v3s(0.0f);
     child.seed = t;
     child.seed64 = prd.seed64;
     child.emit_light = 1;
+    tape_const_w(prd, tape_add(prd, TapeRec()), beam_T);
     trace(S, hit_point, w_o, child, ls);
     prd.seed = child.seed;
     result = result + child.result;
@@ -414,6 +556,7 @@ static void shade_glass(Scene& S, const Mat& m, const F3& o, const F3& d, const 
     float rr = rnd_tea(t);
     PRD child;
     child.probe_path = prd.probe_path;
+    child.tape = prd.tape;
     child.depth = prd.depth + 1;
     child.result = v3s(0.0f);
     child.seed = t;
@@ -422,8 +565,10 @@ static void shade_glass(Scene& S, const Mat& m, const F3& o, const F3& d, const 
     F3 w_o = rr > R ? refr : refl;
     float G_o_m = (m.model == WALTER) ? masking_G1<float>((int)m.dist, w_o, mn, ffnormal, rough) : masking_G1_aniso<float>((int)m.dist, w_o, mn, ffnormal, rough, rough);
     if (G_o_m <= 0.0f) { prd.result = result; S.capped += capped; return; }
+    const int slot = tape_add(prd, TapeRec());
     trace(S, hit_point, w_o, child, ls);
     float weight = (m.model == WALTER) ? abs_i_m * G_i_m * G_o_m / (abs_i_n * abs_n_m) : G_o_m;
+    tape_const_w(prd, slot, weight * beam_T);
     prd.seed = child.seed;
     result = result + child.result * weight;
   }
@@ -453,6 +598,15 @@ static void shade_translucent(Scene& S, const Mat& m, const F3& o, const F3& d, 
     float prob = (beam_T.x + beam_T.y + beam_T.z) / 3.0f;
     if (rnd_accurate(t64) >= prob) return;
     beam_T = beam_T / prob;
+    if (prd.tape) {
+      TapeRec r;
+      r.type = TAPE_BEER;
+      r.mat = (int)(&m - S.mats.data());
+      r.c[0] = h.t;
+      r.c[1] = prob;
+      r.v[0] = beam_T.x; r.v[1] = beam_T.y; r.v[2] = beam_T.z;
+      tape_add(prd, r);
+    }
     recip_ior = P.relative_ior;
     no = -no;
     cos_theta_o = -cos_theta_o;
@@ -472,11 +626,19 @@ static void shade_translucent(Scene& S, const Mat& m, const F3& o, const F3& d, 
     child.result = v3s(0.0f);
     child.emit_light = 1;
     child.probe_path = prd.probe_path;
+    child.tape = prd.tape;
+    const int gslot = (!inside && !prd.probe_path) ? tape_add(prd, TapeRec()) : -1;
     trace(S, xo, wt, child, ls);
     prd.result = prd.result + child.result;
     t = child.seed;
     t64 = child.seed64;
     if (!inside && !prd.probe_path) {
+      if (gslot >= 0) {
+        TapeRec& r = prd.tape->recs[gslot];
+        r.type = TAPE_GATHER;
+        r.mat = (int)(&m - S.mats.data());
+        r.g_begin = (int)prd.tape->probes.size();
+      }
       float chosen = std::fmin(P.transport.x, std::fmin(P.transport.y, P.transport.z));
       F3 acc = v3s(0.0f);
       unsigned N = S.samples;
@@ -488,6 +650,11 @@ static void shade_translucent(Scene& S, const Mat& m, const F3& o, const F3& d, 
           float exp_term = std::exp(-dist * chosen);
           float rnd_number = rnd_accurate(t64);
           if (rnd_number < exp_term) {
+            if (gslot >= 0) {
+              F3 wl = sm.weight * sm.L;
+              prd.tape->probes.push_back(TapeProbe{dist, {wl.x, wl.y, wl.z}, exp_term});
+              prd.tape->recs[gslot].g_count += 1;
+            }
             if (m.dipole_model == DIRECTIONAL_DIPOLE)
               acc = acc + sm.weight * sm.L * dirpole_bssrdf(sm.pos, sm.normal, sm.transmitted, xo, no, P) / exp_term;
             else
@@ -507,6 +674,7 @@ static void shade_translucent(Scene& S, const Mat& m, const F3& o, const F3& d, 
     child.result = v3s(0.0f);
     child.emit_light = 1;
     child.probe_path = prd.probe_path;
+    child.tape = prd.tape;
     trace(S, xo, wr, child, ls);
     prd.result = prd.result + child.result;
     t = child.seed;
@@ -602,6 +770,7 @@ static void trace(Scene& S, const F3& o, const F3& d, PRD& prd, LightSet& ls)
     } else {
       prd.result = S.bg;
     }
+    tape_emit(prd, prd.result);
     return;
   }
   const Mat& m = S.mats[S.info[4 * (size_t)h.prim + 3]];
@@ -611,6 +780,7 @@ static void trace(Scene& S, const F3& o, const F3& d, PRD& prd, LightSet& ls)
       F3 result = v3s(0.0f);
       if (dot(normal, -d) > 0.0f && prd.emit_light) result = v3(m.a[0], m.a[1], m.a[2]);
       prd.result = result;
+      tape_emit(prd, result);
       return;
     }
     case MT_DIFFUSE: shade_diffuse(S, m, o, d, h, prd, ls); return;
@@ -750,6 +920,13 @@ EXPORT long orc_render(void* scene, unsigned first_frame, unsigned n_frames, uns
     worker();
     for (auto& x : th) x.join();
   };
+  if (S.record) {
+    S.tapes.assign((size_t)n_frames * (p_end - p_begin), Tape());
+    S.tape_first = first_frame;
+    S.tape_frames = n_frames;
+    S.tape_p0 = p_begin;
+    S.tape_p1 = p_end;
+  }
   for (unsigned fl = 0; fl < n_frames; ++fl) {
     const unsigned frame = first_frame + fl;
     if (!S.translucent.empty()) {
@@ -775,8 +952,10 @@ EXPORT long orc_render(void* scene, unsigned first_frame, unsigned n_frames, uns
         float ipy = ((float)y + jy) / (float)H * 2.0f - 1.0f;
         F3 dir = normalize(ipx * S.U + ipy * S.V + S.W);
         prd.result = v3s(0.0f);
+        if (S.record) prd.tape = &S.tapes[(size_t)fl * (p_end - p_begin) + k];
         trace(S, S.eye, dir, prd, ls);
         result = result + prd.result;
+        if (prd.tape) prd.tape->valid = std::isfinite(result.x) && std::isfinite(result.y) && std::isfinite(result.z);
       }
       if (path_rad) {
         float* pr = path_rad + 3 * ((size_t)fl * (p_end - p_begin) + k);
@@ -819,6 +998,24 @@ EXPORT void orc_scene_add_translucent_object(void* s, unsigned mat, unsigned fir
   S.translucent.push_back({(int)mat, first_tri, n_tris});
 }
 EXPORT void orc_scene_set_samples(void* s, unsigned n) { ((Scene*)s)->samples = n; }
+// Texture of material `mat`: w x h texels of ch channels, read at the nearest texel of the cube map
+// around center3.
+EXPORT void orc_scene_set_texture(void* s, unsigned mat, const float* data, unsigned w, unsigned h, unsigned ch, const float* center3)
+{
+  Scene& S = *(Scene*)s;
+  Tex t;
+  t.w = w;
+  t.h = h;
+  t.ch = ch;
+  t.data.assign(data, data + (size_t)w * h * ch);
+  S.mats[mat].tex = (int)S.textures.size();
+  S.mats[mat].tcenter = v3(center3[0], center3[1], center3[2]);
+  S.textures.push_back(std::move(t));
+}
+EXPORT unsigned orc_cube_texel(const float* p3, const float* c3, unsigned w, unsigned h)
+{
+  return cube_texel(v3(p3[0], p3[1], p3[2]), v3(c3[0], c3[1], c3[2]), w, h);
+}
 // The probes of the most recent frame rendered (PositionSample records, 80 bytes each).
 EXPORT long orc_scene_probes(void* s, void* out)
 {
@@ -886,4 +1083,318 @@ EXPORT void orc_trace_batch(void* scene, const float* rays8, long n, int brute, 
       }
     }
   }
+}
+
+// ---------------------------------------------------------------- FP64 evaluation of path tapes
+namespace {
+
+// Boundary polynomials of Fresnel.h:93-124 in FP64 (same coefficients).
+static double c1_64(double n)
+{
+  if (n >= 1.0) return -9.23372 + n * (22.2272 + n * (-20.9292 + n * (10.2291 + n * (-2.54396 + n * 0.254913))));
+  return 0.919317 + n * (-3.4793 + n * (6.75335 + n * (-7.80989 + n * (4.98554 - n * 1.36881))));
+}
+static double c2_64(double n)
+{
+  double r;
+  if (n >= 1.0) {
+    r = -1641.1 + n * (1213.67 + n * (-568.556 + n * (164.798 + n * (-27.0181 + n * 1.91826))));
+    r += (((135.926 / n) - 656.175) / n + 1376.53) / n;
+  } else {
+    r = 0.828421 + n * (-2.62051 + n * (3.36231 + n * (-1.95284 + n * (0.236494 + n * 0.145787))));
+  }
+  return r;
+}
+
+struct Eval64 {
+  const Scene& S;
+  const double* P;
+  const long* tex_off;
+  const long* mat_off;
+  double albedo(int tex, int texel, int c) const
+  {
+    long o = tex_off[tex];
+    return o >= 0 ? P[o + 3 * (long)texel + c] : (double)S.textures[tex].data[3 * (size_t)texel + c];
+  }
+  double rough(int tex, int texel) const
+  {
+    long o = tex_off[tex];
+    return o >= 0 ? P[o + texel] : (double)S.textures[tex].data[texel];
+  }
+  // (sigma_a RGB, sigma_s' RGB) of material mat
+  void sigma(int mat, double out[6]) const
+  {
+    long o = mat_off[mat];
+    const Mat& m = S.mats[mat];
+    for (int c = 0; c < 3; ++c) {
+      out[c] = o >= 0 ? P[o + c] : m.sig_a[c];
+      out[3 + c] = o >= 0 ? P[o + 3 + c] : m.sig_sr[c];
+    }
+  }
+};
+
+// GGX D and Smith G1 of a cosine, FP64 (ggx_distribution, ggx_G1_cos).
+static double ggx_D64(double c, double a)
+{
+  double c2 = c * c, t2 = (1.0 - c2) / c2, a2 = a * a;
+  double q = a2 + t2;
+  return a2 / (M_PI * c2 * c2 * q * q);
+}
+static double ggx_G164(double c, double a)
+{
+  double c2 = c * c, t2 = (1.0 - c2) / c2;
+  return 2.0 / (1.0 + std::sqrt(1.0 + a * a * t2));
+}
+static double ggx_dlnD64(double c, double a)
+{
+  double c2 = c * c, t2 = (1.0 - c2) / c2;
+  return 2.0 / a - 4.0 * a / (a * a + t2);
+}
+static double ggx_dlnG164(double c, double a)
+{
+  double c2 = c * c, t2 = (1.0 - c2) / c2;
+  double q = std::sqrt(1.0 + a * a * t2);
+  return -(a * t2 / q) / (1.0 + q);
+}
+
+// Standard dipole of one channel in FP64 and its derivatives with respect to (sigma_a, sigma_s').
+static void dipole64(double dist, double sa_raw, double ssr_raw, double ior, double scale, double& S, double& dSa, double& dSs)
+{
+  const double sa = sa_raw * scale, x = (ssr_raw + sa_raw) * scale;  // absorption, reduced extinction
+  const double D = 1.0 / (3.0 * x), dD = -D / x * scale;
+  const double three_D = 3.0 * D, d3D = 3.0 * dD;
+  const double tr = std::sqrt(sa / D);
+  const double dtr_a = 3.0 * scale * (x + sa) / (2.0 * tr), dtr_s = 3.0 * sa * scale / (2.0 * tr);
+  const double cphi = 0.25 * (1.0 - c1_64(ior)), ce = 0.5 * (1.0 - c2_64(ior));
+  const double A = (1.0 - ce) / (2.0 * cphi);
+  const double ext = 4.0 * A * D, dext = 4.0 * A * dD;
+  const double r2 = dist * dist;
+  const double dr2 = r2 + three_D * three_D, dr = std::sqrt(dr2), ddr = three_D * d3D / dr;
+  const double dv2 = r2 + ext * ext, dv = std::sqrt(dv2), ddv = ext * dext / dv;
+  const double cmf = three_D + ext, dcmf = d3D + dext;
+  const double trr = tr * dr, trv = tr * dv;
+  const double Sr = three_D * (1.0 + trr) / (dr2 * dr) * std::exp(-trr);
+  const double Sv = cmf * (1.0 + trv) / (dv2 * dv) * std::exp(-trv);
+  const double dtrr_a = dtr_a * dr + tr * ddr, dtrr_s = dtr_s * dr + tr * ddr;
+  const double dtrv_a = dtr_a * dv + tr * ddv, dtrv_s = dtr_s * dv + tr * ddv;
+  S = Sr + Sv;
+  dSa = Sr * (d3D / three_D + dtrr_a / (1.0 + trr) - dtrr_a - 3.0 * ddr / dr) + Sv * (dcmf / cmf + dtrv_a / (1.0 + trv) - dtrv_a - 3.0 * ddv / dv);
+  dSs = Sr * (d3D / three_D + dtrr_s / (1.0 + trr) - dtrr_s - 3.0 * ddr / dr) + Sv * (dcmf / cmf + dtrv_s / (1.0 + trv) - dtrv_s - 3.0 * ddv / dv);
+}
+static double global_coeff64(double ior)
+{
+  const double cphi_inv = 0.25 * (1.0 - c1_64(1.0 / ior));
+  return 1.0 / (4.0 * cphi_inv) * 1.0 / (4.0 * M_PI * M_PI);
+}
+
+// One tape: its radiance (L) and, when grad is given, adds dLoss/dL (dl) times dL/dtheta to grad
+// (path replay backprop on the stored vertices: T_k dE_k + (dw_k / w_k) R_{k+1}).
+static void eval_tape(const Eval64& E, const Tape& tp, double L[3], const double* dl, double* grad)
+{
+  const size_t n = tp.recs.size();
+  std::vector<double> Tk(3 * n), ck(3 * n, 0.0), wk(3 * n, 1.0);
+  double T[3] = {1.0, 1.0, 1.0};
+  L[0] = L[1] = L[2] = 0.0;
+  for (size_t k = 0; k < n; ++k) {
+    const TapeRec& r = tp.recs[k];
+    for (int c = 0; c < 3; ++c) Tk[3 * k + c] = T[c];
+    double e[3] = {0, 0, 0}, w[3] = {1, 1, 1};
+    switch (r.type) {
+      case TAPE_EMIT:
+        for (int c = 0; c < 3; ++c) e[c] = r.v[c];
+        break;
+      case TAPE_NEE:
+        for (int c = 0; c < 3; ++c) e[c] = (double)r.v[c] * E.albedo(r.tex, r.texel, c);
+        break;
+      case TAPE_CONST_W:
+        for (int c = 0; c < 3; ++c) w[c] = r.v[c];
+        break;
+      case TAPE_DIFF_W:
+        for (int c = 0; c < 3; ++c) w[c] = E.albedo(r.tex, r.texel, c) / (double)r.c[0];
+        break;
+      case TAPE_METAL_W: {
+        const double a = E.rough(r.tex, r.texel), a0 = r.c[3];
+        const double ratio = ggx_D64(r.c[0], a) * ggx_G164(r.c[1], a) * ggx_G164(r.c[2], a) /
+                             (ggx_D64(r.c[0], a0) * ggx_G164(r.c[1], a0) * ggx_G164(r.c[2], a0));
+        for (int c = 0; c < 3; ++c) w[c] = (double)r.v[c] * ratio;
+        break;
+      }
+      case TAPE_BEER: {
+        double sg[6];
+        E.sigma(r.mat, sg);
+        const Mat& m = E.S.mats[r.mat];
+        for (int c = 0; c < 3; ++c) {
+          const double k = m.dipole_model == DIRECTIONAL_DIPOLE ? (1.0 + m.mcos[c]) : 1.0 / (1.0 - m.mcos[c]);
+          const double ext = (sg[3 + c] * k + sg[c]) * m.scale;
+          w[c] = std::exp(-(double)r.c[0] * ext) / (double)r.c[1];
+        }
+        break;
+      }
+      case TAPE_GATHER: {
+        double sg[6];
+        E.sigma(r.mat, sg);
+        const Mat& m = E.S.mats[r.mat];
+        const double gc = global_coeff64(m.ior);
+        for (int q = 0; q < r.g_count; ++q) {
+          const TapeProbe& pr = tp.probes[r.g_begin + q];
+          for (int c = 0; c < 3; ++c) {
+            double Sv, da, ds;
+            dipole64(pr.dist, sg[c], sg[3 + c], m.ior, m.scale, Sv, da, ds);
+            e[c] += (double)pr.wl[c] * Sv / (double)pr.exp0;
+          }
+        }
+        for (int c = 0; c < 3; ++c) e[c] = e[c] * gc / (double)E.S.samples;
+        break;
+      }
+      default:
+        break;
+    }
+    for (int c = 0; c < 3; ++c) {
+      ck[3 * k + c] = T[c] * e[c];
+      L[c] += ck[3 * k + c];
+      wk[3 * k + c] = w[c];
+      T[c] *= w[c];
+    }
+  }
+  if (!grad) return;
+  // R after record k: what the records beyond k add
+  std::vector<double> R(3 * (n + 1), 0.0);
+  for (size_t k = n; k-- > 0;)
+    for (int c = 0; c < 3; ++c) R[3 * k + c] = R[3 * (k + 1) + c] + ck[3 * k + c];
+  for (size_t k = 0; k < n; ++k) {
+    const TapeRec& r = tp.recs[k];
+    const double* Ra = &R[3 * (k + 1)];  // beyond record k
+    const double* Tc = &Tk[3 * k];
+    switch (r.type) {
+      case TAPE_NEE: {
+        long o = E.tex_off[r.tex];
+        if (o >= 0)
+          for (int c = 0; c < 3; ++c) grad[o + 3 * (long)r.texel + c] += dl[c] * Tc[c] * (double)r.v[c];
+        break;
+      }
+      case TAPE_DIFF_W: {
+        long o = E.tex_off[r.tex];
+        if (o >= 0)
+          for (int c = 0; c < 3; ++c) grad[o + 3 * (long)r.texel + c] += dl[c] * Ra[c] / E.albedo(r.tex, r.texel, c);
+        break;
+      }
+      case TAPE_METAL_W: {
+        long o = E.tex_off[r.tex];
+        if (o >= 0) {
+          const double a = E.rough(r.tex, r.texel);
+          const double s = ggx_dlnD64(r.c[0], a) + ggx_dlnG164(r.c[1], a) + ggx_dlnG164(r.c[2], a);
+          grad[o + r.texel] += s * (dl[0] * Ra[0] + dl[1] * Ra[1] + dl[2] * Ra[2]);
+        }
+        break;
+      }
+      case TAPE_BEER: {
+        long o = E.mat_off[r.mat];
+        if (o >= 0) {
+          const Mat& m = E.S.mats[r.mat];
+          for (int c = 0; c < 3; ++c) {
+            const double k = m.dipole_model == DIRECTIONAL_DIPOLE ? (1.0 + m.mcos[c]) : 1.0 / (1.0 - m.mcos[c]);
+            const double ga = dl[c] * Ra[c] * (-(double)r.c[0] * m.scale);
+            grad[o + c] += ga;
+            grad[o + 3 + c] += ga * k;
+          }
+        }
+        break;
+      }
+      case TAPE_GATHER: {
+        long o = E.mat_off[r.mat];
+        if (o >= 0) {
+          double sg[6];
+          E.sigma(r.mat, sg);
+          const Mat& m = E.S.mats[r.mat];
+          const double gc = global_coeff64(m.ior);
+          for (int q = 0; q < r.g_count; ++q) {
+            const TapeProbe& pr = tp.probes[r.g_begin + q];
+            for (int c = 0; c < 3; ++c) {
+              double Sv, da, ds;
+              dipole64(pr.dist, sg[c], sg[3 + c], m.ior, m.scale, Sv, da, ds);
+              const double f = dl[c] * Tc[c] * gc / (double)E.S.samples * (double)pr.wl[c] / (double)pr.exp0;
+              grad[o + c] += f * da;
+              grad[o + 3 + c] += f * ds;
+            }
+          }
+        }
+        break;
+      }
+      default:
+        break;
+    }
+  }
+}
+
+}  // namespace
+
+EXPORT void orc_scene_record(void* s, int on) { ((Scene*)s)->record = on != 0; }
+// The raw parameters of translucent material mat (FP64 tape evaluation): absorption and reduced
+// scattering per RGB in the material's units, mean cosine, ior, scale.
+EXPORT void orc_scene_set_translucent_raw(void* s, unsigned mat, const double* sig_a3, const double* sig_sr3, const double* mcos3, double ior,
+                                          double scale)
+{
+  Mat& m = ((Scene*)s)->mats[mat];
+  for (int c = 0; c < 3; ++c) {
+    m.sig_a[c] = sig_a3[c];
+    m.sig_sr[c] = sig_sr3[c];
+    m.mcos[c] = mcos3[c];
+  }
+  m.ior = ior;
+  m.scale = scale;
+}
+// Records of the last recorded render: count of tapes, records and gathered probes.
+EXPORT void orc_tape_stats(void* s, long* out3)
+{
+  Scene& S = *(Scene*)s;
+  long r = 0, p = 0;
+  for (const Tape& t : S.tapes) {
+    r += (long)t.recs.size();
+    p += (long)t.probes.size();
+  }
+  out3[0] = (long)S.tapes.size();
+  out3[1] = r;
+  out3[2] = p;
+}
+// FP64 image of the recorded paths for parameters P (tex_off / mat_off: per texture and material the
+// offset of its parameters in P, -1 = the scene's own values): per pixel of the recorded range the
+// mean of its frames' path radiance, img_rgb[(pixel - p0) * 3 + c].  With dimg (dLoss/dimage, same
+// layout) and grad (same layout as P), also adds the FP64 gradient of the loss.
+EXPORT void orc_tape_eval(void* s, const double* P, const long* tex_off, const long* mat_off, double* img_rgb, const double* dimg, double* grad,
+                          int threads)
+{
+  Scene& S = *(Scene*)s;
+  const unsigned npix = S.tape_p1 - S.tape_p0;
+  Eval64 E{S, P, tex_off, mat_off};
+  const double inv = 1.0 / (double)(S.tape_first + S.tape_frames);
+  std::fill(img_rgb, img_rgb + 3 * (size_t)npix, 0.0);
+  // the gradient is accumulated by one thread (small checking renders); the image alone in parallel
+  if (grad) threads = 1;
+  threads = std::max(1, threads);
+  std::atomic<unsigned> next(0);
+  auto worker = [&]() {
+    for (;;) {
+      unsigned b = next.fetch_add(64);
+      if (b >= npix) break;
+      unsigned e = std::min(npix, b + 64);
+      for (unsigned k = b; k < e; ++k) {
+        double acc[3] = {0, 0, 0};
+        double dl[3] = {0, 0, 0};
+        if (dimg)
+          for (int c = 0; c < 3; ++c) dl[c] = dimg[3 * (size_t)k + c] * inv;
+        for (unsigned fl = 0; fl < S.tape_frames; ++fl) {
+          const Tape& tp = S.tapes[(size_t)fl * npix + k];
+          if (!tp.valid) continue;
+          double L[3];
+          eval_tape(E, tp, L, dl, grad);
+          for (int c = 0; c < 3; ++c) acc[c] += L[c];
+        }
+        for (int c = 0; c < 3; ++c) img_rgb[3 * (size_t)k + c] = acc[c] * inv;
+      }
+    }
+  };
+  std::vector<std::thread> th;
+  for (int i = 1; i < threads; ++i) th.emplace_back(worker);
+  worker();
+  for (auto& x : th) x.join();
 }

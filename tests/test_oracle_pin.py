@@ -233,3 +233,41 @@ def test_translucent_oracle_is_deterministic_and_well_formed():
     np.testing.assert_allclose(np.linalg.norm(pr[:, 6:9], axis=1), 1.0, atol=1e-5)
     assert np.all((pr[:, 15:18] >= 0) & (pr[:, 15:18] <= 1)) and np.all(pr[:, 9:12] >= 0)
     assert np.any(pr[:, 9:12] > 0)
+
+
+def test_tape_gradient_matches_fp64_central_differences():
+    """The FP64 path-tape gradient (the adjoint's reference) against FP64 central differences of the
+    loss: albedo texels (next-event estimates and bounce weights), GGX roughness texels and the six
+    dipole sigmas (Beer transmittance and dipole gathers)."""
+    from open_rendering_framework_b200 import scenes
+
+    data, (dif, met, tr) = scenes.inverse_scene(16, 16, subdiv=2, tex_res=18, probe_samples=24, seed=1)
+    O = oc.OracleScene(data)
+    O.record(True)
+    acc, _ = O.render(0, 3, accum=np.zeros((16, 16, 4), np.float32), threads=4)
+    tex_off, mat_off, n = O.param_layout([dif, met, tr])
+    P = np.concatenate([dif.texture.ravel(), met.texture.ravel(), np.asarray(tr.absorption, np.float32),
+                        np.asarray(tr.scattering, np.float32)]).astype(np.float64)
+    img, _ = O.tape_eval(P, tex_off, mat_off)
+    # the tape re-evaluates the rendered image
+    assert np.max(np.abs(img - acc[..., :3].reshape(-1, 3)) / np.maximum(np.abs(acc[..., :3].reshape(-1, 3)), 1e-6)) < 1e-3
+    target = img * 0.5 + 0.01
+    _, g = O.tape_eval(P, tex_off, mat_off, dimg=2.0 * (img - target))
+
+    def loss(Pv):
+        im, _ = O.tape_eval(Pv, tex_off, mat_off)
+        return np.sum((im - target) ** 2)
+
+    nz = np.nonzero(g)[0]
+    n_alb = dif.texture.size
+    alb = nz[nz < n_alb]
+    rgh = nz[(nz >= n_alb) & (nz < n - 6)]
+    assert len(alb) > 10 and len(rgh) > 5
+    rng = np.random.default_rng(2)
+    pick = list(rng.choice(alb, 8, replace=False)) + list(rng.choice(rgh, 5, replace=False)) + list(range(n - 6, n))
+    for i in pick:
+        Pp, Pm = P.copy(), P.copy()
+        Pp[i] += 1e-4
+        Pm[i] -= 1e-4
+        fd = (loss(Pp) - loss(Pm)) / 2e-4
+        assert abs(fd - g[i]) <= 1e-5 * abs(fd) + 1e-12, (i, fd, g[i])
