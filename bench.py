@@ -12,6 +12,12 @@ procedural sky light) rendered as one batch: one step = one batch render of ever
 CUDA-graph launch, with the engine options from the autotuner.  The same frames rendered scene after
 scene through single-scene passes (the plain path) are timed beside it (`plain`).
 
+--workload adjoint: the differentiable configuration -- the single-scene geometry at 5 subdivisions
+with a 256^2 x 3 albedo texture on the box, a 256^2 GGX roughness texture on the conductor sphere and
+a dipole sphere whose sigma_a / sigma_s' are parameters (all seeded U[0.1, 0.9]), 256 x 256 x 64 spp,
+depth 6; L2 loss against a target rendered at 1024 spp from other seeded parameters.  One step = the
+differentiable forward render + the path-replay adjoint; `forward` reports the forward alone.
+
 --workload subsurface: 1024 x 1024 pixels x 256 frames (--spp) of the translucent scene: a
 327,680-triangle jittered icosphere with the dipole BSSRDF (standard; --dipole directional), 4,096
 probes per frame (2^20 over the 256 frames), lit by a 2048 x 1024 procedural sky with a sun lobe of
@@ -60,7 +66,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="single_scene", choices=["single_scene", "subsurface", "batched"])
+    ap.add_argument("--workload", default="single_scene", choices=["single_scene", "subsurface", "batched", "adjoint"])
     ap.add_argument("--scenes", type=int, default=64, help="batched workload: number of scenes")
     ap.add_argument("--spp", type=int, default=None, help="frames per step (default 64, subsurface 256)")
     ap.add_argument("--width", type=int, default=None)
@@ -80,6 +86,10 @@ def workload(args):
     from open_rendering_framework_b200 import scene as sc
     from open_rendering_framework_b200 import scenes
 
+    if args.workload == "adjoint":
+        w = args.width or 256
+        data, _ = scenes.inverse_scene(w, w, subdiv=5, tex_res=256, seed=0)
+        return data, args.spp or 64, ADJOINT
     if args.workload == "subsurface":
         w, h = args.width or 1024, args.height or 1024
         model = sc.DIRECTIONAL_DIPOLE if args.dipole == "directional" else sc.STANDARD_DIPOLE
@@ -412,6 +422,85 @@ def run_batched(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+ADJOINT = ("inverse rendering 256x256, 64 spp, depth 6, RR from depth 3: 12-triangle box with a 256x256x3 albedo texture, "
+           "5-subdivision GGX conductor icosphere with a 256x256 roughness texture, 5-subdivision standard-dipole icosphere "
+           "(sigma_a, sigma_s' per RGB, 500 probes per frame), quad light; parameters seeded U[0.1,0.9]; L2 loss against a "
+           "1024-spp target from other seeded parameters; forward + path-replay adjoint per step")
+
+
+def run_adjoint(args, world, rank, local):
+    import torch
+
+    from open_rendering_framework_b200 import diff
+    from open_rendering_framework_b200 import scene as sc
+    from open_rendering_framework_b200 import scenes
+
+    torch.cuda.set_device(local)
+    W = args.width or 256
+    spp = args.spp or 64
+    data, (dif, met, tr) = scenes.inverse_scene(W, W, subdiv=5, tex_res=256, seed=0)
+    tdata, _ = scenes.inverse_scene(W, W, subdiv=5, tex_res=256, seed=1)
+    T = sc.Renderer(tdata, device=local)
+    T.render(1024)
+    target = torch.from_numpy(T.readback()[..., :3].copy()).cuda()
+    T.close()
+    DS = diff.DiffScene(data, dif, met, tr, device=local)
+    albedo = torch.from_numpy(dif.texture.copy()).cuda().requires_grad_()
+    rough = torch.from_numpy(met.texture.copy()).cuda().requires_grad_()
+    sigma = torch.tensor(list(tr.absorption) + list(tr.scattering), dtype=torch.float32, device="cuda").requires_grad_()
+    path_samples = W * W * spp
+
+    def step():
+        for t in (albedo, rough, sigma):
+            t.grad = None
+        img = diff.render(DS, spp, albedo, rough, sigma)
+        fst = DS.stats()
+        loss = ((img - target) ** 2).sum()
+        loss.backward()
+        ast = DS.stats()
+        return float(loss.item()), fst, ast
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    fwd_ms, adj_ms, seg, gathers = 0.0, 0.0, 0, 0
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        e0.record()
+        for _ in range(args.steps):
+            loss, fst, ast = step()
+            fwd_ms += fst.gpu_ms
+            adj_ms += ast.gpu_ms
+            seg += fst.segments
+            gathers += fst.dipole_gathers
+        e1.record()
+        torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    dev_ms = fwd_ms + adj_ms
+    value = args.steps * path_samples / (dev_ms * 1e-3) / 1e6
+    g = [albedo.grad, rough.grad, sigma.grad]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup),
+        "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": ADJOINT, "path_samples_per_step": path_samples, "parameters": int(sum(t.numel() for t in g)),
+                   "l2": "per-path forward state of %.2f GB re-read by the adjoint" % (path_samples * 16 * 8 / 1e9)},
+        "forward": {"value": args.steps * path_samples / (fwd_ms * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": fwd_ms / args.steps},
+        "adjoint_ms_per_step": adj_ms / args.steps,
+        "fwd_plus_adjoint_over_forward": dev_ms / fwd_ms,
+        "e2e": {"value": args.steps * path_samples / (e2e_ms * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": 6 * 4 + 64,
+                "d2h_bytes_per_step": 4 + 24, "what": "torch.autograd.Function forward + loss + backward, host sigma update and loss read-back"},
+        "loss": loss,
+        "grad_norms": [float(t.norm().item()) for t in g],
+        "gpu_launches": int(fst.kernel_launches + ast.kernel_launches) * args.steps,
+        "clocks": clocks.summary(),
+        "stats": {"segments_per_path": seg / (args.steps * path_samples), "dipole_gathers_per_step": gathers / args.steps},
+    }
+    DS.close()
+    print(json.dumps(line), flush=True)
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -556,6 +645,9 @@ def main():
             run_reference(args, world, rank)
         elif args.workload == "batched":
             run_batched(args, world, rank, local)
+        elif args.workload == "adjoint":
+            if rank == 0:
+                run_adjoint(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:
