@@ -100,6 +100,7 @@ enum {
   PT_ROUGH_TRANSPARENT_SHADER = 3, /* rough_transparent_shader.cu  */
   PT_METALLIC_SHADER = 4,          /* metallic_shader.cu           */
   PT_TRANSLUCENT_SHADER = 5,       /* subsurface_scattering_shader.cu */
+  PT_ROUGH_TRANSLUCENT_SHADER = 6, /* rough_subsurface_scattering_shader.cu */
   PT_AREA_LIGHT_MATERIAL = 100     /* arealight_shader.cu          */
 };
 /* Microfacet model / normal distribution enums: structs.h:242-261. */
@@ -140,6 +141,20 @@ typedef struct pt_translucent_params {
   float scale;
   uint32_t dipole_model;
 } pt_translucent_params;
+/* RoughTranslucentMaterial (RoughTranslucentMaterial.cpp:360-395): the translucent parameters plus
+ * mtl["roughness"], mtl["microfacet_model"] and mtl["normal_distribution"] of its rough dielectric
+ * boundary. */
+typedef struct pt_rough_translucent_params {
+  float scattering[3];
+  float absorption[3];
+  float meancosine[3];
+  float ior;
+  float scale;
+  uint32_t dipole_model;
+  float roughness[2];
+  uint32_t microfacet_model;
+  uint32_t normal_distribution;
+} pt_rough_translucent_params;
 /* gi["radiance"] of a TriangleAreaLight's geometry (Light.cpp:242). */
 typedef struct pt_area_light_params { float radiance[3]; } pt_area_light_params;
 

@@ -186,6 +186,27 @@ static pt_status make_material(uint32_t type, const void* params, size_t size, M
       m.b = make_float4(p->glass_absorption[0], p->glass_absorption[1], p->glass_absorption[2], 0.0f);
       return PT_OK;
     }
+    case PT_ROUGH_TRANSLUCENT_SHADER: {
+      if (size != sizeof(pt_rough_translucent_params)) return fail(PT_INVALID_ARG, "rough translucent material: wrong parameter size");
+      const pt_rough_translucent_params* r = (const pt_rough_translucent_params*)params;
+      if (!(r->roughness[0] > 0.0f && r->roughness[1] > 0.0f && std::isfinite(r->roughness[0]) && std::isfinite(r->roughness[1])))
+        return fail(PT_INVALID_ARG, "rough translucent material: roughness must be finite and > 0");
+      if (r->microfacet_model > PT_MULTISCATTERING_MODEL || r->normal_distribution > PT_GGX_DISTRIBUTION)
+        return fail(PT_INVALID_ARG, "rough translucent material: bad microfacet_model or normal_distribution");
+      pt_translucent_params t;
+      memcpy(t.scattering, r->scattering, sizeof t.scattering);
+      memcpy(t.absorption, r->absorption, sizeof t.absorption);
+      memcpy(t.meancosine, r->meancosine, sizeof t.meancosine);
+      t.ior = r->ior;
+      t.scale = r->scale;
+      t.dipole_model = r->dipole_model;
+      pt_status st = make_material(PT_TRANSLUCENT_SHADER, &t, sizeof t, m, sc);
+      if (st != PT_OK) return st;
+      m.type = PT_ROUGH_TRANSLUCENT_SHADER;
+      m.dist = r->normal_distribution;
+      m.a = make_float4(r->scale, r->roughness[0], r->roughness[1], __int_as_float_host((int)r->microfacet_model));
+      return PT_OK;
+    }
     case PT_TRANSLUCENT_SHADER: {
       if (size != sizeof(pt_translucent_params)) return fail(PT_INVALID_ARG, "translucent material: wrong parameter size");
       const pt_translucent_params* p = (const pt_translucent_params*)params;
@@ -545,7 +566,7 @@ pt_status pt_mesh_add(pt_ctx* ctx, const float* positions, uint32_t n_vertices, 
     }
     c.tri_info.push_back(info);
   }
-  if (c.mats[material_id].type == PT_TRANSLUCENT_SHADER) {
+  if (c.mats[material_id].type == PT_TRANSLUCENT_SHADER || c.mats[material_id].type == PT_ROUGH_TRANSLUCENT_SHADER) {
     // a translucent object with its own probe set; the material's translucent_index is the last
     // object registered with it (OptixSceneLoader.cpp:509-510)
     if (c.trans_objs.size() >= 1024) return fail(PT_CAP_EXCEEDED, "pt_mesh_add: at most 1024 translucent objects");
@@ -737,7 +758,8 @@ pt_status pt_get_scattering_properties(pt_ctx* ctx, uint32_t material_id, void* 
 {
   if (!ctx || !out260) return fail(PT_INVALID_ARG, "pt_get_scattering_properties: null argument");
   if (material_id >= ctx->c.mats.size()) return fail(PT_INVALID_ARG, "pt_get_scattering_properties: no such material");
-  if (ctx->c.mats[material_id].type != PT_TRANSLUCENT_SHADER) return fail(PT_INVALID_ARG, "pt_get_scattering_properties: not a translucent material");
+  if (ctx->c.mats[material_id].type != PT_TRANSLUCENT_SHADER && ctx->c.mats[material_id].type != PT_ROUGH_TRANSLUCENT_SHADER)
+    return fail(PT_INVALID_ARG, "pt_get_scattering_properties: not a translucent material");
   memcpy(out260, &ctx->c.scat[material_id], sizeof(ScatDev));
   return PT_OK;
 }

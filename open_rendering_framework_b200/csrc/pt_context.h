@@ -55,7 +55,7 @@ struct Wavefront {
   // translucent objects: the per-path stack of pending dipole gathers ([slot][path]) and the probes
   uint32_t gather_slots = 0;
   uint64_t gather_cap = 0;
-  DevBuf g_a, g_b, g_c;
+  DevBuf g_a, g_b, g_c, g_d;
   uint64_t probe_cap = 0;                     // PositionSample records held
   DevBuf probes;                              // PositionSample (80 B) per probe, [frame][object][sample]
   DevBuf pc_pos, pc_wl, pc_nrm, pc_tr, pc_cnt;// probes with L != 0, compacted in order per (frame, object)

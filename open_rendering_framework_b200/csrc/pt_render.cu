@@ -66,6 +66,7 @@ struct WfDev {
   float4* g_a;
   float4* g_b;
   float2* g_c;
+  float4* g_d;  // the gather's weight (rough boundary) and 1, or (1, 1, 1, 0) for a smooth boundary
   uint32_t g_slots;
   // adjoint renders: per path (image gradient of the path, pending kind) and (pending d w / w, index)
   float4* adj_a;
@@ -482,6 +483,7 @@ __device__ __forceinline__ int class_of(uint32_t type)
     case MAT_METAL: return QC_METAL;
     case MAT_ROUGH_GLASS: return QC_GLASS;
     case MAT_TRANSLUCENT: return QC_TRANS;
+    case MAT_ROUGH_TRANSLUCENT: return QC_TRANS;
     case MAT_LIGHT: return QC_LIGHT;
     default: return -1;
   }
@@ -1030,6 +1032,143 @@ __global__ void __launch_bounds__(kBlock) k_shade_glass(WfDev w)
 }
 
 // ------------------------------------------------------------------ translucent objects
+// rough_subsurface_scattering_shader.cu:56-455 (REFLECT, TRANSMIT, DIRECTLIGHT and RND_64 defined),
+// one vertex: the microfacet normal from two MD5 draws; a light picked with an MD5 draw and its
+// reflection-only estimate (the multiscatter model: the multiscatter dielectric BSDF), with the shadow
+// ray traced here because the multiscatter evaluation draws tea randoms only when the light is
+// visible; then the smooth shader's Beer roulette and Fresnel choice on the microfacet normal, the
+// refraction / reflection weight on the child, and on a refraction from outside the dipole gather
+// (pushed with that weight; its draws must also exceed 0.001).  Returns whether the path continues.
+__device__ bool rough_translucent_vertex(const SceneDev& S, const WfDev& w, uint32_t pid, const uint4& rg, int depth, const float4& h,
+                                         const float4& o, const float4& d4, const int4& info, const MatDev& m, const ScatDev& P,
+                                         uint32_t& overflow, uint32_t& clamped, int& capped)
+{
+  const float3 d = ld3(d4);
+  float3 normal = shading_normal(S, info, h.y, h.z, __float_as_int(h.w));
+  const float3 ffnormal = faceforward(normal, -d, normal);
+  const float3 hit_pos = ld3(o) + h.x * d;
+  const float3 w_i = -d;
+  float recip_ior = 1.0f / P.relative_ior;
+  float3 beam_T = f3s(1.0f);
+  uint32_t t = rg.x;
+  uint2 t64 = make_uint2(rg.y, rg.z);
+  const float reflect_xi = rnd_md5(t64);
+  const float z1 = rnd_md5(t64);
+  const float z2 = rnd_md5(t64);
+  const float a_x = m.a.y, a_y = m.a.z;
+  const uint32_t model = __float_as_uint(m.a.w), dist = m.dist;
+  const float3 mn = model == WALTER ? sample_normal(dist, ffnormal, z1, z2, a_x) : sample_visible_normal(dist, w_i, ffnormal, a_x, a_y, z1, z2, &capped);
+  const float cos_theta_i = dot(w_i, mn);
+  const bool inside = dot(w_i, normal) < 0.0f;
+  bool emit = (rg.w & META_EMIT) != 0;
+  const float4 t4 = w.thr[pid];
+  // light sample (:93-152)
+  uint32_t li = (uint32_t)((float)S.n_lights * rnd_md5(t64));
+  if (li >= (uint32_t)S.n_lights) { li = (uint32_t)S.n_lights - 1; ++clamped; }
+  const float light_pdf = 1.0f / (float)S.n_lights;
+  const LightRaw ls = S.lights[li];
+  float3 w_l, light_radiance;
+  float ldist;
+  eval_direct(S, hit_pos, ls, w_l, light_radiance, ldist, t, clamped);
+  light_radiance = light_radiance / light_pdf;
+  const float cos_l = dot(ffnormal, w_l);
+  if (!inside && cos_l > 0.0f) {
+    const float V = trace_any(trav_geom(S), hit_pos, w_l, S.integ.scene_epsilon, ldist) ? 0.0f : 1.0f;
+    if (V > 0.0f) {
+      const float3 Li = V * light_radiance;
+      float3 add;
+      if (model == MULTISCATTERING) {
+        const float brdf = ms_dielectric_eval(dist, to_local(w_i, ffnormal), to_local(w_l, ffnormal), recip_ior, a_x, a_y, t, 0u, &capped);
+        add = Li * brdf;
+        emit = false;
+      } else {
+        const float3 rn = normalize(w_i + w_l);
+        const float cr = dot(rn, w_l);
+        float Rr = 1.0f;
+        const float st2 = recip_ior * recip_ior * (1.0f - cr * cr);
+        if (st2 < 1.0f) Rr = fresnel_R(cr, sqrtf(1.0f - st2), recip_ior);
+        const float Gi = masking_G1_aniso(dist, w_i, rn, ffnormal, a_x, a_y);
+        const float Go = masking_G1_aniso(dist, w_l, rn, ffnormal, a_x, a_y);
+        const float D = eval_visible_normal(dist, w_i, rn, ffnormal, a_x, a_y);
+        const float wr = Gi * Go * D / (4.0f * fabsf(dot(w_i, ffnormal) * dot(w_l, ffnormal)));
+        add = Li * Rr * wr;
+        emit = true;
+      }
+      const float4 r = w.rad[pid];
+      w.rad[pid] = make_float4(r.x + t4.x * add.x, r.y + t4.y * add.y, r.z + t4.z * add.z, 0.0f);
+    }
+  }
+  uint32_t meta = rg.w & META_KEEP;
+  bool cont = false, gather = false, child_emit = true;
+  float3 nd = f3s(0.0f), weight = f3s(1.0f);
+  auto roulette_inside = [&]() -> bool {  // Beer transmittance inside, as the smooth shader
+    const float3 ext = m.model == DIRECTIONAL_DIPOLE ? P.deltaEddExtinction : P.extinction;
+    beam_T = expf3((-h.x) * ext);
+    const float prob = (beam_T.x + beam_T.y + beam_T.z) / 3.0f;
+    if (rnd_md5(t64) >= prob) return false;
+    beam_T = beam_T / prob;
+    recip_ior = P.relative_ior;
+    normal = -normal;
+    return true;
+  };
+  if (model == WALTER || model == VISIBLE_NORMALS) {
+    if (!inside || roulette_inside()) {
+      const float st2 = recip_ior * recip_ior * (1.0f - cos_theta_i * cos_theta_i);
+      float cos_t = 1.0f, R = 1.0f;
+      if (st2 < 1.0f) {
+        cos_t = sqrtf(1.0f - st2);
+        R = fresnel_R(cos_theta_i, cos_t, recip_ior);
+      }
+      if (reflect_xi >= R) {
+        nd = recip_ior * (cos_theta_i * mn - w_i) - mn * cos_t;
+        gather = !inside;
+      } else {
+        nd = 2.0f * cos_theta_i * mn - w_i;
+        child_emit = emit;
+      }
+      if (model == WALTER) {
+        const float G_i_m = masking_G1(dist, w_i, mn, ffnormal, a_x);
+        const float abs_i_m = fabsf(dot(w_i, mn)), abs_i_n = fabsf(dot(w_i, ffnormal)), abs_n_m = fabsf(dot(ffnormal, mn));
+        const float G_o_m = masking_G1(dist, nd, mn, ffnormal, a_x);
+        weight = f3s(1.0f) * (abs_i_m * G_i_m * G_o_m / (abs_i_n * abs_n_m));
+      } else {
+        weight = f3s(1.0f) * masking_G1_aniso(dist, nd, mn, ffnormal, a_x, a_y);
+      }
+      cont = true;
+    }
+  } else {  // MULTISCATTERING_MODEL (:287-452)
+    uint32_t order = 0;
+    const float3 w_o = to_world(ms_dielectric_sample(dist, to_local(w_i, normal), 1.0f / P.relative_ior, a_x, a_y, t, order, &capped), normal);
+    const bool is_refraction = dot(w_o, ffnormal) < 0.0f;
+    if (!inside || roulette_inside()) {
+      nd = w_o;
+      gather = is_refraction && !inside;
+      cont = true;
+    }
+  }
+  if (cont) {
+    if (gather && !(rg.w & META_PROBE)) {
+      const uint32_t slot = meta >> META_GSHIFT;
+      if (slot < w.g_slots) {
+        size_t at = (size_t)slot * w.cap + pid;
+        w.g_a[at] = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, t4.x);
+        w.g_b[at] = make_float4(normal.x, normal.y, normal.z, t4.y);
+        w.g_c[at] = make_float2(t4.z, __int_as_float(info.w));
+        w.g_d[at] = make_float4(weight.x, weight.y, weight.z, 1.0f);
+        meta += 1u << META_GSHIFT;
+      } else {
+        ++overflow;
+      }
+    }
+    const float3 nt = ld3(t4) * weight * beam_T;
+    w.ray_o[pid] = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, 0.0f);
+    w.ray_d[pid] = make_float4(nd.x, nd.y, nd.z, 0.0f);
+    w.thr[pid] = make_float4(nt.x, nt.y, nt.z, 0.0f);
+  }
+  w.rng[pid] = make_uint4(t, t64.x, t64.y, meta | (uint32_t)(depth + 1) | (child_emit ? META_EMIT : 0u));
+  return cont;
+}
+
 // subsurface_scattering_shader.cu:55-201 with REFLECT, TRANSMIT and RND_64 defined: the Fresnel
 // choice between the reflected and the refracted ray (one MD5 draw), and inside the object Beer
 // transmittance over the segment with Russian roulette on its mean (extinction, or the
@@ -1050,7 +1189,8 @@ __global__ void __launch_bounds__(kBlock) k_shade_translucent(WfDev w)
   __shared__ uint32_t sm[kWarps + 1];
   const uint32_t n = w.cnt[CNT_Q_TRANS];
   const uint32_t* q = w.q_mat + (size_t)QC_TRANS * w.cap;
-  uint32_t overflow = 0;
+  uint32_t overflow = 0, clamped = 0;
+  int capped = 0;
   for (uint32_t base = blockIdx.x * kBlock; base < n; base += gridDim.x * kBlock) {
     uint32_t i = base + threadIdx.x;
     bool cont = false;
@@ -1067,6 +1207,9 @@ __global__ void __launch_bounds__(kBlock) k_shade_translucent(WfDev w)
         int4 info = __ldg(S.tri_info + prim);
         const MatDev& m = S.mats[info.w];
         const ScatDev& P = S.scat[info.w];
+        if (m.type == MAT_ROUGH_TRANSLUCENT) {
+          cont = rough_translucent_vertex(S, w, pid, rg, depth, h, o, d4, info, m, P, overflow, clamped, capped);
+        } else {
         float3 d = ld3(d4);
         float3 no = shading_normal(S, info, h.y, h.z, prim);
         float3 xo = ld3(o) + h.x * d;
@@ -1110,6 +1253,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_translucent(WfDev w)
                 w.g_a[at] = make_float4(xo.x, xo.y, xo.z, t4.x);
                 w.g_b[at] = make_float4(no.x, no.y, no.z, t4.y);
                 w.g_c[at] = make_float2(t4.z, __int_as_float(info.w));
+                w.g_d[at] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
                 if constexpr (kAdj) {
                   const ItemDev& it = w.items[w.path_item[pid]];
                   const uint64_t local = pid - it.path_begin;
@@ -1134,12 +1278,15 @@ __global__ void __launch_bounds__(kBlock) k_shade_translucent(WfDev w)
           if (kAdj && inside) set_pending(w, pid, PEND_SIGMA, (uint32_t)info.w, 0u, f3s(-h.x * m.a.x));
         }
         w.rng[pid] = make_uint4(rg.x, t64.x, t64.y, meta | (uint32_t)(depth + 1) | META_EMIT);
+        }
       }
     }
     uint32_t c_slot = block_slot(cont, w.cnt + w.out_slot, sm);
     if (cont) w.q_out[c_slot] = pid;
   }
   if (overflow) atomicAdd(cnt64(w.cnt, CNT_ERROR), (unsigned long long)overflow);
+  if (clamped) atomicAdd(cnt64(w.cnt, CNT_CLAMPED), (unsigned long long)clamped);
+  if (capped) atomicAdd(cnt64(w.cnt, CNT_CAPPED), (unsigned long long)capped);
 }
 
 // Paths with pending dipole gathers, appended to `out` (warp-aggregated).
@@ -1196,6 +1343,9 @@ __global__ void __launch_bounds__(kBlock) k_gather(WfDev w, SssDev g, const uint
         continue;
       }
       const float3 xo = ld3(a), no = ld3(b), thr = f3(a.w, b.w, c.x);
+      const float4 gd = w.g_d[at];
+      const bool rough = gd.w != 0.0f;  // rough boundary: draws must exceed 0.001, terms carry the weight
+      const float3 gw = ld3(gd);
       const MatDev& m = S.mats[mat];
       const ScatDev& P = S.scat[mat];
       const uint32_t set_in_item = fl * S.n_trans + m.aux;
@@ -1236,10 +1386,12 @@ __global__ void __launch_bounds__(kBlock) k_gather(WfDev w, SssDev g, const uint
           float3 pos = ld3(__ldg(g.pc_pos + pb + k));
           float dist = length(xo - pos);
           float exp_term = expf(-dist * chosen);
-          if (rnd_md5(t64) < exp_term) {
+          const float rn = rnd_md5(t64);
+          if (rn < exp_term && (!rough || rn > 0.001f)) {
             float3 wl = ld3(__ldg(g.pc_wl + pb + k));
             float3 pn = ld3(__ldg(g.pc_nrm + pb + k)), pt = ld3(__ldg(g.pc_tr + pb + k));
-            acc = acc + wl * dirpole_bssrdf(pos, pn, pt, xo, no, P) / exp_term;
+            float3 term = wl * dirpole_bssrdf(pos, pn, pt, xo, no, P) / exp_term;
+            acc = acc + (rough ? term * gw : term);
           }
         }
       } else {
@@ -1248,9 +1400,11 @@ __global__ void __launch_bounds__(kBlock) k_gather(WfDev w, SssDev g, const uint
           float3 pos = ld3(__ldg(g.pc_pos + pb + k));
           float dist = length(xo - pos);
           float exp_term = expf(-dist * chosen);
-          if (rnd_md5(t64) < exp_term) {
+          const float rn = rnd_md5(t64);
+          if (rn < exp_term && (!rough || rn > 0.001f)) {
             float3 wl = ld3(__ldg(g.pc_wl + pb + k));
-            acc = acc + wl * dipole_bssrdf(dist, sd) / exp_term;
+            float3 term = wl * dipole_bssrdf(dist, sd) / exp_term;
+            acc = acc + (rough ? term * gw : term);
           }
         }
       }
@@ -1319,6 +1473,18 @@ __global__ void __launch_bounds__(kBlock) k_probe_gen(WfDev w, SssDev g, uint64_
         nrm = normalize(perp);
       }
       const float recip_ior = 1.0f / P.relative_ior;
+      // rough objects: the probe's normal is a microfacet normal sampled with two MD5 draws (:130-151)
+      const MatDev& om = S.mats[ob.x];
+      const bool rough = om.type == MAT_ROUGH_TRANSLUCENT;
+      const float r_ax = om.a.y, r_ay = om.a.z;
+      const uint32_t r_model = __float_as_uint(om.a.w), r_dist = om.dist;
+      float3 mnorm = nrm;
+      int capped = 0;
+      auto microfacet = [&](const float3& wdir) {
+        const float z1 = rnd_md5(t64);
+        const float z2 = rnd_md5(t64);
+        mnorm = r_model == WALTER ? sample_normal(r_dist, nrm, z1, z2, r_ax) : sample_visible_normal(r_dist, wdir, nrm, r_ax, r_ay, z1, z2, &capped);
+      };
       float3 Le, w_i, dir = f3s(0.0f);
       if (rnd_lcg(t) < 0.5f) {
         uint32_t li = (uint32_t)((float)S.n_lights * rnd_md5(t64));
@@ -1328,6 +1494,7 @@ __global__ void __launch_bounds__(kBlock) k_probe_gen(WfDev w, SssDev g, uint64_
         float r = 0.0f;
         eval_direct(S, pos, ls, w_i, Le, r, t, clamped);
         dir = w_i;
+        if (rough) microfacet(w_i);
         float cos_i = fmaxf(dot(w_i, nrm), 0.0f);
         if (cos_i > 0.0f) {
           float att = trace_any(S, pos, w_i, S.integ.scene_epsilon, r) ? 0.0f : 1.0f;
@@ -1338,6 +1505,7 @@ __global__ void __launch_bounds__(kBlock) k_probe_gen(WfDev w, SssDev g, uint64_
         w.rad[pid] = make_float4(Le.x, Le.y, Le.z, 0.0f);
       } else {
         w_i = sample_cosine_weighted(nrm, t);
+        if (rough) microfacet(w_i);
         w.ray_o[pid] = make_float4(pos.x, pos.y, pos.z, 0.0f);
         w.ray_d[pid] = make_float4(w_i.x, w_i.y, w_i.z, 0.0f);
         w.thr[pid] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
@@ -1346,18 +1514,30 @@ __global__ void __launch_bounds__(kBlock) k_probe_gen(WfDev w, SssDev g, uint64_
         w.path_item[pid] = (uint16_t)item;
         indirect = true;
       }
-      float cos_i = fmaxf(dot(w_i, nrm), 0.0f);
+      float cos_i = fmaxf(dot(w_i, mnorm), 0.0f);
       float cos_i2 = cos_i * cos_i;
       float st2 = recip_ior * recip_ior * (1.0f - cos_i2);
       float cos_t = sqrtf(1.0f - st2);
-      float3 tr = recip_ior * (cos_i * nrm - w_i) - nrm * cos_t;
+      float3 tr = recip_ior * (cos_i * mnorm - w_i) - mnorm * cos_t;
       float T12 = 1.0f - fresnel_R(cos_i, cos_t, recip_ior);
+      float wgt = T12;  // 1 * T12
+      if (rough) {  // :232-266
+        if (r_model == WALTER) {
+          const float G_i_m = masking_G1_aniso(r_dist, w_i, mnorm, nrm, r_ax, r_ay);
+          const float abs_i_m = fabsf(dot(w_i, mnorm)), abs_i_n = fabsf(dot(w_i, nrm)), abs_n_m = fabsf(dot(nrm, mnorm));
+          const float G_o_m = masking_G1_aniso(r_dist, tr, mnorm, nrm, r_ax, r_ay);
+          wgt = (1.0f * (abs_i_m * G_i_m / (abs_i_n * abs_n_m) * G_o_m)) * T12;
+        } else if (r_model == VISIBLE_NORMALS) {
+          wgt = (1.0f * masking_G1_aniso(r_dist, tr, mnorm, nrm, r_ax, r_ay)) * T12;
+        }
+      }
+      if (capped) atomicAdd(cnt64(w.cnt, CNT_CAPPED), 1ull);
       float4* rec = g.probes + 5 * j;
       rec[0] = make_float4(pos.x, pos.y, pos.z, dir.x);
-      rec[1] = make_float4(dir.y, dir.z, nrm.x, nrm.y);
-      rec[2] = make_float4(nrm.z, 0.0f, 0.0f, 0.0f);
-      rec[3] = make_float4(tr.x, tr.y, tr.z, T12);
-      rec[4] = make_float4(T12, T12, (float)triangles * area, indirect ? 1.0f : 0.0f);
+      rec[1] = make_float4(dir.y, dir.z, mnorm.x, mnorm.y);
+      rec[2] = make_float4(mnorm.z, 0.0f, 0.0f, 0.0f);
+      rec[3] = make_float4(tr.x, tr.y, tr.z, wgt);
+      rec[4] = make_float4(wgt, wgt, (float)triangles * area, indirect ? 1.0f : 0.0f);
     }
     uint32_t slot = block_slot(indirect, w.cnt + w.in_slot, sm);
     if (indirect) w.q_in[slot] = (uint32_t)pid;
@@ -1528,6 +1708,7 @@ static pt_status ensure_sss(Context& c, uint64_t cap, uint32_t slots, uint64_t r
     st = wf.g_a.reserve(n * sizeof(float4), "dipole gather stack");
     if (st == PT_OK) st = wf.g_b.reserve(n * sizeof(float4), "dipole gather stack");
     if (st == PT_OK) st = wf.g_c.reserve(n * sizeof(float2), "dipole gather stack");
+    if (st == PT_OK) st = wf.g_d.reserve(n * sizeof(float4), "dipole gather stack");
     if (st != PT_OK) {
       wf.gather_cap = 0;
       wf.gather_slots = 0;
@@ -1722,6 +1903,7 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
   w.g_a = L.sss ? wf.g_a.as<float4>() : nullptr;
   w.g_b = L.sss ? wf.g_b.as<float4>() : nullptr;
   w.g_c = L.sss ? wf.g_c.as<float2>() : nullptr;
+  w.g_d = L.sss ? wf.g_d.as<float4>() : nullptr;
   w.g_slots = L.sss ? wf.gather_slots : 0;
   w.scenes = c.d_scene_tab.as<SceneDev>();
   w.path_item = wf.path_item.as<uint16_t>();
@@ -1926,9 +2108,12 @@ pt_status pt_render_adjoint(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames
   if (!c.differentiable || !c.adj_valid) return fail(PT_NOT_READY, "pt_render_adjoint: needs a forward pt_render_frames with the differentiable option on");
   if (first_frame != c.adj_first || n_frames != c.adj_frames)
     return fail(PT_INVALID_ARG, "pt_render_adjoint: frames differ from the last differentiable forward render");
-  for (const MatDev& m : c.mats)
+  for (const MatDev& m : c.mats) {
     if (m.type == PT_METALLIC_SHADER && __float_as_int_host(m.tmap.w) >= 0 && m.dist != PT_GGX_DISTRIBUTION)
       return fail(PT_INVALID_ARG, "pt_render_adjoint: roughness gradients are implemented for the GGX distribution");
+    if (m.type == PT_ROUGH_TRANSLUCENT_SHADER)
+      return fail(PT_INVALID_ARG, "pt_render_adjoint: rough translucent materials are not differentiable");
+  }
   pt_status st = prepare_scene(c, "pt_render_adjoint");
   if (st != PT_OK) return st;
   SceneFacts f;

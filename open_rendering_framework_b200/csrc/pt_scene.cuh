@@ -51,12 +51,13 @@ PT_HD int as_int(float f)
 constexpr uint32_t kLeafFlag = 0x80000000u;
 constexpr int kMaxDepth = 62;  // depth bound of the build; the traversal trail has 64 bits
 
-enum MatType : uint32_t { MAT_DIFFUSE = 0, MAT_ROUGH_GLASS = 3, MAT_METAL = 4, MAT_TRANSLUCENT = 5, MAT_LIGHT = 100 };
+enum MatType : uint32_t { MAT_DIFFUSE = 0, MAT_ROUGH_GLASS = 3, MAT_METAL = 4, MAT_TRANSLUCENT = 5, MAT_ROUGH_TRANSLUCENT = 6, MAT_LIGHT = 100 };
 enum DipoleModel : uint32_t { STANDARD_DIPOLE = 0, DIRECTIONAL_DIPOLE = 1 };
 
 // Material record, 16-byte aligned (128 B).
 struct __align__(16) MatDev {
-  uint32_t type, model, dist, aux;  // translucent: model = dipole_model, aux = translucent_index
+  uint32_t type, model, dist, aux;  // translucent: model = dipole_model, aux = translucent_index (rough: dist = normal distribution,
+                                    // a = (scale, roughness x, roughness y, microfacet model))
   float4 a;   // diffuse: color.xyz | metal: roughness.xy | glass: ior, roughness | light: radiance.xyz
   float4 b;   // glass: absorption.xyz
   Cx3 eta;    // metal: 1 / ior (metallic_shader.cu:61), computed on the host

@@ -21,6 +21,7 @@ DIFFUSE_SHADER = 0
 ROUGH_TRANSPARENT_SHADER = 3
 METALLIC_SHADER = 4
 TRANSLUCENT_SHADER = 5
+ROUGH_TRANSLUCENT_SHADER = 6
 AREA_LIGHT_MATERIAL = 100
 STANDARD_DIPOLE, DIRECTIONAL_DIPOLE = 0, 1
 WALTER_MODEL, VISIBLE_NORMALS_MODEL, MULTISCATTERING_MODEL = 0, 1, 2
@@ -49,6 +50,12 @@ class AreaLightParams(ctypes.Structure):
 class TranslucentParams(ctypes.Structure):
     _fields_ = [("scattering", ctypes.c_float * 3), ("absorption", ctypes.c_float * 3), ("meancosine", ctypes.c_float * 3),
                 ("ior", ctypes.c_float), ("scale", ctypes.c_float), ("dipole_model", ctypes.c_uint32)]
+
+
+class RoughTranslucentParams(ctypes.Structure):
+    _fields_ = [("scattering", ctypes.c_float * 3), ("absorption", ctypes.c_float * 3), ("meancosine", ctypes.c_float * 3),
+                ("ior", ctypes.c_float), ("scale", ctypes.c_float), ("dipole_model", ctypes.c_uint32), ("roughness", ctypes.c_float * 2),
+                ("microfacet_model", ctypes.c_uint32), ("normal_distribution", ctypes.c_uint32)]
 
 
 # ScatteringMaterialProperties (structs.h:116-144, 260 bytes) and PositionSample (:105-114, 80 bytes).
@@ -294,6 +301,26 @@ class TranslucentMaterial:
         self.dipole_model = int(m)
 
 
+class RoughTranslucentMaterial(TranslucentMaterial):
+    """Rough translucent surface (RoughTranslucentMaterial.cpp, shader rough_subsurface_scattering_shader.cu):
+    the dipole BSSRDF behind a rough dielectric boundary with mtl["roughness"], mtl["microfacet_model"]
+    and mtl["normal_distribution"] (defaults: roughness 0.1, Walter model, Beckmann distribution)."""
+    type = ROUGH_TRANSLUCENT_SHADER
+
+    def __init__(self, roughness=(0.1, 0.1), microfacet_model=WALTER_MODEL, normal_distribution=BECKMANN_DISTRIBUTION, **kw):
+        super().__init__(**kw)
+        self.roughness = tuple(float(x) for x in roughness)
+        self.microfacet_model = int(microfacet_model)
+        self.normal_distribution = int(normal_distribution)
+
+    def params(self):
+        return RoughTranslucentParams(_f3(self.scattering), _f3(self.absorption), _f3(self.meancosine), self.ior, self.scale, self.dipole_model,
+                                      (ctypes.c_float * 2)(*self.roughness), self.microfacet_model, self.normal_distribution)
+
+    def setRoughness(self, r):
+        self.roughness = tuple(float(x) for x in r)
+
+
 class AreaLightMaterial:
     """The emitter program TriangleAreaLight attaches to its geometry (arealight_shader.cu)."""
     type = AREA_LIGHT_MATERIAL
@@ -409,7 +436,7 @@ class SceneData:
         in mesh order (OptixSceneLoader::computeTranslucentGeometries)."""
         out, first = [], 0
         for m, mid in zip(self.meshes, self.mesh_material):
-            if getattr(m.material, "type", None) == TRANSLUCENT_SHADER:
+            if getattr(m.material, "type", None) in (TRANSLUCENT_SHADER, ROUGH_TRANSLUCENT_SHADER):
                 out.append((mid, first, len(m.vindex)))
             first += len(m.vindex)
         return out

@@ -187,14 +187,20 @@ def subsurface_scene(width=1024, height=1024, subdiv=7, probe_samples=4096, env_
     return sc.SceneData(integrator, camera, background, meshes, [sc.EnvMapLight()], probe_samples=probe_samples)
 
 
-def translucent_box_scene(width=64, height=64, subdiv=3, probe_samples=64, dipole_model=sc.STANDARD_DIPOLE, max_depth=6, two_objects=False):
+def translucent_box_scene(width=64, height=64, subdiv=3, probe_samples=64, dipole_model=sc.STANDARD_DIPOLE, max_depth=6, two_objects=False,
+                          rough=None):
     """A small closed scene for parity checks: the diffuse box, a translucent icosphere (and
-    optionally a second translucent object with its own material), a quad light."""
+    optionally a second translucent object with its own material), a quad light.  rough =
+    (roughness, microfacet model, normal distribution) makes the icosphere a rough translucent one."""
     integrator = sc.PathTracer(max_depth=max_depth, scene_epsilon=1e-4)
     camera = sc.PinholeCamera(eye=(0.0, 0.0, 0.9), lookat=(0.0, 0.0, -1.0), up=(0.0, 1.0, 0.0), vfov=60.0, width=width, height=height)
     background = sc.ConstantBackground((0.0, 0.0, 0.0))
     diffuse = sc.DiffuseMaterial((0.7, 0.7, 0.7))
-    skin = sc.TranslucentMaterial(scattering=(0.74, 0.88, 1.01), absorption=(0.032, 0.17, 0.48), ior=1.3, scale=10.0, dipole_model=dipole_model)
+    kw = dict(scattering=(0.74, 0.88, 1.01), absorption=(0.032, 0.17, 0.48), ior=1.3, scale=10.0, dipole_model=dipole_model)
+    if rough is None:
+        skin = sc.TranslucentMaterial(**kw)
+    else:
+        skin = sc.RoughTranslucentMaterial(roughness=(rough[0], rough[0]), microfacet_model=rough[1], normal_distribution=rough[2], **kw)
     bp, bi = box()
     p, i, n, ni = jittered_icosphere(subdiv, 0.35, (-0.2, -0.6, -0.2), 0.02, 1)
     meshes = [sc.Mesh(bp, bi, diffuse), sc.Mesh(p, i, skin, n, ni)]

@@ -265,6 +265,9 @@ class OracleScene:
                 mab[k, :3] = m.radiance
             elif name == "TranslucentMaterial":
                 pass
+            elif name == "RoughTranslucentMaterial":
+                mmodel[k], mdist[k] = m.microfacet_model, m.normal_distribution
+                mab[k, :2] = m.roughness
             else:
                 raise TypeError(name)
         C = data.camera
@@ -282,7 +285,7 @@ class OracleScene:
                                       fp(cam), C.width, C.height, fp(patch), I_.max_depth, I_.scene_epsilon, I_.rr_start_depth, fp(bg))
         self.tex_of_material = {}
         for k, m in enumerate(data.materials):
-            if type(m).__name__ == "TranslucentMaterial":
+            if type(m).__name__ in ("TranslucentMaterial", "RoughTranslucentMaterial"):
                 props = compute_coefficients(m)
                 self._keep.append(props)
                 lib.orc_scene_set_translucent(self.h, k, fp(props), m.dipole_model)

@@ -28,7 +28,7 @@ namespace {
 
 typedef V3<float> F3;
 
-enum { MT_DIFFUSE = 0, MT_GLASS = 3, MT_METAL = 4, MT_TRANSLUCENT = 5, MT_LIGHT = 100 };
+enum { MT_DIFFUSE = 0, MT_GLASS = 3, MT_METAL = 4, MT_TRANSLUCENT = 5, MT_ROUGH_TRANSLUCENT = 6, MT_LIGHT = 100 };
 enum { STANDARD_DIPOLE = 0, DIRECTIONAL_DIPOLE = 1 };
 
 struct Mat {
@@ -683,6 +683,185 @@ static void shade_translucent(Scene& S, const Mat& m, const F3& o, const F3& d, 
   prd.result = prd.result * beam_T;
 }
 
+// The dipole gather of a translucent entry vertex (subsurface_scattering_shader.cu:126-173 and the rough
+// variant rough_subsurface_scattering_shader.cu:240-283,384-427, where a draw must also exceed 0.001
+// and every term is multiplied by the refraction weight).
+static F3 dipole_gather(Scene& S, const Mat& m, const F3& xo, const F3& no, Seed64& t64, bool rough, const F3& weight)
+{
+  const ScatProps& P = m.props;
+  float chosen = std::fmin(P.transport.x, std::fmin(P.transport.y, P.transport.z));
+  F3 acc = v3s(0.0f);
+  unsigned N = S.samples;
+  const Probe* pr = S.probes.data() + (size_t)m.translucent_index * N;
+  for (unsigned i = 0; i < N; ++i) {
+    const Probe& sm = pr[i];
+    if (dot(sm.L, sm.L) > 0.0f) {
+      float dist = length(xo - sm.pos);
+      float exp_term = std::exp(-dist * chosen);
+      float rnd_number = rnd_accurate(t64);
+      if (rnd_number < exp_term && (!rough || rnd_number > 0.001f)) {
+        F3 term = (m.dipole_model == DIRECTIONAL_DIPOLE) ? sm.weight * sm.L * dirpole_bssrdf(sm.pos, sm.normal, sm.transmitted, xo, no, P) / exp_term
+                                                        : sm.weight * sm.L * dipole_bssrdf(dist, P) / exp_term;
+        acc = acc + (rough ? term * weight : term);
+      }
+    }
+  }
+  return acc * P.global_coeff / (float)N;
+}
+
+// rough_subsurface_scattering_shader.cu:56-455 (REFLECT, TRANSMIT, DIRECTLIGHT and RND_64 defined):
+// microfacet normal from MD5 draws, a light sample with its reflection-only estimate (the multiscatter
+// model: the multiscatter dielectric BSDF), then as the smooth shader with the microfacet normal in
+// the Fresnel choice and the refraction / reflection weight on the child (and on the gather).
+static void shade_rough_translucent(Scene& S, const Mat& m, const F3& o, const F3& d, const HitRec& h, PRD& prd, LightSet& ls)
+{
+  prd.result = v3s(0.0f);
+  if (prd.depth > S.max_depth) return;
+  F3 result = v3s(0.0f);
+  F3 normal = shading_normal(S, h.prim, h.u, h.v);
+  F3 ffnormal = faceforward(normal, -d, normal);
+  F3 hit_pos = o + h.t * d;
+  F3 w_i = -d;
+  const ScatProps& P = m.props;
+  float recip_ior = 1.0f / P.relative_ior;
+  F3 beam_T = v3s(1.0f);
+  u32& t = prd.seed;
+  Seed64& t64 = prd.seed64;
+  float reflect_xi = rnd_accurate(t64);
+  float z1 = rnd_accurate(t64);
+  float z2 = rnd_accurate(t64);
+  const float a_x = m.a[0], a_y = m.a[1];
+  const int dist = (int)m.dist;
+  int capped = 0;
+  F3 mn = (m.model == WALTER) ? sample_normal<float>(dist, ffnormal, z1, z2, a_x)
+                              : sample_visible_normal<float>(dist, w_i, ffnormal, a_x, a_y, z1, z2, &capped);
+  float cos_theta_i = dot(w_i, mn);
+  bool inside = dot(w_i, normal) < 0.0f;
+  // light sample (:93-152)
+  u32 li = (u32)((float)ls.n_lights * rnd_accurate(t64));
+  if ((long)li >= ls.n_lights) { li = (u32)(ls.n_lights - 1); ++ls.oob; }
+  float light_pdf = 1.0f / (float)ls.n_lights;
+  float ldist = 0.0f;
+  F3 light_radiance = v3s(0.0f), w_l = v3s(0.0f);
+  eval_direct<float>(hit_pos, ls.lights[li], ls, w_l, light_radiance, ldist, t);
+  light_radiance = light_radiance / light_pdf;
+  float cos_theta_l = dot(ffnormal, w_l);
+  if (!inside && cos_theta_l > 0.0f) {
+    float V = occluded(S, hit_pos, w_l, S.eps, ldist) ? 0.0f : 1.0f;
+    if (V > 0.0f) {
+      F3 Li = V * light_radiance;
+      F3 e;
+      if (m.model == MULTISCATTERING) {
+        float brdf = ms_dielectric_eval<float>(dist, to_local(w_i, ffnormal), to_local(w_l, ffnormal), recip_ior, a_x, a_y, t, 0, 4096, &capped);
+        e = Li * brdf;
+        prd.emit_light = 0;
+      } else {
+        F3 refl_normal = normalize(w_i + w_l);
+        float cos_refl = dot(refl_normal, w_l);
+        float R_refl = 1.0f;
+        float st2 = recip_ior * recip_ior * (1.0f - cos_refl * cos_refl);
+        if (st2 < 1.0f) R_refl = fresnel_R(cos_refl, std::sqrt(1.0f - st2), recip_ior);
+        float G_i = masking_G1_aniso<float>(dist, w_i, refl_normal, ffnormal, a_x, a_y);
+        float G_o = masking_G1_aniso<float>(dist, w_l, refl_normal, ffnormal, a_x, a_y);
+        float D = eval_visible_normal<float>(dist, w_i, refl_normal, ffnormal, a_x, a_y);
+        float weight_refl = G_i * G_o * D / (4.0f * std::fabs(dot(w_i, ffnormal) * dot(w_l, ffnormal)));
+        e = Li * R_refl * weight_refl;
+        prd.emit_light = 1;
+      }
+      result = result + e;
+      tape_emit(prd, e);
+    }
+  }
+  if (m.model == WALTER || m.model == VISIBLE_NORMALS) {
+    if (inside) {
+      const F3& ext = (m.dipole_model == DIRECTIONAL_DIPOLE) ? P.deltaEddExtinction : P.extinction;
+      beam_T = vexp((-h.t) * ext);
+      float prob = (beam_T.x + beam_T.y + beam_T.z) / 3.0f;
+      if (rnd_accurate(t64) >= prob) { S.capped += capped; return; }
+      beam_T = beam_T / prob;
+      recip_ior = P.relative_ior;
+      normal = -normal;
+    }
+    float st2 = recip_ior * recip_ior * (1.0f - cos_theta_i * cos_theta_i);
+    float cos_t = 1.0f, R = 1.0f;
+    if (st2 < 1.0f) {
+      cos_t = std::sqrt(1.0f - st2);
+      R = fresnel_R(cos_theta_i, cos_t, recip_ior);
+    }
+    auto child_weight = [&](const F3& w_o) {
+      if (m.model == WALTER) {
+        float G_i_m = masking_G1<float>(dist, w_i, mn, ffnormal, a_x);
+        float abs_i_m = std::fabs(dot(w_i, mn)), abs_i_n = std::fabs(dot(w_i, ffnormal)), abs_n_m = std::fabs(dot(ffnormal, mn));
+        float G_o_m = masking_G1<float>(dist, w_o, mn, ffnormal, a_x);
+        return v3s(1.0f) * (abs_i_m * G_i_m * G_o_m / (abs_i_n * abs_n_m));
+      }
+      return v3s(1.0f) * masking_G1_aniso<float>(dist, w_o, mn, ffnormal, a_x, a_y);
+    };
+    if (reflect_xi >= R) {
+      F3 w_t = recip_ior * (cos_theta_i * mn - w_i) - mn * cos_t;
+      PRD child;
+      child.depth = prd.depth + 1;
+      child.seed = t;
+      child.seed64 = t64;
+      child.result = v3s(0.0f);
+      child.emit_light = 1;
+      child.probe_path = prd.probe_path;
+      child.tape = prd.tape;
+      trace(S, hit_pos, w_t, child, ls);
+      F3 weight = child_weight(w_t);
+      result = result + child.result * weight;
+      t = child.seed;
+      t64 = child.seed64;
+      if (!inside && !prd.probe_path) result = result + dipole_gather(S, m, hit_pos, normal, t64, true, weight);
+    }
+    if (reflect_xi < R) {
+      F3 w_r = 2.0f * cos_theta_i * mn - w_i;
+      PRD child;
+      child.depth = prd.depth + 1;
+      child.seed = t;
+      child.seed64 = t64;
+      child.result = v3s(0.0f);
+      child.emit_light = prd.emit_light;
+      child.probe_path = prd.probe_path;
+      child.tape = prd.tape;
+      trace(S, hit_pos, w_r, child, ls);
+      F3 weight = child_weight(w_r);
+      result = result + child.result * weight;
+      t = child.seed;
+      t64 = child.seed64;
+    }
+  } else {  // MULTISCATTERING_MODEL (:287-452)
+    u32 order = 0;
+    F3 w_o = to_world(ms_dielectric_sample<float>(dist, to_local(w_i, normal), 1.0f / P.relative_ior, a_x, a_y, t, order, 4096, &capped), normal);
+    const F3 weight = v3s(1.0f);
+    bool is_refraction = dot(w_o, ffnormal) < 0.0f;
+    if (inside) {
+      const F3& ext = (m.dipole_model == DIRECTIONAL_DIPOLE) ? P.deltaEddExtinction : P.extinction;
+      beam_T = vexp((-h.t) * ext);
+      float prob = (beam_T.x + beam_T.y + beam_T.z) / 3.0f;
+      if (rnd_accurate(t64) >= prob) { S.capped += capped; return; }
+      beam_T = beam_T / prob;
+      recip_ior = P.relative_ior;
+      normal = -normal;
+    }
+    PRD child;
+    child.depth = prd.depth + 1;
+    child.result = v3s(0.0f);
+    child.seed = t;
+    child.emit_light = 1;
+    child.seed64 = t64;
+    child.probe_path = prd.probe_path;
+    child.tape = prd.tape;
+    trace(S, hit_pos, w_o, child, ls);
+    result = result + child.result * weight;
+    t = child.seed;
+    t64 = child.seed64;
+    if (is_refraction && !inside && !prd.probe_path) result = result + dipole_gather(S, m, hit_pos, normal, t64, true, weight);
+  }
+  S.capped += capped;
+  prd.result = result * beam_T;
+}
+
 // sample_camera.cu:48-268 for a smooth translucent object (GLOBAL and RND_64 defined): one
 // PositionSample per launch index of the probe pass of translucent object k.
 static Probe make_probe(Scene& S, unsigned k, unsigned i, unsigned frame, LightSet& ls)
@@ -717,6 +896,16 @@ static Probe make_probe(Scene& S, unsigned k, unsigned i, unsigned frame, LightS
   }
   sm.normal = n;
   float recip_ior = 1.0f / m.props.relative_ior;
+  const bool rough = m.type == MT_ROUGH_TRANSLUCENT;
+  const float a_x = m.a[0], a_y = m.a[1];
+  int capped = 0;
+  // rough objects: the probe's normal is a microfacet normal sampled with two MD5 draws (:130-151)
+  auto microfacet = [&](const F3& wdir) {
+    float z1 = rnd_accurate(t64);
+    float z2 = rnd_accurate(t64);
+    sm.normal = (m.model == WALTER) ? sample_normal<float>((int)m.dist, n, z1, z2, a_x)
+                                    : sample_visible_normal<float>((int)m.dist, wdir, n, a_x, a_y, z1, z2, &capped);
+  };
   F3 Le, w_i;
   if (rnd(t) < 0.5f) {
     u32 li = (u32)((float)ls.n_lights * rnd_accurate(t64));
@@ -727,6 +916,7 @@ static Probe make_probe(Scene& S, unsigned k, unsigned i, unsigned frame, LightS
     w_i = v3s(0.0f);
     eval_direct<float>(sm.pos, ls.lights[li], ls, w_i, Le, r, t);
     sm.dir = w_i;
+    if (rough) microfacet(w_i);
     float cos_theta_i = std::fmax(dot(w_i, n), 0.0f);
     if (cos_theta_i > 0.0f) {
       float att = occluded(S, sm.pos, w_i, S.eps, r) ? 0.0f : 1.0f;
@@ -736,6 +926,7 @@ static Probe make_probe(Scene& S, unsigned k, unsigned i, unsigned frame, LightS
     }
   } else {
     w_i = sample_cosine_weighted<float>(n, t);
+    if (rough) microfacet(w_i);
     PRD pn;
     pn.depth = 0;
     pn.seed = t;
@@ -755,7 +946,26 @@ static Probe make_probe(Scene& S, unsigned k, unsigned i, unsigned frame, LightS
   float cos_t = std::sqrt(1.0f - sin_t2);
   sm.transmitted = recip_ior * (cos_theta_i * sm.normal - w_i) - sm.normal * cos_t;
   float T12 = 1.0f - fresnel_R(cos_theta_i, cos_t, recip_ior);
-  sm.weight = v3s(T12);
+  F3 weight = v3s(1.0f);
+  if (rough) {  // :232-266
+    const int dist = (int)m.dist;
+    if (m.model == WALTER) {
+      float G_i_m = masking_G1_aniso<float>(dist, w_i, sm.normal, n, a_x, a_y);
+      float abs_i_m = std::fabs(dot(w_i, sm.normal)), abs_i_n = std::fabs(dot(w_i, n)), abs_n_m = std::fabs(dot(n, sm.normal));
+      float G_o_m = masking_G1_aniso<float>(dist, sm.transmitted, sm.normal, n, a_x, a_y);
+      weight = weight * (abs_i_m * G_i_m / (abs_i_n * abs_n_m) * G_o_m);
+      weight = weight * v3s(T12);
+    } else if (m.model == VISIBLE_NORMALS) {
+      float G_o_m = masking_G1_aniso<float>(dist, sm.transmitted, sm.normal, n, a_x, a_y);
+      weight = weight * G_o_m;
+      weight = weight * v3s(T12);
+    } else {
+      weight = weight * v3s(T12);
+    }
+  } else {
+    weight = weight * v3s(T12);
+  }
+  sm.weight = weight;
   sm.L = Le * ((float)triangles * area);
   return sm;
 }
@@ -787,6 +997,7 @@ static void trace(Scene& S, const F3& o, const F3& d, PRD& prd, LightSet& ls)
     case MT_METAL: shade_metal(S, m, o, d, h, prd, ls); return;
     case MT_GLASS: shade_glass(S, m, o, d, h, prd, ls); return;
     case MT_TRANSLUCENT: shade_translucent(S, m, o, d, h, prd, ls); return;
+    case MT_ROUGH_TRANSLUCENT: shade_rough_translucent(S, m, o, d, h, prd, ls); return;
     default: prd.result = v3s(0.0f); return;
   }
 }
