@@ -545,6 +545,7 @@ __device__ __forceinline__ uint32_t warp_slot_multi(int cls, uint32_t* counters)
 template <bool kMulti>
 __global__ void __launch_bounds__(kBlock) k_extend_persistent(SceneDev S0, WfDev w, int refill)
 {
+  __shared__ uint2 stk[kShortStack * kBlock];
   const uint32_t n = w.cnt[w.in_slot];
   uint32_t* fetch = w.cnt + CNT_FETCH_EXT;
   TravGeom g = trav_geom(S0);
@@ -560,7 +561,7 @@ __global__ void __launch_bounds__(kBlock) k_extend_persistent(SceneDev S0, WfDev
   Hit h;
   h.t = 0.0f; h.u = h.v = 0.0f; h.prim = -1;
   TravState st;
-  trav_init(st);
+  trav_init(st, stk + threadIdx.x, kBlock);
   for (;;) {
     unsigned idle = __ballot_sync(0xffffffffu, !has);
     if (!drained && (__popc(idle) >= refill || idle == 0xffffffffu)) {
@@ -586,7 +587,7 @@ __global__ void __launch_bounds__(kBlock) k_extend_persistent(SceneDev S0, WfDev
           h.t = kDefaultMax;
           h.u = h.v = 0.0f;
           h.prim = -1;
-          trav_init(st);
+          trav_init(st, stk + threadIdx.x, kBlock);
           has = true;
           done = false;
           ++traced;
@@ -645,6 +646,7 @@ __device__ __forceinline__ void shadow_unoccluded(const SceneDev& S, const WfDev
 template <bool kMulti, bool kAdj>
 __global__ void __launch_bounds__(kBlock) k_shadow_persistent(SceneDev S0, WfDev w, int refill)
 {
+  __shared__ uint2 stk[kShortStack * kBlock];
   const uint32_t n = w.cnt[CNT_SHADOW];
   uint32_t* fetch = w.cnt + CNT_FETCH_SH;
   TravGeom g = trav_geom(S0);
@@ -657,7 +659,7 @@ __global__ void __launch_bounds__(kBlock) k_shadow_persistent(SceneDev S0, WfDev
   RayPre rp;
   rp.inv = f3s(0.0f);
   TravState st;
-  trav_init(st);
+  trav_init(st, stk + threadIdx.x, kBlock);
   for (;;) {
     unsigned idle = __ballot_sync(0xffffffffu, !has);
     if (!drained && (__popc(idle) >= refill || idle == 0xffffffffu)) {
@@ -676,7 +678,7 @@ __global__ void __launch_bounds__(kBlock) k_shadow_persistent(SceneDev S0, WfDev
           tmin = o4.w;
           tmax = d4.w;
           rp = ray_pre(o, d);
-          trav_init(st);
+          trav_init(st, stk + threadIdx.x, kBlock);
           has = true;
           res = 0;
         }

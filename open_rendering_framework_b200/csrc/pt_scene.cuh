@@ -277,22 +277,65 @@ template <class G> PT_HD bool leaf_any(const G& S, uint32_t code, const float3& 
 // that depth is still pending (`pend`), and a second 64-bit word records which child it is
 // (`farc1`); the way back up follows the parent index stored in each node.  No per-ray stack lives
 // in local memory.
+//
+// Optionally a short stack (kShortStack entries, caller-provided, typically shared memory laid out
+// [slot][thread]) caches the pending far children: entry = (far child index, entry distance with its
+// 6 low mantissa bits replaced by the level).  Backtracking then jumps to the deepest pending far child
+// directly instead of walking up through the parents; when the stack has dropped older entries (more
+// than kShortStack pending), the parent walk takes over.  The stored entry distance is rounded down
+// (conservative), and tn <= t_closest * kSlack at pop time decides exactly as re-testing the box would.
+constexpr int kShortStack = 8;
 struct TravState {
   int cur, depth;
   unsigned long long pend, farc1;
+  uint2* stk;   // short stack or null
+  int stride;   // element stride between the stack's slots
+  int top, lo;  // entries [lo, top) are valid (slot = index mod kShortStack)
 };
-PT_HD void trav_init(TravState& st)
+PT_HD void trav_init(TravState& st, uint2* stk = nullptr, int stride = 1)
 {
   st.cur = 0;
   st.depth = 0;
   st.pend = 0ull;
   st.farc1 = 0ull;
+  st.stk = stk;
+  st.stride = stride;
+  st.top = st.lo = 0;
+}
+PT_HD void trav_push(TravState& st, int far, int level, float tn)
+{
+  if (!st.stk) return;
+  uint32_t tb = (uint32_t)as_int(tn);
+  st.stk[(st.top & (kShortStack - 1)) * st.stride] = make_uint2((uint32_t)far, (tb & ~63u) | (uint32_t)level);
+  ++st.top;
+  if (st.top - st.lo > kShortStack) st.lo = st.top - kShortStack;
+}
+PT_HD int highest_bit(unsigned long long x)
+{
+#ifdef __CUDA_ARCH__
+  return 63 - __clzll((long long)x);
+#else
+  return 63 - __builtin_clzll(x);
+#endif
 }
 
 // Backtrack to the deepest pending child.  Closest-hit: the pending far child's box is re-tested
 // against the current closest distance when it is resumed.  Returns false when the root is done.
 template <class G> PT_HD bool trav_backtrack(const G& S, const float3& o, const RayPre& rp, float tmin, float tlimit, TravState& st, bool retest)
 {
+  // short stack: the deepest pending level is the top entry's
+  while (st.pend && st.top > st.lo) {
+    const int L = highest_bit(st.pend);
+    const uint2 e = st.stk[((st.top - 1) & (kShortStack - 1)) * st.stride];
+    if ((int)(e.y & 63u) != L) break;
+    --st.top;
+    st.pend &= ~(1ull << L);
+    if (!retest || as_float((int)(e.y & ~63u)) <= tlimit * kSlack) {
+      st.cur = (int)e.x;
+      st.depth = L + 1;
+      return true;
+    }
+  }
   for (;;) {
     if (st.depth == 0) return false;
     int parent = PT_LDG(reinterpret_cast<const int*>(S.nodes + 4 * (size_t)st.cur + 3) + 2);
@@ -344,6 +387,7 @@ template <class G> PT_HD bool trav_step_closest(const G& S, const float3& o, con
     unsigned long long bit = 1ull << st.depth;
     st.pend |= bit;
     if (near1) st.farc1 &= ~bit; else st.farc1 |= bit;
+    trav_push(st, near1 ? n3.x : n3.y, st.depth, near1 ? t0 : t1);
     st.cur = near1 ? n3.y : n3.x;
     ++st.depth;
     return false;
@@ -372,6 +416,7 @@ template <class G> PT_HD int trav_step_any(const G& S, const float3& o, const fl
     unsigned long long bit = 1ull << st.depth;
     st.pend |= bit;
     st.farc1 |= bit;
+    trav_push(st, n3.y, st.depth, t1);
     st.cur = n3.x;
     ++st.depth;
     return 0;

@@ -28,6 +28,33 @@ extern "C" __attribute__((visibility("default"))) void* ht_build(const float* tr
 }
 extern "C" __attribute__((visibility("default"))) void ht_free(void* h) { delete (HostScene*)h; }
 extern "C" __attribute__((visibility("default"))) unsigned ht_nodes(void* h) { return (unsigned)(((HostScene*)h)->bvh.nodes.size() / 4); }
+// The same traversal with a kShortStack-entry stack of pending far children (as the persistent kernels
+// use it), stride 1.
+extern "C" __attribute__((visibility("default"))) void ht_trace_stack(void* hp, const float* rays, long n, int* prim, float* t, float* bary, int* any)
+{
+  HostScene* h = (HostScene*)hp;
+  for (long i = 0; i < n; ++i) {
+    const float* r = rays + 8 * i;
+    float3 o = make_float3(r[0], r[1], r[2]), d = make_float3(r[4], r[5], r[6]);
+    uint2 stk[kShortStack];
+    RayPre rp = ray_pre(o, d);
+    Hit hh;
+    hh.t = r[7];
+    hh.u = hh.v = 0.0f;
+    hh.prim = -1;
+    TravState st;
+    trav_init(st, stk, 1);
+    while (!trav_step_closest(h->S, o, d, rp, r[3], hh, st)) {}
+    prim[i] = hh.prim;
+    t[i] = hh.prim >= 0 ? hh.t : -1.0f;
+    bary[2 * i] = hh.u;
+    bary[2 * i + 1] = hh.v;
+    trav_init(st, stk, 1);
+    int res;
+    while ((res = trav_step_any(h->S, o, d, rp, r[3], r[7], st)) == 0) {}
+    any[i] = res > 0 ? 1 : 0;
+  }
+}
 // rays: n x 8 floats (origin, tmin, dir, tmax)
 extern "C" __attribute__((visibility("default"))) void ht_trace(void* hp, const float* rays, long n, int* prim, float* t, float* bary, int* any)
 {

@@ -31,6 +31,7 @@ def host_lib():
     L.ht_build.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p]
     L.ht_free.argtypes = [ctypes.c_void_p]
     L.ht_trace.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long] + [ctypes.c_void_p] * 4
+    L.ht_trace_stack.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long] + [ctypes.c_void_p] * 4
     return L
 
 
@@ -60,12 +61,17 @@ def test_host_traversal_matches_brute_force(host_lib, subdiv):
     prim, t = np.empty(n, np.int32), np.empty(n, np.float32)
     bary, anyh = np.empty((n, 2), np.float32), np.empty(n, np.int32)
     host_lib.ht_trace(h, oc.fp(rays), n, oc.fp(prim), oc.fp(t), oc.fp(bary), oc.fp(anyh))
+    # the short-stack variant of the persistent kernels
+    prim2, t2 = np.empty(n, np.int32), np.empty(n, np.float32)
+    bary2, anyh2 = np.empty((n, 2), np.float32), np.empty(n, np.int32)
+    host_lib.ht_trace_stack(h, oc.fp(rays), n, oc.fp(prim2), oc.fp(t2), oc.fp(bary2), oc.fp(anyh2))
     host_lib.ht_free(h)
     bp, bt, bb, ba = oc.OracleScene(data).trace(rays, brute=True)
-    assert np.array_equal(prim, bp)
-    assert np.array_equal(t.view(np.uint32), bt.view(np.uint32))
-    assert np.array_equal(bary.view(np.uint32), bb.view(np.uint32))
-    assert np.array_equal(anyh, ba)
+    for p_, t_, b_, a_ in ((prim, t, bary, anyh), (prim2, t2, bary2, anyh2)):
+        assert np.array_equal(p_, bp)
+        assert np.array_equal(t_.view(np.uint32), bt.view(np.uint32))
+        assert np.array_equal(b_.view(np.uint32), bb.view(np.uint32))
+        assert np.array_equal(a_, ba)
 
 
 def test_single_triangle_and_degenerate_scenes(host_lib):
