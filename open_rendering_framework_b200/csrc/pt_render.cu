@@ -36,6 +36,10 @@ namespace pt {
 
 constexpr int kBlock = 128;
 constexpr int kWarps = kBlock / 32;
+// Resident blocks per SM the persistent traversal kernels are compiled for (register budget).
+#ifndef PT_TRACE_MIN_BLOCKS
+#define PT_TRACE_MIN_BLOCKS 1
+#endif
 
 // Per-path metadata in rng.w
 constexpr uint32_t META_DEPTH = 0xffffu;
@@ -543,7 +547,7 @@ __device__ __forceinline__ uint32_t warp_slot_multi(int cls, uint32_t* counters)
 // kMulti: the rays belong to several scenes (a batch); each lane keeps its ray's scene view in
 // registers.  Otherwise the single scene is the kernel parameter S0.
 template <bool kMulti>
-__global__ void __launch_bounds__(kBlock) k_extend_persistent(SceneDev S0, WfDev w, int refill)
+__global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_extend_persistent(SceneDev S0, WfDev w, int refill)
 {
   __shared__ uint2 stk[kShortStack * kBlock];
   const uint32_t n = w.cnt[w.in_slot];
@@ -562,6 +566,7 @@ __global__ void __launch_bounds__(kBlock) k_extend_persistent(SceneDev S0, WfDev
   h.t = 0.0f; h.u = h.v = 0.0f; h.prim = -1;
   TravState st;
   trav_init(st, stk + threadIdx.x, kBlock);
+  uint32_t leafA = 0, leafB = 0;
   for (;;) {
     unsigned idle = __ballot_sync(0xffffffffu, !has);
     if (!drained && (__popc(idle) >= refill || idle == 0xffffffffu)) {
@@ -596,18 +601,31 @@ __global__ void __launch_bounds__(kBlock) k_extend_persistent(SceneDev S0, WfDev
     }
     if (__ballot_sync(0xffffffffu, has) == 0) break;
     for (;;) {
-      if (has && !done) done = trav_step_closest(g, o, d, rp, eps, h, st);
-      unsigned fin = __ballot_sync(0xffffffffu, !has || done);
+      // a warp-wide phase: intersect the postponed leaves when at least as many lanes hold leaves as can
+      // take a node step, else advance the lanes without leaves by one node
+      const bool lp = has && leafA != 0;
+      const unsigned lmask = __ballot_sync(0xffffffffu, lp);
+      const unsigned nmask = __ballot_sync(0xffffffffu, has && !done && !lp);
+      if (lmask && (nmask == 0 || __popc(lmask) >= __popc(nmask))) {
+        if (lp) {
+          leaf_closest(g, leafA, o, d, eps, h);
+          if (leafB) leaf_closest(g, leafB, o, d, eps, h);
+          leafA = leafB = 0;
+        }
+      } else if (has && !done && !lp) {
+        done = trav_node_closest(g, o, rp, eps, h, st, leafA, leafB);
+      }
+      unsigned fin = __ballot_sync(0xffffffffu, !has || (done && leafA == 0));
       if (fin == 0xffffffffu || (!drained && __popc(fin) >= refill)) break;
     }
     int cls = -1;
-    if (has && done) {
+    if (has && done && leafA == 0) {
       w.hit[pid] = make_float4(h.t, h.u, h.v, as_float(h.prim));
       cls = h.prim < 0 ? QC_MISS : class_of(__ldg(&mats[__ldg(&tinfo[h.prim].w)].type));
     }
     uint32_t slot = warp_slot_multi(cls, w.cnt + CNT_Q_MISS);
     if (cls >= 0) w.q_mat[(size_t)cls * w.cap + slot] = pid;
-    if (has && done) has = false;
+    if (has && done && leafA == 0) has = false;
   }
   traced += __shfl_xor_sync(0xffffffffu, traced, 16);
   traced += __shfl_xor_sync(0xffffffffu, traced, 8);
@@ -644,16 +662,16 @@ __device__ __forceinline__ void shadow_unoccluded(const SceneDev& S, const WfDev
 
 // Persistent any-hit kernel for the shadow queue (same ray replacement).
 template <bool kMulti, bool kAdj>
-__global__ void __launch_bounds__(kBlock) k_shadow_persistent(SceneDev S0, WfDev w, int refill)
+__global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_shadow_persistent(SceneDev S0, WfDev w, int refill)
 {
   __shared__ uint2 stk[kShortStack * kBlock];
   const uint32_t n = w.cnt[CNT_SHADOW];
   uint32_t* fetch = w.cnt + CNT_FETCH_SH;
   TravGeom g = trav_geom(S0);
   const unsigned lane = threadIdx.x & 31;
-  bool has = false, drained = false;
+  bool has = false, drained = false, nodes_done = false;
   int res = 0;
-  uint32_t slot = 0;
+  uint32_t slot = 0, leafA = 0, leafB = 0;
   float3 o = f3s(0.0f), d = f3s(0.0f);
   float tmin = 0.0f, tmax = 0.0f;
   RayPre rp;
@@ -681,12 +699,25 @@ __global__ void __launch_bounds__(kBlock) k_shadow_persistent(SceneDev S0, WfDev
           trav_init(st, stk + threadIdx.x, kBlock);
           has = true;
           res = 0;
+          nodes_done = false;
+          leafA = leafB = 0;
         }
       }
     }
     if (__ballot_sync(0xffffffffu, has) == 0) break;
     for (;;) {
-      if (has && res == 0) res = trav_step_any(g, o, d, rp, tmin, tmax, st);
+      const bool lp = has && res == 0 && leafA != 0;
+      const unsigned lmask = __ballot_sync(0xffffffffu, lp);
+      const unsigned nmask = __ballot_sync(0xffffffffu, has && res == 0 && !nodes_done && !lp);
+      if (lmask && (nmask == 0 || __popc(lmask) >= __popc(nmask))) {
+        if (lp) {
+          if (leaf_any(g, leafA, o, d, tmin, tmax) || (leafB && leaf_any(g, leafB, o, d, tmin, tmax))) res = 1;
+          leafA = leafB = 0;
+        }
+      } else if (has && res == 0 && !nodes_done && !lp) {
+        nodes_done = trav_node_any(g, o, rp, tmin, tmax, st, leafA, leafB);
+      }
+      if (has && res == 0 && nodes_done && leafA == 0) res = -1;
       unsigned fin = __ballot_sync(0xffffffffu, !has || res != 0);
       if (fin == 0xffffffffu || (!drained && __popc(fin) >= refill)) break;
     }

@@ -284,7 +284,10 @@ template <class G> PT_HD bool leaf_any(const G& S, uint32_t code, const float3& 
 // directly instead of walking up through the parents; when the stack has dropped older entries (more
 // than kShortStack pending), the parent walk takes over.  The stored entry distance is rounded down
 // (conservative), and tn <= t_closest * kSlack at pop time decides exactly as re-testing the box would.
-constexpr int kShortStack = 8;
+#ifndef PT_SHORT_STACK
+#define PT_SHORT_STACK 8
+#endif
+constexpr int kShortStack = PT_SHORT_STACK;  // a power of two
 struct TravState {
   int cur, depth;
   unsigned long long pend, farc1;
@@ -427,6 +430,78 @@ template <class G> PT_HD int trav_step_any(const G& S, const float3& o, const fl
     return 0;
   }
   return trav_backtrack(S, o, rp, tmin, tmax, st, false) ? 0 : -1;
+}
+
+// Node-only steps for the persistent kernels' postponed-leaf traversal (T. Aila, S. Laine, "Understanding
+// the efficiency of ray traversal on GPUs", HPG 2009, speculative while-while): the hit leaf children
+// of the node are recorded in (leafA, leafB) instead of being intersected, and the caller intersects
+// them in a warp-wide leaf phase.  The inner children are culled against the closest hit found so far
+// (the postponed leaves can only shorten it, so this is conservative).  Returns true when no node is
+// left (leaves may still be pending).
+template <class G> PT_HD bool trav_node_closest(const G& S, const float3& o, const RayPre& rp, float tmin, const Hit& h, TravState& st,
+                                                uint32_t& leafA, uint32_t& leafB)
+{
+  const float4* nd = S.nodes + 4 * (size_t)st.cur;
+  float4 n0 = PT_LDG(nd), n1 = PT_LDG(nd + 1), n2 = PT_LDG(nd + 2);
+  int4 n3 = PT_LDG(reinterpret_cast<const int4*>(nd + 3));
+  float t0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, rp, tmin, h.t);
+  float t1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, rp, tmin, h.t);
+  bool h0 = t0 != as_float(0x7f800000), h1 = t1 != as_float(0x7f800000);
+  if (h0 && n3.x < 0) { leafA = (uint32_t)n3.x; h0 = false; }
+  if (h1 && n3.y < 0) {
+    if (leafA) leafB = (uint32_t)n3.y;
+    else leafA = (uint32_t)n3.y;
+    h1 = false;
+  }
+  h0 = h0 && t0 <= h.t * kSlack;
+  h1 = h1 && t1 <= h.t * kSlack;
+  if (h0 && h1) {
+    bool near1 = t1 < t0;
+    unsigned long long bit = 1ull << st.depth;
+    st.pend |= bit;
+    if (near1) st.farc1 &= ~bit; else st.farc1 |= bit;
+    trav_push(st, near1 ? n3.x : n3.y, st.depth, near1 ? t0 : t1);
+    st.cur = near1 ? n3.y : n3.x;
+    ++st.depth;
+    return false;
+  }
+  if (h0 || h1) {
+    st.cur = h0 ? n3.x : n3.y;
+    ++st.depth;
+    return false;
+  }
+  return !trav_backtrack(S, o, rp, tmin, h.t, st, true);
+}
+template <class G> PT_HD bool trav_node_any(const G& S, const float3& o, const RayPre& rp, float tmin, float tmax, TravState& st, uint32_t& leafA,
+                                            uint32_t& leafB)
+{
+  const float4* nd = S.nodes + 4 * (size_t)st.cur;
+  float4 n0 = PT_LDG(nd), n1 = PT_LDG(nd + 1), n2 = PT_LDG(nd + 2);
+  int4 n3 = PT_LDG(reinterpret_cast<const int4*>(nd + 3));
+  float t0 = slab(n0.x, n0.y, n0.z, n0.w, n2.x, n2.y, o, rp, tmin, tmax);
+  float t1 = slab(n1.x, n1.y, n1.z, n1.w, n2.z, n2.w, o, rp, tmin, tmax);
+  bool h0 = t0 != as_float(0x7f800000), h1 = t1 != as_float(0x7f800000);
+  if (h0 && n3.x < 0) { leafA = (uint32_t)n3.x; h0 = false; }
+  if (h1 && n3.y < 0) {
+    if (leafA) leafB = (uint32_t)n3.y;
+    else leafA = (uint32_t)n3.y;
+    h1 = false;
+  }
+  if (h0 && h1) {
+    unsigned long long bit = 1ull << st.depth;
+    st.pend |= bit;
+    st.farc1 |= bit;
+    trav_push(st, n3.y, st.depth, t1);
+    st.cur = n3.x;
+    ++st.depth;
+    return false;
+  }
+  if (h0 || h1) {
+    st.cur = h0 ? n3.x : n3.y;
+    ++st.depth;
+    return false;
+  }
+  return !trav_backtrack(S, o, rp, tmin, tmax, st, false);
 }
 
 template <class G> PT_HD Hit trace_closest(const G& S, const float3& o, const float3& d, float tmin, float tmax)
