@@ -14,6 +14,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <future>
 #include <memory>
 #include <thread>
@@ -271,6 +272,76 @@ bool build_bvh(const float* tri_pos, uint32_t n_tris, BvhHost& out)
     out.tri_e2[j] = make_float4(p[6] - p[0], p[7] - p[1], p[8] - p[2], 0.0f);
   }
   return out.depth < 64;
+}
+
+// Collapse: starting from a BVH2 node's two children, the internal child of largest surface area is
+// replaced by its own two children until there are four or no internal child is left (the usual
+// greedy collapse of a binary SAH tree into a wide one).
+bool build_bvh4(const BvhHost& b2, std::vector<float4>& out4, int& depth4)
+{
+  out4.clear();
+  depth4 = 0;
+  struct Kid {
+    int code;          // BVH2 node index (>= 0) or leaf code (< 0)
+    float lo[3], hi[3];
+  };
+  auto kid = [&](int node, int k) {
+    const float4* nd = b2.nodes.data() + 4 * (size_t)node;
+    Kid c;
+    int4 n3;
+    memcpy(&n3, &nd[3], sizeof(n3));
+    c.code = k == 0 ? n3.x : n3.y;
+    const float4& a = nd[k];
+    c.lo[0] = a.x; c.hi[0] = a.y; c.lo[1] = a.z; c.hi[1] = a.w;
+    c.lo[2] = k == 0 ? nd[2].x : nd[2].z;
+    c.hi[2] = k == 0 ? nd[2].y : nd[2].w;
+    return c;
+  };
+  auto area = [](const Kid& c) {
+    float d[3];
+    for (int k = 0; k < 3; ++k) d[k] = std::max(0.0f, c.hi[k] - c.lo[k]);
+    return d[0] * d[1] + d[1] * d[2] + d[2] * d[0];
+  };
+  bool ok = true;
+  std::function<int(int, int)> build = [&](int n2, int depth) -> int {
+    depth4 = std::max(depth4, depth);
+    if (depth >= kMaxDepth4) ok = false;
+    Kid kids[4];
+    int nk = 0;
+    kids[nk++] = kid(n2, 0);
+    kids[nk++] = kid(n2, 1);
+    while (nk < 4) {
+      int best = -1;
+      float ba = -1.0f;
+      for (int j = 0; j < nk; ++j)
+        if (kids[j].code >= 0 && area(kids[j]) > ba) { ba = area(kids[j]); best = j; }
+      if (best < 0) break;
+      const int inner = kids[best].code;
+      kids[best] = kid(inner, 0);
+      kids[nk++] = kid(inner, 1);
+    }
+    const int me = (int)(out4.size() / 8);
+    out4.resize(out4.size() + 8);
+    int codes[4];
+    for (int j = 0; j < 4; ++j) {
+      if (j >= nk) codes[j] = (int)0x80000000u;  // empty slot: a leaf of no triangles behind a far box
+      else if (kids[j].code >= 0) codes[j] = ok ? build(kids[j].code, depth + 1) : 0;
+      else codes[j] = kids[j].code;
+    }
+    float4* nd = out4.data() + 8 * (size_t)me;
+    auto comp = [&](int j, int axis, bool lo) { return j < nk ? (lo ? kids[j].lo[axis] : kids[j].hi[axis]) : 1e30f; };
+    for (int axis = 0; axis < 3; ++axis) {
+      nd[2 * axis] = make_float4(comp(0, axis, true), comp(1, axis, true), comp(2, axis, true), comp(3, axis, true));
+      nd[2 * axis + 1] = make_float4(comp(0, axis, false), comp(1, axis, false), comp(2, axis, false), comp(3, axis, false));
+    }
+    int4 c4 = make_int4(codes[0], codes[1], codes[2], codes[3]);
+    memcpy(&nd[6], &c4, sizeof(c4));
+    nd[7] = make_float4((float)nk, 0.0f, 0.0f, 0.0f);
+    return me;
+  };
+  build(0, 1);
+  if (!ok) out4.clear();
+  return ok;
 }
 
 }  // namespace pt

@@ -18,4 +18,10 @@ struct BvhHost {
 // node encoding (2^27 triangles) or the tree is deeper than the traversal trail allows.
 bool build_bvh(const float* tri_pos, uint32_t n_tris, BvhHost& out);
 
+// The BVH2 collapsed into a 4-wide BVH over the same leaves (8 float4 = 128 bytes per node, root =
+// node 0; layout in pt_scene.cuh).  Returns false (and leaves nodes4 empty) when the 4-wide tree
+// would be deeper than kMaxDepth4 levels, whose pending children the traversal stack could not hold.
+constexpr int kMaxDepth4 = 40;
+bool build_bvh4(const BvhHost& bvh2, std::vector<float4>& nodes4, int& depth4);
+
 }  // namespace pt

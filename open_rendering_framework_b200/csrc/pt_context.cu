@@ -14,6 +14,7 @@ SceneDev Context::view() const
 {
   SceneDev s;
   s.nodes = d_nodes.as<float4>();
+  s.nodes4 = has_bvh4 && use_bvh4 ? d_nodes4.as<float4>() : nullptr;
   s.tri_v0 = d_v0.as<float4>();
   s.tri_e1 = d_e1.as<float4>();
   s.tri_e2 = d_e2.as<float4>();
@@ -611,7 +612,11 @@ pt_status pt_build(pt_ctx* ctx)
   BvhHost bvh;
   if (!build_bvh(c.tri_pos.data(), c.n_tris, bvh)) return fail(PT_CAP_EXCEEDED, "pt_build: scene too large or BVH too deep");
   c.bvh_depth = bvh.depth;
+  std::vector<float4> nodes4;
+  int depth4 = 0;
+  c.has_bvh4 = build_bvh4(bvh, nodes4, depth4);
   pt_status st = upload(c.d_nodes, bvh.nodes, c.stream, "BVH nodes");
+  if (st == PT_OK && c.has_bvh4) st = upload(c.d_nodes4, nodes4, c.stream, "4-wide BVH nodes");
   if (st == PT_OK) st = upload(c.d_v0, bvh.tri_v0, c.stream, "triangles");
   if (st == PT_OK) st = upload(c.d_e1, bvh.tri_e1, c.stream, "triangles");
   if (st == PT_OK) st = upload(c.d_e2, bvh.tri_e2, c.stream, "triangles");
@@ -780,6 +785,11 @@ pt_status pt_set_option(pt_ctx* ctx, const char* name, int64_t value)
     if (value != 0 && value != 1) return fail(PT_INVALID_ARG, "pt_set_option: differentiable must be 0 or 1");
     ctx->c.differentiable = value != 0;
     ctx->c.adj_valid = false;
+    return PT_OK;
+  }
+  if (k == "bvh4") {
+    if (value != 0 && value != 1) return fail(PT_INVALID_ARG, "pt_set_option: bvh4 must be 0 or 1");
+    ctx->c.use_bvh4 = value != 0;
     return PT_OK;
   }
   if (k == "extend_mode") {

@@ -158,9 +158,12 @@ struct Context {
   int bvh_depth = 0;
   uint32_t n_tris = 0;
 
-  DevBuf d_nodes, d_v0, d_e1, d_e2, d_info, d_normals, d_mats, d_lights, d_tri_lights;
+  DevBuf d_nodes, d_nodes4, d_v0, d_e1, d_e2, d_info, d_normals, d_mats, d_lights, d_tri_lights;
+  bool has_bvh4 = false;
+  bool use_bvh4 = true;  // option "bvh4": the persistent traversal kernels walk the 4-wide BVH
   DevBuf d_scat, d_trans_objs, d_trans_pos;
   DevBuf d_scene_tab, d_item_tab;  // scene and item tables of the current pass (this context as the engine)
+  bool pass_w4 = false;            // every scene of the current pass has a 4-wide BVH
   // differentiable renders: the forward state of the last render of frames [adj_first, +adj_frames)
   bool differentiable = false;
   DevBuf d_adj_L, d_adj_G;

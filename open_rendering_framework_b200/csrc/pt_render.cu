@@ -546,10 +546,12 @@ __device__ __forceinline__ uint32_t warp_slot_multi(int cls, uint32_t* counters)
 // on GPUs", HPG 2009: persistent threads with ray replacement).
 // kMulti: the rays belong to several scenes (a batch); each lane keeps its ray's scene view in
 // registers.  Otherwise the single scene is the kernel parameter S0.
-template <bool kMulti>
+// kW4: the 4-wide BVH (node steps of pt_scene.cuh trav4_*, the next target `cur` a node, a leaf or
+// kDone4); otherwise the BVH2 with the postponed-leaf pair (leafA, leafB).
+template <bool kMulti, bool kW4>
 __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_extend_persistent(SceneDev S0, WfDev w, int refill)
 {
-  __shared__ uint2 stk[kShortStack * kBlock];
+  __shared__ uint2 stk[(kW4 ? kRing4 : kShortStack) * kBlock];
   const uint32_t n = w.cnt[w.in_slot];
   uint32_t* fetch = w.cnt + CNT_FETCH_EXT;
   TravGeom g = trav_geom(S0);
@@ -567,6 +569,10 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_extend_persiste
   TravState st;
   trav_init(st, stk + threadIdx.x, kBlock);
   uint32_t leafA = 0, leafB = 0;
+  uint2 spill4[kW4 ? kSpill4 : 1];
+  Stack4 s4;
+  stack4_init(s4, stk + threadIdx.x, kBlock, spill4);
+  int cur = kDone4;
   for (;;) {
     unsigned idle = __ballot_sync(0xffffffffu, !has);
     if (!drained && (__popc(idle) >= refill || idle == 0xffffffffu)) {
@@ -592,7 +598,12 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_extend_persiste
           h.t = kDefaultMax;
           h.u = h.v = 0.0f;
           h.prim = -1;
-          trav_init(st, stk + threadIdx.x, kBlock);
+          if constexpr (kW4) {
+            stack4_init(s4, stk + threadIdx.x, kBlock, spill4);
+            cur = 0;
+          } else {
+            trav_init(st, stk + threadIdx.x, kBlock);
+          }
           has = true;
           done = false;
           ++traced;
@@ -603,17 +614,33 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_extend_persiste
     for (;;) {
       // a warp-wide phase: intersect the postponed leaves when at least as many lanes hold leaves as can
       // take a node step, else advance the lanes without leaves by one node
-      const bool lp = has && leafA != 0;
-      const unsigned lmask = __ballot_sync(0xffffffffu, lp);
-      const unsigned nmask = __ballot_sync(0xffffffffu, has && !done && !lp);
-      if (lmask && (nmask == 0 || __popc(lmask) >= __popc(nmask))) {
-        if (lp) {
-          leaf_closest(g, leafA, o, d, eps, h);
-          if (leafB) leaf_closest(g, leafB, o, d, eps, h);
-          leafA = leafB = 0;
+      if constexpr (kW4) {
+        const bool lp = has && cur < 0;
+        const bool np = has && cur >= 0 && cur != kDone4;
+        const unsigned lmask = __ballot_sync(0xffffffffu, lp);
+        const unsigned nmask = __ballot_sync(0xffffffffu, np);
+        if (lmask && (nmask == 0 || __popc(lmask) >= __popc(nmask))) {
+          if (lp) {
+            leaf_closest(g, (uint32_t)cur, o, d, eps, h);
+            cur = stack4_next(s4, h.t, true);
+          }
+        } else if (np) {
+          cur = trav4_node_closest(g, cur, o, rp, eps, h, s4);
         }
-      } else if (has && !done && !lp) {
-        done = trav_node_closest(g, o, rp, eps, h, st, leafA, leafB);
+        done = cur == kDone4;
+      } else {
+        const bool lp = has && leafA != 0;
+        const unsigned lmask = __ballot_sync(0xffffffffu, lp);
+        const unsigned nmask = __ballot_sync(0xffffffffu, has && !done && !lp);
+        if (lmask && (nmask == 0 || __popc(lmask) >= __popc(nmask))) {
+          if (lp) {
+            leaf_closest(g, leafA, o, d, eps, h);
+            if (leafB) leaf_closest(g, leafB, o, d, eps, h);
+            leafA = leafB = 0;
+          }
+        } else if (has && !done && !lp) {
+          done = trav_node_closest(g, o, rp, eps, h, st, leafA, leafB);
+        }
       }
       unsigned fin = __ballot_sync(0xffffffffu, !has || (done && leafA == 0));
       if (fin == 0xffffffffu || (!drained && __popc(fin) >= refill)) break;
@@ -660,11 +687,11 @@ __device__ __forceinline__ void shadow_unoccluded(const SceneDev& S, const WfDev
   }
 }
 
-// Persistent any-hit kernel for the shadow queue (same ray replacement).
-template <bool kMulti, bool kAdj>
+// Persistent any-hit kernel for the shadow queue (same ray replacement and BVH choice).
+template <bool kMulti, bool kAdj, bool kW4>
 __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_shadow_persistent(SceneDev S0, WfDev w, int refill)
 {
-  __shared__ uint2 stk[kShortStack * kBlock];
+  __shared__ uint2 stk[(kW4 ? kRing4 : kShortStack) * kBlock];
   const uint32_t n = w.cnt[CNT_SHADOW];
   uint32_t* fetch = w.cnt + CNT_FETCH_SH;
   TravGeom g = trav_geom(S0);
@@ -678,6 +705,10 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_shadow_persiste
   rp.inv = f3s(0.0f);
   TravState st;
   trav_init(st, stk + threadIdx.x, kBlock);
+  uint2 spill4[kW4 ? kSpill4 : 1];
+  Stack4 s4;
+  stack4_init(s4, stk + threadIdx.x, kBlock, spill4);
+  int cur = kDone4;
   for (;;) {
     unsigned idle = __ballot_sync(0xffffffffu, !has);
     if (!drained && (__popc(idle) >= refill || idle == 0xffffffffu)) {
@@ -696,7 +727,12 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_shadow_persiste
           tmin = o4.w;
           tmax = d4.w;
           rp = ray_pre(o, d);
-          trav_init(st, stk + threadIdx.x, kBlock);
+          if constexpr (kW4) {
+            stack4_init(s4, stk + threadIdx.x, kBlock, spill4);
+            cur = 0;
+          } else {
+            trav_init(st, stk + threadIdx.x, kBlock);
+          }
           has = true;
           res = 0;
           nodes_done = false;
@@ -706,18 +742,34 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_shadow_persiste
     }
     if (__ballot_sync(0xffffffffu, has) == 0) break;
     for (;;) {
-      const bool lp = has && res == 0 && leafA != 0;
-      const unsigned lmask = __ballot_sync(0xffffffffu, lp);
-      const unsigned nmask = __ballot_sync(0xffffffffu, has && res == 0 && !nodes_done && !lp);
-      if (lmask && (nmask == 0 || __popc(lmask) >= __popc(nmask))) {
-        if (lp) {
-          if (leaf_any(g, leafA, o, d, tmin, tmax) || (leafB && leaf_any(g, leafB, o, d, tmin, tmax))) res = 1;
-          leafA = leafB = 0;
+      if constexpr (kW4) {
+        const bool lp = has && res == 0 && cur < 0;
+        const bool np = has && res == 0 && cur >= 0 && cur != kDone4;
+        const unsigned lmask = __ballot_sync(0xffffffffu, lp);
+        const unsigned nmask = __ballot_sync(0xffffffffu, np);
+        if (lmask && (nmask == 0 || __popc(lmask) >= __popc(nmask))) {
+          if (lp) {
+            if (leaf_any(g, (uint32_t)cur, o, d, tmin, tmax)) res = 1;
+            else cur = stack4_next(s4, tmax, false);
+          }
+        } else if (np) {
+          cur = trav4_node_any(g, cur, o, rp, tmin, tmax, s4);
         }
-      } else if (has && res == 0 && !nodes_done && !lp) {
-        nodes_done = trav_node_any(g, o, rp, tmin, tmax, st, leafA, leafB);
+        if (has && res == 0 && cur == kDone4) res = -1;
+      } else {
+        const bool lp = has && res == 0 && leafA != 0;
+        const unsigned lmask = __ballot_sync(0xffffffffu, lp);
+        const unsigned nmask = __ballot_sync(0xffffffffu, has && res == 0 && !nodes_done && !lp);
+        if (lmask && (nmask == 0 || __popc(lmask) >= __popc(nmask))) {
+          if (lp) {
+            if (leaf_any(g, leafA, o, d, tmin, tmax) || (leafB && leaf_any(g, leafB, o, d, tmin, tmax))) res = 1;
+            leafA = leafB = 0;
+          }
+        } else if (has && res == 0 && !nodes_done && !lp) {
+          nodes_done = trav_node_any(g, o, rp, tmin, tmax, st, leafA, leafB);
+        }
+        if (has && res == 0 && nodes_done && leafA == 0) res = -1;
       }
-      if (has && res == 0 && nodes_done && leafA == 0) res = -1;
       unsigned fin = __ballot_sync(0xffffffffu, !has || res != 0);
       if (fin == 0xffffffffu || (!drained && __popc(fin) >= refill)) break;
     }
@@ -1906,6 +1958,8 @@ pt_status pass_resources(Context& E, const PassLayout& L, const std::vector<Scen
   if (st == PT_OK) st = E.d_scene_tab.reserve(scenes.size() * sizeof(SceneDev), "scene table");
   if (st == PT_OK) st = E.d_item_tab.reserve(std::max<size_t>(L.items.size(), 1) * sizeof(ItemDev), "item table");
   if (st != PT_OK) return st;
+  E.pass_w4 = true;
+  for (const SceneDev& s : scenes) E.pass_w4 = E.pass_w4 && s.nodes4 != nullptr;
   PT_CHECK_CUDA(cudaMemcpyAsync(E.d_scene_tab.p, scenes.data(), scenes.size() * sizeof(SceneDev), cudaMemcpyHostToDevice, E.stream), "scene table");
   PT_CHECK_CUDA(cudaMemcpyAsync(E.d_item_tab.p, L.items.data(), L.items.size() * sizeof(ItemDev), cudaMemcpyHostToDevice, E.stream), "item table");
   return PT_OK;
@@ -1953,14 +2007,20 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
     g.pc_cnt = wf.pc_cnt.as<uint32_t>();
   }
   const int grid_trace = sm_count() * 8, grid_shade = sm_count() * 8;
+  // the 4-wide BVH when every scene of the pass has one (pass_resources)
+  const bool w4 = E.pass_w4;
   int occ_ext = 0, occ_sh = 0;
-  if (multi) {
-    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, k_extend_persistent<true>, kBlock, 0), "occupancy");
-    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, k_shadow_persistent<true, false>, kBlock, 0), "occupancy");
-  } else {
-    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, k_extend_persistent<false>, kBlock, 0), "occupancy");
-    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, k_shadow_persistent<false, false>, kBlock, 0), "occupancy");
-  }
+  auto occupancy = [&](auto ext, auto sh) -> pt_status {
+    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, ext, kBlock, 0), "occupancy");
+    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, sh, kBlock, 0), "occupancy");
+    return PT_OK;
+  };
+  pt_status ost;
+  if (w4) ost = multi ? occupancy(k_extend_persistent<true, true>, k_shadow_persistent<true, false, true>)
+                      : occupancy(k_extend_persistent<false, true>, k_shadow_persistent<false, false, true>);
+  else ost = multi ? occupancy(k_extend_persistent<true, false>, k_shadow_persistent<true, false, false>)
+                   : occupancy(k_extend_persistent<false, false>, k_shadow_persistent<false, false, false>);
+  if (ost != PT_OK) return ost;
   const int grid_persist = sm_count() * std::max(1, std::min(occ_ext, occ_sh));
   const bool prof = c.profile && allow_events;
   PT_CHECK_CUDA(cudaMemsetAsync(w.cnt, 0, kCounters * 4, c.stream), "reset counters");
@@ -2001,8 +2061,13 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
       PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + w.out_slot, 0, 4, c.stream), "reset queues");
       if ((st = prof_begin(PROF_EXTEND)) != PT_OK) return st;
       if (c.opt.extend_mode == 1) {
-        if (multi) k_extend_persistent<true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-        else k_extend_persistent<false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+        if (w4) {
+          if (multi) k_extend_persistent<true, true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          else k_extend_persistent<false, true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+        } else {
+          if (multi) k_extend_persistent<true, false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          else k_extend_persistent<false, false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+        }
       } else {
         k_extend<<<grid_trace, kBlock, 0, c.stream>>>(w);
       }
@@ -2027,10 +2092,17 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
         count_launch();
       }
       if (c.opt.extend_mode == 1) {
-        if (multi && adjoint) k_shadow_persistent<true, true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-        else if (multi) k_shadow_persistent<true, false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-        else if (adjoint) k_shadow_persistent<false, true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-        else k_shadow_persistent<false, false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+        if (w4) {
+          if (multi && adjoint) k_shadow_persistent<true, true, true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          else if (multi) k_shadow_persistent<true, false, true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          else if (adjoint) k_shadow_persistent<false, true, true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          else k_shadow_persistent<false, false, true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+        } else {
+          if (multi && adjoint) k_shadow_persistent<true, true, false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          else if (multi) k_shadow_persistent<true, false, false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          else if (adjoint) k_shadow_persistent<false, true, false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          else k_shadow_persistent<false, false, false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+        }
       } else {
         if (adjoint) k_shadow<true><<<grid_trace, kBlock, 0, c.stream>>>(w);
         else k_shadow<false><<<grid_trace, kBlock, 0, c.stream>>>(w);

@@ -142,6 +142,7 @@ struct IntegratorDev {
 
 struct SceneDev {
   const float4* nodes;
+  const float4* nodes4;  // the 4-wide BVH (8 float4 per node) or null
   const float4* tri_v0;
   const float4* tri_e1;
   const float4* tri_e2;
@@ -184,8 +185,9 @@ struct TravGeom {
   const float4* tri_v0;
   const float4* tri_e1;
   const float4* tri_e2;
+  const float4* nodes4;
 };
-PT_HD TravGeom trav_geom(const SceneDev& S) { return TravGeom{S.nodes, S.tri_v0, S.tri_e1, S.tri_e2}; }
+PT_HD TravGeom trav_geom(const SceneDev& S) { return TravGeom{S.nodes, S.tri_v0, S.tri_e1, S.tri_e2, S.nodes4}; }
 
 struct Ray {
   float3 o, d;
@@ -502,6 +504,116 @@ template <class G> PT_HD bool trav_node_any(const G& S, const float3& o, const R
     return false;
   }
   return !trav_backtrack(S, o, rp, tmin, tmax, st, false);
+}
+
+// ------------------------------------------------------------------ 4-wide BVH traversal
+// Node (128 bytes, one cache line): float4 (lo.x of children 0..3), (hi.x), (lo.y), (hi.y), (lo.z),
+// (hi.z), int4 child codes (>= 0: node, < 0: leaf code as in the BVH2; empty slots are leaves of no
+// triangles behind a box at 1e30), float4 (child count, 0, 0, 0).  Traversal keeps the hit children
+// that are not visited next on a stack, nearest last, with their entry distance; closest-hit pops
+// skip entries beyond the closest hit found so far (entry distance > t * kSlack), as re-testing the
+// box would.  The stack is a ring of kRing4 entries (caller memory, typically shared, [slot][thread])
+// whose oldest entries spill to a per-thread array of kSpill4 entries (caller memory, typically a
+// local array) when it overflows.
+constexpr int kRing4 = 8;
+constexpr int kSpill4 = 3 * 40 + 8;  // three pending children per level, kMaxDepth4 = 40 levels
+constexpr int kDone4 = 0x7fffffff;
+struct Stack4 {
+  uint2* ring;
+  uint2* spill;
+  int stride;
+  int sp, spilled;
+};
+PT_HD void stack4_init(Stack4& s, uint2* ring, int stride, uint2* spill)
+{
+  s.ring = ring;
+  s.spill = spill;
+  s.stride = stride;
+  s.sp = 0;
+  s.spilled = 0;
+}
+PT_HD void stack4_push(Stack4& s, int code, float tn)
+{
+  if (s.sp - s.spilled == kRing4) {
+    s.spill[s.spilled] = s.ring[(s.spilled & (kRing4 - 1)) * s.stride];
+    ++s.spilled;
+  }
+  s.ring[(s.sp & (kRing4 - 1)) * s.stride] = make_uint2((uint32_t)code, (uint32_t)as_int(tn));
+  ++s.sp;
+}
+PT_HD uint2 stack4_pop(Stack4& s)
+{
+  const int i = --s.sp;
+  if (i >= s.spilled) return s.ring[(i & (kRing4 - 1)) * s.stride];
+  s.spilled = i;
+  return s.spill[i];
+}
+// Next node or leaf to visit (kDone4 when none): pops, skipping entries beyond tlimit * kSlack.
+PT_HD int stack4_next(Stack4& s, float tlimit, bool cull)
+{
+  while (s.sp > 0) {
+    const uint2 e = stack4_pop(s);
+    if (!cull || as_float((int)e.y) <= tlimit * kSlack) return (int)e.x;
+  }
+  return kDone4;
+}
+// Tests the four children of node `node`; returns their count of hits, with (code, t) sorted near to
+// far (misses last, at t = +inf).  A five-comparator sorting network on registers.
+PT_HD void cswap4(int code[4], float t[4], int a, int b)
+{
+  const bool sw = t[b] < t[a];
+  const float ta = t[a], tb = t[b];
+  const int ca = code[a], cb = code[b];
+  t[a] = sw ? tb : ta;
+  t[b] = sw ? ta : tb;
+  code[a] = sw ? cb : ca;
+  code[b] = sw ? ca : cb;
+}
+template <class G> PT_HD int node4_hits(const G& S, int node, const float3& o, const RayPre& rp, float tmin, float tmax, int code[4], float t[4])
+{
+  const float4* nd = S.nodes4 + 8 * (size_t)node;
+  const float4 lx = PT_LDG(nd), hx = PT_LDG(nd + 1), ly = PT_LDG(nd + 2), hy = PT_LDG(nd + 3), lz = PT_LDG(nd + 4), hz = PT_LDG(nd + 5);
+  const int4 c = PT_LDG(reinterpret_cast<const int4*>(nd + 6));
+  t[0] = slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, o, rp, tmin, tmax);
+  t[1] = slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, o, rp, tmin, tmax);
+  t[2] = slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, o, rp, tmin, tmax);
+  t[3] = slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, o, rp, tmin, tmax);
+  code[0] = c.x;
+  code[1] = c.y;
+  code[2] = c.z;
+  code[3] = c.w;
+  const float inf = as_float(0x7f800000);
+  const int n = (t[0] != inf) + (t[1] != inf) + (t[2] != inf) + (t[3] != inf);
+  cswap4(code, t, 0, 1);
+  cswap4(code, t, 2, 3);
+  cswap4(code, t, 0, 2);
+  cswap4(code, t, 1, 3);
+  cswap4(code, t, 1, 2);
+  return n;
+}
+// Pushes the hit children after the nearest (far to near) and returns the nearest, or pops the next
+// target when no child was hit.
+PT_HD int node4_advance(int n, const int code[4], const float t[4], Stack4& stk, float tlimit, bool cull)
+{
+#pragma unroll
+  for (int j = 3; j >= 1; --j)
+    if (j < n) stack4_push(stk, code[j], t[j]);
+  return n ? code[0] : stack4_next(stk, tlimit, cull);
+}
+// One closest-hit node step: cur must be a node; returns the next target (node, leaf or kDone4).
+template <class G> PT_HD int trav4_node_closest(const G& S, int cur, const float3& o, const RayPre& rp, float tmin, const Hit& h, Stack4& stk)
+{
+  int code[4];
+  float t[4];
+  const int n = node4_hits(S, cur, o, rp, tmin, h.t, code, t);
+  return node4_advance(n, code, t, stk, h.t, true);
+}
+template <class G> PT_HD int trav4_node_any(const G& S, int cur, const float3& o, const RayPre& rp, float tmin, float tmax, Stack4& stk)
+{
+  int code[4];
+  float t[4];
+  const int n = node4_hits(S, cur, o, rp, tmin, tmax, code, t);
+  return node4_advance(n, code, t, stk, tmax, false);
 }
 
 template <class G> PT_HD Hit trace_closest(const G& S, const float3& o, const float3& d, float tmin, float tmax)

@@ -10,6 +10,7 @@ using namespace pt;
 
 struct HostScene {
   BvhHost bvh;
+  std::vector<float4> nodes4;
   SceneDev S;
 };
 
@@ -23,6 +24,8 @@ extern "C" __attribute__((visibility("default"))) void* ht_build(const float* tr
   h->S.tri_e1 = h->bvh.tri_e1.data();
   h->S.tri_e2 = h->bvh.tri_e2.data();
   h->S.n_tris = n;
+  int depth4 = 0;
+  if (build_bvh4(h->bvh, h->nodes4, depth4)) h->S.nodes4 = h->nodes4.data();
   if (depth_out) *depth_out = h->bvh.depth;
   return h;
 }
@@ -54,6 +57,57 @@ extern "C" __attribute__((visibility("default"))) void ht_trace_stack(void* hp, 
     while ((res = trav_step_any(h->S, o, d, rp, r[3], r[7], st)) == 0) {}
     any[i] = res > 0 ? 1 : 0;
   }
+}
+// The 4-wide BVH walked as the persistent kernels walk it (the next target a node, a leaf or kDone4;
+// a kRing4-entry ring spilling to a local array).  max_sp: the deepest stack seen (above kRing4, the
+// spill path ran).  Returns 0, or -1 when the scene has no 4-wide BVH.
+extern "C" __attribute__((visibility("default"))) int ht_trace4(void* hp, const float* rays, long n, int* prim, float* t, float* bary, int* any, int* max_sp)
+{
+  HostScene* h = (HostScene*)hp;
+  if (!h->S.nodes4) return -1;
+  *max_sp = 0;
+  for (long i = 0; i < n; ++i) {
+    const float* r = rays + 8 * i;
+    float3 o = make_float3(r[0], r[1], r[2]), d = make_float3(r[4], r[5], r[6]);
+    uint2 ring[kRing4], spill[kSpill4];
+    const int stride = 1;
+    RayPre rp = ray_pre(o, d);
+    Hit hh;
+    hh.t = r[7];
+    hh.u = hh.v = 0.0f;
+    hh.prim = -1;
+    Stack4 s4;
+    stack4_init(s4, ring, stride, spill);
+    int cur = 0;
+    while (cur != kDone4) {
+      if (cur < 0) {
+        leaf_closest(h->S, (uint32_t)cur, o, d, r[3], hh);
+        cur = stack4_next(s4, hh.t, true);
+      } else {
+        cur = trav4_node_closest(h->S, cur, o, rp, r[3], hh, s4);
+      }
+      *max_sp = s4.sp > *max_sp ? s4.sp : *max_sp;
+    }
+    prim[i] = hh.prim;
+    t[i] = hh.prim >= 0 ? hh.t : -1.0f;
+    bary[2 * i] = hh.u;
+    bary[2 * i + 1] = hh.v;
+    stack4_init(s4, ring, stride, spill);
+    cur = 0;
+    int res = 0;
+    while (res == 0) {
+      if (cur == kDone4) res = -1;
+      else if (cur < 0) {
+        if (leaf_any(h->S, (uint32_t)cur, o, d, r[3], r[7])) res = 1;
+        else cur = stack4_next(s4, r[7], false);
+      } else {
+        cur = trav4_node_any(h->S, cur, o, rp, r[3], r[7], s4);
+      }
+      *max_sp = s4.sp > *max_sp ? s4.sp : *max_sp;
+    }
+    any[i] = res > 0 ? 1 : 0;
+  }
+  return 0;
 }
 // rays: n x 8 floats (origin, tmin, dir, tmax)
 extern "C" __attribute__((visibility("default"))) void ht_trace(void* hp, const float* rays, long n, int* prim, float* t, float* bary, int* any)

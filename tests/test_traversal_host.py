@@ -1,7 +1,8 @@
-"""The product's BVH builder and stackless traversal (pt_bvh.cu, pt_scene.cuh), compiled for the
-host by tests/native/host_trace.cu, against the brute-force oracle: closest-hit index, t and
-barycentrics and any-hit bit-identical, including rays aimed exactly at vertices and edges.  Runs
-without a GPU (the same code runs on the device in tests/test_render_gpu.py)."""
+"""The product's BVH builders and traversals (pt_bvh.cu, pt_scene.cuh: stackless BVH2, its short-stack
+variant, the 4-wide BVH with its ring-and-spill stack), compiled for the host by
+tests/native/host_trace.cu, against the brute-force oracle: closest-hit index, t and barycentrics and
+any-hit bit-identical, including rays aimed exactly at vertices and edges.  Runs without a GPU (the
+same code runs on the device in tests/test_render_gpu.py)."""
 import ctypes
 import os
 import subprocess
@@ -32,6 +33,7 @@ def host_lib():
     L.ht_free.argtypes = [ctypes.c_void_p]
     L.ht_trace.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long] + [ctypes.c_void_p] * 4
     L.ht_trace_stack.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long] + [ctypes.c_void_p] * 4
+    L.ht_trace4.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long] + [ctypes.c_void_p] * 5
     return L
 
 
@@ -65,9 +67,16 @@ def test_host_traversal_matches_brute_force(host_lib, subdiv):
     prim2, t2 = np.empty(n, np.int32), np.empty(n, np.float32)
     bary2, anyh2 = np.empty((n, 2), np.float32), np.empty(n, np.int32)
     host_lib.ht_trace_stack(h, oc.fp(rays), n, oc.fp(prim2), oc.fp(t2), oc.fp(bary2), oc.fp(anyh2))
+    # the 4-wide BVH of the persistent kernels
+    prim4, t4 = np.empty(n, np.int32), np.empty(n, np.float32)
+    bary4, anyh4 = np.empty((n, 2), np.float32), np.empty(n, np.int32)
+    max_sp = ctypes.c_int()
+    assert host_lib.ht_trace4(h, oc.fp(rays), n, oc.fp(prim4), oc.fp(t4), oc.fp(bary4), oc.fp(anyh4), ctypes.byref(max_sp)) == 0
     host_lib.ht_free(h)
+    if subdiv == (4, 3):
+        assert max_sp.value > 8  # the shared-memory ring overflowed into the spill array
     bp, bt, bb, ba = oc.OracleScene(data).trace(rays, brute=True)
-    for p_, t_, b_, a_ in ((prim, t, bary, anyh), (prim2, t2, bary2, anyh2)):
+    for p_, t_, b_, a_ in ((prim, t, bary, anyh), (prim2, t2, bary2, anyh2), (prim4, t4, bary4, anyh4)):
         assert np.array_equal(p_, bp)
         assert np.array_equal(t_.view(np.uint32), bt.view(np.uint32))
         assert np.array_equal(b_.view(np.uint32), bb.view(np.uint32))
@@ -84,6 +93,10 @@ def test_single_triangle_and_degenerate_scenes(host_lib):
         prim, t = np.empty(2, np.int32), np.empty(2, np.float32)
         bary, anyh = np.empty((2, 2), np.float32), np.empty(2, np.int32)
         host_lib.ht_trace(h, oc.fp(rays), 2, oc.fp(prim), oc.fp(t), oc.fp(bary), oc.fp(anyh))
-        host_lib.ht_free(h)
         assert prim[0] == 0 and t[0] == 1.0 and anyh[0] == 1   # ties between coincident copies go to index 0
+        assert prim[1] == -1 and anyh[1] == 0
+        max_sp = ctypes.c_int()
+        assert host_lib.ht_trace4(h, oc.fp(rays), 2, oc.fp(prim), oc.fp(t), oc.fp(bary), oc.fp(anyh), ctypes.byref(max_sp)) == 0
+        host_lib.ht_free(h)
+        assert prim[0] == 0 and t[0] == 1.0 and anyh[0] == 1
         assert prim[1] == -1 and anyh[1] == 0
