@@ -18,6 +18,12 @@ a dipole sphere whose sigma_a / sigma_s' are parameters (all seeded U[0.1, 0.9])
 depth 6; L2 loss against a target rendered at 1024 spp from other seeded parameters.  One step = the
 differentiable forward render + the path-replay adjoint; `forward` reports the forward alone.
 
+--workload bsdf: the batched BSDF-query configuration -- 2^22 FP32 queries per step (first half GGX,
+second half Beckmann), alpha ~ U[0.05,1], cos(theta_o) ~ U[0.01,1], (u1,u2) from tea<16> seeded by
+the query index, dielectric eta 1.5; per query the sampled visible normal's reflection wi, the
+Walter BSDF value, the pdf and the Fresnel term.  Unit: M queries/s.  Its CPU baseline is the
+reference's own Microfacet/Fresnel headers compiled for the host (oracle/_ref), on all host cores.
+
 --workload subsurface: 1024 x 1024 pixels x 256 frames (--spp) of the translucent scene: a
 327,680-triangle jittered icosphere with the dipole BSSRDF (standard; --dipole directional), 4,096
 probes per frame (2^20 over the 256 frames), lit by a 2048 x 1024 procedural sky with a sun lobe of
@@ -66,7 +72,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="single_scene", choices=["single_scene", "subsurface", "batched", "adjoint"])
+    ap.add_argument("--workload", default="single_scene", choices=["single_scene", "subsurface", "batched", "adjoint", "bsdf"])
+    ap.add_argument("--queries", type=int, default=1 << 22, help="bsdf workload: queries per step")
     ap.add_argument("--scenes", type=int, default=64, help="batched workload: number of scenes")
     ap.add_argument("--spp", type=int, default=None, help="frames per step (default 64, subsurface 256)")
     ap.add_argument("--width", type=int, default=None)
@@ -146,6 +153,10 @@ class ClockSampler:
             self.t.start()
         except (OSError, FileNotFoundError):
             self.proc = None
+        # the timed region starts once the sampler is live (its first row has arrived)
+        t0 = time.perf_counter()
+        while self.proc and not self.rows and self.proc.poll() is None and time.perf_counter() - t0 < 3.0:
+            time.sleep(0.02)
         return self
 
     def _read(self):
@@ -256,6 +267,194 @@ def run_reference_batched(args):
     print(json.dumps(line), flush=True)
 
 
+BSDF = ("batched BSDF queries: %d FP32 queries per step, first half GGX and second half Beckmann, alpha ~ U[0.05,1], "
+        "cos(theta_o) ~ U[0.01,1], (u1,u2) from tea<16> seeded by the query index, dielectric eta 1.5; outputs the sampled "
+        "wi, the Walter BSDF value, the pdf and the Fresnel term")
+BSDF_BYTES_PER_QUERY = 40  # in: wo 12 + alpha 4; out: wi 12 + f 4 + pdf 4 + F 4
+
+
+def bsdf_cpu_sample(n_max, target_s=10.0, threads=None):
+    """Times the reference's own Microfacet/Fresnel headers compiled for the host (oracle/_ref) on the
+    same query batch, over all host cores (one ctypes call per thread and contiguous chunk of query
+    indices; ctypes releases the GIL).  The sample takes equal numbers of queries from the GGX half
+    and the Beckmann half of the batch.  Falls back to the oracle restatement if the compiled
+    reference is absent."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import oracle_ctypes as oc
+
+    threads = threads or os.cpu_count() or 1
+    kind = "reference" if oc.ref() is not None else "port"
+    which = "ref" if kind == "reference" else "orc"
+
+    def run(n_half):
+        jobs = []
+        per = max(1, (n_half + threads - 1) // threads)
+        for base in (0, n_max // 2):
+            for t in range(threads):
+                first = base + t * per
+                cnt = min(per, base + n_half - first)
+                if cnt <= 0:
+                    break
+                wo, alpha = oc.c1_inputs(cnt, first)
+                jobs.append((first, cnt, wo, alpha))
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=threads) as ex:
+            list(ex.map(lambda j: oc.bsdf_queries(j[1], j[0], n_max // 2, j[2], j[3], which=which), jobs))
+        return time.perf_counter() - t0, sum(j[1] for j in jobs)
+
+    dt, done = run(min(n_max // 2, 1 << 14))
+    rate = done / max(dt, 1e-3)
+    dt, done = run(int(min(n_max // 2, max(1 << 14, rate * target_s / 2))))
+    return {"value": done / dt / 1e6, "unit": "M queries/s", "cores": threads, "kind": kind,
+            "sample": "%d queries (half from each distribution's range of the %d-query batch), %s, %d threads, %.1f s" % (
+                done, n_max, "the reference's Microfacet/Fresnel headers compiled for the host with g++ -O2, no fast-math"
+                if kind == "reference" else "the oracle restatement of the reference's math", threads, dt)}
+
+
+def run_bsdf(args, world, rank, local):
+    import torch
+
+    from open_rendering_framework_b200 import _native as nat
+
+    torch.cuda.set_device(local)
+    n = args.queries
+    L = nat.lib()
+    wo = np.empty((3, n), np.float32)
+    alpha = np.empty(n, np.float32)
+    nat.call("pt_c1_make_inputs", n, 0, wo.ctypes.data, alpha.ctypes.data)
+    dev = torch.device("cuda", local)
+    d_wo = torch.from_numpy(wo).to(dev)
+    d_a = torch.from_numpy(alpha).to(dev)
+    d_wi = torch.empty((3, n), dtype=torch.float32, device=dev)
+    d_f, d_pdf, d_F = (torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3))
+    stream = torch.cuda.current_stream(dev)
+    sh = ctypes.c_void_p(stream.cuda_stream)
+
+    def launch():
+        nat.call("pt_bsdf_queries", d_wo.data_ptr(), d_a.data_ptr(), n, 0, n // 2, 1.0 / 1.5, d_wi.data_ptr(), d_f.data_ptr(),
+                 d_pdf.data_ptr(), d_F.data_ptr(), sh)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    for _ in range(max(3, args.warmup)):
+        launch()
+    torch.cuda.synchronize()
+    barrier()
+    launches0 = L.pt_kernel_launch_count()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with ClockSampler(local) as clocks:
+        evs[0].record(stream)
+        for k in range(args.steps):
+            launch()
+            evs[k + 1].record(stream)
+        torch.cuda.synchronize()
+    launches = L.pt_kernel_launch_count() - launches0
+    ms = evs[0].elapsed_time(evs[-1])
+    barrier()
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps * n / (ms_max * 1e-3) / 1e6
+
+    # end to end: host buffers through pt_bsdf_queries_host (H2D of wo and alpha, the kernel, D2H of
+    # wi, f, pdf and F, synchronous) from pinned host memory
+    h_wo = torch.from_numpy(wo).pin_memory()
+    h_a = torch.from_numpy(alpha).pin_memory()
+    h_wi = torch.empty((3, n), dtype=torch.float32).pin_memory()
+    h_f, h_pdf, h_F = (torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(3))
+
+    def host_call():
+        nat.call("pt_bsdf_queries_host", h_wo.data_ptr(), h_a.data_ptr(), n, 0, n // 2, 1.0 / 1.5, h_wi.data_ptr(), h_f.data_ptr(),
+                 h_pdf.data_ptr(), h_F.data_ptr())
+
+    host_call()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        host_call()
+    e2e_s = time.perf_counter() - t0
+    t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.steps * n / float(t.item()) / 1e6
+    same = bool(torch.equal(h_f, d_f.cpu()) and torch.equal(h_wi, d_wi.cpu()))
+
+    peak, peak_kind = load_peaks()
+    launch_ms = ms_max / args.steps
+    achieved = BSDF_BYTES_PER_QUERY * n / (launch_ms * 1e-3) / 1e9
+    per_q = profile_figure("k_bsdf_queries_c1.md", "traffic_bytes_per_query:")
+    line = {
+        "metric": "M BSDF queries/s (batched BSDF queries on 1 B200)", "value": value, "unit": "M queries/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": launch_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": BSDF % n, "queries_per_step": n, "parallelism": "replicas (one independent batch per GPU)",
+                   "l2": "inputs + outputs of %.0f MB per step, larger than L2" % (BSDF_BYTES_PER_QUERY * n / 1e6)},
+        "e2e": {"value": e2e_value, "unit": "M queries/s", "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 24 * n,
+                "what": "pt_bsdf_queries_host from pinned host buffers (copies in, kernel, copies out, synchronous)",
+                "identical_to_device_path": same},
+        "roofline": {"bound": "hbm", "kernel": "k_bsdf_queries", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": per_q * n if per_q else None,
+                     "traffic_unit": "bytes per launch (ncu capture of the same launch size)",
+                     "note": "the kernel is bound by instruction issue (16-round TEA, transcendentals, the Beckmann Newton loop and "
+                             "double erfinv), not by its 40 algorithmic bytes per query"},
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = bsdf_cpu_sample(n)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_reference_bsdf(args):
+    """Reference arm of the bsdf workload: the reference's headers compiled for the host, all host
+    cores, each step a bounded sample of the query batch."""
+    n = args.queries
+    for _ in range(max(0, min(args.warmup, 1))):
+        bsdf_cpu_sample(n, target_s=1.0)
+    vals, secs = [], 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        s = bsdf_cpu_sample(n, target_s=4.0)
+        secs += time.perf_counter() - t0
+        vals.append(s["value"])
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": "M BSDF queries/s (batched BSDF queries on 1 B200)", "value": value, "unit": "M queries/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / max(1, args.steps),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": BSDF % n, "sample_per_step": s["sample"]},
+        "cpu_baseline": dict(s, value=value),
+        "e2e": {"value": value, "unit": "M queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def profile_figure(name, key):
+    """A figure written as `key value` in a committed ncu summary under profiles/."""
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith(key):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
 def run_reference(args, world, rank):
     from open_rendering_framework_b200 import scenes
 
@@ -263,6 +462,8 @@ def run_reference(args, world, rank):
         return
     if args.workload == "batched":
         return run_reference_batched(args)
+    if args.workload == "bsdf":
+        return run_reference_bsdf(args)
     data, _, desc = workload(args)
     from oracle import oracle_ctypes as oc
 
@@ -645,6 +846,8 @@ def main():
             run_reference(args, world, rank)
         elif args.workload == "batched":
             run_batched(args, world, rank, local)
+        elif args.workload == "bsdf":
+            run_bsdf(args, world, rank, local)
         elif args.workload == "adjoint":
             if rank == 0:
                 run_adjoint(args, world, rank, local)

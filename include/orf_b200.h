@@ -96,12 +96,15 @@ typedef struct pt_ctx pt_ctx;
 /* Material types: the values of MaterialType (structs.h:209-225) for the shaders this path
  * implements, plus the emitter material that TriangleAreaLight attaches (arealight_shader.cu). */
 enum {
-  PT_DIFFUSE_SHADER = 0,           /* diffuse_shader.cu            */
-  PT_ROUGH_TRANSPARENT_SHADER = 3, /* rough_transparent_shader.cu  */
-  PT_METALLIC_SHADER = 4,          /* metallic_shader.cu           */
-  PT_TRANSLUCENT_SHADER = 5,       /* subsurface_scattering_shader.cu */
-  PT_ROUGH_TRANSLUCENT_SHADER = 6, /* rough_subsurface_scattering_shader.cu */
-  PT_AREA_LIGHT_MATERIAL = 100     /* arealight_shader.cu          */
+  PT_DIFFUSE_SHADER = 0,              /* diffuse_shader.cu            */
+  PT_TRANSPARENT_SHADER = 2,          /* transparent_shader.cu        */
+  PT_ROUGH_TRANSPARENT_SHADER = 3,    /* rough_transparent_shader.cu  */
+  PT_METALLIC_SHADER = 4,             /* metallic_shader.cu           */
+  PT_TRANSLUCENT_SHADER = 5,          /* subsurface_scattering_shader.cu */
+  PT_ROUGH_TRANSLUCENT_SHADER = 6,    /* rough_subsurface_scattering_shader.cu */
+  PT_LAMBERTIAN_INTERFACE_SHADER = 7, /* lambertian_interface_shader.cu */
+  PT_ROUGH_DIFFUSE_SHADER = 9,        /* rough_diffuse_shader.cu      */
+  PT_AREA_LIGHT_MATERIAL = 100        /* arealight_shader.cu          */
 };
 /* Microfacet model / normal distribution enums: structs.h:242-261. */
 enum { PT_WALTER_MODEL = 0, PT_VISIBLE_NORMALS_MODEL = 1, PT_MULTISCATTERING_MODEL = 2 };
@@ -126,6 +129,30 @@ typedef struct pt_rough_transparent_params {
   uint32_t microfacet_model;
   uint32_t normal_distribution;
 } pt_rough_transparent_params;
+/* mtl["ior"], mtl["glass_absorption"] of TransparentMaterial (TransparentMaterial.cpp:7-20; defaults
+ * ior 1.3, absorption 0): smooth glass with Fresnel reflection / refraction and Beer absorption
+ * inside (transparent_shader.cu:47-115). */
+typedef struct pt_transparent_params {
+  float ior;
+  float glass_absorption[3];
+} pt_transparent_params;
+/* mtl["diffuse_color"], mtl["ior"] of LambertianInterfaceMaterial (LambertianInterfaceMaterial.cpp:7-20;
+ * defaults 1 and 1.3): a Lambertian base under a smooth dielectric interface
+ * (lambertian_interface_shader.cu:51-173). */
+typedef struct pt_lambertian_interface_params {
+  float diffuse_color[3];
+  float ior;
+} pt_lambertian_interface_params;
+/* mtl["diffuse_color"], mtl["ior"], mtl["roughness"], mtl["normal_distribution"], mtl["microfacet_model"]
+ * of RoughDiffuseMaterial (RoughDiffuseMaterial.cpp:7-28; defaults 1, 1.3, (0.1, 0.1), Beckmann,
+ * Walter): a Lambertian base under a rough dielectric interface (rough_diffuse_shader.cu:55-292). */
+typedef struct pt_rough_diffuse_params {
+  float diffuse_color[3];
+  float ior;
+  float roughness[2];
+  uint32_t microfacet_model;
+  uint32_t normal_distribution;
+} pt_rough_diffuse_params;
 /* TranslucentMaterial (TranslucentMaterial.cpp:7-30): scattering and absorption coefficients per
  * RGB channel in 1/mm, the mean cosine of the phase function, the relative index of refraction and
  * the scene-unit scale applied to the coefficients (default 100), plus mtl["dipole_model"]
@@ -183,7 +210,7 @@ void* pt_context_stream(pt_ctx* ctx);
 
 /* PathTracer parameters: context["max_depth"], ["scene_epsilon"], ["exception_color"]
  * (Integrator.cpp:77-93).  rr_start_depth: the diffuse shader's Russian roulette (p = mean albedo,
- * diffuse_shader.cu:165-184) applies from this depth on; 0 is the reference's behaviour. */
+ * diffuse_shader.cu:85-104) applies from this depth on; 0 is the reference's behaviour. */
 pt_status pt_set_integrator(pt_ctx* ctx, uint32_t max_depth, float scene_epsilon, const float exception_color[3],
                             uint32_t rr_start_depth);
 /* PinholeCamera variables eye, U, V, W, patch_origin, patch_dims (Camera.cpp:83-103) and the

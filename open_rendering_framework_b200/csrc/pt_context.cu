@@ -43,6 +43,8 @@ SceneDev Context::view() const
   s.n_lights = (int)lights.size();
   s.n_tri_lights = (int)tri_lights.size();
   s.n_tris = n_tris;
+  s.ana = d_ana.as<float4>();
+  s.n_ana = (uint32_t)(ana.size() / 3);
   s.bg_color = bg_color;
   s.env.tex = d_env_tex.as<float4>();
   s.env.marginal_pdf = d_env_mpdf.as<float>();
@@ -187,6 +189,45 @@ static pt_status make_material(uint32_t type, const void* params, size_t size, M
       m.b = make_float4(p->glass_absorption[0], p->glass_absorption[1], p->glass_absorption[2], 0.0f);
       return PT_OK;
     }
+    case PT_TRANSPARENT_SHADER: {
+      if (size != sizeof(pt_transparent_params)) return fail(PT_INVALID_ARG, "transparent material: wrong parameter size");
+      const pt_transparent_params* p = (const pt_transparent_params*)params;
+      if (!(p->ior > 0.0f && std::isfinite(p->ior))) return fail(PT_INVALID_ARG, "transparent material: ior must be > 0");
+      if (!finite_nonneg3(p->glass_absorption)) return fail(PT_INVALID_ARG, "transparent material: glass_absorption must be finite and >= 0");
+      m.a = make_float4(p->ior, 0.0f, 0.0f, 0.0f);
+      m.b = make_float4(p->glass_absorption[0], p->glass_absorption[1], p->glass_absorption[2], 0.0f);
+      return PT_OK;
+    }
+    case PT_LAMBERTIAN_INTERFACE_SHADER: {
+      if (size != sizeof(pt_lambertian_interface_params)) return fail(PT_INVALID_ARG, "lambertian interface material: wrong parameter size");
+      const pt_lambertian_interface_params* p = (const pt_lambertian_interface_params*)params;
+      if (!finite_nonneg3(p->diffuse_color)) return fail(PT_INVALID_ARG, "lambertian interface material: diffuse_color must be finite and >= 0");
+      if (!(p->ior > 0.0f && std::isfinite(p->ior))) return fail(PT_INVALID_ARG, "lambertian interface material: ior must be > 0");
+      m.a = make_float4(p->diffuse_color[0], p->diffuse_color[1], p->diffuse_color[2], p->ior);
+      m.b = make_float4(two_C1(p->ior), 0.0f, 0.0f, 0.0f);  // r_10 (lambertian_interface_shader.cu:63)
+      return PT_OK;
+    }
+    case PT_ROUGH_DIFFUSE_SHADER: {
+      if (size != sizeof(pt_rough_diffuse_params)) return fail(PT_INVALID_ARG, "rough diffuse material: wrong parameter size");
+      const pt_rough_diffuse_params* p = (const pt_rough_diffuse_params*)params;
+      if (!finite_nonneg3(p->diffuse_color)) return fail(PT_INVALID_ARG, "rough diffuse material: diffuse_color must be finite and >= 0");
+      if (!(p->ior > 0.0f && std::isfinite(p->ior))) return fail(PT_INVALID_ARG, "rough diffuse material: ior must be > 0");
+      if (!(p->roughness[0] > 0.0f && p->roughness[1] > 0.0f && std::isfinite(p->roughness[0]) && std::isfinite(p->roughness[1])))
+        return fail(PT_INVALID_ARG, "rough diffuse material: roughness must be finite and > 0");
+      if (p->microfacet_model > PT_MULTISCATTERING_MODEL || p->normal_distribution > PT_GGX_DISTRIBUTION)
+        return fail(PT_INVALID_ARG, "rough diffuse material: bad microfacet_model or normal_distribution");
+      m.model = p->microfacet_model;
+      m.dist = p->normal_distribution;
+      m.a = make_float4(p->diffuse_color[0], p->diffuse_color[1], p->diffuse_color[2], p->ior);
+      m.b = make_float4(two_C1(p->ior), p->roughness[0], p->roughness[1], 0.0f);  // r_10 (rough_diffuse_shader.cu:70)
+      // the multiscattering conductor walks' eta = MyComplex{1 / ior, 0} per channel (:132-133, :254-255)
+      const float n1_over_n2 = 1.0f / p->ior;
+      for (int c = 0; c < 3; ++c) {
+        m.eta.c[c] = Cx{(double)n1_over_n2, 0.0};
+        m.inv_eta.c[c] = host_recip(m.eta.c[c]);
+      }
+      return PT_OK;
+    }
     case PT_ROUGH_TRANSLUCENT_SHADER: {
       if (size != sizeof(pt_rough_translucent_params)) return fail(PT_INVALID_ARG, "rough translucent material: wrong parameter size");
       const pt_rough_translucent_params* r = (const pt_rough_translucent_params*)params;
@@ -252,7 +293,7 @@ __global__ void k_trace_closest(SceneDev S, const float4* ot, const float4* dt, 
 {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float4 a = ot[i], b = dt[i];
-    Hit h = trace_closest(S, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), a.w, b.w);
+    Hit h = scene_closest(S, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), a.w, b.w);
     prim[i] = h.prim;
     tout[i] = h.prim >= 0 ? h.t : -1.0f;
     bary[2 * i] = h.u;
@@ -263,7 +304,7 @@ __global__ void k_trace_any(SceneDev S, const float4* ot, const float4* dt, uint
 {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float4 a = ot[i], b = dt[i];
-    hit[i] = trace_any(S, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), a.w, b.w) ? 1 : 0;
+    hit[i] = scene_any(S, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), a.w, b.w) ? 1 : 0;
   }
 }
 
@@ -588,7 +629,9 @@ pt_status pt_lights_upload(pt_ctx* ctx, const void* lights, uint32_t n_lights, c
   Context& c = ctx->c;
   c.lights.assign((const LightRaw*)lights, (const LightRaw*)lights + n_lights);
   c.tri_lights.assign((const TriLightRaw*)triangle_lights, (const TriLightRaw*)triangle_lights + n_triangle_lights);
-  for (const LightRaw& l : c.lights) {
+  std::vector<float4> ana;
+  for (uint32_t k = 0; k < n_lights; ++k) {
+    const LightRaw& l = c.lights[k];
     if (l.type > ENVMAP_LIGHT) return fail(PT_INVALID_ARG, "pt_lights_upload: unknown light_type");
     if (l.type == TRIANGLES_AREA_LIGHT) {
       float cnt, start;
@@ -597,10 +640,33 @@ pt_status pt_lights_upload(pt_ctx* ctx, const void* lights, uint32_t n_lights, c
       if (!(cnt >= 1.0f) || !(start >= 0.0f) || (uint64_t)(start + cnt) > n_triangle_lights)
         return fail(PT_INVALID_ARG, "pt_lights_upload: triangle range of a TrianglesAreaLight is outside triangle_light_buffer");
     }
+    if (l.type == DISK_LIGHT || l.type == SPHERICAL_LIGHT) {
+      // DiskLightStruct (position, radius, phi, theta) / SphericalLightStruct (position, radius), structs.h:76-93
+      for (int i = 0; i < 3; ++i)
+        if (!std::isfinite(l.p[i]) || !std::isfinite(l.emitted[i])) return fail(PT_INVALID_ARG, "pt_lights_upload: non-finite disk or sphere light");
+      const float radius = l.pad[0];
+      if (!(radius > 0.0f) || !std::isfinite(radius)) return fail(PT_INVALID_ARG, "pt_lights_upload: disk and sphere lights need a finite radius > 0");
+      float3 normal = f3(0.0f, 1.0f, 0.0f);
+      if (l.type == DISK_LIGHT) {
+        if (!std::isfinite(l.pad[1]) || !std::isfinite(l.pad[2])) return fail(PT_INVALID_ARG, "pt_lights_upload: non-finite disk light angles");
+        // DiskAreaLight::computeNormal (Light.cpp:469-474), evaluated on the host as there
+        const float t_rad = l.pad[2] * kPi / 180.0f, p_rad = l.pad[1] * kPi / 180.0f;
+        normal = f3(sinf(t_rad) * sinf(p_rad), cosf(t_rad), sinf(t_rad) * cosf(p_rad));
+      }
+      const int kind = l.type == DISK_LIGHT ? ANA_DISK : ANA_SPHERE;
+      float kind_f, idx_f;
+      memcpy(&kind_f, &kind, 4);
+      memcpy(&idx_f, &k, 4);
+      ana.push_back(make_float4(l.p[0], l.p[1], l.p[2], radius));
+      ana.push_back(make_float4(normal.x, normal.y, normal.z, kind_f));
+      ana.push_back(make_float4(l.emitted[0], l.emitted[1], l.emitted[2], idx_f));
+    }
   }
+  c.ana.swap(ana);
   PT_CHECK_CUDA(cudaSetDevice(c.device), "cudaSetDevice");
   pt_status st = upload(c.d_lights, c.lights, c.stream, "light buffer");
   if (st == PT_OK) st = upload(c.d_tri_lights, c.tri_lights, c.stream, "triangle light buffer");
+  if (st == PT_OK) st = upload(c.d_ana, c.ana, c.stream, "analytic emitters");
   return st;
 }
 

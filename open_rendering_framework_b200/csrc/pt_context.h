@@ -71,20 +71,27 @@ enum CounterSlot {
   CNT_Q_METAL = 5,
   CNT_Q_GLASS = 6,
   CNT_Q_TRANS = 7,
-  CNT_SHADOW = 8,
-  CNT_FETCH_EXT = 9,
-  CNT_FETCH_SH = 10,
-  CNT_GATHER = 11,
-  CNT_SEGMENTS_LO = 12,  // 64-bit totals as two words each (atomicAdd on unsigned long long)
-  CNT_SHADOW_TOTAL = 14,
-  CNT_CAPPED = 16,
-  CNT_CLAMPED = 18,
-  CNT_ERROR = 20,
-  CNT_PAIRS = 22,        // probe evaluations of the dipole gathers
-  CNT_GATHERS = 24,      // dipole gathers evaluated
+  CNT_Q_LAYERED = 8,
+  CNT_SHADOW = 9,
+  CNT_FETCH_EXT = 10,
+  CNT_FETCH_SH = 11,
+  CNT_GATHER = 12,
+  CNT_SEGMENTS_LO = 14,  // 64-bit totals as two words each at even slots (8-byte aligned atomicAdd on unsigned long long)
+  CNT_SHADOW_TOTAL = 16,
+  CNT_CAPPED = 18,
+  CNT_CLAMPED = 20,
+  CNT_ERROR = 22,
+  CNT_PAIRS = 24,        // probe evaluations of the dipole gathers
+  CNT_GATHERS = 26,      // dipole gathers evaluated
   kCounters = 32
 };
-enum QueueClass { QC_MISS = 0, QC_LIGHT = 1, QC_DIFFUSE = 2, QC_METAL = 3, QC_GLASS = 4, QC_TRANS = 5, kQueues = 6 };
+static_assert(CNT_SEGMENTS_LO % 2 == 0 && CNT_SHADOW_TOTAL % 2 == 0 && CNT_CAPPED % 2 == 0 && CNT_CLAMPED % 2 == 0 &&
+                  CNT_ERROR % 2 == 0 && CNT_PAIRS % 2 == 0 && CNT_GATHERS % 2 == 0 && CNT_GATHERS + 2 <= kCounters,
+              "64-bit counters sit at even slots inside the counter block");
+// Material classes of the extend kernel's binning; QC_LAYERED: a Lambertian base under a smooth or rough
+// dielectric interface (lambertian_interface_shader.cu, rough_diffuse_shader.cu).
+enum QueueClass { QC_MISS = 0, QC_LIGHT = 1, QC_DIFFUSE = 2, QC_METAL = 3, QC_GLASS = 4, QC_TRANS = 5, QC_LAYERED = 6, kQueues = 7 };
+static_assert(CNT_Q_MISS + kQueues - 1 == CNT_Q_LAYERED, "one consecutive count per material class");
 
 // One (scene, frame range) of a wavefront pass.  The camera paths, probes, accumulated pixels and probe
 // sets of a pass are numbered item after item; every path records its item.
@@ -159,6 +166,8 @@ struct Context {
   uint32_t n_tris = 0;
 
   DevBuf d_nodes, d_nodes4, d_v0, d_e1, d_e2, d_info, d_normals, d_mats, d_lights, d_tri_lights;
+  std::vector<float4> ana;  // analytic emitters of the disk and sphere lights (3 float4 each)
+  DevBuf d_ana;
   bool has_bvh4 = false;
   bool use_bvh4 = true;  // option "bvh4": the persistent traversal kernels walk the 4-wide BVH
   DevBuf d_scat, d_trans_objs, d_trans_pos;

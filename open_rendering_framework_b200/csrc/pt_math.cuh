@@ -272,6 +272,16 @@ PT_HD float fresnel_R(float c1, float c2, float e)  // :26-32
   float rs = fresnel_rs(c1, c2, e), rp = fresnel_rp(c1, c2, e);
   return (rs * rs + rp * rp) * 0.5f;
 }
+// Reflectance of a smooth interface for the cosine of incidence c and relative index e, 1 under total
+// internal reflection: the block `R = 1; sin2 = e*e*(1 - c*c); if (sin2 < 1) R = fresnel_R(c, sqrt(1 - sin2), e)`
+// that lambertian_interface_shader.cu:69-76 and rough_diffuse_shader.cu:90-97 repeat for every direction.
+PT_HD float fresnel_interface(float c, float e)
+{
+  float R = 1.0f;
+  const float st2 = e * e * (1.0f - c * c);
+  if (st2 < 1.0f) R = fresnel_R(c, sqrtf(1.0f - st2), e);
+  return R;
+}
 PT_HD float fresnel_R(const float3& wi, const float3& wm, float e)  // :42-54
 {
   float c1 = dot(wi, wm);
@@ -853,12 +863,15 @@ PT_D float3 ms_conductor_eval(uint32_t dist, const float3& wi, const float3& wo,
   return sum;
 }
 // Multiscattering diffuse sample / eval in the local frame, GGX :519-577 / Beckmann :613-674.
+// wm receives the microfacet normal of the walk's last scattering event (the reference's w_m output,
+// which rough_diffuse_shader.cu:196 reads); it stays +z if the walk never scatters.
 PT_D float3 ms_diffuse_sample(uint32_t dist, const float3& wi, float ax, float ay, uint32_t& seed, uint32_t& order, float3& weight,
-                              const float3& rho, int* capped)
+                              const float3& rho, float3& wm, int* capped)
 {
   weight = f3s(1.0f);
   float hr = 1.0f + gauss_inv_cdf(0.9999f);
-  float3 wo = -wi, wm;
+  float3 wo = -wi;
+  wm = f3(0.0f, 0.0f, 1.0f);
   while (order < 100u) {
     float u = rnd_tea(seed);
     hr = sample_height(dist, wo, hr, u, ax, ay);

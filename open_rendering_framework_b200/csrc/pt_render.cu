@@ -276,14 +276,17 @@ __device__ void eval_direct(const SceneDev& S, const float3& pos, const LightRaw
 
 
 // ------------------------------------------------------------------ MD5 stream across vertices
-// The diffuse, conductor and rough-dielectric shaders hand their child ray only the tea seed
-// (diffuse_shader.cu:94-104, metallic_shader.cu:76-156, rough_transparent_shader.cu:114-220): their own
+// The diffuse, conductor, rough-dielectric and layered shaders hand their child ray only the tea seed
+// (diffuse_shader.cu:92-101, metallic_shader.cu:76-156, rough_transparent_shader.cu:114-220,
+// lambertian_interface_shader.cu:143-147, rough_diffuse_shader.cu:207-211): their own
 // MD5 state is never updated from the child, so after such a vertex returns, the dipole gathers of the
 // translucent vertices above it draw from the MD5 state the vertex was entered with (the oracle passes
 // that state down to the child, which the reference leaves uninitialised).  The wavefront keeps one
 // running MD5 state per path and evaluates the gathers at the end, newest first; a vertex of those
 // shaders with gathers pending above it therefore pushes a reset marker holding its entry state,
-// which the gather evaluation restores when it reaches the marker.
+// which the gather evaluation restores when it reaches the marker.  The smooth transparent shader
+// traces its child with its own payload (transparent_shader.cu:110-112), so the MD5 state simply
+// runs on through it and it pushes no marker.
 __device__ __forceinline__ uint32_t push_md5_reset(const WfDev& w, uint32_t pid, uint32_t meta, uint32_t s64x, uint32_t s64y, uint32_t& overflow)
 {
   if (!(meta & META_PROBE) && (meta >> META_GSHIFT) != 0) {
@@ -484,8 +487,11 @@ __device__ __forceinline__ int class_of(uint32_t type)
 {
   switch (type) {
     case MAT_DIFFUSE: return QC_DIFFUSE;
+    case MAT_LAMBERTIAN_INTERFACE: return QC_LAYERED;
+    case MAT_ROUGH_DIFFUSE: return QC_LAYERED;
     case MAT_METAL: return QC_METAL;
     case MAT_ROUGH_GLASS: return QC_GLASS;
+    case MAT_TRANSPARENT: return QC_GLASS;
     case MAT_TRANSLUCENT: return QC_TRANS;
     case MAT_ROUGH_TRANSLUCENT: return QC_TRANS;
     case MAT_LIGHT: return QC_LIGHT;
@@ -506,9 +512,10 @@ __global__ void __launch_bounds__(kBlock) k_extend(WfDev w)
       pid = w.q_in[i];
       const SceneDev& S = scene_of(w, pid);
       float4 o = w.ray_o[pid], d = w.ray_d[pid];
-      Hit h = trace_closest(trav_geom(S), ld3(o), ld3(d), S.integ.scene_epsilon, kDefaultMax);
+      Hit h = scene_closest(S, ld3(o), ld3(d), S.integ.scene_epsilon, kDefaultMax);
       w.hit[pid] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
       if (h.prim < 0) cls = QC_MISS;
+      else if ((uint32_t)h.prim >= S.n_tris) cls = QC_LIGHT;  // a disk or sphere emitter
       else cls = class_of(__ldg(&S.mats[__ldg(&S.tri_info[h.prim].w)].type));
       ++traced;
     }
@@ -647,8 +654,18 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_extend_persiste
     }
     int cls = -1;
     if (has && done && leafA == 0) {
+      // the analytic emitters (disk and sphere lights) after the triangles
+      uint32_t n_tris;
+      if constexpr (kMulti) {
+        const SceneDev& S = scene_of(w, pid);
+        n_tris = S.n_tris;
+        if (S.n_ana) ana_closest(S, o, d, eps, h);
+      } else {
+        n_tris = S0.n_tris;
+        if (S0.n_ana) ana_closest(S0, o, d, eps, h);
+      }
       w.hit[pid] = make_float4(h.t, h.u, h.v, as_float(h.prim));
-      cls = h.prim < 0 ? QC_MISS : class_of(__ldg(&mats[__ldg(&tinfo[h.prim].w)].type));
+      cls = h.prim < 0 ? QC_MISS : (uint32_t)h.prim >= n_tris ? QC_LIGHT : class_of(__ldg(&mats[__ldg(&tinfo[h.prim].w)].type));
     }
     uint32_t slot = warp_slot_multi(cls, w.cnt + CNT_Q_MISS);
     if (cls >= 0) w.q_mat[(size_t)cls * w.cap + slot] = pid;
@@ -775,8 +792,12 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_shadow_persiste
     }
     if (has && res != 0) {
       if (res < 0) {
-        if constexpr (kMulti) shadow_unoccluded<kAdj>(scene_of(w, w.sh_pid[slot]), w, slot);
-        else shadow_unoccluded<kAdj>(S0, w, slot);
+        if constexpr (kMulti) {
+          const SceneDev& S = scene_of(w, w.sh_pid[slot]);
+          if (!(S.n_ana && ana_any(S, o, d, tmin, tmax))) shadow_unoccluded<kAdj>(S, w, slot);
+        } else {
+          if (!(S0.n_ana && ana_any(S0, o, d, tmin, tmax))) shadow_unoccluded<kAdj>(S0, w, slot);
+        }
       }
       has = false;
     }
@@ -821,18 +842,224 @@ __global__ void __launch_bounds__(kBlock) k_shade_light(WfDev w)
     if (!(w.rng[pid].w & META_EMIT)) continue;
     float4 h = w.hit[pid], d = w.ray_d[pid];
     int prim = __float_as_int(h.w);
-    int4 info = __ldg(S.tri_info + prim);
-    float3 normal = shading_normal(S, info, h.y, h.z, prim);
-    if (dot(normal, -ld3(d)) > 0.0f) {
+    float3 normal, Le;
+    if ((uint32_t)prim >= S.n_tris) {  // a disk or sphere light's geometry with the same emitter program
+      const uint32_t k = (uint32_t)prim - S.n_tris;
+      normal = ana_normal(S, k, ld3(w.ray_o[pid]), ld3(d), h.x);
+      Le = ld3(__ldg(S.ana + 3 * k + 2));
+    } else {
+      int4 info = __ldg(S.tri_info + prim);
+      normal = shading_normal(S, info, h.y, h.z, prim);
       const MatDev& m = S.mats[info.w];
+      Le = f3(m.a.x, m.a.y, m.a.z);
+    }
+    if (dot(normal, -ld3(d)) > 0.0f) {
       float4 t = w.thr[pid], r = w.rad[pid];
-      float3 L = kAdj ? ld3(r) - ld3(t) * f3(m.a.x, m.a.y, m.a.z) : ld3(r) + ld3(t) * f3(m.a.x, m.a.y, m.a.z);
+      float3 L = kAdj ? ld3(r) - ld3(t) * Le : ld3(r) + ld3(t) * Le;
       w.rad[pid] = make_float4(L.x, L.y, L.z, 0.0f);
     }
   }
 }
 
-// diffuse_shader.cu:122-187.  Adjoint: an albedo texel's gradient through the next-event estimate
+// rough_diffuse_shader.cu:55-292, one vertex of a Lambertian base under a rough dielectric interface:
+// a visible microfacet normal from two tea draws and its Fresnel reflectance R_i; a light sample whose
+// shadow ray is traced here, because the reference evaluates the multiscattering BSDFs (which draw tea
+// randoms) and clears emit_light only when the light is visible; then, with probability 1 - R_i, the
+// base (cosine-weighted about the microfacet normal, or the multiscattering diffuse walk) and otherwise
+// the mirror reflection about the microfacet normal (or the multiscattering conductor walk with
+// eta = 1 / ior, whose weight the reference does not apply).  Adds the light estimate to the path
+// radiance, writes the continuation ray and throughput, and returns whether the path continues.
+__device__ __forceinline__ bool rough_diffuse_vertex(const SceneDev& S, const WfDev& w, uint32_t pid, const float3& hit_pos, const float3& d,
+                                                  const float3& normal, const float3& ffnormal, const MatDev& m, uint32_t& t, bool& emit,
+                                                  uint32_t& clamped, int& capped)
+{
+  const float3 w_i = -d;
+  const float3 dc = f3(m.a.x, m.a.y, m.a.z);
+  const float n1_over_n2 = 1.0f / m.a.w;
+  const float r_10 = m.b.x;
+  const float a_x = m.b.y, a_y = m.b.z;
+  const uint32_t dist = m.dist;
+  const bool ms = m.model == MULTISCATTERING;
+  const float z1 = rnd_tea(t);
+  const float z2 = rnd_tea(t);
+  const float3 mn = sample_visible_normal(dist, w_i, ffnormal, a_x, a_y, z1, z2, &capped);
+  const float R_i = fresnel_interface(dot(w_i, mn), n1_over_n2);
+  const float T_01_i = 1.0f - R_i;
+  const float4 t4 = w.thr[pid];
+  // direct illumination (:100-178)
+  uint32_t li = (uint32_t)((float)S.n_lights * rnd_tea(t));
+  if (li >= (uint32_t)S.n_lights) { li = (uint32_t)S.n_lights - 1; ++clamped; }
+  const float light_pdf = 1.0f / (float)S.n_lights;
+  const LightRaw ls = S.lights[li];
+  float3 w_l, radiance;
+  float ldist;
+  eval_direct(S, hit_pos, ls, w_l, radiance, ldist, t, clamped);
+  radiance = radiance / light_pdf;
+  const float cos_theta_l = dot(ffnormal, w_l);
+  if (cos_theta_l > 0.0f && !scene_any(S, hit_pos, w_l, S.integ.scene_epsilon, ldist)) {
+    const float3 Li = radiance;  // V * radiance with V = 1
+    float3 add;
+    if (ms) {  // :126-139
+      const float3 lwi = to_local(w_i, ffnormal), lwl = to_local(w_l, ffnormal);
+      add = Li * ms_diffuse_eval(dist, lwi, lwl, a_x, a_y, t, dc, 0u, &capped);
+      add = add + Li * ms_conductor_eval(dist, lwi, lwl, m.eta, m.inv_eta, a_x, a_y, t, 0u, &capped);
+    } else {  // :140-176
+      const float3 refl_normal = normalize(w_i + w_l);
+      const float R_refl = fresnel_interface(dot(refl_normal, w_l), n1_over_n2);
+      const float T_01_diff = 1.0f - fresnel_interface(dot(mn, w_l), n1_over_n2);
+      const float G_i_m_refl = masking_G1_aniso(dist, w_i, refl_normal, ffnormal, a_x, a_y);
+      const float G_o_m_refl = masking_G1_aniso(dist, w_l, refl_normal, ffnormal, a_x, a_y);
+      const float G_o_m_diff = masking_G1_aniso(dist, w_l, mn, ffnormal, a_x, a_y);
+      const float D_refl = eval_visible_normal(dist, w_i, refl_normal, ffnormal, a_x, a_y);
+      const float weight_refl = G_i_m_refl * G_o_m_refl * D_refl / (4.0f * fabsf(dot(w_i, ffnormal) * dot(w_l, ffnormal)));
+      add = Li * kInvPi * cos_theta_l * dc * n1_over_n2 * n1_over_n2 * T_01_i * T_01_diff / (1.0f - dc * r_10) * G_o_m_diff;
+      add = add + Li * R_refl * weight_refl;
+    }
+    emit = false;
+    const float4 r = w.rad[pid];
+    w.rad[pid] = make_float4(r.x + t4.x * add.x, r.y + t4.y * add.y, r.z + t4.z * add.z, 0.0f);
+  }
+  // indirect illumination (:181-289)
+  const float xi = rnd_tea(t);
+  float3 nd, weight;
+  if (xi > R_i) {
+    if (ms) {  // :187-218
+      uint32_t order = 0;
+      float3 wgt, lwm;
+      nd = to_world(ms_diffuse_sample(dist, to_local(w_i, ffnormal), a_x, a_y, t, order, wgt, dc, lwm, &capped), ffnormal);
+      const float T_01_r = 1.0f - fresnel_interface(dot(nd, to_world(lwm, ffnormal)), n1_over_n2);
+      weight = f3s(n1_over_n2 * n1_over_n2 * T_01_r) / (1.0f - dc * r_10) * wgt;
+    } else {  // :219-248
+      nd = sample_cosine_weighted(mn, t);
+      const float cos_theta_r = dot(nd, mn);
+      const float G_o_m = masking_G1_aniso(dist, nd, mn, ffnormal, a_x, a_y);
+      if (G_o_m < 0.0f) return false;
+      const float T_01_r = 1.0f - fresnel_interface(cos_theta_r, n1_over_n2);
+      weight = dc * n1_over_n2 * n1_over_n2 * T_01_r / (1.0f - dc * r_10) * G_o_m;
+    }
+  } else {
+    if (ms) {  // :252-269 (the walk's Fresnel weight is not applied)
+      uint32_t order = 10;
+      float3 wgt;
+      nd = to_world(ms_conductor_sample(dist, to_local(w_i, normal), m.eta, m.inv_eta, a_x, a_y, t, order, wgt, &capped), normal);
+      weight = f3s(1.0f);
+    } else {  // :270-287
+      nd = reflect(d, mn);
+      const float G_o_m = masking_G1_aniso(dist, nd, mn, ffnormal, a_x, a_y);
+      if (G_o_m < 0.0f) return false;
+      weight = f3s(G_o_m);
+    }
+  }
+  const float3 nt = ld3(t4) * weight;
+  w.ray_o[pid] = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, 0.0f);
+  w.ray_d[pid] = make_float4(nd.x, nd.y, nd.z, 0.0f);
+  w.thr[pid] = make_float4(nt.x, nt.y, nt.z, 0.0f);
+  return true;
+}
+
+// Layered materials: a Lambertian base under a dielectric interface.
+//  * lambertian_interface_shader.cu:51-173 (smooth interface): the light sample's estimate carries the
+//    interface's Fresnel transmittance in (T_01_i) and out (T_01_l) and the base's internal reflection
+//    1 / (1 - rho r_10); its shadow ray (over [scene_epsilon, dist]) goes to the shadow queue.  With
+//    probability 1 - R_i the path enters the base (cosine-weighted about the shading normal, weight
+//    rho n^2 T_01_r / (1 - rho r_10)), otherwise it is mirrored about the shading normal with emission on.
+//  * rough_diffuse_shader.cu:55-292 (rough interface): rough_diffuse_vertex, shadow ray inline.
+// Neither is differentiable (pt_render_adjoint rejects them); the adjoint variant only settles the
+// pending gradient of the previous vertex and replays the path.
+template <bool kAdj>
+__global__ void __launch_bounds__(kBlock) k_shade_layered(WfDev w)
+{
+  __shared__ uint32_t sm[kWarps + 1];
+  const uint32_t n = w.cnt[CNT_Q_LAYERED];
+  const uint32_t* q = w.q_mat + (size_t)QC_LAYERED * w.cap;
+  uint32_t clamped = 0, overflow = 0, capped_total = 0;
+  for (uint32_t base = blockIdx.x * kBlock; base < n; base += gridDim.x * kBlock) {
+    const uint32_t i = base + threadIdx.x;
+    bool shadow = false, cont = false;
+    uint32_t pid = 0;
+    float3 hit_pos, w_l, sh_contrib;
+    float sh_tmax = 0.0f, eps = 0.0f;
+    if (i < n) {
+      pid = q[i];
+      const SceneDev& S = scene_of(w, pid);
+      if constexpr (kAdj) apply_pending(S, w, pid);
+      eps = S.integ.scene_epsilon;
+      const uint4 rg = w.rng[pid];
+      const int depth = (int)(rg.w & META_DEPTH);
+      if (depth <= S.integ.max_depth) {  // both shaders end the path at depth > max_depth
+        const float4 h = w.hit[pid], o = w.ray_o[pid], d4 = w.ray_d[pid], t4 = w.thr[pid];
+        const int prim = __float_as_int(h.w);
+        const int4 info = __ldg(S.tri_info + prim);
+        const MatDev& m = S.mats[info.w];
+        const float3 d = ld3(d4);
+        hit_pos = ld3(o) + h.x * d;
+        const float3 normal = shading_normal(S, info, h.y, h.z, prim);
+        const float3 ffnormal = faceforward(normal, -d, normal);
+        uint32_t t = rg.x;
+        bool emit = (rg.w & META_EMIT) != 0;
+        if (m.type == MAT_ROUGH_DIFFUSE) {
+          int capped = 0;
+          cont = rough_diffuse_vertex(S, w, pid, hit_pos, d, normal, ffnormal, m, t, emit, clamped, capped);
+          capped_total += capped;
+        } else {
+          const float3 dc = f3(m.a.x, m.a.y, m.a.z);
+          const float n1_over_n2 = 1.0f / m.a.w, r_10 = m.b.x;
+          const float R_i = fresnel_interface(dot(-d, ffnormal), n1_over_n2);
+          const float T_01_i = 1.0f - R_i;
+          const float draw = rnd_tea(t);
+          uint32_t li = (uint32_t)((float)S.n_lights * draw);
+          if (li >= (uint32_t)S.n_lights) { li = (uint32_t)S.n_lights - 1; ++clamped; }
+          const float light_pdf = 1.0f / (float)S.n_lights;
+          const LightRaw ls = S.lights[li];
+          float3 radiance;
+          float dist;
+          eval_direct(S, hit_pos, ls, w_l, radiance, dist, t, clamped);
+          radiance = radiance / light_pdf;
+          const float cos_theta_l = dot(ffnormal, w_l);
+          if (cos_theta_l > 0.0f) {  // :95-118
+            const float T_01_l = 1.0f - fresnel_interface(cos_theta_l, n1_over_n2);
+            shadow = true;
+            sh_tmax = dist;
+            sh_contrib = ld3(t4) * (radiance * kInvPi * cos_theta_l * dc * n1_over_n2 * n1_over_n2 * T_01_l * T_01_i / (1.0f - dc * r_10));
+            emit = false;
+          }
+          const float xi = rnd_tea(t);
+          float3 nd, wgt;
+          if (xi > R_i) {  // :127-153
+            nd = sample_cosine_weighted(ffnormal, t);
+            const float T_01_r = 1.0f - fresnel_interface(dot(nd, ffnormal), n1_over_n2);
+            wgt = dc * n1_over_n2 * n1_over_n2 * T_01_r / (1.0f - dc * r_10);
+          } else {  // :154-170
+            nd = reflect(d, normal);
+            wgt = f3s(1.0f);
+            emit = true;
+          }
+          const float3 nt = ld3(t4) * wgt;
+          w.ray_o[pid] = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, 0.0f);
+          w.ray_d[pid] = make_float4(nd.x, nd.y, nd.z, 0.0f);
+          w.thr[pid] = make_float4(nt.x, nt.y, nt.z, 0.0f);
+          cont = true;
+        }
+        const uint32_t meta = push_md5_reset(w, pid, rg.w & META_KEEP, rg.y, rg.z, overflow);
+        w.rng[pid] = make_uint4(t, rg.y, rg.z, meta | (uint32_t)(depth + 1) | (emit ? META_EMIT : 0u));
+      }
+    }
+    const uint32_t s_slot = block_slot(shadow, w.cnt + CNT_SHADOW, sm);
+    if (shadow) {
+      w.sh_o[s_slot] = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, eps);
+      w.sh_d[s_slot] = make_float4(w_l.x, w_l.y, w_l.z, sh_tmax);
+      w.sh_c[s_slot] = make_float4(sh_contrib.x, sh_contrib.y, sh_contrib.z, __uint_as_float(kNoTexel));
+      w.sh_pid[s_slot] = pid;
+    }
+    const uint32_t c_slot = block_slot(cont, w.cnt + w.out_slot, sm);
+    if (cont) w.q_out[c_slot] = pid;
+  }
+  if (clamped) atomicAdd(cnt64(w.cnt, CNT_CLAMPED), (unsigned long long)clamped);
+  if (overflow) atomicAdd(cnt64(w.cnt, CNT_ERROR), (unsigned long long)overflow);
+  if (capped_total) atomicAdd(cnt64(w.cnt, CNT_CAPPED), (unsigned long long)capped_total);
+}
+
+// diffuse_shader.cu:42-107.  Adjoint: an albedo texel's gradient through the next-event estimate
 // (resolved with the shadow ray) and through the bounce weight albedo / p (pending).
 template <bool kAdj>
 __global__ void __launch_bounds__(kBlock) k_shade_diffuse(WfDev w)
@@ -875,7 +1102,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_diffuse(WfDev w)
         float3 ffnormal = faceforward(normal, -d, normal);
         uint32_t t = rg.x;
         bool emit = (rg.w & META_EMIT) != 0;
-        // uniform light pick and next-event estimation (:135-161)
+        // uniform light pick and next-event estimation (:55-81)
         float draw = rnd_tea(t);
         if (S.n_lights > 0) {
           uint32_t li = (uint32_t)((float)S.n_lights * draw);
@@ -894,7 +1121,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_diffuse(WfDev w)
             emit = false;
           }
         }
-        // Russian roulette on the mean albedo (:165-184)
+        // Russian roulette on the mean albedo (:85-104)
         float prob = (dc.x + dc.y + dc.z) / 3.0f;
         float xi = rnd_tea(t);
         if (depth < S.integ.rr_start) prob = 1.0f;
@@ -927,7 +1154,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_diffuse(WfDev w)
   if (overflow) atomicAdd(cnt64(w.cnt, CNT_ERROR), (unsigned long long)overflow);
 }
 
-// metallic_shader.cu:232-348.  Adjoint: a GGX roughness texel's gradient through the weight, with
+// metallic_shader.cu:45-161.  Adjoint: a GGX roughness texel's gradient through the weight, with
 // the microfacet normal's sampling detached: d ln w / d alpha = d ln D(m) + d ln G1(wi) + d ln G1(wo)
 // for the Walter and the visible-normal models alike.
 template <bool kAdj>
@@ -1021,8 +1248,36 @@ __global__ void __launch_bounds__(kBlock) k_shade_metal(WfDev w)
   if (overflow) atomicAdd(cnt64(w.cnt, CNT_ERROR), (unsigned long long)overflow);
 }
 
-// rough_transparent_shader.cu:66-225 (no parameters to differentiate: the adjoint only settles the
-// pending gradient of the previous vertex)
+struct DirSeed {
+  float3 dir;
+  uint32_t seed;
+};
+// transparent_shader.cu:90-108: Fresnel reflectance about the shading normal (flipped, with the
+// relative index inverted, when the ray is inside), one tea draw choosing the mirror or the refracted
+// direction.
+__device__ __forceinline__ DirSeed smooth_glass_dir(float3 d, float3 normal, float ior, float cos_theta, uint32_t t)
+{
+  const bool inside = cos_theta < 0.0f;
+  const float n1_over_n2 = inside ? ior : 1.0f / ior;
+  const float3 nn = inside ? -normal : normal;
+  const float ci = inside ? -cos_theta : cos_theta;
+  float R = 1.0f, ctt = 0.0f;
+  const float st2 = n1_over_n2 * n1_over_n2 * (1.0f - ci * ci);
+  if (st2 < 1.0f) {
+    ctt = sqrtf(1.0f - st2);
+    R = fresnel_R(ci, ctt, n1_over_n2);
+  }
+  const float reflect_xi = rnd_tea(t);
+  DirSeed r;
+  r.dir = reflect_xi < R ? reflect(d, nn) : n1_over_n2 * d + nn * (n1_over_n2 * ci - ctt);
+  r.seed = t;
+  return r;
+}
+
+// rough_transparent_shader.cu:66-225, and transparent_shader.cu:47-115 for smooth glass (Beer roulette
+// inside, then the Fresnel choice between the mirror and the refracted direction about the shading
+// normal).  No parameters to differentiate: the adjoint only settles the pending gradient of the
+// previous vertex.
 template <bool kAdj>
 __global__ void __launch_bounds__(kBlock) k_shade_glass(WfDev w)
 {
@@ -1041,11 +1296,14 @@ __global__ void __launch_bounds__(kBlock) k_shade_glass(WfDev w)
       if constexpr (kAdj) apply_pending(S, w, pid);
       uint4 rg = w.rng[pid];
       int depth = (int)(rg.w & META_DEPTH);
-      if (depth < S.integ.max_depth) {
+      // rough_transparent_shader.cu:68 ends paths at depth >= max_depth, transparent_shader.cu:50 at depth > max_depth
+      if (depth < S.integ.max_depth ||
+          (depth == S.integ.max_depth && S.mats[__ldg(&S.tri_info[__float_as_int(w.hit[pid].w)].w)].type == MAT_TRANSPARENT)) {
         float4 h = w.hit[pid], o = w.ray_o[pid], d4 = w.ray_d[pid];
         int prim = __float_as_int(h.w);
         int4 info = __ldg(S.tri_info + prim);
         const MatDev& m = S.mats[info.w];
+        const bool smooth = m.type == MAT_TRANSPARENT;
         const float ior = m.a.x, rough = m.a.y;
         float3 d = ld3(d4);
         float3 hit_point = ld3(o) + h.x * d;
@@ -1065,7 +1323,11 @@ __global__ void __launch_bounds__(kBlock) k_shade_glass(WfDev w)
         int capped = 0;
         float3 w_o;
         float3 weight = f3s(1.0f);
-        if (go) {
+        if (go && smooth) {
+          const DirSeed ds = smooth_glass_dir(d, normal, ior, cos_theta, t);
+          w_o = ds.dir;
+          t = ds.seed;
+        } else if (go) {
           float z1 = rnd_tea(t), z2 = rnd_tea(t);
           if (m.model == MULTISCATTERING) {  // :100-120
             uint32_t order = 0;
@@ -1105,7 +1367,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_glass(WfDev w)
           w.thr[pid] = make_float4(nt.x, nt.y, nt.z, 0.0f);
           cont = true;
         }
-        const uint32_t meta = push_md5_reset(w, pid, rg.w & META_KEEP, rg.y, rg.z, overflow);
+        const uint32_t meta = smooth ? (rg.w & META_KEEP) : push_md5_reset(w, pid, rg.w & META_KEEP, rg.y, rg.z, overflow);
         w.rng[pid] = make_uint4(t, rg.y, rg.z, meta | (uint32_t)(depth + 1) | META_EMIT);
       }
     }
@@ -1158,7 +1420,7 @@ __device__ bool rough_translucent_vertex(const SceneDev& S, const WfDev& w, uint
   light_radiance = light_radiance / light_pdf;
   const float cos_l = dot(ffnormal, w_l);
   if (!inside && cos_l > 0.0f) {
-    const float V = trace_any(trav_geom(S), hit_pos, w_l, S.integ.scene_epsilon, ldist) ? 0.0f : 1.0f;
+    const float V = scene_any(S, hit_pos, w_l, S.integ.scene_epsilon, ldist) ? 0.0f : 1.0f;
     if (V > 0.0f) {
       const float3 Li = V * light_radiance;
       float3 add;
@@ -1582,7 +1844,7 @@ __global__ void __launch_bounds__(kBlock) k_probe_gen(WfDev w, SssDev g, uint64_
         if (rough) microfacet(w_i);
         float cos_i = fmaxf(dot(w_i, nrm), 0.0f);
         if (cos_i > 0.0f) {
-          float att = trace_any(S, pos, w_i, S.integ.scene_epsilon, r) ? 0.0f : 1.0f;
+          float att = scene_any(S, pos, w_i, S.integ.scene_epsilon, r) ? 0.0f : 1.0f;
           Le = Le * (att * cos_i / light_pdf);
         } else {
           Le = f3s(0.0f);
@@ -1699,7 +1961,7 @@ __global__ void __launch_bounds__(256) k_probe_compact(WfDev w, SssDev g)
   if (threadIdx.x == 0) g.pc_cnt[set] = total;
 }
 
-// Shadow rays of diffuse_shader.cu:149-161 (every material's any-hit program is opaque).
+// Shadow rays of diffuse_shader.cu:69-81 (every material's any-hit program is opaque).
 template <bool kAdj>
 __global__ void __launch_bounds__(kBlock) k_shadow(WfDev w)
 {
@@ -1708,7 +1970,7 @@ __global__ void __launch_bounds__(kBlock) k_shadow(WfDev w)
     float4 o = w.sh_o[i], d = w.sh_d[i];
     uint32_t pid = w.sh_pid[i];
     const SceneDev& S = scene_of(w, pid);
-    if (!trace_any(trav_geom(S), ld3(o), ld3(d), o.w, d.w)) shadow_unoccluded<kAdj>(S, w, i);
+    if (!scene_any(S, ld3(o), ld3(d), o.w, d.w)) shadow_unoccluded<kAdj>(S, w, i);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0 && n) atomicAdd(cnt64(w.cnt, CNT_SHADOW_TOTAL), (unsigned long long)n);
 }
@@ -1834,9 +2096,10 @@ pt_status prepare_scene(Context& c, const char* who)
   for (const LightRaw& l : c.lights)
     if (l.type == ENVMAP_LIGHT && !c.env_present) return fail(PT_NOT_READY, std::string(who) + ": an environment-map light needs pt_set_envmap");
   for (const MatDev& m : c.mats)
-    if (m.type == MAT_DIFFUSE && c.lights.empty())
+    if ((m.type == MAT_DIFFUSE || m.type == MAT_LAMBERTIAN_INTERFACE || m.type == MAT_ROUGH_DIFFUSE) && c.lights.empty())
       return fail(PT_NOT_READY, std::string(who) +
-                                    ": diffuse materials need at least one light (light_buffer is indexed unguarded by the diffuse shader)");
+                                    ": diffuse materials need at least one light (light_buffer is indexed unguarded by the diffuse, "
+                                    "lambertian-interface and rough-diffuse shaders)");
   const bool sss = !c.trans_objs.empty();
   if (sss && c.lights.empty())
     return fail(PT_NOT_READY, std::string(who) + ": translucent objects need at least one light (the probe pass samples light_buffer)");
@@ -2078,14 +2341,16 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
         k_shade_diffuse<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
         k_shade_metal<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
         k_shade_glass<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
+        k_shade_layered<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
       } else {
         k_shade_miss<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
         k_shade_light<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
         k_shade_diffuse<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
         k_shade_metal<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
         k_shade_glass<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
+        k_shade_layered<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
       }
-      count_launch(6);
+      count_launch(7);
       if (L.sss) {
         if (adjoint) k_shade_translucent<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
         else k_shade_translucent<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
@@ -2218,6 +2483,8 @@ pt_status pt_render_adjoint(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames
       return fail(PT_INVALID_ARG, "pt_render_adjoint: roughness gradients are implemented for the GGX distribution");
     if (m.type == PT_ROUGH_TRANSLUCENT_SHADER)
       return fail(PT_INVALID_ARG, "pt_render_adjoint: rough translucent materials are not differentiable");
+    if (m.type == PT_TRANSPARENT_SHADER || m.type == PT_LAMBERTIAN_INTERFACE_SHADER || m.type == PT_ROUGH_DIFFUSE_SHADER)
+      return fail(PT_INVALID_ARG, "pt_render_adjoint: transparent, lambertian-interface and rough-diffuse materials are not differentiable");
   }
   pt_status st = prepare_scene(c, "pt_render_adjoint");
   if (st != PT_OK) return st;

@@ -51,17 +51,28 @@ PT_HD int as_int(float f)
 constexpr uint32_t kLeafFlag = 0x80000000u;
 constexpr int kMaxDepth = 62;  // depth bound of the build; the traversal trail has 64 bits
 
-enum MatType : uint32_t { MAT_DIFFUSE = 0, MAT_ROUGH_GLASS = 3, MAT_METAL = 4, MAT_TRANSLUCENT = 5, MAT_ROUGH_TRANSLUCENT = 6, MAT_LIGHT = 100 };
+enum MatType : uint32_t {
+  MAT_DIFFUSE = 0,
+  MAT_TRANSPARENT = 2,
+  MAT_ROUGH_GLASS = 3,
+  MAT_METAL = 4,
+  MAT_TRANSLUCENT = 5,
+  MAT_ROUGH_TRANSLUCENT = 6,
+  MAT_LAMBERTIAN_INTERFACE = 7,
+  MAT_ROUGH_DIFFUSE = 9,
+  MAT_LIGHT = 100
+};
 enum DipoleModel : uint32_t { STANDARD_DIPOLE = 0, DIRECTIONAL_DIPOLE = 1 };
 
 // Material record, 16-byte aligned (128 B).
 struct __align__(16) MatDev {
   uint32_t type, model, dist, aux;  // translucent: model = dipole_model, aux = translucent_index (rough: dist = normal distribution,
                                     // a = (scale, roughness x, roughness y, microfacet model))
-  float4 a;   // diffuse: color.xyz | metal: roughness.xy | glass: ior, roughness | light: radiance.xyz
-  float4 b;   // glass: absorption.xyz
-  Cx3 eta;    // metal: 1 / ior (metallic_shader.cu:61), computed on the host
-  Cx3 inv_eta;// metal: 1 / eta (the walk's inside branch)
+  float4 a;   // diffuse: color.xyz | metal: roughness.xy | glass: ior, roughness | transparent: ior | light: radiance.xyz
+              // lambertian interface, rough diffuse: color.xyz, ior
+  float4 b;   // glass, transparent: absorption.xyz | lambertian interface: two_C1(ior) | rough diffuse: two_C1(ior), roughness.xy
+  Cx3 eta;    // metal: 1 / ior (metallic_shader.cu:61) | rough diffuse: (1 / ior, 0) per channel; computed on the host
+  Cx3 inv_eta;// 1 / eta (the walk's inside branch)
   float4 tmap;// texture: cube-map center xyz, texture id in w (int bits, -1 = none)
 };
 
@@ -177,6 +188,10 @@ struct SceneDev {
   const float4* adj_dimg;
   float adj_dscale;
   float* const* mat_grad;
+  // analytic emitters: the disk and sphere geometry that DiskAreaLight and SphericalLight add to the
+  // scene (Light.cpp:370-503, 505-610), 3 float4 each (see AnaKind); their hits carry index n_tris + k
+  const float4* ana;
+  uint32_t n_ana;
 };
 // The traversal's view of a scene (the four arrays it reads), held in registers by kernels that
 // trace rays of several scenes.
@@ -637,6 +652,109 @@ template <class G> PT_HD bool trace_any(const G& S, const float3& o, const float
   int r;
   while ((r = trav_step_any(S, o, d, rp, tmin, tmax, st)) == 0) {}
   return r > 0;
+}
+
+// ------------------------------------------------------------------ analytic emitters
+// Record k of SceneDev::ana: (position, radius), (disk normal, kind), (radiance, light index); the
+// kind is stored as int bits.  Hits are tested after the triangles, emitters in light order, and
+// replace the current hit only when strictly closer (a tie stays with the lower index).
+enum AnaKind : int { ANA_DISK = 3, ANA_SPHERE = 4 };
+
+// disk_mesh.cu:33-55: the ray's parameter at the disk's plane (rays within scene_epsilon of parallel
+// miss) if that point lies inside the radius.
+PT_HD bool ana_disk_t(const float4& a, const float4& b, const float3& o, const float3& d, float eps, float& t)
+{
+  const float3 position = ld3(a), normal = ld3(b);
+  const float3 O = o - position;
+  const float den = dot(normal, d);
+  if (!(fabsf(den) > eps)) return false;
+  t = -dot(O, normal) / den;
+  const float3 point = o + t * d;
+  const float3 v = point - position;
+  return dot(v, v) <= a.w * a.w;
+}
+// sphere_mesh.cu:44-95: the near root (refined by a second solve from the near point when it lies
+// beyond 10 radii) if it is inside (tmin, tmax), else the far root if that is.
+PT_HD bool ana_sphere_t(const float4& a, const float3& o, const float3& d, float tmin, float tmax, float& t)
+{
+  const float3 O = o - ld3(a);
+  const float radius = a.w;
+  float b = dot(O, d);
+  float c = dot(O, O) - radius * radius;
+  float disc = b * b - c;
+  if (!(disc > 0.0f)) return false;
+  float sdisc = sqrtf(disc);
+  const float root1 = (-b - sdisc);
+  const bool do_refine = fabsf(root1) > 10.f * radius;
+  float root11 = 0.0f;
+  if (do_refine) {
+    const float3 O1 = O + root1 * d;
+    b = dot(O1, d);
+    c = dot(O1, O1) - radius * radius;
+    disc = b * b - c;
+    if (disc > 0.0f) {
+      sdisc = sqrtf(disc);
+      root11 = (-b - sdisc);
+    }
+  }
+  const float t1 = root1 + root11;
+  if (t1 > tmin && t1 < tmax) {
+    t = t1;
+    return true;
+  }
+  const float root2 = (-b + sdisc) + (do_refine ? root1 : 0.0f);
+  if (root2 > tmin && root2 < tmax) {
+    t = root2;
+    return true;
+  }
+  return false;
+}
+// Closest analytic hit in (tmin, h.t): updates h.
+PT_HD void ana_closest(const SceneDev& S, const float3& o, const float3& d, float tmin, Hit& h)
+{
+  for (uint32_t k = 0; k < S.n_ana; ++k) {
+    const float4 a = PT_LDG(S.ana + 3 * k), b = PT_LDG(S.ana + 3 * k + 1);
+    float t;
+    const bool hit = as_int(b.w) == ANA_DISK ? (ana_disk_t(a, b, o, d, S.integ.scene_epsilon, t) && t > tmin && t < h.t)
+                                             : ana_sphere_t(a, o, d, tmin, h.t, t);
+    if (hit) {
+      h.t = t;
+      h.u = h.v = 0.0f;
+      h.prim = (int)(S.n_tris + k);
+    }
+  }
+}
+// Any analytic hit in (tmin, tmax): the emitters are opaque to shadow rays (arealight_shader.cu:27-32).
+PT_HD bool ana_any(const SceneDev& S, const float3& o, const float3& d, float tmin, float tmax)
+{
+  for (uint32_t k = 0; k < S.n_ana; ++k) {
+    const float4 a = PT_LDG(S.ana + 3 * k), b = PT_LDG(S.ana + 3 * k + 1);
+    float t;
+    if (as_int(b.w) == ANA_DISK ? (ana_disk_t(a, b, o, d, S.integ.scene_epsilon, t) && t > tmin && t < tmax)
+                                : ana_sphere_t(a, o, d, tmin, tmax, t))
+      return true;
+  }
+  return false;
+}
+// Unit normal of analytic hit k at parameter t of ray (o, d): the disk's normal, or the sphere's
+// (O + t D) / radius with O = o - center (sphere_mesh.cu:78,87), normalised as the emitter program does.
+PT_HD float3 ana_normal(const SceneDev& S, uint32_t k, const float3& o, const float3& d, float t)
+{
+  const float4 a = PT_LDG(S.ana + 3 * k), b = PT_LDG(S.ana + 3 * k + 1);
+  if (as_int(b.w) == ANA_DISK) return normalize(ld3(b));
+  const float3 O = o - ld3(a);
+  return normalize((O + t * d) / a.w);
+}
+// Closest hit / any hit of the whole scene: the BVH's triangles, then the analytic emitters.
+PT_HD Hit scene_closest(const SceneDev& S, const float3& o, const float3& d, float tmin, float tmax)
+{
+  Hit h = trace_closest(trav_geom(S), o, d, tmin, tmax);
+  if (S.n_ana) ana_closest(S, o, d, tmin, h);
+  return h;
+}
+PT_HD bool scene_any(const SceneDev& S, const float3& o, const float3& d, float tmin, float tmax)
+{
+  return trace_any(trav_geom(S), o, d, tmin, tmax) || (S.n_ana && ana_any(S, o, d, tmin, tmax));
 }
 
 // ------------------------------------------------------------------ environment map (Envmap.h)

@@ -18,10 +18,13 @@ from . import _native as nat
 
 # ---------------------------------------------------------------- enums (structs.h)
 DIFFUSE_SHADER = 0
+TRANSPARENT_SHADER = 2
 ROUGH_TRANSPARENT_SHADER = 3
 METALLIC_SHADER = 4
 TRANSLUCENT_SHADER = 5
 ROUGH_TRANSLUCENT_SHADER = 6
+LAMBERTIAN_INTERFACE_SHADER = 7
+ROUGH_DIFFUSE_SHADER = 9
 AREA_LIGHT_MATERIAL = 100
 STANDARD_DIPOLE, DIRECTIONAL_DIPOLE = 0, 1
 WALTER_MODEL, VISIBLE_NORMALS_MODEL, MULTISCATTERING_MODEL = 0, 1, 2
@@ -40,6 +43,19 @@ class MetallicParams(ctypes.Structure):
 
 class RoughTransparentParams(ctypes.Structure):
     _fields_ = [("ior", ctypes.c_float), ("roughness", ctypes.c_float), ("glass_absorption", ctypes.c_float * 3),
+                ("microfacet_model", ctypes.c_uint32), ("normal_distribution", ctypes.c_uint32)]
+
+
+class TransparentParams(ctypes.Structure):
+    _fields_ = [("ior", ctypes.c_float), ("glass_absorption", ctypes.c_float * 3)]
+
+
+class LambertianInterfaceParams(ctypes.Structure):
+    _fields_ = [("diffuse_color", ctypes.c_float * 3), ("ior", ctypes.c_float)]
+
+
+class RoughDiffuseParams(ctypes.Structure):
+    _fields_ = [("diffuse_color", ctypes.c_float * 3), ("ior", ctypes.c_float), ("roughness", ctypes.c_float * 2),
                 ("microfacet_model", ctypes.c_uint32), ("normal_distribution", ctypes.c_uint32)]
 
 
@@ -263,6 +279,78 @@ class RoughTransparentMaterial:
                                       self.normal_distribution)
 
 
+class TransparentMaterial:
+    """Smooth glass (TransparentMaterial.cpp:7-20, shader transparent_shader.cu): mtl["ior"] and
+    mtl["glass_absorption"]; defaults ior 1.3, no absorption."""
+    type = TRANSPARENT_SHADER
+
+    def __init__(self, ior=1.3, glass_absorption=(0.0, 0.0, 0.0)):
+        self.ior = float(ior)
+        self.glass_absorption = tuple(float(x) for x in glass_absorption)
+
+    def params(self):
+        return TransparentParams(self.ior, _f3(self.glass_absorption))
+
+    def setIor(self, i):
+        self.ior = float(i)
+
+    def setAbsorption(self, a):
+        self.glass_absorption = tuple(float(x) for x in a)
+
+
+class LambertianInterfaceMaterial:
+    """Lambertian base under a smooth dielectric interface (LambertianInterfaceMaterial.cpp:7-20,
+    shader lambertian_interface_shader.cu): mtl["diffuse_color"], mtl["ior"]; defaults 1 and 1.3."""
+    type = LAMBERTIAN_INTERFACE_SHADER
+
+    def __init__(self, color=(1.0, 1.0, 1.0), ior=1.3):
+        self.color = tuple(float(x) for x in color)
+        self.ior = float(ior)
+
+    def params(self):
+        return LambertianInterfaceParams(_f3(self.color), self.ior)
+
+    def setColor(self, c):
+        self.color = tuple(float(x) for x in c)
+
+    def setIor(self, i):
+        self.ior = float(i)
+
+
+class RoughDiffuseMaterial:
+    """Lambertian base under a rough dielectric interface (RoughDiffuseMaterial.cpp:7-28, shader
+    rough_diffuse_shader.cu): mtl["diffuse_color"], mtl["ior"], mtl["roughness"],
+    mtl["normal_distribution"], mtl["microfacet_model"]; defaults 1, 1.3, (0.1, 0.1), Beckmann, Walter."""
+    type = ROUGH_DIFFUSE_SHADER
+
+    def __init__(self, color=(1.0, 1.0, 1.0), ior=1.3, roughness=(0.1, 0.1), microfacet_model=WALTER_MODEL,
+                 normal_distribution=BECKMANN_DISTRIBUTION):
+        self.color = tuple(float(x) for x in color)
+        self.ior = float(ior)
+        self.roughness = tuple(float(x) for x in roughness)
+        self.microfacet_model = int(microfacet_model)
+        self.normal_distribution = int(normal_distribution)
+
+    def params(self):
+        return RoughDiffuseParams(_f3(self.color), self.ior, (ctypes.c_float * 2)(*self.roughness), self.microfacet_model,
+                                  self.normal_distribution)
+
+    def setColor(self, c):
+        self.color = tuple(float(x) for x in c)
+
+    def setIor(self, i):
+        self.ior = float(i)
+
+    def setRoughness(self, r):
+        self.roughness = tuple(float(x) for x in r)
+
+    def setMicrofacetModel(self, m):
+        self.microfacet_model = int(m)
+
+    def setNormalDistribution(self, d):
+        self.normal_distribution = int(d)
+
+
 class TranslucentMaterial:
     """Smooth translucent surface with the dipole BSSRDF (TranslucentMaterial.cpp, shader
     subsurface_scattering_shader.cu).  Coefficients per RGB channel in 1/mm, scaled by `scale` to
@@ -365,6 +453,52 @@ class DirectionalLight:
         self.direction, self.radiance = tuple(direction), tuple(radiance)
 
 
+class DiskAreaLight:
+    """DiskAreaLight (Light.cpp:370-503): a one-sided emitting disk at `position` with `radius`, facing
+    the normal (sin theta sin phi, cos theta, sin theta cos phi) for theta / phi in degrees; defaults
+    of the reference's constructor.  Sampled for next-event estimation (LightSampler.h:73-100) and
+    intersected as analytic geometry (disk_mesh.cu) with the area-light emitter program."""
+
+    def __init__(self, position=(0.0, 0.0, 0.0), radiance=(1.0, 1.0, 1.0), radius=1.0, theta=0.0, phi=0.0):
+        self.position = tuple(float(x) for x in position)
+        self.radiance = tuple(float(x) for x in radiance)
+        self.radius = float(radius)
+        self.theta = float(theta)
+        self.phi = float(phi)
+
+    def setPosition(self, p):
+        self.position = tuple(float(x) for x in p)
+
+    def setRadiance(self, r):
+        self.radiance = tuple(float(x) for x in r)
+
+    def setRadius(self, r):
+        self.radius = float(r)
+
+    def setNormal(self, theta, phi):
+        self.theta, self.phi = float(theta), float(phi)
+
+
+class SphericalLight:
+    """SphericalLight (Light.cpp:505-610): an emitting sphere (default radius 0.05), sampled on the
+    hemisphere facing the shaded point (LightSampler.h:103-141) and intersected as analytic geometry
+    (sphere_mesh.cu) with the area-light emitter program."""
+
+    def __init__(self, position=(0.0, 0.0, 0.0), radiance=(1.0, 1.0, 1.0), radius=0.05):
+        self.position = tuple(float(x) for x in position)
+        self.radiance = tuple(float(x) for x in radiance)
+        self.radius = float(radius)
+
+    def setPosition(self, p):
+        self.position = tuple(float(x) for x in p)
+
+    def setRadiance(self, r):
+        self.radiance = tuple(float(x) for x in r)
+
+    def setRadius(self, r):
+        self.radius = float(r)
+
+
 def light_buffers(lights):
     """light_buffer and triangle_light_buffer for a list of lights (OptixSceneLoader.cpp:284-347)."""
     ls = np.zeros(len(lights), LIGHT_DTYPE)
@@ -385,6 +519,16 @@ def light_buffers(lights):
         elif isinstance(L, EnvMapLight):
             ls[k]["light_type"] = 5
             ls[k]["emitted_radiance"] = (1.0, 1.0, 1.0)
+        elif isinstance(L, DiskAreaLight):  # DiskLightStruct: position, radius, phi, theta (structs.h:76-84)
+            ls[k]["light_type"] = DISK_LIGHT
+            ls[k]["emitted_radiance"] = L.radiance
+            ls[k]["p"] = L.position
+            ls[k]["padding"] = (L.radius, L.phi, L.theta)
+        elif isinstance(L, SphericalLight):  # SphericalLightStruct: position, radius (structs.h:86-93)
+            ls[k]["light_type"] = SPHERICAL_LIGHT
+            ls[k]["emitted_radiance"] = L.radiance
+            ls[k]["p"] = L.position
+            ls[k]["padding"] = (L.radius, 0.0, 0.0)
         elif isinstance(L, DirectionalLight):
             ls[k]["light_type"] = DIRECTIONAL_LIGHT
             ls[k]["emitted_radiance"] = L.radiance

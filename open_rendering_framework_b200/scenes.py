@@ -86,6 +86,51 @@ def single_scene(width=512, height=512, metal_subdiv=6, glass_subdiv=5, max_dept
     return sc.SceneData(integrator, camera, background, meshes, lights)
 
 
+def layered_scene(width=64, height=64, subdiv=3, max_depth=8, rr_start_depth=0, rough_model=sc.WALTER_MODEL,
+                  rough_distribution=sc.BECKMANN_DISTRIBUTION):
+    """The remaining material programs side by side in the diffuse box under the quad light: a Lambertian
+    base under a smooth interface (lambertian_interface_shader.cu), one under a rough interface
+    (rough_diffuse_shader.cu, with the given microfacet model and distribution) and a smooth glass
+    sphere with absorption (transparent_shader.cu)."""
+    integrator = sc.PathTracer(max_depth=max_depth, scene_epsilon=1e-4, rr_start_depth=rr_start_depth)
+    camera = sc.PinholeCamera(eye=(0.0, 0.0, 0.9), lookat=(0.0, 0.0, -1.0), up=(0.0, 1.0, 0.0), vfov=60.0, width=width, height=height)
+    background = sc.ConstantBackground((0.0, 0.0, 0.0))
+    diffuse = sc.DiffuseMaterial((0.7, 0.7, 0.7))
+    lamb = sc.LambertianInterfaceMaterial(color=(0.8, 0.3, 0.2), ior=1.5)
+    rough = sc.RoughDiffuseMaterial(color=(0.2, 0.6, 0.8), ior=1.4, roughness=(0.3, 0.3), microfacet_model=rough_model,
+                                    normal_distribution=rough_distribution)
+    glass = sc.TransparentMaterial(ior=1.5, glass_absorption=(0.5, 0.2, 0.1))
+    bp, bi = box()
+    ap, ai, an, ani = icosphere(subdiv, 0.28, (-0.48, -0.45, -0.45))
+    rp, ri, rn, rni = icosphere(subdiv, 0.28, (0.08, -0.45, -0.6))
+    gp, gi, gn, gni = icosphere(subdiv, 0.25, (0.45, -0.4, -0.2))
+    meshes = [sc.Mesh(bp, bi, diffuse), sc.Mesh(ap, ai, lamb, an, ani), sc.Mesh(rp, ri, rough, rn, rni), sc.Mesh(gp, gi, glass, gn, gni)]
+    lp, li = quad_light((0.0, 0.99, 0.0), 0.25)
+    lights = [sc.TriangleAreaLight(lp, li, (15.0, 15.0, 15.0))]
+    return sc.SceneData(integrator, camera, background, meshes, lights)
+
+
+def analytic_light_scene(width=64, height=64, subdiv=3, max_depth=8, rr_start_depth=0):
+    """The diffuse box lit by a DiskAreaLight under the ceiling (radius 0.2, facing down: theta 180)
+    and a SphericalLight (radius 0.08) above a GGX conductor sphere and a Lambertian-interface sphere;
+    both lights are seen by camera rays through their analytic geometry (disk_mesh.cu, sphere_mesh.cu)
+    and block shadow rays."""
+    integrator = sc.PathTracer(max_depth=max_depth, scene_epsilon=1e-4, rr_start_depth=rr_start_depth)
+    camera = sc.PinholeCamera(eye=(0.0, 0.0, 0.9), lookat=(0.0, 0.0, -1.0), up=(0.0, 1.0, 0.0), vfov=60.0, width=width, height=height)
+    background = sc.ConstantBackground((0.0, 0.0, 0.0))
+    diffuse = sc.DiffuseMaterial((0.7, 0.7, 0.7))
+    metal = sc.MetallicMaterial(ior=((0.2, 3.9), (0.55, 3.15), (0.9, 2.4)), roughness=(0.15, 0.15), microfacet_model=sc.VISIBLE_NORMALS_MODEL,
+                                normal_distribution=sc.GGX_DISTRIBUTION)
+    lamb = sc.LambertianInterfaceMaterial(color=(0.3, 0.7, 0.3), ior=1.5)
+    bp, bi = box()
+    mp, mi, mn, mni = icosphere(subdiv, 0.28, (-0.4, -0.45, -0.5))
+    ap, ai, an, ani = icosphere(subdiv, 0.25, (0.4, -0.5, -0.3))
+    meshes = [sc.Mesh(bp, bi, diffuse), sc.Mesh(mp, mi, metal, mn, mni), sc.Mesh(ap, ai, lamb, an, ani)]
+    lights = [sc.DiskAreaLight(position=(0.0, 0.95, -0.3), radiance=(6.0, 6.0, 5.5), radius=0.2, theta=180.0, phi=0.0),
+              sc.SphericalLight(position=(0.1, 0.1, -0.6), radiance=(20.0, 14.0, 8.0), radius=0.08)]
+    return sc.SceneData(integrator, camera, background, meshes, lights)
+
+
 def sky_envmap(width=2048, height=1024, sun_dir=(0.35, 0.55, 0.45), sun_peak=5.0e4, sun_sigma_deg=1.0):
     """Procedural equirectangular sky in the reference's mapping (envmap.h: u = (atan2(x, z) + pi) / 2pi,
     v = 1 - acos(y) / pi): a vertical gradient from horizon to zenith, a darker ground, and a Gaussian sun

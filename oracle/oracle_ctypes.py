@@ -263,6 +263,17 @@ class OracleScene:
                 mab[k, 4:7] = m.glass_absorption
             elif name == "AreaLightMaterial":
                 mab[k, :3] = m.radiance
+            elif name == "TransparentMaterial":
+                mab[k, 0] = m.ior
+                mab[k, 4:7] = m.glass_absorption
+            elif name == "LambertianInterfaceMaterial":
+                mab[k, :3] = m.color
+                mab[k, 3] = m.ior
+            elif name == "RoughDiffuseMaterial":
+                mmodel[k], mdist[k] = m.microfacet_model, m.normal_distribution
+                mab[k, :3] = m.color
+                mab[k, 3] = m.ior
+                mab[k, 5:7] = m.roughness
             elif name == "TranslucentMaterial":
                 pass
             elif name == "RoughTranslucentMaterial":

@@ -28,7 +28,8 @@ namespace {
 
 typedef V3<float> F3;
 
-enum { MT_DIFFUSE = 0, MT_GLASS = 3, MT_METAL = 4, MT_TRANSLUCENT = 5, MT_ROUGH_TRANSLUCENT = 6, MT_LIGHT = 100 };
+enum { MT_DIFFUSE = 0, MT_TRANSPARENT = 2, MT_GLASS = 3, MT_METAL = 4, MT_TRANSLUCENT = 5, MT_ROUGH_TRANSLUCENT = 6, MT_LAMBERTIAN_INTERFACE = 7,
+       MT_ROUGH_DIFFUSE = 9, MT_LIGHT = 100 };
 enum { STANDARD_DIPOLE = 0, DIRECTIONAL_DIPOLE = 1 };
 
 struct Mat {
@@ -140,6 +141,9 @@ struct Scene {
   std::vector<Node> nodes;
   std::vector<int> order;
   std::atomic<long> capped{0};
+  // the geometry of the disk and sphere lights (Light.cpp:370-503, 505-610), in light order
+  struct Ana { int kind; F3 pos; float radius; F3 normal; F3 radiance; };
+  std::vector<Ana> ana;
 };
 
 // Moller-Trumbore in the same operation order as the CUDA kernel (pt_scene.cuh tri_mt).
@@ -239,6 +243,74 @@ static inline bool box_hit(const Scene::Node& n, const double* o, const double* 
   return t0 <= t1 * (1.0 + 1e-9) + 1e-12;
 }
 
+// disk_mesh.cu:33-55
+static bool ana_disk_t(const Scene::Ana& A, const F3& o, const F3& d, float eps, float& t)
+{
+  F3 O = o - A.pos;
+  float den = dot(A.normal, d);
+  if (!(std::fabs(den) > eps)) return false;
+  t = -dot(O, A.normal) / den;
+  F3 point = o + t * d;
+  F3 v = point - A.pos;
+  float square_dist = dot(v, v);
+  return square_dist <= A.radius * A.radius;
+}
+// sphere_mesh.cu:44-95: the (refined) near root if rtPotentialIntersection accepts it, else the far root
+static bool ana_sphere_t(const Scene::Ana& A, const F3& o, const F3& d, float tmin, float tmax, float& t)
+{
+  F3 O = o - A.pos;
+  F3 D = d;
+  float radius = A.radius;
+  float b = dot(O, D);
+  float c = dot(O, O) - radius * radius;
+  float disc = b * b - c;
+  if (!(disc > 0.0f)) return false;
+  float sdisc = std::sqrt(disc);
+  float root1 = (-b - sdisc);
+  bool do_refine = false;
+  float root11 = 0.0f;
+  if (std::fabs(root1) > 10.f * radius) do_refine = true;
+  if (do_refine) {
+    F3 O1 = O + root1 * D;
+    b = dot(O1, D);
+    c = dot(O1, O1) - radius * radius;
+    disc = b * b - c;
+    if (disc > 0.0f) {
+      sdisc = std::sqrt(disc);
+      root11 = (-b - sdisc);
+    }
+  }
+  if (root1 + root11 > tmin && root1 + root11 < tmax) {
+    t = root1 + root11;
+    return true;
+  }
+  float root2 = (-b + sdisc) + (do_refine ? root1 : 0);
+  if (root2 > tmin && root2 < tmax) {
+    t = root2;
+    return true;
+  }
+  return false;
+}
+// The analytic emitters after the triangles, in light order; a hit replaces the current one only when
+// strictly closer.  Their hits carry index n_tris + k.
+static void ana_closest(const Scene& S, const F3& o, const F3& d, float tmin, HitRec& h)
+{
+  for (size_t k = 0; k < S.ana.size(); ++k) {
+    const Scene::Ana& A = S.ana[k];
+    float t;
+    bool hit = A.kind == DISK_LIGHT ? (ana_disk_t(A, o, d, S.eps, t) && t > tmin && t < h.t) : ana_sphere_t(A, o, d, tmin, h.t, t);
+    if (hit) h = {t, 0.0f, 0.0f, (int)(S.tris.size() + k)};
+  }
+}
+static bool ana_any(const Scene& S, const F3& o, const F3& d, float tmin, float tmax)
+{
+  for (const Scene::Ana& A : S.ana) {
+    float t;
+    if (A.kind == DISK_LIGHT ? (ana_disk_t(A, o, d, S.eps, t) && t > tmin && t < tmax) : ana_sphere_t(A, o, d, tmin, tmax, t)) return true;
+  }
+  return false;
+}
+
 static HitRec closest(const Scene& S, const F3& o, const F3& d, float tmin, float tmax)
 {
   HitRec h = {tmax, 0.0f, 0.0f, -1};
@@ -262,6 +334,7 @@ static HitRec closest(const Scene& S, const F3& o, const F3& d, float tmin, floa
       stack[sp++] = n.right;
     }
   }
+  if (!S.ana.empty()) ana_closest(S, o, d, tmin, h);
   return h;
 }
 
@@ -285,7 +358,7 @@ static bool occluded(const Scene& S, const F3& o, const F3& d, float tmin, float
       stack[sp++] = n.right;
     }
   }
-  return false;
+  return !S.ana.empty() && ana_any(S, o, d, tmin, tmax);
 }
 
 // Shading normal: normalize(rtTransformNormal(normalize(n))) with the identity transform.
@@ -336,7 +409,7 @@ static inline void tape_const_w(PRD& prd, int slot, const F3& w)
 
 static void trace(Scene& S, const F3& o, const F3& d, PRD& prd, LightSet& ls);
 
-// diffuse_shader.cu:122-187
+// diffuse_shader.cu:42-107
 static void shade_diffuse(Scene& S, const Mat& m, const F3& o, const F3& d, const HitRec& h, PRD& prd, LightSet& ls)
 {
   if (prd.depth > S.max_depth) return;
@@ -418,7 +491,7 @@ static void shade_diffuse(Scene& S, const Mat& m, const F3& o, const F3& d, cons
   prd.result = result;
 }
 
-// metallic_shader.cu:232-348
+// metallic_shader.cu:45-161
 static void shade_metal(Scene& S, const Mat& m, const F3& o, const F3& d, const HitRec& h, PRD& prd, LightSet& ls)
 {
   if (prd.depth >= S.max_depth) { prd.result = v3s(0.0f); return; }
@@ -576,7 +649,247 @@ static void shade_glass(Scene& S, const Mat& m, const F3& o, const F3& d, const 
   prd.result = result * beam_T;
 }
 
-// subsurface_scattering_shader.cu:324-470 (REFLECT, TRANSMIT and RND_64 defined).
+// A child path of `prd` with the given emission flag (the reference's fresh PerRayData_radiance: depth + 1,
+// the parent's tea seed, zero result; its MD5 state follows the parent's).
+static inline PRD child_of(const PRD& prd, int emit_light)
+{
+  PRD child;
+  child.probe_path = prd.probe_path;
+  child.tape = prd.tape;
+  child.depth = prd.depth + 1;
+  child.result = v3s(0.0f);
+  child.seed = prd.seed;
+  child.seed64 = prd.seed64;
+  child.emit_light = emit_light;
+  return child;
+}
+
+// transparent_shader.cu:47-115 (DIFFUSE_PART undefined): smooth glass.  The shader increments the
+// payload's own depth and traces the child with that payload, so the child sees depth + 1 and its
+// random numbers and emission flag flow back into this vertex.
+static void shade_transparent(Scene& S, const Mat& m, const F3& o, const F3& d, const HitRec& h, PRD& prd, LightSet& ls)
+{
+  prd.result = v3s(0.0f);
+  if (prd.depth > S.max_depth) return;
+  ++prd.depth;
+  F3 hit_pos = o + h.t * d;
+  F3 normal = shading_normal(S, h.prim, h.u, h.v);
+  u32& t = prd.seed;
+  const float ior = m.a[0];
+  F3 beam_T = v3s(1.0f);
+  float n1_over_n2 = 1.0f / ior;
+  float cos_theta = dot(-d, normal);
+  if (cos_theta < 0.0f) {
+    beam_T = vexp(-h.t * v3(m.b[0], m.b[1], m.b[2]));
+    float prob = (beam_T.x + beam_T.y + beam_T.z) / 3.0f;
+    if (rnd_tea(t) >= prob) return;
+    beam_T = beam_T / prob;
+    n1_over_n2 = ior;
+    normal = -normal;
+    cos_theta = -cos_theta;
+  }
+  float R = 1.0f;
+  float sin_theta_t_sqr = n1_over_n2 * n1_over_n2 * (1.0f - cos_theta * cos_theta);
+  float cos_theta_t = 0;
+  if (sin_theta_t_sqr < 1.0f) {
+    cos_theta_t = std::sqrt(1.0f - sin_theta_t_sqr);
+    R = fresnel_R(cos_theta, cos_theta_t, n1_over_n2);
+  }
+  float reflect_xi = rnd_tea(t);
+  F3 dir;
+  if (reflect_xi < R) dir = reflect(d, normal);
+  else dir = n1_over_n2 * d + normal * (n1_over_n2 * cos_theta - cos_theta_t);
+  prd.emit_light = 1;
+  tape_const_w(prd, tape_add(prd, TapeRec()), beam_T);
+  trace(S, hit_pos, dir, prd, ls);
+  prd.result = prd.result * beam_T;
+}
+
+// R of the interface for cos_i: the repeated block of lambertian_interface_shader.cu:69-76.
+static inline float interface_R(float cos_i, float n1_over_n2)
+{
+  float R = 1.0f;
+  float sin_t_sqr = n1_over_n2 * n1_over_n2 * (1.0f - cos_i * cos_i);
+  if (sin_t_sqr < 1.0f) R = fresnel_R(cos_i, std::sqrt(1.0f - sin_t_sqr), n1_over_n2);
+  return R;
+}
+
+// lambertian_interface_shader.cu:51-173
+static void shade_lambertian_interface(Scene& S, const Mat& m, const F3& o, const F3& d, const HitRec& h, PRD& prd, LightSet& ls)
+{
+  if (prd.depth > S.max_depth) return;
+  F3 hit_pos = o + h.t * d;
+  F3 normal = shading_normal(S, h.prim, h.u, h.v);
+  F3 ffnormal = faceforward(normal, -d, normal);
+  F3 result = v3s(0.0f);
+  u32& t = prd.seed;
+  const F3 dc = v3(m.a[0], m.a[1], m.a[2]);
+  const float ior = m.a[3];
+  float n1_over_n2 = 1.0f / ior;
+  float r_10 = two_C1(ior);
+  float cos_theta_i = dot(-d, ffnormal);
+  float R_i = interface_R(cos_theta_i, n1_over_n2);
+  float T_01_i = 1.0f - R_i;
+  u32 light_idx = (u32)((float)ls.n_lights * rnd_tea(t));
+  if ((long)light_idx >= ls.n_lights) { light_idx = (u32)(ls.n_lights - 1); ++ls.oob; }
+  float light_pdf = 1.0f / (float)ls.n_lights;
+  F3 w_l = v3s(0.0f), radiance = v3s(0.0f);
+  float dist = 0.0f;
+  eval_direct<float>(hit_pos, ls.lights[light_idx], ls, w_l, radiance, dist, t);
+  radiance = radiance / light_pdf;
+  float cos_theta_l = dot(ffnormal, w_l);
+  if (cos_theta_l > 0.0) {
+    float V = occluded(S, hit_pos, w_l, S.eps, dist) ? 0.0f : 1.0f;
+    F3 Li = V * radiance;
+    float T_01_l = 1.0f - interface_R(cos_theta_l, n1_over_n2);
+    F3 e = Li * K<float>::INV_PI * cos_theta_l * dc * n1_over_n2 * n1_over_n2 * T_01_l * T_01_i / (1.0f - dc * r_10);
+    result = result + e;
+    tape_emit(prd, e);
+    prd.emit_light = 0;
+  }
+  float prob = R_i;
+  float xi = rnd_tea(t);
+  if (xi > prob) {
+    F3 diffuse_dir = sample_cosine_weighted<float>(ffnormal, t);
+    float cos_theta_r = dot(diffuse_dir, ffnormal);
+    float T_01_r = 1.0f - interface_R(cos_theta_r, n1_over_n2);
+    PRD child = child_of(prd, prd.emit_light);
+    const int slot = tape_add(prd, TapeRec());
+    trace(S, hit_pos, diffuse_dir, child, ls);
+    F3 wgt = dc * n1_over_n2 * n1_over_n2 * T_01_r / (1.0f - dc * r_10);
+    tape_const_w(prd, slot, wgt);
+    result = result + child.result * dc * n1_over_n2 * n1_over_n2 * T_01_r / (1.0f - dc * r_10);
+    prd.seed = child.seed;
+  } else {
+    F3 refl_dir = reflect(d, normal);
+    PRD child = child_of(prd, 1);
+    tape_const_w(prd, tape_add(prd, TapeRec()), v3s(1.0f));
+    trace(S, hit_pos, refl_dir, child, ls);
+    result = result + child.result;
+    prd.seed = child.seed;
+  }
+  prd.result = result;
+}
+
+// rough_diffuse_shader.cu:55-292
+static void shade_rough_diffuse(Scene& S, const Mat& m, const F3& o, const F3& d, const HitRec& h, PRD& prd, LightSet& ls)
+{
+  if (prd.depth > S.max_depth) return;
+  F3 hit_pos = o + h.t * d;
+  F3 normal = shading_normal(S, h.prim, h.u, h.v);
+  F3 ffnormal = faceforward(normal, -d, normal);
+  F3 w_i = -d;
+  F3 result = v3s(0.0f);
+  u32& t = prd.seed;
+  const F3 dc = v3(m.a[0], m.a[1], m.a[2]);
+  const float ior = m.a[3];
+  float n1_over_n2 = 1.0f / ior;
+  float r_10 = two_C1(ior);
+  const float a_x = m.b[1], a_y = m.b[2];
+  const int dist = (int)m.dist;
+  int capped = 0;
+  float z1 = rnd_tea(t);
+  float z2 = rnd_tea(t);
+  F3 microfacet_normal = sample_visible_normal<float>(dist, w_i, ffnormal, a_x, a_y, z1, z2, &capped);
+  float cos_theta_i = dot(w_i, microfacet_normal);
+  float R_i = interface_R(cos_theta_i, n1_over_n2);
+  float T_01_i = 1.0f - R_i;
+  // direct illumination (:100-178)
+  u32 light_idx = (u32)((float)ls.n_lights * rnd_tea(t));
+  if ((long)light_idx >= ls.n_lights) { light_idx = (u32)(ls.n_lights - 1); ++ls.oob; }
+  float light_pdf = 1.0f / (float)ls.n_lights;
+  F3 w_l = v3s(0.0f), radiance = v3s(0.0f);
+  float ldist = 0.0f;
+  eval_direct<float>(hit_pos, ls.lights[light_idx], ls, w_l, radiance, ldist, t);
+  radiance = radiance / light_pdf;
+  float cos_theta_l = dot(ffnormal, w_l);
+  if (cos_theta_l > 0.0) {
+    float V = occluded(S, hit_pos, w_l, S.eps, ldist) ? 0.0f : 1.0f;
+    if (V > 0.0f) {
+      F3 Li = V * radiance;
+      F3 e;
+      if (m.model == MULTISCATTERING) {
+        F3 lwi = to_local(w_i, ffnormal), lwl = to_local(w_l, ffnormal);
+        F3 diffuse_brdf = ms_diffuse_eval<float>(dist, lwi, lwl, a_x, a_y, t, dc, 0u, 4096, &capped);
+        e = Li * diffuse_brdf;
+        F3 reflected_brdf = ms_conductor_eval<float>(dist, lwi, lwl, m.eta, m.inv_eta, a_x, a_y, t, 0u, 4096, &capped);
+        e = e + Li * reflected_brdf;
+      } else {
+        F3 refl_normal = normalize(w_i + w_l);
+        float R_refl = interface_R(dot(refl_normal, w_l), n1_over_n2);
+        float T_01_diff = 1.0f - interface_R(dot(microfacet_normal, w_l), n1_over_n2);
+        float G_i_m_refl = masking_G1_aniso<float>(dist, w_i, refl_normal, ffnormal, a_x, a_y);
+        float G_o_m_refl = masking_G1_aniso<float>(dist, w_l, refl_normal, ffnormal, a_x, a_y);
+        float G_o_m_diff = masking_G1_aniso<float>(dist, w_l, microfacet_normal, ffnormal, a_x, a_y);
+        float D_refl = eval_visible_normal<float>(dist, w_i, refl_normal, ffnormal, a_x, a_y);
+        float weight_refl = G_i_m_refl * G_o_m_refl * D_refl / (4.0f * std::fabs(dot(w_i, ffnormal) * dot(w_l, ffnormal)));
+        float weight_diff = G_o_m_diff;
+        e = Li * K<float>::INV_PI * cos_theta_l * dc * n1_over_n2 * n1_over_n2 * T_01_i * T_01_diff / (1.0f - dc * r_10) * weight_diff;
+        e = e + Li * R_refl * weight_refl;
+      }
+      result = result + e;
+      tape_emit(prd, e);
+      prd.emit_light = 0;
+    }
+  }
+  // indirect illumination (:181-289)
+  float prob = R_i;
+  float xi = rnd_tea(t);
+  F3 w_o;
+  if (xi > prob) {
+    if (m.model == MULTISCATTERING) {
+      u32 order = 0;
+      F3 w_m = v3(0.0f, 0.0f, 1.0f), weight;
+      F3 lwo = ms_diffuse_sample<float>(dist, to_local(w_i, ffnormal), w_m, a_x, a_y, t, order, weight, dc);
+      w_o = to_world(lwo, ffnormal);
+      w_m = to_world(w_m, ffnormal);
+      float T_01_r = 1.0f - interface_R(dot(w_o, w_m), n1_over_n2);
+      PRD child = child_of(prd, prd.emit_light);
+      const int slot = tape_add(prd, TapeRec());
+      trace(S, hit_pos, w_o, child, ls);
+      tape_const_w(prd, slot, n1_over_n2 * n1_over_n2 * T_01_r / (1.0f - dc * r_10) * weight);
+      result = result + child.result * n1_over_n2 * n1_over_n2 * T_01_r / (1.0f - dc * r_10) * weight;
+      prd.seed = child.seed;
+    } else {
+      F3 diffuse_dir = sample_cosine_weighted<float>(microfacet_normal, t);
+      float cos_theta_r = dot(diffuse_dir, microfacet_normal);
+      float G_o_m = masking_G1_aniso<float>(dist, diffuse_dir, microfacet_normal, ffnormal, a_x, a_y);
+      if (G_o_m < 0.0f) { prd.result = result; S.capped += capped; return; }
+      float T_01_r = 1.0f - interface_R(cos_theta_r, n1_over_n2);
+      PRD child = child_of(prd, prd.emit_light);
+      const int slot = tape_add(prd, TapeRec());
+      trace(S, hit_pos, diffuse_dir, child, ls);
+      tape_const_w(prd, slot, dc * n1_over_n2 * n1_over_n2 * T_01_r / (1.0f - dc * r_10) * G_o_m);
+      result = result + child.result * dc * n1_over_n2 * n1_over_n2 * T_01_r / (1.0f - dc * r_10) * G_o_m;
+      prd.seed = child.seed;
+    }
+  } else {
+    if (m.model == MULTISCATTERING) {
+      u32 order = 10;
+      F3 w_m, weight;
+      F3 lwo = ms_conductor_sample<float>(dist, to_local(w_i, normal), w_m, m.eta, m.inv_eta, a_x, a_y, t, order, weight, 4096, &capped);
+      w_o = to_world(lwo, normal);
+      PRD child = child_of(prd, prd.emit_light);
+      tape_const_w(prd, tape_add(prd, TapeRec()), v3s(1.0f));
+      trace(S, hit_pos, w_o, child, ls);
+      result = result + child.result;
+      prd.seed = child.seed;
+    } else {
+      F3 refl_dir = reflect(d, microfacet_normal);
+      float G_o_m = masking_G1_aniso<float>(dist, refl_dir, microfacet_normal, ffnormal, a_x, a_y);
+      if (G_o_m < 0.0f) { prd.result = result; S.capped += capped; return; }
+      PRD child = child_of(prd, prd.emit_light);
+      tape_const_w(prd, tape_add(prd, TapeRec()), v3s(G_o_m));
+      trace(S, hit_pos, refl_dir, child, ls);
+      result = result + child.result * G_o_m;
+      prd.seed = child.seed;
+    }
+  }
+  S.capped += capped;
+  prd.result = result;
+}
+
+// subsurface_scattering_shader.cu:55-201 (REFLECT, TRANSMIT and RND_64 defined).
 static void shade_translucent(Scene& S, const Mat& m, const F3& o, const F3& d, const HitRec& h, PRD& prd, LightSet& ls)
 {
   prd.result = v3s(0.0f);
@@ -983,6 +1296,16 @@ static void trace(Scene& S, const F3& o, const F3& d, PRD& prd, LightSet& ls)
     tape_emit(prd, prd.result);
     return;
   }
+  if ((size_t)h.prim >= S.tris.size()) {  // a disk or sphere light: arealight_shader.cu:36-50 on its geometry
+    const Scene::Ana& A = S.ana[h.prim - S.tris.size()];
+    F3 normal = A.kind == DISK_LIGHT ? A.normal : ((o - A.pos) + h.t * d) / A.radius;  // disk_mesh.cu:47, sphere_mesh.cu:78,87
+    normal = normalize(normal);
+    F3 result = v3s(0.0f);
+    if (dot(normal, -d) > 0.0f && prd.emit_light) result = A.radiance;
+    prd.result = result;
+    tape_emit(prd, result);
+    return;
+  }
   const Mat& m = S.mats[S.info[4 * (size_t)h.prim + 3]];
   switch (m.type) {
     case MT_LIGHT: {  // arealight_shader.cu:36-50
@@ -996,6 +1319,9 @@ static void trace(Scene& S, const F3& o, const F3& d, PRD& prd, LightSet& ls)
     case MT_DIFFUSE: shade_diffuse(S, m, o, d, h, prd, ls); return;
     case MT_METAL: shade_metal(S, m, o, d, h, prd, ls); return;
     case MT_GLASS: shade_glass(S, m, o, d, h, prd, ls); return;
+    case MT_TRANSPARENT: shade_transparent(S, m, o, d, h, prd, ls); return;
+    case MT_LAMBERTIAN_INTERFACE: shade_lambertian_interface(S, m, o, d, h, prd, ls); return;
+    case MT_ROUGH_DIFFUSE: shade_rough_diffuse(S, m, o, d, h, prd, ls); return;
     case MT_TRANSLUCENT: shade_translucent(S, m, o, d, h, prd, ls); return;
     case MT_ROUGH_TRANSLUCENT: shade_rough_translucent(S, m, o, d, h, prd, ls); return;
     default: prd.result = v3s(0.0f); return;
@@ -1034,10 +1360,31 @@ EXPORT void* orc_scene_create(const float* tri_pos, const int* tri_info, unsigne
       m.eta = crecip3<float>(ior);       // eta = n1 / ior, metallic_shader.cu:61
       m.inv_eta = crecip3<float>(m.eta);
     }
+    if (m.type == MT_ROUGH_DIFFUSE) {  // MyComplex{ n1_over_n2, 0 } per channel, rough_diffuse_shader.cu:132-133
+      const double e = (double)(1.0f / m.a[3]);
+      m.eta = {{e, 0.0}, {e, 0.0}, {e, 0.0}};
+      m.inv_eta = crecip3<float>(m.eta);
+    }
     S->mats.push_back(m);
   }
   S->lights.lights = (const LightStructRaw*)lights;
   S->lights.n_lights = n_lights;
+  for (unsigned k = 0; k < n_lights; ++k) {
+    const LightStructRaw& l = ((const LightStructRaw*)lights)[k];
+    if (l.light_type != DISK_LIGHT && l.light_type != SPHERICAL_LIGHT) continue;
+    Scene::Ana A;
+    A.kind = (int)l.light_type;
+    A.pos = v3(l.p[0], l.p[1], l.p[2]);
+    A.radius = l.pad[0];  // DiskLightStruct / SphericalLightStruct radius, structs.h:76-93
+    A.normal = v3(0.0f, 1.0f, 0.0f);
+    if (A.kind == DISK_LIGHT) {  // DiskAreaLight::computeNormal, Light.cpp:469-474 (theta = pad[2], phi = pad[1], degrees)
+      float t_rad = l.pad[2] * K<float>::PI / 180.0f;
+      float p_rad = l.pad[1] * K<float>::PI / 180.0f;
+      A.normal = v3(std::sin(t_rad) * std::sin(p_rad), std::cos(t_rad), std::sin(t_rad) * std::cos(p_rad));
+    }
+    A.radiance = v3(l.emitted[0], l.emitted[1], l.emitted[2]);
+    S->ana.push_back(A);
+  }
   S->lights.tris = (const TriangleLightRaw*)tri_lights;
   S->lights.n_tris = n_tri_lights;
   S->eye = v3(cam12[0], cam12[1], cam12[2]);
@@ -1274,6 +1621,7 @@ EXPORT void orc_trace_batch(void* scene, const float* rays8, long n, int brute, 
         if (!tri_mt(o, d, S.tris[k], tt, u, v)) continue;
         if (tt > r[3] && (tt < h.t || (tt == h.t && h.prim >= 0 && (int)k < h.prim))) h = {tt, u, v, (int)k};
       }
+      ana_closest(S, o, d, r[3], h);
     } else {
       h = closest(S, o, d, r[3], r[7]);
     }
@@ -1288,6 +1636,7 @@ EXPORT void orc_trace_batch(void* scene, const float* rays8, long n, int brute, 
           float tt, u, v;
           if (tri_mt(o, d, S.tris[k], tt, u, v) && tt > r[3] && tt < r[7]) a = 1;
         }
+        if (!a && ana_any(S, o, d, r[3], r[7])) a = 1;
         any[i] = a;
       } else {
         any[i] = occluded(S, o, d, r[3], r[7]) ? 1 : 0;

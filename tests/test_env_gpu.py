@@ -77,7 +77,7 @@ def test_env_lit_render_matches_cpu_restatement():
 
 
 def test_diffuse_scene_without_lights_is_rejected():
-    # the diffuse shader indexes light_buffer[0] unguarded (diffuse_shader.cu:135); an empty buffer is refused
+    # the diffuse shader indexes light_buffer[0] unguarded (diffuse_shader.cu:55); an empty buffer is refused
     data = scenes.env_scene(8, 8, env_w=64, env_h=32, env_as_light=False)
     R = sc.Renderer(data)
     assert nat.lib().pt_render_frames(R.ctx, 0, 1) == 6  # PT_NOT_READY
