@@ -46,6 +46,7 @@ std::vector<uint64_t> graph_key(const Context& E, const PassLayout& L)
   std::vector<uint64_t> k;
   k.push_back((uint64_t)L.passes);
   k.push_back(L.sss ? 1 : 0);
+  k.push_back(L.layered ? 1 : 0);
   k.push_back(L.g_slots);
   k.push_back(L.items.size());
   for (size_t i = 0; i < L.chunk_paths.size(); ++i) {
@@ -79,11 +80,7 @@ pt_status plan(pt_batch* b, PassLayout& L, std::vector<SceneDev>& tab, uint64_t&
     if (st != PT_OK) return st;
     PT_CHECK_CUDA(cudaEventRecord(c.ext0, c.stream), "batch order");
     PT_CHECK_CUDA(cudaStreamWaitEvent(E.stream, c.ext0, 0), "batch order");
-    SceneFacts f;
-    f.pixels = c.cam.width * c.cam.height;
-    f.n_trans = (uint32_t)c.trans_objs.size();
-    f.samples = c.probe_samples;
-    f.max_depth = c.integ.max_depth;
+    SceneFacts f = scene_facts(c);
     facts.push_back(f);
     uint32_t nf = frames_override ? (*frames_override)[k] : b->frames[k];
     reqs.push_back(ItemReq{(uint32_t)k, c.next_frame, nf});
@@ -255,11 +252,7 @@ pt_status pt_batch_render_sequential(pt_batch* b)
   PT_CHECK_CUDA(cudaEventRecord(E.ev0, E.stream), "event");
   for (size_t k = 0; k < b->scenes.size(); ++k) {
     Context& c = b->scenes[k]->c;
-    SceneFacts f;
-    f.pixels = c.cam.width * c.cam.height;
-    f.n_trans = (uint32_t)c.trans_objs.size();
-    f.samples = c.probe_samples;
-    f.max_depth = c.integ.max_depth;
+    SceneFacts f = scene_facts(c);
     PassLayout L = plan_pass({f}, {ItemReq{0, c.next_frame, b->frames[k]}}, E.max_paths);
     one[0] = c.view();
     pt_status st = pass_resources(E, L, one);

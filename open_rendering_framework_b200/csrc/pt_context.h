@@ -111,6 +111,7 @@ struct ItemDev {
 struct SceneFacts {
   uint32_t pixels = 1, n_trans = 0, samples = 0;
   int max_depth = 0;
+  bool layered = false;  // has a material of queue class QC_LAYERED
 };
 // A request: frames [first_frame, first_frame + n_frames) of scene `scene`.
 struct ItemReq {
@@ -125,6 +126,7 @@ struct PassLayout {
   uint64_t cap_paths = 0, cap_probes = 0, cap_sets = 0;
   int passes = 0;
   bool sss = false;
+  bool layered = false;  // some scene of the pass has layered materials (k_shade_layered is launched)
   uint32_t g_slots = 0;
 };
 
@@ -212,6 +214,8 @@ struct Context {
 struct Context;
 pt_status prepare_scene(Context& c, const char* who);
 uint64_t scene_path_samples(const Context& c, uint32_t n_frames);
+// What the pass planner needs to know of a scene (its size, translucent objects, layered materials).
+SceneFacts scene_facts(const Context& c);
 PassLayout plan_pass(const std::vector<SceneFacts>& facts, const std::vector<ItemReq>& reqs, uint64_t max_paths);
 pt_status pass_resources(Context& E, const PassLayout& L, const std::vector<SceneDev>& scenes);
 pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool multi, bool allow_events, bool adjoint = false);

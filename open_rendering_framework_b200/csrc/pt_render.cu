@@ -2149,12 +2149,25 @@ uint64_t scene_path_samples(const Context& c, uint32_t n_frames)
   return inside_w * inside_h * n_frames;
 }
 
+SceneFacts scene_facts(const Context& c)
+{
+  SceneFacts f;
+  f.pixels = c.cam.width * c.cam.height;
+  f.n_trans = (uint32_t)c.trans_objs.size();
+  f.samples = c.probe_samples;
+  f.max_depth = c.integ.max_depth;
+  for (const MatDev& m : c.mats)
+    if (m.type == MAT_LAMBERTIAN_INTERFACE || m.type == MAT_ROUGH_DIFFUSE) f.layered = true;
+  return f;
+}
+
 PassLayout plan_pass(const std::vector<SceneFacts>& facts, const std::vector<ItemReq>& reqs, uint64_t max_paths)
 {
   PassLayout L;
   uint32_t max_pixels = 1;
   for (const SceneFacts& f : facts) {
     L.passes = std::max(L.passes, f.max_depth + 2);
+    L.layered = L.layered || f.layered;
     max_pixels = std::max(max_pixels, f.pixels);
     if (f.n_trans) {
       L.sss = true;
@@ -2341,16 +2354,19 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
         k_shade_diffuse<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
         k_shade_metal<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
         k_shade_glass<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
-        k_shade_layered<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
       } else {
         k_shade_miss<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
         k_shade_light<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
         k_shade_diffuse<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
         k_shade_metal<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
         k_shade_glass<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
-        k_shade_layered<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
       }
-      count_launch(7);
+      count_launch(6);
+      if (L.layered) {
+        if (adjoint) k_shade_layered<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
+        else k_shade_layered<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
+        count_launch();
+      }
       if (L.sss) {
         if (adjoint) k_shade_translucent<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
         else k_shade_translucent<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
@@ -2437,11 +2453,7 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
   pt_status st = prepare_scene(c, "pt_render_frames");
   if (st != PT_OK) return st;
   if (n_frames == 0) return PT_OK;
-  SceneFacts f;
-  f.pixels = c.cam.width * c.cam.height;
-  f.n_trans = (uint32_t)c.trans_objs.size();
-  f.samples = c.probe_samples;
-  f.max_depth = c.integ.max_depth;
+  SceneFacts f = scene_facts(c);
   if (c.differentiable) {
     // keep what the adjoint needs: each path's radiance and the value of each of its gathers
     const uint64_t n = (uint64_t)n_frames * f.pixels;
@@ -2488,11 +2500,7 @@ pt_status pt_render_adjoint(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames
   }
   pt_status st = prepare_scene(c, "pt_render_adjoint");
   if (st != PT_OK) return st;
-  SceneFacts f;
-  f.pixels = c.cam.width * c.cam.height;
-  f.n_trans = (uint32_t)c.trans_objs.size();
-  f.samples = c.probe_samples;
-  f.max_depth = c.integ.max_depth;
+  SceneFacts f = scene_facts(c);
   PassLayout L = plan_pass({f}, {ItemReq{0, first_frame, n_frames}}, c.max_paths);
   c.adj_dimg = (const float4*)d_dimage;
   c.adj_dscale = 1.0f / (float)((uint64_t)first_frame + n_frames);
