@@ -24,6 +24,12 @@ the query index, dielectric eta 1.5; per query the sampled visible normal's refl
 Walter BSDF value, the pdf and the Fresnel term.  Unit: M queries/s.  Its CPU baseline is the
 reference's own Microfacet/Fresnel headers compiled for the host (oracle/_ref), on all host cores.
 
+--workload ingest: the scene readers -- one step reads a 2048 x 1024 run-length-encoded .hdr sky into
+the environment map (pt_set_envmap_hdr: host parse, device RGBE expansion, CDF build) and a
+327,680-triangle OBJ icosphere with normals (pt_obj_read + arrays), both written from seeded data.
+Unit: MB/s of file bytes.  Its reference arm times the reference's own HDRLoader and glm readers
+compiled for the host (oracle/_ref/libref_io.so) on the same files.
+
 --workload subsurface: 1024 x 1024 pixels x 256 frames (--spp) of the translucent scene: a
 327,680-triangle jittered icosphere with the dipole BSSRDF (standard; --dipole directional), 4,096
 probes per frame (2^20 over the 256 frames), lit by a 2048 x 1024 procedural sky with a sun lobe of
@@ -72,7 +78,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="single_scene", choices=["single_scene", "subsurface", "batched", "adjoint", "bsdf"])
+    ap.add_argument("--workload", default="single_scene", choices=["single_scene", "subsurface", "batched", "adjoint", "bsdf", "ingest"])
     ap.add_argument("--queries", type=int, default=1 << 22, help="bsdf workload: queries per step")
     ap.add_argument("--scenes", type=int, default=64, help="batched workload: number of scenes")
     ap.add_argument("--spp", type=int, default=None, help="frames per step (default 64, subsurface 256)")
@@ -441,6 +447,119 @@ def run_reference_bsdf(args):
     print(json.dumps(line), flush=True)
 
 
+INGEST = ("scene readers: a 2048x1024 run-length-encoded RGBE sky (.hdr) into the environment map and a 327,680-triangle "
+          "icosphere OBJ with vertex normals (v//n faces), written from seeded data")
+
+
+def ingest_files(directory):
+    """The .hdr and .obj files of the ingest workload (written once per run)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import io_samples
+
+    from open_rendering_framework_b200 import scenes
+
+    hdr = os.path.join(directory, "sky.hdr")
+    sky = scenes.sky_envmap(2048, 1024)
+    with open(hdr, "wb") as f:
+        f.write(io_samples.hdr_bytes(io_samples.rgbe_from_float(sky[::-1, :, :3]), rle=True))
+    pos, idx, nrm, nidx = scenes.icosphere(7, 1.0)
+    obj = os.path.join(directory, "sphere.obj")
+    with open(obj, "w") as f:
+        f.write("".join("v %.7g %.7g %.7g\n" % tuple(p) for p in pos))
+        f.write("".join("vn %.7g %.7g %.7g\n" % tuple(n) for n in nrm))
+        f.write("".join("f %d//%d %d//%d %d//%d\n" % (a + 1, x + 1, b + 1, y + 1, c + 1, z + 1) for (a, b, c), (x, y, z) in zip(idx, nidx)))
+    return hdr, obj
+
+
+def run_ingest(args, world, rank, local):
+    import tempfile
+
+    import torch
+
+    from open_rendering_framework_b200 import _native as nat
+    from open_rendering_framework_b200 import scene as sc
+
+    torch.cuda.set_device(local)
+    with tempfile.TemporaryDirectory() as d:
+        hdr, obj = ingest_files(d)
+        nbytes = os.path.getsize(hdr) + os.path.getsize(obj)
+        R = sc.Renderer(__import__("open_rendering_framework_b200.scenes", fromlist=["x"]).single_scene(width=16, height=16, metal_subdiv=1,
+                                                                                                       glass_subdiv=1), device=local)
+        L = nat.lib()
+
+        def step():
+            nat.call("pt_set_envmap_hdr", R.ctx, hdr.encode())
+            m = ctypes.c_void_p()
+            nat.call("pt_obj_read", obj.encode(), ctypes.byref(m))
+            info = (ctypes.c_uint32 * 5)()
+            nat.call("pt_obj_get_info", m, info)
+            pos = np.empty(3 * info[0], np.float32)
+            nrm = np.empty(3 * info[1], np.float32)
+            vi = np.empty(3 * info[3], np.int32)
+            ni = np.empty(3 * info[3], np.int32)
+            nat.call("pt_obj_get_arrays", m, pos.ctypes.data, nrm.ctypes.data, None, vi.ctypes.data, ni.ctypes.data, None, None)
+            nat.call("pt_obj_free", m)
+
+        for _ in range(max(3, args.warmup)):
+            step()
+        torch.cuda.synchronize()
+        launches0 = L.pt_kernel_launch_count()
+        with ClockSampler(local) as clocks:
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                step()
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+        launches = L.pt_kernel_launch_count() - launches0
+        R.close()
+        value = args.steps * nbytes / dt / 1e6
+        line = {
+            "metric": "MB/s of scene files read (ingest)", "value": value, "unit": "MB/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8/f32", "data": "synthetic",
+            "config": {"workload": INGEST, "bytes_per_step": nbytes},
+            "e2e": {"value": value, "unit": "MB/s", "h2d_bytes_per_step": 2048 * 1024 * 4, "d2h_bytes_per_step": 0,
+                    "what": "file bytes read from the page cache through the C ABI, device decode and CDF build included"},
+            "gpu_launches": int(launches), "clocks": clocks.summary(),
+        }
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = ingest_reference(hdr, obj, nbytes, 3)
+        print(json.dumps(line), flush=True)
+
+
+def ingest_reference(hdr, obj, nbytes, reps):
+    """The reference's HDRLoader (loadHDRTexture) and glmReadOBJ compiled for the host, on the same files."""
+    lib = os.path.join(ROOT, "oracle", "_ref", "libref_io.so")
+    if not os.path.exists(lib):
+        return {"value": None, "unit": "MB/s", "cores": 1, "kind": "reference", "sample": "oracle/_ref/libref_io.so not built"}
+    L = ctypes.CDLL(lib)
+    w, h = ctypes.c_uint(), ctypes.c_uint()
+    buf = np.empty(4 * 2048 * 1024, np.float32)
+    counts = (ctypes.c_uint * 5)()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        L.ref_hdr_load(hdr.encode(), buf.ctypes.data_as(ctypes.c_void_p), ctypes.c_ulong(buf.size), ctypes.byref(w), ctypes.byref(h))
+        L.ref_obj_load(obj.encode(), counts, *([None] * 8), 0)
+    dt = time.perf_counter() - t0
+    return {"value": reps * nbytes / dt / 1e6, "unit": "MB/s", "cores": 1, "kind": "reference",
+            "sample": "%d reads of both files by HDRLoader.cpp + glm.cpp compiled for the host (one thread, as in the reference)" % reps}
+
+
+def run_reference_ingest(args):
+    import tempfile
+
+    with tempfile.TemporaryDirectory() as d:
+        hdr, obj = ingest_files(d)
+        nbytes = os.path.getsize(hdr) + os.path.getsize(obj)
+        ingest_reference(hdr, obj, nbytes, 1)
+        s = ingest_reference(hdr, obj, nbytes, max(1, args.steps))
+    line = {"impl": "reference", "metric": "MB/s of scene files read (ingest)", "value": s["value"], "unit": "MB/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": nbytes / (s["value"] or 1) / 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8/f32", "data": "synthetic", "config": {"workload": INGEST},
+            "cpu_baseline": s, "e2e": {"value": s["value"], "unit": "MB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def profile_figure(name, key):
     """A figure written as `key value` in a committed ncu summary under profiles/."""
     path = os.path.join(ROOT, "profiles", name)
@@ -464,6 +583,8 @@ def run_reference(args, world, rank):
         return run_reference_batched(args)
     if args.workload == "bsdf":
         return run_reference_bsdf(args)
+    if args.workload == "ingest":
+        return run_reference_ingest(args)
     data, _, desc = workload(args)
     from oracle import oracle_ctypes as oc
 
@@ -848,6 +969,9 @@ def main():
             run_batched(args, world, rank, local)
         elif args.workload == "bsdf":
             run_bsdf(args, world, rank, local)
+        elif args.workload == "ingest":
+            if rank == 0:
+                run_ingest(args, world, rank, local)
         elif args.workload == "adjoint":
             if rank == 0:
                 run_adjoint(args, world, rank, local)

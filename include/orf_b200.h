@@ -226,6 +226,17 @@ pt_status pt_set_background_constant(pt_ctx* ctx, const float color[3]);
  * Envmap.h:66-98) makes the diffuse shader's next-event estimation sample it; misses after such an
  * estimate then add nothing, as emitter hits do. */
 pt_status pt_set_envmap(pt_ctx* ctx, const float* rgba, uint32_t width, uint32_t height);
+/* EnvMapBackground from a Radiance RGBE file (the loadTexture / loadHDRTexture path of
+ * Background.cpp:57-69, HDRLoader.cpp:225-290): the header and run-length-encoded scanlines are read
+ * on the host, the 4-byte RGBE texels are uploaded and expanded to float4 on the device (row 0 = the
+ * file's last scanline, as loadHDRTexture flips it; alpha 1), then the tables are built as by
+ * pt_set_envmap.  A file the reader rejects returns PT_INVALID_ARG and leaves the background as it was
+ * (the reference prints the error and installs a 1x1 texture of its default color instead). */
+pt_status pt_set_envmap_hdr(pt_ctx* ctx, const char* path);
+/* The same file decoded on the host into float4 texels in the same orientation (HDRLoader.cpp:36-190
+ * with the flip of :274-284).  With rgba NULL only the size is returned; otherwise rgba holds
+ * capacity_floats >= 4 * width * height floats.  Needs no device. */
+pt_status pt_hdr_read(const char* path, float* rgba, uint64_t capacity_floats, uint32_t* width, uint32_t* height);
 /* Copy the environment tables to host memory (any pointer may be NULL). */
 pt_status pt_get_envmap_tables(pt_ctx* ctx, float* marginal_pdf, float* marginal_cdf, float* conditional_pdf, float* conditional_cdf);
 /* Environment queries (parity checks): env_lookup of n_dirs directions (3 floats each) into d_looked,
@@ -320,6 +331,10 @@ pt_status pt_set_max_paths_in_flight(pt_ctx* ctx, uint64_t max_paths);
 /* Frame the next batch render of this scene starts at (advanced by pt_render_frames and by batch
  * renders; reset to 0 by pt_set_camera). */
 pt_status pt_get_next_frame(pt_ctx* ctx, uint32_t* next_frame);
+/* Restores a saved frame (OptixScene::loadBuffer, OptixScene.cpp:253-298): the float4 accumulation
+ * buffer (width * height, as pt_readback returns it) and the number of frames it holds, which becomes
+ * the next frame, so that pt_render_frames(ctx, next_frame, n) continues the running mean exactly. */
+pt_status pt_set_accumulation(pt_ctx* ctx, const float* host_rgba, uint32_t next_frame);
 
 /* ---------------------------------------------------------------- batches of scenes
  * No counterpart in the reference (one OptiX launch per scene).  A batch renders several scenes
@@ -358,11 +373,44 @@ pt_status pt_batch_get_stats(pt_batch* batch, pt_render_stats* out);
  * fastest.  The trials render from frame 0, so every scene's accumulation restarts at frame 0. */
 pt_status pt_batch_autotune(pt_batch* batch, uint32_t frames_per_trial, pt_tune_result* out);
 
+/* ---------------------------------------------------------------- OBJ models (scene ingestion)
+ * A Wavefront OBJ file read with the semantics of the reference's glm reader as ObjLoader flattens it
+ * (glmReadOBJ, glm.cpp:567-1005 and :1603-1690; ObjLoader::loadVertexData, ObjLoader.cpp:193-260):
+ * v / vn / vt records; faces in the forms v, v/t, v//n and v/t/n, polygons fan-triangulated
+ * (v0, v[k-1], v[k]); groups named "<g name>_MAT_<usemtl name>" ("No Group" / "No Material" before
+ * the first g / usemtl), listed newest first with empty groups dropped, and each group's triangles in
+ * file order.  Indices are 0-based; a corner without a normal or texcoord has index -1.  Negative
+ * (relative) indices count back from the last record of their kind read so far (glm resolves only
+ * vertex indices this way).  A mtllib's newmtl / Kd pairs give each group's diffuse color when its
+ * material is defined there.  Needs no device; feed the arrays to pt_mesh_add, one call per group or
+ * one for all with one material. */
+typedef struct pt_obj pt_obj;
+typedef struct pt_obj_info {
+  uint32_t n_vertices, n_normals, n_texcoords, n_triangles, n_groups;
+} pt_obj_info;
+typedef struct pt_obj_group {
+  char name[128];       /* "<g>_MAT_<material>" */
+  char material[128];   /* the usemtl name */
+  uint32_t first_triangle, n_triangles;
+  float diffuse[3];     /* Kd of the material, 0.7 (glm's default) when the library does not define it */
+  int32_t has_diffuse;  /* 1 if the material library defines Kd for it */
+} pt_obj_group;
+pt_status pt_obj_read(const char* path, pt_obj** out);
+pt_status pt_obj_get_info(const pt_obj* obj, pt_obj_info* info);
+/* Any pointer may be NULL.  Sizes: positions / normals 3 floats per record, texcoords 2, the three index
+ * arrays 3 int32 per triangle, group_of_triangle 1 per triangle. */
+pt_status pt_obj_get_arrays(const pt_obj* obj, float* positions, float* normals, float* texcoords, int32_t* vindex, int32_t* nindex,
+                            int32_t* tindex, uint32_t* group_of_triangle);
+pt_status pt_obj_get_group(const pt_obj* obj, uint32_t group, pt_obj_group* out);
+pt_status pt_obj_free(pt_obj* obj);
+
 /* ---------------------------------------------------------------- ray queries (BVH parity)
  * Closest-hit / any-hit queries against the built scene for n rays given as d_orig_tmin
  * (float4: origin.xyz, tmin) and d_dir_tmax (float4: direction.xyz, tmax).  Closest hit writes the
  * original triangle index (-1 for a miss), t and the barycentrics (beta, gamma) of the hit; ties in t
- * go to the lower triangle index.  Any hit writes 1 if some triangle has tmin < t < tmax, else 0. */
+ * go to the lower triangle index.  Any hit writes 1 if some triangle has tmin < t < tmax, else 0.
+ * The disk and sphere lights' geometry counts too: its hits carry index n_triangles + k for the k-th
+ * such light in light_buffer order (barycentrics 0), after the triangles in tie order. */
 pt_status pt_trace_closest(pt_ctx* ctx, const float* d_orig_tmin, const float* d_dir_tmax, uint32_t n, int32_t* d_prim,
                            float* d_t, float* d_bary);
 pt_status pt_trace_any(pt_ctx* ctx, const float* d_orig_tmin, const float* d_dir_tmax, uint32_t n, int32_t* d_hit);

@@ -58,6 +58,14 @@ SIGNATURES = {
     "pt_set_camera": (I32, [P, P, P, P, P, U32, U32, P, P]),
     "pt_set_background_constant": (I32, [P, P]),
     "pt_set_envmap": (I32, [P, P, U32, U32]),
+    "pt_set_envmap_hdr": (I32, [P, ctypes.c_char_p]),
+    "pt_hdr_read": (I32, [ctypes.c_char_p, P, U64, P, P]),
+    "pt_obj_read": (I32, [ctypes.c_char_p, P]),
+    "pt_obj_get_info": (I32, [P, P]),
+    "pt_obj_get_arrays": (I32, [P, P, P, P, P, P, P, P]),
+    "pt_obj_get_group": (I32, [P, U32, P]),
+    "pt_obj_free": (I32, [P]),
+    "pt_set_accumulation": (I32, [P, P, U32]),
     "pt_get_envmap_tables": (I32, [P, P, P, P, P]),
     "pt_env_query": (I32, [P, P, U32, P, P, U32, P, P]),
     "pt_material_create": (I32, [P, U32, P, SZ, P]),

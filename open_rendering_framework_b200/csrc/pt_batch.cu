@@ -1,3 +1,4 @@
+#include <cmath>
 // Batched rendering: several scenes (built contexts) rendered by one wavefront pass.  No counterpart
 // in the reference, which renders one scene per OptiX launch (OptixScene::renderScene,
 // OptixScene.cpp:139-168); every scene of a batch still follows that launch's semantics (its probe
@@ -334,6 +335,21 @@ pt_status pt_get_next_frame(pt_ctx* ctx, uint32_t* out)
 {
   if (!ctx || !out) return fail(PT_INVALID_ARG, "pt_get_next_frame: null argument");
   *out = ctx->c.next_frame;
+  return PT_OK;
+}
+
+pt_status pt_set_accumulation(pt_ctx* ctx, const float* host_rgba, uint32_t next_frame)
+{
+  if (!ctx || !host_rgba) return fail(PT_INVALID_ARG, "pt_set_accumulation: null argument");
+  Context& c = ctx->c;
+  if (!c.camera_set) return fail(PT_NOT_READY, "pt_set_accumulation: camera not set");
+  const size_t n = (size_t)c.cam.width * c.cam.height * 4;
+  for (size_t k = 0; k < n; ++k)
+    if (!std::isfinite(host_rgba[k])) return fail(PT_INVALID_ARG, "pt_set_accumulation: non-finite value");
+  PT_CHECK_CUDA(cudaSetDevice(c.device), "cudaSetDevice");
+  PT_CHECK_CUDA(cudaMemcpyAsync(c.d_accum.p, host_rgba, n * sizeof(float), cudaMemcpyHostToDevice, c.stream), "pt_set_accumulation");
+  PT_CHECK_CUDA(cudaStreamSynchronize(c.stream), "pt_set_accumulation");
+  c.next_frame = next_frame;
   return PT_OK;
 }
 

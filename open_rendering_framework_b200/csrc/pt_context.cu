@@ -489,6 +489,20 @@ pt_status pt_set_envmap(pt_ctx* ctx, const float* rgba, uint32_t width, uint32_t
   for (uint64_t k = 0; k < 4ull * width * height; ++k)
     if (!std::isfinite(rgba[k]) || rgba[k] < 0.0f) return fail(PT_INVALID_ARG, "pt_set_envmap: texels must be finite and >= 0");
   size_t n = (size_t)width * height;
+  pt_status st = env_reserve(c, width, height);
+  if (st != PT_OK) return st;
+  PT_CHECK_CUDA(cudaMemcpyAsync(c.d_env_tex.p, rgba, n * sizeof(float4), cudaMemcpyHostToDevice, c.stream), "env upload");
+  if ((st = env_build_tables(c, width, height)) != PT_OK) return st;
+  PT_CHECK_CUDA(cudaStreamSynchronize(c.stream), "pt_set_envmap");
+  return PT_OK;
+}
+
+}  // extern "C"
+
+namespace pt {
+pt_status env_reserve(Context& c, uint32_t width, uint32_t height)
+{
+  size_t n = (size_t)width * height;
   pt_status st = c.d_env_tex.reserve(n * sizeof(float4), "env texture");
   if (st == PT_OK) st = c.d_env_lum.reserve(n * 4, "env luminance");
   if (st == PT_OK) st = c.d_env_cpdf.reserve(n * 4, "env conditional pdf");
@@ -496,8 +510,12 @@ pt_status pt_set_envmap(pt_ctx* ctx, const float* rgba, uint32_t width, uint32_t
   if (st == PT_OK) st = c.d_env_mf.reserve((size_t)height * 4, "env marginal");
   if (st == PT_OK) st = c.d_env_mpdf.reserve((size_t)height * 4, "env marginal pdf");
   if (st == PT_OK) st = c.d_env_mcdf.reserve((size_t)height * 4, "env marginal cdf");
-  if (st != PT_OK) return st;
-  PT_CHECK_CUDA(cudaMemcpyAsync(c.d_env_tex.p, rgba, n * sizeof(float4), cudaMemcpyHostToDevice, c.stream), "env upload");
+  return st;
+}
+
+pt_status env_build_tables(Context& c, uint32_t width, uint32_t height)
+{
+  size_t n = (size_t)width * height;
   c.env_w = (int)width;
   c.env_h = (int)height;
   c.env_present = true;
@@ -507,10 +525,12 @@ pt_status pt_set_envmap(pt_ctx* ctx, const float* rgba, uint32_t width, uint32_t
                                                          c.d_env_ccdf.as<float>());
   k_env_marginal<<<1, 32, 0, c.stream>>>(E, c.d_env_mf.as<float>(), c.d_env_mpdf.as<float>(), c.d_env_mcdf.as<float>(), c.d_env_ccdf.as<float>());
   count_launch(3);
-  PT_CHECK_CUDA(cudaGetLastError(), "pt_set_envmap launch");
-  PT_CHECK_CUDA(cudaStreamSynchronize(c.stream), "pt_set_envmap");
+  PT_CHECK_CUDA(cudaGetLastError(), "environment CDF build");
   return PT_OK;
 }
+}  // namespace pt
+
+extern "C" {
 
 pt_status pt_get_envmap_tables(pt_ctx* ctx, float* marginal_pdf, float* marginal_cdf, float* conditional_pdf, float* conditional_cdf)
 {

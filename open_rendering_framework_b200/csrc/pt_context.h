@@ -214,6 +214,10 @@ struct Context {
 struct Context;
 pt_status prepare_scene(Context& c, const char* who);
 uint64_t scene_path_samples(const Context& c, uint32_t n_frames);
+// Environment map: device buffers for a width x height texture and its tables, and the CDF build over
+// the texels in d_env_tex (env_cameras.cu:23-75), queued on the context's stream.
+pt_status env_reserve(Context& c, uint32_t width, uint32_t height);
+pt_status env_build_tables(Context& c, uint32_t width, uint32_t height);
 // What the pass planner needs to know of a scene (its size, translucent objects, layered materials).
 SceneFacts scene_facts(const Context& c);
 PassLayout plan_pass(const std::vector<SceneFacts>& facts, const std::vector<ItemReq>& reqs, uint64_t max_paths);

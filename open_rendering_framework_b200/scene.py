@@ -11,6 +11,7 @@ every value before any device work.
 """
 import ctypes
 import math
+import os
 
 import numpy as np
 
@@ -191,10 +192,25 @@ class ConstantBackground:
         self.background_color = tuple(c)
 
 
-class EnvMapBackground:
-    """EnvMapBackground (Background.cpp:57-69): float4 texels [H, W, 4], row 0 at v = 0."""
+def read_hdr(path):
+    """A Radiance RGBE file decoded on the host (pt_hdr_read): float4 texels [H, W, 4], row 0 = the file's
+    last scanline, as loadHDRTexture orients it (HDRLoader.cpp:225-290)."""
+    w, h = ctypes.c_uint32(), ctypes.c_uint32()
+    nat.call("pt_hdr_read", os.fsencode(path), None, 0, ctypes.byref(w), ctypes.byref(h))
+    out = np.empty((h.value, w.value, 4), np.float32)
+    nat.call("pt_hdr_read", os.fsencode(path), out.ctypes.data, out.size, ctypes.byref(w), ctypes.byref(h))
+    return out
 
-    def __init__(self, rgba):
+
+class EnvMapBackground:
+    """EnvMapBackground (Background.cpp:57-69): float4 texels [H, W, 4], row 0 at v = 0, or a Radiance
+    .hdr file given by `path` (the reference's loadTexture path), which the renderer uploads as RGBE and
+    expands on the device (pt_set_envmap_hdr); `rgba` then holds the same texels decoded on the host."""
+
+    def __init__(self, rgba=None, path=None):
+        self.path = None if path is None else os.fspath(path)
+        if self.path is not None:
+            rgba = read_hdr(self.path)
         self.rgba = np.ascontiguousarray(rgba, np.float32)
         assert self.rgba.ndim == 3 and self.rgba.shape[2] == 4
 
@@ -551,6 +567,41 @@ class Mesh:
         self.material = material
 
 
+class ObjGroup(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 128), ("material", ctypes.c_char * 128), ("first_triangle", ctypes.c_uint32),
+                ("n_triangles", ctypes.c_uint32), ("diffuse", ctypes.c_float * 3), ("has_diffuse", ctypes.c_int32)]
+
+
+def load_obj(path, material=None, materials=None):
+    """The groups of a Wavefront OBJ file (pt_obj_read: glm's reader as ObjLoader flattens it) as Meshes:
+    one per non-empty group, sharing the file's vertex and normal arrays.  A group's material is
+    materials[<usemtl name>] if given, else `material`, else a DiffuseMaterial of the group's Kd."""
+    obj = ctypes.c_void_p()
+    nat.call("pt_obj_read", os.fsencode(path), ctypes.byref(obj))
+    try:
+        info = (ctypes.c_uint32 * 5)()
+        nat.call("pt_obj_get_info", obj, info)
+        nv, nn, nt, ntri, ng = list(info)
+        pos = np.zeros((nv, 3), np.float32)
+        nrm = np.zeros((max(nn, 1), 3), np.float32)
+        vidx = np.zeros((ntri, 3), np.int32)
+        nidx = np.zeros((ntri, 3), np.int32)
+        nat.call("pt_obj_get_arrays", obj, pos.ctypes.data, nrm.ctypes.data if nn else None, None, vidx.ctypes.data, nidx.ctypes.data,
+                 None, None)
+        meshes = []
+        for k in range(ng):
+            g = ObjGroup()
+            nat.call("pt_obj_get_group", obj, k, ctypes.byref(g))
+            name = g.material.decode()
+            mat = (materials or {}).get(name) or material or DiffuseMaterial(tuple(g.diffuse))
+            tri = slice(g.first_triangle, g.first_triangle + g.n_triangles)
+            ni = nidx[tri]
+            meshes.append(Mesh(pos, vidx[tri], mat, nrm if nn and np.all(ni >= 0) else None, ni if nn and np.all(ni >= 0) else None))
+        return meshes
+    finally:
+        nat.call("pt_obj_free", obj)
+
+
 # ---------------------------------------------------------------- scene flattening
 class SceneData:
     """Everything a render needs, flattened in one fixed order that the GPU context and the CPU
@@ -666,7 +717,9 @@ class Renderer:
         self.frame = 0
 
     def apply_background(self):
-        if isinstance(self.background, EnvMapBackground):
+        if isinstance(self.background, EnvMapBackground) and self.background.path is not None:
+            nat.call("pt_set_envmap_hdr", self.ctx, os.fsencode(self.background.path))
+        elif isinstance(self.background, EnvMapBackground):
             e = self.background.rgba
             nat.call("pt_set_envmap", self.ctx, e.ctypes.data, e.shape[1], e.shape[0])
         else:
