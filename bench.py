@@ -639,7 +639,7 @@ def run_batched(args, world, rank, local):
     B = sc.Batch(Rs, spp, device=local)
     stream = torch.cuda.ExternalStream(B.stream())
     path_samples = sum(d.camera.width * d.camera.height * p for d, p, _ in S)
-    tune = B.autotune(frames_per_trial=1)
+    tune = B.autotune(frames_per_trial=4)
 
     def barrier():
         if world > 1:

@@ -45,7 +45,8 @@ struct DevBuf {
 // Wavefront buffers, sized for `cap` paths in flight.
 struct Wavefront {
   uint64_t cap = 0;
-  DevBuf ray_o, ray_d, thr, rad, rng, hit;   // per path
+  DevBuf state;                               // per path, one 64-byte record: ray origin, ray direction, throughput, rng
+  DevBuf rad, hit;                            // per path
   DevBuf path_item;                           // per path: its item of the pass (uint16)
   DevBuf adj_a, adj_b;                        // adjoint renders: per path image gradient and pending gradient
   DevBuf q_a, q_b;                            // active queues (path ids)

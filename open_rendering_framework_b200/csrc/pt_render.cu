@@ -49,12 +49,21 @@ constexpr uint32_t META_PROBE = 1u << 18;  // a probe's indirect path (sample_ca
 constexpr int META_GSHIFT = 24;            // pending dipole gathers on the path's stack (8 bits)
 constexpr uint32_t META_KEEP = ~(META_DEPTH | META_EMIT);
 
+// One 16-byte field of the per-path state records: field k of path i sits at rec[4 i + k], so the four
+// fields of a path (ray origin, ray direction, throughput, rng state) share one 64-byte record.  A shading
+// kernel reading and rewriting a path at a random id touches two whole 32-byte sectors instead of four
+// half sectors of four arrays, and the extend kernel reads the ray from a single sector.
+template <class T> struct Field4 {
+  T* p;
+  __device__ __forceinline__ T& operator[](uint64_t i) const { return p[4 * i]; }
+};
+
 struct WfDev {
-  float4* ray_o;
-  float4* ray_d;
-  float4* thr;
+  Field4<float4> ray_o;
+  Field4<float4> ray_d;
+  Field4<float4> thr;
   float4* rad;
-  uint4* rng;
+  Field4<uint4> rng;
   float4* hit;
   uint32_t* q_in;
   uint32_t* q_out;
@@ -2022,11 +2031,8 @@ static pt_status ensure_wavefront(Context& c, uint64_t cap)
   if (wf.cap >= cap && wf.counters.p) return PT_OK;
   pt_status st = PT_OK;
   const size_t f4 = sizeof(float4), u4 = sizeof(uint4);
-  if (st == PT_OK) st = wf.ray_o.reserve(cap * f4, "wavefront ray origins");
-  if (st == PT_OK) st = wf.ray_d.reserve(cap * f4, "wavefront ray directions");
-  if (st == PT_OK) st = wf.thr.reserve(cap * f4, "wavefront throughput");
+  if (st == PT_OK) st = wf.state.reserve(cap * (3 * f4 + u4), "wavefront path records");
   if (st == PT_OK) st = wf.rad.reserve(cap * f4, "wavefront radiance");
-  if (st == PT_OK) st = wf.rng.reserve(cap * u4, "wavefront rng");
   if (st == PT_OK) st = wf.hit.reserve(cap * f4, "wavefront hits");
   if (st == PT_OK) st = wf.path_item.reserve(cap * 2, "wavefront path items");
   if (st == PT_OK) st = wf.q_a.reserve(cap * 4, "queue");
@@ -2250,11 +2256,12 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
   Context& c = E;
   WfDev w;
   Wavefront& wf = c.wf;
-  w.ray_o = wf.ray_o.as<float4>();
-  w.ray_d = wf.ray_d.as<float4>();
-  w.thr = wf.thr.as<float4>();
+  float4* rec = wf.state.as<float4>();
+  w.ray_o = Field4<float4>{rec};
+  w.ray_d = Field4<float4>{rec + 1};
+  w.thr = Field4<float4>{rec + 2};
   w.rad = wf.rad.as<float4>();
-  w.rng = wf.rng.as<uint4>();
+  w.rng = Field4<uint4>{reinterpret_cast<uint4*>(rec + 3)};
   w.hit = wf.hit.as<float4>();
   w.q_mat = wf.q_mat.as<uint32_t>();
   w.sh_o = wf.sh_o.as<float4>();
