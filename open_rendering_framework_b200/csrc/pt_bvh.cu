@@ -57,16 +57,17 @@ struct TmpNode {
 };
 
 constexpr int kBins = 32;
-constexpr int kMaxLeaf = 8;
 constexpr int kForcedMaxLeaf = 15;
 constexpr int kMedianDepth = 48;
-constexpr float kTravCost = 1.2f;
 
 struct Builder {
   const std::vector<TriRef>& refs;
   std::vector<uint32_t>& idx;
   std::atomic<int> max_depth{0};
-  Builder(const std::vector<TriRef>& r, std::vector<uint32_t>& i) : refs(r), idx(i) {}
+  const int kMaxLeaf;      // largest leaf the SAH may choose
+  const float kTravCost;   // SAH cost of a node step relative to one triangle test
+  Builder(const std::vector<TriRef>& r, std::vector<uint32_t>& i, const BvhParams& p)
+      : refs(r), idx(i), kMaxLeaf(p.max_leaf), kTravCost(p.trav_cost) {}
 
   Box bounds(uint32_t b, uint32_t e, Box* cbox) const
   {
@@ -218,7 +219,7 @@ void flatten(const TmpNode* n, int parent, std::vector<float4>& out, int& index_
 
 }  // namespace
 
-bool build_bvh(const float* tri_pos, uint32_t n_tris, BvhHost& out)
+bool build_bvh(const float* tri_pos, uint32_t n_tris, BvhHost& out, const BvhParams& params)
 {
   out = BvhHost();
   if (n_tris >= (1u << 27)) return false;
@@ -233,7 +234,7 @@ bool build_bvh(const float* tri_pos, uint32_t n_tris, BvhHost& out)
   }
   std::vector<uint32_t> idx(n_tris);
   for (uint32_t i = 0; i < n_tris; ++i) idx[i] = i;
-  Builder B(refs, idx);
+  Builder B(refs, idx, params);
   // Root: an internal node whose two children split the triangles; with fewer than two triangles
   // the second child is an empty leaf.
   TmpNode root;

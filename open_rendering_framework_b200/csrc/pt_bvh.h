@@ -14,9 +14,16 @@ struct BvhHost {
   int depth = 0;                             // levels including the leaves
 };
 
+// Binned-SAH parameters: the cost of a node step relative to one triangle test, and the largest leaf
+// the SAH may choose (1..15; a leaf is forced only where no split separates the centroids).
+struct BvhParams {
+  float trav_cost = 1.2f;
+  int max_leaf = 8;
+};
+
 // tri_pos: 9 floats per triangle (v0, v1, v2).  Returns false if the scene is too large for the
 // node encoding (2^27 triangles) or the tree is deeper than the traversal trail allows.
-bool build_bvh(const float* tri_pos, uint32_t n_tris, BvhHost& out);
+bool build_bvh(const float* tri_pos, uint32_t n_tris, BvhHost& out, const BvhParams& params = BvhParams());
 
 // The BVH2 collapsed into a 4-wide BVH over the same leaves (8 float4 = 128 bytes per node, root =
 // node 0; layout in pt_scene.cuh).  Returns false (and leaves nodes4 empty) when the 4-wide tree

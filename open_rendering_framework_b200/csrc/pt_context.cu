@@ -696,7 +696,7 @@ pt_status pt_build(pt_ctx* ctx)
   Context& c = ctx->c;
   if (c.n_tris == 0) return fail(PT_NOT_READY, "pt_build: no meshes");
   BvhHost bvh;
-  if (!build_bvh(c.tri_pos.data(), c.n_tris, bvh)) return fail(PT_CAP_EXCEEDED, "pt_build: scene too large or BVH too deep");
+  if (!build_bvh(c.tri_pos.data(), c.n_tris, bvh, c.bvh_params)) return fail(PT_CAP_EXCEEDED, "pt_build: scene too large or BVH too deep");
   c.bvh_depth = bvh.depth;
   std::vector<float4> nodes4;
   int depth4 = 0;
@@ -871,6 +871,16 @@ pt_status pt_set_option(pt_ctx* ctx, const char* name, int64_t value)
     if (value != 0 && value != 1) return fail(PT_INVALID_ARG, "pt_set_option: differentiable must be 0 or 1");
     ctx->c.differentiable = value != 0;
     ctx->c.adj_valid = false;
+    return PT_OK;
+  }
+  if (k == "bvh_trav_cost_milli") {  // SAH node-step cost x 1000 (default 1200), for the next pt_build
+    if (value < 100 || value > 20000) return fail(PT_INVALID_ARG, "pt_set_option: bvh_trav_cost_milli must be in [100, 20000]");
+    ctx->c.bvh_params.trav_cost = (float)value / 1000.0f;
+    return PT_OK;
+  }
+  if (k == "bvh_max_leaf") {  // largest SAH leaf (default 8), for the next pt_build
+    if (value < 1 || value > 15) return fail(PT_INVALID_ARG, "pt_set_option: bvh_max_leaf must be in [1, 15]");
+    ctx->c.bvh_params.max_leaf = (int)value;
     return PT_OK;
   }
   if (k == "bvh4") {

@@ -6,6 +6,7 @@
 #include <memory>
 #include <vector>
 
+#include "pt_bvh.h"
 #include "pt_common.cuh"
 #include "pt_scene.cuh"
 
@@ -171,6 +172,7 @@ struct Context {
   DevBuf d_nodes, d_nodes4, d_v0, d_e1, d_e2, d_info, d_normals, d_mats, d_lights, d_tri_lights;
   std::vector<float4> ana;  // analytic emitters of the disk and sphere lights (3 float4 each)
   DevBuf d_ana;
+  BvhParams bvh_params;    // options "bvh_trav_cost_milli" and "bvh_max_leaf", applied by pt_build
   bool has_bvh4 = false;
   bool use_bvh4 = true;  // option "bvh4": the persistent traversal kernels walk the 4-wide BVH
   DevBuf d_scat, d_trans_objs, d_trans_pos;

@@ -38,7 +38,7 @@ constexpr int kBlock = 128;
 constexpr int kWarps = kBlock / 32;
 // Resident blocks per SM the persistent traversal kernels are compiled for (register budget).
 #ifndef PT_TRACE_MIN_BLOCKS
-#define PT_TRACE_MIN_BLOCKS 1
+#define PT_TRACE_MIN_BLOCKS 8
 #endif
 
 // Per-path metadata in rng.w
@@ -580,6 +580,7 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_extend_persiste
   float3 o = f3s(0.0f), d = f3s(0.0f);
   RayPre rp;
   rp.inv = f3s(0.0f);
+  rp.sx = rp.sy = rp.sz = 0;
   Hit h;
   h.t = 0.0f; h.u = h.v = 0.0f; h.prim = -1;
   TravState st;
@@ -729,6 +730,7 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_shadow_persiste
   float tmin = 0.0f, tmax = 0.0f;
   RayPre rp;
   rp.inv = f3s(0.0f);
+  rp.sx = rp.sy = rp.sz = 0;
   TravState st;
   trav_init(st, stk + threadIdx.x, kBlock);
   uint2 spill4[kW4 ? kSpill4 : 1];

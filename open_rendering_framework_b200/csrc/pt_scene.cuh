@@ -216,6 +216,7 @@ struct Hit {
 // ------------------------------------------------------------------ intersection primitives
 struct RayPre {
   float3 inv;
+  int sx, sy, sz;  // 1 where the direction component is negative: the near slab plane is the box's hi
 };
 PT_HD RayPre ray_pre(const float3& o, const float3& d)
 {
@@ -224,6 +225,9 @@ PT_HD RayPre ray_pre(const float3& o, const float3& d)
   float dy = fabsf(d.y) > 1e-20f ? d.y : copysignf(1e-20f, d.y);
   float dz = fabsf(d.z) > 1e-20f ? d.z : copysignf(1e-20f, d.z);
   r.inv = f3(1.0f / dx, 1.0f / dy, 1.0f / dz);
+  r.sx = r.inv.x < 0.0f;
+  r.sy = r.inv.y < 0.0f;
+  r.sz = r.inv.z < 0.0f;
   return r;
 }
 // Slab test of one child box; returns the entry distance, or +inf on a miss.  Each slab distance is
@@ -584,15 +588,28 @@ PT_HD void cswap4(int code[4], float t[4], int a, int b)
   code[a] = sw ? cb : ca;
   code[b] = sw ? ca : cb;
 }
+// The slab test of `slab` with the near and far planes of each axis chosen by the direction's sign
+// (loaded from the node's lo or hi plane row): the same products, so the same distances and the same
+// decisions, without the per-axis min / max that orders them.
+PT_HD float slab_nf(float nx, float fx, float ny, float fy, float nz, float fz, const float3& o, const RayPre& r, float tmin, float tmax)
+{
+  const float tnx = (nx - o.x) * r.inv.x, tfx = (fx - o.x) * r.inv.x;
+  const float tny = (ny - o.y) * r.inv.y, tfy = (fy - o.y) * r.inv.y;
+  const float tnz = (nz - o.z) * r.inv.z, tfz = (fz - o.z) * r.inv.z;
+  const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+  const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax * kSlack));
+  return tn <= tf * kSlack ? tn : as_float(0x7f800000);
+}
 template <class G> PT_HD int node4_hits(const G& S, int node, const float3& o, const RayPre& rp, float tmin, float tmax, int code[4], float t[4])
 {
   const float4* nd = S.nodes4 + 8 * (size_t)node;
-  const float4 lx = PT_LDG(nd), hx = PT_LDG(nd + 1), ly = PT_LDG(nd + 2), hy = PT_LDG(nd + 3), lz = PT_LDG(nd + 4), hz = PT_LDG(nd + 5);
+  const float4 nx = PT_LDG(nd + rp.sx), fx = PT_LDG(nd + 1 - rp.sx), ny = PT_LDG(nd + 2 + rp.sy), fy = PT_LDG(nd + 3 - rp.sy);
+  const float4 nz = PT_LDG(nd + 4 + rp.sz), fz = PT_LDG(nd + 5 - rp.sz);
   const int4 c = PT_LDG(reinterpret_cast<const int4*>(nd + 6));
-  t[0] = slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, o, rp, tmin, tmax);
-  t[1] = slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, o, rp, tmin, tmax);
-  t[2] = slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, o, rp, tmin, tmax);
-  t[3] = slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, o, rp, tmin, tmax);
+  t[0] = slab_nf(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, o, rp, tmin, tmax);
+  t[1] = slab_nf(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, o, rp, tmin, tmax);
+  t[2] = slab_nf(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, o, rp, tmin, tmax);
+  t[3] = slab_nf(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, o, rp, tmin, tmax);
   code[0] = c.x;
   code[1] = c.y;
   code[2] = c.z;
