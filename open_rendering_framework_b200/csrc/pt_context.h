@@ -52,6 +52,7 @@ struct Wavefront {
   DevBuf adj_a, adj_b;                        // adjoint renders: per path image gradient and pending gradient
   DevBuf q_a, q_b;                            // active queues (path ids)
   DevBuf q_mat;                               // per-material-class queues, kQueues x cap
+  DevBuf cls_of, bin;                         // class per queue position (bytes) and binning block counts
   DevBuf sh_o, sh_d, sh_c, sh_pid;            // shadow-ray queue
   DevBuf counters;                            // kCounters uint32
   // translucent objects: the per-path stack of pending dipole gathers ([slot][path]) and the probes

@@ -3,10 +3,10 @@
 //
 // One call of pt_render_frames traces every (pixel, frame) camera sample of a group of frames at
 // once.  Per bounce:
-//   extend   closest hit through the stackless BVH; each path id is appended to the queue of its
-//            hit's material class (miss, emitter, diffuse, conductor, rough dielectric, translucent) -- the sort
-//            by material key -- with block-aggregated appends (warp ballots + shared-memory prefix,
-//            one global atomic per block and class)
+//   extend   closest hit through the BVH; the class of each ray's hit (miss, emitter, diffuse, conductor,
+//            rough dielectric, translucent, layered) is recorded by queue position
+//   bin      a stable partition of the queue by class into the material queues -- the sort by material
+//            key -- (warp ballots + shared-memory prefix per block, a scan over the blocks)
 //   shade    one kernel per material class, following diffuse_shader.cu, metallic_shader.cu,
 //            rough_transparent_shader.cu, arealight_shader.cu, constantbg.cu; continuing paths are
 //            appended to the next active queue and diffuse next-event estimation to the shadow queue
@@ -68,6 +68,8 @@ struct WfDev {
   uint32_t* q_in;
   uint32_t* q_out;
   uint32_t* q_mat;  // kQueues * cap
+  uint8_t* cls_of;  // material class of the ray at each position of q_in (written by extend, binned by k_bin_*)
+  uint32_t* bin;    // kBinBlocks x kQueues class counts, then offsets, of the binning blocks
   float4* sh_o;
   float4* sh_d;
   float4* sh_c;
@@ -141,33 +143,6 @@ __device__ __forceinline__ uint32_t block_slot(bool want, uint32_t* counter, uin
   return slot;
 }
 
-// Multi-queue variant: cls in [0, kQueues) or -1.
-__device__ __forceinline__ uint32_t block_slot_multi(int cls, uint32_t* counters /* kQueues consecutive */, uint32_t* smem /* kWarps*kQueues + kQueues */)
-{
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  uint32_t rank = 0;
-#pragma unroll
-  for (int q = 0; q < kQueues; ++q) {
-    unsigned m = __ballot_sync(0xffffffffu, cls == q);
-    if (lane == 0) smem[warp * kQueues + q] = __popc(m);
-    if (cls == q) rank = __popc(m & lanemask_lt());
-  }
-  __syncthreads();
-  if (threadIdx.x < kQueues) {
-    int q = threadIdx.x;
-    uint32_t total = 0;
-    for (int w = 0; w < kWarps; ++w) {
-      uint32_t c = smem[w * kQueues + q];
-      smem[w * kQueues + q] = total;
-      total += c;
-    }
-    smem[kWarps * kQueues + q] = total ? atomicAdd(counters + q, total) : 0u;
-  }
-  __syncthreads();
-  uint32_t slot = cls >= 0 ? smem[kWarps * kQueues + cls] + smem[warp * kQueues + cls] + rank : 0u;
-  __syncthreads();
-  return slot;
-}
 
 // Shading normal of a hit: normalize(rtTransformNormal(normalize(n))) with the identity transform,
 // where n is the interpolated vertex normal or the geometric normal (triangle_mesh.cu:63-70,
@@ -510,7 +485,6 @@ __device__ __forceinline__ int class_of(uint32_t type)
 
 __global__ void __launch_bounds__(kBlock) k_extend(WfDev w)
 {
-  __shared__ uint32_t sm[kWarps * kQueues + kQueues];
   const uint32_t n = w.cnt[w.in_slot];
   uint32_t traced = 0;
   for (uint32_t base = blockIdx.x * kBlock; base < n; base += gridDim.x * kBlock) {
@@ -526,33 +500,13 @@ __global__ void __launch_bounds__(kBlock) k_extend(WfDev w)
       if (h.prim < 0) cls = QC_MISS;
       else if ((uint32_t)h.prim >= S.n_tris) cls = QC_LIGHT;  // a disk or sphere emitter
       else cls = class_of(__ldg(&S.mats[__ldg(&S.tri_info[h.prim].w)].type));
+      w.cls_of[i] = (uint8_t)cls;
       ++traced;
     }
-    uint32_t slot = block_slot_multi(cls, w.cnt + CNT_Q_MISS, sm);
-    if (cls >= 0) w.q_mat[(size_t)cls * w.cap + slot] = pid;
   }
   if (traced) atomicAdd(cnt64(w.cnt, CNT_SEGMENTS_LO), (unsigned long long)traced);
 }
 
-// Warp-aggregated multi-queue append (no block barrier): lanes with cls in [0, kQueues) get distinct
-// slots; one atomic per warp and class.  All lanes of the warp must call it.
-__device__ __forceinline__ uint32_t warp_slot_multi(int cls, uint32_t* counters)
-{
-  const unsigned lane = threadIdx.x & 31;
-  uint32_t slot = 0;
-#pragma unroll
-  for (int q = 0; q < kQueues; ++q) {
-    unsigned m = __ballot_sync(0xffffffffu, cls == q);
-    if (m) {
-      int leader = __ffs(m) - 1;
-      uint32_t base = 0;
-      if ((int)lane == leader) base = atomicAdd(counters + q, (uint32_t)__popc(m));
-      base = __shfl_sync(0xffffffffu, base, leader);
-      if (cls == q) slot = base + __popc(m & lanemask_lt());
-    }
-  }
-  return slot;
-}
 
 // Persistent closest-hit kernel with dynamic ray fetch: every warp keeps 32 rays in flight and,
 // whenever at least `refill` of its lanes have finished (or the queue is drained and all have),
@@ -576,7 +530,7 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_extend_persiste
   const int4* tinfo = S0.tri_info;
   const unsigned lane = threadIdx.x & 31;
   bool has = false, done = false, drained = false;
-  uint32_t pid = 0, traced = 0;
+  uint32_t pid = 0, qi = 0, traced = 0;
   float3 o = f3s(0.0f), d = f3s(0.0f);
   RayPre rp;
   rp.inv = f3s(0.0f);
@@ -601,6 +555,7 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_extend_persiste
         uint32_t i = base + __popc(idle & lanemask_lt());
         if (i < n) {
           pid = w.q_in[i];
+          qi = i;
           if constexpr (kMulti) {
             const SceneDev& S = scene_of(w, pid);
             g = trav_geom(S);
@@ -676,9 +631,8 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_extend_persiste
       }
       w.hit[pid] = make_float4(h.t, h.u, h.v, as_float(h.prim));
       cls = h.prim < 0 ? QC_MISS : (uint32_t)h.prim >= n_tris ? QC_LIGHT : class_of(__ldg(&mats[__ldg(&tinfo[h.prim].w)].type));
+      w.cls_of[qi] = (uint8_t)cls;
     }
-    uint32_t slot = warp_slot_multi(cls, w.cnt + CNT_Q_MISS);
-    if (cls >= 0) w.q_mat[(size_t)cls * w.cap + slot] = pid;
     if (has && done && leafA == 0) has = false;
   }
   traced += __shfl_xor_sync(0xffffffffu, traced, 16);
@@ -687,6 +641,116 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_extend_persiste
   traced += __shfl_xor_sync(0xffffffffu, traced, 2);
   traced += __shfl_xor_sync(0xffffffffu, traced, 1);
   if (lane == 0 && traced) atomicAdd(cnt64(w.cnt, CNT_SEGMENTS_LO), (unsigned long long)traced);
+}
+
+// ------------------------------------------------------------------ binning by material (the sort by material key)
+// The extend kernels record the class of the ray at each queue position (cls_of); these three kernels
+// partition the queue stably by class into the material queues, so that each queue keeps the order of
+// the rays it came from: camera rays in pixel order, later bounces in the order the shading kernels
+// appended them.  Neighbouring entries of a material queue then address neighbouring path records
+// (coalesced state reads and writes in the shading kernels) and emit spatially coherent shadow rays.
+// kBinBlocks blocks each own the contiguous range [n b / B, n (b + 1) / B) of the queue.
+constexpr int kBinBlocks = 296;
+constexpr int kBinThreads = 256;
+constexpr int kBinWarps = kBinThreads / 32;
+static_assert(kBinBlocks <= 1024, "one scan thread per binning block");
+
+__device__ __forceinline__ void bin_range(uint32_t n, uint32_t& b0, uint32_t& b1)
+{
+  b0 = (uint32_t)((uint64_t)n * blockIdx.x / gridDim.x);
+  b1 = (uint32_t)((uint64_t)n * (blockIdx.x + 1) / gridDim.x);
+}
+
+__global__ void __launch_bounds__(kBinThreads) k_bin_count(WfDev w)
+{
+  __shared__ uint32_t cnt[kQueues];
+  const uint32_t n = w.cnt[w.in_slot];
+  uint32_t b0, b1;
+  bin_range(n, b0, b1);
+  if (threadIdx.x < kQueues) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  uint32_t local[kQueues];
+#pragma unroll
+  for (int q = 0; q < kQueues; ++q) local[q] = 0;
+  for (uint32_t i = b0 + threadIdx.x; i < b1; i += kBinThreads) {
+    const uint32_t c = w.cls_of[i];
+#pragma unroll
+    for (int q = 0; q < kQueues; ++q) local[q] += c == (uint32_t)q;
+  }
+#pragma unroll
+  for (int q = 0; q < kQueues; ++q) {
+    uint32_t v = local[q];
+    for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(&cnt[q], v);
+  }
+  __syncthreads();
+  if (threadIdx.x < kQueues) w.bin[blockIdx.x * kQueues + threadIdx.x] = cnt[threadIdx.x];
+}
+
+// One block: exclusive scan of every class's block counts (in place) and the class totals.
+__global__ void __launch_bounds__(1024) k_bin_scan(WfDev w, int blocks)
+{
+  __shared__ uint32_t warp_sum[32];
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  for (int q = 0; q < kQueues; ++q) {
+    const uint32_t v = t < blocks ? w.bin[t * kQueues + q] : 0u;
+    uint32_t x = v;  // inclusive warp scan
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+      if (lane >= off) x += y;
+    }
+    if (lane == 31) warp_sum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      uint32_t s = warp_sum[lane];
+      for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, s, off);
+        if (lane >= off) s += y;
+      }
+      warp_sum[lane] = s;  // inclusive over warps
+    }
+    __syncthreads();
+    const uint32_t excl = x - v + (wid ? warp_sum[wid - 1] : 0u);
+    if (t < blocks) w.bin[t * kQueues + q] = excl;
+    if (t == 0) w.cnt[CNT_Q_MISS + q] = warp_sum[31];
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kBinThreads) k_bin_scatter(WfDev w)
+{
+  __shared__ uint32_t base[kQueues];
+  __shared__ uint32_t wcount[kBinWarps][kQueues];
+  const uint32_t n = w.cnt[w.in_slot];
+  uint32_t b0, b1;
+  bin_range(n, b0, b1);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x < kQueues) base[threadIdx.x] = w.bin[blockIdx.x * kQueues + threadIdx.x];
+  for (uint32_t c0 = b0; c0 < b1; c0 += kBinThreads) {
+    const uint32_t i = c0 + threadIdx.x;
+    const int c = i < b1 ? (int)w.cls_of[i] : -1;
+    uint32_t rank = 0;
+#pragma unroll
+    for (int q = 0; q < kQueues; ++q) {
+      const unsigned m = __ballot_sync(0xffffffffu, c == q);
+      if (c == q) rank = __popc(m & ((1u << lane) - 1u));
+      if (lane == 0) wcount[wid][q] = __popc(m);
+    }
+    __syncthreads();
+    if (threadIdx.x < kQueues) {  // warp prefix per class, then advance the class base for the next chunk
+      const int q = threadIdx.x;
+      uint32_t run = base[q];
+      for (int k = 0; k < kBinWarps; ++k) {
+        const uint32_t v = wcount[k][q];
+        wcount[k][q] = run;
+        run += v;
+      }
+      base[q] = run;
+    }
+    __syncthreads();
+    if (c >= 0) w.q_mat[(size_t)c * w.cap + wcount[wid][c] + rank] = w.q_in[i];
+    __syncthreads();
+  }
 }
 
 // Adds an unoccluded next-event estimate to the path (kAdj: takes it off R, and adds the albedo
@@ -2040,6 +2104,8 @@ static pt_status ensure_wavefront(Context& c, uint64_t cap)
   if (st == PT_OK) st = wf.q_a.reserve(cap * 4, "queue");
   if (st == PT_OK) st = wf.q_b.reserve(cap * 4, "queue");
   if (st == PT_OK) st = wf.q_mat.reserve(cap * 4 * kQueues, "material queues");
+  if (st == PT_OK) st = wf.cls_of.reserve(cap, "material classes of the queue");
+  if (st == PT_OK) st = wf.bin.reserve(kBinBlocks * kQueues * 4, "material binning counts");
   if (st == PT_OK) st = wf.sh_o.reserve(cap * f4, "shadow queue");
   if (st == PT_OK) st = wf.sh_d.reserve(cap * f4, "shadow queue");
   if (st == PT_OK) st = wf.sh_c.reserve(cap * f4, "shadow queue");
@@ -2266,6 +2332,8 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
   w.rng = Field4<uint4>{reinterpret_cast<uint4*>(rec + 3)};
   w.hit = wf.hit.as<float4>();
   w.q_mat = wf.q_mat.as<uint32_t>();
+  w.cls_of = wf.cls_of.as<uint8_t>();
+  w.bin = wf.bin.as<uint32_t>();
   w.sh_o = wf.sh_o.as<float4>();
   w.sh_d = wf.sh_d.as<float4>();
   w.sh_c = wf.sh_c.as<float4>();
@@ -2357,6 +2425,10 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
         k_extend<<<grid_trace, kBlock, 0, c.stream>>>(w);
       }
       if ((st = prof_end()) != PT_OK) return st;
+      k_bin_count<<<kBinBlocks, kBinThreads, 0, c.stream>>>(w);
+      k_bin_scan<<<1, 1024, 0, c.stream>>>(w, kBinBlocks);
+      k_bin_scatter<<<kBinBlocks, kBinThreads, 0, c.stream>>>(w);
+      count_launch(3);
       if (adjoint) {
         k_shade_miss<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
         k_shade_light<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
