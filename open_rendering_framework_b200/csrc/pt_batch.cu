@@ -57,7 +57,7 @@ std::vector<uint64_t> graph_key(const Context& E, const PassLayout& L)
     k.push_back(L.chunk_pixels[i]);
     k.push_back(L.chunk_sets[i]);
   }
-  for (const void* p : {E.wf.state.p, E.wf.g_a.p, E.wf.probes.p, E.d_scene_tab.p, E.d_item_tab.p, E.wf.counters.p, E.wf.path_item.p})
+  for (const void* p : {E.wf.rays.p, E.wf.state.p, E.wf.g_a.p, E.wf.probes.p, E.d_scene_tab.p, E.d_item_tab.p, E.wf.counters.p, E.wf.path_item.p})
     k.push_back((uint64_t)(uintptr_t)p);
   k.push_back(E.wf.cap);
   k.push_back((uint64_t)E.opt.extend_mode);

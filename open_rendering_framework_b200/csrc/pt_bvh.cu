@@ -307,11 +307,11 @@ bool build_bvh4(const BvhHost& b2, std::vector<float4>& out4, int& depth4)
   std::function<int(int, int)> build = [&](int n2, int depth) -> int {
     depth4 = std::max(depth4, depth);
     if (depth >= kMaxDepth4) ok = false;
-    Kid kids[4];
+    Kid kids[kWide];
     int nk = 0;
     kids[nk++] = kid(n2, 0);
     kids[nk++] = kid(n2, 1);
-    while (nk < 4) {
+    while (nk < kWide) {  // open the internal child of largest surface area
       int best = -1;
       float ba = -1.0f;
       for (int j = 0; j < nk; ++j)
@@ -321,23 +321,28 @@ bool build_bvh4(const BvhHost& b2, std::vector<float4>& out4, int& depth4)
       kids[best] = kid(inner, 0);
       kids[nk++] = kid(inner, 1);
     }
-    const int me = (int)(out4.size() / 8);
-    out4.resize(out4.size() + 8);
-    int codes[4];
-    for (int j = 0; j < 4; ++j) {
+    const int me = (int)(out4.size() / kWideStride);
+    out4.resize(out4.size() + kWideStride, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+    int codes[kWide];
+    for (int j = 0; j < kWide; ++j) {
       if (j >= nk) codes[j] = (int)0x80000000u;  // empty slot: a leaf of no triangles behind a far box
       else if (kids[j].code >= 0) codes[j] = ok ? build(kids[j].code, depth + 1) : 0;
       else codes[j] = kids[j].code;
     }
-    float4* nd = out4.data() + 8 * (size_t)me;
+    float4* nd = out4.data() + kWideStride * (size_t)me;
     auto comp = [&](int j, int axis, bool lo) { return j < nk ? (lo ? kids[j].lo[axis] : kids[j].hi[axis]) : 1e30f; };
-    for (int axis = 0; axis < 3; ++axis) {
-      nd[2 * axis] = make_float4(comp(0, axis, true), comp(1, axis, true), comp(2, axis, true), comp(3, axis, true));
-      nd[2 * axis + 1] = make_float4(comp(0, axis, false), comp(1, axis, false), comp(2, axis, false), comp(3, axis, false));
+    for (int axis = 0; axis < 3; ++axis)
+      for (int r = 0; r < kWideRow; ++r) {
+        nd[(2 * axis) * kWideRow + r] = make_float4(comp(4 * r, axis, true), comp(4 * r + 1, axis, true), comp(4 * r + 2, axis, true),
+                                                    comp(4 * r + 3, axis, true));
+        nd[(2 * axis + 1) * kWideRow + r] = make_float4(comp(4 * r, axis, false), comp(4 * r + 1, axis, false),
+                                                        comp(4 * r + 2, axis, false), comp(4 * r + 3, axis, false));
+      }
+    for (int r = 0; r < kWideRow; ++r) {
+      int4 c4 = make_int4(codes[4 * r], codes[4 * r + 1], codes[4 * r + 2], codes[4 * r + 3]);
+      memcpy(&nd[6 * kWideRow + r], &c4, sizeof(c4));
     }
-    int4 c4 = make_int4(codes[0], codes[1], codes[2], codes[3]);
-    memcpy(&nd[6], &c4, sizeof(c4));
-    nd[7] = make_float4((float)nk, 0.0f, 0.0f, 0.0f);
+    if (kWideStride > 7 * kWideRow) nd[7 * kWideRow] = make_float4((float)nk, 0.0f, 0.0f, 0.0f);
     return me;
   };
   build(0, 1);

@@ -5,6 +5,8 @@
 
 #include <vector>
 
+#include "pt_scene.cuh"
+
 namespace pt {
 
 struct BvhHost {
@@ -25,10 +27,11 @@ struct BvhParams {
 // node encoding (2^27 triangles) or the tree is deeper than the traversal trail allows.
 bool build_bvh(const float* tri_pos, uint32_t n_tris, BvhHost& out, const BvhParams& params = BvhParams());
 
-// The BVH2 collapsed into a 4-wide BVH over the same leaves (8 float4 = 128 bytes per node, root =
-// node 0; layout in pt_scene.cuh).  Returns false (and leaves nodes4 empty) when the 4-wide tree
-// would be deeper than kMaxDepth4 levels, whose pending children the traversal stack could not hold.
-constexpr int kMaxDepth4 = 40;
+// The BVH2 collapsed into a wide BVH of kWide children per node over the same leaves (kWideStride
+// float4 per node, root = node 0; layout in pt_scene.cuh).  Returns false (and leaves nodes4 empty)
+// when the wide tree would be deeper than kMaxDepthWide levels, whose pending children the traversal
+// stack could not hold.
+constexpr int kMaxDepth4 = kMaxDepthWide;
 bool build_bvh4(const BvhHost& bvh2, std::vector<float4>& nodes4, int& depth4);
 
 }  // namespace pt

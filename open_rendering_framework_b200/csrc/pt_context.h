@@ -46,7 +46,7 @@ struct DevBuf {
 // Wavefront buffers, sized for `cap` paths in flight.
 struct Wavefront {
   uint64_t cap = 0;
-  DevBuf state;                               // per path, one 64-byte record: ray origin, ray direction, throughput, rng
+  DevBuf rays, state;                         // per path, 32-byte records: (ray origin, direction), (throughput, rng)
   DevBuf rad, hit;                            // per path
   DevBuf path_item;                           // per path: its item of the pass (uint16)
   DevBuf adj_a, adj_b;                        // adjoint renders: per path image gradient and pending gradient

@@ -49,27 +49,28 @@ constexpr uint32_t META_PROBE = 1u << 18;  // a probe's indirect path (sample_ca
 constexpr int META_GSHIFT = 24;            // pending dipole gathers on the path's stack (8 bits)
 constexpr uint32_t META_KEEP = ~(META_DEPTH | META_EMIT);
 
-// One 16-byte field of the per-path state records: field k of path i sits at rec[4 i + k], so the four
-// fields of a path (ray origin, ray direction, throughput, rng state) share one 64-byte record.  A shading
-// kernel reading and rewriting a path at a random id touches two whole 32-byte sectors instead of four
-// half sectors of four arrays, and the extend kernel reads the ray from a single sector.
-template <class T> struct Field4 {
+// One 16-byte field of a per-path pair record: field k of path i sits at rec[2 i + k].  The ray (origin,
+// direction) and the path state (throughput, rng state) are two 32-byte records per path, each one
+// whole sector: a shading kernel reading and rewriting a path at a random id touches two whole sectors
+// instead of four half sectors of four arrays, and the extend kernel reads exactly the ray's sector
+// (consecutive paths' rays are contiguous).
+template <class T> struct Field2 {
   T* p;
-  __device__ __forceinline__ T& operator[](uint64_t i) const { return p[4 * i]; }
+  __device__ __forceinline__ T& operator[](uint64_t i) const { return p[2 * i]; }
 };
 
 struct WfDev {
-  Field4<float4> ray_o;
-  Field4<float4> ray_d;
-  Field4<float4> thr;
+  Field2<float4> ray_o;
+  Field2<float4> ray_d;
+  Field2<float4> thr;
   float4* rad;
-  Field4<uint4> rng;
+  Field2<uint4> rng;
   float4* hit;
   uint32_t* q_in;
   uint32_t* q_out;
   uint32_t* q_mat;  // kQueues * cap
   uint8_t* cls_of;  // material class of the ray at each position of q_in (written by extend, binned by k_bin_*)
-  uint32_t* bin;    // kBinBlocks x kQueues class counts, then offsets, of the binning blocks
+  uint32_t* bin;    // per chunk of kBinChunk queue positions: kQueues class counts, then starts in the queues
   float4* sh_o;
   float4* sh_d;
   float4* sh_c;
@@ -649,52 +650,67 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_extend_persiste
 // the rays it came from: camera rays in pixel order, later bounces in the order the shading kernels
 // appended them.  Neighbouring entries of a material queue then address neighbouring path records
 // (coalesced state reads and writes in the shading kernels) and emit spatially coherent shadow rays.
-// kBinBlocks blocks each own the contiguous range [n b / B, n (b + 1) / B) of the queue.
-constexpr int kBinBlocks = 296;
+// The queue is cut into chunks of kBinChunk positions (kBinItems consecutive positions per thread);
+// k_bin_count counts every chunk's classes, k_bin_scan turns the counts into each chunk's start in
+// every material queue (one block, chunk order), and k_bin_scatter writes every chunk's entries there.
 constexpr int kBinThreads = 256;
+constexpr int kBinItems = 8;
+constexpr int kBinChunk = kBinThreads * kBinItems;
 constexpr int kBinWarps = kBinThreads / 32;
-static_assert(kBinBlocks <= 1024, "one scan thread per binning block");
 
-__device__ __forceinline__ void bin_range(uint32_t n, uint32_t& b0, uint32_t& b1)
+// The classes of the kBinItems positions of this thread in chunk k (-1 past the end of the queue).
+__device__ __forceinline__ void bin_load(const WfDev& w, uint32_t n, uint32_t k, int c[kBinItems])
 {
-  b0 = (uint32_t)((uint64_t)n * blockIdx.x / gridDim.x);
-  b1 = (uint32_t)((uint64_t)n * (blockIdx.x + 1) / gridDim.x);
+  const uint32_t i0 = k * kBinChunk + threadIdx.x * kBinItems;
+  if (i0 + kBinItems <= n) {
+    const uint2 v = *reinterpret_cast<const uint2*>(w.cls_of + i0);
+#pragma unroll
+    for (int j = 0; j < kBinItems; ++j) c[j] = (int)(((j < 4 ? v.x : v.y) >> (8 * (j & 3))) & 0xffu);
+  } else {
+#pragma unroll
+    for (int j = 0; j < kBinItems; ++j) c[j] = i0 + j < n ? (int)w.cls_of[i0 + j] : -1;
+  }
 }
 
 __global__ void __launch_bounds__(kBinThreads) k_bin_count(WfDev w)
 {
   __shared__ uint32_t cnt[kQueues];
   const uint32_t n = w.cnt[w.in_slot];
-  uint32_t b0, b1;
-  bin_range(n, b0, b1);
-  if (threadIdx.x < kQueues) cnt[threadIdx.x] = 0;
-  __syncthreads();
-  uint32_t local[kQueues];
+  const uint32_t chunks = (n + kBinChunk - 1) / kBinChunk;
+  for (uint32_t k = blockIdx.x; k < chunks; k += gridDim.x) {
+    if (threadIdx.x < kQueues) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    int c[kBinItems];
+    bin_load(w, n, k, c);
 #pragma unroll
-  for (int q = 0; q < kQueues; ++q) local[q] = 0;
-  for (uint32_t i = b0 + threadIdx.x; i < b1; i += kBinThreads) {
-    const uint32_t c = w.cls_of[i];
+    for (int q = 0; q < kQueues; ++q) {
+      uint32_t v = 0;
 #pragma unroll
-    for (int q = 0; q < kQueues; ++q) local[q] += c == (uint32_t)q;
+      for (int j = 0; j < kBinItems; ++j) v += c[j] == q;
+      for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      if ((threadIdx.x & 31) == 0 && v) atomicAdd(&cnt[q], v);
+    }
+    __syncthreads();
+    if (threadIdx.x < kQueues) w.bin[(size_t)k * kQueues + threadIdx.x] = cnt[threadIdx.x];
   }
-#pragma unroll
-  for (int q = 0; q < kQueues; ++q) {
-    uint32_t v = local[q];
-    for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-    if ((threadIdx.x & 31) == 0 && v) atomicAdd(&cnt[q], v);
-  }
-  __syncthreads();
-  if (threadIdx.x < kQueues) w.bin[blockIdx.x * kQueues + threadIdx.x] = cnt[threadIdx.x];
 }
 
-// One block: exclusive scan of every class's block counts (in place) and the class totals.
-__global__ void __launch_bounds__(1024) k_bin_scan(WfDev w, int blocks)
+// One block of 1024 threads: per class, the exclusive scan of the chunk counts (in place, chunk order)
+// and the class totals (the material queue counts).
+__global__ void __launch_bounds__(1024) k_bin_scan(WfDev w)
 {
   __shared__ uint32_t warp_sum[32];
+  const uint32_t n = w.cnt[w.in_slot];
+  const uint32_t chunks = (n + kBinChunk - 1) / kBinChunk;
+  const uint32_t per = (chunks + 1023) / 1024;  // consecutive chunks per thread
   const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
   for (int q = 0; q < kQueues; ++q) {
-    const uint32_t v = t < blocks ? w.bin[t * kQueues + q] : 0u;
-    uint32_t x = v;  // inclusive warp scan
+    uint32_t v = 0;
+    for (uint32_t j = 0; j < per; ++j) {
+      const uint32_t k = t * per + j;
+      if (k < chunks) v += w.bin[(size_t)k * kQueues + q];
+    }
+    uint32_t x = v;  // inclusive warp scan of the per-thread sums
     for (int off = 1; off < 32; off <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
       if (lane >= off) x += y;
@@ -707,11 +723,18 @@ __global__ void __launch_bounds__(1024) k_bin_scan(WfDev w, int blocks)
         const uint32_t y = __shfl_up_sync(0xffffffffu, s, off);
         if (lane >= off) s += y;
       }
-      warp_sum[lane] = s;  // inclusive over warps
+      warp_sum[lane] = s;
     }
     __syncthreads();
-    const uint32_t excl = x - v + (wid ? warp_sum[wid - 1] : 0u);
-    if (t < blocks) w.bin[t * kQueues + q] = excl;
+    uint32_t run = x - v + (wid ? warp_sum[wid - 1] : 0u);
+    for (uint32_t j = 0; j < per; ++j) {
+      const uint32_t k = t * per + j;
+      if (k < chunks) {
+        const uint32_t c = w.bin[(size_t)k * kQueues + q];
+        w.bin[(size_t)k * kQueues + q] = run;
+        run += c;
+      }
+    }
     if (t == 0) w.cnt[CNT_Q_MISS + q] = warp_sum[31];
     __syncthreads();
   }
@@ -719,36 +742,44 @@ __global__ void __launch_bounds__(1024) k_bin_scan(WfDev w, int blocks)
 
 __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(WfDev w)
 {
-  __shared__ uint32_t base[kQueues];
-  __shared__ uint32_t wcount[kBinWarps][kQueues];
+  __shared__ uint32_t wtot[kBinWarps][kQueues];
   const uint32_t n = w.cnt[w.in_slot];
-  uint32_t b0, b1;
-  bin_range(n, b0, b1);
+  const uint32_t chunks = (n + kBinChunk - 1) / kBinChunk;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (threadIdx.x < kQueues) base[threadIdx.x] = w.bin[blockIdx.x * kQueues + threadIdx.x];
-  for (uint32_t c0 = b0; c0 < b1; c0 += kBinThreads) {
-    const uint32_t i = c0 + threadIdx.x;
-    const int c = i < b1 ? (int)w.cls_of[i] : -1;
-    uint32_t rank = 0;
+  for (uint32_t k = blockIdx.x; k < chunks; k += gridDim.x) {
+    int c[kBinItems];
+    bin_load(w, n, k, c);
+    uint32_t pos[kQueues];
+#pragma unroll
+    for (int q = 0; q < kQueues; ++q) {  // exclusive prefix of this thread's count over the warp
+      uint32_t v = 0;
+#pragma unroll
+      for (int j = 0; j < kBinItems; ++j) v += c[j] == q;
+      uint32_t x = v;
+      for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off) x += y;
+      }
+      pos[q] = x - v;
+      if (lane == 31) wtot[wid][q] = x;
+    }
+    __syncthreads();
 #pragma unroll
     for (int q = 0; q < kQueues; ++q) {
-      const unsigned m = __ballot_sync(0xffffffffu, c == q);
-      if (c == q) rank = __popc(m & ((1u << lane) - 1u));
-      if (lane == 0) wcount[wid][q] = __popc(m);
+      uint32_t base = w.bin[(size_t)k * kQueues + q];
+      for (int ww = 0; ww < wid; ++ww) base += wtot[ww][q];
+      pos[q] += base;
     }
-    __syncthreads();
-    if (threadIdx.x < kQueues) {  // warp prefix per class, then advance the class base for the next chunk
-      const int q = threadIdx.x;
-      uint32_t run = base[q];
-      for (int k = 0; k < kBinWarps; ++k) {
-        const uint32_t v = wcount[k][q];
-        wcount[k][q] = run;
-        run += v;
-      }
-      base[q] = run;
+    const uint32_t i0 = k * kBinChunk + threadIdx.x * kBinItems;
+#pragma unroll
+    for (int j = 0; j < kBinItems; ++j) {
+      if (c[j] < 0) continue;
+      uint32_t at = 0;
+#pragma unroll
+      for (int q = 0; q < kQueues; ++q)
+        if (c[j] == q) at = pos[q]++;
+      w.q_mat[(size_t)c[j] * w.cap + at] = w.q_in[i0 + j];
     }
-    __syncthreads();
-    if (c >= 0) w.q_mat[(size_t)c * w.cap + wcount[wid][c] + rank] = w.q_in[i];
     __syncthreads();
   }
 }
@@ -2097,7 +2128,8 @@ static pt_status ensure_wavefront(Context& c, uint64_t cap)
   if (wf.cap >= cap && wf.counters.p) return PT_OK;
   pt_status st = PT_OK;
   const size_t f4 = sizeof(float4), u4 = sizeof(uint4);
-  if (st == PT_OK) st = wf.state.reserve(cap * (3 * f4 + u4), "wavefront path records");
+  if (st == PT_OK) st = wf.rays.reserve(cap * 2 * f4, "wavefront ray records");
+  if (st == PT_OK) st = wf.state.reserve(cap * (f4 + u4), "wavefront path-state records");
   if (st == PT_OK) st = wf.rad.reserve(cap * f4, "wavefront radiance");
   if (st == PT_OK) st = wf.hit.reserve(cap * f4, "wavefront hits");
   if (st == PT_OK) st = wf.path_item.reserve(cap * 2, "wavefront path items");
@@ -2105,7 +2137,7 @@ static pt_status ensure_wavefront(Context& c, uint64_t cap)
   if (st == PT_OK) st = wf.q_b.reserve(cap * 4, "queue");
   if (st == PT_OK) st = wf.q_mat.reserve(cap * 4 * kQueues, "material queues");
   if (st == PT_OK) st = wf.cls_of.reserve(cap, "material classes of the queue");
-  if (st == PT_OK) st = wf.bin.reserve(kBinBlocks * kQueues * 4, "material binning counts");
+  if (st == PT_OK) st = wf.bin.reserve(((cap + kBinChunk - 1) / kBinChunk) * kQueues * 4, "material binning counts");
   if (st == PT_OK) st = wf.sh_o.reserve(cap * f4, "shadow queue");
   if (st == PT_OK) st = wf.sh_d.reserve(cap * f4, "shadow queue");
   if (st == PT_OK) st = wf.sh_c.reserve(cap * f4, "shadow queue");
@@ -2324,12 +2356,13 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
   Context& c = E;
   WfDev w;
   Wavefront& wf = c.wf;
-  float4* rec = wf.state.as<float4>();
-  w.ray_o = Field4<float4>{rec};
-  w.ray_d = Field4<float4>{rec + 1};
-  w.thr = Field4<float4>{rec + 2};
+  float4* rays = wf.rays.as<float4>();
+  float4* state = wf.state.as<float4>();
+  w.ray_o = Field2<float4>{rays};
+  w.ray_d = Field2<float4>{rays + 1};
+  w.thr = Field2<float4>{state};
   w.rad = wf.rad.as<float4>();
-  w.rng = Field4<uint4>{reinterpret_cast<uint4*>(rec + 3)};
+  w.rng = Field2<uint4>{reinterpret_cast<uint4*>(state + 1)};
   w.hit = wf.hit.as<float4>();
   w.q_mat = wf.q_mat.as<uint32_t>();
   w.cls_of = wf.cls_of.as<uint8_t>();
@@ -2375,6 +2408,7 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
                    : occupancy(k_extend_persistent<false, false>, k_shadow_persistent<false, false, false>);
   if (ost != PT_OK) return ost;
   const int grid_persist = sm_count() * std::max(1, std::min(occ_ext, occ_sh));
+  const int grid_bin = sm_count() * 8;
   const bool prof = c.profile && allow_events;
   PT_CHECK_CUDA(cudaMemsetAsync(w.cnt, 0, kCounters * 4, c.stream), "reset counters");
   c.prof_pairs = 0;
@@ -2425,9 +2459,9 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
         k_extend<<<grid_trace, kBlock, 0, c.stream>>>(w);
       }
       if ((st = prof_end()) != PT_OK) return st;
-      k_bin_count<<<kBinBlocks, kBinThreads, 0, c.stream>>>(w);
-      k_bin_scan<<<1, 1024, 0, c.stream>>>(w, kBinBlocks);
-      k_bin_scatter<<<kBinBlocks, kBinThreads, 0, c.stream>>>(w);
+      k_bin_count<<<grid_bin, kBinThreads, 0, c.stream>>>(w);
+      k_bin_scan<<<1, 1024, 0, c.stream>>>(w);
+      k_bin_scatter<<<grid_bin, kBinThreads, 0, c.stream>>>(w);
       count_launch(3);
       if (adjoint) {
         k_shade_miss<true><<<grid_shade, kBlock, 0, c.stream>>>(w);

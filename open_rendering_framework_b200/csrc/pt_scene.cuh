@@ -153,7 +153,7 @@ struct IntegratorDev {
 
 struct SceneDev {
   const float4* nodes;
-  const float4* nodes4;  // the 4-wide BVH (8 float4 per node) or null
+  const float4* nodes4;  // the wide BVH (kWide children per node, kWideStride float4 each) or null
   const float4* tri_v0;
   const float4* tri_e1;
   const float4* tri_e2;
@@ -525,17 +525,26 @@ template <class G> PT_HD bool trav_node_any(const G& S, const float3& o, const R
   return !trav_backtrack(S, o, rp, tmin, tmax, st, false);
 }
 
-// ------------------------------------------------------------------ 4-wide BVH traversal
-// Node (128 bytes, one cache line): float4 (lo.x of children 0..3), (hi.x), (lo.y), (hi.y), (lo.z),
-// (hi.z), int4 child codes (>= 0: node, < 0: leaf code as in the BVH2; empty slots are leaves of no
-// triangles behind a box at 1e30), float4 (child count, 0, 0, 0).  Traversal keeps the hit children
-// that are not visited next on a stack, nearest last, with their entry distance; closest-hit pops
-// skip entries beyond the closest hit found so far (entry distance > t * kSlack), as re-testing the
-// box would.  The stack is a ring of kRing4 entries (caller memory, typically shared, [slot][thread])
-// whose oldest entries spill to a per-thread array of kSpill4 entries (caller memory, typically a
-// local array) when it overflows.
+// ------------------------------------------------------------------ wide BVH traversal
+// Width kWide = 4 or 8 children per node (PT_BVH_WIDE at compile time).  Node: six plane rows -- lo.x
+// of the children, hi.x, lo.y, hi.y, lo.z, hi.z -- of kWide floats each (kWide / 4 float4 per row),
+// then kWide int child codes (>= 0: node, < 0: leaf code as in the BVH2; empty slots are leaves of no
+// triangles behind a box at 1e30); 4-wide nodes are padded to 128 bytes (8 float4), 8-wide nodes take
+// 224 bytes (14 float4).  Traversal keeps the hit children that are not visited next on a stack, nearest
+// last, with their entry distance; closest-hit pops skip entries beyond the closest hit found so far
+// (entry distance > t * kSlack), as re-testing the box would.  The stack is a ring of kRing4 entries
+// (caller memory, typically shared, [slot][thread]) whose oldest entries spill to a per-thread array of
+// kSpill4 entries (caller memory, typically a local array) when it overflows.
+#ifndef PT_BVH_WIDE
+#define PT_BVH_WIDE 4
+#endif
+constexpr int kWide = PT_BVH_WIDE;
+static_assert(kWide == 4 || kWide == 8, "the wide BVH has 4 or 8 children per node");
+constexpr int kWideRow = kWide / 4;                  // float4 per plane row
+constexpr int kWideStride = kWide == 4 ? 8 : 14;     // float4 per node
+constexpr int kMaxDepthWide = kWide == 4 ? 40 : 24;  // levels the stack is sized for
 constexpr int kRing4 = 8;
-constexpr int kSpill4 = 3 * 40 + 8;  // three pending children per level, kMaxDepth4 = 40 levels
+constexpr int kSpill4 = (kWide - 1) * kMaxDepthWide + 8;  // kWide - 1 pending children per level
 constexpr int kDone4 = 0x7fffffff;
 struct Stack4 {
   uint2* ring;
@@ -600,50 +609,96 @@ PT_HD float slab_nf(float nx, float fx, float ny, float fy, float nz, float fz, 
   const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax * kSlack));
   return tn <= tf * kSlack ? tn : as_float(0x7f800000);
 }
-template <class G> PT_HD int node4_hits(const G& S, int node, const float3& o, const RayPre& rp, float tmin, float tmax, int code[4], float t[4])
+PT_HD int popc32(unsigned m)
 {
-  const float4* nd = S.nodes4 + 8 * (size_t)node;
-  const float4 nx = PT_LDG(nd + rp.sx), fx = PT_LDG(nd + 1 - rp.sx), ny = PT_LDG(nd + 2 + rp.sy), fy = PT_LDG(nd + 3 - rp.sy);
-  const float4 nz = PT_LDG(nd + 4 + rp.sz), fz = PT_LDG(nd + 5 - rp.sz);
-  const int4 c = PT_LDG(reinterpret_cast<const int4*>(nd + 6));
-  t[0] = slab_nf(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, o, rp, tmin, tmax);
-  t[1] = slab_nf(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, o, rp, tmin, tmax);
-  t[2] = slab_nf(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, o, rp, tmin, tmax);
-  t[3] = slab_nf(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, o, rp, tmin, tmax);
-  code[0] = c.x;
-  code[1] = c.y;
-  code[2] = c.z;
-  code[3] = c.w;
+#ifdef __CUDA_ARCH__
+  return __popc(m);
+#else
+  return __builtin_popcount(m);
+#endif
+}
+// Tests the kWide children of node `node`: their codes and entry distances (+inf for a miss); with
+// kWide == 4 sorted near to far by a five-comparator network, returning the count of hits.
+template <class G> PT_HD int node4_hits(const G& S, int node, const float3& o, const RayPre& rp, float tmin, float tmax, int code[kWide],
+                                        float t[kWide])
+{
+  const float4* nd = S.nodes4 + kWideStride * (size_t)node;
+#pragma unroll
+  for (int r = 0; r < kWideRow; ++r) {
+    const float4 nx = PT_LDG(nd + (0 + rp.sx) * kWideRow + r), fx = PT_LDG(nd + (1 - rp.sx) * kWideRow + r);
+    const float4 ny = PT_LDG(nd + (2 + rp.sy) * kWideRow + r), fy = PT_LDG(nd + (3 - rp.sy) * kWideRow + r);
+    const float4 nz = PT_LDG(nd + (4 + rp.sz) * kWideRow + r), fz = PT_LDG(nd + (5 - rp.sz) * kWideRow + r);
+    const int4 c = PT_LDG(reinterpret_cast<const int4*>(nd + 6 * kWideRow + r));
+    t[4 * r + 0] = slab_nf(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, o, rp, tmin, tmax);
+    t[4 * r + 1] = slab_nf(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, o, rp, tmin, tmax);
+    t[4 * r + 2] = slab_nf(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, o, rp, tmin, tmax);
+    t[4 * r + 3] = slab_nf(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, o, rp, tmin, tmax);
+    code[4 * r + 0] = c.x;
+    code[4 * r + 1] = c.y;
+    code[4 * r + 2] = c.z;
+    code[4 * r + 3] = c.w;
+  }
   const float inf = as_float(0x7f800000);
-  const int n = (t[0] != inf) + (t[1] != inf) + (t[2] != inf) + (t[3] != inf);
-  cswap4(code, t, 0, 1);
-  cswap4(code, t, 2, 3);
-  cswap4(code, t, 0, 2);
-  cswap4(code, t, 1, 3);
-  cswap4(code, t, 1, 2);
+  int n = 0;
+#pragma unroll
+  for (int k = 0; k < kWide; ++k) n += t[k] != inf;
+  if constexpr (kWide == 4) {
+    cswap4(code, t, 0, 1);
+    cswap4(code, t, 2, 3);
+    cswap4(code, t, 0, 2);
+    cswap4(code, t, 1, 3);
+    cswap4(code, t, 1, 2);
+  }
   return n;
 }
-// Pushes the hit children after the nearest (far to near) and returns the nearest, or pops the next
-// target when no child was hit.
-PT_HD int node4_advance(int n, const int code[4], const float t[4], Stack4& stk, float tlimit, bool cull)
+// Pushes the hit children other than the nearest, farthest first (so that they pop nearest first),
+// and returns the nearest, or pops the next target when no child was hit.  4-wide: the children come
+// sorted; 8-wide: repeated selection of the farthest remaining hit child over registers.
+PT_HD int node4_advance(int n, const int code[kWide], const float t[kWide], Stack4& stk, float tlimit, bool cull)
 {
+  if constexpr (kWide == 4) {
 #pragma unroll
-  for (int j = 3; j >= 1; --j)
-    if (j < n) stack4_push(stk, code[j], t[j]);
-  return n ? code[0] : stack4_next(stk, tlimit, cull);
+    for (int j = 3; j >= 1; --j)
+      if (j < n) stack4_push(stk, code[j], t[j]);
+    return n ? code[0] : stack4_next(stk, tlimit, cull);
+  } else {
+    if (!n) return stack4_next(stk, tlimit, cull);
+    const float inf = as_float(0x7f800000);
+    unsigned m = 0;
+#pragma unroll
+    for (int k = 0; k < kWide; ++k) m |= (t[k] != inf ? 1u : 0u) << k;
+    while (popc32(m) > 1) {
+      float best = -1.0f;
+      int bc = 0;
+      unsigned bb = 0;
+#pragma unroll
+      for (int k = 0; k < kWide; ++k) {
+        const bool take = ((m >> k) & 1u) && t[k] > best;
+        best = take ? t[k] : best;
+        bc = take ? code[k] : bc;
+        bb = take ? 1u << k : bb;
+      }
+      stack4_push(stk, bc, best);
+      m &= ~bb;
+    }
+    int c = 0;
+#pragma unroll
+    for (int k = 0; k < kWide; ++k) c = (m >> k) & 1u ? code[k] : c;
+    return c;
+  }
 }
 // One closest-hit node step: cur must be a node; returns the next target (node, leaf or kDone4).
 template <class G> PT_HD int trav4_node_closest(const G& S, int cur, const float3& o, const RayPre& rp, float tmin, const Hit& h, Stack4& stk)
 {
-  int code[4];
-  float t[4];
+  int code[kWide];
+  float t[kWide];
   const int n = node4_hits(S, cur, o, rp, tmin, h.t, code, t);
   return node4_advance(n, code, t, stk, h.t, true);
 }
 template <class G> PT_HD int trav4_node_any(const G& S, int cur, const float3& o, const RayPre& rp, float tmin, float tmax, Stack4& stk)
 {
-  int code[4];
-  float t[4];
+  int code[kWide];
+  float t[kWide];
   const int n = node4_hits(S, cur, o, rp, tmin, tmax, code, t);
   return node4_advance(n, code, t, stk, tmax, false);
 }

@@ -1,5 +1,5 @@
 """The product's BVH builders and traversals (pt_bvh.cu, pt_scene.cuh: stackless BVH2, its short-stack
-variant, the 4-wide BVH with its ring-and-spill stack), compiled for the host by
+variant, the 4- and 8-wide BVHs with their ring-and-spill stack), compiled for the host by
 tests/native/host_trace.cu, against the brute-force oracle: closest-hit index, t and barycentrics and
 any-hit bit-identical, including rays aimed exactly at vertices and edges.  Runs without a GPU (the
 same code runs on the device in tests/test_render_gpu.py)."""
@@ -14,20 +14,23 @@ from oracle import oracle_ctypes as oc
 from open_rendering_framework_b200 import scenes
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SO = os.path.join(HERE, "native", "_build", "libhost_trace.so")
+SO = os.path.join(HERE, "native", "_build", "libhost_trace_w%d.so")
 SRC = [os.path.join(HERE, "native", "host_trace.cu"),
        os.path.join(HERE, "..", "open_rendering_framework_b200", "csrc", "pt_bvh.cu")]
 HDR = [os.path.join(HERE, "..", "open_rendering_framework_b200", "csrc", f) for f in ("pt_scene.cuh", "pt_math.cuh", "pt_bvh.h")]
 
 
-@pytest.fixture(scope="module")
-def host_lib():
+@pytest.fixture(scope="module", params=[4, 8], ids=["bvh4", "bvh8"])
+def host_lib(request):
+    # the wide BVH compiled at both widths (PT_BVH_WIDE), whichever the library uses
+    so = SO % request.param
     newest = max(os.path.getmtime(p) for p in SRC + HDR)
-    if not os.path.exists(SO) or os.path.getmtime(SO) < newest:
-        os.makedirs(os.path.dirname(SO), exist_ok=True)
+    if not os.path.exists(so) or os.path.getmtime(so) < newest:
+        os.makedirs(os.path.dirname(so), exist_ok=True)
         subprocess.run(["/usr/local/cuda/bin/nvcc", "-std=c++17", "-O2", "--fmad=false", "-Wno-deprecated-gpu-targets",
-                        "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-shared"] + SRC + ["-o", SO], check=True)
-    L = ctypes.CDLL(SO)
+                        "-DPT_BVH_WIDE=%d" % request.param, "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-shared"]
+                       + SRC + ["-o", so], check=True)
+    L = ctypes.CDLL(so)
     L.ht_build.restype = ctypes.c_void_p
     L.ht_build.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p]
     L.ht_free.argtypes = [ctypes.c_void_p]
