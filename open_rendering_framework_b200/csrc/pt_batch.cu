@@ -48,6 +48,7 @@ std::vector<uint64_t> graph_key(const Context& E, const PassLayout& L)
   k.push_back((uint64_t)L.passes);
   k.push_back(L.sss ? 1 : 0);
   k.push_back(L.layered ? 1 : 0);
+  k.push_back(L.ms ? 1 : 0);
   k.push_back(L.g_slots);
   k.push_back(L.items.size());
   for (size_t i = 0; i < L.chunk_paths.size(); ++i) {

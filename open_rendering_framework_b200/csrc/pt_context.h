@@ -115,6 +115,7 @@ struct SceneFacts {
   uint32_t pixels = 1, n_trans = 0, samples = 0;
   int max_depth = 0;
   bool layered = false;  // has a material of queue class QC_LAYERED
+  bool ms = false;       // has a conductor or rough dielectric of the multiple-scattering model
 };
 // A request: frames [first_frame, first_frame + n_frames) of scene `scene`.
 struct ItemReq {
@@ -130,6 +131,7 @@ struct PassLayout {
   int passes = 0;
   bool sss = false;
   bool layered = false;  // some scene of the pass has layered materials (k_shade_layered is launched)
+  bool ms = false;       // some scene of the pass has multiple-scattering conductors or dielectrics
   uint32_t g_slots = 0;
 };
 

@@ -40,7 +40,6 @@ constexpr int kWarps = kBlock / 32;
 #ifndef PT_TRACE_MIN_BLOCKS
 #define PT_TRACE_MIN_BLOCKS 8
 #endif
-
 // Per-path metadata in rng.w
 constexpr uint32_t META_DEPTH = 0xffffu;
 constexpr uint32_t META_EMIT = 1u << 16;
@@ -91,6 +90,7 @@ struct WfDev {
   const SceneDev* scenes;
   const ItemDev* items;
   uint32_t n_items;
+  uint32_t multi;  // 0: every path of the pass renders scenes[0]
   uint16_t* path_item;
 };
 
@@ -116,7 +116,11 @@ __device__ __forceinline__ uint32_t find_item(const ItemDev* items, uint32_t n, 
   }
   return lo;
 }
-__device__ __forceinline__ const SceneDev& scene_of(const WfDev& w, uint32_t pid) { return w.scenes[w.items[w.path_item[pid]].scene]; }
+__device__ __forceinline__ const SceneDev& scene_of(const WfDev& w, uint32_t pid)
+{
+  const uint32_t k = w.multi ? w.items[w.path_item[pid]].scene : 0u;
+  return w.scenes[k];
+}
 
 __device__ __forceinline__ unsigned lanemask_lt() { return (1u << (threadIdx.x & 31)) - 1u; }
 __device__ __forceinline__ unsigned long long* cnt64(uint32_t* cnt, int slot) { return reinterpret_cast<unsigned long long*>(cnt + slot); }
@@ -1091,9 +1095,9 @@ __global__ void __launch_bounds__(kBlock) k_shade_layered(WfDev w)
       if constexpr (kAdj) apply_pending(S, w, pid);
       eps = S.integ.scene_epsilon;
       const uint4 rg = w.rng[pid];
+      const float4 h = w.hit[pid], o = w.ray_o[pid], d4 = w.ray_d[pid], t4 = w.thr[pid];
       const int depth = (int)(rg.w & META_DEPTH);
       if (depth <= S.integ.max_depth) {  // both shaders end the path at depth > max_depth
-        const float4 h = w.hit[pid], o = w.ray_o[pid], d4 = w.ray_d[pid], t4 = w.thr[pid];
         const int prim = __float_as_int(h.w);
         const int4 info = __ldg(S.tri_info + prim);
         const MatDev& m = S.mats[info.w];
@@ -1187,10 +1191,12 @@ __global__ void __launch_bounds__(kBlock) k_shade_diffuse(WfDev w)
       const SceneDev& S = scene_of(w, pid);
       if constexpr (kAdj) apply_pending(S, w, pid);
       eps = S.integ.scene_epsilon;
+      // the path's records are loaded before the depth test (every queued id has them), so that their
+      // latency overlaps the scene lookup
       uint4 rg = w.rng[pid];
+      float4 h = w.hit[pid], o = w.ray_o[pid], d4 = w.ray_d[pid], t4 = w.thr[pid];
       int depth = (int)(rg.w & META_DEPTH);
       if (depth <= S.integ.max_depth) {
-        float4 h = w.hit[pid], o = w.ray_o[pid], d4 = w.ray_d[pid], t4 = w.thr[pid];
         int prim = __float_as_int(h.w);
         int4 info = __ldg(S.tri_info + prim);
         const MatDev& m = S.mats[info.w];
@@ -1263,7 +1269,9 @@ __global__ void __launch_bounds__(kBlock) k_shade_diffuse(WfDev w)
 // metallic_shader.cu:45-161.  Adjoint: a GGX roughness texel's gradient through the weight, with
 // the microfacet normal's sampling detached: d ln w / d alpha = d ln D(m) + d ln G1(wi) + d ln G1(wo)
 // for the Walter and the visible-normal models alike.
-template <bool kAdj>
+// kMS: some conductor of the pass uses the multiple-scattering model (else that code is left out,
+// which keeps the kernel's instruction footprint small).
+template <bool kAdj, bool kMS>
 __global__ void __launch_bounds__(kBlock) k_shade_metal(WfDev w)
 {
   __shared__ uint32_t sm[kWarps + 1];
@@ -1280,9 +1288,9 @@ __global__ void __launch_bounds__(kBlock) k_shade_metal(WfDev w)
       const SceneDev& S = scene_of(w, pid);
       if constexpr (kAdj) apply_pending(S, w, pid);
       uint4 rg = w.rng[pid];
+      float4 h = w.hit[pid], o = w.ray_o[pid], d4 = w.ray_d[pid];
       int depth = (int)(rg.w & META_DEPTH);
       if (depth < S.integ.max_depth) {
-        float4 h = w.hit[pid], o = w.ray_o[pid], d4 = w.ray_d[pid];
         int prim = __float_as_int(h.w);
         int4 info = __ldg(S.tri_info + prim);
         const MatDev& m = S.mats[info.w];
@@ -1304,7 +1312,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_metal(WfDev w)
         int capped = 0;
         float3 w_o, weight;
         bool go = true;
-        if (m.model == MULTISCATTERING) {
+        if (kMS && m.model == MULTISCATTERING) {
           uint32_t order = 0;
           float3 lwo = ms_conductor_sample(m.dist, to_local(w_i, normal), m.eta, m.inv_eta, a_x, a_y, seed, order, weight, &capped);
           w_o = to_world(lwo, normal);
@@ -1384,7 +1392,8 @@ __device__ __forceinline__ DirSeed smooth_glass_dir(float3 d, float3 normal, flo
 // inside, then the Fresnel choice between the mirror and the refracted direction about the shading
 // normal).  No parameters to differentiate: the adjoint only settles the pending gradient of the
 // previous vertex.
-template <bool kAdj>
+// kMS: some rough dielectric of the pass uses the multiple-scattering model (as for k_shade_metal).
+template <bool kAdj, bool kMS>
 __global__ void __launch_bounds__(kBlock) k_shade_glass(WfDev w)
 {
   __shared__ uint32_t sm[kWarps + 1];
@@ -1401,11 +1410,11 @@ __global__ void __launch_bounds__(kBlock) k_shade_glass(WfDev w)
       const SceneDev& S = scene_of(w, pid);
       if constexpr (kAdj) apply_pending(S, w, pid);
       uint4 rg = w.rng[pid];
+      float4 h = w.hit[pid], o = w.ray_o[pid], d4 = w.ray_d[pid];
       int depth = (int)(rg.w & META_DEPTH);
       // rough_transparent_shader.cu:68 ends paths at depth >= max_depth, transparent_shader.cu:50 at depth > max_depth
       if (depth < S.integ.max_depth ||
-          (depth == S.integ.max_depth && S.mats[__ldg(&S.tri_info[__float_as_int(w.hit[pid].w)].w)].type == MAT_TRANSPARENT)) {
-        float4 h = w.hit[pid], o = w.ray_o[pid], d4 = w.ray_d[pid];
+          (depth == S.integ.max_depth && S.mats[__ldg(&S.tri_info[__float_as_int(h.w)].w)].type == MAT_TRANSPARENT)) {
         int prim = __float_as_int(h.w);
         int4 info = __ldg(S.tri_info + prim);
         const MatDev& m = S.mats[info.w];
@@ -1435,7 +1444,7 @@ __global__ void __launch_bounds__(kBlock) k_shade_glass(WfDev w)
           t = ds.seed;
         } else if (go) {
           float z1 = rnd_tea(t), z2 = rnd_tea(t);
-          if (m.model == MULTISCATTERING) {  // :100-120
+          if (kMS && m.model == MULTISCATTERING) {  // :100-120
             uint32_t order = 0;
             float3 lwo = ms_dielectric_sample(m.dist, to_local(w_i, normal), 1.0f / ior, rough, rough, t, order, &capped);
             w_o = to_world(lwo, normal);
@@ -1653,9 +1662,9 @@ __global__ void __launch_bounds__(kBlock) k_shade_translucent(WfDev w)
       const SceneDev& S = scene_of(w, pid);
       if constexpr (kAdj) apply_pending(S, w, pid);
       uint4 rg = w.rng[pid];
+      float4 h = w.hit[pid], o = w.ray_o[pid], d4 = w.ray_d[pid];
       int depth = (int)(rg.w & META_DEPTH);
       if (depth <= S.integ.max_depth) {
-        float4 h = w.hit[pid], o = w.ray_o[pid], d4 = w.ray_d[pid];
         int prim = __float_as_int(h.w);
         int4 info = __ldg(S.tri_info + prim);
         const MatDev& m = S.mats[info.w];
@@ -2264,6 +2273,7 @@ SceneFacts scene_facts(const Context& c)
   f.max_depth = c.integ.max_depth;
   for (const MatDev& m : c.mats)
     if (m.type == MAT_LAMBERTIAN_INTERFACE || m.type == MAT_ROUGH_DIFFUSE) f.layered = true;
+    else if ((m.type == MAT_METAL || m.type == MAT_ROUGH_GLASS) && m.model == MULTISCATTERING) f.ms = true;
   return f;
 }
 
@@ -2274,6 +2284,7 @@ PassLayout plan_pass(const std::vector<SceneFacts>& facts, const std::vector<Ite
   for (const SceneFacts& f : facts) {
     L.passes = std::max(L.passes, f.max_depth + 2);
     L.layered = L.layered || f.layered;
+    L.ms = L.ms || f.ms;
     max_pixels = std::max(max_pixels, f.pixels);
     if (f.n_trans) {
       L.sss = true;
@@ -2351,6 +2362,21 @@ pt_status pass_resources(Context& E, const PassLayout& L, const std::vector<Scen
 // the camera paths, the deferred gathers and the accumulation.  Only kernel launches and memsets of
 // device state: the whole sequence can be captured into a CUDA graph.  multi: the pass spans
 // several scenes (the traversal kernels then read each ray's scene from the table; otherwise S0).
+// One full wave of a grid-stride kernel: the SM count times the blocks of kBlock threads that fit on an
+// SM at the kernel's register and shared-memory use (cached per kernel and thread).
+template <class K> int full_wave(K kernel)
+{
+  static thread_local std::vector<std::pair<const void*, int>> cache;
+  const void* key = reinterpret_cast<const void*>(kernel);
+  for (const auto& e : cache)
+    if (e.first == key) return e.second;
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, kBlock, 0) != cudaSuccess || blocks < 1) blocks = 8;
+  const int grid = sm_count() * blocks;
+  cache.emplace_back(key, grid);
+  return grid;
+}
+
 pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool multi, bool allow_events, bool adjoint)
 {
   Context& c = E;
@@ -2379,6 +2405,7 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
   w.g_d = L.sss ? wf.g_d.as<float4>() : nullptr;
   w.g_slots = L.sss ? wf.gather_slots : 0;
   w.scenes = c.d_scene_tab.as<SceneDev>();
+  w.multi = multi ? 1u : 0u;
   w.path_item = wf.path_item.as<uint16_t>();
   w.adj_a = adjoint ? wf.adj_a.as<float4>() : nullptr;
   w.adj_b = adjoint ? wf.adj_b.as<float4>() : nullptr;
@@ -2464,27 +2491,37 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
       k_bin_scatter<<<grid_bin, kBinThreads, 0, c.stream>>>(w);
       count_launch(3);
       if (adjoint) {
-        k_shade_miss<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
-        k_shade_light<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
-        k_shade_diffuse<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
-        k_shade_metal<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
-        k_shade_glass<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
+        k_shade_miss<true><<<full_wave(k_shade_miss<true>), kBlock, 0, c.stream>>>(w);
+        k_shade_light<true><<<full_wave(k_shade_light<true>), kBlock, 0, c.stream>>>(w);
+        k_shade_diffuse<true><<<full_wave(k_shade_diffuse<true>), kBlock, 0, c.stream>>>(w);
+        if (L.ms) {
+          k_shade_metal<true, true><<<full_wave(k_shade_metal<true, true>), kBlock, 0, c.stream>>>(w);
+          k_shade_glass<true, true><<<full_wave(k_shade_glass<true, true>), kBlock, 0, c.stream>>>(w);
+        } else {
+          k_shade_metal<true, false><<<full_wave(k_shade_metal<true, false>), kBlock, 0, c.stream>>>(w);
+          k_shade_glass<true, false><<<full_wave(k_shade_glass<true, false>), kBlock, 0, c.stream>>>(w);
+        }
       } else {
-        k_shade_miss<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
-        k_shade_light<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
-        k_shade_diffuse<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
-        k_shade_metal<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
-        k_shade_glass<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
+        k_shade_miss<false><<<full_wave(k_shade_miss<false>), kBlock, 0, c.stream>>>(w);
+        k_shade_light<false><<<full_wave(k_shade_light<false>), kBlock, 0, c.stream>>>(w);
+        k_shade_diffuse<false><<<full_wave(k_shade_diffuse<false>), kBlock, 0, c.stream>>>(w);
+        if (L.ms) {
+          k_shade_metal<false, true><<<full_wave(k_shade_metal<false, true>), kBlock, 0, c.stream>>>(w);
+          k_shade_glass<false, true><<<full_wave(k_shade_glass<false, true>), kBlock, 0, c.stream>>>(w);
+        } else {
+          k_shade_metal<false, false><<<full_wave(k_shade_metal<false, false>), kBlock, 0, c.stream>>>(w);
+          k_shade_glass<false, false><<<full_wave(k_shade_glass<false, false>), kBlock, 0, c.stream>>>(w);
+        }
       }
       count_launch(6);
       if (L.layered) {
-        if (adjoint) k_shade_layered<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
-        else k_shade_layered<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
+        if (adjoint) k_shade_layered<true><<<full_wave(k_shade_layered<true>), kBlock, 0, c.stream>>>(w);
+        else k_shade_layered<false><<<full_wave(k_shade_layered<false>), kBlock, 0, c.stream>>>(w);
         count_launch();
       }
       if (L.sss) {
-        if (adjoint) k_shade_translucent<true><<<grid_shade, kBlock, 0, c.stream>>>(w);
-        else k_shade_translucent<false><<<grid_shade, kBlock, 0, c.stream>>>(w);
+        if (adjoint) k_shade_translucent<true><<<full_wave(k_shade_translucent<true>), kBlock, 0, c.stream>>>(w);
+        else k_shade_translucent<false><<<full_wave(k_shade_translucent<false>), kBlock, 0, c.stream>>>(w);
         count_launch();
       }
       if (c.opt.extend_mode == 1) {

@@ -546,6 +546,7 @@ constexpr int kMaxDepthWide = kWide == 4 ? 40 : 24;  // levels the stack is size
 constexpr int kRing4 = 8;
 constexpr int kSpill4 = (kWide - 1) * kMaxDepthWide + 8;  // kWide - 1 pending children per level
 constexpr int kDone4 = 0x7fffffff;
+
 struct Stack4 {
   uint2* ring;
   uint2* spill;
@@ -618,9 +619,10 @@ PT_HD int popc32(unsigned m)
 #endif
 }
 // Tests the kWide children of node `node`: their codes and entry distances (+inf for a miss); with
-// kWide == 4 sorted near to far by a five-comparator network, returning the count of hits.
-template <class G> PT_HD int node4_hits(const G& S, int node, const float3& o, const RayPre& rp, float tmin, float tmax, int code[kWide],
-                                        float t[kWide])
+// kSort and kWide == 4 sorted near to far by a five-comparator network (else in slot order),
+// returning the count of hits.
+template <bool kSort = true, class G>
+PT_HD int node4_hits(const G& S, int node, const float3& o, const RayPre& rp, float tmin, float tmax, int code[kWide], float t[kWide])
 {
   const float4* nd = S.nodes4 + kWideStride * (size_t)node;
 #pragma unroll
@@ -642,7 +644,7 @@ template <class G> PT_HD int node4_hits(const G& S, int node, const float3& o, c
   int n = 0;
 #pragma unroll
   for (int k = 0; k < kWide; ++k) n += t[k] != inf;
-  if constexpr (kWide == 4) {
+  if constexpr (kSort && kWide == 4) {
     cswap4(code, t, 0, 1);
     cswap4(code, t, 2, 3);
     cswap4(code, t, 0, 2);
@@ -695,12 +697,26 @@ template <class G> PT_HD int trav4_node_closest(const G& S, int cur, const float
   const int n = node4_hits(S, cur, o, rp, tmin, h.t, code, t);
   return node4_advance(n, code, t, stk, h.t, true);
 }
+// Any-hit node step.  Whether some triangle lies in (tmin, tmax) does not depend on the order in which
+// the hit children are visited, so they are taken in slot order without sorting: all but the last hit
+// child are pushed, the last is visited next.
 template <class G> PT_HD int trav4_node_any(const G& S, int cur, const float3& o, const RayPre& rp, float tmin, float tmax, Stack4& stk)
 {
   int code[kWide];
   float t[kWide];
-  const int n = node4_hits(S, cur, o, rp, tmin, tmax, code, t);
-  return node4_advance(n, code, t, stk, tmax, false);
+  node4_hits<false>(S, cur, o, rp, tmin, tmax, code, t);
+  const float inf = as_float(0x7f800000);
+  int next = kDone4;
+  float tnext = 0.0f;
+#pragma unroll
+  for (int k = 0; k < kWide; ++k) {
+    if (t[k] != inf) {
+      if (next != kDone4) stack4_push(stk, next, tnext);
+      next = code[k];
+      tnext = t[k];
+    }
+  }
+  return next != kDone4 ? next : stack4_next(stk, tmax, false);
 }
 
 template <class G> PT_HD Hit trace_closest(const G& S, const float3& o, const float3& d, float tmin, float tmax)

@@ -21,10 +21,10 @@
 // loadHDRTexture(path): the float4 buffer (row j = the file's scanline ny-1-j) and its size.  The
 // reference leaves the fourth channel uninitialised, so only RGB is defined.  Returns 0 when the
 // loader failed (the reference then installs a 1x1 texture of the default color).
-// The reference's header parsing misreads the resolution line of its own data/CedarCity.hdr (and then
-// throws a C string that nothing catches) when the process's C or C++ locale is not the classic one
-// (as after numpy has been imported into a Python process); it is therefore run under the classic
-// "C" locale, for the C library and for the streams it opens.
+// The reference's readers parse numbers with the C library and with iostreams, whose results depend on
+// the process's C and C++ locales (a locale with a decimal comma reads "1.5" as 1); they are therefore
+// run under the classic "C" locale, for the C library and for the streams they open, whatever locale
+// the calling process has set.
 struct CLocale {
   std::string saved;
   std::locale saved_cpp;
