@@ -277,7 +277,7 @@ pt_status pt_get_render_stats(pt_ctx* ctx, pt_render_stats* out);
  *   "differentiable" 1 = renders keep the forward state pt_render_adjoint needs (default 0)
  *   "extend_mode"  0 = one ray per thread with block-aggregated queue appends,
  *                  1 = persistent warps that refill finished lanes with new rays (default)
- *   "refill"       persistent kernels refill a warp when at least this many lanes are idle (1..32, default 24)
+ *   "refill"       persistent kernels refill a warp when at least this many lanes are idle (1..32, default 20)
  *   "bvh4"         1 = the persistent kernels walk the 4-wide BVH (default), 0 = the BVH2
  *   "bvh_trav_cost_milli"  SAH cost of a node step x 1000 relative to a triangle test (default 1200) and
  *   "bvh_max_leaf"         the largest leaf the SAH may choose (1..15, default 8): applied by the next pt_build */

@@ -292,8 +292,8 @@ pt_status pt_batch_autotune(pt_batch* b, uint32_t frames_per_trial, pt_tune_resu
   struct Cand { int mode, refill; uint64_t max_paths; };
   std::vector<Cand> cands;
   for (uint64_t mp : {1ull << 22, 1ull << 23, 1ull << 24})
-    for (int r : {8, 16, 24, 32}) cands.push_back({1, r, mp});
-  cands.push_back({0, 24, 1ull << 23});
+    for (int r : {16, 20, 24}) cands.push_back({1, r, mp});
+  cands.push_back({0, 20, 1ull << 23});
   float best = 0.0f;
   Cand win = cands.front();
   uint32_t trials = 0;

@@ -140,7 +140,7 @@ enum ProfKind { PROF_EXTEND = 0, PROF_GATHER = 1 };
 // Tunable launch options (pt_set_option); the autotuner searches over these.
 struct Options {
   int extend_mode = 1;  // 0: one ray per thread, block-aggregated appends; 1: persistent warps with ray refill
-  int refill = 24;      // persistent kernels: refill when at least this many lanes of a warp are idle (1..32)
+  int refill = 20;      // persistent kernels: refill when at least this many lanes of a warp are idle (1..32)
 };
 
 struct Context {
