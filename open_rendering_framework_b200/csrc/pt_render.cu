@@ -36,10 +36,15 @@ namespace pt {
 
 constexpr int kBlock = 128;
 constexpr int kWarps = kBlock / 32;
-// Resident blocks per SM the persistent traversal kernels are compiled for (register budget).
-#ifndef PT_TRACE_MIN_BLOCKS
-#define PT_TRACE_MIN_BLOCKS 8
+// Threads per block of the persistent traversal kernels, and the resident blocks per SM they are
+// compiled for (register budget: 1,024 threads per SM at 64 registers).
+#ifndef PT_TRACE_BLOCK
+#define PT_TRACE_BLOCK 128
 #endif
+#ifndef PT_TRACE_MIN_BLOCKS
+#define PT_TRACE_MIN_BLOCKS (1024 / PT_TRACE_BLOCK)
+#endif
+constexpr int kTraceBlock = PT_TRACE_BLOCK;
 // Per-path metadata in rng.w
 constexpr uint32_t META_DEPTH = 0xffffu;
 constexpr uint32_t META_EMIT = 1u << 16;
@@ -524,9 +529,9 @@ __global__ void __launch_bounds__(kBlock) k_extend(WfDev w)
 // kW4: the 4-wide BVH (node steps of pt_scene.cuh trav4_*, the next target `cur` a node, a leaf or
 // kDone4); otherwise the BVH2 with the postponed-leaf pair (leafA, leafB).
 template <bool kMulti, bool kW4>
-__global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_extend_persistent(SceneDev S0, WfDev w, int refill)
+__global__ void __launch_bounds__(kTraceBlock, PT_TRACE_MIN_BLOCKS) k_extend_persistent(SceneDev S0, WfDev w, int refill)
 {
-  __shared__ uint2 stk[(kW4 ? kRing4 : kShortStack) * kBlock];
+  __shared__ uint2 stk[(kW4 ? kRing4 : kShortStack) * kTraceBlock];
   const uint32_t n = w.cnt[w.in_slot];
   uint32_t* fetch = w.cnt + CNT_FETCH_EXT;
   TravGeom g = trav_geom(S0);
@@ -543,11 +548,11 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_extend_persiste
   Hit h;
   h.t = 0.0f; h.u = h.v = 0.0f; h.prim = -1;
   TravState st;
-  trav_init(st, stk + threadIdx.x, kBlock);
+  trav_init(st, stk + threadIdx.x, kTraceBlock);
   uint32_t leafA = 0, leafB = 0;
   uint2 spill4[kW4 ? kSpill4 : 1];
   Stack4 s4;
-  stack4_init(s4, stk + threadIdx.x, kBlock, spill4);
+  stack4_init(s4, stk + threadIdx.x, kTraceBlock, spill4);
   int cur = kDone4;
   for (;;) {
     unsigned idle = __ballot_sync(0xffffffffu, !has);
@@ -576,10 +581,10 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_extend_persiste
           h.u = h.v = 0.0f;
           h.prim = -1;
           if constexpr (kW4) {
-            stack4_init(s4, stk + threadIdx.x, kBlock, spill4);
+            stack4_init(s4, stk + threadIdx.x, kTraceBlock, spill4);
             cur = 0;
           } else {
-            trav_init(st, stk + threadIdx.x, kBlock);
+            trav_init(st, stk + threadIdx.x, kTraceBlock);
           }
           has = true;
           done = false;
@@ -815,9 +820,9 @@ __device__ __forceinline__ void shadow_unoccluded(const SceneDev& S, const WfDev
 
 // Persistent any-hit kernel for the shadow queue (same ray replacement and BVH choice).
 template <bool kMulti, bool kAdj, bool kW4>
-__global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_shadow_persistent(SceneDev S0, WfDev w, int refill)
+__global__ void __launch_bounds__(kTraceBlock, PT_TRACE_MIN_BLOCKS) k_shadow_persistent(SceneDev S0, WfDev w, int refill)
 {
-  __shared__ uint2 stk[(kW4 ? kRing4 : kShortStack) * kBlock];
+  __shared__ uint2 stk[(kW4 ? kRing4 : kShortStack) * kTraceBlock];
   const uint32_t n = w.cnt[CNT_SHADOW];
   uint32_t* fetch = w.cnt + CNT_FETCH_SH;
   TravGeom g = trav_geom(S0);
@@ -831,10 +836,10 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_shadow_persiste
   rp.inv = f3s(0.0f);
   rp.sx = rp.sy = rp.sz = 0;
   TravState st;
-  trav_init(st, stk + threadIdx.x, kBlock);
+  trav_init(st, stk + threadIdx.x, kTraceBlock);
   uint2 spill4[kW4 ? kSpill4 : 1];
   Stack4 s4;
-  stack4_init(s4, stk + threadIdx.x, kBlock, spill4);
+  stack4_init(s4, stk + threadIdx.x, kTraceBlock, spill4);
   int cur = kDone4;
   for (;;) {
     unsigned idle = __ballot_sync(0xffffffffu, !has);
@@ -855,10 +860,10 @@ __global__ void __launch_bounds__(kBlock, PT_TRACE_MIN_BLOCKS) k_shadow_persiste
           tmax = d4.w;
           rp = ray_pre(o, d);
           if constexpr (kW4) {
-            stack4_init(s4, stk + threadIdx.x, kBlock, spill4);
+            stack4_init(s4, stk + threadIdx.x, kTraceBlock, spill4);
             cur = 0;
           } else {
-            trav_init(st, stk + threadIdx.x, kBlock);
+            trav_init(st, stk + threadIdx.x, kTraceBlock);
           }
           has = true;
           res = 0;
@@ -2424,8 +2429,8 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
   const bool w4 = E.pass_w4;
   int occ_ext = 0, occ_sh = 0;
   auto occupancy = [&](auto ext, auto sh) -> pt_status {
-    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, ext, kBlock, 0), "occupancy");
-    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, sh, kBlock, 0), "occupancy");
+    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, ext, kTraceBlock, 0), "occupancy");
+    PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, sh, kTraceBlock, 0), "occupancy");
     return PT_OK;
   };
   pt_status ost;
@@ -2476,11 +2481,11 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
       if ((st = prof_begin(PROF_EXTEND)) != PT_OK) return st;
       if (c.opt.extend_mode == 1) {
         if (w4) {
-          if (multi) k_extend_persistent<true, true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-          else k_extend_persistent<false, true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          if (multi) k_extend_persistent<true, true><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          else k_extend_persistent<false, true><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
         } else {
-          if (multi) k_extend_persistent<true, false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-          else k_extend_persistent<false, false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          if (multi) k_extend_persistent<true, false><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          else k_extend_persistent<false, false><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
         }
       } else {
         k_extend<<<grid_trace, kBlock, 0, c.stream>>>(w);
@@ -2526,15 +2531,15 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
       }
       if (c.opt.extend_mode == 1) {
         if (w4) {
-          if (multi && adjoint) k_shadow_persistent<true, true, true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-          else if (multi) k_shadow_persistent<true, false, true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-          else if (adjoint) k_shadow_persistent<false, true, true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-          else k_shadow_persistent<false, false, true><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          if (multi && adjoint) k_shadow_persistent<true, true, true><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          else if (multi) k_shadow_persistent<true, false, true><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          else if (adjoint) k_shadow_persistent<false, true, true><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          else k_shadow_persistent<false, false, true><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
         } else {
-          if (multi && adjoint) k_shadow_persistent<true, true, false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-          else if (multi) k_shadow_persistent<true, false, false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-          else if (adjoint) k_shadow_persistent<false, true, false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-          else k_shadow_persistent<false, false, false><<<grid_persist, kBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          if (multi && adjoint) k_shadow_persistent<true, true, false><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          else if (multi) k_shadow_persistent<true, false, false><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          else if (adjoint) k_shadow_persistent<false, true, false><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          else k_shadow_persistent<false, false, false><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
         }
       } else {
         if (adjoint) k_shadow<true><<<grid_trace, kBlock, 0, c.stream>>>(w);

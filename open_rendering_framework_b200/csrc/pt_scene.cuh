@@ -543,7 +543,11 @@ static_assert(kWide == 4 || kWide == 8, "the wide BVH has 4 or 8 children per no
 constexpr int kWideRow = kWide / 4;                  // float4 per plane row
 constexpr int kWideStride = kWide == 4 ? 8 : 14;     // float4 per node
 constexpr int kMaxDepthWide = kWide == 4 ? 40 : 24;  // levels the stack is sized for
-constexpr int kRing4 = 8;
+#ifndef PT_RING4
+#define PT_RING4 8
+#endif
+constexpr int kRing4 = PT_RING4;  // a power of two
+static_assert((kRing4 & (kRing4 - 1)) == 0, "the ring stack's size is a power of two");
 constexpr int kSpill4 = (kWide - 1) * kMaxDepthWide + 8;  // kWide - 1 pending children per level
 constexpr int kDone4 = 0x7fffffff;
 
