@@ -14,21 +14,23 @@ from oracle import oracle_ctypes as oc
 from open_rendering_framework_b200 import scenes
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SO = os.path.join(HERE, "native", "_build", "libhost_trace_w%d.so")
+SO = os.path.join(HERE, "native", "_build", "libhost_trace_w%d_q%d.so")
 SRC = [os.path.join(HERE, "native", "host_trace.cu"),
        os.path.join(HERE, "..", "open_rendering_framework_b200", "csrc", "pt_bvh.cu")]
 HDR = [os.path.join(HERE, "..", "open_rendering_framework_b200", "csrc", f) for f in ("pt_scene.cuh", "pt_math.cuh", "pt_bvh.h")]
 
 
-@pytest.fixture(scope="module", params=[4, 8], ids=["bvh4", "bvh8"])
+@pytest.fixture(scope="module", params=[(4, 0), (8, 0), (4, 1)], ids=["bvh4", "bvh8", "bvh4q"])
 def host_lib(request):
-    # the wide BVH compiled at both widths (PT_BVH_WIDE), whichever the library uses
-    so = SO % request.param
+    # the wide BVH compiled at both widths (PT_BVH_WIDE) and with quantized 4-wide nodes (PT_BVH_QUANT),
+    # whichever the library uses
+    width, quant = request.param
+    so = SO % (width, quant)
     newest = max(os.path.getmtime(p) for p in SRC + HDR)
     if not os.path.exists(so) or os.path.getmtime(so) < newest:
         os.makedirs(os.path.dirname(so), exist_ok=True)
         subprocess.run(["/usr/local/cuda/bin/nvcc", "-std=c++17", "-O2", "--fmad=false", "-Wno-deprecated-gpu-targets",
-                        "-DPT_BVH_WIDE=%d" % request.param, "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-shared"]
+                        "-DPT_BVH_WIDE=%d" % width, "-DPT_BVH_QUANT=%d" % quant, "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-shared"]
                        + SRC + ["-o", so], check=True)
     L = ctypes.CDLL(so)
     L.ht_build.restype = ctypes.c_void_p
@@ -103,3 +105,31 @@ def test_single_triangle_and_degenerate_scenes(host_lib):
         host_lib.ht_free(h)
         assert prim[0] == 0 and t[0] == 1.0 and anyh[0] == 1
         assert prim[1] == -1 and anyh[1] == 0
+
+
+def test_host_traversal_far_from_origin(host_lib):
+    # the scene shrunk 100x and moved 500 units away from the origin: node boxes a few thousand ulps
+    # wide, so the quantized boxes' grids and the transformed slab test run at their coarsest
+    data = scenes.single_scene(width=8, height=8, metal_subdiv=3, glass_subdiv=2)
+    for m in data.meshes:
+        m.positions = np.ascontiguousarray(m.positions * np.float32(0.01) + np.float32(500.0), np.float32)
+    tp, _, _ = data.flat_triangles()
+    h = host_lib.ht_build(oc.fp(tp), len(tp), None)
+    assert h
+    rays = edge_and_random_rays(tp, 4000, 5)
+    rays[:, 0:3] = rays[:, 0:3] * np.float32(0.01) + np.float32(500.0)
+    rays[:, 3] = 1e-6
+    d = (tp[np.random.default_rng(5).integers(0, len(tp), len(rays)), 0:3] - rays[:, 0:3]).astype(np.float64)
+    rays[:, 4:7] = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    n = len(rays)
+    prim4, t4 = np.empty(n, np.int32), np.empty(n, np.float32)
+    bary4, anyh4 = np.empty((n, 2), np.float32), np.empty(n, np.int32)
+    max_sp = ctypes.c_int()
+    assert host_lib.ht_trace4(h, oc.fp(rays), n, oc.fp(prim4), oc.fp(t4), oc.fp(bary4), oc.fp(anyh4), ctypes.byref(max_sp)) == 0
+    host_lib.ht_free(h)
+    bp, bt, bb, ba = oc.OracleScene(data).trace(rays, brute=True)
+    assert np.mean(bp >= 0) > 0.5
+    assert np.array_equal(prim4, bp)
+    assert np.array_equal(t4.view(np.uint32), bt.view(np.uint32))
+    assert np.array_equal(bary4.view(np.uint32), bb.view(np.uint32))
+    assert np.array_equal(anyh4, ba)
