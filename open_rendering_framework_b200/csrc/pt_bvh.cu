@@ -275,36 +275,6 @@ bool build_bvh(const float* tri_pos, uint32_t n_tris, BvhHost& out, const BvhPar
   return out.depth < 64;
 }
 
-// Quantization of one axis of a quantized 4-wide node (layout and the slab test in pt_scene.cuh): the
-// smallest power of two s and a float origin p such that every child plane lands on the grid
-// p + q s (q in 0..255) at least one whole quantum outside its box: q_lo = floor((lo - p) / s - 1),
-// q_hi = ceil((hi - p) / s + 1), with p <= min lo - 2 s.  Worked in double, where these differences of
-// floats are exact or off by far less than the quantum.
-static void quantize_axis(const float* lo, const float* hi, int n, float& p_out, float& s_out, uint8_t* qlo, uint8_t* qhi)
-{
-  double m = lo[0], M = hi[0];
-  for (int j = 1; j < n; ++j) {
-    m = std::min(m, (double)lo[j]);
-    M = std::max(M, (double)hi[j]);
-  }
-  const double ext = std::max(0.0, M - m);
-  int e = ext > 0.0 ? (int)std::ceil(std::log2(ext / 250.0)) - 1 : -126;
-  e = std::max(e, -126);
-  for (;; ++e) {
-    const double s = std::ldexp(1.0, e);
-    float p = (float)(m - 2.0 * s);
-    if ((double)p > m - 2.0 * s) p = std::nextafter(p, -INFINITY);
-    if (std::ceil((M - (double)p) / s + 1.0) > 255.0) continue;
-    p_out = p;
-    s_out = (float)s;
-    for (int j = 0; j < n; ++j) {
-      qlo[j] = (uint8_t)std::floor(((double)lo[j] - (double)p) / s - 1.0);
-      qhi[j] = (uint8_t)std::ceil(((double)hi[j] - (double)p) / s + 1.0);
-    }
-    return;
-  }
-}
-
 // Collapse: starting from a BVH2 node's two children, the internal child of largest surface area is
 // replaced by its own two children until there are four or no internal child is left (the usual
 // greedy collapse of a binary SAH tree into a wide one).
@@ -360,41 +330,6 @@ bool build_bvh4(const BvhHost& b2, std::vector<float4>& out4, int& depth4)
       else codes[j] = kids[j].code;
     }
     float4* nd = out4.data() + kWideStride * (size_t)me;
-    if constexpr (kQuant) {
-      float p[3], s[3];
-      uint32_t qlo[3] = {0, 0, 0}, qhi[3] = {0, 0, 0};
-      // children that hold triangles; empty slots and empty leaves (the BVH2 parks their boxes at
-      // 1e30) get inverted boxes
-      int full[kWide], nf = 0;
-      for (int j = 0; j < nk; ++j)
-        if (kids[j].code >= 0 || (kids[j].code & 15) != 0) full[nf++] = j;
-      for (int axis = 0; axis < 3; ++axis) {
-        float lo[kWide], hi[kWide];
-        for (int f = 0; f < nf; ++f) {
-          lo[f] = kids[full[f]].lo[axis];
-          hi[f] = kids[full[f]].hi[axis];
-        }
-        uint8_t ql[kWide], qh[kWide];
-        if (nf) quantize_axis(lo, hi, nf, p[axis], s[axis], ql, qh);
-        else p[axis] = 0.0f, s[axis] = 1.0f;
-        for (int f = 0; f < nf; ++f) {
-          qlo[axis] |= (uint32_t)ql[f] << (8 * full[f]);
-          qhi[axis] |= (uint32_t)qh[f] << (8 * full[f]);
-        }
-        for (int j = 0; j < kWide; ++j) {
-          bool isfull = false;
-          for (int f = 0; f < nf; ++f) isfull = isfull || full[f] == j;
-          if (!isfull) qlo[axis] |= 255u << (8 * j);
-        }
-      }
-      auto fbits = [](uint32_t w) { float f; memcpy(&f, &w, 4); return f; };
-      nd[0] = make_float4(p[0], p[1], p[2], s[0]);
-      nd[1] = make_float4(fbits(qlo[0]), fbits(qhi[0]), fbits(qlo[1]), fbits(qhi[1]));
-      nd[2] = make_float4(fbits(qlo[2]), fbits(qhi[2]), s[1], s[2]);
-      int4 c4 = make_int4(codes[0], codes[1], codes[2], codes[3]);
-      memcpy(&nd[3], &c4, sizeof(c4));
-      return me;
-    }
     auto comp = [&](int j, int axis, bool lo) { return j < nk ? (lo ? kids[j].lo[axis] : kids[j].hi[axis]) : 1e30f; };
     for (int axis = 0; axis < 3; ++axis)
       for (int r = 0; r < kWideRow; ++r) {

@@ -541,27 +541,8 @@ template <class G> PT_HD bool trav_node_any(const G& S, const float3& o, const R
 #endif
 constexpr int kWide = PT_BVH_WIDE;
 static_assert(kWide == 4 || kWide == 8, "the wide BVH has 4 or 8 children per node");
-// Quantized 4-wide nodes (PT_BVH_QUANT=1, 4-wide only): 64 bytes per node instead of 128.
-//   float4 0: (p.x, p.y, p.z, s.x)         p = the node's grid origin, s = 2^e per axis
-//   float4 1: words lo.x, hi.x, lo.y, hi.y  (byte k = child k's plane in quanta: plane = p + q * s)
-//   float4 2: words lo.z, hi.z, then s.y, s.z
-//   int4   3: the four child codes
-// The builder pads every child box by at least one quantum on every side (quantize_axis in
-// pt_bvh.cu).  The slab test transforms the ray instead of the planes: per node and axis
-// a = (p - o) / d - 2^23 s / d and b = s / d, then per plane t = fma(2^23 + q, b, a), where 2^23 + q
-// is the byte spliced into the mantissa of 2^23.  Against the exact distance to the padded plane
-// this is off by at most ~6 ulp of t plus 0.51 quanta (the rounding of a), which the padding covers,
-// so the test is at least as permissive as the robust slab test of the unpadded box.  A zero
-// direction component makes b infinite and every distance of that axis NaN, which fminf / fmaxf
-// drop: that axis then culls nothing.  Empty slots carry inverted boxes (lo 255, hi 0) over leaves
-// of no triangles.
-#ifndef PT_BVH_QUANT
-#define PT_BVH_QUANT 0
-#endif
-constexpr bool kQuant = PT_BVH_QUANT != 0 && kWide == 4;
-static_assert(PT_BVH_QUANT == 0 || kWide == 4, "quantized nodes are 4-wide");
 constexpr int kWideRow = kWide / 4;                  // float4 per plane row
-constexpr int kWideStride = kQuant ? 4 : (kWide == 4 ? 8 : 14);  // float4 per node
+constexpr int kWideStride = kWide == 4 ? 8 : 14;     // float4 per node
 constexpr int kMaxDepthWide = kWide == 4 ? 40 : 24;  // levels the stack is sized for
 #ifndef PT_RING4
 #define PT_RING4 8
@@ -645,65 +626,10 @@ PT_HD int popc32(unsigned m)
 // Tests the kWide children of node `node`: their codes and entry distances (+inf for a miss); with
 // kSort and kWide == 4 sorted near to far by a five-comparator network (else in slot order),
 // returning the count of hits.
-// 2^23 + byte k of w, as a float (exact).
-PT_HD float quant_byte(uint32_t w, int k)
-{
-#ifdef __CUDA_ARCH__
-  return __int_as_float((int)__byte_perm(w, 0x4B000000u, 0x7440u | (unsigned)k));
-#else
-  return as_float((int)(0x4B000000u | ((w >> (8 * k)) & 0xffu)));
-#endif
-}
-PT_HD float fma_rn(float a, float b, float c)
-{
-#ifdef __CUDA_ARCH__
-  return __fmaf_rn(a, b, c);
-#else
-  return fmaf(a, b, c);
-#endif
-}
 template <bool kSort = true, class G>
 PT_HD int node4_hits(const G& S, int node, const float3& o, const RayPre& rp, float tmin, float tmax, int code[kWide], float t[kWide])
 {
   const float4* nd = S.nodes4 + kWideStride * (size_t)node;
-  if constexpr (kQuant) {
-    const float4 h0 = PT_LDG(nd), h1 = PT_LDG(nd + 1), h2 = PT_LDG(nd + 2);
-    const int4 c = PT_LDG(reinterpret_cast<const int4*>(nd + 3));
-    const float bx = h0.w * rp.inv.x, by = h2.z * rp.inv.y, bz = h2.w * rp.inv.z;
-    const float ax = fma_rn(-8388608.0f, bx, (h0.x - o.x) * rp.inv.x);
-    const float ay = fma_rn(-8388608.0f, by, (h0.y - o.y) * rp.inv.y);
-    const float az = fma_rn(-8388608.0f, bz, (h0.z - o.z) * rp.inv.z);
-    const uint32_t lx = (uint32_t)as_int(h1.x), hx = (uint32_t)as_int(h1.y), ly = (uint32_t)as_int(h1.z), hy = (uint32_t)as_int(h1.w);
-    const uint32_t lz = (uint32_t)as_int(h2.x), hz = (uint32_t)as_int(h2.y);
-    const uint32_t nx = rp.sx ? hx : lx, fx = rp.sx ? lx : hx;
-    const uint32_t ny = rp.sy ? hy : ly, fy = rp.sy ? ly : hy;
-    const uint32_t nz = rp.sz ? hz : lz, fz = rp.sz ? lz : hz;
-    const float tlo = tmin, thi = tmax * kSlack;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const float tn = fmaxf(fmaxf(fma_rn(quant_byte(nx, k), bx, ax), fma_rn(quant_byte(ny, k), by, ay)),
-                             fmaxf(fma_rn(quant_byte(nz, k), bz, az), tlo));
-      const float tf = fminf(fminf(fma_rn(quant_byte(fx, k), bx, ax), fma_rn(quant_byte(fy, k), by, ay)),
-                             fminf(fma_rn(quant_byte(fz, k), bz, az), thi));
-      t[k] = tn <= tf * kSlack ? tn : as_float(0x7f800000);
-    }
-    code[0] = c.x;
-    code[1] = c.y;
-    code[2] = c.z;
-    code[3] = c.w;
-    const float inf = as_float(0x7f800000);
-    int n = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) n += t[k] != inf;
-    if constexpr (kSort) {
-      cswap4(code, t, 0, 1);
-      cswap4(code, t, 2, 3);
-      cswap4(code, t, 0, 2);
-      cswap4(code, t, 1, 3);
-      cswap4(code, t, 1, 2);
-    }
-    return n;
-  }
 #pragma unroll
   for (int r = 0; r < kWideRow; ++r) {
     const float4 nx = PT_LDG(nd + (0 + rp.sx) * kWideRow + r), fx = PT_LDG(nd + (1 - rp.sx) * kWideRow + r);
