@@ -179,3 +179,48 @@ def test_invalid_parameters_rejected():
     assert nat.lib().pt_set_integrator(R.ctx, 5, float("nan"), None, 0) == 1
     assert nat.lib().pt_render_frames(None, 0, 1) == 1
     R.close()
+
+
+@pytest.mark.gpu
+def test_bvh_hits_far_from_origin_bit_exact():
+    # the scene shrunk 100x and moved 500 units from the origin: coordinates on a coarse float grid, so
+    # many rays have an exactly zero direction component and run exactly inside a box's face plane
+    # (the slab tests must not cull those boxes)
+    data = small_scene()
+    for m in data.meshes:
+        m.positions = np.ascontiguousarray(m.positions * np.float32(0.01) + np.float32(500.0), np.float32)
+    R = sc.Renderer(data)
+    O = oc.OracleScene(data)
+    tp, _, _ = data.flat_triangles()
+    rng = np.random.default_rng(5)
+    n = 8000
+    pick = rng.integers(0, len(tp), n)
+    w = rng.dirichlet([1, 1, 1], n).astype(np.float32)
+    w[: n // 3] = np.array([1, 0, 0], np.float32)
+    w[n // 3: 2 * n // 3] = np.array([0.5, 0.5, 0], np.float32)
+    targets = tp[pick, 0:3] * w[:, 0:1] + tp[pick, 3:6] * w[:, 1:2] + tp[pick, 6:9] * w[:, 2:3]
+    orig = (rng.uniform(-0.9, 0.9, (n, 3)) * 0.01 + 500.0).astype(np.float32)
+    orig[::4, 1] = targets[::4, 1]  # a quarter of the rays run in the horizontal plane of their target
+    d = (targets - orig).astype(np.float64)
+    keep = np.linalg.norm(d, axis=1) > 0
+    d, orig = d[keep], orig[keep]
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    n = len(d)
+    assert np.mean(np.any(d == 0, axis=1)) > 0.2  # the case under test occurs
+    rays = np.concatenate([orig, np.full((n, 1), 1e-6), d, np.full((n, 1), 1e27)], 1).astype(np.float32)
+    d_ot = torch.from_numpy(np.ascontiguousarray(rays[:, :4])).cuda()
+    d_dt = torch.from_numpy(np.ascontiguousarray(rays[:, 4:])).cuda()
+    prim = torch.empty(n, dtype=torch.int32, device="cuda")
+    t = torch.empty(n, dtype=torch.float32, device="cuda")
+    bary = torch.empty((n, 2), dtype=torch.float32, device="cuda")
+    anyh = torch.empty(n, dtype=torch.int32, device="cuda")
+    nat.call("pt_trace_closest", R.ctx, d_ot.data_ptr(), d_dt.data_ptr(), n, prim.data_ptr(), t.data_ptr(), bary.data_ptr())
+    nat.call("pt_trace_any", R.ctx, d_ot.data_ptr(), d_dt.data_ptr(), n, anyh.data_ptr())
+    R.sync()
+    bp, bt, bb, ba = O.trace(rays, brute=True)
+    assert (bp >= 0).mean() > 0.5
+    assert np.array_equal(prim.cpu().numpy(), bp)
+    assert np.array_equal(t.cpu().numpy().view(np.uint32), bt.view(np.uint32))
+    assert np.array_equal(bary.cpu().numpy().view(np.uint32), bb.view(np.uint32))
+    assert np.array_equal(anyh.cpu().numpy(), ba)
+    R.close()
