@@ -190,6 +190,25 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
+def max_over_ranks(x, world, device="cuda"):
+    """The largest of the ranks' values of x: one all-reduce (MAX) that every rank makes at the same
+    point (a multi-GPU time is the slowest rank's).  One rank: x itself."""
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(units_per_rank, world, steps, seconds_max):
+    """Whole-job throughput of independent replicas, in millions of units per second: the units all
+    ranks processed over the slowest rank's time."""
+    return world * steps * units_per_rank / seconds_max / 1e6
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -362,13 +381,9 @@ def run_bsdf(args, world, rank, local):
     launches = L.pt_kernel_launch_count() - launches0
     ms = evs[0].elapsed_time(evs[-1])
     barrier()
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * args.steps * n / (ms_max * 1e-3) / 1e6
+    t_max = max_over_ranks(ms, world, dev)
+    ms_max = t_max
+    value = replica_throughput(n, world, args.steps, ms_max * 1e-3)
 
     # end to end: host buffers through pt_bsdf_queries_host (H2D of wo and alpha, the kernel, D2H of
     # wi, f, pdf and F, synchronous) from pinned host memory
@@ -387,12 +402,8 @@ def run_bsdf(args, world, rank, local):
     for _ in range(args.steps):
         host_call()
     e2e_s = time.perf_counter() - t0
-    t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.steps * n / float(t.item()) / 1e6
+    t_max = max_over_ranks(e2e_s, world, dev)
+    e2e_value = replica_throughput(n, world, args.steps, t_max)
     same = bool(torch.equal(h_f, d_f.cpu()) and torch.equal(h_wi, d_wi.cpu()))
 
     peak, peak_kind = load_peaks()
@@ -663,13 +674,9 @@ def run_batched(args, world, rank, local):
         torch.cuda.synchronize()
     launches = L.pt_kernel_launch_count() - launches0
     ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * args.steps * path_samples / (ms_max * 1e-3) / 1e6
+    t_max = max_over_ranks(ms, world, "cuda")
+    ms_max = t_max
+    value = replica_throughput(path_samples, world, args.steps, ms_max * 1e-3)
     # the plain path: the same frames, scene after scene, each by its own single-scene pass
     B.render_sequential()
     torch.cuda.synchronize()
@@ -718,12 +725,8 @@ def run_batched(args, world, rank, local):
         e2e_step()
     f1.record(stream)
     torch.cuda.synchronize()
-    t = torch.tensor([f0.elapsed_time(f1)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.steps * path_samples / (float(t.item()) * 1e-3) / 1e6
+    t_max = max_over_ranks(f0.elapsed_time(f1), world, "cuda")
+    e2e_value = replica_throughput(path_samples, world, args.steps, t_max * 1e-3)
     st = B.stats()
     peak, peak_kind = load_peaks()
     kinds = {}
@@ -879,13 +882,9 @@ def run_ours(args, world, rank, local):
     launches = L.pt_kernel_launch_count() - launches0
     ms = e0.elapsed_time(e1)
     barrier()
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * args.steps * path_samples / (ms_max * 1e-3) / 1e6
+    t_max = max_over_ranks(ms, world, "cuda")
+    ms_max = t_max
+    value = replica_throughput(path_samples, world, args.steps, ms_max * 1e-3)
 
     # ---- end-to-end through the public API with host buffers
     img_host = torch.empty((height, width, 4), dtype=torch.float32, pin_memory=True)
@@ -912,12 +911,8 @@ def run_ours(args, world, rank, local):
     f1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = f0.elapsed_time(f1)
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.steps * path_samples / (float(t.item()) * 1e-3) / 1e6
+    t_max = max_over_ranks(e2e_ms, world, "cuda")
+    e2e_value = replica_throughput(path_samples, world, args.steps, t_max * 1e-3)
 
     # ---- roofline of the dominant kernel (closest-hit extend), from a separately profiled render
     nat.call("pt_set_profiling", R.ctx, 1)
