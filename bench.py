@@ -86,6 +86,7 @@ def parse():
     ap.add_argument("--height", type=int, default=None)
     ap.add_argument("--dipole", default="standard", choices=["standard", "directional"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-arms", action="store_true", help="single scene: skip the batched and forward+adjoint arms and the relMSE")
     return ap.parse_args()
 
 
@@ -125,19 +126,40 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def traffic_per_segment_from_profile():
-    """DRAM bytes per traced segment of the extend kernel, from the committed ncu summary (a small
-    capture of the same kernel; traffic grows in proportion to the rays a launch traces)."""
-    path = os.path.join(ROOT, "profiles", "k_extend_single_scene.md")
+def extend_capture_record():
+    """Per-segment figures of the extend kernel from its committed ncu record
+    (profiles/k_extend_single_scene_ncu.csv: the raw ncu rows of every k_extend_persistent launch of the
+    first render of the capture command, preceded by '#' lines that give the segments those launches
+    traced, from the same command's JSON line).  Returns {"warp_inst_per_segment",
+    "thread_inst_per_warp_inst", "dram_bytes_per_segment", "segments", "launches"} or None."""
+    import csv
+
+    path = os.path.join(ROOT, "profiles", "k_extend_single_scene_ncu.csv")
     if not os.path.exists(path):
         return None
-    for line in open(path):
-        if line.startswith("traffic_bytes_per_segment:"):
-            try:
-                return float(line.split(":", 1)[1].strip())
-            except ValueError:
-                return None
-    return None
+    segments = None
+    rows = []
+    with open(path) as fh:
+        for line in fh:
+            if line.startswith("#"):
+                if "segments:" in line:
+                    segments = float(line.split("segments:", 1)[1].split()[0].replace(",", ""))
+                continue
+            rows.append(line)
+    table = list(csv.reader(rows))
+    if segments is None or len(table) < 3:
+        return None
+    head, data = table[0], [r for r in table[2:] if len(r) == len(table[0])]  # row 1 holds the units
+
+    def total(name):
+        k = head.index(name)
+        return sum(float(r[k].replace(",", "")) for r in data)
+
+    warp = total("smsp__inst_executed.sum")
+    thread = total("smsp__thread_inst_executed.sum")
+    dram = total("dram__bytes_read.sum") + total("dram__bytes_write.sum")
+    return {"warp_inst_per_segment": warp / segments, "thread_inst_per_warp_inst": thread / warp, "dram_bytes_per_segment": dram / segments,
+            "segments": segments, "launches": len(data)}
 
 
 class ClockSampler:
@@ -634,7 +656,31 @@ BATCHED = ("batched render of %d seeded procedural scenes in one pass (CUDA grap
            "spp log-uniform over 4-256, 128x64 procedural sky as background and light, max depth 8, Russian roulette from depth 3")
 
 
-def run_batched(args, world, rank, local):
+def rel_mse(img, ref):
+    """Mean over pixels and channels of (I - I_ref)^2 / (I_ref^2 + 1e-2)."""
+    img = np.asarray(img, np.float64)[..., :3]
+    ref = np.asarray(ref, np.float64)[..., :3]
+    return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+def reference_image(R, spp, factor=16):
+    """The same scene at factor x spp from frames [spp, spp + factor*spp), independent of the frames
+    0..spp-1 of the measured image: rendered into a cleared accumulation buffer starting at frame spp,
+    whose running mean then holds sum / (spp + factor*spp), rescaled to the mean of those frames."""
+    from open_rendering_framework_b200 import _native as nat
+
+    R.apply_camera()
+    n = factor * spp
+    nat.call("pt_render_frames", R.ctx, spp, n)
+    R.frame = spp + n
+    img = R.readback().astype(np.float64)
+    return img * ((spp + n) / n)
+
+
+def measure_batched(args, world, local, relmse=True):
+    """The batched configuration (64 seeded scenes in one pass from a CUDA graph): device-timed
+    throughput, the same frames scene after scene (plain), the reference's launch pattern, the
+    end-to-end figure, and the images' relMSE against 16x-spp references."""
     import torch
 
     from open_rendering_framework_b200 import _native as nat
@@ -642,8 +688,7 @@ def run_batched(args, world, rank, local):
     from open_rendering_framework_b200 import scenes
 
     torch.cuda.set_device(local)
-    # each rank renders its own batch (replicas): scene seeds differ by rank only through nothing -- the
-    # same batch, so the per-rank work is fixed (weak scaling)
+    # each rank renders its own copy of the batch (replicas: per-rank work fixed, weak scaling)
     S = scenes.batch_scenes(args.scenes, seed=0)
     Rs = [sc.Renderer(d, device=local) for d, _, _ in S]
     spp = [p for _, p, _ in S]
@@ -658,7 +703,7 @@ def run_batched(args, world, rank, local):
 
             dist.barrier()
 
-    for _ in range(args.warmup):
+    for _ in range(max(3, args.warmup)):
         B.render()
     torch.cuda.synchronize()
     barrier()
@@ -673,9 +718,7 @@ def run_batched(args, world, rank, local):
         e1.record(stream)
         torch.cuda.synchronize()
     launches = L.pt_kernel_launch_count() - launches0
-    ms = e0.elapsed_time(e1)
-    t_max = max_over_ranks(ms, world, "cuda")
-    ms_max = t_max
+    ms_max = max_over_ranks(e0.elapsed_time(e1), world, "cuda")
     value = replica_throughput(path_samples, world, args.steps, ms_max * 1e-3)
     # the plain path: the same frames, scene after scene, each by its own single-scene pass
     B.render_sequential()
@@ -700,8 +743,9 @@ def run_batched(args, world, rank, local):
     torch.cuda.synchronize()
     plain_per_frame = path_samples / (time.perf_counter() - w0) / 1e6
     B._sync_frames()
-    # end to end: per step every scene's camera and materials set from the host, the batch render, and
-    # every image read back into pinned host memory
+    # end to end: per step every scene's camera and materials set from the host (which also clears
+    # every accumulation buffer), the batch render of frames 0..spp-1, and every image read back into
+    # pinned host memory
     imgs = [torch.empty((d.camera.height, d.camera.width, 4), dtype=torch.float32, pin_memory=True) for d, _, _ in S]
     h2d = sum(ctypes.sizeof(m.params()) for d, _, _ in S for m in d.materials) + 12 * 4 * len(S)
     d2h = sum(im.numel() * 4 for im in imgs)
@@ -728,19 +772,15 @@ def run_batched(args, world, rank, local):
     t_max = max_over_ranks(f0.elapsed_time(f1), world, "cuda")
     e2e_value = replica_throughput(path_samples, world, args.steps, t_max * 1e-3)
     st = B.stats()
-    peak, peak_kind = load_peaks()
     kinds = {}
     for _, p, info in S:
         kinds[info["material"]] = kinds.get(info["material"], 0) + 1
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic",
-        "config": {"workload": BATCHED % len(S), "path_samples_per_step": path_samples, "scenes": len(S), "materials": kinds,
-                   "parallelism": "replicas (one independent batch per GPU)",
-                   "l2": "inputs larger than L2: %.1f GB of path state per chunk" % (tune.max_paths_in_flight * 178 / 1e9)},
-        "plain": {"value": plain, "unit": UNIT, "what": "the same frames rendered scene after scene by single-scene passes"},
-        "batched_over_plain": value / plain,
+    out = {
+        "value": value, "unit": UNIT, "ms_per_step": ms_max / args.steps, "steps": args.steps, "warmup": max(3, args.warmup),
+        "workload": BATCHED % len(S), "path_samples_per_step": path_samples, "scenes": len(S), "materials": kinds,
+        "timing": "CUDA events on the batch stream around the graph launches",
+        "plain_same_frames": {"value": plain, "unit": UNIT, "what": "the same frames rendered scene after scene by single-scene passes"},
+        "batched_over_plain_same_frames": value / plain,
         "plain_per_frame": {"value": plain_per_frame, "unit": UNIT,
                             "what": "the same frames rendered one pass per frame per scene, scene after scene (the "
                                     "reference's launch pattern), host-timed between device synchronisations"},
@@ -748,18 +788,49 @@ def run_batched(args, world, rank, local):
         "autotune": {"extend_mode": tune.extend_mode, "refill": tune.refill, "max_paths_in_flight": tune.max_paths_in_flight,
                      "trials": tune.trials, "best_calibration_mpaths_per_s": tune.best_mpaths_per_s},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "roofline": {"bound": "hbm", "kernel": "k_extend_persistent", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
-                     "peak_source": peak_kind, "traffic": None,
-                     "note": "the batch runs from a CUDA graph without per-kernel events; the extend kernel's roofline is "
-                             "reported by the single-scene workload"},
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
         "stats": {"segments_per_path": st.segments / max(1, st.path_samples), "dipole_gathers": st.dipole_gathers,
                   "dipole_pairs": st.dipole_pairs},
+        "l2": "inputs larger than L2: %.1f GB of path state per chunk" % (tune.max_paths_in_flight * 178 / 1e9),
     }
+    if relmse:
+        # relMSE of each scene's batched image (frames 0..spp-1, the e2e step's) against its 16x-spp
+        # reference; the plain path renders bit-identical images (tests/test_batch_gpu.py), so its
+        # relMSE on the same frames is the same number
+        t0 = time.perf_counter()
+        errs = []
+        for R, im, p in zip(Rs, imgs, spp):
+            ref = reference_image(R, p)
+            errs.append(rel_mse(im.numpy(), ref))
+        out["relmse_vs_16x_spp"] = {"mean_over_scenes": float(np.mean(errs)), "max_over_scenes": float(np.max(errs)),
+                                    "per_scene": [float(e) for e in errs], "reference": "frames [spp, 17 spp) of each scene",
+                                    "plain_same_frames": "identical (bit-identical images)", "seconds": time.perf_counter() - t0}
     B.close()
     for R in Rs:
         R.close()
+    return out
+
+
+def run_batched(args, world, rank, local):
+    peak, peak_kind = load_peaks()
+    m = measure_batched(args, world, local)
+    line = {
+        "metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": m["warmup"],
+        "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": m["workload"], "path_samples_per_step": m["path_samples_per_step"], "scenes": m["scenes"],
+                   "materials": m["materials"], "parallelism": "replicas (one independent batch per GPU)", "l2": m["l2"]},
+        "e2e": m["e2e"], "gpu_launches": m["gpu_launches"], "clocks": m["clocks"],
+        "roofline": {"bound": "issue", "kernel": "k_extend_persistent", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
+                     "peak_source": peak_kind, "traffic": None,
+                     "note": "the batch runs from a CUDA graph without per-kernel events; the extend kernel's roofline is "
+                             "reported by the single-scene workload"},
+    }
+    for k in ("plain_same_frames", "batched_over_plain_same_frames", "plain_per_frame", "batched_over_plain_per_frame", "autotune", "stats",
+              "relmse_vs_16x_spp"):
+        if k in m:
+            line[k] = m[k]
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -770,7 +841,10 @@ ADJOINT = ("inverse rendering 256x256, 64 spp, depth 6, RR from depth 3: 12-tria
            "1024-spp target from other seeded parameters; forward + path-replay adjoint per step")
 
 
-def run_adjoint(args, world, rank, local):
+def measure_adjoint(args, local, relmse=True):
+    """The differentiable configuration: forward (differentiable) render + path-replay adjoint per
+    step, device-timed per phase; the end-to-end figure through the torch.autograd.Function; the
+    forward image's relMSE against a 16x-spp reference."""
     import torch
 
     from open_rendering_framework_b200 import diff
@@ -778,8 +852,8 @@ def run_adjoint(args, world, rank, local):
     from open_rendering_framework_b200 import scenes
 
     torch.cuda.set_device(local)
-    W = args.width or 256
-    spp = args.spp or 64
+    W = 256
+    spp = 64
     data, (dif, met, tr) = scenes.inverse_scene(W, W, subdiv=5, tex_res=256, seed=0)
     tdata, _ = scenes.inverse_scene(W, W, subdiv=5, tex_res=256, seed=1)
     T = sc.Renderer(tdata, device=local)
@@ -791,6 +865,7 @@ def run_adjoint(args, world, rank, local):
     rough = torch.from_numpy(met.texture.copy()).cuda().requires_grad_()
     sigma = torch.tensor(list(tr.absorption) + list(tr.scattering), dtype=torch.float32, device="cuda").requires_grad_()
     path_samples = W * W * spp
+    last = {}
 
     def step():
         for t in (albedo, rough, sigma):
@@ -800,11 +875,12 @@ def run_adjoint(args, world, rank, local):
         loss = ((img - target) ** 2).sum()
         loss.backward()
         ast = DS.stats()
+        last["img"] = img
         return float(loss.item()), fst, ast
 
     for _ in range(max(3, args.warmup)):
         step()
-    fwd_ms, adj_ms, seg, gathers = 0.0, 0.0, 0, 0
+    fwd_ms, adj_ms, seg, gathers, launches = 0.0, 0.0, 0, 0, 0
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
@@ -816,30 +892,51 @@ def run_adjoint(args, world, rank, local):
             adj_ms += ast.gpu_ms
             seg += fst.segments
             gathers += fst.dipole_gathers
+            launches += fst.kernel_launches + ast.kernel_launches
         e1.record()
         torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
     dev_ms = fwd_ms + adj_ms
-    value = args.steps * path_samples / (dev_ms * 1e-3) / 1e6
     g = [albedo.grad, rough.grad, sigma.grad]
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup),
-        "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic",
-        "config": {"workload": ADJOINT, "path_samples_per_step": path_samples, "parameters": int(sum(t.numel() for t in g)),
-                   "l2": "per-path forward state of %.2f GB re-read by the adjoint" % (path_samples * 16 * 8 / 1e9)},
+    out = {
+        "value": args.steps * path_samples / (dev_ms * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": dev_ms / args.steps, "steps": args.steps,
+        "warmup": max(3, args.warmup), "workload": ADJOINT, "path_samples_per_step": path_samples,
+        "parameters": int(sum(t.numel() for t in g)),
+        "timing": "device time of the forward and adjoint launches (CUDA events on the scene stream)",
         "forward": {"value": args.steps * path_samples / (fwd_ms * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": fwd_ms / args.steps},
         "adjoint_ms_per_step": adj_ms / args.steps,
         "fwd_plus_adjoint_over_forward": dev_ms / fwd_ms,
+        "target_fwd_plus_adjoint_le_3x_forward": bool(dev_ms / fwd_ms <= 3.0),
         "e2e": {"value": args.steps * path_samples / (e2e_ms * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": 6 * 4 + 64,
                 "d2h_bytes_per_step": 4 + 24, "what": "torch.autograd.Function forward + loss + backward, host sigma update and loss read-back"},
         "loss": loss,
         "grad_norms": [float(t.norm().item()) for t in g],
-        "gpu_launches": int(fst.kernel_launches + ast.kernel_launches) * args.steps,
+        "gpu_launches": int(launches),
         "clocks": clocks.summary(),
         "stats": {"segments_per_path": seg / (args.steps * path_samples), "dipole_gathers_per_step": gathers / args.steps},
+        "l2": "per-path forward state of %.2f GB re-read by the adjoint" % (path_samples * 16 * 8 / 1e9),
     }
+    if relmse:
+        img = last["img"].detach().cpu().numpy()
+        ref = reference_image(DS.R, spp)
+        out["relmse_vs_16x_spp"] = {"forward_image": rel_mse(img, ref), "reference": "frames [64, 1088) of the same scene and parameters"}
     DS.close()
+    return out
+
+
+def run_adjoint(args, world, rank, local):
+    m = measure_adjoint(args, local)
+    line = {
+        "metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": m["warmup"],
+        "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": m["workload"], "path_samples_per_step": m["path_samples_per_step"], "parameters": m["parameters"],
+                   "l2": m["l2"]},
+        "e2e": m["e2e"], "gpu_launches": m["gpu_launches"], "clocks": m["clocks"],
+    }
+    for k in ("forward", "adjoint_ms_per_step", "fwd_plus_adjoint_over_forward", "target_fwd_plus_adjoint_le_3x_forward", "loss",
+              "grad_norms", "stats", "relmse_vs_16x_spp"):
+        line[k] = m[k]
     print(json.dumps(line), flush=True)
 
 
@@ -864,8 +961,12 @@ def run_ours(args, world, rank, local):
             dist.barrier()
 
     # ---- device-timed steps
-    for _ in range(args.warmup):
+    first_render = None
+    for k in range(args.warmup):
         R.render(spp)
+        if k == 0:
+            s0 = R.stats()  # the first render's extend launches are what the committed ncu record captures
+            first_render = {"segments": int(s0.segments), "extend_launches": int(s0.extend_launches), "frames": [0, spp]}
     R.sync()
     barrier()
     torch.cuda.synchronize()
@@ -914,28 +1015,47 @@ def run_ours(args, world, rank, local):
     t_max = max_over_ranks(e2e_ms, world, "cuda")
     e2e_value = replica_throughput(path_samples, world, args.steps, t_max * 1e-3)
 
+    # ---- image error of this arm: the e2e step's image (frames 0..spp-1) against a 16x-spp reference
+    relmse = None
+    if args.workload == "single_scene" and not args.no_arms:
+        img = img_host.numpy().copy()
+        relmse = {"value": rel_mse(img, reference_image(R, spp)), "reference": "frames [%d, %d) of the same scene" % (spp, 17 * spp)}
+
     # ---- roofline of the dominant kernel (closest-hit extend), from a separately profiled render
     nat.call("pt_set_profiling", R.ctx, 1)
     R.render(spp)
     st = R.stats()
     nat.call("pt_set_profiling", R.ctx, 0)
     peak, peak_kind = load_peaks()
-    ext_bytes = st.segments * EXTEND_BYTES_PER_SEGMENT
-    # per launch: algorithmic bytes of one launch / that launch's average duration == totals ratio
-    achieved = ext_bytes / (st.extend_ms * 1e-3) / 1e9 if st.extend_ms > 0 else None
-    per_seg = traffic_per_segment_from_profile()
+    ext_s = st.extend_ms * 1e-3
     launches_ext = max(1, st.extend_launches)
-    traffic = per_seg * st.segments / launches_ext if per_seg else None
-    roofline = {"bound": "hbm", "kernel": "k_extend (closest-hit traversal + material binning)",
-                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                "peak_source": peak_kind,
-                "traffic": traffic, "traffic_unit": "bytes per launch (ncu small-case capture scaled by rays per launch)",
+    # HBM view: algorithmic bytes of one launch / that launch's average duration == the totals' ratio
+    hbm_achieved = st.segments * EXTEND_BYTES_PER_SEGMENT / ext_s / 1e9 if ext_s > 0 else None
+    rec = extend_capture_record()
+    hbm = {"achieved": hbm_achieved, "peak": peak, "unit": "GB/s", "frac": hbm_achieved / peak if hbm_achieved else None,
+           "peak_source": peak_kind, "algorithmic_bytes_per_segment": EXTEND_BYTES_PER_SEGMENT,
+           "traffic": rec["dram_bytes_per_segment"] * st.segments / launches_ext if rec else None,
+           "traffic_unit": "DRAM bytes per launch (ncu record of the same kernel, scaled by the segments a launch traces)"}
+    # issue view: warp instructions per segment (ncu record) x segments / extend time, against one warp
+    # instruction per clock per SM sub-partition (4 per SM) at the sampled SM clock
+    sm_mhz = clocks.summary().get("sm_mhz") or 1965.0
+    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+    issue_peak = n_sm * 4 * sm_mhz * 1e6 / 1e9
+    issue_achieved = rec["warp_inst_per_segment"] * st.segments / ext_s / 1e9 if (rec and ext_s > 0) else None
+    roofline = {"bound": "issue", "kernel": "k_extend_persistent (closest-hit traversal + material class record)",
+                "achieved": issue_achieved, "peak": issue_peak, "unit": "G warp instructions/s",
+                "frac": issue_achieved / issue_peak if issue_achieved else None,
+                "peak_source": "1 warp instruction / clock / SM sub-partition x 4 x %d SMs x median SM clock %.0f MHz" % (n_sm, sm_mhz),
+                "warp_instructions_per_segment": rec["warp_inst_per_segment"] if rec else None,
+                "threads_per_warp_instruction": rec["thread_inst_per_warp_inst"] if rec else None,
+                "traffic": hbm["traffic"], "traffic_unit": hbm["traffic_unit"],
+                "hbm": hbm,
+                "extend_ms_per_launch": st.extend_ms / launches_ext,
                 "extend_share_of_render": st.extend_ms / st.gpu_ms if st.gpu_ms else None,
                 "segments_per_path": st.segments / st.path_samples, "shadow_rays_per_path": st.shadow_rays / st.path_samples,
-                "algorithmic_bytes_per_segment": EXTEND_BYTES_PER_SEGMENT,
-                "giga_rays_per_s": (st.segments + st.shadow_rays) / (st.gpu_ms * 1e-3) / 1e9}
+                "giga_rays_per_s": (st.segments + st.shadow_rays) / (st.gpu_ms * 1e-3) / 1e9,
+                "record": "profiles/k_extend_single_scene_ncu.csv" if rec else None}
     if args.workload == "subsurface":
-        roofline["traffic"] = None  # the committed traffic figure is the single-scene kernel's
         # integer-issue bound: 64 INT32 lanes per clock per SM at the sampled SM clock, divided by the
         # thread instructions one pair takes (ncu capture of k_gather)
         sm_mhz = clocks.summary().get("sm_mhz") or 1965.0
@@ -962,11 +1082,20 @@ def run_ours(args, world, rank, local):
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
         "stats": {"capped_walks": st.capped_walks, "clamped_indices": st.clamped_indices, "dipole_gathers": st.dipole_gathers,
-                  "dipole_pairs": st.dipole_pairs},
+                  "dipole_pairs": st.dipole_pairs, "first_render": first_render},
     }
+    if relmse:
+        line["relmse_vs_16x_spp"] = relmse
+    R.close()
+    if args.workload == "single_scene" and world == 1 and not args.no_arms:
+        # the metric's other two arms on the same GPU: the 64-scene batch and forward + adjoint
+        line["batched"] = measure_batched(args, world, local)
+        line["fwd_adjoint"] = measure_adjoint(args, local)
+        line["arms"] = ("value = plain single-scene arm; batched = the 64-scene batch in one CUDA-graph pass; fwd_adjoint = the "
+                        "differentiable configuration (forward + path-replay adjoint); each carries its own e2e and its image relMSE "
+                        "against a 16x-spp reference of the same scene")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(data)
-    R.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
 

@@ -185,6 +185,54 @@ typedef struct pt_rough_translucent_params {
 /* gi["radiance"] of a TriangleAreaLight's geometry (Light.cpp:242). */
 typedef struct pt_area_light_params { float radiance[3]; } pt_area_light_params;
 
+/* ---------------------------------------------------------------- per-query BSSRDF and walk batches
+ * The device functions the shading kernels call, evaluated on a batch of independent queries (for
+ * parity checks and for tools that tabulate a material); asynchronous on `stream`. */
+
+/* Dipole BSSRDF values of one translucent material: the per-(hit, probe) terms of the dipole gather
+ * (subsurface_scattering_shader.cu:126-173): dipole_bssrdf (dipoles/standard_dipole.h:8-30) of a
+ * distance, or dirpole_bssrdf (dipoles/directional_dipole.h:37-72) of (xi, ni, w12, xo, no), as
+ * params->dipole_model selects, on the ScatteringMaterialProperties that
+ * TranslucentMaterial::computeCoefficients (TranslucentMaterial.cpp:303-330) derives from params.
+ * d_in: the standard dipole reads n distances; the directional one 15 x n floats as SoA rows
+ * (xi.x, xi.y, xi.z, ni.xyz, w12.xyz, xo.xyz, no.xyz).  precision 0: FP32 in the reference's
+ * operation order (what the renders compute), d_S = 3 x n floats (SoA r, g, b); precision 1: the
+ * coefficients and the dipole evaluated in FP64, d_S = 3 x n doubles. */
+pt_status pt_bssrdf_queries(const pt_translucent_params* params, uint32_t precision, const float* d_in, uint64_t n, void* d_S,
+                            void* stream);
+
+/* Multiscattering random walks (Microfacet.h:95-177: MicrofacetGGX.h:412-640,
+ * MicrofacetBeckmann.h:445-736) and the complex conductor Fresnel (Fresnel.h:78-91), per query, in
+ * the frame of `normal` as the shaders call them. */
+enum {
+  PT_MSQ_DIELECTRIC_EVAL = 0,    /* microfacet_multiscattering_dielectric_BSDF_eval    */
+  PT_MSQ_DIELECTRIC_SAMPLE = 1,  /* microfacet_multiscattering_dielectric_BSDF_sample  */
+  PT_MSQ_CONDUCTOR_EVAL = 2,     /* microfacet_multiscattering_conductor_BSDF_eval     */
+  PT_MSQ_CONDUCTOR_SAMPLE = 3,   /* microfacet_multiscattering_conductor_BSDF_sample   */
+  PT_MSQ_DIFFUSE_EVAL = 4,       /* microfacet_multiscattering_diffuse_BSDF_eval       */
+  PT_MSQ_DIFFUSE_SAMPLE = 5,     /* microfacet_multiscattering_diffuse_BSDF_sample     */
+  PT_MSQ_CONDUCTOR_FRESNEL = 6,  /* fresnel_MyComplex_R(wi, m, eta)                    */
+  PT_MSQ_VISIBLE_NORMAL = 7      /* microfacet_sample_visible_normal (Microfacet.h:76-87) with
+                                    (z1, z2) two rnd_tea draws from the query's seed            */
+};
+typedef struct pt_microfacet_batch {
+  uint32_t op;                   /* PT_MSQ_*                                                    */
+  uint32_t normal_distribution;  /* PT_BECKMANN_DISTRIBUTION / PT_GGX_DISTRIBUTION              */
+  float normal[3];               /* shading normal of every query                                */
+  float eta;                     /* dielectric walks: the relative index the shader passes        */
+  double ior[6];                 /* conductor walks and Fresnel: complex eta (re, im) per RGB     */
+  float rho[3];                  /* diffuse walks: the albedo                                     */
+} pt_microfacet_batch;
+/* Per query k (SoA arrays of n): d_wi (3 x n), d_wo (3 x n: the evaluated direction; the microfacet
+ * normal for PT_MSQ_CONDUCTOR_FRESNEL; unread by the sample ops), d_alpha (ax = ay), d_seed (the tea
+ * state, advanced in place), d_order (the eval ops read it as the order bound, 0 = all; the sample
+ * ops add the walk's scattering events to it).  d_out (3 x n): the value (the dielectric eval's
+ * scalar in all three rows), the sampled direction or microfacet normal, or F; d_weight (3 x n,
+ * sample ops; may be NULL): the sampled walk's weight (1 for the dielectric walk and the visible
+ * normal). */
+pt_status pt_microfacet_queries(const pt_microfacet_batch* batch, const float* d_wi, const float* d_wo, const float* d_alpha,
+                                uint32_t* d_seed, uint32_t* d_order, uint64_t n, float* d_out, float* d_weight, void* stream);
+
 /* Counters of the most recent pt_render_frames call. */
 typedef struct pt_render_stats {
   uint64_t path_samples;    /* camera samples traced (pixels in the patch x frames)           */

@@ -50,6 +50,8 @@ SIGNATURES = {
     "pt_bsdf_queries_host": (I32, [P, P, U64, U64, U64, F32, P, P, P, P]),
     "pt_bsdf_queries_host_noalloc": (I32, [P, P, U64, U64, U64, F32, P, P, P, P]),
     "pt_c1_make_inputs": (I32, [U64, U64, P, P]),
+    "pt_bssrdf_queries": (I32, [P, U32, P, U64, P, P]),
+    "pt_microfacet_queries": (I32, [P, P, P, P, P, P, U64, P, P, P]),
     "pt_rng_streams": (I32, [I32, P, U64, U32, P, P]),
     "pt_context_create": (I32, [I32, P]),
     "pt_context_destroy": (I32, [P]),

@@ -4,8 +4,8 @@
 // Layout: structure-of-arrays, 16 B read (wo.xyz + alpha) and 24 B written (wi.xyz, f, pdf, F) per
 // query, all coalesced.  The kernel is ALU-bound (16-round TEA, transcendentals, the Beckmann
 // Newton loop in double/float), so it runs a grid-stride loop over a grid sized to a multiple of the
-// SM count; queries are ordered GGX-then-Beckmann, so warps never mix distributions except at the
-// single boundary warp.
+// SM count; queries are ordered GGX-then-Beckmann and each distribution's range is its own launch of
+// a kernel specialised on it.
 #include <mutex>
 #include <vector>
 
@@ -16,24 +16,28 @@ namespace pt {
 
 __device__ unsigned long long g_bsdf_capped = 0;
 
+// One launch per distribution: a kernel instance holds only its own distribution's code, so an SM
+// never runs GGX and Beckmann warps side by side (a single kernel over the mixed batch thrashed the
+// instruction cache: "no instruction" was its top stall).  Queries k in [k_begin, k_end) of the batch.
+template <uint32_t kDist>
 __global__ void __launch_bounds__(256) k_bsdf_queries(const float* __restrict__ wo_soa, const float* __restrict__ alpha, uint64_t n,
-                                                      uint64_t first, uint64_t n_ggx_below, float eta, float* __restrict__ wi_soa,
-                                                      float* __restrict__ f_out, float* __restrict__ pdf_out, float* __restrict__ F_out)
+                                                      uint64_t k_begin, uint64_t k_end, uint64_t first, float eta,
+                                                      float* __restrict__ wi_soa, float* __restrict__ f_out, float* __restrict__ pdf_out,
+                                                      float* __restrict__ F_out)
 {
   const float3 nrm = f3(0.0f, 0.0f, 1.0f);
-  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
+  for (uint64_t k = k_begin + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < k_end; k += (uint64_t)gridDim.x * blockDim.x) {
     uint64_t i = first + k;
     uint32_t s = tea16((uint32_t)i, 0u);
     float u1 = rnd_tea(s);
     float u2 = rnd_tea(s);
-    uint32_t dist = (i < n_ggx_below) ? GGX : BECKMANN;
     float3 wo = f3(__ldg(wo_soa + k), __ldg(wo_soa + n + k), __ldg(wo_soa + 2 * n + k));
     float a = __ldg(alpha + k);
     int capped = 0;
-    float3 m = sample_visible_normal(dist, wo, nrm, a, a, u1, u2, &capped);
+    float3 m = sample_visible_normal(kDist, wo, nrm, a, a, u1, u2, &capped);
     float3 wi = reflect(-wo, m);
-    f_out[k] = walter_bsdf(dist, wo, wi, nrm, a, eta);
-    pdf_out[k] = eval_visible_normal(dist, wo, m, nrm, a, a) / (4.0f * fabsf(dot(wo, m)));
+    f_out[k] = walter_bsdf(kDist, wo, wi, nrm, a, eta);
+    pdf_out[k] = eval_visible_normal(kDist, wo, m, nrm, a, a) / (4.0f * fabsf(dot(wo, m)));
     F_out[k] = fresnel_R(wo, m, eta);
     wi_soa[k] = wi.x;
     wi_soa[n + k] = wi.y;
@@ -101,11 +105,22 @@ pt_status pt_bsdf_queries(const float* d_wo_soa, const float* d_alpha, uint64_t 
   if (n == 0) return PT_OK;
   if (!d_wo_soa || !d_alpha || !d_wi_soa || !d_f || !d_pdf || !d_F) return fail(PT_INVALID_ARG, "pt_bsdf_queries: null pointer");
   if (!(eta > 0.0f)) return fail(PT_INVALID_ARG, "pt_bsdf_queries: eta must be > 0");
+  // queries with global index first + k < n_ggx_below are GGX, the rest Beckmann
+  const uint64_t n_ggx = n_ggx_below <= first_index ? 0 : (n_ggx_below - first_index < n ? n_ggx_below - first_index : n);
   const int block = 256;
-  int grid = grid_for(n, block, 8);
-  k_bsdf_queries<<<grid, block, 0, (cudaStream_t)stream>>>(d_wo_soa, d_alpha, n, first_index, n_ggx_below, eta, d_wi_soa, d_f, d_pdf, d_F);
-  count_launch();
-  PT_CHECK_CUDA(cudaGetLastError(), "pt_bsdf_queries launch");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (n_ggx > 0) {
+    k_bsdf_queries<GGX><<<grid_for(n_ggx, block, 8), block, 0, st>>>(d_wo_soa, d_alpha, n, 0, n_ggx, first_index, eta, d_wi_soa, d_f, d_pdf,
+                                                                     d_F);
+    count_launch();
+    PT_CHECK_CUDA(cudaGetLastError(), "pt_bsdf_queries launch (GGX)");
+  }
+  if (n_ggx < n) {
+    k_bsdf_queries<BECKMANN><<<grid_for(n - n_ggx, block, 8), block, 0, st>>>(d_wo_soa, d_alpha, n, n_ggx, n, first_index, eta, d_wi_soa,
+                                                                              d_f, d_pdf, d_F);
+    count_launch();
+    PT_CHECK_CUDA(cudaGetLastError(), "pt_bsdf_queries launch (Beckmann)");
+  }
   return PT_OK;
 }
 

@@ -64,7 +64,7 @@ SceneDev Context::view() const
 
 // 1.0f / MyComplex in the reference's arithmetic (MyComplex.h:155-160 with :18-23): the squared
 // magnitude is powf(float |c|, 2) and the quotient is formed in double.
-static Cx host_recip(const Cx& b)
+Cx host_recip(const Cx& b)
 {
   float r = (float)b.re, i = (float)b.im;
   float ab = sqrtf(r * r + i * i);
@@ -82,29 +82,13 @@ static float __int_as_float_host(int i)
   return f;
 }
 
-// The boundary polynomials of Fresnel.h:93-124 (two_C1, three_C2, C_phi, C_E).
-static float two_C1(float n)
-{
-  if (n >= 1.0f) return -9.23372f + n * (22.2272f + n * (-20.9292f + n * (10.2291f + n * (-2.54396f + n * 0.254913f))));
-  return 0.919317f + n * (-3.4793f + n * (6.75335f + n * (-7.80989f + n * (4.98554f - n * 1.36881f))));
-}
-static float three_C2(float n)
-{
-  float r;
-  if (n >= 1.0f) {
-    r = -1641.1f + n * (1213.67f + n * (-568.556f + n * (164.798f + n * (-27.0181f + n * 1.91826f))));
-    r += (((135.926f / n) - 656.175f) / n + 1376.53f) / n;
-  } else {
-    r = 0.828421f + n * (-2.62051f + n * (3.36231f + n * (-1.95284f + n * (0.236494f + n * 0.145787f))));
-  }
-  return r;
-}
-static float C_phi(float n) { return 0.25f * (1.0f - two_C1(n)); }
-static float C_E(float n) { return 0.5f * (1.0f - three_C2(n)); }
+static float two_C1(float n) { return two_C1_t<float>(n); }
+static float C_phi(float n) { return C_phi_t<float>(n); }
+static float C_E(float n) { return C_E_t<float>(n); }
 
 // TranslucentMaterial::computeCoefficients (TranslucentMaterial.cpp:303-330) with ior_outside = 1,
 // evaluated in FP32 on the host in the same order.
-static ScatDev compute_coefficients(const pt_translucent_params& q)
+ScatDev compute_coefficients(const pt_translucent_params& q)
 {
   ScatDev p;
   memset(&p, 0, sizeof(p));

@@ -12,6 +12,32 @@
 
 namespace pt {
 
+// The boundary polynomials of Fresnel.h:93-124 (two_C1, three_C2, C_phi, C_E) on the host, in the
+// scalar type R with the reference's float coefficients (R = float is the reference's arithmetic).
+template <class R> inline R two_C1_t(R n)
+{
+  if (n >= R(1)) return R(-9.23372f) + n * (R(22.2272f) + n * (R(-20.9292f) + n * (R(10.2291f) + n * (R(-2.54396f) + n * R(0.254913f)))));
+  return R(0.919317f) + n * (R(-3.4793f) + n * (R(6.75335f) + n * (R(-7.80989f) + n * (R(4.98554f) - n * R(1.36881f)))));
+}
+template <class R> inline R three_C2_t(R n)
+{
+  R r;
+  if (n >= R(1)) {
+    r = R(-1641.1f) + n * (R(1213.67f) + n * (R(-568.556f) + n * (R(164.798f) + n * (R(-27.0181f) + n * R(1.91826f)))));
+    r += (((R(135.926f) / n) - R(656.175f)) / n + R(1376.53f)) / n;
+  } else {
+    r = R(0.828421f) + n * (R(-2.62051f) + n * (R(3.36231f) + n * (R(-1.95284f) + n * (R(0.236494f) + n * R(0.145787f)))));
+  }
+  return r;
+}
+template <class R> inline R C_phi_t(R n) { return R(0.25f) * (R(1) - two_C1_t<R>(n)); }
+template <class R> inline R C_E_t(R n) { return R(0.5f) * (R(1) - three_C2_t<R>(n)); }
+
+// 1.0f / MyComplex in the reference's arithmetic (MyComplex.h:155-160), evaluated on the host.
+Cx host_recip(const Cx& b);
+// TranslucentMaterial::computeCoefficients (TranslucentMaterial.cpp:303-330), FP32 on the host.
+ScatDev compute_coefficients(const pt_translucent_params& q);
+
 // Owning device allocation (cudaMalloc / cudaFree), reused when large enough.
 struct DevBuf {
   void* p = nullptr;

@@ -200,20 +200,25 @@ def load_json_scene(path, base_dir=None, rr_start_depth=0, unsupported_material=
     return JsonScene(data, int(doc.get("frame_count", 0)), buffer_path, doc, path)
 
 
-def save_checkpoint(renderer, json_path, document=None):
-    """OptixScene::saveScene (OptixScene.cpp:200-232): the scene document with "frame_count" (the frames
-    rendered so far) and "buffer_path" (a .raw file of width * height float4 next to it, written from the
-    context's accumulation buffer)."""
-    base = os.path.splitext(json_path)[0]
-    raw = base + ".raw"
+def save_checkpoint(renderer, json_path, document):
+    """OptixScene::saveScene (OptixScene.cpp:200-232): writes the scene document to `json_path` itself,
+    with "frame_count" (the frames rendered so far) and "buffer_path" (a .raw file of width * height
+    float4 beside it, written from the context's accumulation buffer).  `document` is the scene's JSON
+    document (a JsonScene or its `document` dict), so that the saved file reloads as a complete scene
+    through load_json_scene, as the reference's saved scenes do."""
+    if isinstance(document, JsonScene):
+        document = document.document
+    if not isinstance(document, dict) or not document:
+        raise ValueError("save_checkpoint needs the scene document (JsonScene.document) so that the file reloads as a scene")
+    raw = os.path.splitext(json_path)[0] + ".raw"
     img = renderer.readback()
     np.ascontiguousarray(img, np.float32).tofile(raw)
-    doc = dict(document or {})
+    doc = dict(document)
     doc["frame_count"] = int(renderer.frame)
     doc["buffer_path"] = os.path.basename(raw)
-    with open(base + ".json", "w") as f:
+    with open(json_path, "w") as f:
         json.dump(doc, f, indent=1)
-    return base + ".json"
+    return json_path
 
 
 def load_checkpoint(renderer, json_path):

@@ -69,6 +69,16 @@ class TranslucentParams(ctypes.Structure):
                 ("ior", ctypes.c_float), ("scale", ctypes.c_float), ("dipole_model", ctypes.c_uint32)]
 
 
+class MicrofacetBatch(ctypes.Structure):
+    """pt_microfacet_batch: one batch of multiscattering-walk / conductor-Fresnel queries."""
+    _fields_ = [("op", ctypes.c_uint32), ("normal_distribution", ctypes.c_uint32), ("normal", ctypes.c_float * 3), ("eta", ctypes.c_float),
+                ("ior", ctypes.c_double * 6), ("rho", ctypes.c_float * 3)]
+
+
+MSQ_OPS = {"dielectric_eval": 0, "dielectric_sample": 1, "conductor_eval": 2, "conductor_sample": 3, "diffuse_eval": 4,
+           "diffuse_sample": 5, "conductor_fresnel": 6, "visible_normal": 7}
+
+
 class RoughTranslucentParams(ctypes.Structure):
     _fields_ = [("scattering", ctypes.c_float * 3), ("absorption", ctypes.c_float * 3), ("meancosine", ctypes.c_float * 3),
                 ("ior", ctypes.c_float), ("scale", ctypes.c_float), ("dipole_model", ctypes.c_uint32), ("roughness", ctypes.c_float * 2),

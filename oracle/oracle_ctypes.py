@@ -88,6 +88,8 @@ def ref():
         _sig(lib, "ref_set_scattering_properties", None, [P, L])
         _sig(lib, "ref_dipole_bssrdf", None, [F, P])
         _sig(lib, "ref_dirpole_bssrdf", None, [P, P, P, P, P, P])
+        _sig(lib, "ref_bssrdf_queries", None, [U, L, P, P])
+        _sig(lib, "ref_microfacet_queries", None, [U, U, P, F, P, P, L, P, P, P, P, P, P, P])
         _sig(lib, "ref_C_phi", F, [F])
         _sig(lib, "ref_C_E", F, [F])
         _sig(lib, "ref_sizeof", I, [ctypes.c_char_p])
@@ -134,6 +136,9 @@ def orc():
         _sig(lib, "orc_sample_barycentric_f", None, [P, P])
         _sig(lib, "orc_create_onb_f", None, [P, P, P])
         _sig(lib, "orc_direct_illumination_f", None, [P, P, L, P, L, L, P, P, P, P])
+        _sig(lib, "orc_microfacet_queries_f", None, [U, U, P, F, P, P, L, P, P, P, P, P, P, P, I])
+        _sig(lib, "orc_microfacet_queries_d", None, [U, U, P, F, P, P, L, P, P, P, P, P, P, P, I])
+        _sig(lib, "orc_bsdf_given_m_f", None, [L, P, P, P, F, P, P, P, P, P])
         _sig(lib, "orc_C_phi_f", F, [F])
         _sig(lib, "orc_C_E_f", F, [F])
         _orc = lib
@@ -190,6 +195,8 @@ def _trace_sigs(lib):
     _sig(lib, "orc_compute_coefficients", None, [P, P, P, F, F, P])
     _sig(lib, "orc_dipole_bssrdf", None, [P, F, P])
     _sig(lib, "orc_dirpole_bssrdf", None, [P, P, P, P, P, P, P])
+    _sig(lib, "orc_bssrdf_queries_f", None, [P, P, P, F, F, U, L, P, P, I])
+    _sig(lib, "orc_bssrdf_queries_d", None, [P, P, P, F, F, U, L, P, P, I])
     lib._trace_bound = True
 
 
@@ -422,3 +429,63 @@ class OracleScene:
             self.close()
         except Exception:
             pass
+
+
+def bssrdf_queries(params, model, inputs, fp64=False, which="orc", threads=1):
+    """A batch of BSSRDF values S[3][n] of one translucent material.  params: (absorption[3],
+    scattering[3], meancosine[3], ior, scale) as pt_translucent_params holds them; model 0 (standard
+    dipole) takes inputs = dist[n], model 1 (directional) inputs = [15][n] (xi, ni, w12, xo, no).
+    which="ref" runs the reference's own dipoles compiled for the host on the FP32 coefficients of
+    the restatement (bit-identical to TranslucentMaterial::computeCoefficients); fp64 derives the
+    coefficients and evaluates in double."""
+    sa, ss, g, ior, scale = params
+    sa, ss, g = (np.ascontiguousarray(v, np.float32) for v in (sa, ss, g))
+    inputs = np.ascontiguousarray(inputs, np.float32)
+    n = inputs.shape[-1]
+    if which == "ref":
+        assert not fp64
+        lib = orc()
+        _trace_sigs(lib)
+        props = np.zeros(65, np.float32)
+        lib.orc_compute_coefficients(fp(sa), fp(ss), fp(g), ior, scale, fp(props))
+        out = np.empty((3, n), np.float32)
+        ref().ref_set_scattering_properties(fp(props), 260)
+        ref().ref_bssrdf_queries(model, n, fp(inputs), fp(out))
+        return out
+    lib = orc()
+    _trace_sigs(lib)
+    out = np.empty((3, n), np.float64 if fp64 else np.float32)
+    f = lib.orc_bssrdf_queries_d if fp64 else lib.orc_bssrdf_queries_f
+    f(fp(sa), fp(ss), fp(g), ior, scale, model, n, fp(inputs), fp(out), threads)
+    return out
+
+
+MF_OPS = {"dielectric_eval": 0, "dielectric_sample": 1, "conductor_eval": 2, "conductor_sample": 3, "diffuse_eval": 4,
+          "diffuse_sample": 5, "conductor_fresnel": 6, "visible_normal": 7}
+
+
+def microfacet_queries(op, dist, wi, wo, alpha, seed, order, normal=(0.0, 0.0, 1.0), eta=1.0 / 1.5, ior=(1.0, 0.0) * 3,
+                       rho=(1.0, 1.0, 1.0), fp64=False, which="orc", threads=1):
+    """A batch of multiscattering-walk / conductor-Fresnel queries (see orc_microfacet_queries_f):
+    returns (out[3][n], weight[3][n], seed after, order after)."""
+    op = MF_OPS[op] if isinstance(op, str) else int(op)
+    wi = np.ascontiguousarray(wi, np.float32)
+    wo = np.ascontiguousarray(wo, np.float32)
+    alpha = np.ascontiguousarray(alpha, np.float32)
+    seed = np.ascontiguousarray(seed, np.uint32).copy()
+    order = np.ascontiguousarray(order, np.uint32).copy()
+    n = alpha.size
+    n3 = np.asarray(normal, np.float32)
+    ior6 = np.asarray(ior, np.float64).reshape(6)
+    rho3 = np.asarray(rho, np.float32)
+    dt = np.float64 if fp64 else np.float32
+    out = np.zeros((3, n), dt)
+    weight = np.zeros((3, n), dt)
+    if which == "ref":
+        assert not fp64
+        ref().ref_microfacet_queries(op, dist, fp(n3), eta, fp(ior6), fp(rho3), n, fp(wi), fp(wo), fp(alpha), fp(seed), fp(order),
+                                     fp(out), fp(weight))
+    else:
+        f = orc().orc_microfacet_queries_d if fp64 else orc().orc_microfacet_queries_f
+        f(op, dist, fp(n3), eta, fp(ior6), fp(rho3), n, fp(wi), fp(wo), fp(alpha), fp(seed), fp(order), fp(out), fp(weight), threads)
+    return out, weight, seed, order

@@ -264,3 +264,90 @@ EXPORT void orc_direct_illumination_f(const float* pos, const void* lights, long
 }
 EXPORT float orc_C_phi_f(float n) { return C_phi<float>(n); }
 EXPORT float orc_C_E_f(float n) { return C_E<float>(n); }
+
+// --------------------------------------------------------------------------- batched walk queries
+// A batch of multiscattering-walk or conductor-Fresnel queries in the frame of the normal n3, the
+// calls the shaders make (Microfacet.h:95-177 in the world frame; Fresnel.h:78-91).  SoA inputs
+// wi[3][n], wo[3][n] (the evaluated direction; the microfacet normal for op 6), alpha[n] (ax = ay),
+// seed[n] (advanced in place), order[n] (the eval ops read it; the sample ops add the walk's
+// scattering events to it).  Outputs out[3][n]: the value (dielectric eval: the scalar in all three
+// channels), the sampled direction (sample ops) or F (op 6); weight[3][n]: the sample ops' weight
+// (conductor, diffuse).  ops: 0 dielectric eval, 1 dielectric sample, 2 conductor eval, 3 conductor
+// sample, 4 diffuse eval, 5 diffuse sample, 6 conductor Fresnel, 7 visible-normal sample with (z1, z2)
+// two rnd_tea draws from the seed.
+template <class R>
+static void mf_batch(unsigned op, unsigned dist, const float* n3, float eta, const double* ior6, const float* rho3, long n, const float* wi,
+                     const float* wo, const float* alpha, unsigned* seed, unsigned* order, R* out, R* weight, int threads)
+{
+  const V3<R> nn = ld<R>(n3);
+  const Cx3 e = ldc(ior6), ie = crecip3<R>(e);
+  const V3<R> rho = ld<R>(rho3);
+  auto work = [&](long k0, long k1) {
+    for (long k = k0; k < k1; ++k) {
+      const V3<R> a = v3((R)wi[k], (R)wi[n + k], (R)wi[2 * n + k]);
+      const V3<R> b = v3((R)wo[k], (R)wo[n + k], (R)wo[2 * n + k]);
+      const R al = (R)alpha[k];
+      u32 s = seed[k], o = order[k];
+      int capped = 0;
+      V3<R> r = v3s(R(0)), w = v3s(R(1)), wm;
+      switch (op) {
+        case 0: r = v3s(ms_dielectric_eval<R>((int)dist, to_local(a, nn), to_local(b, nn), (R)eta, al, al, s, o, 1 << 24, &capped)); break;
+        case 1: r = to_world(ms_dielectric_sample<R>((int)dist, to_local(a, nn), (R)eta, al, al, s, o, 1 << 24, &capped), nn); break;
+        case 2: r = ms_conductor_eval<R>((int)dist, to_local(a, nn), to_local(b, nn), e, ie, al, al, s, o, 1 << 24, &capped); break;
+        case 3: r = to_world(ms_conductor_sample<R>((int)dist, to_local(a, nn), wm, e, ie, al, al, s, o, w, 1 << 24, &capped), nn); break;
+        case 4: r = ms_diffuse_eval<R>((int)dist, to_local(a, nn), to_local(b, nn), al, al, s, rho, o, 1 << 24, &capped); break;
+        case 5: r = to_world(ms_diffuse_sample<R>((int)dist, to_local(a, nn), wm, al, al, s, o, w, rho), nn); break;
+        case 7: {
+          const R z1 = (R)rnd_tea(s), z2 = (R)rnd_tea(s);
+          r = sample_visible_normal<R>((int)dist, a, nn, al, al, z1, z2);
+          break;
+        }
+        default: r = fresnel_complex<R>(a, b, e); break;
+      }
+      seed[k] = s;
+      order[k] = o;
+      out[k] = r.x; out[n + k] = r.y; out[2 * n + k] = r.z;
+      if (weight) { weight[k] = w.x; weight[n + k] = w.y; weight[2 * n + k] = w.z; }
+    }
+  };
+  if (threads <= 1 || n < 1024) { work(0, n); return; }
+  std::vector<std::thread> th;
+  long chunk = (n + threads - 1) / threads;
+  for (int t = 0; t < threads; ++t) {
+    long k0 = t * chunk, k1 = std::min(n, k0 + chunk);
+    if (k0 < k1) th.emplace_back(work, k0, k1);
+  }
+  for (auto& x : th) x.join();
+}
+EXPORT void orc_microfacet_queries_f(unsigned op, unsigned dist, const float* n3, float eta, const double* ior6, const float* rho3, long n,
+                                     const float* wi, const float* wo, const float* alpha, unsigned* seed, unsigned* order, float* out,
+                                     float* weight, int threads)
+{
+  mf_batch<float>(op, dist, n3, eta, ior6, rho3, n, wi, wo, alpha, seed, order, out, weight, threads);
+}
+EXPORT void orc_microfacet_queries_d(unsigned op, unsigned dist, const float* n3, float eta, const double* ior6, const float* rho3, long n,
+                                     const float* wi, const float* wo, const float* alpha, unsigned* seed, unsigned* order, double* out,
+                                     double* weight, int threads)
+{
+  mf_batch<double>(op, dist, n3, eta, ior6, rho3, n, wi, wo, alpha, seed, order, out, weight, threads);
+}
+
+// The config-1 composition of bsdf_queries with the microfacet normal given instead of sampled:
+// wi = reflect(-wo, m), f, pdf and F as there (FP32).  Used to trace a query whose GPU result differs
+// from the oracle back to the sampled normal.
+EXPORT void orc_bsdf_given_m_f(long n, const int* dist_of, const float* wo_soa, const float* alpha, float eta, const float* m_soa,
+                               float* wi_soa, float* f, float* pdf, float* F)
+{
+  const V3<float> nrm = v3(0.0f, 0.0f, 1.0f);
+  for (long k = 0; k < n; ++k) {
+    const int dist = dist_of[k];
+    V3<float> wo = v3(wo_soa[k], wo_soa[n + k], wo_soa[2 * n + k]);
+    V3<float> m = v3(m_soa[k], m_soa[n + k], m_soa[2 * n + k]);
+    const float a = alpha[k];
+    V3<float> wi = reflect(-wo, m);
+    f[k] = walter_bsdf(dist, wo, wi, nrm, a, eta);
+    pdf[k] = eval_visible_normal(dist, wo, m, nrm, a, a) / (4.0f * std::fabs(dot(wo, m)));
+    F[k] = fresnel_R(wo, m, eta);
+    wi_soa[k] = wi.x; wi_soa[n + k] = wi.y; wi_soa[2 * n + k] = wi.z;
+  }
+}

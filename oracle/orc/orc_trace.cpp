@@ -1603,6 +1603,55 @@ EXPORT void orc_dirpole_bssrdf(const void* props260, const float* xi, const floa
   out3[0] = r.x; out3[1] = r.y; out3[2] = r.z;
 }
 
+// Runs fn(k0, k1) over [0, n) in contiguous chunks on `threads` host threads.
+template <class Fn> static void parallel_for(long n, int threads, Fn fn)
+{
+  threads = std::max(1, threads);
+  if (threads == 1 || n < 4096) { fn(0, n); return; }
+  const long chunk = (n + threads - 1) / threads;
+  std::vector<std::thread> th;
+  for (int t = 0; t < threads; ++t) {
+    const long k0 = t * chunk, k1 = std::min(n, k0 + chunk);
+    if (k0 >= k1) break;
+    th.emplace_back(fn, k0, k1);
+  }
+  for (auto& x : th) x.join();
+}
+
+// A batch of BSSRDF queries of one translucent material given by its raw parameters (absorption,
+// scattering, meancosine per RGB, ior, scale: pt_translucent_params), coefficients derived and the
+// dipole evaluated in R: standard dipole (model 0) on dist[n], directional (model 1) on 15 x n SoA
+// geometry (xi, ni, w12, xo, no).  S is 3 x n SoA.
+template <class R>
+static void bssrdf_batch(const float* sa, const float* ss, const float* g, float ior, float scale, unsigned model, long n, const float* in, R* S,
+                         int threads)
+{
+  const ScatPropsT<R> P = compute_coefficients_t<R>(sa, ss, g, ior, scale);
+  parallel_for(n, threads, [&](long k0, long k1) {
+    for (long k = k0; k < k1; ++k) {
+      V3<R> r;
+      if (model == 0) {
+        r = dipole_bssrdf<R>((R)in[k], P);
+      } else {
+        V3<R> v[5];
+        for (int j = 0; j < 5; ++j) v[j] = v3<R>(in[(3 * j) * n + k], in[(3 * j + 1) * n + k], in[(3 * j + 2) * n + k]);
+        r = dirpole_bssrdf<R>(v[0], v[1], v[2], v[3], v[4], P);
+      }
+      S[k] = r.x; S[n + k] = r.y; S[2 * n + k] = r.z;
+    }
+  });
+}
+EXPORT void orc_bssrdf_queries_f(const float* sa, const float* ss, const float* g, float ior, float scale, unsigned model, long n,
+                                 const float* in, float* S, int threads)
+{
+  bssrdf_batch<float>(sa, ss, g, ior, scale, model, n, in, S, threads);
+}
+EXPORT void orc_bssrdf_queries_d(const float* sa, const float* ss, const float* g, float ior, float scale, unsigned model, long n,
+                                 const float* in, double* S, int threads)
+{
+  bssrdf_batch<double>(sa, ss, g, ior, scale, model, n, in, S, threads);
+}
+
 EXPORT long orc_capped(void* scene) { return ((Scene*)scene)->capped.load(); }
 
 // Closest / any hit for a batch of rays (origin.xyz, tmin, dir.xyz, tmax per 8 floats): BVH

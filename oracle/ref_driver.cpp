@@ -236,6 +236,37 @@ EXPORT void ref_ms_diffuse_sample(const float* wi, const float* n, float ax, flo
   st3(weight_out, weight);
 }
 
+// The batch of walk / conductor-Fresnel queries of orc_microfacet_queries_f (same layout and ops), on
+// the reference's own functions.
+EXPORT void ref_microfacet_queries(unsigned int op, unsigned int dist, const float* n3, float eta, const double* ior6, const float* rho3,
+                                   long n, const float* wi, const float* wo, const float* alpha, unsigned int* seed,
+                                   unsigned int* order, float* out, float* weight)
+{
+  for (long k = 0; k < n; ++k) {
+    const float a[3] = {wi[k], wi[n + k], wi[2 * n + k]};
+    const float b[3] = {wo[k], wo[n + k], wo[2 * n + k]};
+    float r[3] = {0.0f, 0.0f, 0.0f}, w[3] = {1.0f, 1.0f, 1.0f};
+    switch (op) {
+      case 0: r[0] = r[1] = r[2] = ref_ms_dielectric_eval(a, b, n3, eta, alpha[k], alpha[k], seed + k, order[k], dist); break;
+      case 1: ref_ms_dielectric_sample(a, n3, eta, alpha[k], alpha[k], seed + k, order + k, dist, r); break;
+      case 2: ref_ms_conductor_eval(a, b, n3, ior6, alpha[k], alpha[k], seed + k, order[k], dist, r); break;
+      case 3: ref_ms_conductor_sample(a, n3, ior6, alpha[k], alpha[k], seed + k, order + k, dist, r, w); break;
+      case 4: ref_ms_diffuse_eval(a, b, n3, alpha[k], alpha[k], seed + k, order[k], rho3, dist, r); break;
+      case 5: ref_ms_diffuse_sample(a, n3, alpha[k], alpha[k], seed + k, order + k, rho3, dist, r, w); break;
+      case 7: {
+        uint s = seed[k];
+        const float z1 = rnd_tea(s), z2 = rnd_tea(s);
+        seed[k] = s;
+        ref_sample_visible_normal(a, n3, alpha[k], alpha[k], z1, z2, dist, r);
+        break;
+      }
+      default: ref_fresnel_complex(a, b, ior6, r); break;
+    }
+    out[k] = r[0]; out[n + k] = r[1]; out[2 * n + k] = r[2];
+    if (weight) { weight[k] = w[0]; weight[n + k] = w[1]; weight[2 * n + k] = w[2]; }
+  }
+}
+
 // ---------------------------------------------------------------- sampling helpers
 EXPORT void ref_sample_cosine_weighted(const float* n, unsigned int* seed, float* out3)
 {
@@ -313,6 +344,22 @@ EXPORT void ref_dirpole_bssrdf(const float* xi, const float* ni, const float* w1
                                const float* no, float* out3)
 {
   st3(out3, dirpole_bssrdf(ld3(xi), ld3(ni), ld3(w12), ld3(xo), ld3(no), g_props));
+}
+// A batch of BSSRDF queries on the properties set last: standard dipole (model 0) on dist[n], or the
+// directional dipole (model 1) on 15 x n SoA geometry (xi, ni, w12, xo, no); S is 3 x n SoA.
+EXPORT void ref_bssrdf_queries(unsigned int model, long n, const float* in, float* S)
+{
+  for (long k = 0; k < n; ++k) {
+    float3 r;
+    if (model == 0) {
+      r = dipole_bssrdf(in[k], g_props);
+    } else {
+      float3 v[5];
+      for (int j = 0; j < 5; ++j) v[j] = make_float3(in[(3 * j) * n + k], in[(3 * j + 1) * n + k], in[(3 * j + 2) * n + k]);
+      r = dirpole_bssrdf(v[0], v[1], v[2], v[3], v[4], g_props);
+    }
+    S[k] = r.x; S[n + k] = r.y; S[2 * n + k] = r.z;
+  }
 }
 EXPORT float ref_C_phi(float n) { return C_phi(n); }
 EXPORT float ref_C_E(float n) { return C_E(n); }

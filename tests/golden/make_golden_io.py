@@ -5,6 +5,7 @@ for the host by oracle/Makefile.  It reads the sample files of tests/io_samples.
 own data/CedarCity.hdr and data/Plane.obj; what it returns is recorded here (the .hdr texels as RGB
 float32 -- the reference leaves the fourth channel undefined -- and the .obj arrays as ObjLoader
 flattens them).  Run from the repository root:  python tests/golden/make_golden_io.py
+(ORF_REFERENCE names the reference checkout whose data/ folder is read).
 """
 import ctypes
 import hashlib
@@ -20,7 +21,7 @@ sys.path.insert(0, os.path.dirname(HERE))
 import io_samples  # noqa: E402
 
 REF_IO = os.path.join(ROOT, "oracle", "_ref", "libref_io.so")
-REF_DATA = "/root/reference/data"
+REF_DATA = os.path.join(os.environ.get("ORF_REFERENCE", "/root/reference"), "data")
 OUT = os.path.join(HERE, "ref_io.npz")
 
 

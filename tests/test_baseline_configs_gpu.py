@@ -1,0 +1,140 @@
+"""GPU parity at the benchmark configurations' own sizes, against the CPU restatement of the
+reference's recursive tracer (oracle/orc/orc_trace.cpp), on bands of the full-size images.
+
+* Single scene (512 x 512, depth 8, Russian roulette from depth 3, the 12 + 81,920 + 20,480 + 2
+  triangle scene): a 32-row band over 4 frames -- at least 97% of its pixels within 1e-3 relative and
+  relMSE below 1e-3 (the image bar of the render tests); and a 16-row band at the configuration's 64
+  spp, whose relMSE against the oracle must be below the oracle's own sample variance (relMSE of one
+  half of the frames against the other half).
+* Subsurface (1024 x 1024, 327,680-triangle jittered icosphere, standard dipole with the seeded
+  coefficients, 4,096 probes per frame, 2048 x 1024 sky + sun as background and light): an 8-row band
+  through the sphere over 2 frames -- 95% of pixels within 1e-3 and relMSE below 1e-4 (the translucent
+  bars: the gathers' MD5 streams are identical, an acceptance test exp_term against a draw can flip
+  where CUDA's expf and glibc's differ by an ulp).
+* Batched: the first heightfield scene and the first dipole scene of the 64-scene batch, at their
+  full resolution and triangle count, rendered together by one batched pass (pt_batch_render), compared
+  on a 16-row band over 2 frames with the scene-by-scene image bars.
+The bands are rendered on the GPU through the camera patch (patch_origin / patch_dims,
+path_tracer.cu:36-43) and on the CPU over the same pixel range; the random streams are keyed by the
+full-image pixel index in both, so the band is the same sample set as the full image's rows.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle_ctypes as oc
+from open_rendering_framework_b200 import scene as sc
+from open_rendering_framework_b200 import scenes
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+THREADS = os.cpu_count() or 1
+
+
+def rel_mse(img, ref):
+    img = np.asarray(img, np.float64)[..., :3]
+    ref = np.asarray(ref, np.float64)[..., :3]
+    return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+def pixel_fraction(got, ref, tol=1e-3):
+    r = np.abs(got[..., :3].astype(np.float64) - ref[..., :3]) / np.maximum(np.abs(ref[..., :3]), 1e-3)
+    return float(np.mean(np.all(r <= tol, axis=-1)))
+
+
+def gpu_band(data, y0, rows, frames):
+    W = data.camera.width
+    data.camera.patch_origin = (0, y0)
+    data.camera.patch_dims = (W - 1, rows - 1)
+    R = sc.Renderer(data)
+    R.render(frames)
+    img = R.readback()
+    st = R.stats()
+    R.close()
+    data.camera.patch_origin = (0, 0)
+    data.camera.patch_dims = (W, data.camera.height)
+    return img[y0:y0 + rows], st
+
+
+def oracle_band(data, y0, rows, frames, path_radiance=False):
+    W, H = data.camera.width, data.camera.height
+    O = oc.OracleScene(data)
+    acc, pr = O.render(0, frames, accum=np.zeros((H, W, 4), np.float32), p_begin=W * y0, p_end=W * (y0 + rows),
+                       path_radiance=path_radiance, threads=THREADS)
+    O.close()
+    return acc[y0:y0 + rows], pr
+
+
+def test_single_scene_configuration_band_matches_oracle():
+    data = scenes.single_scene()
+    assert (data.camera.width, data.camera.height) == (512, 512) and data.n_triangles() == 12 + 81920 + 20480 + 2
+    y0, rows, frames = 240, 32, 4
+    got, st = gpu_band(data, y0, rows, frames)
+    ref, _ = oracle_band(data, y0, rows, frames)
+    assert st.path_samples == 512 * rows * frames
+    frac, err = pixel_fraction(got, ref), rel_mse(got, ref)
+    print("single-scene band %d rows x 512 x %d frames: %.4f of pixels within 1e-3, relMSE %.3e, %.2f segments per path" % (
+        rows, frames, frac, err, st.segments / st.path_samples))
+    assert np.all(np.isfinite(got))
+    assert frac >= 0.97 and err < 1e-3
+
+
+def test_single_scene_configuration_converged_band_below_sample_variance():
+    data = scenes.single_scene()
+    y0, rows, spp = 300, 16, 64
+    got, _ = gpu_band(data, y0, rows, spp)
+    ref, pr = oracle_band(data, y0, rows, spp, path_radiance=True)
+    a = pr[: spp // 2].mean(axis=0).reshape(rows, 512, 3)
+    b = pr[spp // 2:].mean(axis=0).reshape(rows, 512, 3)
+    half = rel_mse(a, b)
+    err = rel_mse(got, ref)
+    print("single-scene converged band (16 rows x 512 x 64 spp): relMSE GPU vs oracle %.3e, oracle half-vs-half %.3e" % (err, half))
+    assert err < half
+    assert err < 2e-3
+
+
+def test_subsurface_configuration_band_matches_oracle():
+    data = scenes.subsurface_scene()
+    assert (data.camera.width, data.camera.height) == (1024, 1024) and data.n_triangles() == 327680
+    y0, rows, frames = 508, 8, 2
+    got, st = gpu_band(data, y0, rows, frames)
+    ref, _ = oracle_band(data, y0, rows, frames)
+    frac, err = pixel_fraction(got, ref), rel_mse(got, ref)
+    print("subsurface band %d rows x 1024 x %d frames: %.4f of pixels within 1e-3, relMSE %.3e, %d gathers, %d pairs" % (
+        rows, frames, frac, err, st.dipole_gathers, st.dipole_pairs))
+    assert st.dipole_gathers > 0
+    assert np.all(np.isfinite(got))
+    assert frac >= 0.95 and err < 1e-4
+
+
+def first_scene(S, pred):
+    for k, (d, spp, info) in enumerate(S):
+        if pred(info):
+            return k, d, info
+    raise AssertionError("no such scene in the batch")
+
+
+def test_batched_configuration_scenes_match_oracle():
+    S = scenes.batch_scenes(64, seed=0)
+    kh, dh, ih = first_scene(S, lambda i: i["mesh"] == "grid")
+    kd, dd, idp = first_scene(S, lambda i: i["material"] == "dipole")
+    frames = 2
+    Rs = [sc.Renderer(dh), sc.Renderer(dd)]
+    B = sc.Batch(Rs, [frames, frames])
+    B.render()
+    imgs = [R.readback() for R in Rs]
+    B.close()
+    for R in Rs:
+        R.close()
+    for k, d, info, img in ((kh, dh, ih, imgs[0]), (kd, dd, idp, imgs[1])):
+        H = d.camera.height
+        rows = 16
+        y0 = H // 2 - rows // 2
+        ref, _ = oracle_band(d, y0, rows, frames)
+        got = img[y0:y0 + rows]
+        frac, err = pixel_fraction(got, ref), rel_mse(got, ref)
+        print("batch scene %d (%s): %.4f of band pixels within 1e-3, relMSE %.3e" % (k, info, frac, err))
+        assert np.all(np.isfinite(got))
+        assert frac >= 0.95 and err < 1e-3, (k, info, frac, err)

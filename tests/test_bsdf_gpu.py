@@ -9,7 +9,8 @@ Bars (stated in the tests):
   atan2f, tanf, erff, ...) differ by 1-2 ulp on a few percent of arguments, and the sampled normal
   feeds D(m), whose relative sensitivity grows like 1/alpha^2, so a last-bit difference in m becomes
   1e-5..1e-2 in f on ~0.5% of queries.  The FP32 reference itself is off by up to 0.3-350x relative
-  from FP64 on the worst queries.  Maxima and percentiles are written to gpurun_out/.
+  from FP64 on the worst queries.  Maxima, percentiles and the worst query indices are printed and
+  written to the test's temporary directory.
 """
 import ctypes
 import json
@@ -76,7 +77,7 @@ def run_gpu_queries(wo, alpha, first, n_ggx_below, eta):
 
 
 @pytest.mark.parametrize("first,ggx_fraction", [(0, 0.5), (1 << 21, 1.0), (3 << 20, 0.0)])
-def test_bsdf_queries_match_oracle(first, ggx_fraction):
+def test_bsdf_queries_match_oracle(first, ggx_fraction, tmp_path):
     n = 1 << 18
     eta = np.float32(1.0 / 1.5)
     wo, alpha = oc.c1_inputs(n, first)
@@ -106,13 +107,12 @@ def test_bsdf_queries_match_oracle(first, ggx_fraction):
             "p99.99_fp32_oracle_vs_fp64": float(np.quantile(e3264, 0.9999)),
         }
         worst[name] = [int(first + i) for i in np.argsort(e)[-8:]]
-    os.makedirs("gpurun_out", exist_ok=True)
-    with open(os.path.join("gpurun_out", "bsdf_parity_%d.json" % first), "w") as fh:
+    with open(tmp_path / ("bsdf_parity_%d.json" % first), "w") as fh:
         json.dump({"report": report, "worst_query_indices": worst}, fh, indent=1)
     for name, r in report.items():
         assert r["fraction_within_1e-5"] >= MIN_FRACTION, (name, r)
         assert r["p99.99_gpu_vs_fp64"] <= FP64_P9999_RATIO * r["p99.99_fp32_oracle_vs_fp64"] + 1e-7, (name, r)
-    print(json.dumps({"first": first, "ggx_fraction": ggx_fraction, "n": n, "report": report}))
+    print(json.dumps({"first": first, "ggx_fraction": ggx_fraction, "n": n, "report": report, "worst_query_indices": worst}))
 
 
 def test_bsdf_queries_host_path_matches_device_path():
@@ -139,3 +139,75 @@ def test_empty_and_edge_inputs():
             assert np.array_equal(np.isfinite(g), np.isfinite(r))
             m = np.isfinite(r)
             assert np.all(rel_err(g[m], r[m], 1e-6) < 1e-4)
+
+
+def ulp_distance(a, b):
+    """Distance in units in the last place between float32 arrays (same sign assumed near zero)."""
+    ia = np.ascontiguousarray(a, np.float32).view(np.int32).astype(np.int64)
+    ib = np.ascontiguousarray(b, np.float32).view(np.int32).astype(np.int64)
+    ia = np.where(ia < 0, -(ia & 0x7FFFFFFF), ia)
+    ib = np.where(ib < 0, -(ib & 0x7FFFFFFF), ib)
+    return np.abs(ia - ib)
+
+
+def gpu_visible_normals(wo, alpha, seeds, dist):
+    """The microfacet normals the BSDF kernel samples, from the same device function
+    (pt_microfacet_queries, PT_MSQ_VISIBLE_NORMAL, normal +z)."""
+    from open_rendering_framework_b200 import scene as sc
+
+    n = alpha.size
+    b = sc.MicrofacetBatch(sc.MSQ_OPS["visible_normal"], dist, (ctypes.c_float * 3)(0.0, 0.0, 1.0), 0.0, (ctypes.c_double * 6)(1, 0, 1, 0, 1, 0),
+                           (ctypes.c_float * 3)(1, 1, 1))
+    d_wo, d_a = dev(wo), dev(alpha)
+    d_seed = dev(seeds.view(np.int32))
+    d_order = torch.zeros(n, dtype=torch.int32, device="cuda")
+    out = torch.empty((3, n), dtype=torch.float32, device="cuda")
+    nat.call("pt_microfacet_queries", ctypes.byref(b), d_wo.data_ptr(), d_wo.data_ptr(), d_a.data_ptr(), d_seed.data_ptr(),
+             d_order.data_ptr(), n, out.data_ptr(), None, None)
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+@pytest.mark.parametrize("first", [0, 3 << 20])
+def test_bsdf_queries_outside_1e5_trace_to_the_sampled_normal(first):
+    """Triage of every query outside 1e-5: (a) the GPU's sampled microfacet normal differs from the
+    FP32 oracle's in its last bits (the transcendentals of the slope sampling: acosf / atan2f / tanf
+    for GGX, erff and the erfinv Newton loop for Beckmann); (b) the oracle's own FP32 composition
+    evaluated at the GPU's normal reproduces the GPU's wi bit for bit and its f, pdf and F within
+    1e-5.  Every outlier must fall in that class: the residue is last-ulp transcendental difference in
+    the sampling step, not a difference of logic."""
+    n = 1 << 18
+    n_ggx_below = first + n // 2
+    eta = np.float32(1.0 / 1.5)
+    wo, alpha = oc.c1_inputs(n, first)
+    g_wi, g_f, g_pdf, g_F = run_gpu_queries(wo, alpha, first, n_ggx_below, eta)
+    r_wi, r_f, r_pdf, r_F = oc.bsdf_queries(n, first, n_ggx_below, wo, alpha, eta=eta, threads=os.cpu_count() or 1)
+    e = np.maximum.reduce([np.linalg.norm(g_wi.astype(np.float64) - r_wi, axis=0), rel_err(g_f, r_f), rel_err(g_pdf, r_pdf), rel_err(g_F, r_F)])
+    idx = np.flatnonzero(e > REL_TOL)
+    assert idx.size < 0.01 * n
+    O = oc.orc()
+    seeds = np.array([O.orc_tea16(int(first + k), 0) for k in idx], np.uint32)
+    dist = np.where(first + idx < n_ggx_below, 1, 0).astype(np.int32)
+    wo_b = np.ascontiguousarray(wo[:, idx])
+    a_b = np.ascontiguousarray(alpha[idx])
+    m_gpu = np.empty((3, idx.size), np.float32)
+    m_orc = np.empty((3, idx.size), np.float32)
+    for d in (0, 1):
+        sel = np.flatnonzero(dist == d)
+        if sel.size == 0:
+            continue
+        m_gpu[:, sel] = gpu_visible_normals(np.ascontiguousarray(wo_b[:, sel]), np.ascontiguousarray(a_b[sel]), seeds[sel].copy(), d)
+        m_orc[:, sel] = oc.microfacet_queries("visible_normal", d, wo_b[:, sel], wo_b[:, sel], a_b[sel], seeds[sel], np.zeros(sel.size))[0]
+    wi2 = np.empty((3, idx.size), np.float32)
+    f2, pdf2, F2 = (np.empty(idx.size, np.float32) for _ in range(3))
+    O.orc_bsdf_given_m_f(idx.size, oc.fp(dist), oc.fp(wo_b), oc.fp(a_b), eta, oc.fp(m_gpu), oc.fp(wi2), oc.fp(f2), oc.fp(pdf2), oc.fp(F2))
+    ulps = ulp_distance(m_gpu, m_orc).max(axis=0)
+    normal_differs = ulps > 0
+    wi_same = np.all(wi2.view(np.uint32) == g_wi[:, idx].view(np.uint32), axis=0)
+    eval_same = np.maximum.reduce([rel_err(g_f[idx], f2), rel_err(g_pdf[idx], pdf2), rel_err(g_F[idx], F2)]) <= REL_TOL
+    explained = normal_differs & wi_same & eval_same
+    report = {"queries": n, "outside_1e-5": int(idx.size), "normal_differs": int(normal_differs.sum()), "wi_reproduced": int(wi_same.sum()),
+              "f_pdf_F_reproduced": int(eval_same.sum()), "explained": int(explained.sum()),
+              "ulps_of_normal_p50_p99_max": [int(np.quantile(ulps, 0.5)), int(np.quantile(ulps, 0.99)), int(ulps.max())] if idx.size else None}
+    print("bsdf triage first=%d: %s" % (first, json.dumps(report)))
+    assert report["explained"] == idx.size, report

@@ -14,7 +14,6 @@ from open_rendering_framework_b200 import _native as nat
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
-REL_TOL = 1e-5  # the tolerance of the BSDF parity tests
 MAX_QUERIES = 65536
 
 
@@ -26,11 +25,10 @@ def run(entry, wo, alpha, first, n_ggx):
     return wi, f, pdf, F
 
 
-def close(a, b):
-    a = np.asarray(a, np.float64)
-    b = np.asarray(b, np.float64)
-    both_nan = np.isnan(a) & np.isnan(b)
-    return bool(np.all(both_nan | (np.abs(a - b) <= REL_TOL * np.maximum(np.abs(b), 1e-30))))
+def same_bits(a, b):
+    """Both entry points run the same kernel on the same inputs, so every output word -- NaNs
+    included -- must be identical."""
+    return bool(np.array_equal(np.ascontiguousarray(a).view(np.uint32), np.ascontiguousarray(b).view(np.uint32)))
 
 
 def test_noalloc_matches_allocating_entry_on_two_calls_in_a_row():
@@ -40,7 +38,7 @@ def test_noalloc_matches_allocating_entry_on_two_calls_in_a_row():
         got = run("pt_bsdf_queries_host_noalloc", wo, alpha, first, n_ggx)
         ref = run("pt_bsdf_queries_host", wo, alpha, first, n_ggx)
         for g, r in zip(got, ref):
-            assert close(g, r)
+            assert same_bits(g, r)
 
 
 def test_noalloc_rejects_batches_beyond_the_array():
