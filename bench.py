@@ -78,7 +78,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="single_scene", choices=["single_scene", "subsurface", "batched", "adjoint", "bsdf", "ingest"])
+    ap.add_argument("--workload", default="single_scene", choices=["single_scene", "subsurface", "batched", "adjoint", "bsdf", "ingest", "build"])
     ap.add_argument("--queries", type=int, default=1 << 22, help="bsdf workload: queries per step")
     ap.add_argument("--scenes", type=int, default=64, help="batched workload: number of scenes")
     ap.add_argument("--spp", type=int, default=None, help="frames per step (default 64, subsurface 256)")
@@ -618,6 +618,10 @@ def run_reference(args, world, rank):
         return run_reference_bsdf(args)
     if args.workload == "ingest":
         return run_reference_ingest(args)
+    if args.workload == "build":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference builds its BVH inside OptiX (Trbvh / Sbvh, "
+                                                              "OptixSceneLoader.cpp:136), which has no CPU build and is not on this box"}), flush=True)
+        return
     data, _, desc = workload(args)
     from oracle import oracle_ctypes as oc
 
@@ -940,6 +944,89 @@ def run_adjoint(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+BUILD = ("BVH build: the subsurface configuration's 327,680-triangle jittered icosphere and the 64 meshes of the batched "
+         "configuration (1e3-5e5 triangles each), host binned-SAH builder vs device LBVH builder (option bvh_builder); "
+         "the single-scene render (512x512, 64 spp) traced over each builder's tree")
+
+
+def run_build(args, world, rank, local):
+    """Milliseconds per million triangles of the device LBVH builder (Morton codes, radix sort, Karras
+    hierarchy, SAH leaves, 4-wide collapse, all on the device) against the host binned-SAH builder,
+    and the single-scene render speed over each tree (the trees' quality)."""
+    import torch
+
+    from open_rendering_framework_b200 import scene as sc
+    from open_rendering_framework_b200 import scenes
+
+    torch.cuda.set_device(local)
+    reps = max(3, args.steps)
+
+    def build_times(data, builder):
+        R = sc.Renderer(data, device=local, build_options={"bvh_builder": builder})
+        for _ in range(max(1, args.warmup)):
+            R.rebuild(bvh_builder=builder)
+        ms, dev = [], []
+        for _ in range(reps):
+            R.rebuild(bvh_builder=builder)
+            b = R.build_info()
+            ms.append(b.build_ms)
+            dev.append(b.device_ms)
+        info = R.build_info().as_dict()
+        R.close()
+        return statistics.median(ms), statistics.median(dev), info
+
+    with ClockSampler(local) as clocks:
+        c3 = scenes.subsurface_scene(64, 64)  # the mesh is what is built; a small camera keeps set-up cheap
+        c3_host = build_times(c3, 0)
+        c3_dev = build_times(c3, 1)
+        S = scenes.batch_scenes(args.scenes, seed=0, size_scale=1 / 16)
+        tot_tris = sum(d.n_triangles for d, _, _ in S)
+        c4 = {0: [0.0, 0.0], 1: [0.0, 0.0]}
+        for d, _, _ in S:
+            for b in (0, 1):
+                ms, dev, _ = build_times(d, b)
+                c4[b][0] += ms
+                c4[b][1] += dev
+        # the trees' quality: the single-scene render over each
+        render = {}
+        data = scenes.single_scene()
+        for b in (0, 1):
+            R = sc.Renderer(data, device=local, build_options={"bvh_builder": b})
+            for _ in range(max(1, args.warmup)):
+                R.render(64)
+            stream = torch.cuda.ExternalStream(R.stream())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            n = max(3, args.steps // 2)
+            for _ in range(n):
+                R.render(64)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            render[b] = {"value": n * 512 * 512 * 64 / (e0.elapsed_time(e1) * 1e-3) / 1e6, "unit": UNIT, "sah_cost": R.build_info().sah_cost,
+                         "build": R.build_info().as_dict()}
+            R.close()
+    n3 = c3_dev[2]["n_triangles"]
+    per_m = lambda ms, n: ms / (n / 1e6)
+    line = {
+        "metric": "ms per million triangles (BVH build, device LBVH)", "value": per_m(c3_dev[0], n3), "unit": "ms/Mtri", "n_gpus": 1,
+        "steps": reps, "warmup": max(1, args.warmup), "ms_per_step": c3_dev[0], "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": BUILD, "triangles": n3, "batch_meshes": len(S), "batch_triangles": tot_tris},
+        "subsurface_mesh": {"device": {"ms": c3_dev[0], "device_ms": c3_dev[1], "ms_per_mtri": per_m(c3_dev[0], n3), "tree": c3_dev[2]},
+                            "host": {"ms": c3_host[0], "ms_per_mtri": per_m(c3_host[0], n3), "tree": c3_host[2]},
+                            "host_over_device": c3_host[0] / c3_dev[0]},
+        "batch_meshes": {"device": {"ms": c4[1][0], "device_ms": c4[1][1], "ms_per_mtri": per_m(c4[1][0], tot_tris)},
+                         "host": {"ms": c4[0][0], "ms_per_mtri": per_m(c4[0][0], tot_tris)}, "host_over_device": c4[0][0] / c4[1][0]},
+        "single_scene_render": {"host_tree": render[0], "device_tree": render[1], "device_over_host": render[1]["value"] / render[0]["value"]},
+        "e2e": {"value": per_m(c3_dev[0], n3), "unit": "ms/Mtri", "h2d_bytes_per_step": 36 * n3, "d2h_bytes_per_step": 0,
+                "what": "pt_build's BVH step through the C ABI from the host triangle list (upload included)"},
+        "cpu_baseline": {"value": per_m(c3_host[0], n3), "unit": "ms/Mtri", "cores": os.cpu_count() or 1, "kind": "port",
+                         "sample": "the library's host binned-SAH builder on the same mesh (the reference's OptiX builders cannot run here)"},
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -1116,6 +1203,9 @@ def main():
         elif args.workload == "adjoint":
             if rank == 0:
                 run_adjoint(args, world, rank, local)
+        elif args.workload == "build":
+            if rank == 0:
+                run_build(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -250,6 +250,23 @@ typedef struct pt_render_stats {
   float gather_ms;          /* device time of the dipole gather kernel (when profiling)       */
 } pt_render_stats;
 
+/* The acceleration structure of the last pt_build (no counterpart in the reference, whose OptiX
+ * builders report nothing). */
+typedef struct pt_build_info {
+  uint32_t builder;       /* 0: binned SAH on the host (default); 1: LBVH on the device (option "bvh_builder") */
+  uint32_t n_triangles;
+  uint32_t bvh2_nodes;    /* child-pair nodes written                                                */
+  uint32_t bvh2_depth;    /* levels including the leaves                                             */
+  uint32_t wide_nodes;    /* 4-wide nodes (0 when the 4-wide tree is too deep for the traversal)      */
+  uint32_t wide_depth;
+  float build_ms;         /* wall time of the BVH step of pt_build (the device builder's includes its
+                             upload of the triangles and its per-level synchronisations)             */
+  float device_ms;        /* device builder: time between CUDA events around its work on the stream */
+  float sah_cost;         /* SAH cost of the BVH2: node step cost (option bvh_trav_cost_milli) plus
+                             the children's costs weighted by their surface areas, one per triangle
+                             in a leaf; computed by pt_get_build_info                                 */
+} pt_build_info;
+
 /* Create / destroy a context on CUDA device `device`. */
 pt_status pt_context_create(int device, pt_ctx** out);
 pt_status pt_context_destroy(pt_ctx* ctx);
@@ -328,12 +345,18 @@ pt_status pt_get_render_stats(pt_ctx* ctx, pt_render_stats* out);
  *   "refill"       persistent kernels refill a warp when at least this many lanes are idle (1..32, default 20)
  *   "bvh4"         1 = the persistent kernels walk the 4-wide BVH (default), 0 = the BVH2
  *   "bvh_trav_cost_milli"  SAH cost of a node step x 1000 relative to a triangle test (default 1200) and
- *   "bvh_max_leaf"         the largest leaf the SAH may choose (1..15, default 8): applied by the next pt_build */
+ *   "bvh_max_leaf"         the largest leaf the SAH may choose (1..15, default 8): applied by the next pt_build
+ *   "bvh_builder"  0 = binned SAH on the host threads (default), 1 = LBVH on the device (Morton codes,
+ *                  radix sort, Karras hierarchy, SAH leaves, device 4-wide collapse; the reference's
+ *                  OptiX builders, OptixSceneLoader.cpp:136, also run on the device): next pt_build */
 pt_status pt_set_option(pt_ctx* ctx, const char* name, int64_t value);
 /* When enabled, CUDA events bracket every extend (closest-hit) and dipole-gather launch and
  * pt_get_render_stats reports their summed device times in extend_ms and gather_ms.  Off by default (the events serialise nothing
  * but cost a few microseconds per bounce). */
 pt_status pt_set_profiling(pt_ctx* ctx, int enable);
+/* The acceleration structure of the last pt_build, with its SAH cost evaluated on the host (the
+ * device-built tree is read back for that). */
+pt_status pt_get_build_info(pt_ctx* ctx, pt_build_info* out);
 /* Textures (no counterpart in the reference's shaders, which read constant material parameters; they
  * carry the per-texel parameters of differentiable renders).  A texture is width x height texels of 1
  * or 3 float channels, texel (x, y) channel c at [(y*width + x)*channels + c].  pt_texture_create

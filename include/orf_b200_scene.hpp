@@ -117,6 +117,27 @@ class ConstantBackground {
   float3 background_color;
 };
 
+// EnvMapBackground (Background.h:44, Background.cpp:57-69): an equirectangular environment map, either
+// float4 texels (width x height, row 0 at v = 0) or a Radiance .hdr file read as the reference's
+// loadHDRTexture reads it (pt_set_envmap_hdr: host parse, device RGBE expansion, CDF build).
+class EnvMapBackground {
+ public:
+  explicit EnvMapBackground(std::string hdr_path) : path(std::move(hdr_path)) {}
+  EnvMapBackground(std::vector<float> rgba, uint32_t width, uint32_t height) : texels(std::move(rgba)), w(width), h(height) {}
+  void apply(pt_ctx* ctx) const
+  {
+    if (!path.empty())
+      check(pt_set_envmap_hdr(ctx, path.c_str()), "pt_set_envmap_hdr");
+    else
+      check(pt_set_envmap(ctx, texels.data(), w, h), "pt_set_envmap");
+  }
+
+ private:
+  std::string path;
+  std::vector<float> texels;
+  uint32_t w = 0, h = 0;
+};
+
 // ---------------------------------------------------------------- Material.h
 class MyMaterial {
  public:
@@ -180,16 +201,226 @@ class RoughTransparentMaterial : public MyMaterial {
   }
 };
 
+// TransparentMaterial (Material.h:230, TransparentMaterial.cpp:7-20): smooth dielectric.
+class TransparentMaterial : public MyMaterial {
+ public:
+  float ior = 1.3f;
+  float3 glass_absorption{0, 0, 0};
+  void setIor(float i) { ior = i; }
+  void setAbsorption(float3 a) { glass_absorption = a; }
+  uint32_t getType() const override { return PT_TRANSPARENT_SHADER; }
+  std::vector<unsigned char> params() const override
+  {
+    pt_transparent_params p;
+    p.ior = ior;
+    memcpy(p.glass_absorption, glass_absorption.data(), 12);
+    return DiffuseMaterial::bytes(p);
+  }
+};
+// LambertianInterfaceMaterial (Material.h:133, LambertianInterfaceMaterial.cpp:7-20): a Lambertian base
+// under a smooth dielectric interface.
+class LambertianInterfaceMaterial : public MyMaterial {
+ public:
+  float3 color{1, 1, 1};
+  float ior = 1.3f;
+  void setColor(float3 c) { color = c; }
+  void setIor(float i) { ior = i; }
+  uint32_t getType() const override { return PT_LAMBERTIAN_INTERFACE_SHADER; }
+  std::vector<unsigned char> params() const override
+  {
+    pt_lambertian_interface_params p;
+    memcpy(p.diffuse_color, color.data(), 12);
+    p.ior = ior;
+    return DiffuseMaterial::bytes(p);
+  }
+};
+// RoughDiffuseMaterial (Material.h:167, RoughDiffuseMaterial.cpp:7-28): a Lambertian base under a
+// rough dielectric interface.
+class RoughDiffuseMaterial : public MyMaterial {
+ public:
+  float3 color{1, 1, 1};
+  float ior = 1.3f;
+  std::array<float, 2> roughness{0.1f, 0.1f};
+  uint32_t microfacet_model = PT_WALTER_MODEL, normal_distribution = PT_BECKMANN_DISTRIBUTION;
+  void setColor(float3 c) { color = c; }
+  void setIor(float i) { ior = i; }
+  void setRoughness(std::array<float, 2> r) { roughness = r; }
+  void setMicrofacetModel(uint32_t m) { microfacet_model = m; }
+  void setNormalDistribution(uint32_t d) { normal_distribution = d; }
+  uint32_t getType() const override { return PT_ROUGH_DIFFUSE_SHADER; }
+  std::vector<unsigned char> params() const override
+  {
+    pt_rough_diffuse_params p;
+    memcpy(p.diffuse_color, color.data(), 12);
+    p.ior = ior;
+    memcpy(p.roughness, roughness.data(), 8);
+    p.microfacet_model = microfacet_model;
+    p.normal_distribution = normal_distribution;
+    return DiffuseMaterial::bytes(p);
+  }
+};
+// TranslucentMaterial (Material.h:357, TranslucentMaterial.cpp:7-30): dipole BSSRDF under a smooth
+// boundary.  Coefficients per RGB in 1/mm, scaled by `scale`; defaults: the "Apple" entry of
+// getDefaultMaterial (TranslucentMaterial.cpp:245-250), scale 100, standard dipole.
+class TranslucentMaterial : public MyMaterial {
+ public:
+  float3 scattering{2.29f, 2.39f, 1.97f}, absorption{0.0030f, 0.0034f, 0.0046f}, meancosine{0, 0, 0};
+  float ior = 1.3f, scale = 100.0f;
+  uint32_t dipole_model = PT_STANDARD_DIPOLE;
+  void setScattering(float3 v) { scattering = v; }
+  void setAbsorption(float3 v) { absorption = v; }
+  void setMeanCosine(float3 v) { meancosine = v; }
+  void setIor(float i) { ior = i; }
+  void setScale(float v) { scale = v; }
+  void setDipoleModel(uint32_t m) { dipole_model = m; }
+  uint32_t getType() const override { return PT_TRANSLUCENT_SHADER; }
+  std::vector<unsigned char> params() const override { return DiffuseMaterial::bytes(translucent()); }
+
+ protected:
+  pt_translucent_params translucent() const
+  {
+    pt_translucent_params p;
+    memcpy(p.scattering, scattering.data(), 12);
+    memcpy(p.absorption, absorption.data(), 12);
+    memcpy(p.meancosine, meancosine.data(), 12);
+    p.ior = ior;
+    p.scale = scale;
+    p.dipole_model = dipole_model;
+    return p;
+  }
+};
+// RoughTranslucentMaterial (Material.h:416, RoughTranslucentMaterial.cpp:360-395): the dipole under a
+// rough dielectric boundary.
+class RoughTranslucentMaterial : public TranslucentMaterial {
+ public:
+  std::array<float, 2> roughness{0.1f, 0.1f};
+  uint32_t microfacet_model = PT_WALTER_MODEL, normal_distribution = PT_BECKMANN_DISTRIBUTION;
+  void setRoughness(std::array<float, 2> r) { roughness = r; }
+  void setMicrofacetModel(uint32_t m) { microfacet_model = m; }
+  void setNormalDistribution(uint32_t d) { normal_distribution = d; }
+  uint32_t getType() const override { return PT_ROUGH_TRANSLUCENT_SHADER; }
+  std::vector<unsigned char> params() const override
+  {
+    const pt_translucent_params t = translucent();
+    pt_rough_translucent_params p;
+    memcpy(p.scattering, t.scattering, 12);
+    memcpy(p.absorption, t.absorption, 12);
+    memcpy(p.meancosine, t.meancosine, 12);
+    p.ior = t.ior;
+    p.scale = t.scale;
+    p.dipole_model = t.dipole_model;
+    memcpy(p.roughness, roughness.data(), 8);
+    p.microfacet_model = microfacet_model;
+    p.normal_distribution = normal_distribution;
+    return DiffuseMaterial::bytes(p);
+  }
+};
+
 // ---------------------------------------------------------------- Light.h
 // LightStruct / TriangleLight byte layouts (structs.h:42-103).
 struct LightStruct { uint32_t light_type; float emitted_radiance[3]; float p[3]; float padding[3]; };
 struct TriangleLight { float v0[3], v1[3], v2[3], n0[3], n1[3], n2[3]; uint32_t has_normals; float emission[3]; float area; };
 static_assert(sizeof(LightStruct) == 40 && sizeof(TriangleLight) == 92, "reference light layouts");
 
-class TriangleAreaLight {
+// light_type values of LightStruct (structs.h:27-34).
+enum : uint32_t { POINT_LIGHT = 0, DIRECTIONAL_LIGHT = 1, TRIANGLES_AREA_LIGHT = 2, DISK_LIGHT = 3, SPHERICAL_LIGHT = 4, ENVMAP_LIGHT = 5 };
+
+// Light (Light.h:10): each light adds its light_buffer record (and a TrianglesAreaLight its emitter
+// mesh and triangle_light_buffer records) as OptixSceneLoader::addLight / updateLights do.
+class OptixScene;
+class Light {
+ public:
+  virtual ~Light() = default;
+  virtual void append(OptixScene& scene, std::vector<LightStruct>& lights, std::vector<TriangleLight>& tris) const = 0;
+};
+// PointLight (Light.h:28, Light.cpp:26-60).
+class PointLight : public Light {
+ public:
+  PointLight(float3 position, float3 radiance) : position(position), radiance(radiance) {}
+  void setPosition(float3 p) { position = p; }
+  void setRadiance(float3 r) { radiance = r; }
+  void append(OptixScene&, std::vector<LightStruct>& ls, std::vector<TriangleLight>&) const override
+  {
+    LightStruct s{};
+    s.light_type = POINT_LIGHT;
+    memcpy(s.emitted_radiance, radiance.data(), 12);
+    memcpy(s.p, position.data(), 12);
+    ls.push_back(s);
+  }
+  float3 position, radiance;
+};
+// DirectionalLight (Light.h:49, Light.cpp:62-100): the stored direction is normalised in FP32.
+class DirectionalLight : public Light {
+ public:
+  DirectionalLight(float3 direction, float3 radiance) : direction(direction), radiance(radiance) {}
+  void setDirection(float3 d) { direction = d; }
+  void setRadiance(float3 r) { radiance = r; }
+  void append(OptixScene&, std::vector<LightStruct>& ls, std::vector<TriangleLight>&) const override
+  {
+    LightStruct s{};
+    s.light_type = DIRECTIONAL_LIGHT;
+    memcpy(s.emitted_radiance, radiance.data(), 12);
+    const float len = std::sqrt(direction[0] * direction[0] + direction[1] * direction[1] + direction[2] * direction[2]);
+    for (int k = 0; k < 3; ++k) s.p[k] = direction[k] / len;
+    ls.push_back(s);
+  }
+  float3 direction, radiance;
+};
+// DiskAreaLight (Light.h:133, Light.cpp:370-503): position, radius and the normal's angles theta / phi
+// in degrees (DiskLightStruct, structs.h:76-84); its geometry is intersected analytically.
+class DiskAreaLight : public Light {
+ public:
+  DiskAreaLight(float3 position, float3 radiance, float radius = 1.0f, float theta = 0.0f, float phi = 0.0f)
+      : position(position), radiance(radiance), radius(radius), theta(theta), phi(phi) {}
+  void append(OptixScene&, std::vector<LightStruct>& ls, std::vector<TriangleLight>&) const override
+  {
+    LightStruct s{};
+    s.light_type = DISK_LIGHT;
+    memcpy(s.emitted_radiance, radiance.data(), 12);
+    memcpy(s.p, position.data(), 12);
+    s.padding[0] = radius;
+    s.padding[1] = phi;
+    s.padding[2] = theta;
+    ls.push_back(s);
+  }
+  float3 position, radiance;
+  float radius, theta, phi;
+};
+// SphericalLight (Light.h:167, Light.cpp:505-610): position and radius (SphericalLightStruct,
+// structs.h:86-93); its geometry is intersected analytically.
+class SphericalLight : public Light {
+ public:
+  SphericalLight(float3 position, float3 radiance, float radius = 0.05f) : position(position), radiance(radiance), radius(radius) {}
+  void append(OptixScene&, std::vector<LightStruct>& ls, std::vector<TriangleLight>&) const override
+  {
+    LightStruct s{};
+    s.light_type = SPHERICAL_LIGHT;
+    memcpy(s.emitted_radiance, radiance.data(), 12);
+    memcpy(s.p, position.data(), 12);
+    s.padding[0] = radius;
+    ls.push_back(s);
+  }
+  float3 position, radiance;
+  float radius;
+};
+// The environment map as a light (light_type 5): next-event estimation samples it through its
+// marginal / conditional CDFs (Envmap.h:66-98).  Needs an EnvMapBackground.
+class EnvMapLight : public Light {
+ public:
+  void append(OptixScene&, std::vector<LightStruct>& ls, std::vector<TriangleLight>&) const override
+  {
+    LightStruct s{};
+    s.light_type = ENVMAP_LIGHT;
+    s.emitted_radiance[0] = s.emitted_radiance[1] = s.emitted_radiance[2] = 1.0f;
+    ls.push_back(s);
+  }
+};
+// TrianglesAreaLight (Light.h:97, Light.cpp:240-368): an emitting triangle mesh.
+class TriangleAreaLight : public Light {
  public:
   TriangleAreaLight(std::vector<float> positions, std::vector<int32_t> vindex, float3 radiance)
       : positions(std::move(positions)), vindex(std::move(vindex)), radiance(radiance) {}
+  void append(OptixScene& scene, std::vector<LightStruct>& ls, std::vector<TriangleLight>& tl) const override;
   std::vector<float> positions;
   std::vector<int32_t> vindex;
   float3 radiance;
@@ -240,43 +471,46 @@ class OptixScene {
                       material_id, &first),
           "pt_mesh_add");
   }
+  void setBackground(const EnvMapBackground& b) { b.apply(ctx); }
+  // context["samples"]: probe points per translucent object and frame (OptixSceneLoader.cpp:11-17).
+  void setProbeCount(uint32_t samples) { check(pt_set_probe_count(ctx, samples), "pt_set_probe_count"); }
   // Adds the lights' emitter meshes and uploads light_buffer / triangle_light_buffer as
   // OptixSceneLoader::addLight / loadTriangleLightBuffer / updateLights do (OptixSceneLoader.cpp:284-410).
-  void setLights(const std::vector<TriangleAreaLight>& lights)
+  void setLights(const std::vector<std::shared_ptr<Light>>& lights)
   {
     std::vector<LightStruct> ls;
     std::vector<TriangleLight> tl;
-    for (const TriangleAreaLight& L : lights) {
-      pt_area_light_params ap;
-      memcpy(ap.radiance, L.radiance.data(), 12);
-      uint32_t mid;
-      check(pt_material_create(ctx, PT_AREA_LIGHT_MATERIAL, &ap, sizeof(ap), &mid), "pt_material_create");
-      Mesh m{L.positions, L.vindex, {}, {}, nullptr};
-      addMesh(m, mid);
-      LightStruct s{};
-      s.light_type = 2;  // TRIANGLES_AREA_LIGHT
-      memcpy(s.emitted_radiance, L.radiance.data(), 12);
-      size_t ntri = L.vindex.size() / 3;
-      s.p[0] = (float)ntri;
-      s.p[1] = (float)tl.size();
-      s.p[2] = (float)(tl.size() + ntri - 1);
-      ls.push_back(s);
-      for (size_t t = 0; t < ntri; ++t) {
-        TriangleLight r{};
-        const float* a = &L.positions[3 * L.vindex[3 * t]];
-        const float* b = &L.positions[3 * L.vindex[3 * t + 1]];
-        const float* c = &L.positions[3 * L.vindex[3 * t + 2]];
-        memcpy(r.v0, a, 12);
-        memcpy(r.v1, b, 12);
-        memcpy(r.v2, c, 12);
-        float e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]}, e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
-        float px = e1[1] * e2[2] - e1[2] * e2[1], py = e1[2] * e2[0] - e1[0] * e2[2], pz = e1[0] * e2[1] - e1[1] * e2[0];
-        r.area = (float)(0.5 * std::sqrt(px * px + py * py + pz * pz));  // Light.cpp:296
-        memcpy(r.emission, L.radiance.data(), 12);
-        tl.push_back(r);
-      }
+    for (const auto& L : lights) L->append(*this, ls, tl);
+    check(pt_lights_upload(ctx, ls.empty() ? nullptr : ls.data(), (uint32_t)ls.size(), tl.empty() ? nullptr : tl.data(), (uint32_t)tl.size()),
+          "pt_lights_upload");
+  }
+  void setLights(const std::vector<TriangleAreaLight>& lights)
+  {
+    std::vector<std::shared_ptr<Light>> all;
+    for (const TriangleAreaLight& L : lights) all.push_back(std::make_shared<TriangleAreaLight>(L));
+    setLights(all);
+  }
+  // The groups of an OBJ file (glm's reader as ObjLoader flattens it, pt_obj_read) as meshes of one
+  // material, sharing the file's vertex and normal arrays.
+  void addObj(const std::string& path, uint32_t material_id)
+  {
+    pt_obj* obj = nullptr;
+    check(pt_obj_read(path.c_str(), &obj), "pt_obj_read");
+    pt_obj_info info;
+    pt_status st = pt_obj_get_info(obj, &info);
+    Mesh m;
+    if (st == PT_OK) {
+      m.positions.resize(3 * (size_t)info.n_vertices);
+      m.normals.resize(3 * (size_t)info.n_normals);
+      m.vindex.resize(3 * (size_t)info.n_triangles);
+      m.nindex.resize(3 * (size_t)info.n_triangles);
+      st = pt_obj_get_arrays(obj, m.positions.data(), m.normals.empty() ? nullptr : m.normals.data(), nullptr, m.vindex.data(),
+                             m.normals.empty() ? nullptr : m.nindex.data(), nullptr, nullptr);
     }
-    check(pt_lights_upload(ctx, ls.data(), (uint32_t)ls.size(), tl.data(), (uint32_t)tl.size()), "pt_lights_upload");
+    pt_obj_free(obj);
+    check(st, "pt_obj_get_arrays");
+    if (m.normals.empty()) m.nindex.clear();
+    addMesh(m, material_id);
   }
   void initContext() { check(pt_build(ctx), "pt_build"); }
   // OptixScene::renderScene (OptixScene.cpp:139-168): frame++ and one integrator pass.
@@ -300,5 +534,37 @@ class OptixScene {
   pt_ctx* ctx = nullptr;
   uint32_t width = 0, height = 0, frame = 0;
 };
+
+inline void TriangleAreaLight::append(OptixScene& scene, std::vector<LightStruct>& ls, std::vector<TriangleLight>& tl) const
+{
+  pt_area_light_params ap;
+  memcpy(ap.radiance, radiance.data(), 12);
+  uint32_t mid;
+  check(pt_material_create(scene.handle(), PT_AREA_LIGHT_MATERIAL, &ap, sizeof(ap), &mid), "pt_material_create");
+  Mesh m{positions, vindex, {}, {}, nullptr};
+  scene.addMesh(m, mid);
+  LightStruct s{};
+  s.light_type = TRIANGLES_AREA_LIGHT;
+  memcpy(s.emitted_radiance, radiance.data(), 12);
+  size_t ntri = vindex.size() / 3;
+  s.p[0] = (float)ntri;
+  s.p[1] = (float)tl.size();
+  s.p[2] = (float)(tl.size() + ntri - 1);
+  ls.push_back(s);
+  for (size_t t = 0; t < ntri; ++t) {
+    TriangleLight r{};
+    const float* a = &positions[3 * vindex[3 * t]];
+    const float* b = &positions[3 * vindex[3 * t + 1]];
+    const float* c = &positions[3 * vindex[3 * t + 2]];
+    memcpy(r.v0, a, 12);
+    memcpy(r.v1, b, 12);
+    memcpy(r.v2, c, 12);
+    float e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]}, e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+    float px = e1[1] * e2[2] - e1[2] * e2[1], py = e1[2] * e2[0] - e1[0] * e2[2], pz = e1[0] * e2[1] - e1[1] * e2[0];
+    r.area = (float)(0.5 * std::sqrt(px * px + py * py + pz * pz));  // Light.cpp:296
+    memcpy(r.emission, radiance.data(), 12);
+    tl.push_back(r);
+  }
+}
 
 }  // namespace orf

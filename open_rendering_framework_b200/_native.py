@@ -101,6 +101,7 @@ SIGNATURES = {
     "pt_get_probes": (I32, [P, P, U64, P]),
     "pt_get_scattering_properties": (I32, [P, U32, P]),
     "pt_set_profiling": (I32, [P, I32]),
+    "pt_get_build_info": (I32, [P, P]),
     "pt_set_option": (I32, [P, ctypes.c_char_p, ctypes.c_int64]),
     "pt_trace_closest": (I32, [P, P, P, U32, P, P, P]),
     "pt_trace_any": (I32, [P, P, P, U32, P]),

@@ -1,0 +1,531 @@
+// BVH construction on the device: a linear BVH over Morton codes (T. Karras, "Maximizing Parallelism
+// in the Construction of BVHs, Octrees, and k-d Trees", HPG 2012) with SAH-chosen leaves, written in
+// the child-pair BVH2 layout of pt_scene.cuh, then collapsed level by level into the 4-wide layout.
+//
+// The reference builds its acceleration structure on the device through OptiX (Trbvh / Sbvh,
+// OptixSceneLoader.cpp:136, ObjLoader.cpp:387-399).  Hits are decided by the triangle test alone
+// (closest t, ties to the lower triangle index), so this tree gives the same hits as the host SAH
+// tree and as a brute-force loop; it trades a little traversal speed for a build that takes
+// milliseconds instead of a host pass over the triangles.
+//
+// Passes (all on the context's stream):
+//   1. triangle boxes and the centroids' bounds (ordered-integer atomics);
+//   2. 30-bit Morton codes of the centroids in those bounds;
+//   3. a stable least-significant-digit radix sort of (code, triangle) in four 8-bit passes: per-block
+//      digit counts, one exclusive scan over (digit, block), a scatter ranked within each warp by
+//      __match_any_sync;
+//   4. the Karras hierarchy: internal node i covers a contiguous range of the sorted triangles and
+//      splits it at the highest differing bit (equal codes are ordered by index);
+//   5. bottom-up boxes and SAH costs (the second of a node's two children to finish computes it); a node
+//      of at most `max_leaf` triangles whose leaf cost (one per triangle) does not exceed its split cost
+//      (trav_cost + the children's costs weighted by their areas) becomes a leaf;
+//   6. the BVH2 nodes, the triangles in leaf order, and the tree depth (every leaf walks to the root);
+//   7. the 4-wide collapse: one launch per level, each wide node opening its BVH2 node's internal
+//      child of largest area until it has four children (the host collapse's rule), its internal
+//      children appended to the next level's work list.
+// The wide tree's depth is bounded by the traversal stack; a deeper tree leaves the 4-wide BVH unset.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "pt_common.cuh"
+#include "pt_context.h"
+
+namespace pt {
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kRadix = 256;
+constexpr int kWarpsPerBlock = kBlock / 32;
+constexpr uint32_t kEmptyLeaf = 0x80000000u;
+
+__device__ __forceinline__ uint32_t f2ord(float f)
+{
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord2f(uint32_t u) { return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u); }
+
+__device__ __forceinline__ float area_of(const float4& lo, const float4& hi)
+{
+  const float dx = fmaxf(0.0f, hi.x - lo.x), dy = fmaxf(0.0f, hi.y - lo.y), dz = fmaxf(0.0f, hi.z - lo.z);
+  return dx * dy + dy * dz + dz * dx;
+}
+
+// Pass 1: per triangle its box (sorted later), and the bounds of the centroids (box midpoints, as
+// the host builder takes them).
+__global__ void __launch_bounds__(kBlock) k_tri_boxes(const float* __restrict__ tri, uint32_t n, float4* __restrict__ box_lo,
+                                                      float4* __restrict__ box_hi, uint32_t* __restrict__ cbounds)
+{
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float* p = tri + 9 * (size_t)i;
+    float bl[3], bh[3], c[3];
+    for (int k = 0; k < 3; ++k) {
+      bl[k] = fminf(fminf(p[k], p[3 + k]), p[6 + k]);
+      bh[k] = fmaxf(fmaxf(p[k], p[3 + k]), p[6 + k]);
+      c[k] = 0.5f * (bl[k] + bh[k]);
+      lo[k] = fminf(lo[k], c[k]);
+      hi[k] = fmaxf(hi[k], c[k]);
+    }
+    box_lo[i] = make_float4(bl[0], bl[1], bl[2], 0.0f);
+    box_hi[i] = make_float4(bh[0], bh[1], bh[2], 0.0f);
+  }
+  for (int k = 0; k < 3; ++k) {
+    for (int off = 16; off > 0; off >>= 1) {
+      lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], off));
+      hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], off));
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    for (int k = 0; k < 3; ++k) {
+      atomicMin(cbounds + k, f2ord(lo[k]));
+      atomicMax(cbounds + 3 + k, f2ord(hi[k]));
+    }
+  }
+}
+
+// 10 bits of x spread to every third bit.
+__device__ __forceinline__ uint32_t spread10(uint32_t x)
+{
+  x &= 0x3ffu;
+  x = (x | (x << 16)) & 0x030000ffu;
+  x = (x | (x << 8)) & 0x0300f00fu;
+  x = (x | (x << 4)) & 0x030c30c3u;
+  x = (x | (x << 2)) & 0x09249249u;
+  return x;
+}
+
+// Pass 2: Morton code of each centroid in the centroid bounds; idx = the triangle.
+__global__ void __launch_bounds__(kBlock) k_morton(const float4* __restrict__ box_lo, const float4* __restrict__ box_hi, uint32_t n,
+                                                   const uint32_t* __restrict__ cbounds, uint32_t* __restrict__ keys, uint32_t* __restrict__ idx)
+{
+  float lo[3], inv[3];
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = ord2f(cbounds[k]);
+    const float ext = ord2f(cbounds[3 + k]) - lo[k];
+    inv[k] = ext > 0.0f ? 1024.0f / ext : 0.0f;
+  }
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float4 a = box_lo[i], b = box_hi[i];
+    const float c[3] = {0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z)};
+    uint32_t q[3];
+    for (int k = 0; k < 3; ++k) {
+      const float t = (c[k] - lo[k]) * inv[k];
+      q[k] = t <= 0.0f ? 0u : (t >= 1023.0f ? 1023u : (uint32_t)t);
+    }
+    keys[i] = (spread10(q[0]) << 2) | (spread10(q[1]) << 1) | spread10(q[2]);
+    idx[i] = i;
+  }
+}
+
+// Pass 3a: digit counts of one block of kBlock keys, stored digit-major: hist[digit * nblocks + block].
+__global__ void __launch_bounds__(kBlock) k_radix_hist(const uint32_t* __restrict__ keys, uint32_t n, int shift, uint32_t* __restrict__ hist)
+{
+  __shared__ uint32_t cnt[kRadix];
+  cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+  if (i < n) atomicAdd(&cnt[(keys[i] >> shift) & (kRadix - 1)], 1u);
+  __syncthreads();
+  hist[threadIdx.x * gridDim.x + blockIdx.x] = cnt[threadIdx.x];
+}
+
+// Pass 3b: exclusive scan of `total` counts by one block of 1024 threads (contiguous chunks).
+__global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* __restrict__ a, uint32_t total)
+{
+  __shared__ uint32_t part[1024];
+  const uint32_t chunk = (total + 1023) / 1024;
+  const uint32_t b = threadIdx.x * chunk, e = min(total, b + chunk);
+  uint32_t s = 0;
+  for (uint32_t i = b; i < e; ++i) s += a[i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {  // inclusive Hillis-Steele scan of the partial sums
+    const uint32_t v = threadIdx.x >= (uint32_t)off ? part[threadIdx.x - off] : 0u;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  uint32_t run = threadIdx.x ? part[threadIdx.x - 1] : 0u;
+  for (uint32_t i = b; i < e; ++i) {
+    const uint32_t v = a[i];
+    a[i] = run;
+    run += v;
+  }
+}
+
+// Pass 3c: stable scatter.  A key's destination is its digit's offset for this block, plus the keys of
+// that digit in earlier warps of the block, plus those in earlier lanes of its warp.
+__global__ void __launch_bounds__(kBlock) k_radix_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t n,
+                                                          int shift, const uint32_t* __restrict__ offs, uint32_t* __restrict__ kout,
+                                                          uint32_t* __restrict__ vout)
+{
+  __shared__ uint32_t wcnt[kWarpsPerBlock][kRadix];
+  for (int j = threadIdx.x; j < kWarpsPerBlock * kRadix; j += kBlock) (&wcnt[0][0])[j] = 0;
+  __syncthreads();
+  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+  const bool valid = i < n;
+  const uint32_t key = valid ? kin[i] : 0u;
+  const uint32_t digit = valid ? (key >> shift) & (kRadix - 1) : (uint32_t)kRadix;  // kRadix matches no real digit
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t peers = __match_any_sync(0xffffffffu, digit);
+  const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+  if (valid && rank == 0) wcnt[warp][digit] = __popc(peers);
+  __syncthreads();
+  if (!valid) return;
+  uint32_t pos = offs[digit * gridDim.x + blockIdx.x] + rank;
+  for (int w = 0; w < warp; ++w) pos += wcnt[w][digit];
+  kout[pos] = key;
+  vout[pos] = vin[i];
+}
+
+// Karras' delta: length of the common prefix of keys i and j, extended by the indices for equal keys;
+// -1 outside [0, n).
+__device__ __forceinline__ int kdelta(const uint32_t* __restrict__ keys, int n, int i, int j)
+{
+  if (j < 0 || j >= n) return -1;
+  const uint32_t a = keys[i], b = keys[j];
+  return a == b ? 32 + __clz((uint32_t)(i ^ j)) : __clz(a ^ b);
+}
+
+// Pass 4: internal node i of n - 1.  Children >= 0 are internal nodes, < 0 are leaves ~j (sorted
+// position j).  first / last: the sorted range the node covers.
+__global__ void __launch_bounds__(kBlock) k_karras(const uint32_t* __restrict__ keys, int n, int2* __restrict__ child,
+                                                   int* __restrict__ iparent, int* __restrict__ lparent, int2* __restrict__ range)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  const int d = (kdelta(keys, n, i, i + 1) - kdelta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+  const int dmin = kdelta(keys, n, i, i - d);
+  int lmax = 2;
+  while (kdelta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+  int l = 0;
+  for (int t = lmax >> 1; t >= 1; t >>= 1)
+    if (kdelta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+  const int j = i + l * d;
+  const int dnode = kdelta(keys, n, i, j);
+  int s = 0, t = l;
+  do {
+    t = (t + 1) >> 1;
+    if (kdelta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+  } while (t > 1);
+  const int gamma = i + s * d + min(d, 0);
+  const int first = min(i, j), last = max(i, j);
+  const int left = first == gamma ? ~gamma : gamma;
+  const int right = last == gamma + 1 ? ~(gamma + 1) : gamma + 1;
+  child[i] = make_int2(left, right);
+  range[i] = make_int2(first, last);
+  if (left >= 0) iparent[left] = i; else lparent[~left] = i;
+  if (right >= 0) iparent[right] = i; else lparent[~right] = i;
+  if (i == 0) iparent[0] = -1;
+}
+
+struct NodeRec {
+  float4 lo, hi;  // box; lo.w = SAH cost, hi.w = triangle count (as float)
+};
+
+// Pass 5: bottom-up boxes and SAH costs.  One thread per leaf walks up; at each internal node the
+// first arriving child stops, the second computes the node (its sibling's record is then complete:
+// every record is written before the __threadfence that precedes the arrival counter).
+__global__ void __launch_bounds__(kBlock) k_bottom_up(int n, const uint32_t* __restrict__ order, const float4* __restrict__ box_lo,
+                                                      const float4* __restrict__ box_hi, const int2* __restrict__ child,
+                                                      const int* __restrict__ iparent, const int* __restrict__ lparent,
+                                                      NodeRec* leafrec, NodeRec* noderec, uint32_t* visits, uint8_t* collapse,
+                                                      float trav_cost, int max_leaf)
+{
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const uint32_t tri = order[j];
+  NodeRec r;
+  r.lo = box_lo[tri];
+  r.hi = box_hi[tri];
+  r.lo.w = 1.0f;
+  r.hi.w = 1.0f;
+  leafrec[j] = r;
+  __threadfence();
+  int p = lparent[j];
+  while (p >= 0) {
+    if (atomicAdd(visits + p, 1u) == 0u) return;
+    __threadfence();
+    const int2 c = child[p];
+    NodeRec a, b;
+    const NodeRec* pa = c.x >= 0 ? noderec + c.x : leafrec + ~c.x;
+    const NodeRec* pb = c.y >= 0 ? noderec + c.y : leafrec + ~c.y;
+    a.lo = __ldcg(&pa->lo);
+    a.hi = __ldcg(&pa->hi);
+    b.lo = __ldcg(&pb->lo);
+    b.hi = __ldcg(&pb->hi);
+    NodeRec m;
+    m.lo = make_float4(fminf(a.lo.x, b.lo.x), fminf(a.lo.y, b.lo.y), fminf(a.lo.z, b.lo.z), 0.0f);
+    m.hi = make_float4(fmaxf(a.hi.x, b.hi.x), fmaxf(a.hi.y, b.hi.y), fmaxf(a.hi.z, b.hi.z), 0.0f);
+    const float count = a.hi.w + b.hi.w;
+    const float A = area_of(m.lo, m.hi);
+    const float wa = A > 0.0f ? area_of(a.lo, a.hi) / A : 0.5f, wb = A > 0.0f ? area_of(b.lo, b.hi) / A : 0.5f;
+    const float split_cost = trav_cost + wa * a.lo.w + wb * b.lo.w;
+    const bool leaf = count <= (float)max_leaf && count <= split_cost;
+    m.lo.w = leaf ? count : split_cost;
+    m.hi.w = count;
+    collapse[p] = leaf ? 1 : 0;
+    __stcg(&noderec[p].lo, m.lo);
+    __stcg(&noderec[p].hi, m.hi);
+    __threadfence();
+    p = iparent[p];
+  }
+}
+
+// The code of child c (>= 0 internal, < 0 leaf ~j) as the BVH2 stores it, and its record.
+__device__ __forceinline__ int child_code(int c, const int2* range, const uint8_t* collapse)
+{
+  if (c < 0) return (int)(kEmptyLeaf | ((uint32_t)(~c) << 4) | 1u);
+  if (collapse[c]) {
+    const int2 r = range[c];
+    return (int)(kEmptyLeaf | ((uint32_t)r.x << 4) | (uint32_t)(r.y - r.x + 1));
+  }
+  return c;
+}
+
+// Pass 6a: the BVH2 nodes (internal node p at index p; nodes inside a leaf subtree are written too
+// and never reached).  The root of a tree that is a single leaf holds that leaf and an empty one.
+__global__ void __launch_bounds__(kBlock) k_write_bvh2(int n, const int2* __restrict__ child, const int* __restrict__ iparent,
+                                                       const int2* __restrict__ range, const uint8_t* __restrict__ collapse,
+                                                       const NodeRec* __restrict__ leafrec, const NodeRec* __restrict__ noderec,
+                                                       float4* __restrict__ nodes)
+{
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n - 1) return;
+  int c0, c1;
+  NodeRec r0, r1;
+  if (p == 0 && collapse[0]) {
+    c0 = (int)(kEmptyLeaf | (uint32_t)n);  // first 0, count n (<= 15)
+    c1 = (int)kEmptyLeaf;
+    r0 = noderec[0];
+    r1.lo = make_float4(1e30f, 1e30f, 1e30f, 0.0f);
+    r1.hi = r1.lo;
+  } else {
+    const int2 c = child[p];
+    c0 = child_code(c.x, range, collapse);
+    c1 = child_code(c.y, range, collapse);
+    r0 = c.x >= 0 ? noderec[c.x] : leafrec[~c.x];
+    r1 = c.y >= 0 ? noderec[c.y] : leafrec[~c.y];
+  }
+  float4* nd = nodes + 4 * (size_t)p;
+  nd[0] = make_float4(r0.lo.x, r0.hi.x, r0.lo.y, r0.hi.y);
+  nd[1] = make_float4(r1.lo.x, r1.hi.x, r1.lo.y, r1.hi.y);
+  nd[2] = make_float4(r0.lo.z, r0.hi.z, r1.lo.z, r1.hi.z);
+  nd[3] = make_float4(__int_as_float(c0), __int_as_float(c1), __int_as_float(iparent[p]), 0.0f);
+}
+
+// Pass 6b: triangles in leaf (sorted) order as Moller-Trumbore records, and the BVH2 depth (levels
+// including the leaves): each triangle counts the internal nodes above it that the tree keeps (those
+// inside a leaf's subtree are not nodes of the tree), plus its leaf.
+__global__ void __launch_bounds__(kBlock) k_write_tris(int n, const float* __restrict__ tri, const uint32_t* __restrict__ order,
+                                                       const int* __restrict__ lparent, const int* __restrict__ iparent,
+                                                       const uint8_t* __restrict__ collapse, float4* __restrict__ v0, float4* __restrict__ e1,
+                                                       float4* __restrict__ e2, int* __restrict__ max_depth)
+{
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const uint32_t i = order[j];
+  const float* p = tri + 9 * (size_t)i;
+  v0[j] = make_float4(p[0], p[1], p[2], __int_as_float((int)i));
+  e1[j] = make_float4(p[3] - p[0], p[4] - p[1], p[5] - p[2], 0.0f);
+  e2[j] = make_float4(p[6] - p[0], p[7] - p[1], p[8] - p[2], 0.0f);
+  int d = 1, steps = 0;
+  for (int q = lparent[j]; q >= 0 && steps < n; q = iparent[q], ++steps) d += collapse[q] ? 0 : 1;
+  if (collapse[0]) d = 2;  // a single-leaf tree: the root and its leaf
+  atomicMax(max_depth, d);
+}
+
+struct Kid {
+  int code;
+  float lo[3], hi[3];
+};
+__device__ __forceinline__ Kid kid_of(const float4* __restrict__ nodes, int node, int k)
+{
+  const float4* nd = nodes + 4 * (size_t)node;
+  const float4 a = nd[k], z = nd[2], c = nd[3];
+  Kid r;
+  r.code = __float_as_int(k == 0 ? c.x : c.y);
+  r.lo[0] = a.x; r.hi[0] = a.y; r.lo[1] = a.z; r.hi[1] = a.w;
+  r.lo[2] = k == 0 ? z.x : z.z;
+  r.hi[2] = k == 0 ? z.y : z.w;
+  return r;
+}
+__device__ __forceinline__ float kid_area(const Kid& c)
+{
+  float d[3];
+  for (int k = 0; k < 3; ++k) d[k] = fmaxf(0.0f, c.hi[k] - c.lo[k]);
+  return d[0] * d[1] + d[1] * d[2] + d[2] * d[0];
+}
+
+// Pass 7: one level of the 4-wide collapse.  Work item (BVH2 node, wide node index); each internal
+// child gets the next wide index from *wide_count and becomes a work item of the next level.
+__global__ void __launch_bounds__(128) k_collapse_level(const float4* __restrict__ nodes, const int2* __restrict__ work_in, uint32_t n_in,
+                                                        int2* __restrict__ work_out, uint32_t* __restrict__ n_out, uint32_t* __restrict__ wide_count,
+                                                        uint32_t wide_cap, float4* __restrict__ nodes4, uint32_t* __restrict__ overflow)
+{
+  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= n_in) return;
+  const int2 item = work_in[w];
+  Kid kids[kWide];
+  int nk = 0;
+  kids[nk++] = kid_of(nodes, item.x, 0);
+  kids[nk++] = kid_of(nodes, item.x, 1);
+  while (nk < kWide) {
+    int best = -1;
+    float ba = -1.0f;
+    for (int j = 0; j < nk; ++j)
+      if (kids[j].code >= 0 && kid_area(kids[j]) > ba) { ba = kid_area(kids[j]); best = j; }
+    if (best < 0) break;
+    const int inner = kids[best].code;
+    kids[best] = kid_of(nodes, inner, 0);
+    kids[nk++] = kid_of(nodes, inner, 1);
+  }
+  int codes[kWide];
+  for (int j = 0; j < kWide; ++j) {
+    if (j >= nk) {
+      codes[j] = (int)kEmptyLeaf;
+    } else if (kids[j].code >= 0) {
+      const uint32_t slot = atomicAdd(wide_count, 1u);
+      if (slot >= wide_cap) {
+        atomicAdd(overflow, 1u);
+        codes[j] = (int)kEmptyLeaf;
+      } else {
+        codes[j] = (int)slot;
+        work_out[atomicAdd(n_out, 1u)] = make_int2(kids[j].code, (int)slot);
+      }
+    } else {
+      codes[j] = kids[j].code;
+    }
+  }
+  float4* nd = nodes4 + kWideStride * (size_t)item.y;
+  for (int axis = 0; axis < 3; ++axis)
+    for (int r = 0; r < kWideRow; ++r) {
+      float l[4], h[4];
+      for (int q = 0; q < 4; ++q) {
+        const int j = 4 * r + q;
+        l[q] = j < nk ? kids[j].lo[axis] : 1e30f;
+        h[q] = j < nk ? kids[j].hi[axis] : 1e30f;
+      }
+      nd[(2 * axis) * kWideRow + r] = make_float4(l[0], l[1], l[2], l[3]);
+      nd[(2 * axis + 1) * kWideRow + r] = make_float4(h[0], h[1], h[2], h[3]);
+    }
+  for (int r = 0; r < kWideRow; ++r)
+    nd[6 * kWideRow + r] = make_float4(__int_as_float(codes[4 * r]), __int_as_float(codes[4 * r + 1]), __int_as_float(codes[4 * r + 2]),
+                                       __int_as_float(codes[4 * r + 3]));
+  if (kWideStride > 7 * kWideRow) nd[7 * kWideRow] = make_float4((float)nk, 0.0f, 0.0f, 0.0f);
+}
+
+}  // namespace
+
+pt_status build_bvh_device(Context& c)
+{
+  const uint32_t n = c.n_tris;
+  if (n < 2) return fail(PT_INVALID_ARG, "device BVH build: needs at least two triangles");
+  if (n >= (1u << 27)) return fail(PT_CAP_EXCEEDED, "device BVH build: more than 2^27 triangles");
+  cudaStream_t st = c.stream;
+  PT_CHECK_CUDA(cudaEventRecord(c.ev0, st), "device BVH build");
+  const uint32_t nb = (n + kBlock - 1) / kBlock;
+  DevBuf tri, blo, bhi, keys_a, keys_b, idx_a, idx_b, hist, cb, child, ipar, lpar, range, leafrec, noderec, visits, collapse, depth,
+      work_a, work_b, counters;
+  pt_status s = tri.reserve((size_t)n * 9 * sizeof(float), "device BVH build");
+  if (s == PT_OK) s = blo.reserve((size_t)n * sizeof(float4), "device BVH build");
+  if (s == PT_OK) s = bhi.reserve((size_t)n * sizeof(float4), "device BVH build");
+  if (s == PT_OK) s = keys_a.reserve((size_t)n * 4, "device BVH build");
+  if (s == PT_OK) s = keys_b.reserve((size_t)n * 4, "device BVH build");
+  if (s == PT_OK) s = idx_a.reserve((size_t)n * 4, "device BVH build");
+  if (s == PT_OK) s = idx_b.reserve((size_t)n * 4, "device BVH build");
+  if (s == PT_OK) s = hist.reserve((size_t)kRadix * nb * 4, "device BVH build");
+  if (s == PT_OK) s = cb.reserve(6 * 4, "device BVH build");
+  if (s == PT_OK) s = child.reserve((size_t)(n - 1) * sizeof(int2), "device BVH build");
+  if (s == PT_OK) s = range.reserve((size_t)(n - 1) * sizeof(int2), "device BVH build");
+  if (s == PT_OK) s = ipar.reserve((size_t)(n - 1) * 4, "device BVH build");
+  if (s == PT_OK) s = lpar.reserve((size_t)n * 4, "device BVH build");
+  if (s == PT_OK) s = leafrec.reserve((size_t)n * sizeof(NodeRec), "device BVH build");
+  if (s == PT_OK) s = noderec.reserve((size_t)(n - 1) * sizeof(NodeRec), "device BVH build");
+  if (s == PT_OK) s = visits.reserve((size_t)(n - 1) * 4, "device BVH build");
+  if (s == PT_OK) s = collapse.reserve((size_t)(n - 1), "device BVH build");
+  if (s == PT_OK) s = depth.reserve(4, "device BVH build");
+  if (s == PT_OK) s = work_a.reserve((size_t)n * sizeof(int2), "device BVH build");
+  if (s == PT_OK) s = work_b.reserve((size_t)n * sizeof(int2), "device BVH build");
+  if (s == PT_OK) s = counters.reserve(4 * 4, "device BVH build");
+  if (s == PT_OK) s = c.d_nodes.reserve((size_t)(n - 1) * 4 * sizeof(float4), "BVH nodes");
+  if (s == PT_OK) s = c.d_nodes4.reserve((size_t)(n - 1) * kWideStride * sizeof(float4), "4-wide BVH nodes");
+  if (s == PT_OK) s = c.d_v0.reserve((size_t)n * sizeof(float4), "triangles");
+  if (s == PT_OK) s = c.d_e1.reserve((size_t)n * sizeof(float4), "triangles");
+  if (s == PT_OK) s = c.d_e2.reserve((size_t)n * sizeof(float4), "triangles");
+  if (s != PT_OK) return s;
+  PT_CHECK_CUDA(cudaMemcpyAsync(tri.p, c.tri_pos.data(), (size_t)n * 9 * sizeof(float), cudaMemcpyHostToDevice, st), "device BVH build H2D");
+  const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+  PT_CHECK_CUDA(cudaMemcpyAsync(cb.p, init, sizeof(init), cudaMemcpyHostToDevice, st), "device BVH build H2D");
+  PT_CHECK_CUDA(cudaMemsetAsync(visits.p, 0, (size_t)(n - 1) * 4, st), "device BVH build");
+  PT_CHECK_CUDA(cudaMemsetAsync(depth.p, 0, 4, st), "device BVH build");
+  PT_CHECK_CUDA(cudaMemsetAsync(counters.p, 0, 16, st), "device BVH build");
+  const int g = grid_for(n, kBlock, 8);
+  k_tri_boxes<<<g, kBlock, 0, st>>>(tri.as<float>(), n, blo.as<float4>(), bhi.as<float4>(), cb.as<uint32_t>());
+  k_morton<<<g, kBlock, 0, st>>>(blo.as<float4>(), bhi.as<float4>(), n, cb.as<uint32_t>(), keys_a.as<uint32_t>(), idx_a.as<uint32_t>());
+  count_launch(2);
+  uint32_t *kin = keys_a.as<uint32_t>(), *kout = keys_b.as<uint32_t>(), *vin = idx_a.as<uint32_t>(), *vout = idx_b.as<uint32_t>();
+  for (int shift = 0; shift < 32; shift += 8) {  // four passes: the sorted keys end in keys_a
+    k_radix_hist<<<nb, kBlock, 0, st>>>(kin, n, shift, hist.as<uint32_t>());
+    k_scan_exclusive<<<1, 1024, 0, st>>>(hist.as<uint32_t>(), kRadix * nb);
+    k_radix_scatter<<<nb, kBlock, 0, st>>>(kin, vin, n, shift, hist.as<uint32_t>(), kout, vout);
+    count_launch(3);
+    std::swap(kin, kout);
+    std::swap(vin, vout);
+  }
+  const int gi = (int)((n - 1 + kBlock - 1) / kBlock), gl = (int)nb;
+  k_karras<<<gi, kBlock, 0, st>>>(kin, (int)n, child.as<int2>(), ipar.as<int>(), lpar.as<int>(), range.as<int2>());
+  k_bottom_up<<<gl, kBlock, 0, st>>>((int)n, vin, blo.as<float4>(), bhi.as<float4>(), child.as<int2>(), ipar.as<int>(), lpar.as<int>(),
+                                     leafrec.as<NodeRec>(), noderec.as<NodeRec>(), visits.as<uint32_t>(), collapse.as<uint8_t>(),
+                                     c.bvh_params.trav_cost, c.bvh_params.max_leaf);
+  k_write_bvh2<<<gi, kBlock, 0, st>>>((int)n, child.as<int2>(), ipar.as<int>(), range.as<int2>(), collapse.as<uint8_t>(), leafrec.as<NodeRec>(),
+                                      noderec.as<NodeRec>(), c.d_nodes.as<float4>());
+  k_write_tris<<<gl, kBlock, 0, st>>>((int)n, tri.as<float>(), vin, lpar.as<int>(), ipar.as<int>(), collapse.as<uint8_t>(), c.d_v0.as<float4>(),
+                                      c.d_e1.as<float4>(), c.d_e2.as<float4>(), depth.as<int>());
+  count_launch(4);
+  PT_CHECK_CUDA(cudaGetLastError(), "device BVH build launch");
+  // 4-wide collapse, level by level (root: BVH2 node 0 -> wide node 0)
+  uint32_t* cnt = counters.as<uint32_t>();  // [0] wide nodes allocated, [1] next level's items, [2] overflow
+  const uint32_t one = 1;
+  const int2 root = make_int2(0, 0);
+  PT_CHECK_CUDA(cudaMemcpyAsync(cnt, &one, 4, cudaMemcpyHostToDevice, st), "device BVH collapse");
+  PT_CHECK_CUDA(cudaMemcpyAsync(work_a.p, &root, sizeof(root), cudaMemcpyHostToDevice, st), "device BVH collapse");
+  int2 *win = work_a.as<int2>(), *wout = work_b.as<int2>();
+  uint32_t n_in = 1;
+  int levels = 0;
+  bool too_deep = false;
+  while (n_in > 0) {
+    if (levels + 1 >= kMaxDepth4) { too_deep = true; break; }  // wide node depth (root = 1) stays below kMaxDepth4
+    PT_CHECK_CUDA(cudaMemsetAsync(cnt + 1, 0, 4, st), "device BVH collapse");
+    k_collapse_level<<<(n_in + 127) / 128, 128, 0, st>>>(c.d_nodes.as<float4>(), win, n_in, wout, cnt + 1, cnt, n - 1, c.d_nodes4.as<float4>(),
+                                                         cnt + 2);
+    count_launch();
+    ++levels;
+    PT_CHECK_CUDA(cudaMemcpyAsync(&n_in, cnt + 1, 4, cudaMemcpyDeviceToHost, st), "device BVH collapse");
+    PT_CHECK_CUDA(cudaStreamSynchronize(st), "device BVH collapse");
+    std::swap(win, wout);
+  }
+  uint32_t host_cnt[3] = {0, 0, 0};
+  int d2 = 0;
+  PT_CHECK_CUDA(cudaMemcpyAsync(host_cnt, cnt, 12, cudaMemcpyDeviceToHost, st), "device BVH build");
+  PT_CHECK_CUDA(cudaMemcpyAsync(&d2, depth.p, 4, cudaMemcpyDeviceToHost, st), "device BVH build");
+  PT_CHECK_CUDA(cudaEventRecord(c.ev1, st), "device BVH build");
+  PT_CHECK_CUDA(cudaStreamSynchronize(st), "device BVH build");
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, c.ev0, c.ev1);
+  if (d2 >= 64) return fail(PT_CAP_EXCEEDED, "device BVH build: the tree is deeper than the traversal trail allows");
+  c.bvh_depth = d2;
+  c.has_bvh4 = !too_deep && host_cnt[2] == 0;
+  c.build_info.builder = 1;
+  c.build_info.device_ms = ms;
+  c.build_info.bvh2_nodes = n - 1;
+  c.build_info.bvh2_depth = (uint32_t)d2;
+  c.build_info.wide_nodes = host_cnt[0];
+  c.build_info.wide_depth = (uint32_t)levels;
+  return PT_OK;
+}
+
+}  // namespace pt

@@ -1,5 +1,7 @@
 // C ABI: context lifetime, scene objects (integrator, camera, background, materials, meshes,
 // lights), BVH build and upload, readback, and the closest/any-hit query kernels.
+#include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -679,17 +681,38 @@ pt_status pt_build(pt_ctx* ctx)
   CTX_CHECK(ctx);
   Context& c = ctx->c;
   if (c.n_tris == 0) return fail(PT_NOT_READY, "pt_build: no meshes");
-  BvhHost bvh;
-  if (!build_bvh(c.tri_pos.data(), c.n_tris, bvh, c.bvh_params)) return fail(PT_CAP_EXCEEDED, "pt_build: scene too large or BVH too deep");
-  c.bvh_depth = bvh.depth;
-  std::vector<float4> nodes4;
-  int depth4 = 0;
-  c.has_bvh4 = build_bvh4(bvh, nodes4, depth4);
-  pt_status st = upload(c.d_nodes, bvh.nodes, c.stream, "BVH nodes");
-  if (st == PT_OK && c.has_bvh4) st = upload(c.d_nodes4, nodes4, c.stream, "4-wide BVH nodes");
-  if (st == PT_OK) st = upload(c.d_v0, bvh.tri_v0, c.stream, "triangles");
-  if (st == PT_OK) st = upload(c.d_e1, bvh.tri_e1, c.stream, "triangles");
-  if (st == PT_OK) st = upload(c.d_e2, bvh.tri_e2, c.stream, "triangles");
+  PT_CHECK_CUDA(cudaSetDevice(c.device), "cudaSetDevice");
+  const auto t0 = std::chrono::steady_clock::now();
+  pt_status st = PT_OK;
+  bool on_device = false;
+  memset(&c.build_info, 0, sizeof(c.build_info));
+  if (c.bvh_builder == 1 && c.n_tris >= 2) {
+    st = build_bvh_device(c);
+    on_device = st == PT_OK;
+    if (st != PT_OK && st != PT_CAP_EXCEEDED) return st;  // too deep: the host builder takes over
+    st = PT_OK;
+  }
+  if (!on_device) {
+    BvhHost bvh;
+    if (!build_bvh(c.tri_pos.data(), c.n_tris, bvh, c.bvh_params)) return fail(PT_CAP_EXCEEDED, "pt_build: scene too large or BVH too deep");
+    c.bvh_depth = bvh.depth;
+    std::vector<float4> nodes4;
+    int depth4 = 0;
+    c.has_bvh4 = build_bvh4(bvh, nodes4, depth4);
+    st = upload(c.d_nodes, bvh.nodes, c.stream, "BVH nodes");
+    if (st == PT_OK && c.has_bvh4) st = upload(c.d_nodes4, nodes4, c.stream, "4-wide BVH nodes");
+    if (st == PT_OK) st = upload(c.d_v0, bvh.tri_v0, c.stream, "triangles");
+    if (st == PT_OK) st = upload(c.d_e1, bvh.tri_e1, c.stream, "triangles");
+    if (st == PT_OK) st = upload(c.d_e2, bvh.tri_e2, c.stream, "triangles");
+    if (st == PT_OK) PT_CHECK_CUDA(cudaStreamSynchronize(c.stream), "pt_build upload");
+    c.build_info.builder = 0;
+    c.build_info.bvh2_nodes = (uint32_t)(bvh.nodes.size() / 4);
+    c.build_info.bvh2_depth = (uint32_t)bvh.depth;
+    c.build_info.wide_nodes = c.has_bvh4 ? (uint32_t)(nodes4.size() / kWideStride) : 0u;
+    c.build_info.wide_depth = c.has_bvh4 ? (uint32_t)depth4 : 0u;
+  }
+  c.build_info.n_triangles = c.n_tris;
+  c.build_info.build_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (st == PT_OK) st = upload(c.d_info, c.tri_info, c.stream, "triangle info");
   if (st == PT_OK) st = upload(c.d_normals, c.normals, c.stream, "normals");
   if (st == PT_OK) st = upload(c.d_mats, c.mats, c.stream, "materials");
@@ -867,6 +890,11 @@ pt_status pt_set_option(pt_ctx* ctx, const char* name, int64_t value)
     ctx->c.bvh_params.max_leaf = (int)value;
     return PT_OK;
   }
+  if (k == "bvh_builder") {
+    if (value != 0 && value != 1) return fail(PT_INVALID_ARG, "pt_set_option: bvh_builder must be 0 (host SAH) or 1 (device LBVH)");
+    ctx->c.bvh_builder = (int)value;
+    return PT_OK;
+  }
   if (k == "bvh4") {
     if (value != 0 && value != 1) return fail(PT_INVALID_ARG, "pt_set_option: bvh4 must be 0 or 1");
     ctx->c.use_bvh4 = value != 0;
@@ -888,6 +916,57 @@ pt_status pt_set_profiling(pt_ctx* ctx, int enable)
 {
   if (!ctx) return fail(PT_INVALID_ARG, "null context");
   ctx->c.profile = enable != 0;
+  return PT_OK;
+}
+
+pt_status pt_get_build_info(pt_ctx* ctx, pt_build_info* out)
+{
+  CTX_CHECK(ctx);
+  Context& c = ctx->c;
+  if (!out) return fail(PT_INVALID_ARG, "pt_get_build_info: null output");
+  if (!c.built) return fail(PT_NOT_READY, "pt_get_build_info: call pt_build first");
+  *out = c.build_info;
+  // SAH cost of the BVH2 from its child-pair nodes: cost(node) = trav_cost + sum over its two children
+  // of area(child) / area(node) * cost(child), a leaf costing its triangle count
+  std::vector<float4> nodes(4 * (size_t)c.build_info.bvh2_nodes);
+  PT_CHECK_CUDA(cudaMemcpyAsync(nodes.data(), c.d_nodes.p, nodes.size() * sizeof(float4), cudaMemcpyDeviceToHost, c.stream), "pt_get_build_info");
+  PT_CHECK_CUDA(cudaStreamSynchronize(c.stream), "pt_get_build_info");
+  const float trav = c.bvh_params.trav_cost;
+  auto area = [](float lx, float hx, float ly, float hy, float lz, float hz) {
+    const float dx = std::max(0.0f, hx - lx), dy = std::max(0.0f, hy - ly), dz = std::max(0.0f, hz - lz);
+    return (double)(dx * dy + dy * dz + dz * dx);
+  };
+  // post-order over an explicit stack: cost[node] once both children are done
+  std::vector<double> cost(c.build_info.bvh2_nodes, -1.0);
+  std::vector<int> stack{0};
+  while (!stack.empty()) {
+    const int p = stack.back();
+    const float4* nd = nodes.data() + 4 * (size_t)p;
+    int code[2];
+    memcpy(&code[0], &nd[3].x, 4);
+    memcpy(&code[1], &nd[3].y, 4);
+    bool ready = true;
+    for (int k = 0; k < 2; ++k)
+      if (code[k] >= 0 && cost[code[k]] < 0.0) {
+        if ((uint32_t)code[k] >= c.build_info.bvh2_nodes) return fail(PT_CUDA_ERROR, "pt_get_build_info: malformed BVH");
+        stack.push_back(code[k]);
+        ready = false;
+      }
+    if (!ready) continue;
+    stack.pop_back();
+    const double a0 = area(nd[0].x, nd[0].y, nd[0].z, nd[0].w, nd[2].x, nd[2].y);
+    const double a1 = area(nd[1].x, nd[1].y, nd[1].z, nd[1].w, nd[2].z, nd[2].w);
+    const double A = area(std::min(nd[0].x, nd[1].x), std::max(nd[0].y, nd[1].y), std::min(nd[0].z, nd[1].z), std::max(nd[0].w, nd[1].w),
+                          std::min(nd[2].x, nd[2].z), std::max(nd[2].y, nd[2].w));
+    double sum = trav;
+    for (int k = 0; k < 2; ++k) {
+      const double ck = code[k] >= 0 ? cost[code[k]] : (double)((uint32_t)code[k] & 15u);
+      const double ak = k == 0 ? a0 : a1;
+      if (A > 0.0 && ak < 1e20) sum += ak / A * ck;
+    }
+    cost[p] = sum;
+  }
+  out->sah_cost = (float)cost[0];
   return PT_OK;
 }
 

@@ -204,6 +204,8 @@ struct Context {
   BvhParams bvh_params;    // options "bvh_trav_cost_milli" and "bvh_max_leaf", applied by pt_build
   bool has_bvh4 = false;
   bool use_bvh4 = true;  // option "bvh4": the persistent traversal kernels walk the 4-wide BVH
+  int bvh_builder = 0;   // option "bvh_builder": 0 host binned SAH, 1 device LBVH
+  pt_build_info build_info{};
   DevBuf d_scat, d_trans_objs, d_trans_pos;
   DevBuf d_scene_tab, d_item_tab;  // scene and item tables of the current pass (this context as the engine)
   bool pass_w4 = false;            // every scene of the current pass has a 4-wide BVH
@@ -242,6 +244,11 @@ struct Context {
 
   SceneDev view() const;
 };
+
+// The LBVH of pt_bvh_device.cu built on the device from tri_pos into d_nodes, d_nodes4, d_v0/e1/e2
+// (sets bvh_depth, has_bvh4 and build_info); PT_CAP_EXCEEDED when the tree is too deep for the
+// traversal trail.
+pt_status build_bvh_device(Context& c);
 
 struct Context;
 pt_status prepare_scene(Context& c, const char* who);

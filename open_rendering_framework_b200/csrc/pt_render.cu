@@ -28,6 +28,7 @@
 // is a fixed sequence of launches with no host synchronisation (CUDA-graph capturable).
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 
 #include "pt_context.h"
 #include "pt_dipole.cuh"
@@ -542,9 +543,7 @@ __global__ void __launch_bounds__(kTraceBlock, PT_TRACE_MIN_BLOCKS) k_extend_per
   bool has = false, done = false, drained = false;
   uint32_t pid = 0, qi = 0, traced = 0;
   float3 o = f3s(0.0f), d = f3s(0.0f);
-  RayPre rp;
-  rp.inv = f3s(0.0f);
-  rp.sx = rp.sy = rp.sz = 0;
+  std::conditional_t<kW4, RayPre4, RayPre> rp{};
   Hit h;
   h.t = 0.0f; h.u = h.v = 0.0f; h.prim = -1;
   TravState st;
@@ -576,7 +575,8 @@ __global__ void __launch_bounds__(kTraceBlock, PT_TRACE_MIN_BLOCKS) k_extend_per
           float4 o4 = w.ray_o[pid], d4 = w.ray_d[pid];
           o = ld3(o4);
           d = ld3(d4);
-          rp = ray_pre(o, d);
+          if constexpr (kW4) rp = ray_pre4(o, d);
+          else rp = ray_pre(o, d);
           h.t = kDefaultMax;
           h.u = h.v = 0.0f;
           h.prim = -1;
@@ -607,7 +607,7 @@ __global__ void __launch_bounds__(kTraceBlock, PT_TRACE_MIN_BLOCKS) k_extend_per
             cur = stack4_next(s4, h.t, true);
           }
         } else if (np) {
-          cur = trav4_node_closest(g, cur, o, rp, eps, h, s4);
+          cur = trav4_node_closest(g, cur, rp, eps, h, s4);
         }
         done = cur == kDone4;
       } else {
@@ -832,9 +832,7 @@ __global__ void __launch_bounds__(kTraceBlock, PT_TRACE_MIN_BLOCKS) k_shadow_per
   uint32_t slot = 0, leafA = 0, leafB = 0;
   float3 o = f3s(0.0f), d = f3s(0.0f);
   float tmin = 0.0f, tmax = 0.0f;
-  RayPre rp;
-  rp.inv = f3s(0.0f);
-  rp.sx = rp.sy = rp.sz = 0;
+  std::conditional_t<kW4, RayPre4, RayPre> rp{};
   TravState st;
   trav_init(st, stk + threadIdx.x, kTraceBlock);
   uint2 spill4[kW4 ? kSpill4 : 1];
@@ -858,7 +856,8 @@ __global__ void __launch_bounds__(kTraceBlock, PT_TRACE_MIN_BLOCKS) k_shadow_per
           d = ld3(d4);
           tmin = o4.w;
           tmax = d4.w;
-          rp = ray_pre(o, d);
+          if constexpr (kW4) rp = ray_pre4(o, d);
+          else rp = ray_pre(o, d);
           if constexpr (kW4) {
             stack4_init(s4, stk + threadIdx.x, kTraceBlock, spill4);
             cur = 0;
@@ -885,7 +884,7 @@ __global__ void __launch_bounds__(kTraceBlock, PT_TRACE_MIN_BLOCKS) k_shadow_per
             else cur = stack4_next(s4, tmax, false);
           }
         } else if (np) {
-          cur = trav4_node_any(g, cur, o, rp, tmin, tmax, s4);
+          cur = trav4_node_any(g, cur, rp, tmin, tmax, s4);
         }
         if (has && res == 0 && cur == kDone4) res = -1;
       } else {

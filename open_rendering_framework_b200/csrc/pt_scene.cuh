@@ -603,16 +603,79 @@ PT_HD void cswap4(int code[4], float t[4], int a, int b)
   code[a] = sw ? cb : ca;
   code[b] = sw ? ca : cb;
 }
-// The slab test of `slab` with the near and far planes of each axis chosen by the direction's sign
-// (loaded from the node's lo or hi plane row): the same products, so the same distances and the same
-// decisions, without the per-axis min / max that orders them.
-PT_HD float slab_nf(float nx, float fx, float ny, float fy, float nz, float fz, const float3& o, const RayPre& r, float tmin, float tmax)
+// Ray constants of the wide BVH's slab test, which takes one fused multiply-add per plane:
+// t = fma(plane, inv, -o * inv).  The product o * inv is rounded once per ray, an absolute error of
+// at most 2^-24 |o * inv| in every slab distance of that axis (the fma itself rounds once, a relative
+// error that the relative slack kSlack covers as in `slab`).  Each axis therefore carries a margin E
+// >= 16 x that bound: near distances are lowered by E and far distances raised by E (cn = -o*inv - E,
+// cf = -o*inv + E), so the test can only keep more boxes than the exact one.  A direction component of
+// magnitude below 2^-64 (a zero one included) is taken as +-2^-64 so that every constant is finite: the
+// ray then drifts at most 2^-64 t off its line, which the absolute part of E (2^-40 in space, times
+// |inv|) covers for t up to 2^24 -- far beyond any scene, whose other axes bound t.
+constexpr float kInvMax = 18446744073709551616.0f;  // 2^64
+constexpr float kRelMargin = 9.5367431640625e-07f;  // 2^-20
+constexpr float kAbsMargin = 9.094947017729282e-13f; // 2^-40
+struct RayPre4 {
+  float3 inv;     // 1 / d, clamped to +-2^64
+  float3 cn, cf;  // per axis: -(o * inv) - E, -(o * inv) + E
+  int sx, sy, sz; // 1 where the direction component is negative: the near plane is the box's hi
+};
+PT_HD float clamp_inv(float d)
 {
-  const float tnx = (nx - o.x) * r.inv.x, tfx = (fx - o.x) * r.inv.x;
-  const float tny = (ny - o.y) * r.inv.y, tfy = (fy - o.y) * r.inv.y;
-  const float tnz = (nz - o.z) * r.inv.z, tfz = (fz - o.z) * r.inv.z;
-  const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
-  const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax * kSlack));
+  const float r = 1.0f / d;
+  return fabsf(r) <= kInvMax ? r : copysignf(kInvMax, d);
+}
+PT_HD RayPre4 ray_pre4(const float3& o, const float3& d)
+{
+  RayPre4 r;
+  r.inv = f3(clamp_inv(d.x), clamp_inv(d.y), clamp_inv(d.z));
+  const float ox = o.x * r.inv.x, oy = o.y * r.inv.y, oz = o.z * r.inv.z;
+  const float ex = fabsf(ox) * kRelMargin + kAbsMargin * fabsf(r.inv.x);
+  const float ey = fabsf(oy) * kRelMargin + kAbsMargin * fabsf(r.inv.y);
+  const float ez = fabsf(oz) * kRelMargin + kAbsMargin * fabsf(r.inv.z);
+  r.cn = f3(-ox - ex, -oy - ey, -oz - ez);
+  r.cf = f3(-ox + ex, -oy + ey, -oz + ez);
+  r.sx = r.inv.x < 0.0f;
+  r.sy = r.inv.y < 0.0f;
+  r.sz = r.inv.z < 0.0f;
+  return r;
+}
+PT_HD float fma_rn(float a, float b, float c)
+{
+#ifdef __CUDA_ARCH__
+  return __fmaf_rn(a, b, c);
+#else
+  return fmaf(a, b, c);
+#endif
+}
+PT_HD float max3f(float a, float b, float c)
+{
+#ifdef __CUDA_ARCH__
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+#else
+  return fmaxf(fmaxf(a, b), c);
+#endif
+}
+PT_HD float min3f(float a, float b, float c)
+{
+#ifdef __CUDA_ARCH__
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+#else
+  return fminf(fminf(a, b), c);
+#endif
+}
+// The wide node's slab test of one child, with the near and far planes of each axis chosen by the
+// direction's sign (loaded from the node's lo or hi plane row): one fma per plane and three-input
+// min / max; returns the (lowered) entry distance, or +inf on a miss.  The planes are finite (an empty
+// slot's are 1e30) and so are the constants, so no distance is NaN.
+PT_HD float slab4(float nx, float fx, float ny, float fy, float nz, float fz, const RayPre4& r, float tmin, float tmax)
+{
+  const float tn = fmaxf(max3f(fma_rn(nx, r.inv.x, r.cn.x), fma_rn(ny, r.inv.y, r.cn.y), fma_rn(nz, r.inv.z, r.cn.z)), tmin);
+  const float tf = min3f(fma_rn(fx, r.inv.x, r.cf.x), fma_rn(fy, r.inv.y, r.cf.y), fminf(fma_rn(fz, r.inv.z, r.cf.z), tmax * kSlack));
   return tn <= tf * kSlack ? tn : as_float(0x7f800000);
 }
 PT_HD int popc32(unsigned m)
@@ -627,7 +690,7 @@ PT_HD int popc32(unsigned m)
 // kSort and kWide == 4 sorted near to far by a five-comparator network (else in slot order),
 // returning the count of hits.
 template <bool kSort = true, class G>
-PT_HD int node4_hits(const G& S, int node, const float3& o, const RayPre& rp, float tmin, float tmax, int code[kWide], float t[kWide])
+PT_HD int node4_hits(const G& S, int node, const RayPre4& rp, float tmin, float tmax, int code[kWide], float t[kWide])
 {
   const float4* nd = S.nodes4 + kWideStride * (size_t)node;
 #pragma unroll
@@ -636,10 +699,10 @@ PT_HD int node4_hits(const G& S, int node, const float3& o, const RayPre& rp, fl
     const float4 ny = PT_LDG(nd + (2 + rp.sy) * kWideRow + r), fy = PT_LDG(nd + (3 - rp.sy) * kWideRow + r);
     const float4 nz = PT_LDG(nd + (4 + rp.sz) * kWideRow + r), fz = PT_LDG(nd + (5 - rp.sz) * kWideRow + r);
     const int4 c = PT_LDG(reinterpret_cast<const int4*>(nd + 6 * kWideRow + r));
-    t[4 * r + 0] = slab_nf(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, o, rp, tmin, tmax);
-    t[4 * r + 1] = slab_nf(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, o, rp, tmin, tmax);
-    t[4 * r + 2] = slab_nf(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, o, rp, tmin, tmax);
-    t[4 * r + 3] = slab_nf(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, o, rp, tmin, tmax);
+    t[4 * r + 0] = slab4(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, rp, tmin, tmax);
+    t[4 * r + 1] = slab4(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, rp, tmin, tmax);
+    t[4 * r + 2] = slab4(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, rp, tmin, tmax);
+    t[4 * r + 3] = slab4(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, rp, tmin, tmax);
     code[4 * r + 0] = c.x;
     code[4 * r + 1] = c.y;
     code[4 * r + 2] = c.z;
@@ -695,21 +758,21 @@ PT_HD int node4_advance(int n, const int code[kWide], const float t[kWide], Stac
   }
 }
 // One closest-hit node step: cur must be a node; returns the next target (node, leaf or kDone4).
-template <class G> PT_HD int trav4_node_closest(const G& S, int cur, const float3& o, const RayPre& rp, float tmin, const Hit& h, Stack4& stk)
+template <class G> PT_HD int trav4_node_closest(const G& S, int cur, const RayPre4& rp, float tmin, const Hit& h, Stack4& stk)
 {
   int code[kWide];
   float t[kWide];
-  const int n = node4_hits(S, cur, o, rp, tmin, h.t, code, t);
+  const int n = node4_hits(S, cur, rp, tmin, h.t, code, t);
   return node4_advance(n, code, t, stk, h.t, true);
 }
 // Any-hit node step.  Whether some triangle lies in (tmin, tmax) does not depend on the order in which
 // the hit children are visited, so they are taken in slot order without sorting: all but the last hit
 // child are pushed, the last is visited next.
-template <class G> PT_HD int trav4_node_any(const G& S, int cur, const float3& o, const RayPre& rp, float tmin, float tmax, Stack4& stk)
+template <class G> PT_HD int trav4_node_any(const G& S, int cur, const RayPre4& rp, float tmin, float tmax, Stack4& stk)
 {
   int code[kWide];
   float t[kWide];
-  node4_hits<false>(S, cur, o, rp, tmin, tmax, code, t);
+  node4_hits<false>(S, cur, rp, tmin, tmax, code, t);
   const float inf = as_float(0x7f800000);
   int next = kDone4;
   float tnext = 0.0f;

@@ -69,6 +69,16 @@ class TranslucentParams(ctypes.Structure):
                 ("ior", ctypes.c_float), ("scale", ctypes.c_float), ("dipole_model", ctypes.c_uint32)]
 
 
+class BuildInfo(ctypes.Structure):
+    """pt_build_info: the acceleration structure of the last pt_build."""
+    _fields_ = [("builder", ctypes.c_uint32), ("n_triangles", ctypes.c_uint32), ("bvh2_nodes", ctypes.c_uint32), ("bvh2_depth", ctypes.c_uint32),
+                ("wide_nodes", ctypes.c_uint32), ("wide_depth", ctypes.c_uint32), ("build_ms", ctypes.c_float), ("device_ms", ctypes.c_float),
+                ("sah_cost", ctypes.c_float)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class MicrofacetBatch(ctypes.Structure):
     """pt_microfacet_batch: one batch of multiscattering-walk / conductor-Fresnel queries."""
     _fields_ = [("op", ctypes.c_uint32), ("normal_distribution", ctypes.c_uint32), ("normal", ctypes.c_float * 3), ("eta", ctypes.c_float),
@@ -672,7 +682,7 @@ class SceneData:
 class Renderer:
     """Owns a pt_ctx and plays the part of OptixScene: scene setup, build, renderScene()."""
 
-    def __init__(self, data, device=0, max_paths_in_flight=None):
+    def __init__(self, data, device=0, max_paths_in_flight=None, build_options=None):
         self.data = data
         self.integrator, self.camera, self.background = data.integrator, data.camera, data.background
         self.frame = 0
@@ -709,7 +719,21 @@ class Renderer:
                      None if m.nindex is None else m.nindex.ctypes.data, mid, ctypes.byref(first))
         lb, tb = data.light_buffer, data.triangle_light_buffer
         nat.call("pt_lights_upload", self.ctx, lb.ctypes.data if len(lb) else None, len(lb), tb.ctypes.data if len(tb) else None, len(tb))
+        for name, value in (build_options or {}).items():
+            nat.call("pt_set_option", self.ctx, name.encode(), int(value))
         nat.call("pt_build", self.ctx)
+
+    def rebuild(self, **options):
+        """Set build options (e.g. bvh_builder=1) and rebuild the acceleration structure (pt_build)."""
+        for name, value in options.items():
+            nat.call("pt_set_option", self.ctx, name.encode(), int(value))
+        nat.call("pt_build", self.ctx)
+
+    def build_info(self):
+        """pt_build_info of the last build (SAH cost included)."""
+        b = BuildInfo()
+        nat.call("pt_get_build_info", self.ctx, ctypes.byref(b))
+        return b
 
     def update_material(self, mat):
         """Push changed parameters of a material already in the scene."""

@@ -131,6 +131,31 @@ def analytic_light_scene(width=64, height=64, subdiv=3, max_depth=8, rr_start_de
     return sc.SceneData(integrator, camera, background, meshes, lights)
 
 
+def open_lights_scene(width=64, height=64, subdiv=3, max_depth=8, rr_start_depth=0):
+    """An open scene (no enclosing box: a 6 x 6 diffuse floor quad under a black background) lit by a
+    DirectionalLight and a PointLight (LightSampler.h:20-37): a diffuse icosphere, a GGX conductor
+    icosphere and a Lambertian-interface icosphere on the floor, so that the lights' shadow rays reach
+    the light (a directional light's to infinity) or are blocked by the spheres."""
+    integrator = sc.PathTracer(max_depth=max_depth, scene_epsilon=1e-4, rr_start_depth=rr_start_depth)
+    camera = sc.PinholeCamera(eye=(0.0, 0.6, 1.6), lookat=(0.0, -0.2, 0.0), up=(0.0, 1.0, 0.0), vfov=50.0, width=width, height=height)
+    background = sc.ConstantBackground((0.0, 0.0, 0.0))
+    floor = sc.DiffuseMaterial((0.6, 0.6, 0.6))
+    diffuse = sc.DiffuseMaterial((0.8, 0.3, 0.2))
+    metal = sc.MetallicMaterial(ior=((0.2, 3.9), (0.55, 3.15), (0.9, 2.4)), roughness=(0.2, 0.2), microfacet_model=sc.WALTER_MODEL,
+                                normal_distribution=sc.GGX_DISTRIBUTION)
+    lamb = sc.LambertianInterfaceMaterial(color=(0.2, 0.4, 0.8), ior=1.5)
+    fp_ = np.array([(-3, -0.5, -3), (3, -0.5, -3), (3, -0.5, 3), (-3, -0.5, 3)], np.float32)
+    fi = np.array([(0, 2, 1), (0, 3, 2)], np.int32)
+    dp, di, dn, dni = icosphere(subdiv, 0.25, (-0.5, -0.25, -0.2))
+    mp, mi, mn, mni = icosphere(subdiv, 0.25, (0.0, -0.25, -0.5))
+    lp, li, ln, lni = icosphere(subdiv, 0.25, (0.5, -0.25, -0.1))
+    meshes = [sc.Mesh(fp_, fi, floor), sc.Mesh(dp, di, diffuse, dn, dni), sc.Mesh(mp, mi, metal, mn, mni), sc.Mesh(lp, li, lamb, ln, lni)]
+    d = np.array([-0.4, -1.0, -0.3])
+    d /= np.linalg.norm(d)
+    lights = [sc.DirectionalLight(direction=tuple(d), radiance=(2.5, 2.4, 2.2)), sc.PointLight(position=(0.6, 1.2, 0.8), radiance=(4.0, 3.0, 2.0))]
+    return sc.SceneData(integrator, camera, background, meshes, lights)
+
+
 def sky_envmap(width=2048, height=1024, sun_dir=(0.35, 0.55, 0.45), sun_peak=5.0e4, sun_sigma_deg=1.0):
     """Procedural equirectangular sky in the reference's mapping (envmap.h: u = (atan2(x, z) + pi) / 2pi,
     v = 1 - acos(y) / pi): a vertical gradient from horizon to zenith, a darker ground, and a Gaussian sun

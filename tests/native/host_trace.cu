@@ -71,7 +71,7 @@ extern "C" __attribute__((visibility("default"))) int ht_trace4(void* hp, const 
     float3 o = make_float3(r[0], r[1], r[2]), d = make_float3(r[4], r[5], r[6]);
     uint2 ring[kRing4], spill[kSpill4];
     const int stride = 1;
-    RayPre rp = ray_pre(o, d);
+    RayPre4 rp = ray_pre4(o, d);
     Hit hh;
     hh.t = r[7];
     hh.u = hh.v = 0.0f;
@@ -84,7 +84,7 @@ extern "C" __attribute__((visibility("default"))) int ht_trace4(void* hp, const 
         leaf_closest(h->S, (uint32_t)cur, o, d, r[3], hh);
         cur = stack4_next(s4, hh.t, true);
       } else {
-        cur = trav4_node_closest(h->S, cur, o, rp, r[3], hh, s4);
+        cur = trav4_node_closest(h->S, cur, rp, r[3], hh, s4);
       }
       *max_sp = s4.sp > *max_sp ? s4.sp : *max_sp;
     }
@@ -101,7 +101,7 @@ extern "C" __attribute__((visibility("default"))) int ht_trace4(void* hp, const 
         if (leaf_any(h->S, (uint32_t)cur, o, d, r[3], r[7])) res = 1;
         else cur = stack4_next(s4, r[7], false);
       } else {
-        cur = trav4_node_any(h->S, cur, o, rp, r[3], r[7], s4);
+        cur = trav4_node_any(h->S, cur, rp, r[3], r[7], s4);
       }
       *max_sp = s4.sp > *max_sp ? s4.sp : *max_sp;
     }

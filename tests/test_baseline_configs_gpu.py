@@ -69,7 +69,7 @@ def oracle_band(data, y0, rows, frames, path_radiance=False):
 
 def test_single_scene_configuration_band_matches_oracle():
     data = scenes.single_scene()
-    assert (data.camera.width, data.camera.height) == (512, 512) and data.n_triangles() == 12 + 81920 + 20480 + 2
+    assert (data.camera.width, data.camera.height) == (512, 512) and data.n_triangles == 12 + 81920 + 20480 + 2
     y0, rows, frames = 240, 32, 4
     got, st = gpu_band(data, y0, rows, frames)
     ref, _ = oracle_band(data, y0, rows, frames)
@@ -97,7 +97,7 @@ def test_single_scene_configuration_converged_band_below_sample_variance():
 
 def test_subsurface_configuration_band_matches_oracle():
     data = scenes.subsurface_scene()
-    assert (data.camera.width, data.camera.height) == (1024, 1024) and data.n_triangles() == 327680
+    assert (data.camera.width, data.camera.height) == (1024, 1024) and data.n_triangles == 327680
     y0, rows, frames = 508, 8, 2
     got, st = gpu_band(data, y0, rows, frames)
     ref, _ = oracle_band(data, y0, rows, frames)

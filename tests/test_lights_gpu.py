@@ -1,6 +1,7 @@
-"""GPU parity of the disk and sphere lights' analytic geometry (disk_mesh.cu, sphere_mesh.cu): camera
-rays see the emitters through the area-light program, shadow rays are blocked by them, and their
-next-event estimates follow LightSampler.h.  Checked against the CPU restatement through the C ABI.
+"""GPU parity of the directional and point lights' next-event estimates, and of the disk and sphere
+lights' analytic geometry (disk_mesh.cu, sphere_mesh.cu): camera rays see the emitters through the
+area-light program, shadow rays are blocked by them, and their next-event estimates follow
+LightSampler.h.  Checked against the CPU restatement through the C ABI.
 
 Bars: closest-hit index, t and barycentrics and any-hit bit-identical to the oracle's brute-force loop
 (triangles, then the emitters in light order, ties to the lower index); images as for the other
@@ -73,6 +74,27 @@ def test_disk_and_sphere_light_images_match_the_oracle():
     rel = np.abs(got[..., :3] - ref[..., :3]) / np.maximum(np.abs(ref[..., :3]), 1e-3)
     pix_ok = np.all(rel <= 1e-3, axis=-1).mean()
     print("pixels within 1e-3:", pix_ok, "relMSE", rel_mse(got, ref), "max", float(ref.max()))
+    assert pix_ok >= 0.97
+    assert rel_mse(got, ref) < 1e-3
+    R.close()
+
+
+def test_directional_and_point_light_images_match_the_oracle():
+    """DirectionalLight and PointLight next-event estimation (LightSampler.h:20-37) in an open scene."""
+    w = h = 48
+    data = scenes.open_lights_scene(w, h)
+    assert [type(L).__name__ for L in data.lights] == ["DirectionalLight", "PointLight"]
+    R = sc.Renderer(data)
+    R.render(4)
+    got = R.readback()
+    O = oc.OracleScene(data)
+    ref, _ = O.render(0, 4, accum=np.zeros((h, w, 4), np.float32), threads=8)
+    assert np.all(np.isfinite(got))
+    lit = float(np.mean(ref[..., :3].sum(-1) > 0))
+    rel = np.abs(got[..., :3] - ref[..., :3]) / np.maximum(np.abs(ref[..., :3]), 1e-3)
+    pix_ok = np.all(rel <= 1e-3, axis=-1).mean()
+    print("directional + point: pixels within 1e-3:", pix_ok, "relMSE", rel_mse(got, ref), "lit fraction", lit)
+    assert lit > 0.3
     assert pix_ok >= 0.97
     assert rel_mse(got, ref) < 1e-3
     R.close()

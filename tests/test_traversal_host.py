@@ -132,3 +132,52 @@ def test_host_traversal_far_from_origin(host_lib):
     assert np.array_equal(t4.view(np.uint32), bt.view(np.uint32))
     assert np.array_equal(bary4.view(np.uint32), bb.view(np.uint32))
     assert np.array_equal(anyh4, ba)
+
+
+@pytest.mark.parametrize("plane", [0.0, 0.5, -3.0])
+def test_host_traversal_rays_inside_a_box_face_plane(host_lib, plane):
+    # triangles with one vertex on the plane x = plane (or y, z) and the rest on one side of it, so that
+    # the plane is a face of many boxes; rays with an exactly zero direction component that start on
+    # the plane and run inside it, aimed at those vertices: their hits are exactly on box faces
+    rng = np.random.default_rng(int(abs(plane) * 10) + 7)
+    tris, rays = [], []
+    for axis in range(3):
+        for k in range(300):
+            v0 = rng.uniform(-1, 1, 3).astype(np.float32)
+            v0[axis] = plane
+            side = -1.0 if k % 2 else 1.0
+            v1 = v0 + rng.uniform(0.05, 0.4, 3).astype(np.float32) * side
+            v2 = v0 + rng.uniform(0.05, 0.4, 3).astype(np.float32) * side * np.array([1, -1, 1], np.float32)
+            v1[axis] = plane + side * rng.uniform(0.05, 0.4)
+            v2[axis] = plane + side * rng.uniform(0.05, 0.4)
+            tris.append(np.concatenate([v0, v1, v2]))
+            o = rng.uniform(-1, 1, 3).astype(np.float32)
+            o[axis] = plane
+            d = (v0 - o).astype(np.float64)
+            d[axis] = 0.0
+            d /= np.linalg.norm(d)
+            d = d.astype(np.float32)
+            d[axis] = 0.0
+            rays.append(np.concatenate([o, [1e-5], d, [1e27]]))
+    tp = np.ascontiguousarray(np.array(tris, np.float32))
+    rays = np.ascontiguousarray(np.array(rays, np.float32))
+    h = host_lib.ht_build(oc.fp(tp), len(tp), None)
+    n = len(rays)
+    prim4, t4 = np.empty(n, np.int32), np.empty(n, np.float32)
+    bary4, anyh4 = np.empty((n, 2), np.float32), np.empty(n, np.int32)
+    max_sp = ctypes.c_int()
+    assert host_lib.ht_trace4(h, oc.fp(rays), n, oc.fp(prim4), oc.fp(t4), oc.fp(bary4), oc.fp(anyh4), ctypes.byref(max_sp)) == 0
+    host_lib.ht_free(h)
+    # brute force over the same triangles (the oracle's scene needs meshes: one mesh of the triangles)
+    from open_rendering_framework_b200 import scene as sc
+
+    P = tp.reshape(-1, 3)
+    I = np.arange(len(P), dtype=np.int32).reshape(-1, 3)
+    base = scenes.single_scene(width=8, height=8, metal_subdiv=1, glass_subdiv=1)
+    data = sc.SceneData(base.integrator, base.camera, base.background, [sc.Mesh(P, I, base.meshes[1].material)], [])
+    bp, bt, bb, ba = oc.OracleScene(data).trace(rays, brute=True)
+    assert np.mean(bp >= 0) > 0.3
+    assert np.array_equal(prim4, bp)
+    assert np.array_equal(t4.view(np.uint32), bt.view(np.uint32))
+    assert np.array_equal(bary4.view(np.uint32), bb.view(np.uint32))
+    assert np.array_equal(anyh4, ba)
