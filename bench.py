@@ -790,7 +790,7 @@ def measure_batched(args, world, local, relmse=True):
                                     "reference's launch pattern), host-timed between device synchronisations"},
         "batched_over_plain_per_frame": value / plain_per_frame,
         "autotune": {"extend_mode": tune.extend_mode, "refill": tune.refill, "max_paths_in_flight": tune.max_paths_in_flight,
-                     "trials": tune.trials, "best_calibration_mpaths_per_s": tune.best_mpaths_per_s},
+                     "bin_items": tune.bin_items, "trials": tune.trials, "best_calibration_mpaths_per_s": tune.best_mpaths_per_s},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),

@@ -343,6 +343,8 @@ pt_status pt_get_render_stats(pt_ctx* ctx, pt_render_stats* out);
  *   "extend_mode"  0 = one ray per thread with block-aggregated queue appends,
  *                  1 = persistent warps that refill finished lanes with new rays (default)
  *   "refill"       persistent kernels refill a warp when at least this many lanes are idle (1..32, default 20)
+ *   "bin_items"    the sort granularity of the material binning: queue positions per thread, 256 threads
+ *                  per chunk (4, 8 or 16; default 8)
  *   "bvh4"         1 = the persistent kernels walk the 4-wide BVH (default), 0 = the BVH2
  *   "bvh_trav_cost_milli"  SAH cost of a node step x 1000 relative to a triangle test (default 1200) and
  *   "bvh_max_leaf"         the largest leaf the SAH may choose (1..15, default 8): applied by the next pt_build
@@ -425,6 +427,7 @@ typedef struct pt_tune_result {
   uint64_t max_paths_in_flight; /* chosen paths per wavefront chunk                     */
   float best_mpaths_per_s;      /* calibration throughput of the winner                 */
   uint32_t trials;              /* configurations timed                                 */
+  uint32_t bin_items;           /* chosen "bin_items" (the sort granularity)             */
 } pt_tune_result;
 pt_status pt_batch_create(int device, pt_batch** out);
 pt_status pt_batch_destroy(pt_batch* batch);
@@ -443,8 +446,9 @@ pt_status pt_batch_render_sequential(pt_batch* batch);
 /* Counters and device time of the last batch render (synchronizes). */
 pt_status pt_batch_get_stats(pt_batch* batch, pt_render_stats* out);
 /* Times short renders (min(frames_per_render, frames_per_trial) frames of every scene) over the
- * engine options -- extend kernel, warp refill threshold, paths per wavefront chunk -- and keeps the
- * fastest.  The trials render from frame 0, so every scene's accumulation restarts at frame 0. */
+ * engine options -- extend kernel, warp refill threshold, paths per wavefront chunk (the queue tile),
+ * then the material binning's positions per thread (the sort granularity) for the winner -- and keeps
+ * the fastest.  The trials render from frame 0, so every scene's accumulation restarts at frame 0. */
 pt_status pt_batch_autotune(pt_batch* batch, uint32_t frames_per_trial, pt_tune_result* out);
 
 /* ---------------------------------------------------------------- OBJ models (scene ingestion)

@@ -315,9 +315,32 @@ pt_status pt_batch_autotune(pt_batch* b, uint32_t frames_per_trial, pt_tune_resu
       win = cd;
     }
   }
+  // second stage: the sort granularity (queue positions per binning thread) for the winner
+  int win_items = E.opt.bin_items;
+  E.opt.extend_mode = win.mode;
+  E.opt.refill = win.refill;
+  E.max_paths = win.max_paths;
+  for (int items : {4, 16}) {
+    if (items == win_items) continue;
+    E.opt.bin_items = items;
+    for (size_t k = 0; k < b->scenes.size(); ++k) b->scenes[k]->c.next_frame = 0;
+    pt_status st = render(b, false, &trial_frames, false);
+    if (st == PT_OK) st = render(b, false, &trial_frames, false);
+    if (st != PT_OK) return st;
+    PT_CHECK_CUDA(cudaStreamSynchronize(E.stream), "autotune");
+    float ms = 0.0f;
+    PT_CHECK_CUDA(cudaEventElapsedTime(&ms, E.ev0, E.ev1), "autotune timing");
+    const float rate = ms > 0.0f ? (float)E.stats.path_samples / ms : 0.0f;
+    ++trials;
+    if (rate > best) {
+      best = rate;
+      win_items = items;
+    }
+  }
   E.opt = saved_opt;
   E.opt.extend_mode = win.mode;
   E.opt.refill = win.refill;
+  E.opt.bin_items = win_items;
   E.max_paths = win.max_paths;
   (void)saved_max;
   drop_graph(b);
@@ -329,6 +352,7 @@ pt_status pt_batch_autotune(pt_batch* b, uint32_t frames_per_trial, pt_tune_resu
   out->max_paths_in_flight = win.max_paths;
   out->best_mpaths_per_s = best / 1e3f;
   out->trials = trials;
+  out->bin_items = (uint32_t)win_items;
   return PT_OK;
 }
 

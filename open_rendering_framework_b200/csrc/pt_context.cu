@@ -906,6 +906,9 @@ pt_status pt_set_option(pt_ctx* ctx, const char* name, int64_t value)
   } else if (k == "refill") {
     if (value < 1 || value > 32) return fail(PT_INVALID_ARG, "pt_set_option: refill must be in [1, 32]");
     ctx->c.opt.refill = (int)value;
+  } else if (k == "bin_items") {
+    if (value != 4 && value != 8 && value != 16) return fail(PT_INVALID_ARG, "pt_set_option: bin_items must be 4, 8 or 16");
+    ctx->c.opt.bin_items = (int)value;
   } else {
     return fail(PT_INVALID_ARG, "pt_set_option: unknown option " + k);
   }

@@ -167,6 +167,7 @@ enum ProfKind { PROF_EXTEND = 0, PROF_GATHER = 1 };
 struct Options {
   int extend_mode = 1;  // 0: one ray per thread, block-aggregated appends; 1: persistent warps with ray refill
   int refill = 20;      // persistent kernels: refill when at least this many lanes of a warp are idle (1..32)
+  int bin_items = 8;    // material binning: queue positions per thread (4, 8 or 16; 256 threads per chunk)
 };
 
 struct Context {

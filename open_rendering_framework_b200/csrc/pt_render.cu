@@ -659,43 +659,61 @@ __global__ void __launch_bounds__(kTraceBlock, PT_TRACE_MIN_BLOCKS) k_extend_per
 // the rays it came from: camera rays in pixel order, later bounces in the order the shading kernels
 // appended them.  Neighbouring entries of a material queue then address neighbouring path records
 // (coalesced state reads and writes in the shading kernels) and emit spatially coherent shadow rays.
-// The queue is cut into chunks of kBinChunk positions (kBinItems consecutive positions per thread);
-// k_bin_count counts every chunk's classes, k_bin_scan turns the counts into each chunk's start in
-// every material queue (one block, chunk order), and k_bin_scatter writes every chunk's entries there.
+// The queue is cut into chunks of kBinThreads * kItems positions (kItems consecutive positions per
+// thread; kItems = 4, 8 or 16, the launch option "bin_items" that the autotuner sets -- the sort
+// granularity); k_bin_count counts every chunk's classes, k_bin_scan turns the counts into each
+// chunk's start in every material queue (one block, chunk order), and k_bin_scatter writes every
+// chunk's entries there.
 constexpr int kBinThreads = 256;
-constexpr int kBinItems = 8;
-constexpr int kBinChunk = kBinThreads * kBinItems;
+constexpr int kBinItemsMin = 4;
 constexpr int kBinWarps = kBinThreads / 32;
+__host__ __device__ constexpr uint32_t bin_chunk(int items) { return (uint32_t)kBinThreads * (uint32_t)items; }
 
-// The classes of the kBinItems positions of this thread in chunk k (-1 past the end of the queue).
-__device__ __forceinline__ void bin_load(const WfDev& w, uint32_t n, uint32_t k, int c[kBinItems])
+// The classes of the kItems positions of this thread in chunk k (-1 past the end of the queue); a full
+// run is one aligned vector load of kItems bytes.
+template <int kItems>
+__device__ __forceinline__ void bin_load(const WfDev& w, uint32_t n, uint32_t k, int c[kItems])
 {
-  const uint32_t i0 = k * kBinChunk + threadIdx.x * kBinItems;
-  if (i0 + kBinItems <= n) {
-    const uint2 v = *reinterpret_cast<const uint2*>(w.cls_of + i0);
+  const uint32_t i0 = k * bin_chunk(kItems) + threadIdx.x * kItems;
+  if (i0 + kItems <= n) {
+    uint32_t v[kItems / 4];
+    if constexpr (kItems == 4) {
+      v[0] = *reinterpret_cast<const uint32_t*>(w.cls_of + i0);
+    } else if constexpr (kItems == 8) {
+      const uint2 u = *reinterpret_cast<const uint2*>(w.cls_of + i0);
+      v[0] = u.x;
+      v[1] = u.y;
+    } else {
+      const uint4 u = *reinterpret_cast<const uint4*>(w.cls_of + i0);
+      v[0] = u.x;
+      v[1] = u.y;
+      v[2] = u.z;
+      v[3] = u.w;
+    }
 #pragma unroll
-    for (int j = 0; j < kBinItems; ++j) c[j] = (int)(((j < 4 ? v.x : v.y) >> (8 * (j & 3))) & 0xffu);
+    for (int j = 0; j < kItems; ++j) c[j] = (int)((v[j >> 2] >> (8 * (j & 3))) & 0xffu);
   } else {
 #pragma unroll
-    for (int j = 0; j < kBinItems; ++j) c[j] = i0 + j < n ? (int)w.cls_of[i0 + j] : -1;
+    for (int j = 0; j < kItems; ++j) c[j] = i0 + j < n ? (int)w.cls_of[i0 + j] : -1;
   }
 }
 
+template <int kItems>
 __global__ void __launch_bounds__(kBinThreads) k_bin_count(WfDev w)
 {
   __shared__ uint32_t cnt[kQueues];
   const uint32_t n = w.cnt[w.in_slot];
-  const uint32_t chunks = (n + kBinChunk - 1) / kBinChunk;
+  const uint32_t chunks = (n + bin_chunk(kItems) - 1) / bin_chunk(kItems);
   for (uint32_t k = blockIdx.x; k < chunks; k += gridDim.x) {
     if (threadIdx.x < kQueues) cnt[threadIdx.x] = 0;
     __syncthreads();
-    int c[kBinItems];
-    bin_load(w, n, k, c);
+    int c[kItems];
+    bin_load<kItems>(w, n, k, c);
 #pragma unroll
     for (int q = 0; q < kQueues; ++q) {
       uint32_t v = 0;
 #pragma unroll
-      for (int j = 0; j < kBinItems; ++j) v += c[j] == q;
+      for (int j = 0; j < kItems; ++j) v += c[j] == q;
       for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
       if ((threadIdx.x & 31) == 0 && v) atomicAdd(&cnt[q], v);
     }
@@ -706,11 +724,11 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_count(WfDev w)
 
 // One block of 1024 threads: per class, the exclusive scan of the chunk counts (in place, chunk order)
 // and the class totals (the material queue counts).
-__global__ void __launch_bounds__(1024) k_bin_scan(WfDev w)
+__global__ void __launch_bounds__(1024) k_bin_scan(WfDev w, uint32_t chunk)
 {
   __shared__ uint32_t warp_sum[32];
   const uint32_t n = w.cnt[w.in_slot];
-  const uint32_t chunks = (n + kBinChunk - 1) / kBinChunk;
+  const uint32_t chunks = (n + chunk - 1) / chunk;
   const uint32_t per = (chunks + 1023) / 1024;  // consecutive chunks per thread
   const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
   for (int q = 0; q < kQueues; ++q) {
@@ -749,21 +767,22 @@ __global__ void __launch_bounds__(1024) k_bin_scan(WfDev w)
   }
 }
 
+template <int kItems>
 __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(WfDev w)
 {
   __shared__ uint32_t wtot[kBinWarps][kQueues];
   const uint32_t n = w.cnt[w.in_slot];
-  const uint32_t chunks = (n + kBinChunk - 1) / kBinChunk;
+  const uint32_t chunks = (n + bin_chunk(kItems) - 1) / bin_chunk(kItems);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (uint32_t k = blockIdx.x; k < chunks; k += gridDim.x) {
-    int c[kBinItems];
-    bin_load(w, n, k, c);
+    int c[kItems];
+    bin_load<kItems>(w, n, k, c);
     uint32_t pos[kQueues];
 #pragma unroll
     for (int q = 0; q < kQueues; ++q) {  // exclusive prefix of this thread's count over the warp
       uint32_t v = 0;
 #pragma unroll
-      for (int j = 0; j < kBinItems; ++j) v += c[j] == q;
+      for (int j = 0; j < kItems; ++j) v += c[j] == q;
       uint32_t x = v;
       for (int off = 1; off < 32; off <<= 1) {
         const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
@@ -779,9 +798,9 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(WfDev w)
       for (int ww = 0; ww < wid; ++ww) base += wtot[ww][q];
       pos[q] += base;
     }
-    const uint32_t i0 = k * kBinChunk + threadIdx.x * kBinItems;
+    const uint32_t i0 = k * bin_chunk(kItems) + threadIdx.x * kItems;
 #pragma unroll
-    for (int j = 0; j < kBinItems; ++j) {
+    for (int j = 0; j < kItems; ++j) {
       if (c[j] < 0) continue;
       uint32_t at = 0;
 #pragma unroll
@@ -791,6 +810,15 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_scatter(WfDev w)
     }
     __syncthreads();
   }
+}
+
+// The three binning launches at kItems positions per thread.
+template <int kItems>
+static void launch_binning(const WfDev& w, int grid, cudaStream_t st)
+{
+  k_bin_count<kItems><<<grid, kBinThreads, 0, st>>>(w);
+  k_bin_scan<<<1, 1024, 0, st>>>(w, bin_chunk(kItems));
+  k_bin_scatter<kItems><<<grid, kBinThreads, 0, st>>>(w);
 }
 
 // Adds an unoccluded next-event estimate to the path (kAdj: takes it off R, and adds the albedo
@@ -2150,7 +2178,7 @@ static pt_status ensure_wavefront(Context& c, uint64_t cap)
   if (st == PT_OK) st = wf.q_b.reserve(cap * 4, "queue");
   if (st == PT_OK) st = wf.q_mat.reserve(cap * 4 * kQueues, "material queues");
   if (st == PT_OK) st = wf.cls_of.reserve(cap, "material classes of the queue");
-  if (st == PT_OK) st = wf.bin.reserve(((cap + kBinChunk - 1) / kBinChunk) * kQueues * 4, "material binning counts");
+  if (st == PT_OK) st = wf.bin.reserve(((cap + bin_chunk(kBinItemsMin) - 1) / bin_chunk(kBinItemsMin)) * kQueues * 4, "material binning counts");
   if (st == PT_OK) st = wf.sh_o.reserve(cap * f4, "shadow queue");
   if (st == PT_OK) st = wf.sh_d.reserve(cap * f4, "shadow queue");
   if (st == PT_OK) st = wf.sh_c.reserve(cap * f4, "shadow queue");
@@ -2490,9 +2518,9 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
         k_extend<<<grid_trace, kBlock, 0, c.stream>>>(w);
       }
       if ((st = prof_end()) != PT_OK) return st;
-      k_bin_count<<<grid_bin, kBinThreads, 0, c.stream>>>(w);
-      k_bin_scan<<<1, 1024, 0, c.stream>>>(w);
-      k_bin_scatter<<<grid_bin, kBinThreads, 0, c.stream>>>(w);
+      if (c.opt.bin_items == 4) launch_binning<4>(w, grid_bin, c.stream);
+      else if (c.opt.bin_items == 16) launch_binning<16>(w, grid_bin, c.stream);
+      else launch_binning<8>(w, grid_bin, c.stream);
       count_launch(3);
       if (adjoint) {
         k_shade_miss<true><<<full_wave(k_shade_miss<true>), kBlock, 0, c.stream>>>(w);

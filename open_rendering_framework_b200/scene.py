@@ -820,7 +820,7 @@ class Renderer:
 # ---------------------------------------------------------------- batches (no counterpart in the reference)
 class TuneResult(ctypes.Structure):
     _fields_ = [("extend_mode", ctypes.c_int32), ("refill", ctypes.c_int32), ("max_paths_in_flight", ctypes.c_uint64),
-                ("best_mpaths_per_s", ctypes.c_float), ("trials", ctypes.c_uint32)]
+                ("best_mpaths_per_s", ctypes.c_float), ("trials", ctypes.c_uint32), ("bin_items", ctypes.c_uint32)]
 
 
 class Batch:

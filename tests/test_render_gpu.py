@@ -121,18 +121,19 @@ def test_converged_image_matches_and_is_below_sample_variance():
 @pytest.mark.parametrize("big", [False, True])
 def test_traversal_variants_leave_identical_images(big):
     # the persistent kernels on the 4-wide BVH and on the BVH2, and the one-ray-per-thread kernels,
-    # find the same closest hits and occlusions, so the images are bit-identical
+    # find the same closest hits and occlusions, so the images are bit-identical;
     data = scenes.single_scene(width=24, height=24) if big else small_scene(24, 24)
     imgs = []
-    for opts in ({}, {"bvh4": 0}, {"extend_mode": 0}):
+    # the material binning is a stable partition, the same for every chunk size (sort granularity)
+    for opts in ({}, {"bvh4": 0}, {"extend_mode": 0}, {"bin_items": 4}, {"bin_items": 16}):
         R = sc.Renderer(data)
         for k, v in opts.items():
             nat.call("pt_set_option", R.ctx, k.encode(), v)
         R.render(3)
         imgs.append(R.readback())
         R.close()
-    assert np.array_equal(imgs[0].view(np.uint32), imgs[1].view(np.uint32))
-    assert np.array_equal(imgs[0].view(np.uint32), imgs[2].view(np.uint32))
+    for img in imgs[1:]:
+        assert np.array_equal(imgs[0].view(np.uint32), img.view(np.uint32))
 
 
 def test_render_frames_in_one_call_equal_frame_by_frame():
