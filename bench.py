@@ -1,10 +1,23 @@
-"""Benchmark: Mpath-samples/s of the single-scene wavefront render on one B200 (per GPU replica).
+"""Benchmark: Mpath-samples/s of the single-scene wavefront render on one B200 (per GPU replica), with the
+metric's other two arms -- the 64-scene batch and forward + adjoint -- in the same default line.
 
 Workload (one step, default --workload single_scene): 512 x 512 pixels x 64 camera samples (frames)
 of the procedural single scene (box of 12 diffuse triangles, 81,920-triangle GGX conductor
 icosphere, 20,480-triangle Beckmann dielectric icosphere, 0.25 x 0.25 quad light of radiance 15),
 max depth 8, Russian roulette from depth 3 -- 16,777,216 path samples per step, traced as one
 wavefront launch group.
+
+The default line (single scene, one GPU) also carries `batched` and `fwd_adjoint` objects (the two
+workloads below, each device-timed with its own `e2e`) and, for each arm, the relMSE of its image against
+a 16x-spp render of the same scene (frames after the measured ones, so the two are independent).  Its
+`roofline` is the extend kernel's instruction-issue roofline: warp instructions per traced segment from
+the committed ncu record (profiles/k_extend_single_scene_ncu.csv) times the segments of a live-timed
+render, against one warp instruction per clock per SM sub-partition at the sampled SM clock; the HBM
+view (56 algorithmic bytes per segment) sits beside it.
+
+--workload build: the BVH builders -- the subsurface mesh (327,680 triangles) and the 64 batch meshes,
+host binned SAH vs the device LBVH (option bvh_builder), in ms per million triangles, and the
+single-scene render over each tree.
 
 --workload batched: 64 seeded procedural scenes (icospheres or heightfields of 1e3-5e5 triangles,
 diffuse / GGX / Beckmann / rough-dielectric / dipole materials, 128^2-1024^2 pixels, 4-256 spp,

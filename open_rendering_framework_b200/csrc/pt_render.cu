@@ -1807,10 +1807,8 @@ __global__ void __launch_bounds__(kBlock) k_gather_collect(WfDev w, uint64_t n_p
 // dipole.  The sum times global_coeff / samples is added to the path's radiance, weighted by the
 // throughput at the vertex.  One thread per path: the MD5 stream is one sequential chain.
 //
-// A differentiable forward render also stores each gather's value with the path (adj_G).  kAdj: the
-// same gathers replayed (same MD5 chain) for the gradient of the standard dipole with respect to the
-// material's sigma_a and sigma_s' per channel; the acceptance probability exp_term is detached.
-template <bool kAdj>
+// A differentiable forward render also stores each gather's value with the path (adj_G); the adjoint
+// replays the same gathers in k_gather_adjoint.
 __global__ void __launch_bounds__(kBlock) k_gather(WfDev w, SssDev g, const uint32_t* list)
 {
   const uint32_t n = w.cnt[CNT_GATHER];
@@ -1825,8 +1823,6 @@ __global__ void __launch_bounds__(kBlock) k_gather(WfDev w, SssDev g, const uint
     float4 r4 = w.rad[pid];
     float3 L = ld3(r4);
     const uint64_t gp = S.adj_G ? (uint64_t)(it.first_frame + fl - S.adj_first) * it.pixels + (pid - it.path_begin) % it.pixels : 0;
-    float3 dl = f3s(0.0f);
-    if constexpr (kAdj) dl = ld3(w.adj_a[pid]);
     for (int slot = (int)(rg.w >> META_GSHIFT) - 1; slot >= 0; --slot) {
       size_t at = (size_t)slot * w.cap + pid;
       float4 a = w.g_a[at], b = w.g_b[at];
@@ -1847,35 +1843,7 @@ __global__ void __launch_bounds__(kBlock) k_gather(WfDev w, SssDev g, const uint
       const uint32_t nc = g.pc_cnt[it.set_begin + set_in_item];
       const float chosen = fminf(P.transport.x, fminf(P.transport.y, P.transport.z));
       float3 acc = f3s(0.0f);
-      if constexpr (kAdj) {
-        // standard dipole only (pt_render_adjoint rejects the directional one)
-        float* gr = S.mat_grad[mat];
-        float3 ga = f3s(0.0f), gs = f3s(0.0f);
-        const float scale = m.a.x;
-        const float3 sa = P.absorption, rx = P.reducedExtinction, A = P.A;
-        for (uint32_t k = 0; k < nc; ++k) {
-          float3 pos = ld3(__ldg(g.pc_pos + pb + k));
-          float dist = length(xo - pos);
-          float exp_term = expf(-dist * chosen);
-          if (rnd_md5(t64) < exp_term) {
-            float3 wl = ld3(__ldg(g.pc_wl + pb + k));
-            Dual2 sx = dipole_channel_grad(dist, sa.x, rx.x, A.x, scale);
-            Dual2 sy = dipole_channel_grad(dist, sa.y, rx.y, A.y, scale);
-            Dual2 sz = dipole_channel_grad(dist, sa.z, rx.z, A.z, scale);
-            ga = ga + wl * f3(sx.da, sy.da, sz.da) / exp_term;
-            gs = gs + wl * f3(sx.ds, sy.ds, sz.ds) / exp_term;
-          }
-        }
-        if (gr) {
-          const float3 f = dl * thr * P.global_coeff / (float)S.probe_samples;
-          atomicAdd(gr + 0, f.x * ga.x);
-          atomicAdd(gr + 1, f.y * ga.y);
-          atomicAdd(gr + 2, f.z * ga.z);
-          atomicAdd(gr + 3, f.x * gs.x);
-          atomicAdd(gr + 4, f.y * gs.y);
-          atomicAdd(gr + 5, f.z * gs.z);
-        }
-      } else if (m.model == DIRECTIONAL_DIPOLE) {
+      if (m.model == DIRECTIONAL_DIPOLE) {
         for (uint32_t k = 0; k < nc; ++k) {
           float3 pos = ld3(__ldg(g.pc_pos + pb + k));
           float dist = length(xo - pos);
@@ -1902,17 +1870,173 @@ __global__ void __launch_bounds__(kBlock) k_gather(WfDev w, SssDev g, const uint
           }
         }
       }
-      if constexpr (!kAdj) {
-        float3 contrib = acc * P.global_coeff / (float)S.probe_samples;
-        L = L + thr * contrib;
-        if (S.adj_G) S.adj_G[gp * S.adj_slots + slot] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
-      }
+      const float3 contrib = acc * P.global_coeff / (float)S.probe_samples;
+      L = L + thr * contrib;
+      if (S.adj_G) S.adj_G[gp * S.adj_slots + slot] = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
       pairs += nc;
       ++gathers;
     }
-    if constexpr (!kAdj) w.rad[pid] = make_float4(L.x, L.y, L.z, r4.w);
+    w.rad[pid] = make_float4(L.x, L.y, L.z, r4.w);
     w.rng[pid] = make_uint4(rg.x, t64.x, t64.y, rg.w);
   }
+  if (pairs) atomicAdd(cnt64(w.cnt, CNT_PAIRS), pairs);
+  if (gathers) atomicAdd(cnt64(w.cnt, CNT_GATHERS), gathers);
+}
+
+// The adjoint gathers, warp by warp: lanes walk their paths' gathers and probes (one probe or one gather
+// set-up per step: distance, the detached acceptance test on one MD5 draw -- the same chain as the
+// forward gather), and every accepted pair of a differentiated material goes to the warp's queue in
+// shared memory; whenever 32 pairs are queued, the whole warp evaluates them, one pair per lane, the
+// standard dipole's derivatives with respect to sigma_a and sigma_s' per channel (dipole_channel_grad)
+// times the pair's weight * L / p and its gather's factor (image gradient x throughput x global_coeff /
+// samples), and adds them to the material's gradient buffer (one warp reduction and six atomics when
+// the 32 pairs share a material).  The derivative, the costly part, thus runs on full warps instead of
+// on the lanes that happened to accept a pair.
+struct AdjPair {
+  float dist, p;    // distance to the probe, acceptance probability exp_term
+  uint32_t wl;      // index of the probe's weight * L in pc_wl
+  uint32_t scene;   // the pair's scene in the pass
+  float3 f;         // factor of its gather
+  int mat;
+};
+constexpr int kAdjQueue = 64;  // per warp; at most 31 + 32 entries are held
+
+__device__ __forceinline__ void adj_pairs_eval(const WfDev& w, const SssDev& g, const AdjPair* q, int count, int lane)
+{
+  float3 ga = f3s(0.0f), gs = f3s(0.0f);
+  float* gr = nullptr;
+  if (lane < count) {
+    const AdjPair e = q[lane];
+    const SceneDev& S = w.scenes[e.scene];
+    const ScatDev& P = S.scat[e.mat];
+    const float scale = S.mats[e.mat].a.x;
+    gr = S.mat_grad[e.mat];
+    const float3 wl = ld3(__ldg(g.pc_wl + e.wl));
+    const Dual2 sx = dipole_channel_grad(e.dist, P.absorption.x, P.reducedExtinction.x, P.A.x, scale);
+    const Dual2 sy = dipole_channel_grad(e.dist, P.absorption.y, P.reducedExtinction.y, P.A.y, scale);
+    const Dual2 sz = dipole_channel_grad(e.dist, P.absorption.z, P.reducedExtinction.z, P.A.z, scale);
+    const float3 k = e.f * wl / e.p;
+    ga = k * f3(sx.da, sy.da, sz.da);
+    gs = k * f3(sx.ds, sy.ds, sz.ds);
+  }
+  const unsigned long long g0 = __shfl_sync(0xffffffffu, (unsigned long long)gr, 0);
+  if (__all_sync(0xffffffffu, lane >= count || (unsigned long long)gr == g0)) {
+    float v[6] = {ga.x, ga.y, ga.z, gs.x, gs.y, gs.z};
+#pragma unroll
+    for (int j = 0; j < 6; ++j)
+      for (int off = 16; off; off >>= 1) v[j] += __shfl_xor_sync(0xffffffffu, v[j], off);
+    if (lane == 0 && g0) {
+      float* d = (float*)g0;
+#pragma unroll
+      for (int j = 0; j < 6; ++j) atomicAdd(d + j, v[j]);
+    }
+  } else if (gr) {
+    atomicAdd(gr + 0, ga.x);
+    atomicAdd(gr + 1, ga.y);
+    atomicAdd(gr + 2, ga.z);
+    atomicAdd(gr + 3, gs.x);
+    atomicAdd(gr + 4, gs.y);
+    atomicAdd(gr + 5, gs.z);
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_gather_adjoint(WfDev w, SssDev g, const uint32_t* list)
+{
+  __shared__ AdjPair queue[kWarps][kAdjQueue];
+  const uint32_t n = w.cnt[CNT_GATHER];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  AdjPair* q = queue[wid];
+  int qn = 0;  // warp-uniform
+  unsigned long long pairs = 0, gathers = 0;
+  for (uint32_t base = (blockIdx.x * kWarps + wid) * 32u; base < n; base += gridDim.x * kBlock) {
+    const uint32_t i = base + lane;
+    bool active = i < n;
+    uint32_t pid = 0, scene = 0, fl = 0, pb = 0, nc = 0, k = 0;
+    int slot = -1, mat = 0;
+    const ItemDev* it = nullptr;
+    const SceneDev* S = nullptr;
+    uint4 rg = make_uint4(0, 0, 0, 0);
+    uint2 t64 = make_uint2(0, 0);
+    float3 dl = f3s(0.0f), xo = f3s(0.0f), f = f3s(0.0f);
+    float chosen = 0.0f;
+    bool diff = false;
+    if (active) {
+      pid = list[i];
+      it = &w.items[w.path_item[pid]];
+      scene = it->scene;
+      S = &w.scenes[scene];
+      rg = w.rng[pid];
+      t64 = make_uint2(rg.y, rg.z);
+      fl = (uint32_t)((pid - it->path_begin) / it->pixels);
+      dl = ld3(w.adj_a[pid]);
+      slot = (int)(rg.w >> META_GSHIFT) - 1;
+    }
+    while (__any_sync(0xffffffffu, active)) {
+      bool want = false;
+      AdjPair e;
+      if (active) {
+        if (k >= nc) {  // the next gather of the path (or its end)
+          if (slot < 0) {
+            w.rng[pid] = make_uint4(rg.x, t64.x, t64.y, rg.w);
+            active = false;
+          } else {
+            const size_t at = (size_t)slot * w.cap + pid;
+            const float4 a = w.g_a[at], b = w.g_b[at];
+            const float2 c = w.g_c[at];
+            --slot;
+            mat = __float_as_int(c.y);
+            if (mat < 0) {  // reset marker: the MD5 state the vertex below was entered with
+              t64 = make_uint2(__float_as_uint(a.x), __float_as_uint(a.y));
+            } else {
+              xo = ld3(a);
+              const float3 thr = f3(a.w, b.w, c.x);
+              const MatDev& m = S->mats[mat];
+              const ScatDev& P = S->scat[mat];
+              const uint32_t set_in_item = fl * S->n_trans + m.aux;
+              pb = (uint32_t)(it->probe_begin + (size_t)set_in_item * S->probe_samples);
+              nc = g.pc_cnt[it->set_begin + set_in_item];
+              k = 0;
+              chosen = fminf(P.transport.x, fminf(P.transport.y, P.transport.z));
+              f = dl * thr * P.global_coeff / (float)S->probe_samples;
+              diff = S->mat_grad[mat] != nullptr;
+              pairs += nc;
+              ++gathers;
+            }
+          }
+        } else {  // one probe of the gather
+          const float3 pos = ld3(__ldg(g.pc_pos + pb + k));
+          const float dist = length(xo - pos);
+          const float exp_term = expf(-dist * chosen);
+          if (rnd_md5(t64) < exp_term && diff) {
+            want = true;
+            e.dist = dist;
+            e.p = exp_term;
+            e.wl = pb + k;
+            e.scene = scene;
+            e.f = f;
+            e.mat = mat;
+          }
+          ++k;
+        }
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, want);
+      if (want) q[qn + __popc(m & lanemask_lt())] = e;
+      qn += __popc(m);
+      __syncwarp();
+      if (qn >= 32) {
+        adj_pairs_eval(w, g, q, 32, lane);
+        __syncwarp();
+        const int rest = qn - 32;
+        AdjPair moved;
+        if (lane < rest) moved = q[32 + lane];
+        __syncwarp();
+        if (lane < rest) q[lane] = moved;
+        qn = rest;
+        __syncwarp();
+      }
+    }
+  }
+  if (qn > 0) adj_pairs_eval(w, g, q, qn, lane);
   if (pairs) atomicAdd(cnt64(w.cnt, CNT_PAIRS), pairs);
   if (gathers) atomicAdd(cnt64(w.cnt, CNT_GATHERS), gathers);
 }
@@ -2610,8 +2734,8 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
       uint32_t* list = wf.q_a.as<uint32_t>();
       k_gather_collect<<<grid_for(n_paths, kBlock, 16), kBlock, 0, c.stream>>>(w, n_paths, list);
       if ((st = prof_begin(PROF_GATHER)) != PT_OK) return st;
-      if (adjoint) k_gather<true><<<grid_shade, kBlock, 0, c.stream>>>(w, g, list);
-      else k_gather<false><<<grid_shade, kBlock, 0, c.stream>>>(w, g, list);
+      if (adjoint) k_gather_adjoint<<<grid_shade, kBlock, 0, c.stream>>>(w, g, list);
+      else k_gather<<<grid_shade, kBlock, 0, c.stream>>>(w, g, list);
       if ((st = prof_end()) != PT_OK) return st;
       count_launch(2);
     }
