@@ -813,13 +813,23 @@ def measure_batched(args, world, local, relmse=True):
     }
     if relmse:
         # relMSE of each scene's batched image (frames 0..spp-1, the e2e step's) against its 16x-spp
-        # reference; the plain path renders bit-identical images (tests/test_batch_gpu.py), so its
-        # relMSE on the same frames is the same number
+        # reference, frames [spp, 17 spp): one more batched pass over the same scenes (the scene contexts
+        # hold no wavefront buffers of their own; the batch engine's are shared), each accumulation
+        # cleared with its next frame set to spp (pt_set_accumulation), the running mean rescaled to the
+        # mean of those frames.  The plain path renders bit-identical images (tests/test_batch_gpu.py),
+        # so its relMSE on the same frames is the same number.
         t0 = time.perf_counter()
+        imgs_np = [im.numpy().copy() for im in imgs]
+        B2 = sc.Batch(Rs, [16 * p for p in spp], device=local)
+        for R, p in zip(Rs, spp):
+            zeros = np.zeros((R.data.camera.height, R.data.camera.width, 4), np.float32)
+            nat.call("pt_set_accumulation", R.ctx, zeros.ctypes.data, p)
+        B2.render()
         errs = []
-        for R, im, p in zip(Rs, imgs, spp):
-            ref = reference_image(R, p)
-            errs.append(rel_mse(im.numpy(), ref))
+        for R, im, p in zip(Rs, imgs_np, spp):
+            ref = R.readback().astype(np.float64) * (17.0 / 16.0)
+            errs.append(rel_mse(im, ref))
+        B2.close()
         out["relmse_vs_16x_spp"] = {"mean_over_scenes": float(np.mean(errs)), "max_over_scenes": float(np.max(errs)),
                                     "per_scene": [float(e) for e in errs], "reference": "frames [spp, 17 spp) of each scene",
                                     "plain_same_frames": "identical (bit-identical images)", "seconds": time.perf_counter() - t0}
@@ -858,7 +868,7 @@ ADJOINT = ("inverse rendering 256x256, 64 spp, depth 6, RR from depth 3: 12-tria
            "1024-spp target from other seeded parameters; forward + path-replay adjoint per step")
 
 
-def measure_adjoint(args, local, relmse=True):
+def measure_adjoint(args, local, relmse=True, spp=None, width=None):
     """The differentiable configuration: forward (differentiable) render + path-replay adjoint per
     step, device-timed per phase; the end-to-end figure through the torch.autograd.Function; the
     forward image's relMSE against a 16x-spp reference."""
@@ -869,8 +879,8 @@ def measure_adjoint(args, local, relmse=True):
     from open_rendering_framework_b200 import scenes
 
     torch.cuda.set_device(local)
-    W = 256
-    spp = 64
+    W = width or 256
+    spp = spp or 64
     data, (dif, met, tr) = scenes.inverse_scene(W, W, subdiv=5, tex_res=256, seed=0)
     tdata, _ = scenes.inverse_scene(W, W, subdiv=5, tex_res=256, seed=1)
     T = sc.Renderer(tdata, device=local)
@@ -942,7 +952,7 @@ def measure_adjoint(args, local, relmse=True):
 
 
 def run_adjoint(args, world, rank, local):
-    m = measure_adjoint(args, local)
+    m = measure_adjoint(args, local, spp=args.spp, width=args.width)
     line = {
         "metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": m["warmup"],
         "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",

@@ -275,6 +275,19 @@ bool build_bvh(const float* tri_pos, uint32_t n_tris, BvhHost& out, const BvhPar
   return out.depth < 64;
 }
 
+float scene_diagonal(const float* tri_pos, uint32_t n)
+{
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (size_t i = 0; i < (size_t)n * 3; ++i)
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], tri_pos[3 * i + k]);
+      hi[k] = std::max(hi[k], tri_pos[3 * i + k]);
+    }
+  double d2 = 0.0;
+  for (int k = 0; k < 3; ++k) d2 += (double)(hi[k] - lo[k]) * (hi[k] - lo[k]);
+  return n ? (float)std::sqrt(d2) : 0.0f;
+}
+
 // Collapse: starting from a BVH2 node's two children, the internal child of largest surface area is
 // replaced by its own two children until there are four or no internal child is left (the usual
 // greedy collapse of a binary SAH tree into a wide one).

@@ -34,4 +34,8 @@ bool build_bvh(const float* tri_pos, uint32_t n_tris, BvhHost& out, const BvhPar
 constexpr int kMaxDepth4 = kMaxDepthWide;
 bool build_bvh4(const BvhHost& bvh2, std::vector<float4>& nodes4, int& depth4);
 
+// The diagonal of the bounding box of n triangles (9 floats each): the scale of the box tests' margin
+// (SceneDev::trav_scale).
+float scene_diagonal(const float* tri_pos, uint32_t n);
+
 }  // namespace pt

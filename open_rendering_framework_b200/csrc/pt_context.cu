@@ -17,6 +17,7 @@ SceneDev Context::view() const
   SceneDev s;
   s.nodes = d_nodes.as<float4>();
   s.nodes4 = has_bvh4 && use_bvh4 ? d_nodes4.as<float4>() : nullptr;
+  s.trav_scale = trav_scale;
   s.tri_v0 = d_v0.as<float4>();
   s.tri_e1 = d_e1.as<float4>();
   s.tri_e2 = d_e2.as<float4>();
@@ -682,6 +683,7 @@ pt_status pt_build(pt_ctx* ctx)
   Context& c = ctx->c;
   if (c.n_tris == 0) return fail(PT_NOT_READY, "pt_build: no meshes");
   PT_CHECK_CUDA(cudaSetDevice(c.device), "cudaSetDevice");
+  c.trav_scale = scene_diagonal(c.tri_pos.data(), c.n_tris);
   const auto t0 = std::chrono::steady_clock::now();
   pt_status st = PT_OK;
   bool on_device = false;

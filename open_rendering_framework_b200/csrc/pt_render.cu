@@ -575,8 +575,8 @@ __global__ void __launch_bounds__(kTraceBlock, PT_TRACE_MIN_BLOCKS) k_extend_per
           float4 o4 = w.ray_o[pid], d4 = w.ray_d[pid];
           o = ld3(o4);
           d = ld3(d4);
-          if constexpr (kW4) rp = ray_pre4(o, d);
-          else rp = ray_pre(o, d);
+          if constexpr (kW4) rp = ray_pre4(o, d, g.trav_scale);
+          else rp = ray_pre(o, d, g.trav_scale);
           h.t = kDefaultMax;
           h.u = h.v = 0.0f;
           h.prim = -1;
@@ -884,8 +884,8 @@ __global__ void __launch_bounds__(kTraceBlock, PT_TRACE_MIN_BLOCKS) k_shadow_per
           d = ld3(d4);
           tmin = o4.w;
           tmax = d4.w;
-          if constexpr (kW4) rp = ray_pre4(o, d);
-          else rp = ray_pre(o, d);
+          if constexpr (kW4) rp = ray_pre4(o, d, g.trav_scale);
+          else rp = ray_pre(o, d, g.trav_scale);
           if constexpr (kW4) {
             stack4_init(s4, stk + threadIdx.x, kTraceBlock, spill4);
             cur = 0;

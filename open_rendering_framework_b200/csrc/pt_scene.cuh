@@ -154,6 +154,7 @@ struct IntegratorDev {
 struct SceneDev {
   const float4* nodes;
   const float4* nodes4;  // the wide BVH (kWide children per node, kWideStride float4 each) or null
+  float trav_scale;      // the diagonal of the triangles' bounding box (sizes the box tests' margin)
   const float4* tri_v0;
   const float4* tri_e1;
   const float4* tri_e2;
@@ -201,8 +202,9 @@ struct TravGeom {
   const float4* tri_e1;
   const float4* tri_e2;
   const float4* nodes4;
+  float trav_scale;
 };
-PT_HD TravGeom trav_geom(const SceneDev& S) { return TravGeom{S.nodes, S.tri_v0, S.tri_e1, S.tri_e2, S.nodes4}; }
+PT_HD TravGeom trav_geom(const SceneDev& S) { return TravGeom{S.nodes, S.tri_v0, S.tri_e1, S.tri_e2, S.nodes4, S.trav_scale}; }
 
 struct Ray {
   float3 o, d;
@@ -214,11 +216,25 @@ struct Hit {
 };
 
 // ------------------------------------------------------------------ intersection primitives
+// The box tests only prune: the triangle test alone decides hits, so a box must never be culled when
+// the triangle test reports a hit inside it.  The triangle test rounds too: a ray aimed at a vertex or an
+// edge can be reported to hit a triangle at a point that lies just outside the triangle (a barycentric
+// that is slightly negative rounds to 0), i.e. just outside its box, by a distance of the order of the
+// float spacing of the coordinates and of the distance travelled.  Seen along the ray, that point can
+// lie far before the box's entry distance when the ray runs nearly parallel to the face it crosses
+// (the distance is divided by the direction component).  Every box test therefore widens each slab by a
+// margin in space of 2^-18 (|o_axis| + S) + 2^-40, S the diagonal of the scene's triangles (trav_scale):
+// in distance along the ray that is the margin times |1/d_axis|.  (Observed: a hit 1e-8 outside a face
+// crossed with d.x = 3e-4, 3e-5 before the box's entry distance -- beyond a relative slack of 1e-5.)
+constexpr float kMarginRel = 3.814697265625e-06f;   // 2^-18
+constexpr float kMarginAbs = 9.094947017729282e-13f; // 2^-40
+PT_HD float slab_margin(float o, float inv, float scale) { return (kMarginRel * (fabsf(o) + scale) + kMarginAbs) * fabsf(inv); }
 struct RayPre {
   float3 inv;
   int sx, sy, sz;  // 1 where the direction component is negative: the near slab plane is the box's hi
+  float E;         // the largest per-axis margin along the ray (axes with a finite reciprocal)
 };
-PT_HD RayPre ray_pre(const float3& o, const float3& d)
+PT_HD RayPre ray_pre(const float3& o, const float3& d, float scale)
 {
   // IEEE reciprocals: a zero component gives +-inf, so a slab distance (plane - o) * inv is +-inf, or
   // NaN when the origin lies exactly on the plane; the slab tests take near / far planes by the
@@ -229,21 +245,26 @@ PT_HD RayPre ray_pre(const float3& o, const float3& d)
   r.sx = r.inv.x < 0.0f;
   r.sy = r.inv.y < 0.0f;
   r.sz = r.inv.z < 0.0f;
+  const float inf = as_float(0x7f800000);
+  const float ex = fabsf(r.inv.x) < inf ? slab_margin(o.x, r.inv.x, scale) : 0.0f;
+  const float ey = fabsf(r.inv.y) < inf ? slab_margin(o.y, r.inv.y, scale) : 0.0f;
+  const float ez = fabsf(r.inv.z) < inf ? slab_margin(o.z, r.inv.z, scale) : 0.0f;
+  r.E = fmaxf(fmaxf(ex, ey), ez);
   return r;
 }
-// Slab test of one child box; returns the entry distance, or +inf on a miss.  Each slab distance is
-// (plane - origin) * (1/d): two correctly rounded operations, so its relative error is at most
-// 2 ulp plus the 1 ulp of the reciprocal, and the exit distance is widened by kSlack (>> 3 ulp)
-// before the comparison (the robust slab test of T. Ize, "Robust BVH Ray Traversal", JCGT 2013).
-// The triangle test alone decides hits; boxes only prune, so the widening costs a little culling.
+// Slab test of one child box; returns the (lowered) entry distance, or +inf on a miss.  Each slab
+// distance is (plane - origin) * (1/d): two correctly rounded operations, so its relative error is at
+// most 2 ulp plus the 1 ulp of the reciprocal, which the relative slack kSlack (>> 3 ulp) covers (the
+// robust slab test of T. Ize, "Robust BVH Ray Traversal", JCGT 2013); the margin E widens the interval
+// as described above.
 constexpr float kSlack = 1.00001f;
 PT_HD float slab(float lox, float hix, float loy, float hiy, float loz, float hiz, const float3& o, const RayPre& r, float tmin, float tmax)
 {
   const float tnx = ((r.sx ? hix : lox) - o.x) * r.inv.x, tfx = ((r.sx ? lox : hix) - o.x) * r.inv.x;
   const float tny = ((r.sy ? hiy : loy) - o.y) * r.inv.y, tfy = ((r.sy ? loy : hiy) - o.y) * r.inv.y;
   const float tnz = ((r.sz ? hiz : loz) - o.z) * r.inv.z, tfz = ((r.sz ? loz : hiz) - o.z) * r.inv.z;
-  const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
-  const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax * kSlack));
+  const float tn = fmaxf(fmaxf(fmaxf(tnx, tny), tnz) - r.E, tmin);
+  const float tf = fminf(fminf(fminf(tfx, tfy), tfz) + r.E, tmax * kSlack);
   return tn <= tf * kSlack ? tn : as_float(0x7f800000);
 }
 // Moller-Trumbore (T. Moller, B. Trumbore, "Fast, minimum storage ray-triangle intersection",
@@ -606,15 +627,14 @@ PT_HD void cswap4(int code[4], float t[4], int a, int b)
 // Ray constants of the wide BVH's slab test, which takes one fused multiply-add per plane:
 // t = fma(plane, inv, -o * inv).  The product o * inv is rounded once per ray, an absolute error of
 // at most 2^-24 |o * inv| in every slab distance of that axis (the fma itself rounds once, a relative
-// error that the relative slack kSlack covers as in `slab`).  Each axis therefore carries a margin E
-// >= 16 x that bound: near distances are lowered by E and far distances raised by E (cn = -o*inv - E,
-// cf = -o*inv + E), so the test can only keep more boxes than the exact one.  A direction component of
-// magnitude below 2^-64 (a zero one included) is taken as +-2^-64 so that every constant is finite: the
-// ray then drifts at most 2^-64 t off its line, which the absolute part of E (2^-40 in space, times
-// |inv|) covers for t up to 2^24 -- far beyond any scene, whose other axes bound t.
+// error that the relative slack kSlack covers as in `slab`).  Each axis carries the margin of `slab`,
+// (2^-18 (|o| + S) + 2^-40) |inv| -- more than 16 x that rounding bound as well: near distances are
+// lowered and far distances raised by it (cn = -o*inv - E, cf = -o*inv + E), so the test keeps every box
+// the exact test keeps, and more.  A direction component of magnitude below 2^-64 (a zero one included)
+// is taken as +-2^-64 so that every constant is finite: the ray then drifts at most 2^-64 t off its
+// line, which the absolute part of the margin (2^-40 in space) covers for t up to 2^24 -- far beyond any
+// scene, whose other axes bound t.
 constexpr float kInvMax = 18446744073709551616.0f;  // 2^64
-constexpr float kRelMargin = 9.5367431640625e-07f;  // 2^-20
-constexpr float kAbsMargin = 9.094947017729282e-13f; // 2^-40
 struct RayPre4 {
   float3 inv;     // 1 / d, clamped to +-2^64
   float3 cn, cf;  // per axis: -(o * inv) - E, -(o * inv) + E
@@ -625,14 +645,12 @@ PT_HD float clamp_inv(float d)
   const float r = 1.0f / d;
   return fabsf(r) <= kInvMax ? r : copysignf(kInvMax, d);
 }
-PT_HD RayPre4 ray_pre4(const float3& o, const float3& d)
+PT_HD RayPre4 ray_pre4(const float3& o, const float3& d, float scale)
 {
   RayPre4 r;
   r.inv = f3(clamp_inv(d.x), clamp_inv(d.y), clamp_inv(d.z));
   const float ox = o.x * r.inv.x, oy = o.y * r.inv.y, oz = o.z * r.inv.z;
-  const float ex = fabsf(ox) * kRelMargin + kAbsMargin * fabsf(r.inv.x);
-  const float ey = fabsf(oy) * kRelMargin + kAbsMargin * fabsf(r.inv.y);
-  const float ez = fabsf(oz) * kRelMargin + kAbsMargin * fabsf(r.inv.z);
+  const float ex = slab_margin(o.x, r.inv.x, scale), ey = slab_margin(o.y, r.inv.y, scale), ez = slab_margin(o.z, r.inv.z, scale);
   r.cn = f3(-ox - ex, -oy - ey, -oz - ez);
   r.cf = f3(-ox + ex, -oy + ey, -oz + ez);
   r.sx = r.inv.x < 0.0f;
@@ -793,7 +811,7 @@ template <class G> PT_HD Hit trace_closest(const G& S, const float3& o, const fl
   h.t = tmax;
   h.u = h.v = 0.0f;
   h.prim = -1;
-  RayPre rp = ray_pre(o, d);
+  RayPre rp = ray_pre(o, d, S.trav_scale);
   TravState st;
   trav_init(st);
   while (!trav_step_closest(S, o, d, rp, tmin, h, st)) {}
@@ -802,7 +820,7 @@ template <class G> PT_HD Hit trace_closest(const G& S, const float3& o, const fl
 
 template <class G> PT_HD bool trace_any(const G& S, const float3& o, const float3& d, float tmin, float tmax)
 {
-  RayPre rp = ray_pre(o, d);
+  RayPre rp = ray_pre(o, d, S.trav_scale);
   TravState st;
   trav_init(st);
   int r;

@@ -14,10 +14,8 @@ struct HostScene {
   SceneDev S;
 };
 
-extern "C" __attribute__((visibility("default"))) void* ht_build(const float* tri_pos, unsigned n, int* depth_out)
+static void host_scene_views(HostScene* h, unsigned n)
 {
-  HostScene* h = new HostScene();
-  if (!build_bvh(tri_pos, n, h->bvh)) { delete h; return nullptr; }
   memset(&h->S, 0, sizeof(h->S));
   h->S.nodes = h->bvh.nodes.data();
   h->S.tri_v0 = h->bvh.tri_v0.data();
@@ -26,7 +24,29 @@ extern "C" __attribute__((visibility("default"))) void* ht_build(const float* tr
   h->S.n_tris = n;
   int depth4 = 0;
   if (build_bvh4(h->bvh, h->nodes4, depth4)) h->S.nodes4 = h->nodes4.data();
+}
+
+extern "C" __attribute__((visibility("default"))) void* ht_build(const float* tri_pos, unsigned n, int* depth_out)
+{
+  HostScene* h = new HostScene();
+  if (!build_bvh(tri_pos, n, h->bvh)) { delete h; return nullptr; }
+  host_scene_views(h, n);
+  h->S.trav_scale = scene_diagonal(tri_pos, n);
   if (depth_out) *depth_out = h->bvh.depth;
+  return h;
+}
+// A tree given as child-pair BVH2 nodes and leaf-order triangle records (the device builder's layout,
+// restated on the host by tests/lbvh_host.py), with its 4-wide collapse.
+extern "C" __attribute__((visibility("default"))) void* ht_from_arrays(const float* nodes, unsigned n_nodes, const float* v0, const float* e1,
+                                                                       const float* e2, unsigned n, const float* tri_pos)
+{
+  HostScene* h = new HostScene();
+  h->bvh.nodes.assign((const float4*)nodes, (const float4*)nodes + 4 * (size_t)n_nodes);
+  h->bvh.tri_v0.assign((const float4*)v0, (const float4*)v0 + n);
+  h->bvh.tri_e1.assign((const float4*)e1, (const float4*)e1 + n);
+  h->bvh.tri_e2.assign((const float4*)e2, (const float4*)e2 + n);
+  host_scene_views(h, n);
+  h->S.trav_scale = scene_diagonal(tri_pos, n);
   return h;
 }
 extern "C" __attribute__((visibility("default"))) void ht_free(void* h) { delete (HostScene*)h; }
@@ -40,7 +60,7 @@ extern "C" __attribute__((visibility("default"))) void ht_trace_stack(void* hp, 
     const float* r = rays + 8 * i;
     float3 o = make_float3(r[0], r[1], r[2]), d = make_float3(r[4], r[5], r[6]);
     uint2 stk[kShortStack];
-    RayPre rp = ray_pre(o, d);
+    RayPre rp = ray_pre(o, d, h->S.trav_scale);
     Hit hh;
     hh.t = r[7];
     hh.u = hh.v = 0.0f;
@@ -71,7 +91,7 @@ extern "C" __attribute__((visibility("default"))) int ht_trace4(void* hp, const 
     float3 o = make_float3(r[0], r[1], r[2]), d = make_float3(r[4], r[5], r[6]);
     uint2 ring[kRing4], spill[kSpill4];
     const int stride = 1;
-    RayPre4 rp = ray_pre4(o, d);
+    RayPre4 rp = ray_pre4(o, d, h->S.trav_scale);
     Hit hh;
     hh.t = r[7];
     hh.u = hh.v = 0.0f;

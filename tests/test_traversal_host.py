@@ -38,6 +38,9 @@ def host_lib(request):
     L.ht_trace.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long] + [ctypes.c_void_p] * 4
     L.ht_trace_stack.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long] + [ctypes.c_void_p] * 4
     L.ht_trace4.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long] + [ctypes.c_void_p] * 5
+    L.ht_from_arrays.restype = ctypes.c_void_p
+    L.ht_from_arrays.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint,
+                                 ctypes.c_void_p]
     return L
 
 
@@ -181,3 +184,40 @@ def test_host_traversal_rays_inside_a_box_face_plane(host_lib, plane):
     assert np.array_equal(t4.view(np.uint32), bt.view(np.uint32))
     assert np.array_equal(bary4.view(np.uint32), bb.view(np.uint32))
     assert np.array_equal(anyh4, ba)
+
+
+def test_host_traversal_over_the_device_builders_tree(host_lib):
+    # The device builder's tree (restated by tests/lbvh_host.py) has single-triangle leaves whose boxes end
+    # exactly at shared vertices.  Rays aimed at vertices can be reported by the triangle test to hit
+    # just outside a triangle (a rounded barycentric), before the box's entry distance when the ray runs
+    # nearly parallel to the face it crosses: the box tests' spatial margin keeps those boxes.  Both
+    # traversals (stackless BVH2 and 4-wide) must match brute force bit for bit.
+    import lbvh_host
+    from open_rendering_framework_b200 import scene as sc
+
+    base = scenes.single_scene(width=16, height=16, metal_subdiv=1, glass_subdiv=1)
+    meshes = [m for m in base.meshes if not isinstance(m.material, sc.AreaLightMaterial)]
+    p, i, nrm, ni = scenes.heightfield(40, extent=1.8, y0=-0.6, seed=4)
+    meshes.append(sc.Mesh(p, i, meshes[0].material, nrm, ni))
+    data = sc.SceneData(base.integrator, base.camera, base.background, meshes, base.lights)
+    tp = np.ascontiguousarray(data.flat_triangles()[0], np.float32)
+    nodes, v0, e1, e2 = lbvh_host.build(tp)
+    h = host_lib.ht_from_arrays(oc.fp(np.ascontiguousarray(nodes)), len(nodes), oc.fp(v0), oc.fp(e1), oc.fp(e2), len(tp), oc.fp(tp))
+    O = oc.OracleScene(data)
+    rng = np.random.default_rng(0)
+    for seed in range(6):
+        # random rays plus rays aimed exactly at triangle vertices and edge midpoints
+        rays = edge_and_random_rays(tp, 20000, seed)
+        n = len(rays)
+        bp, bt, bb, ba = O.trace(rays, brute=True)
+        out = [np.empty(n, np.int32), np.empty(n, np.float32), np.empty((n, 2), np.float32), np.empty(n, np.int32)]
+        host_lib.ht_trace(h, oc.fp(rays), n, *[oc.fp(a) for a in out])
+        out4 = [np.empty(n, np.int32), np.empty(n, np.float32), np.empty((n, 2), np.float32), np.empty(n, np.int32)]
+        max_sp = ctypes.c_int()
+        assert host_lib.ht_trace4(h, oc.fp(rays), n, *[oc.fp(a) for a in out4], ctypes.byref(max_sp)) == 0
+        for p_, t_, b_, a_ in (out, out4):
+            assert np.array_equal(p_, bp), (seed, np.flatnonzero(p_ != bp)[:5])
+            assert np.array_equal(t_.view(np.uint32), bt.view(np.uint32))
+            assert np.array_equal(b_.view(np.uint32), bb.view(np.uint32))
+            assert np.array_equal(a_, ba)
+    host_lib.ht_free(h)
