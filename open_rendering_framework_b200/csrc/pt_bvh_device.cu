@@ -361,13 +361,16 @@ __device__ __forceinline__ float kid_area(const Kid& c)
 }
 
 // Pass 7: one level of the 4-wide collapse.  Work item (BVH2 node, wide node index); each internal
-// child gets the next wide index from *wide_count and becomes a work item of the next level.
-__global__ void __launch_bounds__(128) k_collapse_level(const float4* __restrict__ nodes, const int2* __restrict__ work_in, uint32_t n_in,
-                                                        int2* __restrict__ work_out, uint32_t* __restrict__ n_out, uint32_t* __restrict__ wide_count,
-                                                        uint32_t wide_cap, float4* __restrict__ nodes4, uint32_t* __restrict__ overflow)
+// child gets the next wide index from *wide_count and becomes a work item of the next level.  The
+// level's item count is read on the device (*n_in_ptr), so the levels launch back to back; the grid
+// of level L covers min(4^L, n - 1) items, the most that level can hold.
+__global__ void __launch_bounds__(128) k_collapse_level(const float4* __restrict__ nodes, const int2* __restrict__ work_in,
+                                                        const uint32_t* __restrict__ n_in_ptr, int2* __restrict__ work_out,
+                                                        uint32_t* __restrict__ n_out, uint32_t* __restrict__ wide_count, uint32_t wide_cap,
+                                                        float4* __restrict__ nodes4, uint32_t* __restrict__ overflow)
 {
   const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
-  if (w >= n_in) return;
+  if (w >= *n_in_ptr) return;
   const int2 item = work_in[w];
   Kid kids[kWide];
   int nk = 0;
@@ -418,6 +421,44 @@ __global__ void __launch_bounds__(128) k_collapse_level(const float4* __restrict
   if (kWideStride > 7 * kWideRow) nd[7 * kWideRow] = make_float4((float)nk, 0.0f, 0.0f, 0.0f);
 }
 
+// Offsets of the build's temporaries in one scratch allocation (256-byte aligned), kept by the context
+// for later rebuilds.
+struct BuildLayout {
+  size_t tri, blo, bhi, keys_a, keys_b, idx_a, idx_b, hist, cb, child, range, ipar, lpar, leafrec, noderec, visits, collapse, depth, work_a,
+      work_b, counters, total;
+  BuildLayout(uint32_t n, uint32_t nb)
+  {
+    size_t at = 0;
+    auto take = [&](size_t bytes) {
+      const size_t here = at;
+      at += (bytes + 255) & ~(size_t)255;
+      return here;
+    };
+    tri = take((size_t)n * 9 * sizeof(float));
+    blo = take((size_t)n * sizeof(float4));
+    bhi = take((size_t)n * sizeof(float4));
+    keys_a = take((size_t)n * 4);
+    keys_b = take((size_t)n * 4);
+    idx_a = take((size_t)n * 4);
+    idx_b = take((size_t)n * 4);
+    hist = take((size_t)kRadix * nb * 4);
+    cb = take(6 * 4);
+    child = take((size_t)(n - 1) * sizeof(int2));
+    range = take((size_t)(n - 1) * sizeof(int2));
+    ipar = take((size_t)(n - 1) * 4);
+    lpar = take((size_t)n * 4);
+    leafrec = take((size_t)n * sizeof(NodeRec));
+    noderec = take((size_t)(n - 1) * sizeof(NodeRec));
+    visits = take((size_t)(n - 1) * 4);
+    collapse = take((size_t)(n - 1));
+    depth = take(4);
+    work_a = take((size_t)n * sizeof(int2));
+    work_b = take((size_t)n * sizeof(int2));
+    counters = take((size_t)(kMaxDepth4 + 4) * 4);
+    total = at;
+  }
+};
+
 }  // namespace
 
 pt_status build_bvh_device(Context& c)
@@ -426,105 +467,96 @@ pt_status build_bvh_device(Context& c)
   if (n < 2) return fail(PT_INVALID_ARG, "device BVH build: needs at least two triangles");
   if (n >= (1u << 27)) return fail(PT_CAP_EXCEEDED, "device BVH build: more than 2^27 triangles");
   cudaStream_t st = c.stream;
-  PT_CHECK_CUDA(cudaEventRecord(c.ev0, st), "device BVH build");
   const uint32_t nb = (n + kBlock - 1) / kBlock;
-  DevBuf tri, blo, bhi, keys_a, keys_b, idx_a, idx_b, hist, cb, child, ipar, lpar, range, leafrec, noderec, visits, collapse, depth,
-      work_a, work_b, counters;
-  pt_status s = tri.reserve((size_t)n * 9 * sizeof(float), "device BVH build");
-  if (s == PT_OK) s = blo.reserve((size_t)n * sizeof(float4), "device BVH build");
-  if (s == PT_OK) s = bhi.reserve((size_t)n * sizeof(float4), "device BVH build");
-  if (s == PT_OK) s = keys_a.reserve((size_t)n * 4, "device BVH build");
-  if (s == PT_OK) s = keys_b.reserve((size_t)n * 4, "device BVH build");
-  if (s == PT_OK) s = idx_a.reserve((size_t)n * 4, "device BVH build");
-  if (s == PT_OK) s = idx_b.reserve((size_t)n * 4, "device BVH build");
-  if (s == PT_OK) s = hist.reserve((size_t)kRadix * nb * 4, "device BVH build");
-  if (s == PT_OK) s = cb.reserve(6 * 4, "device BVH build");
-  if (s == PT_OK) s = child.reserve((size_t)(n - 1) * sizeof(int2), "device BVH build");
-  if (s == PT_OK) s = range.reserve((size_t)(n - 1) * sizeof(int2), "device BVH build");
-  if (s == PT_OK) s = ipar.reserve((size_t)(n - 1) * 4, "device BVH build");
-  if (s == PT_OK) s = lpar.reserve((size_t)n * 4, "device BVH build");
-  if (s == PT_OK) s = leafrec.reserve((size_t)n * sizeof(NodeRec), "device BVH build");
-  if (s == PT_OK) s = noderec.reserve((size_t)(n - 1) * sizeof(NodeRec), "device BVH build");
-  if (s == PT_OK) s = visits.reserve((size_t)(n - 1) * 4, "device BVH build");
-  if (s == PT_OK) s = collapse.reserve((size_t)(n - 1), "device BVH build");
-  if (s == PT_OK) s = depth.reserve(4, "device BVH build");
-  if (s == PT_OK) s = work_a.reserve((size_t)n * sizeof(int2), "device BVH build");
-  if (s == PT_OK) s = work_b.reserve((size_t)n * sizeof(int2), "device BVH build");
-  if (s == PT_OK) s = counters.reserve(4 * 4, "device BVH build");
+  const BuildLayout Lo(n, nb);
+  pt_status s = c.d_build_scratch.reserve(Lo.total, "device BVH build scratch");
   if (s == PT_OK) s = c.d_nodes.reserve((size_t)(n - 1) * 4 * sizeof(float4), "BVH nodes");
   if (s == PT_OK) s = c.d_nodes4.reserve((size_t)(n - 1) * kWideStride * sizeof(float4), "4-wide BVH nodes");
   if (s == PT_OK) s = c.d_v0.reserve((size_t)n * sizeof(float4), "triangles");
   if (s == PT_OK) s = c.d_e1.reserve((size_t)n * sizeof(float4), "triangles");
   if (s == PT_OK) s = c.d_e2.reserve((size_t)n * sizeof(float4), "triangles");
   if (s != PT_OK) return s;
-  PT_CHECK_CUDA(cudaMemcpyAsync(tri.p, c.tri_pos.data(), (size_t)n * 9 * sizeof(float), cudaMemcpyHostToDevice, st), "device BVH build H2D");
+  char* base = c.d_build_scratch.as<char>();
+  float* tri = (float*)(base + Lo.tri);
+  float4 *blo = (float4*)(base + Lo.blo), *bhi = (float4*)(base + Lo.bhi);
+  uint32_t *keys_a = (uint32_t*)(base + Lo.keys_a), *keys_b = (uint32_t*)(base + Lo.keys_b);
+  uint32_t *idx_a = (uint32_t*)(base + Lo.idx_a), *idx_b = (uint32_t*)(base + Lo.idx_b);
+  uint32_t *hist = (uint32_t*)(base + Lo.hist), *cb = (uint32_t*)(base + Lo.cb);
+  int2 *child = (int2*)(base + Lo.child), *range = (int2*)(base + Lo.range);
+  int *ipar = (int*)(base + Lo.ipar), *lpar = (int*)(base + Lo.lpar);
+  NodeRec *leafrec = (NodeRec*)(base + Lo.leafrec), *noderec = (NodeRec*)(base + Lo.noderec);
+  uint32_t* visits = (uint32_t*)(base + Lo.visits);
+  uint8_t* collapse = (uint8_t*)(base + Lo.collapse);
+  int* depth = (int*)(base + Lo.depth);
+  int2 *work_a = (int2*)(base + Lo.work_a), *work_b = (int2*)(base + Lo.work_b);
+  // counters: [0] wide nodes allocated, [1] overflow, [2 + L] items of collapse level L
+  uint32_t* cnt = (uint32_t*)(base + Lo.counters);
+  PT_CHECK_CUDA(cudaEventRecord(c.ev0, st), "device BVH build");
+  PT_CHECK_CUDA(cudaMemcpyAsync(tri, c.tri_pos.data(), (size_t)n * 9 * sizeof(float), cudaMemcpyHostToDevice, st), "device BVH build H2D");
   const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
-  PT_CHECK_CUDA(cudaMemcpyAsync(cb.p, init, sizeof(init), cudaMemcpyHostToDevice, st), "device BVH build H2D");
-  PT_CHECK_CUDA(cudaMemsetAsync(visits.p, 0, (size_t)(n - 1) * 4, st), "device BVH build");
-  PT_CHECK_CUDA(cudaMemsetAsync(depth.p, 0, 4, st), "device BVH build");
-  PT_CHECK_CUDA(cudaMemsetAsync(counters.p, 0, 16, st), "device BVH build");
+  PT_CHECK_CUDA(cudaMemcpyAsync(cb, init, sizeof(init), cudaMemcpyHostToDevice, st), "device BVH build H2D");
+  PT_CHECK_CUDA(cudaMemsetAsync(visits, 0, (size_t)(n - 1) * 4, st), "device BVH build");
+  PT_CHECK_CUDA(cudaMemsetAsync(depth, 0, 4, st), "device BVH build");
+  // the root: BVH2 node 0 becomes wide node 0, the one item of level 0
+  std::vector<uint32_t> cinit(kMaxDepth4 + 4, 0u);
+  cinit[0] = 1;
+  cinit[2] = 1;
+  PT_CHECK_CUDA(cudaMemcpyAsync(cnt, cinit.data(), cinit.size() * 4, cudaMemcpyHostToDevice, st), "device BVH build H2D");
+  const int2 root = make_int2(0, 0);
+  PT_CHECK_CUDA(cudaMemcpyAsync(work_a, &root, sizeof(root), cudaMemcpyHostToDevice, st), "device BVH build H2D");
   const int g = grid_for(n, kBlock, 8);
-  k_tri_boxes<<<g, kBlock, 0, st>>>(tri.as<float>(), n, blo.as<float4>(), bhi.as<float4>(), cb.as<uint32_t>());
-  k_morton<<<g, kBlock, 0, st>>>(blo.as<float4>(), bhi.as<float4>(), n, cb.as<uint32_t>(), keys_a.as<uint32_t>(), idx_a.as<uint32_t>());
+  k_tri_boxes<<<g, kBlock, 0, st>>>(tri, n, blo, bhi, cb);
+  k_morton<<<g, kBlock, 0, st>>>(blo, bhi, n, cb, keys_a, idx_a);
   count_launch(2);
-  uint32_t *kin = keys_a.as<uint32_t>(), *kout = keys_b.as<uint32_t>(), *vin = idx_a.as<uint32_t>(), *vout = idx_b.as<uint32_t>();
+  uint32_t *kin = keys_a, *kout = keys_b, *vin = idx_a, *vout = idx_b;
   for (int shift = 0; shift < 32; shift += 8) {  // four passes: the sorted keys end in keys_a
-    k_radix_hist<<<nb, kBlock, 0, st>>>(kin, n, shift, hist.as<uint32_t>());
-    k_scan_exclusive<<<1, 1024, 0, st>>>(hist.as<uint32_t>(), kRadix * nb);
-    k_radix_scatter<<<nb, kBlock, 0, st>>>(kin, vin, n, shift, hist.as<uint32_t>(), kout, vout);
+    k_radix_hist<<<nb, kBlock, 0, st>>>(kin, n, shift, hist);
+    k_scan_exclusive<<<1, 1024, 0, st>>>(hist, kRadix * nb);
+    k_radix_scatter<<<nb, kBlock, 0, st>>>(kin, vin, n, shift, hist, kout, vout);
     count_launch(3);
     std::swap(kin, kout);
     std::swap(vin, vout);
   }
   const int gi = (int)((n - 1 + kBlock - 1) / kBlock), gl = (int)nb;
-  k_karras<<<gi, kBlock, 0, st>>>(kin, (int)n, child.as<int2>(), ipar.as<int>(), lpar.as<int>(), range.as<int2>());
-  k_bottom_up<<<gl, kBlock, 0, st>>>((int)n, vin, blo.as<float4>(), bhi.as<float4>(), child.as<int2>(), ipar.as<int>(), lpar.as<int>(),
-                                     leafrec.as<NodeRec>(), noderec.as<NodeRec>(), visits.as<uint32_t>(), collapse.as<uint8_t>(),
-                                     c.bvh_params.trav_cost, c.bvh_params.max_leaf);
-  k_write_bvh2<<<gi, kBlock, 0, st>>>((int)n, child.as<int2>(), ipar.as<int>(), range.as<int2>(), collapse.as<uint8_t>(), leafrec.as<NodeRec>(),
-                                      noderec.as<NodeRec>(), c.d_nodes.as<float4>());
-  k_write_tris<<<gl, kBlock, 0, st>>>((int)n, tri.as<float>(), vin, lpar.as<int>(), ipar.as<int>(), collapse.as<uint8_t>(), c.d_v0.as<float4>(),
-                                      c.d_e1.as<float4>(), c.d_e2.as<float4>(), depth.as<int>());
+  k_karras<<<gi, kBlock, 0, st>>>(kin, (int)n, child, ipar, lpar, range);
+  k_bottom_up<<<gl, kBlock, 0, st>>>((int)n, vin, blo, bhi, child, ipar, lpar, leafrec, noderec, visits, collapse, c.bvh_params.trav_cost,
+                                     c.bvh_params.max_leaf);
+  k_write_bvh2<<<gi, kBlock, 0, st>>>((int)n, child, ipar, range, collapse, leafrec, noderec, c.d_nodes.as<float4>());
+  k_write_tris<<<gl, kBlock, 0, st>>>((int)n, tri, vin, lpar, ipar, collapse, c.d_v0.as<float4>(), c.d_e1.as<float4>(), c.d_e2.as<float4>(),
+                                      depth);
   count_launch(4);
-  PT_CHECK_CUDA(cudaGetLastError(), "device BVH build launch");
-  // 4-wide collapse, level by level (root: BVH2 node 0 -> wide node 0)
-  uint32_t* cnt = counters.as<uint32_t>();  // [0] wide nodes allocated, [1] next level's items, [2] overflow
-  const uint32_t one = 1;
-  const int2 root = make_int2(0, 0);
-  PT_CHECK_CUDA(cudaMemcpyAsync(cnt, &one, 4, cudaMemcpyHostToDevice, st), "device BVH collapse");
-  PT_CHECK_CUDA(cudaMemcpyAsync(work_a.p, &root, sizeof(root), cudaMemcpyHostToDevice, st), "device BVH collapse");
-  int2 *win = work_a.as<int2>(), *wout = work_b.as<int2>();
-  uint32_t n_in = 1;
-  int levels = 0;
-  bool too_deep = false;
-  while (n_in > 0) {
-    if (levels + 1 >= kMaxDepth4) { too_deep = true; break; }  // wide node depth (root = 1) stays below kMaxDepth4
-    PT_CHECK_CUDA(cudaMemsetAsync(cnt + 1, 0, 4, st), "device BVH collapse");
-    k_collapse_level<<<(n_in + 127) / 128, 128, 0, st>>>(c.d_nodes.as<float4>(), win, n_in, wout, cnt + 1, cnt, n - 1, c.d_nodes4.as<float4>(),
-                                                         cnt + 2);
+  // 4-wide collapse: levels 0 .. kMaxDepth4 - 2 (wide depth, root = 1, below kMaxDepth4)
+  int2 *win = work_a, *wout = work_b;
+  uint64_t cap_items = 1;
+  for (int L = 0; L + 1 < kMaxDepth4; ++L) {
+    const uint32_t grid = (uint32_t)((std::min<uint64_t>(cap_items, n - 1) + 127) / 128);
+    k_collapse_level<<<grid, 128, 0, st>>>(c.d_nodes.as<float4>(), win, cnt + 2 + L, wout, cnt + 3 + L, cnt, n - 1, c.d_nodes4.as<float4>(),
+                                           cnt + 1);
     count_launch();
-    ++levels;
-    PT_CHECK_CUDA(cudaMemcpyAsync(&n_in, cnt + 1, 4, cudaMemcpyDeviceToHost, st), "device BVH collapse");
-    PT_CHECK_CUDA(cudaStreamSynchronize(st), "device BVH collapse");
     std::swap(win, wout);
+    cap_items = std::min<uint64_t>(cap_items * 4, (uint64_t)n);
   }
-  uint32_t host_cnt[3] = {0, 0, 0};
+  PT_CHECK_CUDA(cudaGetLastError(), "device BVH build launch");
+  std::vector<uint32_t> host_cnt(kMaxDepth4 + 4, 0u);
   int d2 = 0;
-  PT_CHECK_CUDA(cudaMemcpyAsync(host_cnt, cnt, 12, cudaMemcpyDeviceToHost, st), "device BVH build");
-  PT_CHECK_CUDA(cudaMemcpyAsync(&d2, depth.p, 4, cudaMemcpyDeviceToHost, st), "device BVH build");
+  PT_CHECK_CUDA(cudaMemcpyAsync(host_cnt.data(), cnt, host_cnt.size() * 4, cudaMemcpyDeviceToHost, st), "device BVH build");
+  PT_CHECK_CUDA(cudaMemcpyAsync(&d2, depth, 4, cudaMemcpyDeviceToHost, st), "device BVH build");
   PT_CHECK_CUDA(cudaEventRecord(c.ev1, st), "device BVH build");
   PT_CHECK_CUDA(cudaStreamSynchronize(st), "device BVH build");
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, c.ev0, c.ev1);
   if (d2 >= 64) return fail(PT_CAP_EXCEEDED, "device BVH build: the tree is deeper than the traversal trail allows");
+  int levels = 0;
+  while (levels + 1 < kMaxDepth4 && host_cnt[2 + levels] > 0) ++levels;
+  const bool too_deep = host_cnt[2 + kMaxDepth4 - 1] > 0;  // items left for a level the traversal stack cannot hold
   c.bvh_depth = d2;
-  c.has_bvh4 = !too_deep && host_cnt[2] == 0;
+  c.has_bvh4 = !too_deep && host_cnt[1] == 0;
   c.build_info.builder = 1;
   c.build_info.device_ms = ms;
   c.build_info.bvh2_nodes = n - 1;
   c.build_info.bvh2_depth = (uint32_t)d2;
-  c.build_info.wide_nodes = host_cnt[0];
-  c.build_info.wide_depth = (uint32_t)levels;
+  c.build_info.wide_nodes = c.has_bvh4 ? host_cnt[0] : 0u;
+  c.build_info.wide_depth = c.has_bvh4 ? (uint32_t)levels : 0u;
   return PT_OK;
 }
 

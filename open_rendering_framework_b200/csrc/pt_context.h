@@ -208,6 +208,7 @@ struct Context {
   int bvh_builder = 0;   // option "bvh_builder": 0 host binned SAH, 1 device LBVH
   float trav_scale = 0.0f;  // diagonal of the triangles' bounding box (the box tests' margin), set by pt_build
   pt_build_info build_info{};
+  DevBuf d_build_scratch;  // the device builder's temporaries, kept for rebuilds
   DevBuf d_scat, d_trans_objs, d_trans_pos;
   DevBuf d_scene_tab, d_item_tab;  // scene and item tables of the current pass (this context as the engine)
   bool pass_w4 = false;            // every scene of the current pass has a 4-wide BVH
