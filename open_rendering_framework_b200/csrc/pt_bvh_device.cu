@@ -12,8 +12,8 @@
 //   1. triangle boxes and the centroids' bounds (ordered-integer atomics);
 //   2. 30-bit Morton codes of the centroids in those bounds;
 //   3. a stable least-significant-digit radix sort of (code, triangle) in four 8-bit passes: per-block
-//      digit counts, one exclusive scan over (digit, block), a scatter ranked within each warp by
-//      __match_any_sync;
+//      digit counts stored digit-major, a scan of each digit's row by its own block (the rows' totals
+//      scanned again by every scatter block), a scatter ranked within each warp by __match_any_sync;
 //   4. the Karras hierarchy: internal node i covers a contiguous range of the sorted triangles and
 //      splits it at the highest differing bit (equal codes are ordered by index);
 //   5. bottom-up boxes and SAH costs (the second of a node's two children to finish computes it); a node
@@ -132,37 +132,63 @@ __global__ void __launch_bounds__(kBlock) k_radix_hist(const uint32_t* __restric
   hist[threadIdx.x * gridDim.x + blockIdx.x] = cnt[threadIdx.x];
 }
 
-// Pass 3b: exclusive scan of `total` counts by one block of 1024 threads (contiguous chunks).
-__global__ void __launch_bounds__(1024) k_scan_exclusive(uint32_t* __restrict__ a, uint32_t total)
+// Exclusive scan of one value per thread over the block (kBlock threads): warp shuffles, then the
+// warps' totals from shared memory; *total receives the block's sum.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_tot, uint32_t& total)
 {
-  __shared__ uint32_t part[1024];
-  const uint32_t chunk = (total + 1023) / 1024;
-  const uint32_t b = threadIdx.x * chunk, e = min(total, b + chunk);
-  uint32_t s = 0;
-  for (uint32_t i = b; i < e; ++i) s += a[i];
-  part[threadIdx.x] = s;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+    if (lane >= off) x += y;
+  }
+  if (lane == 31) warp_tot[warp] = x;
   __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {  // inclusive Hillis-Steele scan of the partial sums
-    const uint32_t v = threadIdx.x >= (uint32_t)off ? part[threadIdx.x - off] : 0u;
-    __syncthreads();
-    part[threadIdx.x] += v;
-    __syncthreads();
+  uint32_t before = 0, all = 0;
+#pragma unroll
+  for (int w = 0; w < kWarpsPerBlock; ++w) {
+    const uint32_t t = warp_tot[w];
+    before += w < warp ? t : 0u;
+    all += t;
   }
-  uint32_t run = threadIdx.x ? part[threadIdx.x - 1] : 0u;
-  for (uint32_t i = b; i < e; ++i) {
-    const uint32_t v = a[i];
-    a[i] = run;
-    run += v;
-  }
+  __syncthreads();  // warp_tot may be reused
+  total = all;
+  return before + x - v;
 }
 
-// Pass 3c: stable scatter.  A key's destination is its digit's offset for this block, plus the keys of
-// that digit in earlier warps of the block, plus those in earlier lanes of its warp.
+// Pass 3b: the digit-major counts scanned row by row: block d turns row d (the counts of digit d in
+// blocks 0 .. nb - 1) into its exclusive prefix sums and stores the row's total in row_tot[d].  The
+// scatter adds the exclusive scan of the 256 row totals (the digit's start in the output).
+__global__ void __launch_bounds__(kBlock) k_radix_row_scan(uint32_t* __restrict__ hist, uint32_t nb, uint32_t* __restrict__ row_tot)
+{
+  __shared__ uint32_t wt[kWarpsPerBlock];
+  uint32_t* row = hist + (size_t)blockIdx.x * nb;
+  uint32_t carry = 0;
+  for (uint32_t b = 0; b < nb; b += kBlock) {
+    const uint32_t i = b + threadIdx.x;
+    const uint32_t v = i < nb ? row[i] : 0u;
+    uint32_t tot;
+    const uint32_t ex = block_exclusive_scan(v, wt, tot);
+    if (i < nb) row[i] = carry + ex;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) row_tot[blockIdx.x] = carry;
+}
+
+// Pass 3c: stable scatter.  A key's destination is its digit's start (the exclusive scan of the row
+// totals), plus the keys of that digit in earlier blocks (the row scan), in earlier warps of the block
+// and in earlier lanes of its warp.
+static_assert(kBlock == kRadix, "the scatter scans the kRadix row totals with one value per thread");
 __global__ void __launch_bounds__(kBlock) k_radix_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t n,
-                                                          int shift, const uint32_t* __restrict__ offs, uint32_t* __restrict__ kout,
-                                                          uint32_t* __restrict__ vout)
+                                                          int shift, const uint32_t* __restrict__ offs, const uint32_t* __restrict__ row_tot,
+                                                          uint32_t* __restrict__ kout, uint32_t* __restrict__ vout)
 {
   __shared__ uint32_t wcnt[kWarpsPerBlock][kRadix];
+  __shared__ uint32_t base[kRadix];
+  __shared__ uint32_t wt[kWarpsPerBlock];
+  uint32_t all;
+  base[threadIdx.x] = block_exclusive_scan(row_tot[threadIdx.x], wt, all);
   for (int j = threadIdx.x; j < kWarpsPerBlock * kRadix; j += kBlock) (&wcnt[0][0])[j] = 0;
   __syncthreads();
   const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
@@ -175,7 +201,7 @@ __global__ void __launch_bounds__(kBlock) k_radix_scatter(const uint32_t* __rest
   if (valid && rank == 0) wcnt[warp][digit] = __popc(peers);
   __syncthreads();
   if (!valid) return;
-  uint32_t pos = offs[digit * gridDim.x + blockIdx.x] + rank;
+  uint32_t pos = base[digit] + offs[digit * gridDim.x + blockIdx.x] + rank;
   for (int w = 0; w < warp; ++w) pos += wcnt[w][digit];
   kout[pos] = key;
   vout[pos] = vin[i];
@@ -363,68 +389,70 @@ __device__ __forceinline__ float kid_area(const Kid& c)
 // Pass 7: one level of the 4-wide collapse.  Work item (BVH2 node, wide node index); each internal
 // child gets the next wide index from *wide_count and becomes a work item of the next level.  The
 // level's item count is read on the device (*n_in_ptr), so the levels launch back to back; the grid
-// of level L covers min(4^L, n - 1) items, the most that level can hold.
+// of level L covers min(4^L, n - 1) items, the most that level can hold, up to 8 blocks per SM (the
+// threads stride over the rest).
 __global__ void __launch_bounds__(128) k_collapse_level(const float4* __restrict__ nodes, const int2* __restrict__ work_in,
                                                         const uint32_t* __restrict__ n_in_ptr, int2* __restrict__ work_out,
                                                         uint32_t* __restrict__ n_out, uint32_t* __restrict__ wide_count, uint32_t wide_cap,
                                                         float4* __restrict__ nodes4, uint32_t* __restrict__ overflow)
 {
-  const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
-  if (w >= *n_in_ptr) return;
-  const int2 item = work_in[w];
-  Kid kids[kWide];
-  int nk = 0;
-  kids[nk++] = kid_of(nodes, item.x, 0);
-  kids[nk++] = kid_of(nodes, item.x, 1);
-  while (nk < kWide) {
-    int best = -1;
-    float ba = -1.0f;
-    for (int j = 0; j < nk; ++j)
-      if (kids[j].code >= 0 && kid_area(kids[j]) > ba) { ba = kid_area(kids[j]); best = j; }
-    if (best < 0) break;
-    const int inner = kids[best].code;
-    kids[best] = kid_of(nodes, inner, 0);
-    kids[nk++] = kid_of(nodes, inner, 1);
-  }
-  int codes[kWide];
-  for (int j = 0; j < kWide; ++j) {
-    if (j >= nk) {
-      codes[j] = (int)kEmptyLeaf;
-    } else if (kids[j].code >= 0) {
-      const uint32_t slot = atomicAdd(wide_count, 1u);
-      if (slot >= wide_cap) {
-        atomicAdd(overflow, 1u);
+  const uint32_t n_in = *n_in_ptr;
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < n_in; w += gridDim.x * blockDim.x) {
+    const int2 item = work_in[w];
+    Kid kids[kWide];
+    int nk = 0;
+    kids[nk++] = kid_of(nodes, item.x, 0);
+    kids[nk++] = kid_of(nodes, item.x, 1);
+    while (nk < kWide) {
+      int best = -1;
+      float ba = -1.0f;
+      for (int j = 0; j < nk; ++j)
+        if (kids[j].code >= 0 && kid_area(kids[j]) > ba) { ba = kid_area(kids[j]); best = j; }
+      if (best < 0) break;
+      const int inner = kids[best].code;
+      kids[best] = kid_of(nodes, inner, 0);
+      kids[nk++] = kid_of(nodes, inner, 1);
+    }
+    int codes[kWide];
+    for (int j = 0; j < kWide; ++j) {
+      if (j >= nk) {
         codes[j] = (int)kEmptyLeaf;
+      } else if (kids[j].code >= 0) {
+        const uint32_t slot = atomicAdd(wide_count, 1u);
+        if (slot >= wide_cap) {
+          atomicAdd(overflow, 1u);
+          codes[j] = (int)kEmptyLeaf;
+        } else {
+          codes[j] = (int)slot;
+          work_out[atomicAdd(n_out, 1u)] = make_int2(kids[j].code, (int)slot);
+        }
       } else {
-        codes[j] = (int)slot;
-        work_out[atomicAdd(n_out, 1u)] = make_int2(kids[j].code, (int)slot);
+        codes[j] = kids[j].code;
       }
-    } else {
-      codes[j] = kids[j].code;
     }
+    float4* nd = nodes4 + kWideStride * (size_t)item.y;
+    for (int axis = 0; axis < 3; ++axis)
+      for (int r = 0; r < kWideRow; ++r) {
+        float l[4], h[4];
+        for (int q = 0; q < 4; ++q) {
+          const int j = 4 * r + q;
+          l[q] = j < nk ? kids[j].lo[axis] : 1e30f;
+          h[q] = j < nk ? kids[j].hi[axis] : 1e30f;
+        }
+        nd[(2 * axis) * kWideRow + r] = make_float4(l[0], l[1], l[2], l[3]);
+        nd[(2 * axis + 1) * kWideRow + r] = make_float4(h[0], h[1], h[2], h[3]);
+      }
+    for (int r = 0; r < kWideRow; ++r)
+      nd[6 * kWideRow + r] = make_float4(__int_as_float(codes[4 * r]), __int_as_float(codes[4 * r + 1]), __int_as_float(codes[4 * r + 2]),
+                                         __int_as_float(codes[4 * r + 3]));
+    if (kWideStride > 7 * kWideRow) nd[7 * kWideRow] = make_float4((float)nk, 0.0f, 0.0f, 0.0f);
   }
-  float4* nd = nodes4 + kWideStride * (size_t)item.y;
-  for (int axis = 0; axis < 3; ++axis)
-    for (int r = 0; r < kWideRow; ++r) {
-      float l[4], h[4];
-      for (int q = 0; q < 4; ++q) {
-        const int j = 4 * r + q;
-        l[q] = j < nk ? kids[j].lo[axis] : 1e30f;
-        h[q] = j < nk ? kids[j].hi[axis] : 1e30f;
-      }
-      nd[(2 * axis) * kWideRow + r] = make_float4(l[0], l[1], l[2], l[3]);
-      nd[(2 * axis + 1) * kWideRow + r] = make_float4(h[0], h[1], h[2], h[3]);
-    }
-  for (int r = 0; r < kWideRow; ++r)
-    nd[6 * kWideRow + r] = make_float4(__int_as_float(codes[4 * r]), __int_as_float(codes[4 * r + 1]), __int_as_float(codes[4 * r + 2]),
-                                       __int_as_float(codes[4 * r + 3]));
-  if (kWideStride > 7 * kWideRow) nd[7 * kWideRow] = make_float4((float)nk, 0.0f, 0.0f, 0.0f);
 }
 
 // Offsets of the build's temporaries in one scratch allocation (256-byte aligned), kept by the context
 // for later rebuilds.
 struct BuildLayout {
-  size_t tri, blo, bhi, keys_a, keys_b, idx_a, idx_b, hist, cb, child, range, ipar, lpar, leafrec, noderec, visits, collapse, depth, work_a,
+  size_t tri, blo, bhi, keys_a, keys_b, idx_a, idx_b, hist, rowtot, cb, child, range, ipar, lpar, leafrec, noderec, visits, collapse, depth, work_a,
       work_b, counters, total;
   BuildLayout(uint32_t n, uint32_t nb)
   {
@@ -442,6 +470,7 @@ struct BuildLayout {
     idx_a = take((size_t)n * 4);
     idx_b = take((size_t)n * 4);
     hist = take((size_t)kRadix * nb * 4);
+    rowtot = take((size_t)kRadix * 4);
     cb = take(6 * 4);
     child = take((size_t)(n - 1) * sizeof(int2));
     range = take((size_t)(n - 1) * sizeof(int2));
@@ -481,7 +510,7 @@ pt_status build_bvh_device(Context& c)
   float4 *blo = (float4*)(base + Lo.blo), *bhi = (float4*)(base + Lo.bhi);
   uint32_t *keys_a = (uint32_t*)(base + Lo.keys_a), *keys_b = (uint32_t*)(base + Lo.keys_b);
   uint32_t *idx_a = (uint32_t*)(base + Lo.idx_a), *idx_b = (uint32_t*)(base + Lo.idx_b);
-  uint32_t *hist = (uint32_t*)(base + Lo.hist), *cb = (uint32_t*)(base + Lo.cb);
+  uint32_t *hist = (uint32_t*)(base + Lo.hist), *rowtot = (uint32_t*)(base + Lo.rowtot), *cb = (uint32_t*)(base + Lo.cb);
   int2 *child = (int2*)(base + Lo.child), *range = (int2*)(base + Lo.range);
   int *ipar = (int*)(base + Lo.ipar), *lpar = (int*)(base + Lo.lpar);
   NodeRec *leafrec = (NodeRec*)(base + Lo.leafrec), *noderec = (NodeRec*)(base + Lo.noderec);
@@ -511,8 +540,8 @@ pt_status build_bvh_device(Context& c)
   uint32_t *kin = keys_a, *kout = keys_b, *vin = idx_a, *vout = idx_b;
   for (int shift = 0; shift < 32; shift += 8) {  // four passes: the sorted keys end in keys_a
     k_radix_hist<<<nb, kBlock, 0, st>>>(kin, n, shift, hist);
-    k_scan_exclusive<<<1, 1024, 0, st>>>(hist, kRadix * nb);
-    k_radix_scatter<<<nb, kBlock, 0, st>>>(kin, vin, n, shift, hist, kout, vout);
+    k_radix_row_scan<<<kRadix, kBlock, 0, st>>>(hist, nb, rowtot);
+    k_radix_scatter<<<nb, kBlock, 0, st>>>(kin, vin, n, shift, hist, rowtot, kout, vout);
     count_launch(3);
     std::swap(kin, kout);
     std::swap(vin, vout);
@@ -529,7 +558,7 @@ pt_status build_bvh_device(Context& c)
   int2 *win = work_a, *wout = work_b;
   uint64_t cap_items = 1;
   for (int L = 0; L + 1 < kMaxDepth4; ++L) {
-    const uint32_t grid = (uint32_t)((std::min<uint64_t>(cap_items, n - 1) + 127) / 128);
+    const int grid = grid_for(std::min<uint64_t>(cap_items, n - 1), 128, 8);
     k_collapse_level<<<grid, 128, 0, st>>>(c.d_nodes.as<float4>(), win, cnt + 2 + L, wout, cnt + 3 + L, cnt, n - 1, c.d_nodes4.as<float4>(),
                                            cnt + 1);
     count_launch();
