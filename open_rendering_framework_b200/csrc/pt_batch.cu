@@ -63,6 +63,9 @@ std::vector<uint64_t> graph_key(const Context& E, const PassLayout& L)
   k.push_back(E.wf.cap);
   k.push_back((uint64_t)E.opt.extend_mode);
   k.push_back((uint64_t)E.opt.refill);
+  k.push_back((uint64_t)E.opt.bin_items);
+  k.push_back((uint64_t)E.opt.overlap);
+  k.push_back((uint64_t)E.pass_w4);
   return k;
 }
 

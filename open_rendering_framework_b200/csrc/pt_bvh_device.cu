@@ -72,6 +72,10 @@ __global__ void __launch_bounds__(kBlock) k_tri_boxes(const float* __restrict__ 
     box_lo[i] = make_float4(bl[0], bl[1], bl[2], 0.0f);
     box_hi[i] = make_float4(bh[0], bh[1], bh[2], 0.0f);
   }
+  // warp, then block reduction: one atomic per bound and block
+  __shared__ uint32_t red[6];
+  if (threadIdx.x < 6) red[threadIdx.x] = threadIdx.x < 3 ? 0xffffffffu : 0u;
+  __syncthreads();
   for (int k = 0; k < 3; ++k) {
     for (int off = 16; off > 0; off >>= 1) {
       lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], off));
@@ -80,10 +84,13 @@ __global__ void __launch_bounds__(kBlock) k_tri_boxes(const float* __restrict__ 
   }
   if ((threadIdx.x & 31) == 0) {
     for (int k = 0; k < 3; ++k) {
-      atomicMin(cbounds + k, f2ord(lo[k]));
-      atomicMax(cbounds + 3 + k, f2ord(hi[k]));
+      atomicMin(red + k, f2ord(lo[k]));
+      atomicMax(red + 3 + k, f2ord(hi[k]));
     }
   }
+  __syncthreads();
+  if (threadIdx.x < 3) atomicMin(cbounds + threadIdx.x, red[threadIdx.x]);
+  else if (threadIdx.x < 6) atomicMax(cbounds + threadIdx.x, red[threadIdx.x]);
 }
 
 // 10 bits of x spread to every third bit.

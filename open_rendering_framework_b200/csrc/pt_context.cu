@@ -409,6 +409,10 @@ pt_status pt_context_destroy(pt_ctx* ctx)
     if (ev) cudaEventDestroy(ev);
   for (cudaEvent_t ev : c.prof_events)
     if (ev) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : {c.ev_fork, c.ev_join, c.ev_shade, c.ev_shadow})
+    if (ev) cudaEventDestroy(ev);
+  for (cudaStream_t sd : c.side)
+    if (sd) cudaStreamDestroy(sd);
   cudaStream_t s = c.stream;
   delete ctx;  // frees device buffers
   if (s) cudaStreamDestroy(s);
@@ -911,6 +915,9 @@ pt_status pt_set_option(pt_ctx* ctx, const char* name, int64_t value)
   } else if (k == "bin_items") {
     if (value != 4 && value != 8 && value != 16) return fail(PT_INVALID_ARG, "pt_set_option: bin_items must be 4, 8 or 16");
     ctx->c.opt.bin_items = (int)value;
+  } else if (k == "overlap") {
+    if (value != 0 && value != 1) return fail(PT_INVALID_ARG, "pt_set_option: overlap must be 0 or 1");
+    ctx->c.opt.overlap = (int)value;
   } else {
     return fail(PT_INVALID_ARG, "pt_set_option: unknown option " + k);
   }

@@ -101,8 +101,8 @@ enum CounterSlot {
   CNT_Q_GLASS = 6,
   CNT_Q_TRANS = 7,
   CNT_Q_LAYERED = 8,
-  CNT_SHADOW = 9,
-  CNT_FETCH_EXT = 10,
+  CNT_FETCH_EXT = 9,     // slots 2..9 are reset at the start of each bounce,
+  CNT_SHADOW = 10,       // 10..11 before its shading (the previous bounce's shadow rays may still run)
   CNT_FETCH_SH = 11,
   CNT_GATHER = 12,
   CNT_SEGMENTS_LO = 14,  // 64-bit totals as two words each at even slots (8-byte aligned atomicAdd on unsigned long long)
@@ -168,6 +168,8 @@ struct Options {
   int extend_mode = 1;  // 0: one ray per thread, block-aggregated appends; 1: persistent warps with ray refill
   int refill = 20;      // persistent kernels: refill when at least this many lanes of a warp are idle (1..32)
   int bin_items = 8;    // material binning: queue positions per thread (4, 8 or 16; 256 threads per chunk)
+  int overlap = 1;      // 1: a bounce's shading classes on two streams and its shadow rays beside the next
+                        // bounce's extend and binning; 0: every launch in order on the context stream
 };
 
 struct Context {
@@ -237,6 +239,11 @@ struct Context {
   uint64_t max_paths = 1ull << 24;
 
   Options opt;
+  // the overlapped schedule: side[0] runs the shading kernels of the smaller classes, side[1] the
+  // shadow rays; events fork from and join into `stream` (created by pass_resources, before any
+  // graph capture)
+  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_shade = nullptr, ev_shadow = nullptr;
   bool profile = false;
   std::vector<cudaEvent_t> prof_events;  // pairs around each extend and gather launch when profiling
   std::vector<int> prof_kind;            // PROF_EXTEND or PROF_GATHER per pair

@@ -2509,6 +2509,11 @@ pt_status pass_resources(Context& E, const PassLayout& L, const std::vector<Scen
   if (st != PT_OK) return st;
   E.pass_w4 = true;
   for (const SceneDev& s : scenes) E.pass_w4 = E.pass_w4 && s.nodes4 != nullptr;
+  // the overlapped schedule's streams and events (created here, outside any graph capture)
+  for (cudaStream_t& sd : E.side)
+    if (!sd) PT_CHECK_CUDA(cudaStreamCreateWithFlags(&sd, cudaStreamNonBlocking), "side stream");
+  for (cudaEvent_t* ev : {&E.ev_fork, &E.ev_join, &E.ev_shade, &E.ev_shadow})
+    if (!*ev) PT_CHECK_CUDA(cudaEventCreateWithFlags(ev, cudaEventDisableTiming), "stream event");
   PT_CHECK_CUDA(cudaMemcpyAsync(E.d_scene_tab.p, scenes.data(), scenes.size() * sizeof(SceneDev), cudaMemcpyHostToDevice, E.stream), "scene table");
   PT_CHECK_CUDA(cudaMemcpyAsync(E.d_item_tab.p, L.items.data(), L.items.size() * sizeof(ItemDev), cudaMemcpyHostToDevice, E.stream), "item table");
   return PT_OK;
@@ -2623,11 +2628,28 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
     PT_CHECK_CUDA(cudaMemsetAsync(w.cnt, 0, (CNT_FETCH_SH + 1) * 4, c.stream), "reset queues");
     return PT_OK;
   };
+  // The overlapped schedule (option "overlap", off while profiling so that the extend events time the
+  // extend kernel alone).  A bounce's shading kernels work on disjoint paths and only append to the
+  // next-ray and shadow-ray queues through atomics, so the smaller classes (miss, light, conductor,
+  // dielectric) run on side[0] beside the diffuse, layered and translucent kernels on the context
+  // stream.  The shadow rays of bounce b touch only the shadow queue, the path radiance (and, in the
+  // adjoint, the adjoint state and gradients); the extend and binning of bounce b + 1 touch neither,
+  // so the shadow kernel runs on side[1] beside them, and bounce b + 1's shading, which rewrites the
+  // shadow queue and adds to the radiance, waits for it.  Every path's arithmetic is its own, so the
+  // images do not depend on the schedule.
+  const bool overlap = c.opt.overlap && !prof && c.side[0] && c.side[1];
+  cudaStream_t s_small = overlap ? c.side[0] : c.stream;
+  cudaStream_t s_shadow = overlap ? c.side[1] : c.stream;
+  auto wait_on = [&](cudaStream_t waiter, cudaStream_t from, cudaEvent_t ev) -> pt_status {
+    PT_CHECK_CUDA(cudaEventRecord(ev, from), "stream fork / join");
+    PT_CHECK_CUDA(cudaStreamWaitEvent(waiter, ev, 0), "stream fork / join");
+    return PT_OK;
+  };
   // L.passes = max_depth + 2 bounces: every path has ended by then (each shader stops at max_depth).
   auto bounces = [&](bool adj_pass) -> pt_status {
     const bool adjoint = adj_pass;
     for (int b = 0; b < L.passes; ++b) {
-      PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_Q_MISS, 0, (CNT_FETCH_SH - CNT_Q_MISS + 1) * 4, c.stream), "reset queues");
+      PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_Q_MISS, 0, (CNT_FETCH_EXT - CNT_Q_MISS + 1) * 4, c.stream), "reset queues");
       PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + w.out_slot, 0, 4, c.stream), "reset queues");
       if ((st = prof_begin(PROF_EXTEND)) != PT_OK) return st;
       if (c.opt.extend_mode == 1) {
@@ -2646,27 +2668,31 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
       else if (c.opt.bin_items == 16) launch_binning<16>(w, grid_bin, c.stream);
       else launch_binning<8>(w, grid_bin, c.stream);
       count_launch(3);
+      // the previous bounce's shadow rays are done before this bounce's shading refills their queue
+      if (overlap && b > 0 && (st = wait_on(c.stream, s_shadow, c.ev_shadow)) != PT_OK) return st;
+      PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_SHADOW, 0, (CNT_FETCH_SH - CNT_SHADOW + 1) * 4, c.stream), "reset queues");
+      if (overlap && (st = wait_on(s_small, c.stream, c.ev_fork)) != PT_OK) return st;
       if (adjoint) {
-        k_shade_miss<true><<<full_wave(k_shade_miss<true>), kBlock, 0, c.stream>>>(w);
-        k_shade_light<true><<<full_wave(k_shade_light<true>), kBlock, 0, c.stream>>>(w);
         k_shade_diffuse<true><<<full_wave(k_shade_diffuse<true>), kBlock, 0, c.stream>>>(w);
+        k_shade_miss<true><<<full_wave(k_shade_miss<true>), kBlock, 0, s_small>>>(w);
+        k_shade_light<true><<<full_wave(k_shade_light<true>), kBlock, 0, s_small>>>(w);
         if (L.ms) {
-          k_shade_metal<true, true><<<full_wave(k_shade_metal<true, true>), kBlock, 0, c.stream>>>(w);
-          k_shade_glass<true, true><<<full_wave(k_shade_glass<true, true>), kBlock, 0, c.stream>>>(w);
+          k_shade_metal<true, true><<<full_wave(k_shade_metal<true, true>), kBlock, 0, s_small>>>(w);
+          k_shade_glass<true, true><<<full_wave(k_shade_glass<true, true>), kBlock, 0, s_small>>>(w);
         } else {
-          k_shade_metal<true, false><<<full_wave(k_shade_metal<true, false>), kBlock, 0, c.stream>>>(w);
-          k_shade_glass<true, false><<<full_wave(k_shade_glass<true, false>), kBlock, 0, c.stream>>>(w);
+          k_shade_metal<true, false><<<full_wave(k_shade_metal<true, false>), kBlock, 0, s_small>>>(w);
+          k_shade_glass<true, false><<<full_wave(k_shade_glass<true, false>), kBlock, 0, s_small>>>(w);
         }
       } else {
-        k_shade_miss<false><<<full_wave(k_shade_miss<false>), kBlock, 0, c.stream>>>(w);
-        k_shade_light<false><<<full_wave(k_shade_light<false>), kBlock, 0, c.stream>>>(w);
         k_shade_diffuse<false><<<full_wave(k_shade_diffuse<false>), kBlock, 0, c.stream>>>(w);
+        k_shade_miss<false><<<full_wave(k_shade_miss<false>), kBlock, 0, s_small>>>(w);
+        k_shade_light<false><<<full_wave(k_shade_light<false>), kBlock, 0, s_small>>>(w);
         if (L.ms) {
-          k_shade_metal<false, true><<<full_wave(k_shade_metal<false, true>), kBlock, 0, c.stream>>>(w);
-          k_shade_glass<false, true><<<full_wave(k_shade_glass<false, true>), kBlock, 0, c.stream>>>(w);
+          k_shade_metal<false, true><<<full_wave(k_shade_metal<false, true>), kBlock, 0, s_small>>>(w);
+          k_shade_glass<false, true><<<full_wave(k_shade_glass<false, true>), kBlock, 0, s_small>>>(w);
         } else {
-          k_shade_metal<false, false><<<full_wave(k_shade_metal<false, false>), kBlock, 0, c.stream>>>(w);
-          k_shade_glass<false, false><<<full_wave(k_shade_glass<false, false>), kBlock, 0, c.stream>>>(w);
+          k_shade_metal<false, false><<<full_wave(k_shade_metal<false, false>), kBlock, 0, s_small>>>(w);
+          k_shade_glass<false, false><<<full_wave(k_shade_glass<false, false>), kBlock, 0, s_small>>>(w);
         }
       }
       count_launch(6);
@@ -2680,27 +2706,34 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
         else k_shade_translucent<false><<<full_wave(k_shade_translucent<false>), kBlock, 0, c.stream>>>(w);
         count_launch();
       }
+      if (overlap) {
+        // join the smaller classes, then fork the shadow rays off the joined stream
+        if ((st = wait_on(c.stream, s_small, c.ev_join)) != PT_OK) return st;
+        if ((st = wait_on(s_shadow, c.stream, c.ev_shade)) != PT_OK) return st;
+      }
       if (c.opt.extend_mode == 1) {
         if (w4) {
-          if (multi && adjoint) k_shadow_persistent<true, true, true><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-          else if (multi) k_shadow_persistent<true, false, true><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-          else if (adjoint) k_shadow_persistent<false, true, true><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-          else k_shadow_persistent<false, false, true><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          if (multi && adjoint) k_shadow_persistent<true, true, true><<<grid_persist, kTraceBlock, 0, s_shadow>>>(S0, w, c.opt.refill);
+          else if (multi) k_shadow_persistent<true, false, true><<<grid_persist, kTraceBlock, 0, s_shadow>>>(S0, w, c.opt.refill);
+          else if (adjoint) k_shadow_persistent<false, true, true><<<grid_persist, kTraceBlock, 0, s_shadow>>>(S0, w, c.opt.refill);
+          else k_shadow_persistent<false, false, true><<<grid_persist, kTraceBlock, 0, s_shadow>>>(S0, w, c.opt.refill);
         } else {
-          if (multi && adjoint) k_shadow_persistent<true, true, false><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-          else if (multi) k_shadow_persistent<true, false, false><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-          else if (adjoint) k_shadow_persistent<false, true, false><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-          else k_shadow_persistent<false, false, false><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          if (multi && adjoint) k_shadow_persistent<true, true, false><<<grid_persist, kTraceBlock, 0, s_shadow>>>(S0, w, c.opt.refill);
+          else if (multi) k_shadow_persistent<true, false, false><<<grid_persist, kTraceBlock, 0, s_shadow>>>(S0, w, c.opt.refill);
+          else if (adjoint) k_shadow_persistent<false, true, false><<<grid_persist, kTraceBlock, 0, s_shadow>>>(S0, w, c.opt.refill);
+          else k_shadow_persistent<false, false, false><<<grid_persist, kTraceBlock, 0, s_shadow>>>(S0, w, c.opt.refill);
         }
       } else {
-        if (adjoint) k_shadow<true><<<grid_trace, kBlock, 0, c.stream>>>(w);
-        else k_shadow<false><<<grid_trace, kBlock, 0, c.stream>>>(w);
+        if (adjoint) k_shadow<true><<<grid_trace, kBlock, 0, s_shadow>>>(w);
+        else k_shadow<false><<<grid_trace, kBlock, 0, s_shadow>>>(w);
       }
       count_launch();
       ++c.stats.extend_launches;
       std::swap(w.q_in, w.q_out);
       std::swap(w.in_slot, w.out_slot);
     }
+    // the last bounce's shadow rays join the context stream before anything reads the radiance
+    if (overlap && (st = wait_on(c.stream, s_shadow, c.ev_shadow)) != PT_OK) return st;
     return PT_OK;
   };
   const ItemDev* items = c.d_item_tab.as<ItemDev>();

@@ -729,6 +729,10 @@ class Renderer:
             nat.call("pt_set_option", self.ctx, name.encode(), int(value))
         nat.call("pt_build", self.ctx)
 
+    def set_option(self, name, value):
+        """A launch option or mode of pt_set_option (e.g. "overlap", "refill", "bin_items")."""
+        nat.call("pt_set_option", self.ctx, name.encode(), int(value))
+
     def build_info(self):
         """pt_build_info of the last build (SAH cost included)."""
         b = BuildInfo()

@@ -2,7 +2,9 @@
 
 A batched render of frames [f, f+n) of a scene must leave exactly the image pt_render_frames(ctx, f,
 n) leaves -- the same kernels on the same seeds, only the path-id layout differs -- so every check
-here is bit-exact against the scenes rendered one by one.
+here is bit-exact against the scenes rendered one by one (those with every launch in order on one
+stream, the batch with its shading classes and shadow rays overlapped on two more streams, inside the
+captured graph too).
 """
 import numpy as np
 import pytest
@@ -37,6 +39,7 @@ def test_batched_render_equals_scene_by_scene(use_graph):
     solo = []
     for data, spp, _ in S:
         R = sc.Renderer(data)
+        R.set_option("overlap", 0)  # the in-order schedule; the batch engine overlaps (the default)
         R.render(spp)
         R.render(spp)
         solo.append(R.readback())

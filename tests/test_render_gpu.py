@@ -124,8 +124,9 @@ def test_traversal_variants_leave_identical_images(big):
     # find the same closest hits and occlusions, so the images are bit-identical;
     data = scenes.single_scene(width=24, height=24) if big else small_scene(24, 24)
     imgs = []
-    # the material binning is a stable partition, the same for every chunk size (sort granularity)
-    for opts in ({}, {"bvh4": 0}, {"extend_mode": 0}, {"bin_items": 4}, {"bin_items": 16}):
+    # the material binning is a stable partition, the same for every chunk size (sort granularity);
+    # every path's arithmetic is its own, so the overlapped and the in-order schedules agree
+    for opts in ({}, {"bvh4": 0}, {"extend_mode": 0}, {"bin_items": 4}, {"bin_items": 16}, {"overlap": 0}):
         R = sc.Renderer(data)
         for k, v in opts.items():
             nat.call("pt_set_option", R.ctx, k.encode(), v)

@@ -144,8 +144,14 @@ def test_frame_grouping_does_not_change_the_image():
         B.renderScene()
     b = B.readback()
     assert np.array_equal(bits(a), bits(b))
+    # the in-order schedule (probe pass, camera paths and gathers) leaves the same image
+    C = sc.Renderer(data)
+    C.set_option("overlap", 0)
+    C.render(4)
+    assert np.array_equal(bits(a), bits(C.readback()))
     A.close()
     B.close()
+    C.close()
 
 
 def test_material_update_and_probe_count_validation():
