@@ -470,6 +470,8 @@ def run_bsdf(args, world, rank, local):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = bsdf_cpu_sample(n)
+        one = bsdf_cpu_sample(n, target_s=2.0, threads=1)
+        line["cpu_baseline"]["one_core"] = {"value": one["value"], "unit": one["unit"], "sample": one["sample"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
 

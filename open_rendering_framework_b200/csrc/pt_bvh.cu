@@ -11,6 +11,8 @@
 // the depth stays below the traversal's 64-level trail.  Subtrees with more than 32k triangles are
 // built on separate host threads.
 #include <algorithm>
+#include <array>
+#include <limits>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -288,10 +290,19 @@ float scene_diagonal(const float* tri_pos, uint32_t n)
   return n ? (float)std::sqrt(d2) : 0.0f;
 }
 
-// Collapse: starting from a BVH2 node's two children, the internal child of largest surface area is
-// replaced by its own two children until there are four or no internal child is left (the usual
-// greedy collapse of a binary SAH tree into a wide one).
-bool build_bvh4(const BvhHost& b2, std::vector<float4>& out4, int& depth4)
+// Collapse of the BVH2 into the wide layout over the same leaves.
+//  * collapse 0 (greedy): starting from a BVH2 node's two children, the internal child of largest
+//    surface area is replaced by its own two children until there are four or no internal child is
+//    left (the usual greedy collapse of a binary SAH tree into a wide one).
+//  * collapse 1 (SAH-optimal over the given BVH2): a dynamic program over the BVH2 picks, for every wide
+//    node, which BVH2 nodes below it become its up to four children, minimising the SAH cost
+//    sum(wide nodes) wide_cost * A + sum(leaves) A * triangles, the BVH2's leaves kept as they are (the
+//    cost model of H. Ylitie, T. Karras, S. Laine, "Efficient Incoherent Ray Traversal on GPUs Through
+//    Compressed Wide BVHs", HPG 2017, for 4 children and fixed leaves):
+//      W(x)    = wide_cost * A(x) + D(x, 4)                   x as the root of a wide node
+//      D(x, j) = min_{k=1..j-1} S(left(x), k) + S(right(x), j - k)   x's children in at most j slots
+//      S(y, 1) = leaf cost, or W(y);  S(y, i >= 2) = min(S(y, 1), D(y, i))   y in at most i slots
+bool build_bvh4(const BvhHost& b2, std::vector<float4>& out4, int& depth4, const BvhParams& params)
 {
   out4.clear();
   depth4 = 0;
@@ -316,12 +327,99 @@ bool build_bvh4(const BvhHost& b2, std::vector<float4>& out4, int& depth4)
     for (int k = 0; k < 3; ++k) d[k] = std::max(0.0f, c.hi[k] - c.lo[k]);
     return d[0] * d[1] + d[1] * d[2] + d[2] * d[0];
   };
-  bool ok = true;
-  std::function<int(int, int)> build = [&](int n2, int depth) -> int {
-    depth4 = std::max(depth4, depth);
-    if (depth >= kMaxDepth4) ok = false;
-    Kid kids[kWide];
+  const size_t n_nodes = b2.nodes.size() / 4;
+  // SAH-optimal choices: per BVH2 node y and slot budget i (1..4), choice[y][i] = 0 for "y in one slot
+  // (its own wide node)", else the slots k given to y's first child when y is opened (i - k to the
+  // second); wsplit[x] the split of W(x)'s four slots.
+  std::vector<std::array<uint8_t, kWide + 1>> choice;
+  std::vector<uint8_t> wsplit;
+  if (params.collapse == 1 && n_nodes > 0) {
+    choice.assign(n_nodes, {});
+    wsplit.assign(n_nodes, 1);
+    std::vector<std::array<double, kWide + 1>> S(n_nodes);
+    std::vector<double> A(n_nodes, 0.0);
+    const double inf = std::numeric_limits<double>::infinity();
+    // children before parents: a reverse pre-order of the BVH2
+    std::vector<int> order;
+    order.reserve(n_nodes);
+    std::vector<int> todo{0};
+    while (!todo.empty()) {
+      const int x = todo.back();
+      todo.pop_back();
+      order.push_back(x);
+      for (int k = 0; k < 2; ++k) {
+        const Kid c = kid(x, k);
+        if (c.code >= 0) {
+          A[c.code] = area(c);
+          todo.push_back(c.code);
+        }
+      }
+    }
+    {
+      const Kid a = kid(0, 0), b = kid(0, 1);
+      Kid u = a;
+      for (int k = 0; k < 3; ++k) {
+        u.lo[k] = std::min(a.lo[k], b.lo[k]);
+        u.hi[k] = std::max(a.hi[k], b.hi[k]);
+      }
+      A[0] = area(u);
+    }
+    auto slot_cost = [&](const Kid& c, int i) -> double {  // S(c, i)
+      if (c.code >= 0) return S[c.code][i];
+      const double count = (double)((uint32_t)c.code & 15u);
+      return (double)area(c) * count;
+    };
+    auto dist = [&](int x, int j, int& best_k) -> double {  // D(x, j)
+      const Kid l = kid(x, 0), r = kid(x, 1);
+      double best = inf;
+      best_k = 1;
+      for (int k = 1; k < j; ++k) {
+        const double c = slot_cost(l, k) + slot_cost(r, j - k);
+        if (c < best) {
+          best = c;
+          best_k = k;
+        }
+      }
+      return best;
+    };
+    for (auto it = order.rbegin(); it != order.rend(); ++it) {
+      const int x = *it;
+      int k4 = 1;
+      const double w = (double)params.wide_cost * A[x] + dist(x, kWide, k4);
+      wsplit[x] = (uint8_t)k4;
+      S[x][1] = w;
+      choice[x][1] = 0;
+      for (int i = 2; i <= kWide; ++i) {
+        int k = 1;
+        const double d = dist(x, i, k);
+        if (d < w) {
+          S[x][i] = d;
+          choice[x][i] = (uint8_t)k;
+        } else {
+          S[x][i] = w;
+          choice[x][i] = 0;
+        }
+      }
+    }
+  }
+  // the children (BVH2 nodes or leaves) of the wide node rooted at BVH2 node n2
+  auto children = [&](int n2, Kid* kids) -> int {
     int nk = 0;
+    if (params.collapse == 1) {
+      std::function<void(const Kid&, int)> place = [&](const Kid& c, int slots) {
+        if (c.code < 0 || choice[c.code][slots] == 0) {
+          kids[nk++] = c;
+          return;
+        }
+        const int k = choice[c.code][slots];
+        place(kid(c.code, 0), k);
+        place(kid(c.code, 1), slots - k);
+      };
+      const int k = wsplit[n2];
+      place(kid(n2, 0), k);
+      place(kid(n2, 1), kWide - k);
+      return nk;
+    }
     kids[nk++] = kid(n2, 0);
     kids[nk++] = kid(n2, 1);
     while (nk < kWide) {  // open the internal child of largest surface area
@@ -334,6 +432,14 @@ bool build_bvh4(const BvhHost& b2, std::vector<float4>& out4, int& depth4)
       kids[best] = kid(inner, 0);
       kids[nk++] = kid(inner, 1);
     }
+    return nk;
+  };
+  bool ok = true;
+  std::function<int(int, int)> build = [&](int n2, int depth) -> int {
+    depth4 = std::max(depth4, depth);
+    if (depth >= kMaxDepth4) ok = false;
+    Kid kids[kWide];
+    const int nk = children(n2, kids);
     const int me = (int)(out4.size() / kWideStride);
     out4.resize(out4.size() + kWideStride, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
     int codes[kWide];

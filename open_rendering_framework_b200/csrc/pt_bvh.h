@@ -21,6 +21,8 @@ struct BvhHost {
 struct BvhParams {
   float trav_cost = 1.2f;
   int max_leaf = 8;
+  int collapse = 1;         // 4-wide collapse: 0 greedy (largest area opened first), 1 SAH-optimal
+  float wide_cost = 1.5f;   // SAH cost of a wide node visit relative to one triangle test (collapse 1)
 };
 
 // tri_pos: 9 floats per triangle (v0, v1, v2).  Returns false if the scene is too large for the
@@ -32,7 +34,7 @@ bool build_bvh(const float* tri_pos, uint32_t n_tris, BvhHost& out, const BvhPar
 // when the wide tree would be deeper than kMaxDepthWide levels, whose pending children the traversal
 // stack could not hold.
 constexpr int kMaxDepth4 = kMaxDepthWide;
-bool build_bvh4(const BvhHost& bvh2, std::vector<float4>& nodes4, int& depth4);
+bool build_bvh4(const BvhHost& bvh2, std::vector<float4>& nodes4, int& depth4, const BvhParams& params = BvhParams());
 
 // The diagonal of the bounding box of n triangles (9 floats each): the scale of the box tests' margin
 // (SceneDev::trav_scale).

@@ -704,7 +704,7 @@ pt_status pt_build(pt_ctx* ctx)
     c.bvh_depth = bvh.depth;
     std::vector<float4> nodes4;
     int depth4 = 0;
-    c.has_bvh4 = build_bvh4(bvh, nodes4, depth4);
+    c.has_bvh4 = build_bvh4(bvh, nodes4, depth4, c.bvh_params);
     st = upload(c.d_nodes, bvh.nodes, c.stream, "BVH nodes");
     if (st == PT_OK && c.has_bvh4) st = upload(c.d_nodes4, nodes4, c.stream, "4-wide BVH nodes");
     if (st == PT_OK) st = upload(c.d_v0, bvh.tri_v0, c.stream, "triangles");
@@ -894,6 +894,16 @@ pt_status pt_set_option(pt_ctx* ctx, const char* name, int64_t value)
   if (k == "bvh_max_leaf") {  // largest SAH leaf (default 8), for the next pt_build
     if (value < 1 || value > 15) return fail(PT_INVALID_ARG, "pt_set_option: bvh_max_leaf must be in [1, 15]");
     ctx->c.bvh_params.max_leaf = (int)value;
+    return PT_OK;
+  }
+  if (k == "bvh_collapse") {  // host builder's 4-wide collapse: 0 greedy, 1 SAH-optimal (default); next pt_build
+    if (value != 0 && value != 1) return fail(PT_INVALID_ARG, "pt_set_option: bvh_collapse must be 0 or 1");
+    ctx->c.bvh_params.collapse = (int)value;
+    return PT_OK;
+  }
+  if (k == "bvh_wide_cost_milli") {  // SAH cost of a wide node visit x 1000 (default 1500), for the next pt_build
+    if (value < 100 || value > 20000) return fail(PT_INVALID_ARG, "pt_set_option: bvh_wide_cost_milli must be in [100, 20000]");
+    ctx->c.bvh_params.wide_cost = (float)value / 1000.0f;
     return PT_OK;
   }
   if (k == "bvh_builder") {

@@ -14,7 +14,7 @@ struct HostScene {
   SceneDev S;
 };
 
-static void host_scene_views(HostScene* h, unsigned n)
+static void host_scene_views(HostScene* h, unsigned n, const BvhParams& params = BvhParams())
 {
   memset(&h->S, 0, sizeof(h->S));
   h->S.nodes = h->bvh.nodes.data();
@@ -23,7 +23,7 @@ static void host_scene_views(HostScene* h, unsigned n)
   h->S.tri_e2 = h->bvh.tri_e2.data();
   h->S.n_tris = n;
   int depth4 = 0;
-  if (build_bvh4(h->bvh, h->nodes4, depth4)) h->S.nodes4 = h->nodes4.data();
+  if (build_bvh4(h->bvh, h->nodes4, depth4, params)) h->S.nodes4 = h->nodes4.data();
 }
 
 extern "C" __attribute__((visibility("default"))) void* ht_build(const float* tri_pos, unsigned n, int* depth_out)
@@ -35,8 +35,22 @@ extern "C" __attribute__((visibility("default"))) void* ht_build(const float* tr
   if (depth_out) *depth_out = h->bvh.depth;
   return h;
 }
+// The same with the 4-wide collapse chosen (0 greedy, 1 SAH-optimal) and its wide-node cost.
+extern "C" __attribute__((visibility("default"))) void* ht_build_collapse(const float* tri_pos, unsigned n, int collapse, float wide_cost,
+                                                                          unsigned* wide_nodes)
+{
+  HostScene* h = new HostScene();
+  BvhParams params;
+  params.collapse = collapse;
+  params.wide_cost = wide_cost;
+  if (!build_bvh(tri_pos, n, h->bvh, params)) { delete h; return nullptr; }
+  host_scene_views(h, n, params);
+  h->S.trav_scale = scene_diagonal(tri_pos, n);
+  if (wide_nodes) *wide_nodes = (unsigned)(h->nodes4.size() / kWideStride);
+  return h;
+}
 // A tree given as child-pair BVH2 nodes and leaf-order triangle records (the device builder's layout,
-// restated on the host by tests/lbvh_host.py), with its 4-wide collapse.
+// restated on the host by tests/lbvh_host.py), with its 4-wide collapse (greedy, as on the device).
 extern "C" __attribute__((visibility("default"))) void* ht_from_arrays(const float* nodes, unsigned n_nodes, const float* v0, const float* e1,
                                                                        const float* e2, unsigned n, const float* tri_pos)
 {
@@ -45,7 +59,9 @@ extern "C" __attribute__((visibility("default"))) void* ht_from_arrays(const flo
   h->bvh.tri_v0.assign((const float4*)v0, (const float4*)v0 + n);
   h->bvh.tri_e1.assign((const float4*)e1, (const float4*)e1 + n);
   h->bvh.tri_e2.assign((const float4*)e2, (const float4*)e2 + n);
-  host_scene_views(h, n);
+  BvhParams greedy;  // the device builder's collapse rule
+  greedy.collapse = 0;
+  host_scene_views(h, n, greedy);
   h->S.trav_scale = scene_diagonal(tri_pos, n);
   return h;
 }

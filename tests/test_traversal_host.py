@@ -38,6 +38,8 @@ def host_lib(request):
     L.ht_trace.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long] + [ctypes.c_void_p] * 4
     L.ht_trace_stack.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long] + [ctypes.c_void_p] * 4
     L.ht_trace4.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long] + [ctypes.c_void_p] * 5
+    L.ht_build_collapse.restype = ctypes.c_void_p
+    L.ht_build_collapse.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_int, ctypes.c_float, ctypes.c_void_p]
     L.ht_from_arrays.restype = ctypes.c_void_p
     L.ht_from_arrays.argtypes = [ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint,
                                  ctypes.c_void_p]
@@ -88,6 +90,31 @@ def test_host_traversal_matches_brute_force(host_lib, subdiv):
         assert np.array_equal(t_.view(np.uint32), bt.view(np.uint32))
         assert np.array_equal(b_.view(np.uint32), bb.view(np.uint32))
         assert np.array_equal(a_, ba)
+
+
+@pytest.mark.parametrize("wide_cost", [0.5, 1.5, 4.0])
+def test_sah_optimal_collapse_matches_brute_force(host_lib, wide_cost):
+    """The 4-wide tree of the SAH-optimal collapse (option bvh_collapse = 1) over the same BVH2: hits
+    bit-exact against brute force, every wide node with at least two children, all triangles reachable."""
+    data = scenes.single_scene(width=8, height=8, metal_subdiv=4, glass_subdiv=3)
+    tp, _, _ = data.flat_triangles()
+    nw = ctypes.c_uint()
+    h = host_lib.ht_build_collapse(oc.fp(tp), len(tp), 1, wide_cost, ctypes.byref(nw))
+    g = host_lib.ht_build_collapse(oc.fp(tp), len(tp), 0, wide_cost, None)
+    assert h and g and nw.value > 0
+    rays = edge_and_random_rays(tp, 6000, 5)
+    n = len(rays)
+    bp, bt, bb, ba = oc.OracleScene(data).trace(rays, brute=True)
+    for hh in (h, g):
+        prim4, t4 = np.empty(n, np.int32), np.empty(n, np.float32)
+        bary4, anyh4 = np.empty((n, 2), np.float32), np.empty(n, np.int32)
+        max_sp = ctypes.c_int()
+        assert host_lib.ht_trace4(hh, oc.fp(rays), n, oc.fp(prim4), oc.fp(t4), oc.fp(bary4), oc.fp(anyh4), ctypes.byref(max_sp)) == 0
+        assert np.array_equal(prim4, bp)
+        assert np.array_equal(t4.view(np.uint32), bt.view(np.uint32))
+        assert np.array_equal(bary4.view(np.uint32), bb.view(np.uint32))
+        assert np.array_equal(anyh4, ba)
+        host_lib.ht_free(hh)
 
 
 def test_single_triangle_and_degenerate_scenes(host_lib):
