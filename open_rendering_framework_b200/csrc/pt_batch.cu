@@ -126,7 +126,7 @@ pt_status render(pt_batch* b, bool graph, const std::vector<uint32_t>* frames_ov
       cudaGraph_t g = nullptr;
       const uint64_t k0 = pt_kernel_launch_count();
       PT_CHECK_CUDA(cudaStreamBeginCapture(E.stream, cudaStreamCaptureModeThreadLocal), "graph capture");
-      st = launch_pass(E, L, tab[0], multi, false);
+      st = launch_pass(E, L, tab, multi, false);
       const uint64_t captured = pt_kernel_launch_count() - k0;
       cudaError_t e = cudaStreamEndCapture(E.stream, &g);
       if (st != PT_OK) {
@@ -150,7 +150,7 @@ pt_status render(pt_batch* b, bool graph, const std::vector<uint32_t>* frames_ov
     count_launch(b->graph_kernels);  // the graph's kernel nodes run once per launch
   } else {
     PT_CHECK_CUDA(cudaEventRecord(E.ev0, E.stream), "event");
-    if ((st = launch_pass(E, L, tab[0], multi, true)) != PT_OK) return st;
+    if ((st = launch_pass(E, L, tab, multi, true)) != PT_OK) return st;
     PT_CHECK_CUDA(cudaEventRecord(E.ev1, E.stream), "event");
   }
   E.stats.path_samples = samples;
@@ -261,7 +261,7 @@ pt_status pt_batch_render_sequential(pt_batch* b)
     PassLayout L = plan_pass({f}, {ItemReq{0, c.next_frame, b->frames[k]}}, E.max_paths);
     one[0] = c.view();
     pt_status st = pass_resources(E, L, one);
-    if (st == PT_OK) st = launch_pass(E, L, one[0], false, false);
+    if (st == PT_OK) st = launch_pass(E, L, one, false, false);
     if (st != PT_OK) return st;
     samples += scene_path_samples(c, b->frames[k]);
     c.next_frame += b->frames[k];

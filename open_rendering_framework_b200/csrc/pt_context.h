@@ -271,7 +271,7 @@ pt_status env_build_tables(Context& c, uint32_t width, uint32_t height);
 SceneFacts scene_facts(const Context& c);
 PassLayout plan_pass(const std::vector<SceneFacts>& facts, const std::vector<ItemReq>& reqs, uint64_t max_paths);
 pt_status pass_resources(Context& E, const PassLayout& L, const std::vector<SceneDev>& scenes);
-pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool multi, bool allow_events, bool adjoint = false);
+pt_status launch_pass(Context& E, const PassLayout& L, const std::vector<SceneDev>& tab, bool multi, bool allow_events, bool adjoint = false);
 
 }  // namespace pt
 

@@ -96,7 +96,8 @@ struct WfDev {
   const SceneDev* scenes;
   const ItemDev* items;
   uint32_t n_items;
-  uint32_t multi;  // 0: every path of the pass renders scenes[0]
+  uint32_t multi;   // 0: every path of the chunk renders scenes[scene0]
+  uint32_t scene0;
   uint16_t* path_item;
 };
 
@@ -124,7 +125,7 @@ __device__ __forceinline__ uint32_t find_item(const ItemDev* items, uint32_t n, 
 }
 __device__ __forceinline__ const SceneDev& scene_of(const WfDev& w, uint32_t pid)
 {
-  const uint32_t k = w.multi ? w.items[w.path_item[pid]].scene : 0u;
+  const uint32_t k = w.multi ? w.items[w.path_item[pid]].scene : w.scene0;
   return w.scenes[k];
 }
 
@@ -2538,8 +2539,12 @@ template <class K> int full_wave(K kernel)
   return grid;
 }
 
-pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool multi, bool allow_events, bool adjoint)
+pt_status launch_pass(Context& E, const PassLayout& L, const std::vector<SceneDev>& tab, bool multi_pass, bool allow_events, bool adjoint)
 {
+  // per chunk: a chunk whose paths all render one scene runs the single-scene kernels on that scene
+  // (its record as a kernel parameter, no per-ray scene lookup), else the multi-scene kernels
+  SceneDev S0 = tab[0];
+  bool multi = multi_pass;
   Context& c = E;
   WfDev w;
   Wavefront& wf = c.wf;
@@ -2567,6 +2572,7 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
   w.g_slots = L.sss ? wf.gather_slots : 0;
   w.scenes = c.d_scene_tab.as<SceneDev>();
   w.multi = multi ? 1u : 0u;
+  w.scene0 = 0;
   w.path_item = wf.path_item.as<uint16_t>();
   w.adj_a = adjoint ? wf.adj_a.as<float4>() : nullptr;
   w.adj_b = adjoint ? wf.adj_b.as<float4>() : nullptr;
@@ -2583,19 +2589,24 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
   const int grid_trace = sm_count() * 8, grid_shade = sm_count() * 8;
   // the 4-wide BVH when every scene of the pass has one (pass_resources)
   const bool w4 = E.pass_w4;
-  int occ_ext = 0, occ_sh = 0;
-  auto occupancy = [&](auto ext, auto sh) -> pt_status {
+  // persistent grids: the SM count times the resident blocks of the single- and multi-scene kernels
+  int grid_persist_of[2] = {0, 0};
+  auto occupancy = [&](auto ext, auto sh, int& grid) -> pt_status {
+    int occ_ext = 0, occ_sh = 0;
     PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_ext, ext, kTraceBlock, 0), "occupancy");
     PT_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_sh, sh, kTraceBlock, 0), "occupancy");
+    grid = sm_count() * std::max(1, std::min(occ_ext, occ_sh));
     return PT_OK;
   };
   pt_status ost;
-  if (w4) ost = multi ? occupancy(k_extend_persistent<true, true>, k_shadow_persistent<true, false, true>)
-                      : occupancy(k_extend_persistent<false, true>, k_shadow_persistent<false, false, true>);
-  else ost = multi ? occupancy(k_extend_persistent<true, false>, k_shadow_persistent<true, false, false>)
-                   : occupancy(k_extend_persistent<false, false>, k_shadow_persistent<false, false, false>);
+  if (w4) ost = occupancy(k_extend_persistent<false, true>, k_shadow_persistent<false, false, true>, grid_persist_of[0]);
+  else ost = occupancy(k_extend_persistent<false, false>, k_shadow_persistent<false, false, false>, grid_persist_of[0]);
+  if (ost == PT_OK && multi_pass) {
+    if (w4) ost = occupancy(k_extend_persistent<true, true>, k_shadow_persistent<true, false, true>, grid_persist_of[1]);
+    else ost = occupancy(k_extend_persistent<true, false>, k_shadow_persistent<true, false, false>, grid_persist_of[1]);
+  }
   if (ost != PT_OK) return ost;
-  const int grid_persist = sm_count() * std::max(1, std::min(occ_ext, occ_sh));
+  int grid_persist = grid_persist_of[0];
   const int grid_bin = sm_count() * 8;
   const bool prof = c.profile && allow_events;
   PT_CHECK_CUDA(cudaMemsetAsync(w.cnt, 0, kCounters * 4, c.stream), "reset counters");
@@ -2743,6 +2754,13 @@ pt_status launch_pass(Context& E, const PassLayout& L, const SceneDev& S0, bool 
     const uint32_t ie = k + 1 < n_chunks ? L.chunk_item_begin[k + 1] : (uint32_t)L.items.size();
     w.items = items + ib;
     w.n_items = ie - ib;
+    bool one_scene = true;
+    for (uint32_t i = ib + 1; i < ie; ++i) one_scene = one_scene && L.items[i].scene == L.items[ib].scene;
+    multi = multi_pass && !one_scene;
+    w.multi = multi ? 1u : 0u;
+    w.scene0 = multi ? 0u : L.items[ib].scene;
+    S0 = tab[w.scene0];
+    grid_persist = grid_persist_of[multi ? 1 : 0];
     const uint64_t n_paths = L.chunk_paths[k], n_probes = L.chunk_probes[k];
     if (n_probes) {
       for (uint64_t j0 = 0; j0 < n_probes; j0 += w.cap) {
@@ -2813,7 +2831,7 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
   uint64_t launches0 = pt_kernel_launch_count();
   memset(&c.stats, 0, sizeof(c.stats));
   PT_CHECK_CUDA(cudaEventRecord(c.ev0, c.stream), "event");
-  if ((st = launch_pass(c, L, scenes[0], false, true)) != PT_OK) return st;
+  if ((st = launch_pass(c, L, scenes, false, true)) != PT_OK) return st;
   PT_CHECK_CUDA(cudaEventRecord(c.ev1, c.stream), "event");
   c.stats.path_samples = scene_path_samples(c, n_frames);
   c.stats.kernel_launches = (uint32_t)(pt_kernel_launch_count() - launches0);
@@ -2854,7 +2872,7 @@ pt_status pt_render_adjoint(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames
   uint64_t launches0 = pt_kernel_launch_count();
   memset(&c.stats, 0, sizeof(c.stats));
   PT_CHECK_CUDA(cudaEventRecord(c.ev0, c.stream), "event");
-  if ((st = launch_pass(c, L, scenes[0], false, true, true)) != PT_OK) return st;
+  if ((st = launch_pass(c, L, scenes, false, true, true)) != PT_OK) return st;
   PT_CHECK_CUDA(cudaEventRecord(c.ev1, c.stream), "event");
   c.stats.path_samples = scene_path_samples(c, n_frames);
   c.stats.kernel_launches = (uint32_t)(pt_kernel_launch_count() - launches0);
