@@ -354,6 +354,8 @@ pt_status pt_get_render_stats(pt_ctx* ctx, pt_render_stats* out);
  *   "bvh_collapse" the host builder's 4-wide collapse: 0 = greedy (the internal child of largest area opened
  *                  first), 1 = SAH-optimal over the BVH2 (dynamic program; default); with
  *   "bvh_wide_cost_milli"  SAH cost of a wide node visit x 1000 for collapse 1 (default 1500): next pt_build
+ *   "bvh_treelets" device builder: rounds of treelet restructuring of the LBVH (0..4, default 3; the
+ *                  reference's OptiX "Trbvh" builder restructures treelets likewise): next pt_build
  *   "bvh_builder"  0 = binned SAH on the host threads (default), 1 = LBVH on the device (Morton codes,
  *                  radix sort, Karras hierarchy, SAH leaves, device 4-wide collapse; the reference's
  *                  OptiX builders, OptixSceneLoader.cpp:136, also run on the device): next pt_build */

@@ -259,6 +259,11 @@ struct NodeRec {
   float4 lo, hi;  // box; lo.w = SAH cost, hi.w = triangle count (as float)
 };
 
+// Every walk from a leaf to the root is bounded: a walk longer than kMaxWalk levels means a broken tree
+// (the BVH2 may not reach depth 64 anyway); the kernel then raises *err and stops, and the host
+// discards the build.
+constexpr int kMaxWalk = 256;
+
 // Pass 5: bottom-up boxes and SAH costs.  One thread per leaf walks up; at each internal node the
 // first arriving child stops, the second computes the node (its sibling's record is then complete:
 // every record is written before the __threadfence that precedes the arrival counter).
@@ -266,7 +271,7 @@ __global__ void __launch_bounds__(kBlock) k_bottom_up(int n, const uint32_t* __r
                                                       const float4* __restrict__ box_hi, const int2* __restrict__ child,
                                                       const int* __restrict__ iparent, const int* __restrict__ lparent,
                                                       NodeRec* leafrec, NodeRec* noderec, uint32_t* visits, uint8_t* collapse,
-                                                      float trav_cost, int max_leaf)
+                                                      float trav_cost, int max_leaf, int* err)
 {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
@@ -278,8 +283,12 @@ __global__ void __launch_bounds__(kBlock) k_bottom_up(int n, const uint32_t* __r
   r.hi.w = 1.0f;
   leafrec[j] = r;
   __threadfence();
-  int p = lparent[j];
+  int p = lparent[j], steps = 0;
   while (p >= 0) {
+    if (p >= n - 1 || ++steps > kMaxWalk) {
+      atomicExch(err, 1);
+      return;
+    }
     if (atomicAdd(visits + p, 1u) == 0u) return;
     __threadfence();
     const int2 c = child[p];
@@ -308,10 +317,223 @@ __global__ void __launch_bounds__(kBlock) k_bottom_up(int n, const uint32_t* __r
   }
 }
 
-// The code of child c (>= 0 internal, < 0 leaf ~j) as the BVH2 stores it, and its record.
-__device__ __forceinline__ int child_code(int c, const int2* range, const uint8_t* collapse)
+// Pass 5b (option bvh_treelets, rounds of it): treelet restructuring (T. Karras, T. Aila, "Fast
+// Parallel Construction of High-Quality Bounding Volume Hierarchies", HPG 2013; the "Trbvh" builder the
+// reference requests from OptiX, OptixSceneLoader.cpp:136).  Bottom-up as pass 5: at each internal node
+// of at least kTreeletMin triangles whose subtrees are complete, the node and its descendants form a
+// treelet of up to 7 leaves (the treelet leaf of largest area is opened while there are fewer than 7),
+// and a dynamic program over the 127 subsets of those leaves finds the topology of least SAH cost
+//   c(S) = min( trav_cost * A(S) + min over splits P of S of c(P) + c(S \ P),  A(S) * N(S) if N(S) <= max_leaf )
+// (a treelet leaf's c is A x its subtree's cost per area, noderec lo.w).  The warp that finds such nodes
+// processes them one after the other, all lanes sharing each dynamic program; the treelet's internal
+// nodes are reused for the new topology, and their boxes, counts and costs rewritten.  Only the nodes
+// below the treelet's root change, and nothing else touches them once both of the root's subtrees are
+// complete, so each treelet depends on its own subtree only: the result does not depend on the order
+// in which warps arrive.
+constexpr int kTreeletLeaves = 7;
+constexpr int kTreeletSets = 1 << kTreeletLeaves;
+constexpr int kTreeletMin = 8;  // smaller subtrees end inside a leaf of up to 8 triangles anyway
+
+struct TreeletShared {
+  float area[kTreeletSets];
+  float cost[kTreeletSets];
+  uint8_t part[kTreeletSets];
+};
+
+__device__ __forceinline__ NodeRec load_rec(const NodeRec* r)
 {
-  if (c < 0) return (int)(kEmptyLeaf | ((uint32_t)(~c) << 4) | 1u);
+  NodeRec a;
+  a.lo = __ldcg(&r->lo);
+  a.hi = __ldcg(&r->hi);
+  return a;
+}
+
+// One treelet at `root`, processed by the whole warp (root uniform across the warp).
+__device__ void treelet_optimize(int root, int2* child, int* iparent, int* lparent, const NodeRec* leafrec, NodeRec* noderec,
+                                 TreeletShared& sh, float trav_cost, int max_leaf)
+{
+  const int lane = threadIdx.x & 31;
+  // form the treelet (every lane the same, from the same records)
+  int leaves[kTreeletLeaves], inner[kTreeletLeaves - 1];
+  NodeRec lrec[kTreeletLeaves];
+  int nl = 0, ni = 0;
+  inner[ni++] = root;
+  {
+    const int2 c = __ldcg(&child[root]);
+    leaves[nl++] = c.x;
+    leaves[nl++] = c.y;
+  }
+  for (int k = 0; k < nl; ++k) lrec[k] = load_rec(leaves[k] >= 0 ? noderec + leaves[k] : leafrec + ~leaves[k]);
+  while (nl < kTreeletLeaves) {
+    int best = -1;
+    float ba = -1.0f;
+    for (int k = 0; k < nl; ++k) {
+      if (leaves[k] < 0) continue;
+      const float a = area_of(lrec[k].lo, lrec[k].hi);
+      if (a > ba) { ba = a; best = k; }
+    }
+    if (best < 0) break;
+    const int x = leaves[best];
+    inner[ni++] = x;
+    const int2 c = __ldcg(&child[x]);
+    leaves[best] = c.x;
+    lrec[best] = load_rec(c.x >= 0 ? noderec + c.x : leafrec + ~c.x);
+    leaves[nl] = c.y;
+    lrec[nl] = load_rec(c.y >= 0 ? noderec + c.y : leafrec + ~c.y);
+    ++nl;
+  }
+  const int full = (1 << nl) - 1;
+  // subset areas and the treelet leaves' own costs
+  for (int set = lane + 1; set <= full; set += 32) {
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int k = 0; k < nl; ++k) {
+      if (!((set >> k) & 1)) continue;
+      lo[0] = fminf(lo[0], lrec[k].lo.x); lo[1] = fminf(lo[1], lrec[k].lo.y); lo[2] = fminf(lo[2], lrec[k].lo.z);
+      hi[0] = fmaxf(hi[0], lrec[k].hi.x); hi[1] = fmaxf(hi[1], lrec[k].hi.y); hi[2] = fmaxf(hi[2], lrec[k].hi.z);
+    }
+    const float dx = fmaxf(0.0f, hi[0] - lo[0]), dy = fmaxf(0.0f, hi[1] - lo[1]), dz = fmaxf(0.0f, hi[2] - lo[2]);
+    sh.area[set] = dx * dy + dy * dz + dz * dx;
+    if (__popc(set) == 1) {
+      const int k = __ffs(set) - 1;
+      sh.cost[set] = sh.area[set] * lrec[k].lo.w;
+      sh.part[set] = 0;
+    }
+  }
+  __syncwarp();
+  // subsets by increasing size: every split of a subset is into smaller ones
+  for (int size = 2; size <= nl; ++size) {
+    for (int set = lane + 1; set <= full; set += 32) {
+      if (__popc(set) != size) continue;
+      const int low = set & -set;  // each split once: the part holding the lowest leaf
+      float best = INFINITY;
+      int bp = low;
+      for (int part = (set - 1) & set; part; part = (part - 1) & set) {
+        if (!(part & low)) continue;
+        const float c = sh.cost[part] + sh.cost[set ^ part];
+        if (c < best) { best = c; bp = part; }
+      }
+      float n_tris = 0.0f;
+      for (int k = 0; k < nl; ++k) n_tris += ((set >> k) & 1) ? lrec[k].hi.w : 0.0f;
+      const float split = trav_cost * sh.area[set] + best;
+      const float leaf = n_tris <= (float)max_leaf ? sh.area[set] * n_tris : INFINITY;
+      sh.cost[set] = fminf(split, leaf);
+      sh.part[set] = (uint8_t)bp;
+    }
+    __syncwarp();
+  }
+  // rebuild the treelet on its internal nodes (lane 0): pre-order assignment, then the records
+  // bottom-up (reverse of the assignment order)
+  if (lane == 0) {
+    int node_set[kTreeletLeaves - 1];
+    int used = 1;
+    node_set[0] = full;
+    for (int q = 0; q < used; ++q) {
+      const int set = node_set[q];
+      const int a = sh.part[set], b = set ^ a;
+      int code[2];
+      const int sides[2] = {a, b};
+      for (int h = 0; h < 2; ++h) {
+        if (__popc(sides[h]) == 1) {
+          code[h] = leaves[__ffs(sides[h]) - 1];
+        } else {
+          node_set[used] = sides[h];
+          code[h] = inner[used++];
+        }
+        if (code[h] >= 0) iparent[code[h]] = inner[q];
+        else lparent[~code[h]] = inner[q];
+      }
+      __stcg(&child[inner[q]], make_int2(code[0], code[1]));
+    }
+    for (int q = used - 1; q >= 0; --q) {
+      const int2 c = child[inner[q]];
+      const NodeRec a = load_rec(c.x >= 0 ? noderec + c.x : leafrec + ~c.x);
+      const NodeRec b = load_rec(c.y >= 0 ? noderec + c.y : leafrec + ~c.y);
+      NodeRec m;
+      m.lo = make_float4(fminf(a.lo.x, b.lo.x), fminf(a.lo.y, b.lo.y), fminf(a.lo.z, b.lo.z), 0.0f);
+      m.hi = make_float4(fmaxf(a.hi.x, b.hi.x), fmaxf(a.hi.y, b.hi.y), fmaxf(a.hi.z, b.hi.z), a.hi.w + b.hi.w);
+      const float A = area_of(m.lo, m.hi);
+      m.lo.w = A > 0.0f ? sh.cost[node_set[q]] / A : a.lo.w + b.lo.w;  // cost per area, as pass 5 keeps it
+      __stcg(&noderec[inner[q]].lo, m.lo);
+      __stcg(&noderec[inner[q]].hi, m.hi);
+    }
+  }
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(kBlock) k_treelets(int n, int2* child, int* iparent, int* lparent, const NodeRec* leafrec, NodeRec* noderec,
+                                                     uint32_t* visits, float trav_cost, int max_leaf, int* err)
+{
+  __shared__ TreeletShared sh[kWarpsPerBlock];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  bool active = j < n;
+  int p = active ? lparent[j] : -1, steps = 0;
+  for (;;) {
+    bool ready = false;
+    if (active) {
+      if (p < 0 || p >= n - 1 || ++steps > kMaxWalk) {
+        if (p >= n - 1 || steps > kMaxWalk) atomicExch(err, 1);
+        active = false;
+      } else if (atomicAdd(visits + p, 1u) == 0u) {
+        active = false;
+      } else {
+        ready = true;
+      }
+    }
+    __threadfence();
+    unsigned m = __ballot_sync(0xffffffffu, ready);
+    if (!__any_sync(0xffffffffu, active) && m == 0) break;
+    while (m) {
+      const int src = __ffs(m) - 1;
+      m &= m - 1;
+      const int node = __shfl_sync(0xffffffffu, p, src);
+      if (__ldcg(&noderec[node].hi.w) >= (float)kTreeletMin)
+        treelet_optimize(node, child, iparent, lparent, leafrec, noderec, sh[threadIdx.x >> 5], trav_cost, max_leaf);
+    }
+    __threadfence();
+    if (ready) p = __ldcg(&iparent[p]);
+  }
+}
+
+// Pass 5c: each leaf's position in the tree's left-to-right leaf order (the triangles are written in that
+// order, so every subtree covers a contiguous range): the triangle counts of the left siblings on the
+// way up; and for each internal node the range of its subtree, set by its leftmost leaf.
+__global__ void __launch_bounds__(kBlock) k_leaf_positions(int n, const int2* __restrict__ child, const int* __restrict__ iparent,
+                                                           const int* __restrict__ lparent, const NodeRec* __restrict__ noderec,
+                                                           uint32_t* __restrict__ pos_of, int2* __restrict__ range, int* __restrict__ err)
+{
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  uint32_t pos = 0;
+  int c = ~j, steps = 0;
+  for (int q = lparent[j]; q >= 0; q = iparent[q]) {
+    if (q >= n - 1 || ++steps > kMaxWalk) {
+      atomicExch(err, 1);
+      pos_of[j] = 0;
+      return;
+    }
+    const int2 k = child[q];
+    if (k.y == c) pos += k.x >= 0 ? (uint32_t)noderec[k.x].hi.w : 1u;
+    c = q;
+  }
+  if (pos >= (uint32_t)n) {
+    atomicExch(err, 1);
+    pos = 0;
+  }
+  pos_of[j] = pos;
+  c = ~j;
+  steps = 0;
+  for (int q = lparent[j]; q >= 0 && q < n - 1 && child[q].x == c && ++steps <= kMaxWalk; q = iparent[q]) {
+    const int last = (int)pos + (int)noderec[q].hi.w - 1;
+    if (last >= n) atomicExch(err, 1);
+    range[q] = make_int2((int)pos, last < n ? last : n - 1);
+    c = q;
+  }
+}
+
+// The code of child c (>= 0 internal, < 0 leaf ~j) as the BVH2 stores it, and its record.
+__device__ __forceinline__ int child_code(int c, const int2* range, const uint8_t* collapse, const uint32_t* pos_of)
+{
+  if (c < 0) return (int)(kEmptyLeaf | (pos_of[~c] << 4) | 1u);
   if (collapse[c]) {
     const int2 r = range[c];
     return (int)(kEmptyLeaf | ((uint32_t)r.x << 4) | (uint32_t)(r.y - r.x + 1));
@@ -323,8 +545,8 @@ __device__ __forceinline__ int child_code(int c, const int2* range, const uint8_
 // and never reached).  The root of a tree that is a single leaf holds that leaf and an empty one.
 __global__ void __launch_bounds__(kBlock) k_write_bvh2(int n, const int2* __restrict__ child, const int* __restrict__ iparent,
                                                        const int2* __restrict__ range, const uint8_t* __restrict__ collapse,
-                                                       const NodeRec* __restrict__ leafrec, const NodeRec* __restrict__ noderec,
-                                                       float4* __restrict__ nodes)
+                                                       const uint32_t* __restrict__ pos_of, const NodeRec* __restrict__ leafrec,
+                                                       const NodeRec* __restrict__ noderec, float4* __restrict__ nodes)
 {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n - 1) return;
@@ -338,8 +560,8 @@ __global__ void __launch_bounds__(kBlock) k_write_bvh2(int n, const int2* __rest
     r1.hi = r1.lo;
   } else {
     const int2 c = child[p];
-    c0 = child_code(c.x, range, collapse);
-    c1 = child_code(c.y, range, collapse);
+    c0 = child_code(c.x, range, collapse, pos_of);
+    c1 = child_code(c.y, range, collapse, pos_of);
     r0 = c.x >= 0 ? noderec[c.x] : leafrec[~c.x];
     r1 = c.y >= 0 ? noderec[c.y] : leafrec[~c.y];
   }
@@ -350,23 +572,31 @@ __global__ void __launch_bounds__(kBlock) k_write_bvh2(int n, const int2* __rest
   nd[3] = make_float4(__int_as_float(c0), __int_as_float(c1), __int_as_float(iparent[p]), 0.0f);
 }
 
-// Pass 6b: triangles in leaf (sorted) order as Moller-Trumbore records, and the BVH2 depth (levels
+// Pass 6b: triangles in leaf order (pass 5c) as Moller-Trumbore records, and the BVH2 depth (levels
 // including the leaves): each triangle counts the internal nodes above it that the tree keeps (those
 // inside a leaf's subtree are not nodes of the tree), plus its leaf.
 __global__ void __launch_bounds__(kBlock) k_write_tris(int n, const float* __restrict__ tri, const uint32_t* __restrict__ order,
-                                                       const int* __restrict__ lparent, const int* __restrict__ iparent,
-                                                       const uint8_t* __restrict__ collapse, float4* __restrict__ v0, float4* __restrict__ e1,
-                                                       float4* __restrict__ e2, int* __restrict__ max_depth)
+                                                       const uint32_t* __restrict__ pos_of, const int* __restrict__ lparent,
+                                                       const int* __restrict__ iparent, const uint8_t* __restrict__ collapse,
+                                                       float4* __restrict__ v0, float4* __restrict__ e1, float4* __restrict__ e2,
+                                                       int* __restrict__ max_depth)  // max_depth[0] depth, [1] error
 {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
-  const uint32_t i = order[j];
+  const uint32_t i = order[j], at = pos_of[j];
+  if (at >= (uint32_t)n) return;  // k_leaf_positions raised the error
   const float* p = tri + 9 * (size_t)i;
-  v0[j] = make_float4(p[0], p[1], p[2], __int_as_float((int)i));
-  e1[j] = make_float4(p[3] - p[0], p[4] - p[1], p[5] - p[2], 0.0f);
-  e2[j] = make_float4(p[6] - p[0], p[7] - p[1], p[8] - p[2], 0.0f);
+  v0[at] = make_float4(p[0], p[1], p[2], __int_as_float((int)i));
+  e1[at] = make_float4(p[3] - p[0], p[4] - p[1], p[5] - p[2], 0.0f);
+  e2[at] = make_float4(p[6] - p[0], p[7] - p[1], p[8] - p[2], 0.0f);
   int d = 1, steps = 0;
-  for (int q = lparent[j]; q >= 0 && steps < n; q = iparent[q], ++steps) d += collapse[q] ? 0 : 1;
+  for (int q = lparent[j]; q >= 0; q = iparent[q]) {
+    if (q >= n - 1 || ++steps > kMaxWalk) {
+      atomicExch(max_depth + 1, 1);  // the error word after the depth
+      return;
+    }
+    d += collapse[q] ? 0 : 1;
+  }
   if (collapse[0]) d = 2;  // a single-leaf tree: the root and its leaf
   atomicMax(max_depth, d);
 }
@@ -459,7 +689,7 @@ __global__ void __launch_bounds__(128) k_collapse_level(const float4* __restrict
 // Offsets of the build's temporaries in one scratch allocation (256-byte aligned), kept by the context
 // for later rebuilds.
 struct BuildLayout {
-  size_t tri, blo, bhi, keys_a, keys_b, idx_a, idx_b, hist, rowtot, cb, child, range, ipar, lpar, leafrec, noderec, visits, collapse, depth, work_a,
+  size_t tri, blo, bhi, keys_a, keys_b, idx_a, idx_b, hist, rowtot, posof, cb, child, range, ipar, lpar, leafrec, noderec, visits, collapse, depth, work_a,
       work_b, counters, total;
   BuildLayout(uint32_t n, uint32_t nb)
   {
@@ -478,6 +708,7 @@ struct BuildLayout {
     idx_b = take((size_t)n * 4);
     hist = take((size_t)kRadix * nb * 4);
     rowtot = take((size_t)kRadix * 4);
+    posof = take((size_t)n * 4);
     cb = take(6 * 4);
     child = take((size_t)(n - 1) * sizeof(int2));
     range = take((size_t)(n - 1) * sizeof(int2));
@@ -487,7 +718,7 @@ struct BuildLayout {
     noderec = take((size_t)(n - 1) * sizeof(NodeRec));
     visits = take((size_t)(n - 1) * 4);
     collapse = take((size_t)(n - 1));
-    depth = take(4);
+    depth = take(8);  // [0] BVH2 depth, [1] error raised by the treelet / position passes
     work_a = take((size_t)n * sizeof(int2));
     work_b = take((size_t)n * sizeof(int2));
     counters = take((size_t)(kMaxDepth4 + 4) * 4);
@@ -518,6 +749,7 @@ pt_status build_bvh_device(Context& c)
   uint32_t *keys_a = (uint32_t*)(base + Lo.keys_a), *keys_b = (uint32_t*)(base + Lo.keys_b);
   uint32_t *idx_a = (uint32_t*)(base + Lo.idx_a), *idx_b = (uint32_t*)(base + Lo.idx_b);
   uint32_t *hist = (uint32_t*)(base + Lo.hist), *rowtot = (uint32_t*)(base + Lo.rowtot), *cb = (uint32_t*)(base + Lo.cb);
+  uint32_t* pos_of = (uint32_t*)(base + Lo.posof);
   int2 *child = (int2*)(base + Lo.child), *range = (int2*)(base + Lo.range);
   int *ipar = (int*)(base + Lo.ipar), *lpar = (int*)(base + Lo.lpar);
   NodeRec *leafrec = (NodeRec*)(base + Lo.leafrec), *noderec = (NodeRec*)(base + Lo.noderec);
@@ -532,7 +764,7 @@ pt_status build_bvh_device(Context& c)
   const uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
   PT_CHECK_CUDA(cudaMemcpyAsync(cb, init, sizeof(init), cudaMemcpyHostToDevice, st), "device BVH build H2D");
   PT_CHECK_CUDA(cudaMemsetAsync(visits, 0, (size_t)(n - 1) * 4, st), "device BVH build");
-  PT_CHECK_CUDA(cudaMemsetAsync(depth, 0, 4, st), "device BVH build");
+  PT_CHECK_CUDA(cudaMemsetAsync(depth, 0, 8, st), "device BVH build");
   // the root: BVH2 node 0 becomes wide node 0, the one item of level 0
   std::vector<uint32_t> cinit(kMaxDepth4 + 4, 0u);
   cinit[0] = 1;
@@ -556,11 +788,25 @@ pt_status build_bvh_device(Context& c)
   const int gi = (int)((n - 1 + kBlock - 1) / kBlock), gl = (int)nb;
   k_karras<<<gi, kBlock, 0, st>>>(kin, (int)n, child, ipar, lpar, range);
   k_bottom_up<<<gl, kBlock, 0, st>>>((int)n, vin, blo, bhi, child, ipar, lpar, leafrec, noderec, visits, collapse, c.bvh_params.trav_cost,
-                                     c.bvh_params.max_leaf);
-  k_write_bvh2<<<gi, kBlock, 0, st>>>((int)n, child, ipar, range, collapse, leafrec, noderec, c.d_nodes.as<float4>());
-  k_write_tris<<<gl, kBlock, 0, st>>>((int)n, tri, vin, lpar, ipar, collapse, c.d_v0.as<float4>(), c.d_e1.as<float4>(), c.d_e2.as<float4>(),
-                                      depth);
-  count_launch(4);
+                                     c.bvh_params.max_leaf, depth + 1);
+  count_launch(2);
+  for (int r = 0; r < c.bvh_params.treelet_rounds; ++r) {
+    PT_CHECK_CUDA(cudaMemsetAsync(visits, 0, (size_t)(n - 1) * 4, st), "device BVH build");
+    k_treelets<<<gl, kBlock, 0, st>>>((int)n, child, ipar, lpar, leafrec, noderec, visits, c.bvh_params.trav_cost, c.bvh_params.max_leaf,
+                                      depth + 1);
+    count_launch();
+  }
+  if (c.bvh_params.treelet_rounds > 0) {  // the leaf collapse and costs over the final topology
+    PT_CHECK_CUDA(cudaMemsetAsync(visits, 0, (size_t)(n - 1) * 4, st), "device BVH build");
+    k_bottom_up<<<gl, kBlock, 0, st>>>((int)n, vin, blo, bhi, child, ipar, lpar, leafrec, noderec, visits, collapse, c.bvh_params.trav_cost,
+                                       c.bvh_params.max_leaf, depth + 1);
+    count_launch();
+  }
+  k_leaf_positions<<<gl, kBlock, 0, st>>>((int)n, child, ipar, lpar, noderec, pos_of, range, depth + 1);
+  k_write_bvh2<<<gi, kBlock, 0, st>>>((int)n, child, ipar, range, collapse, pos_of, leafrec, noderec, c.d_nodes.as<float4>());
+  k_write_tris<<<gl, kBlock, 0, st>>>((int)n, tri, vin, pos_of, lpar, ipar, collapse, c.d_v0.as<float4>(), c.d_e1.as<float4>(),
+                                      c.d_e2.as<float4>(), depth);
+  count_launch(3);
   // 4-wide collapse: levels 0 .. kMaxDepth4 - 2 (wide depth, root = 1, below kMaxDepth4)
   int2 *win = work_a, *wout = work_b;
   uint64_t cap_items = 1;
@@ -574,13 +820,15 @@ pt_status build_bvh_device(Context& c)
   }
   PT_CHECK_CUDA(cudaGetLastError(), "device BVH build launch");
   std::vector<uint32_t> host_cnt(kMaxDepth4 + 4, 0u);
-  int d2 = 0;
+  int d2e[2] = {0, 0};
   PT_CHECK_CUDA(cudaMemcpyAsync(host_cnt.data(), cnt, host_cnt.size() * 4, cudaMemcpyDeviceToHost, st), "device BVH build");
-  PT_CHECK_CUDA(cudaMemcpyAsync(&d2, depth, 4, cudaMemcpyDeviceToHost, st), "device BVH build");
+  PT_CHECK_CUDA(cudaMemcpyAsync(d2e, depth, 8, cudaMemcpyDeviceToHost, st), "device BVH build");
   PT_CHECK_CUDA(cudaEventRecord(c.ev1, st), "device BVH build");
   PT_CHECK_CUDA(cudaStreamSynchronize(st), "device BVH build");
   float ms = 0.0f;
   cudaEventElapsedTime(&ms, c.ev0, c.ev1);
+  const int d2 = d2e[0];
+  if (d2e[1]) return fail(PT_CAP_EXCEEDED, "device BVH build: inconsistent tree after restructuring");
   if (d2 >= 64) return fail(PT_CAP_EXCEEDED, "device BVH build: the tree is deeper than the traversal trail allows");
   int levels = 0;
   while (levels + 1 < kMaxDepth4 && host_cnt[2 + levels] > 0) ++levels;

@@ -906,6 +906,11 @@ pt_status pt_set_option(pt_ctx* ctx, const char* name, int64_t value)
     ctx->c.bvh_params.wide_cost = (float)value / 1000.0f;
     return PT_OK;
   }
+  if (k == "bvh_treelets") {  // device builder: rounds of treelet restructuring (default 3), for the next pt_build
+    if (value < 0 || value > 4) return fail(PT_INVALID_ARG, "pt_set_option: bvh_treelets must be in [0, 4]");
+    ctx->c.bvh_params.treelet_rounds = (int)value;
+    return PT_OK;
+  }
   if (k == "bvh_builder") {
     if (value != 0 && value != 1) return fail(PT_INVALID_ARG, "pt_set_option: bvh_builder must be 0 (host SAH) or 1 (device LBVH)");
     ctx->c.bvh_builder = (int)value;

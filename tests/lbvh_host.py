@@ -2,7 +2,9 @@
 restated on the host in numpy / Python, so that traversal over an LBVH-shaped tree -- single-triangle
 leaves with boxes that end exactly at shared vertices -- can be checked against brute force without a
 GPU.  Same steps as the kernels: centroid bounds, 30-bit Morton codes, a stable sort, the Karras
-hierarchy (equal codes ordered by position), bottom-up boxes and SAH leaf choice, child-pair nodes."""
+hierarchy (equal codes ordered by position), bottom-up boxes and SAH leaf choice, child-pair nodes.
+It restates the builder without treelet restructuring (option bvh_treelets = 0), whose trees keep the
+Morton order of the leaves."""
 import numpy as np
 
 f32 = np.float32

@@ -1,5 +1,6 @@
-"""The device BVH builder (option "bvh_builder" = 1: LBVH over Morton codes with SAH leaves and a
-device 4-wide collapse) against brute force and against the host SAH builder.
+"""The device BVH builder (option "bvh_builder" = 1: LBVH over Morton codes, treelet restructuring
+(option "bvh_treelets" rounds), SAH leaves and a device 4-wide collapse) against brute force and
+against the host SAH builder.
 
 Hits are decided by the triangle test alone (closest t, ties to the lower triangle index), so any valid
 tree must give bit-identical closest hits (index, t, barycentrics) and any-hit answers to a brute-force
@@ -81,11 +82,12 @@ def heightfield_scene():
     return sc.SceneData(base.integrator, base.camera, base.background, meshes, base.lights)
 
 
+@pytest.mark.parametrize("treelets", [0, 2])
 @pytest.mark.parametrize("which", ["single_scene", "heightfield", "duplicated"])
-def test_device_bvh_hits_bit_exact_vs_brute_force(which):
+def test_device_bvh_hits_bit_exact_vs_brute_force(which, treelets):
     data = {"single_scene": lambda: scenes.single_scene(width=16, height=16), "heightfield": heightfield_scene,
             "duplicated": duplicated_scene}[which]()
-    R = sc.Renderer(data, build_options=DEVICE)
+    R = sc.Renderer(data, build_options=dict(DEVICE, bvh_treelets=treelets))
     info = R.build_info()
     print(which, info.as_dict())
     assert info.builder == 1 and info.n_triangles == data.n_triangles
@@ -121,6 +123,24 @@ def test_device_bvh_tiny_scenes(n_tris):
     O = oc.OracleScene(data)
     assert_same_hits(gpu_trace(R, rays), O.trace(rays, brute=True))
     R.close()
+
+
+def test_treelet_restructuring_lowers_the_sah_cost():
+    """Rounds of treelet restructuring lower the SAH cost of the device tree on the single-scene
+    configuration's geometry, toward the host binned-SAH tree's."""
+    data = scenes.single_scene(width=16, height=16)
+    costs = {}
+    for rounds in (0, 1, 2, 3):
+        R = sc.Renderer(data, build_options=dict(DEVICE, bvh_treelets=rounds))
+        info = R.build_info()
+        assert info.builder == 1
+        costs[rounds] = info.sah_cost
+        R.close()
+    R = sc.Renderer(data)
+    host = R.build_info().sah_cost
+    R.close()
+    print("SAH cost by treelet rounds:", costs, "host binned SAH:", host)
+    assert costs[1] < costs[0] and costs[2] <= costs[1] * 1.001 and costs[3] <= costs[2] * 1.001
 
 
 @pytest.mark.parametrize("which", ["single_scene", "translucent"])
