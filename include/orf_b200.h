@@ -351,11 +351,13 @@ pt_status pt_get_render_stats(pt_ctx* ctx, pt_render_stats* out);
  *   "bvh4"         1 = the persistent kernels walk the 4-wide BVH (default), 0 = the BVH2
  *   "bvh_trav_cost_milli"  SAH cost of a node step x 1000 relative to a triangle test (default 1200) and
  *   "bvh_max_leaf"         the largest leaf the SAH may choose (1..15, default 8): applied by the next pt_build
- *   "bvh_collapse" the host builder's 4-wide collapse: 0 = greedy (the internal child of largest area opened
+ *   "bvh_collapse" the 4-wide collapse of either builder: 0 = greedy (the internal child of largest area opened
  *                  first), 1 = SAH-optimal over the BVH2 (dynamic program; default); with
  *   "bvh_wide_cost_milli"  SAH cost of a wide node visit x 1000 for collapse 1 (default 1500): next pt_build
  *   "bvh_treelets" device builder: rounds of treelet restructuring of the LBVH (0..4, default 3; the
  *                  reference's OptiX "Trbvh" builder restructures treelets likewise): next pt_build
+ *   "bvh_treelet_min"      device builder: only subtrees of at least this many triangles form treelets
+ *                          (default 8): next pt_build
  *   "bvh_builder"  0 = binned SAH on the host threads (default), 1 = LBVH on the device (Morton codes,
  *                  radix sort, Karras hierarchy, SAH leaves, device 4-wide collapse; the reference's
  *                  OptiX builders, OptixSceneLoader.cpp:136, also run on the device): next pt_build */

@@ -24,6 +24,7 @@ struct BvhParams {
   int collapse = 1;         // 4-wide collapse: 0 greedy (largest area opened first), 1 SAH-optimal
   float wide_cost = 1.5f;   // SAH cost of a wide node visit relative to one triangle test (collapse 1)
   int treelet_rounds = 3;   // device builder: rounds of treelet restructuring after the LBVH (0 = none)
+  int treelet_min = 8;      // device builder: treelets only at nodes of at least this many triangles
 };
 
 // tri_pos: 9 floats per triangle (v0, v1, v2).  Returns false if the scene is too large for the

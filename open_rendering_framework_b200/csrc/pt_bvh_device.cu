@@ -19,10 +19,13 @@
 //   5. bottom-up boxes and SAH costs (the second of a node's two children to finish computes it); a node
 //      of at most `max_leaf` triangles whose leaf cost (one per triangle) does not exceed its split cost
 //      (trav_cost + the children's costs weighted by their areas) becomes a leaf;
+//   5b. rounds of treelet restructuring (option bvh_treelets), then pass 5 again over the new topology;
+//   5c. each leaf's position in the tree's left-to-right order and each node's range of positions;
 //   6. the BVH2 nodes, the triangles in leaf order, and the tree depth (every leaf walks to the root);
-//   7. the 4-wide collapse: one launch per level, each wide node opening its BVH2 node's internal
-//      child of largest area until it has four children (the host collapse's rule), its internal
-//      children appended to the next level's work list.
+//   7. the 4-wide collapse: one launch per level, each wide node taking the children the SAH-optimal
+//      dynamic program chose (bvh_collapse = 1, the host builder's rule; a bottom-up pass computes it)
+//      or opening its BVH2 node's internal child of largest area until it has four (bvh_collapse = 0),
+//      its internal children appended to the next level's work list.
 // The wide tree's depth is bounded by the traversal stack; a deeper tree leaves the 4-wide BVH unset.
 #include <algorithm>
 #include <cmath>
@@ -320,7 +323,7 @@ __global__ void __launch_bounds__(kBlock) k_bottom_up(int n, const uint32_t* __r
 // Pass 5b (option bvh_treelets, rounds of it): treelet restructuring (T. Karras, T. Aila, "Fast
 // Parallel Construction of High-Quality Bounding Volume Hierarchies", HPG 2013; the "Trbvh" builder the
 // reference requests from OptiX, OptixSceneLoader.cpp:136).  Bottom-up as pass 5: at each internal node
-// of at least kTreeletMin triangles whose subtrees are complete, the node and its descendants form a
+// of at least `treelet_min` triangles (option bvh_treelet_min) whose subtrees are complete, the node and its descendants form a
 // treelet of up to 7 leaves (the treelet leaf of largest area is opened while there are fewer than 7),
 // and a dynamic program over the 127 subsets of those leaves finds the topology of least SAH cost
 //   c(S) = min( trav_cost * A(S) + min over splits P of S of c(P) + c(S \ P),  A(S) * N(S) if N(S) <= max_leaf )
@@ -332,7 +335,6 @@ __global__ void __launch_bounds__(kBlock) k_bottom_up(int n, const uint32_t* __r
 // in which warps arrive.
 constexpr int kTreeletLeaves = 7;
 constexpr int kTreeletSets = 1 << kTreeletLeaves;
-constexpr int kTreeletMin = 8;  // smaller subtrees end inside a leaf of up to 8 triangles anyway
 
 struct TreeletShared {
   float area[kTreeletSets];
@@ -444,15 +446,22 @@ __device__ void treelet_optimize(int root, int2* child, int* iparent, int* lpare
       }
       __stcg(&child[inner[q]], make_int2(code[0], code[1]));
     }
-    for (int q = used - 1; q >= 0; --q) {
-      const int2 c = child[inner[q]];
-      const NodeRec a = load_rec(c.x >= 0 ? noderec + c.x : leafrec + ~c.x);
-      const NodeRec b = load_rec(c.y >= 0 ? noderec + c.y : leafrec + ~c.y);
+    // each rewired node's record from the treelet leaves it covers (already in registers)
+    for (int q = 0; q < used; ++q) {
+      const int set = node_set[q];
       NodeRec m;
-      m.lo = make_float4(fminf(a.lo.x, b.lo.x), fminf(a.lo.y, b.lo.y), fminf(a.lo.z, b.lo.z), 0.0f);
-      m.hi = make_float4(fmaxf(a.hi.x, b.hi.x), fmaxf(a.hi.y, b.hi.y), fmaxf(a.hi.z, b.hi.z), a.hi.w + b.hi.w);
+      m.lo = make_float4(INFINITY, INFINITY, INFINITY, 0.0f);
+      m.hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.0f);
+      float cost_sum = 0.0f;
+      for (int k = 0; k < nl; ++k) {
+        if (!((set >> k) & 1)) continue;
+        m.lo.x = fminf(m.lo.x, lrec[k].lo.x); m.lo.y = fminf(m.lo.y, lrec[k].lo.y); m.lo.z = fminf(m.lo.z, lrec[k].lo.z);
+        m.hi.x = fmaxf(m.hi.x, lrec[k].hi.x); m.hi.y = fmaxf(m.hi.y, lrec[k].hi.y); m.hi.z = fmaxf(m.hi.z, lrec[k].hi.z);
+        m.hi.w += lrec[k].hi.w;
+        cost_sum += lrec[k].lo.w;
+      }
       const float A = area_of(m.lo, m.hi);
-      m.lo.w = A > 0.0f ? sh.cost[node_set[q]] / A : a.lo.w + b.lo.w;  // cost per area, as pass 5 keeps it
+      m.lo.w = A > 0.0f ? sh.cost[set] / A : cost_sum;  // cost per area, as pass 5 keeps it
       __stcg(&noderec[inner[q]].lo, m.lo);
       __stcg(&noderec[inner[q]].hi, m.hi);
     }
@@ -461,7 +470,7 @@ __device__ void treelet_optimize(int root, int2* child, int* iparent, int* lpare
 }
 
 __global__ void __launch_bounds__(kBlock) k_treelets(int n, int2* child, int* iparent, int* lparent, const NodeRec* leafrec, NodeRec* noderec,
-                                                     uint32_t* visits, float trav_cost, int max_leaf, int* err)
+                                                     uint32_t* visits, float trav_cost, int max_leaf, int treelet_min, int* err)
 {
   __shared__ TreeletShared sh[kWarpsPerBlock];
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -486,7 +495,7 @@ __global__ void __launch_bounds__(kBlock) k_treelets(int n, int2* child, int* ip
       const int src = __ffs(m) - 1;
       m &= m - 1;
       const int node = __shfl_sync(0xffffffffu, p, src);
-      if (__ldcg(&noderec[node].hi.w) >= (float)kTreeletMin)
+      if (__ldcg(&noderec[node].hi.w) >= (float)treelet_min)
         treelet_optimize(node, child, iparent, lparent, leafrec, noderec, sh[threadIdx.x >> 5], trav_cost, max_leaf);
     }
     __threadfence();
@@ -623,6 +632,67 @@ __device__ __forceinline__ float kid_area(const Kid& c)
   return d[0] * d[1] + d[1] * d[2] + d[2] * d[0];
 }
 
+// Pass 6c (bvh_collapse = 1): the SAH-optimal 4-wide collapse's dynamic program over the BVH2 as
+// written (the host builder's rule, pt_bvh.cu): per internal node x, S(x, i) = the least SAH cost of x's
+// subtree placed in at most i slots of its parent's wide node (i = 1: x becomes a wide node of its own,
+// W(x) = wide_cost A(x) + D(x, 4); i >= 2: min(W(x), D(x, i)), D(x, i) = min over k of
+// S(child 0, k) + S(child 1, i - k); a leaf costs A x its triangles in any number of slots).  Bottom-up
+// with arrival counters like pass 5; nodes inside a leaf (collapsed) are passed through.  choice[x]:
+// byte 0 the split k of W(x)'s four slots, bytes 1..3 the split k for i = 2..4 (0: x stays whole).
+__device__ __forceinline__ float dp_slot_cost(const Kid& c, int i, const float4* __restrict__ dp_cost)
+{
+  if (c.code < 0) return kid_area(c) * (float)((uint32_t)c.code & 15u);
+  const float4 s = __ldcg(dp_cost + c.code);
+  return i == 1 ? s.x : (i == 2 ? s.y : (i == 3 ? s.z : s.w));
+}
+__global__ void __launch_bounds__(kBlock) k_collapse_dp(int n, const float4* __restrict__ nodes, const int* __restrict__ iparent,
+                                                        const int* __restrict__ lparent, const uint8_t* __restrict__ collapse,
+                                                        uint32_t* visits, float wide_cost, float4* dp_cost, uint32_t* dp_choice, int* err)
+{
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  int p = lparent[j], steps = 0;
+  while (p >= 0) {
+    if (p >= n - 1 || ++steps > kMaxWalk) {
+      atomicExch(err, 1);
+      return;
+    }
+    if (atomicAdd(visits + p, 1u) == 0u) return;
+    __threadfence();
+    if (!collapse[p]) {
+      const Kid a = kid_of(nodes, p, 0), b = kid_of(nodes, p, 1);
+      float D[5];
+      int K[5];
+      for (int i = 2; i <= 4; ++i) {
+        D[i] = INFINITY;
+        K[i] = 1;
+        for (int k = 1; k < i; ++k) {
+          const float c = dp_slot_cost(a, k, dp_cost) + dp_slot_cost(b, i - k, dp_cost);
+          if (c < D[i]) { D[i] = c; K[i] = k; }
+        }
+      }
+      Kid u = a;
+      for (int k = 0; k < 3; ++k) {
+        u.lo[k] = fminf(a.lo[k], b.lo[k]);
+        u.hi[k] = fmaxf(a.hi[k], b.hi[k]);
+      }
+      const float W = wide_cost * kid_area(u) + D[4];
+      float S[5];
+      uint32_t ch = (uint32_t)K[4];
+      S[1] = W;
+      for (int i = 2; i <= 4; ++i) {
+        const bool open = D[i] < W;
+        S[i] = open ? D[i] : W;
+        ch |= (uint32_t)(open ? K[i] : 0) << (8 * (i - 1));
+      }
+      __stcg(dp_cost + p, make_float4(S[1], S[2], S[3], S[4]));
+      __stcg(dp_choice + p, ch);
+    }
+    __threadfence();
+    p = iparent[p];
+  }
+}
+
 // Pass 7: one level of the 4-wide collapse.  Work item (BVH2 node, wide node index); each internal
 // child gets the next wide index from *wide_count and becomes a work item of the next level.  The
 // level's item count is read on the device (*n_in_ptr), so the levels launch back to back; the grid
@@ -631,24 +701,47 @@ __device__ __forceinline__ float kid_area(const Kid& c)
 __global__ void __launch_bounds__(128) k_collapse_level(const float4* __restrict__ nodes, const int2* __restrict__ work_in,
                                                         const uint32_t* __restrict__ n_in_ptr, int2* __restrict__ work_out,
                                                         uint32_t* __restrict__ n_out, uint32_t* __restrict__ wide_count, uint32_t wide_cap,
-                                                        float4* __restrict__ nodes4, uint32_t* __restrict__ overflow)
+                                                        float4* __restrict__ nodes4, uint32_t* __restrict__ overflow,
+                                                        const uint32_t* __restrict__ dp_choice)
 {
   const uint32_t n_in = *n_in_ptr;
   for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < n_in; w += gridDim.x * blockDim.x) {
     const int2 item = work_in[w];
     Kid kids[kWide];
     int nk = 0;
-    kids[nk++] = kid_of(nodes, item.x, 0);
-    kids[nk++] = kid_of(nodes, item.x, 1);
-    while (nk < kWide) {
-      int best = -1;
-      float ba = -1.0f;
-      for (int j = 0; j < nk; ++j)
-        if (kids[j].code >= 0 && kid_area(kids[j]) > ba) { ba = kid_area(kids[j]); best = j; }
-      if (best < 0) break;
-      const int inner = kids[best].code;
-      kids[best] = kid_of(nodes, inner, 0);
-      kids[nk++] = kid_of(nodes, inner, 1);
+    if (dp_choice) {
+      // the children the dynamic program chose: each (BVH2 child, slots) is kept whole or split again
+      struct Open {
+        Kid c;
+        int slots;
+      } todo[kWide];
+      int nt = 0;
+      const int k0 = min(max((int)(dp_choice[item.x] & 0xffu), 1), kWide - 1);
+      todo[nt++] = {kid_of(nodes, item.x, 1), kWide - k0};
+      todo[nt++] = {kid_of(nodes, item.x, 0), k0};
+      while (nt > 0 && nk < kWide) {
+        const Open o = todo[--nt];
+        const int k = o.c.code >= 0 && o.slots >= 2 ? (int)((dp_choice[o.c.code] >> (8 * (o.slots - 1))) & 0xffu) : 0;
+        if (k <= 0 || k >= o.slots || nt + 2 > kWide) {
+          kids[nk++] = o.c;
+        } else {
+          todo[nt++] = {kid_of(nodes, o.c.code, 1), o.slots - k};
+          todo[nt++] = {kid_of(nodes, o.c.code, 0), k};
+        }
+      }
+    } else {
+      kids[nk++] = kid_of(nodes, item.x, 0);
+      kids[nk++] = kid_of(nodes, item.x, 1);
+      while (nk < kWide) {
+        int best = -1;
+        float ba = -1.0f;
+        for (int j = 0; j < nk; ++j)
+          if (kids[j].code >= 0 && kid_area(kids[j]) > ba) { ba = kid_area(kids[j]); best = j; }
+        if (best < 0) break;
+        const int inner = kids[best].code;
+        kids[best] = kid_of(nodes, inner, 0);
+        kids[nk++] = kid_of(nodes, inner, 1);
+      }
     }
     int codes[kWide];
     for (int j = 0; j < kWide; ++j) {
@@ -689,7 +782,7 @@ __global__ void __launch_bounds__(128) k_collapse_level(const float4* __restrict
 // Offsets of the build's temporaries in one scratch allocation (256-byte aligned), kept by the context
 // for later rebuilds.
 struct BuildLayout {
-  size_t tri, blo, bhi, keys_a, keys_b, idx_a, idx_b, hist, rowtot, posof, cb, child, range, ipar, lpar, leafrec, noderec, visits, collapse, depth, work_a,
+  size_t tri, blo, bhi, keys_a, keys_b, idx_a, idx_b, hist, rowtot, posof, dpcost, dpchoice, cb, child, range, ipar, lpar, leafrec, noderec, visits, collapse, depth, work_a,
       work_b, counters, total;
   BuildLayout(uint32_t n, uint32_t nb)
   {
@@ -709,6 +802,8 @@ struct BuildLayout {
     hist = take((size_t)kRadix * nb * 4);
     rowtot = take((size_t)kRadix * 4);
     posof = take((size_t)n * 4);
+    dpcost = take((size_t)(n - 1) * sizeof(float4));
+    dpchoice = take((size_t)(n - 1) * 4);
     cb = take(6 * 4);
     child = take((size_t)(n - 1) * sizeof(int2));
     range = take((size_t)(n - 1) * sizeof(int2));
@@ -750,6 +845,8 @@ pt_status build_bvh_device(Context& c)
   uint32_t *idx_a = (uint32_t*)(base + Lo.idx_a), *idx_b = (uint32_t*)(base + Lo.idx_b);
   uint32_t *hist = (uint32_t*)(base + Lo.hist), *rowtot = (uint32_t*)(base + Lo.rowtot), *cb = (uint32_t*)(base + Lo.cb);
   uint32_t* pos_of = (uint32_t*)(base + Lo.posof);
+  float4* dp_cost = (float4*)(base + Lo.dpcost);
+  uint32_t* dp_choice = (uint32_t*)(base + Lo.dpchoice);
   int2 *child = (int2*)(base + Lo.child), *range = (int2*)(base + Lo.range);
   int *ipar = (int*)(base + Lo.ipar), *lpar = (int*)(base + Lo.lpar);
   NodeRec *leafrec = (NodeRec*)(base + Lo.leafrec), *noderec = (NodeRec*)(base + Lo.noderec);
@@ -793,7 +890,7 @@ pt_status build_bvh_device(Context& c)
   for (int r = 0; r < c.bvh_params.treelet_rounds; ++r) {
     PT_CHECK_CUDA(cudaMemsetAsync(visits, 0, (size_t)(n - 1) * 4, st), "device BVH build");
     k_treelets<<<gl, kBlock, 0, st>>>((int)n, child, ipar, lpar, leafrec, noderec, visits, c.bvh_params.trav_cost, c.bvh_params.max_leaf,
-                                      depth + 1);
+                                      c.bvh_params.treelet_min, depth + 1);
     count_launch();
   }
   if (c.bvh_params.treelet_rounds > 0) {  // the leaf collapse and costs over the final topology
@@ -807,13 +904,21 @@ pt_status build_bvh_device(Context& c)
   k_write_tris<<<gl, kBlock, 0, st>>>((int)n, tri, vin, pos_of, lpar, ipar, collapse, c.d_v0.as<float4>(), c.d_e1.as<float4>(),
                                       c.d_e2.as<float4>(), depth);
   count_launch(3);
+  const bool dp = c.bvh_params.collapse == 1;
+  if (dp) {
+    PT_CHECK_CUDA(cudaMemsetAsync(visits, 0, (size_t)(n - 1) * 4, st), "device BVH build");
+    PT_CHECK_CUDA(cudaMemsetAsync(dp_choice, 0, (size_t)(n - 1) * 4, st), "device BVH build");
+    k_collapse_dp<<<gl, kBlock, 0, st>>>((int)n, c.d_nodes.as<float4>(), ipar, lpar, collapse, visits, c.bvh_params.wide_cost, dp_cost,
+                                         dp_choice, depth + 1);
+    count_launch();
+  }
   // 4-wide collapse: levels 0 .. kMaxDepth4 - 2 (wide depth, root = 1, below kMaxDepth4)
   int2 *win = work_a, *wout = work_b;
   uint64_t cap_items = 1;
   for (int L = 0; L + 1 < kMaxDepth4; ++L) {
     const int grid = grid_for(std::min<uint64_t>(cap_items, n - 1), 128, 8);
     k_collapse_level<<<grid, 128, 0, st>>>(c.d_nodes.as<float4>(), win, cnt + 2 + L, wout, cnt + 3 + L, cnt, n - 1, c.d_nodes4.as<float4>(),
-                                           cnt + 1);
+                                           cnt + 1, dp ? dp_choice : nullptr);
     count_launch();
     std::swap(win, wout);
     cap_items = std::min<uint64_t>(cap_items * 4, (uint64_t)n);

@@ -896,7 +896,7 @@ pt_status pt_set_option(pt_ctx* ctx, const char* name, int64_t value)
     ctx->c.bvh_params.max_leaf = (int)value;
     return PT_OK;
   }
-  if (k == "bvh_collapse") {  // host builder's 4-wide collapse: 0 greedy, 1 SAH-optimal (default); next pt_build
+  if (k == "bvh_collapse") {  // 4-wide collapse of either builder: 0 greedy, 1 SAH-optimal (default); next pt_build
     if (value != 0 && value != 1) return fail(PT_INVALID_ARG, "pt_set_option: bvh_collapse must be 0 or 1");
     ctx->c.bvh_params.collapse = (int)value;
     return PT_OK;
@@ -904,6 +904,11 @@ pt_status pt_set_option(pt_ctx* ctx, const char* name, int64_t value)
   if (k == "bvh_wide_cost_milli") {  // SAH cost of a wide node visit x 1000 (default 1500), for the next pt_build
     if (value < 100 || value > 20000) return fail(PT_INVALID_ARG, "pt_set_option: bvh_wide_cost_milli must be in [100, 20000]");
     ctx->c.bvh_params.wide_cost = (float)value / 1000.0f;
+    return PT_OK;
+  }
+  if (k == "bvh_treelet_min") {  // device builder: smallest subtree (triangles) that forms a treelet (default 8)
+    if (value < 2 || value > 1 << 20) return fail(PT_INVALID_ARG, "pt_set_option: bvh_treelet_min must be in [2, 2^20]");
+    ctx->c.bvh_params.treelet_min = (int)value;
     return PT_OK;
   }
   if (k == "bvh_treelets") {  // device builder: rounds of treelet restructuring (default 3), for the next pt_build

@@ -1,6 +1,6 @@
 """The device BVH builder (option "bvh_builder" = 1: LBVH over Morton codes, treelet restructuring
-(option "bvh_treelets" rounds), SAH leaves and a device 4-wide collapse) against brute force and
-against the host SAH builder.
+(option "bvh_treelets" rounds), SAH leaves and a device 4-wide collapse, SAH-optimal or greedy by option
+"bvh_collapse") against brute force and against the host SAH builder.
 
 Hits are decided by the triangle test alone (closest t, ties to the lower triangle index), so any valid
 tree must give bit-identical closest hits (index, t, barycentrics) and any-hit answers to a brute-force
@@ -82,12 +82,13 @@ def heightfield_scene():
     return sc.SceneData(base.integrator, base.camera, base.background, meshes, base.lights)
 
 
-@pytest.mark.parametrize("treelets", [0, 2])
+@pytest.mark.parametrize("opts", [{"bvh_treelets": 0}, {"bvh_treelets": 2}, {"bvh_treelets": 2, "bvh_collapse": 0}],
+                         ids=["lbvh", "treelets", "treelets-greedy-collapse"])
 @pytest.mark.parametrize("which", ["single_scene", "heightfield", "duplicated"])
-def test_device_bvh_hits_bit_exact_vs_brute_force(which, treelets):
+def test_device_bvh_hits_bit_exact_vs_brute_force(which, opts):
     data = {"single_scene": lambda: scenes.single_scene(width=16, height=16), "heightfield": heightfield_scene,
             "duplicated": duplicated_scene}[which]()
-    R = sc.Renderer(data, build_options=dict(DEVICE, bvh_treelets=treelets))
+    R = sc.Renderer(data, build_options=dict(DEVICE, **opts))
     info = R.build_info()
     print(which, info.as_dict())
     assert info.builder == 1 and info.n_triangles == data.n_triangles
