@@ -340,6 +340,10 @@ struct TreeletShared {
   float area[kTreeletSets];
   float cost[kTreeletSets];
   uint8_t part[kTreeletSets];
+  NodeRec leaf_rec[kTreeletLeaves];
+  float leaf_area[kTreeletLeaves];
+  int leaves[kTreeletLeaves], inner[kTreeletLeaves - 1], node_set[kTreeletLeaves - 1];
+  int nl, used;
 };
 
 __device__ __forceinline__ NodeRec load_rec(const NodeRec* r)
@@ -350,83 +354,145 @@ __device__ __forceinline__ NodeRec load_rec(const NodeRec* r)
   return a;
 }
 
-// One treelet at `root`, processed by the whole warp (root uniform across the warp).
+// The bits of i deposited, lowest first, into the set bits of mask.
+__device__ __forceinline__ int deposit_bits(int i, int mask)
+{
+  int r = 0;
+  for (int b = 0; mask; ++b) {
+    const int low = mask & -mask;
+    r |= ((i >> b) & 1) ? low : 0;
+    mask ^= low;
+  }
+  return r;
+}
+
+// The 127 nonempty subsets of seven leaves ordered by size (then value); subsets of k leaves sit at
+// [set_start(k), set_start(k + 1)).  A treelet of fewer leaves uses the entries that fit in it.
+__constant__ uint8_t kSetsBySize[kTreeletSets - 1] = {
+    1, 2, 4, 8, 16, 32, 64, 3, 5, 6, 9, 10, 12, 17, 18, 20,
+    24, 33, 34, 36, 40, 48, 65, 66, 68, 72, 80, 96, 7, 11, 13, 14,
+    19, 21, 22, 25, 26, 28, 35, 37, 38, 41, 42, 44, 49, 50, 52, 56,
+    67, 69, 70, 73, 74, 76, 81, 82, 84, 88, 97, 98, 100, 104, 112, 15,
+    23, 27, 29, 30, 39, 43, 45, 46, 51, 53, 54, 57, 58, 60, 71, 75,
+    77, 78, 83, 85, 86, 89, 90, 92, 99, 101, 102, 105, 106, 108, 113, 114,
+    116, 120, 31, 47, 55, 59, 61, 62, 79, 87, 91, 93, 94, 103, 107, 109,
+    110, 115, 117, 118, 121, 122, 124, 63, 95, 111, 119, 123, 125, 126, 127};
+__host__ __device__ constexpr int set_start(int k)
+{
+  return k <= 1 ? 0 : k == 2 ? 7 : k == 3 ? 28 : k == 4 ? 63 : k == 5 ? 98 : k == 6 ? 119 : k == 7 ? 126 : 127;
+}
+static_assert(kTreeletLeaves == 7, "the subset table is written for seven leaves");
+
+// The cost and the chosen split of subset `set` from its best split cost.
+__device__ __forceinline__ void treelet_finish(TreeletShared& sh, int set, float best, int bp, float trav_cost, int max_leaf)
+{
+  float n_tris = 0.0f;
+  for (int k = 0; k < sh.nl; ++k) n_tris += ((set >> k) & 1) ? sh.leaf_rec[k].hi.w : 0.0f;
+  const float split = trav_cost * sh.area[set] + best;
+  const float leaf = n_tris <= (float)max_leaf ? sh.area[set] * n_tris : INFINITY;
+  sh.cost[set] = fminf(split, leaf);
+  sh.part[set] = (uint8_t)bp;
+}
+
+// One treelet at `root`, processed by the whole warp (root uniform across the warp).  Each split of a
+// subset is counted once, by the part that holds the subset's lowest leaf.  Subsets of up to five leaves
+// take one lane each; those of six and seven (31 and 63 splits) are shared by the warp and reduced to
+// the least cost (ties to the smaller part).
 __device__ void treelet_optimize(int root, int2* child, int* iparent, int* lparent, const NodeRec* leafrec, NodeRec* noderec,
                                  TreeletShared& sh, float trav_cost, int max_leaf)
 {
   const int lane = threadIdx.x & 31;
-  // form the treelet (every lane the same, from the same records)
-  int leaves[kTreeletLeaves], inner[kTreeletLeaves - 1];
-  NodeRec lrec[kTreeletLeaves];
-  int nl = 0, ni = 0;
-  inner[ni++] = root;
-  {
+  if (lane == 0) {  // form the treelet: open the treelet leaf of largest area while there are fewer than 7
+    int nl = 0, ni = 0;
+    auto put = [&](int k, int code) {
+      const NodeRec r = load_rec(code >= 0 ? noderec + code : leafrec + ~code);
+      sh.leaves[k] = code;
+      sh.leaf_rec[k] = r;
+      sh.leaf_area[k] = code >= 0 ? area_of(r.lo, r.hi) : -1.0f;  // -1: a triangle, never opened
+    };
+    sh.inner[ni++] = root;
     const int2 c = __ldcg(&child[root]);
-    leaves[nl++] = c.x;
-    leaves[nl++] = c.y;
-  }
-  for (int k = 0; k < nl; ++k) lrec[k] = load_rec(leaves[k] >= 0 ? noderec + leaves[k] : leafrec + ~leaves[k]);
-  while (nl < kTreeletLeaves) {
-    int best = -1;
-    float ba = -1.0f;
-    for (int k = 0; k < nl; ++k) {
-      if (leaves[k] < 0) continue;
-      const float a = area_of(lrec[k].lo, lrec[k].hi);
-      if (a > ba) { ba = a; best = k; }
+    put(nl++, c.x);
+    put(nl++, c.y);
+    while (nl < kTreeletLeaves) {
+      int best = -1;
+      float ba = -1.0f;
+      for (int k = 0; k < nl; ++k)
+        if (sh.leaf_area[k] > ba) { ba = sh.leaf_area[k]; best = k; }
+      if (best < 0) break;
+      const int x = sh.leaves[best];
+      sh.inner[ni++] = x;
+      const int2 g = __ldcg(&child[x]);
+      put(best, g.x);
+      put(nl++, g.y);
     }
-    if (best < 0) break;
-    const int x = leaves[best];
-    inner[ni++] = x;
-    const int2 c = __ldcg(&child[x]);
-    leaves[best] = c.x;
-    lrec[best] = load_rec(c.x >= 0 ? noderec + c.x : leafrec + ~c.x);
-    leaves[nl] = c.y;
-    lrec[nl] = load_rec(c.y >= 0 ? noderec + c.y : leafrec + ~c.y);
-    ++nl;
+    sh.nl = nl;
   }
+  __syncwarp();
+  const int nl = sh.nl;
   const int full = (1 << nl) - 1;
   // subset areas and the treelet leaves' own costs
   for (int set = lane + 1; set <= full; set += 32) {
     float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (int k = 0; k < nl; ++k) {
       if (!((set >> k) & 1)) continue;
-      lo[0] = fminf(lo[0], lrec[k].lo.x); lo[1] = fminf(lo[1], lrec[k].lo.y); lo[2] = fminf(lo[2], lrec[k].lo.z);
-      hi[0] = fmaxf(hi[0], lrec[k].hi.x); hi[1] = fmaxf(hi[1], lrec[k].hi.y); hi[2] = fmaxf(hi[2], lrec[k].hi.z);
+      const NodeRec& r = sh.leaf_rec[k];
+      lo[0] = fminf(lo[0], r.lo.x); lo[1] = fminf(lo[1], r.lo.y); lo[2] = fminf(lo[2], r.lo.z);
+      hi[0] = fmaxf(hi[0], r.hi.x); hi[1] = fmaxf(hi[1], r.hi.y); hi[2] = fmaxf(hi[2], r.hi.z);
     }
     const float dx = fmaxf(0.0f, hi[0] - lo[0]), dy = fmaxf(0.0f, hi[1] - lo[1]), dz = fmaxf(0.0f, hi[2] - lo[2]);
     sh.area[set] = dx * dy + dy * dz + dz * dx;
     if (__popc(set) == 1) {
-      const int k = __ffs(set) - 1;
-      sh.cost[set] = sh.area[set] * lrec[k].lo.w;
+      sh.cost[set] = sh.area[set] * sh.leaf_rec[__ffs(set) - 1].lo.w;
       sh.part[set] = 0;
     }
   }
   __syncwarp();
-  // subsets by increasing size: every split of a subset is into smaller ones
-  for (int size = 2; size <= nl; ++size) {
-    for (int set = lane + 1; set <= full; set += 32) {
-      if (__popc(set) != size) continue;
-      const int low = set & -set;  // each split once: the part holding the lowest leaf
+  // subsets by increasing size (every split of a subset is into smaller ones): up to five leaves one
+  // subset per lane, six and seven leaves (8 subsets, 31 or 63 splits) shared by the warp
+  for (int size = 2; size <= nl && size <= 5; ++size) {
+    for (int e = set_start(size) + lane; e < set_start(size + 1); e += 32) {
+      const int set = kSetsBySize[e];
+      if (set > full) continue;
+      const int low = set & -set, rest = set ^ low;
       float best = INFINITY;
       int bp = low;
-      for (int part = (set - 1) & set; part; part = (part - 1) & set) {
-        if (!(part & low)) continue;
+      for (int sub = (rest - 1) & rest;; sub = (sub - 1) & rest) {  // the proper subsets of rest
+        const int part = low | sub;
         const float c = sh.cost[part] + sh.cost[set ^ part];
         if (c < best) { best = c; bp = part; }
+        if (sub == 0) break;
       }
-      float n_tris = 0.0f;
-      for (int k = 0; k < nl; ++k) n_tris += ((set >> k) & 1) ? lrec[k].hi.w : 0.0f;
-      const float split = trav_cost * sh.area[set] + best;
-      const float leaf = n_tris <= (float)max_leaf ? sh.area[set] * n_tris : INFINITY;
-      sh.cost[set] = fminf(split, leaf);
-      sh.part[set] = (uint8_t)bp;
+      treelet_finish(sh, set, best, bp, trav_cost, max_leaf);
     }
     __syncwarp();
   }
-  // rebuild the treelet on its internal nodes (lane 0): pre-order assignment, then the records
-  // bottom-up (reverse of the assignment order)
+  for (int size = 6; size <= nl; ++size) {
+    for (int e = set_start(size); e < set_start(size + 1); ++e) {
+      const int set = kSetsBySize[e];
+      if (set > full) continue;
+      const int low = set & -set, rest = set ^ low;
+      const int n_split = (1 << (size - 1)) - 1;
+      float best = INFINITY;
+      int bp = low;
+      for (int i = lane; i < n_split; i += 32) {
+        const int part = low | deposit_bits(i, rest);
+        const float c = sh.cost[part] + sh.cost[set ^ part];
+        if (c < best || (c == best && part < bp)) { best = c; bp = part; }
+      }
+      for (int off = 16; off > 0; off >>= 1) {
+        const float ob = __shfl_xor_sync(0xffffffffu, best, off);
+        const int op = __shfl_xor_sync(0xffffffffu, bp, off);
+        if (ob < best || (ob == best && op < bp)) { best = ob; bp = op; }
+      }
+      if (lane == 0) treelet_finish(sh, set, best, bp, trav_cost, max_leaf);
+    }
+    __syncwarp();
+  }
+  // rebuild the treelet on its internal nodes: the pre-order assignment (lane 0), then each rewired
+  // node's record from the treelet leaves it covers (one lane per node)
   if (lane == 0) {
-    int node_set[kTreeletLeaves - 1];
+    int* node_set = sh.node_set;
     int used = 1;
     node_set[0] = full;
     for (int q = 0; q < used; ++q) {
@@ -436,34 +502,39 @@ __device__ void treelet_optimize(int root, int2* child, int* iparent, int* lpare
       const int sides[2] = {a, b};
       for (int h = 0; h < 2; ++h) {
         if (__popc(sides[h]) == 1) {
-          code[h] = leaves[__ffs(sides[h]) - 1];
+          code[h] = sh.leaves[__ffs(sides[h]) - 1];
         } else {
           node_set[used] = sides[h];
-          code[h] = inner[used++];
+          code[h] = sh.inner[used++];
         }
-        if (code[h] >= 0) iparent[code[h]] = inner[q];
-        else lparent[~code[h]] = inner[q];
+        if (code[h] >= 0) iparent[code[h]] = sh.inner[q];
+        else lparent[~code[h]] = sh.inner[q];
       }
-      __stcg(&child[inner[q]], make_int2(code[0], code[1]));
+      __stcg(&child[sh.inner[q]], make_int2(code[0], code[1]));
     }
-    // each rewired node's record from the treelet leaves it covers (already in registers)
-    for (int q = 0; q < used; ++q) {
-      const int set = node_set[q];
+    sh.used = used;
+  }
+  __syncwarp();
+  {
+    const int q = lane;
+    if (q < sh.used) {
+      const int set = sh.node_set[q];
       NodeRec m;
       m.lo = make_float4(INFINITY, INFINITY, INFINITY, 0.0f);
       m.hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.0f);
       float cost_sum = 0.0f;
       for (int k = 0; k < nl; ++k) {
         if (!((set >> k) & 1)) continue;
-        m.lo.x = fminf(m.lo.x, lrec[k].lo.x); m.lo.y = fminf(m.lo.y, lrec[k].lo.y); m.lo.z = fminf(m.lo.z, lrec[k].lo.z);
-        m.hi.x = fmaxf(m.hi.x, lrec[k].hi.x); m.hi.y = fmaxf(m.hi.y, lrec[k].hi.y); m.hi.z = fmaxf(m.hi.z, lrec[k].hi.z);
-        m.hi.w += lrec[k].hi.w;
-        cost_sum += lrec[k].lo.w;
+        const NodeRec& r = sh.leaf_rec[k];
+        m.lo.x = fminf(m.lo.x, r.lo.x); m.lo.y = fminf(m.lo.y, r.lo.y); m.lo.z = fminf(m.lo.z, r.lo.z);
+        m.hi.x = fmaxf(m.hi.x, r.hi.x); m.hi.y = fmaxf(m.hi.y, r.hi.y); m.hi.z = fmaxf(m.hi.z, r.hi.z);
+        m.hi.w += r.hi.w;
+        cost_sum += r.lo.w;
       }
       const float A = area_of(m.lo, m.hi);
       m.lo.w = A > 0.0f ? sh.cost[set] / A : cost_sum;  // cost per area, as pass 5 keeps it
-      __stcg(&noderec[inner[q]].lo, m.lo);
-      __stcg(&noderec[inner[q]].hi, m.hi);
+      __stcg(&noderec[sh.inner[q]].lo, m.lo);
+      __stcg(&noderec[sh.inner[q]].hi, m.hi);
     }
   }
   __syncwarp();
