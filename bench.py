@@ -139,45 +139,76 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def ncu_record(name):
+    """Totals per metric over the launches of a committed ncu record under profiles/ (the tool's CSV:
+    either one row per (launch, metric) from `--csv --log-file`, or one row per launch from
+    `ncu -i ... --page raw --csv`), and the `# key: value` header lines above it.  None if absent."""
+    import csv
+
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None
+    header, rows = {}, []
+    with open(path) as fh:
+        for line in fh:
+            if line.startswith("#"):
+                if ":" in line:
+                    k, v = line[1:].split(":", 1)
+                    header[k.strip()] = v.strip()
+                continue
+            rows.append(line)
+    table = list(csv.reader(rows))
+    if len(table) < 2:
+        return None
+    head = table[0]
+    totals, launches = {}, set()
+    num = lambda x: float(x.replace(",", ""))
+    if "Metric Name" in head:
+        k_id, k_name, k_val = head.index("ID"), head.index("Metric Name"), head.index("Metric Value")
+        for r in table[1:]:
+            if len(r) == len(head):
+                launches.add(r[k_id])
+                totals[r[k_name]] = totals.get(r[k_name], 0.0) + num(r[k_val])
+    else:
+        first = head.index("CC") + 1
+        for r in table[2:]:  # row 1 holds the units
+            if len(r) != len(head):
+                continue
+            launches.add(r[head.index("ID")])
+            for k in range(first, len(head)):
+                totals[head[k]] = totals.get(head[k], 0.0) + num(r[k])
+    return {"totals": totals, "launches": len(launches), "header": header}
+
+
 def extend_capture_record():
     """Per-segment figures of the extend kernel from its committed ncu record
     (profiles/k_extend_single_scene_ncu.csv: the raw ncu rows of every k_extend_persistent launch of the
     first render of the capture command, preceded by '#' lines that give the segments those launches
     traced, from the same command's JSON line).  Returns {"warp_inst_per_segment",
     "thread_inst_per_warp_inst", "dram_bytes_per_segment", "segments", "launches"} or None."""
-    import csv
+    rec = ncu_record("k_extend_single_scene_ncu.csv")
+    if not rec or "segments" not in rec["header"]:
+        return None
+    segments = float(rec["header"]["segments"].split()[0].replace(",", ""))
+    t = rec["totals"]
+    warp = t.get("smsp__inst_executed.sum", 0.0)
+    if warp <= 0 or segments <= 0:
+        return None
+    dram = t["dram__bytes_read.sum"] + t["dram__bytes_write.sum"]
+    return {"warp_inst_per_segment": warp / segments, "thread_inst_per_warp_inst": t["smsp__thread_inst_executed.sum"] / warp,
+            "dram_bytes_per_segment": dram / segments, "segments": segments, "launches": rec["launches"]}
 
-    path = os.path.join(ROOT, "profiles", "k_extend_single_scene_ncu.csv")
-    if not os.path.exists(path):
+
+def bsdf_capture_record():
+    """Per-query figures of the BSDF-query kernels from their committed ncu record
+    (profiles/k_bsdf_queries_c1_ncu.csv: both launches of one step, the query count in its header)."""
+    rec = ncu_record("k_bsdf_queries_c1_ncu.csv")
+    if not rec or "queries" not in rec["header"]:
         return None
-    segments = None
-    rows = []
-    with open(path) as fh:
-        for line in fh:
-            if line.startswith("#"):
-                if "segments:" in line:
-                    segments = float(line.split("segments:", 1)[1].split()[0].replace(",", ""))
-                continue
-            rows.append(line)
-    table = list(csv.reader(rows))
-    if segments is None or len(table) < 2:
-        return None
-    # ncu --csv --log-file: one row per (launch, metric) with columns ID, Metric Name, Metric Value
-    head = table[0]
-    k_id, k_name, k_val = head.index("ID"), head.index("Metric Name"), head.index("Metric Value")
-    totals, launches = {}, set()
-    for r in table[1:]:
-        if len(r) != len(head):
-            continue
-        launches.add(r[k_id])
-        totals[r[k_name]] = totals.get(r[k_name], 0.0) + float(r[k_val].replace(",", ""))
-    warp = totals.get("smsp__inst_executed.sum", 0.0)
-    if warp <= 0:
-        return None
-    thread = totals["smsp__thread_inst_executed.sum"]
-    dram = totals["dram__bytes_read.sum"] + totals["dram__bytes_write.sum"]
-    return {"warp_inst_per_segment": warp / segments, "thread_inst_per_warp_inst": thread / warp, "dram_bytes_per_segment": dram / segments,
-            "segments": segments, "launches": len(launches)}
+    q = float(rec["header"]["queries"])
+    t = rec["totals"]
+    return {"warp_inst_per_query": t["smsp__inst_executed.sum"] / q,
+            "dram_bytes_per_query": (t["dram__bytes_read.sum"] + t["dram__bytes_write.sum"]) / q, "launches": rec["launches"]}
 
 
 class ClockSampler:
@@ -449,7 +480,11 @@ def run_bsdf(args, world, rank, local):
     peak, peak_kind = load_peaks()
     launch_ms = ms_max / args.steps
     achieved = BSDF_BYTES_PER_QUERY * n / (launch_ms * 1e-3) / 1e9
-    per_q = profile_figure("k_bsdf_queries_c1.md", "traffic_bytes_per_query:")
+    rec = bsdf_capture_record()
+    sm_mhz = clocks.summary().get("sm_mhz") or 1965.0
+    n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+    issue_peak = n_sm * 4 * sm_mhz * 1e6 / 1e9
+    issue_achieved = rec["warp_inst_per_query"] * n / (launch_ms * 1e-3) / 1e9 if rec else None
     line = {
         "metric": "M BSDF queries/s (batched BSDF queries on 1 B200)", "value": value, "unit": "M queries/s", "n_gpus": world,
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": launch_ms, "higher_is_better": True, "scaling": "weak",
@@ -459,12 +494,17 @@ def run_bsdf(args, world, rank, local):
         "e2e": {"value": e2e_value, "unit": "M queries/s", "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 24 * n,
                 "what": "pt_bsdf_queries_host from pinned host buffers (copies in, kernel, copies out, synchronous)",
                 "identical_to_device_path": same},
-        "roofline": {"bound": "hbm", "kernel": "k_bsdf_queries", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind,
-                     "traffic": per_q * n if per_q else None,
-                     "traffic_unit": "bytes per launch (ncu capture of the same launch size)",
-                     "note": "the kernel is bound by instruction issue (16-round TEA, transcendentals, the Beckmann Newton loop and "
-                             "double erfinv), not by its 40 algorithmic bytes per query"},
+        "roofline": {"bound": "issue", "kernel": "k_bsdf_queries (GGX and Beckmann launches of one step)",
+                     "achieved": issue_achieved, "peak": issue_peak, "unit": "G warp instructions/s",
+                     "frac": issue_achieved / issue_peak if issue_achieved else None,
+                     "peak_source": "1 warp instruction / clock / SM sub-partition x 4 x %d SMs x median SM clock %.0f MHz" % (n_sm, sm_mhz),
+                     "warp_instructions_per_query": rec["warp_inst_per_query"] if rec else None,
+                     "traffic": rec["dram_bytes_per_query"] * n if rec else None,
+                     "traffic_unit": "DRAM bytes per step (ncu record of the same launch size, profiles/k_bsdf_queries_c1_ncu.csv)",
+                     "hbm": {"achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                             "algorithmic_bytes_per_query": BSDF_BYTES_PER_QUERY},
+                     "note": "the kernels are bound by instruction issue (16-round TEA, transcendentals, the Beckmann Newton loop and "
+                             "double erfinv), not by their 40 algorithmic bytes per query"},
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
     }
@@ -611,20 +651,6 @@ def run_reference_ingest(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "u8/f32", "data": "synthetic", "config": {"workload": INGEST},
             "cpu_baseline": s, "e2e": {"value": s["value"], "unit": "MB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-
-
-def profile_figure(name, key):
-    """A figure written as `key value` in a committed ncu summary under profiles/."""
-    path = os.path.join(ROOT, "profiles", name)
-    if not os.path.exists(path):
-        return None
-    for line in open(path):
-        if line.startswith(key):
-            try:
-                return float(line.split(":", 1)[1].strip())
-            except ValueError:
-                return None
-    return None
 
 
 def run_reference(args, world, rank):
