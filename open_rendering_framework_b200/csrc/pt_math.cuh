@@ -164,7 +164,9 @@ PT_HD float3 to_world(const float3& w, const float3& n)  // helpers.h:294-299
 }
 // Double-precision erfinv of helpers.h:301-377: M. Giles, "Approximating the erfinv function",
 // GPU Computing Gems Jade Edition (2011), three polynomial branches in w = -log((1-x)(1+x)).
-PT_HD double erfinv_giles(double x)
+// One out-of-line copy: the Beckmann sampler calls it three times, and inlined copies (a double log
+// and three long polynomials each) crowded the instruction cache of the kernels that use it.
+static __host__ __device__ __noinline__ double erfinv_giles(double x)
 {
   double w = -log((1.0 - x) * (1.0 + x)), p;
   if (w < 6.25) {
