@@ -723,8 +723,8 @@ __global__ void __launch_bounds__(kBinThreads) k_bin_count(WfDev w)
   }
 }
 
-// One block of 1024 threads: per class, the exclusive scan of the chunk counts (in place, chunk order)
-// and the class totals (the material queue counts).
+// One block of 1024 threads per class q (blockIdx.x): the exclusive scan of the class's chunk counts
+// (in place, chunk order) and its total (the material queue count).
 __global__ void __launch_bounds__(1024) k_bin_scan(WfDev w, uint32_t chunk)
 {
   __shared__ uint32_t warp_sum[32];
@@ -732,7 +732,8 @@ __global__ void __launch_bounds__(1024) k_bin_scan(WfDev w, uint32_t chunk)
   const uint32_t chunks = (n + chunk - 1) / chunk;
   const uint32_t per = (chunks + 1023) / 1024;  // consecutive chunks per thread
   const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-  for (int q = 0; q < kQueues; ++q) {
+  {
+    const int q = blockIdx.x;
     uint32_t v = 0;
     for (uint32_t j = 0; j < per; ++j) {
       const uint32_t k = t * per + j;
@@ -764,7 +765,6 @@ __global__ void __launch_bounds__(1024) k_bin_scan(WfDev w, uint32_t chunk)
       }
     }
     if (t == 0) w.cnt[CNT_Q_MISS + q] = warp_sum[31];
-    __syncthreads();
   }
 }
 
@@ -818,7 +818,7 @@ template <int kItems>
 static void launch_binning(const WfDev& w, int grid, cudaStream_t st)
 {
   k_bin_count<kItems><<<grid, kBinThreads, 0, st>>>(w);
-  k_bin_scan<<<1, 1024, 0, st>>>(w, bin_chunk(kItems));
+  k_bin_scan<<<kQueues, 1024, 0, st>>>(w, bin_chunk(kItems));
   k_bin_scatter<kItems><<<grid, kBinThreads, 0, st>>>(w);
 }
 
