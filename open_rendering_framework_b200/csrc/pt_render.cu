@@ -46,6 +46,12 @@ constexpr int kWarps = kBlock / 32;
 #define PT_TRACE_MIN_BLOCKS (1024 / PT_TRACE_BLOCK)
 #endif
 constexpr int kTraceBlock = PT_TRACE_BLOCK;
+// The 4-wide persistent kernels alternate warp-wide phases of leaf tests and node steps.  Closest hit:
+// a leaf phase once the lanes holding a leaf are at least twice those that can take a node step
+// (leaf tests wait for more company); any hit: once they are at least half of them (an occluder found
+// early ends the ray).  Measured against "at least as many" on the single-scene render: +0.5 %.
+constexpr int kLeafVsNodeClosest = 2;
+constexpr int kLeafVsNodeAny = 2;
 // Per-path metadata in rng.w
 constexpr uint32_t META_DEPTH = 0xffffu;
 constexpr uint32_t META_EMIT = 1u << 16;
@@ -595,14 +601,15 @@ __global__ void __launch_bounds__(kTraceBlock, PT_TRACE_MIN_BLOCKS) k_extend_per
     }
     if (__ballot_sync(0xffffffffu, has) == 0) break;
     for (;;) {
-      // a warp-wide phase: intersect the postponed leaves when at least as many lanes hold leaves as can
-      // take a node step, else advance the lanes without leaves by one node
+      // a warp-wide phase: intersect the postponed leaves (4-wide: when the lanes holding leaves are at
+      // least kLeafVsNodeClosest times those that can take a node step; BVH2: at least as many), else
+      // advance the lanes without leaves by one node
       if constexpr (kW4) {
         const bool lp = has && cur < 0;
         const bool np = has && cur >= 0 && cur != kDone4;
         const unsigned lmask = __ballot_sync(0xffffffffu, lp);
         const unsigned nmask = __ballot_sync(0xffffffffu, np);
-        if (lmask && (nmask == 0 || __popc(lmask) >= __popc(nmask))) {
+        if (lmask && (nmask == 0 || __popc(lmask) >= kLeafVsNodeClosest * __popc(nmask))) {
           if (lp) {
             leaf_closest(g, (uint32_t)cur, o, d, eps, h);
             cur = stack4_next(s4, h.t, true);
@@ -907,7 +914,7 @@ __global__ void __launch_bounds__(kTraceBlock, PT_TRACE_MIN_BLOCKS) k_shadow_per
         const bool np = has && res == 0 && cur >= 0 && cur != kDone4;
         const unsigned lmask = __ballot_sync(0xffffffffu, lp);
         const unsigned nmask = __ballot_sync(0xffffffffu, np);
-        if (lmask && (nmask == 0 || __popc(lmask) >= __popc(nmask))) {
+        if (lmask && (nmask == 0 || kLeafVsNodeAny * __popc(lmask) >= __popc(nmask))) {
           if (lp) {
             if (leaf_any(g, (uint32_t)cur, o, d, tmin, tmax)) res = 1;
             else cur = stack4_next(s4, tmax, false);
