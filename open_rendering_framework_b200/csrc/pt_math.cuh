@@ -339,8 +339,9 @@ PT_D Cx csqrt_polar(const Cx& c)  // :195-202
   sincos(th, &s, &co);
   return Cx{ab * co, ab * s};
 }
-// One channel of fresnel_MyComplex_R, Fresnel.h:78-91.
-PT_D float fresnel_complex1(float ci, float si, const Cx& e)
+// One channel of fresnel_MyComplex_R, Fresnel.h:78-91.  Out of line: its three inlined copies per
+// conductor (double atan, sincos and divisions each) crowded the conductor kernel's instruction cache.
+static __device__ __noinline__ float fresnel_complex1(float ci, float si, const Cx& e)
 {
   Cx st{e.re * (double)si, e.im * (double)si};
   Cx p2 = csq_polar(st);
