@@ -348,6 +348,9 @@ pt_status pt_get_render_stats(pt_ctx* ctx, pt_render_stats* out);
  *   "overlap"      1 = each bounce's shading kernels run on two streams and its shadow rays are traced
  *                  beside the next bounce's extend and binning (default); 0 = every launch in order on
  *                  the context stream.  Images are identical either way.
+ *   "dual"         1 = a pass without translucent materials splits its paths into chunks of half the
+ *                  wavefront and runs them two at a time on two wavefronts with streams of their own
+ *                  (default); 0 = one wavefront.  Images are identical either way.
  *   "bvh4"         1 = the persistent kernels walk the 4-wide BVH (default), 0 = the BVH2
  *   "bvh_trav_cost_milli"  SAH cost of a node step x 1000 relative to a triangle test (default 1200) and
  *   "bvh_max_leaf"         the largest leaf the SAH may choose (1..15, default 8): applied by the next pt_build

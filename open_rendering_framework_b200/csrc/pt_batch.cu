@@ -58,13 +58,16 @@ std::vector<uint64_t> graph_key(const Context& E, const PassLayout& L)
     k.push_back(L.chunk_pixels[i]);
     k.push_back(L.chunk_sets[i]);
   }
-  for (const void* p : {E.wf.rays.p, E.wf.state.p, E.wf.g_a.p, E.wf.probes.p, E.d_scene_tab.p, E.d_item_tab.p, E.wf.counters.p, E.wf.path_item.p})
+  for (const void* p : {E.wf.rays.p, E.wf.state.p, E.wf.g_a.p, E.wf.probes.p, E.d_scene_tab.p, E.d_item_tab.p, E.wf.counters.p, E.wf.path_item.p,
+                        E.wf2.rays.p, E.wf2.state.p, E.wf2.counters.p, E.wf2.path_item.p})
     k.push_back((uint64_t)(uintptr_t)p);
   k.push_back(E.wf.cap);
   k.push_back((uint64_t)E.opt.extend_mode);
   k.push_back((uint64_t)E.opt.refill);
   k.push_back((uint64_t)E.opt.bin_items);
   k.push_back((uint64_t)E.opt.overlap);
+  k.push_back((uint64_t)E.opt.dual);
+  k.push_back((uint64_t)L.dual);
   k.push_back((uint64_t)E.pass_w4);
   return k;
 }
@@ -93,7 +96,7 @@ pt_status plan(pt_batch* b, PassLayout& L, std::vector<SceneDev>& tab, uint64_t&
     samples += scene_path_samples(c, nf);
   }
   PT_CHECK_CUDA(cudaSetDevice(E.device), "cudaSetDevice");
-  L = plan_pass(facts, reqs, E.max_paths);
+  L = plan_pass(facts, reqs, E.max_paths, E.opt.dual != 0);
   return PT_OK;
 }
 
@@ -258,7 +261,7 @@ pt_status pt_batch_render_sequential(pt_batch* b)
   for (size_t k = 0; k < b->scenes.size(); ++k) {
     Context& c = b->scenes[k]->c;
     SceneFacts f = scene_facts(c);
-    PassLayout L = plan_pass({f}, {ItemReq{0, c.next_frame, b->frames[k]}}, E.max_paths);
+    PassLayout L = plan_pass({f}, {ItemReq{0, c.next_frame, b->frames[k]}}, E.max_paths, E.opt.dual != 0);
     one[0] = c.view();
     pt_status st = pass_resources(E, L, one);
     if (st == PT_OK) st = launch_pass(E, L, one, false, false);

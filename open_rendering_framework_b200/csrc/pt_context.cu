@@ -409,9 +409,10 @@ pt_status pt_context_destroy(pt_ctx* ctx)
     if (ev) cudaEventDestroy(ev);
   for (cudaEvent_t ev : c.prof_events)
     if (ev) cudaEventDestroy(ev);
-  for (cudaEvent_t ev : {c.ev_fork, c.ev_join, c.ev_shade, c.ev_shadow})
+  for (cudaEvent_t ev : {c.ev_fork, c.ev_join, c.ev_shade, c.ev_shadow, c.ev2_fork, c.ev2_join, c.ev2_shade, c.ev2_shadow, c.ev_start,
+                         c.ev_acc, c.ev_end2})
     if (ev) cudaEventDestroy(ev);
-  for (cudaStream_t sd : c.side)
+  for (cudaStream_t sd : {c.side[0], c.side[1], c.side2[0], c.side2[1], c.stream2})
     if (sd) cudaStreamDestroy(sd);
   cudaStream_t s = c.stream;
   delete ctx;  // frees device buffers
@@ -935,6 +936,9 @@ pt_status pt_set_option(pt_ctx* ctx, const char* name, int64_t value)
   } else if (k == "bin_items") {
     if (value != 4 && value != 8 && value != 16) return fail(PT_INVALID_ARG, "pt_set_option: bin_items must be 4, 8 or 16");
     ctx->c.opt.bin_items = (int)value;
+  } else if (k == "dual") {
+    if (value != 0 && value != 1) return fail(PT_INVALID_ARG, "pt_set_option: dual must be 0 or 1");
+    ctx->c.opt.dual = (int)value;
   } else if (k == "overlap") {
     if (value != 0 && value != 1) return fail(PT_INVALID_ARG, "pt_set_option: overlap must be 0 or 1");
     ctx->c.opt.overlap = (int)value;

@@ -156,6 +156,7 @@ struct PassLayout {
   uint64_t cap_paths = 0, cap_probes = 0, cap_sets = 0;
   int passes = 0;
   bool sss = false;
+  bool dual = false;     // chunks alternate between two wavefronts that run at once (two pipelines)
   bool layered = false;  // some scene of the pass has layered materials (k_shade_layered is launched)
   bool ms = false;       // some scene of the pass has multiple-scattering conductors or dielectrics
   uint32_t g_slots = 0;
@@ -170,6 +171,8 @@ struct Options {
   int bin_items = 8;    // material binning: queue positions per thread (4, 8 or 16; 256 threads per chunk)
   int overlap = 1;      // 1: a bounce's shading classes on two streams and its shadow rays beside the next
                         // bounce's extend and binning; 0: every launch in order on the context stream
+  int dual = 1;         // 1: passes without translucent materials split their paths into chunks of half the
+                        // wavefront that run two at a time on two wavefronts (two pipelines); 0: one wavefront
 };
 
 struct Context {
@@ -244,6 +247,13 @@ struct Context {
   // graph capture)
   cudaStream_t side[2] = {nullptr, nullptr};
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_shade = nullptr, ev_shadow = nullptr;
+  // the second pipeline of dual passes: its wavefront, its three streams and events, and the events
+  // that start it after the context stream, order the chunks' accumulations and join it back
+  Wavefront wf2;
+  cudaStream_t stream2 = nullptr, side2[2] = {nullptr, nullptr};
+  cudaEvent_t ev2_fork = nullptr, ev2_join = nullptr, ev2_shade = nullptr, ev2_shadow = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_acc = nullptr, ev_end2 = nullptr;
+  bool pass_dual = false;  // the last pass ran two pipelines (its counters are in wf and wf2)
   bool profile = false;
   std::vector<cudaEvent_t> prof_events;  // pairs around each extend and gather launch when profiling
   std::vector<int> prof_kind;            // PROF_EXTEND or PROF_GATHER per pair
@@ -269,7 +279,9 @@ pt_status env_reserve(Context& c, uint32_t width, uint32_t height);
 pt_status env_build_tables(Context& c, uint32_t width, uint32_t height);
 // What the pass planner needs to know of a scene (its size, translucent objects, layered materials).
 SceneFacts scene_facts(const Context& c);
-PassLayout plan_pass(const std::vector<SceneFacts>& facts, const std::vector<ItemReq>& reqs, uint64_t max_paths);
+// dual: a pass without translucent materials is planned in chunks of at most max_paths / 2 paths that
+// launch_pass runs two at a time (PassLayout::dual).
+PassLayout plan_pass(const std::vector<SceneFacts>& facts, const std::vector<ItemReq>& reqs, uint64_t max_paths, bool dual = false);
 pt_status pass_resources(Context& E, const PassLayout& L, const std::vector<SceneDev>& scenes);
 pt_status launch_pass(Context& E, const PassLayout& L, const std::vector<SceneDev>& tab, bool multi, bool allow_events, bool adjoint = false);
 

@@ -2295,9 +2295,8 @@ __global__ void k_geo_normals(SceneDev S, float4* geo)
   }
 }
 
-static pt_status ensure_wavefront(Context& c, uint64_t cap)
+static pt_status ensure_wavefront(Wavefront& wf, uint64_t cap)
 {
-  Wavefront& wf = c.wf;
   if (wf.cap >= cap && wf.counters.p) return PT_OK;
   pt_status st = PT_OK;
   const size_t f4 = sizeof(float4), u4 = sizeof(uint4);
@@ -2441,7 +2440,7 @@ SceneFacts scene_facts(const Context& c)
   return f;
 }
 
-PassLayout plan_pass(const std::vector<SceneFacts>& facts, const std::vector<ItemReq>& reqs, uint64_t max_paths)
+PassLayout plan_pass(const std::vector<SceneFacts>& facts, const std::vector<ItemReq>& reqs, uint64_t max_paths, bool dual)
 {
   PassLayout L;
   uint32_t max_pixels = 1;
@@ -2456,6 +2455,10 @@ PassLayout plan_pass(const std::vector<SceneFacts>& facts, const std::vector<Ite
     }
   }
   if (L.sss) max_paths = std::min<uint64_t>(max_paths, std::max<uint64_t>(max_pixels, (4ull << 30) / ((uint64_t)L.g_slots * 40)));
+  if (dual && !L.sss) {
+    L.dual = true;
+    max_paths = std::max<uint64_t>(1, max_paths / 2);
+  }
   uint64_t paths = 0, probes = 0, pix = 0;
   uint32_t sets = 0;
   auto close_chunk = [&]() {
@@ -2510,7 +2513,8 @@ PassLayout plan_pass(const std::vector<SceneFacts>& facts, const std::vector<Ite
 // E's stream).  Nothing here may run while E's stream is being captured.
 pt_status pass_resources(Context& E, const PassLayout& L, const std::vector<SceneDev>& scenes)
 {
-  pt_status st = ensure_wavefront(E, L.cap_paths);
+  pt_status st = ensure_wavefront(E.wf, L.cap_paths);
+  if (st == PT_OK && L.dual) st = ensure_wavefront(E.wf2, L.cap_paths);
   if (st == PT_OK && L.sss) st = ensure_sss(E, E.wf.cap, L.g_slots, L.cap_probes, L.cap_sets);
   if (st == PT_OK) st = E.d_scene_tab.reserve(scenes.size() * sizeof(SceneDev), "scene table");
   if (st == PT_OK) st = E.d_item_tab.reserve(std::max<size_t>(L.items.size(), 1) * sizeof(ItemDev), "item table");
@@ -2522,6 +2526,12 @@ pt_status pass_resources(Context& E, const PassLayout& L, const std::vector<Scen
     if (!sd) PT_CHECK_CUDA(cudaStreamCreateWithFlags(&sd, cudaStreamNonBlocking), "side stream");
   for (cudaEvent_t* ev : {&E.ev_fork, &E.ev_join, &E.ev_shade, &E.ev_shadow})
     if (!*ev) PT_CHECK_CUDA(cudaEventCreateWithFlags(ev, cudaEventDisableTiming), "stream event");
+  if (L.dual) {
+    for (cudaStream_t* sd : {&E.stream2, &E.side2[0], &E.side2[1]})
+      if (!*sd) PT_CHECK_CUDA(cudaStreamCreateWithFlags(sd, cudaStreamNonBlocking), "second pipeline stream");
+    for (cudaEvent_t* ev : {&E.ev2_fork, &E.ev2_join, &E.ev2_shade, &E.ev2_shadow, &E.ev_start, &E.ev_acc, &E.ev_end2})
+      if (!*ev) PT_CHECK_CUDA(cudaEventCreateWithFlags(ev, cudaEventDisableTiming), "stream event");
+  }
   PT_CHECK_CUDA(cudaMemcpyAsync(E.d_scene_tab.p, scenes.data(), scenes.size() * sizeof(SceneDev), cudaMemcpyHostToDevice, E.stream), "scene table");
   PT_CHECK_CUDA(cudaMemcpyAsync(E.d_item_tab.p, L.items.data(), L.items.size() * sizeof(ItemDev), cudaMemcpyHostToDevice, E.stream), "item table");
   return PT_OK;
@@ -2553,45 +2563,59 @@ pt_status launch_pass(Context& E, const PassLayout& L, const std::vector<SceneDe
   SceneDev S0 = tab[0];
   bool multi = multi_pass;
   Context& c = E;
-  WfDev w;
-  Wavefront& wf = c.wf;
-  float4* rays = wf.rays.as<float4>();
-  float4* state = wf.state.as<float4>();
-  w.ray_o = Field2<float4>{rays};
-  w.ray_d = Field2<float4>{rays + 1};
-  w.thr = Field2<float4>{state};
-  w.rad = wf.rad.as<float4>();
-  w.rng = Field2<uint4>{reinterpret_cast<uint4*>(state + 1)};
-  w.hit = wf.hit.as<float4>();
-  w.q_mat = wf.q_mat.as<uint32_t>();
-  w.cls_of = wf.cls_of.as<uint8_t>();
-  w.bin = wf.bin.as<uint32_t>();
-  w.sh_o = wf.sh_o.as<float4>();
-  w.sh_d = wf.sh_d.as<float4>();
-  w.sh_c = wf.sh_c.as<float4>();
-  w.sh_pid = wf.sh_pid.as<uint32_t>();
-  w.cnt = wf.counters.as<uint32_t>();
-  w.cap = wf.cap;
-  w.g_a = L.sss ? wf.g_a.as<float4>() : nullptr;
-  w.g_b = L.sss ? wf.g_b.as<float4>() : nullptr;
-  w.g_c = L.sss ? wf.g_c.as<float2>() : nullptr;
-  w.g_d = L.sss ? wf.g_d.as<float4>() : nullptr;
-  w.g_slots = L.sss ? wf.gather_slots : 0;
-  w.scenes = c.d_scene_tab.as<SceneDev>();
-  w.multi = multi ? 1u : 0u;
-  w.scene0 = 0;
-  w.path_item = wf.path_item.as<uint16_t>();
-  w.adj_a = adjoint ? wf.adj_a.as<float4>() : nullptr;
-  w.adj_b = adjoint ? wf.adj_b.as<float4>() : nullptr;
+  // the device view of one wavefront (dual passes: one per pipeline)
+  auto make_w = [&](Wavefront& wf) {
+    WfDev v;
+    float4* rays = wf.rays.as<float4>();
+    float4* state = wf.state.as<float4>();
+    v.ray_o = Field2<float4>{rays};
+    v.ray_d = Field2<float4>{rays + 1};
+    v.thr = Field2<float4>{state};
+    v.rad = wf.rad.as<float4>();
+    v.rng = Field2<uint4>{reinterpret_cast<uint4*>(state + 1)};
+    v.hit = wf.hit.as<float4>();
+    v.q_mat = wf.q_mat.as<uint32_t>();
+    v.cls_of = wf.cls_of.as<uint8_t>();
+    v.bin = wf.bin.as<uint32_t>();
+    v.sh_o = wf.sh_o.as<float4>();
+    v.sh_d = wf.sh_d.as<float4>();
+    v.sh_c = wf.sh_c.as<float4>();
+    v.sh_pid = wf.sh_pid.as<uint32_t>();
+    v.cnt = wf.counters.as<uint32_t>();
+    v.cap = wf.cap;
+    v.g_a = L.sss ? wf.g_a.as<float4>() : nullptr;
+    v.g_b = L.sss ? wf.g_b.as<float4>() : nullptr;
+    v.g_c = L.sss ? wf.g_c.as<float2>() : nullptr;
+    v.g_d = L.sss ? wf.g_d.as<float4>() : nullptr;
+    v.g_slots = L.sss ? wf.gather_slots : 0;
+    v.scenes = c.d_scene_tab.as<SceneDev>();
+    v.multi = multi ? 1u : 0u;
+    v.scene0 = 0;
+    v.path_item = wf.path_item.as<uint16_t>();
+    v.adj_a = adjoint ? wf.adj_a.as<float4>() : nullptr;
+    v.adj_b = adjoint ? wf.adj_b.as<float4>() : nullptr;
+    return v;
+  };
+  const size_t n_chunks = L.chunk_paths.size();
+  const bool prof = c.profile && allow_events;
+  // two pipelines: chunk k runs on wavefront k % 2 with that pipeline's streams; the accumulations
+  // (each chunk's frames folded into its scenes' running means) stay in chunk order
+  const bool dual = L.dual && !adjoint && !prof && n_chunks >= 2 && c.stream2 && c.wf2.cap >= L.cap_paths;
+  const WfDev w_of[2] = {make_w(c.wf), dual ? make_w(c.wf2) : make_w(c.wf)};
+  Wavefront* const wf_of[2] = {&c.wf, dual ? &c.wf2 : &c.wf};
+  WfDev w = w_of[0];
+  Wavefront* wf = wf_of[0];
+  c.pass_dual = dual;
+  Wavefront& wf0 = c.wf;
   SssDev g;
   memset(&g, 0, sizeof(g));
   if (L.sss) {
-    g.probes = wf.probes.as<float4>();
-    g.pc_pos = wf.pc_pos.as<float4>();
-    g.pc_wl = wf.pc_wl.as<float4>();
-    g.pc_nrm = wf.pc_nrm.as<float4>();
-    g.pc_tr = wf.pc_tr.as<float4>();
-    g.pc_cnt = wf.pc_cnt.as<uint32_t>();
+    g.probes = wf0.probes.as<float4>();
+    g.pc_pos = wf0.pc_pos.as<float4>();
+    g.pc_wl = wf0.pc_wl.as<float4>();
+    g.pc_nrm = wf0.pc_nrm.as<float4>();
+    g.pc_tr = wf0.pc_tr.as<float4>();
+    g.pc_cnt = wf0.pc_cnt.as<uint32_t>();
   }
   const int grid_trace = sm_count() * 8, grid_shade = sm_count() * 8;
   // the 4-wide BVH when every scene of the pass has one (pass_resources)
@@ -2615,8 +2639,12 @@ pt_status launch_pass(Context& E, const PassLayout& L, const std::vector<SceneDe
   if (ost != PT_OK) return ost;
   int grid_persist = grid_persist_of[0];
   const int grid_bin = sm_count() * 8;
-  const bool prof = c.profile && allow_events;
-  PT_CHECK_CUDA(cudaMemsetAsync(w.cnt, 0, kCounters * 4, c.stream), "reset counters");
+  PT_CHECK_CUDA(cudaMemsetAsync(w_of[0].cnt, 0, kCounters * 4, c.stream), "reset counters");
+  if (dual) {  // the second pipeline starts after everything queued on the context stream so far
+    PT_CHECK_CUDA(cudaEventRecord(c.ev_start, c.stream), "second pipeline start");
+    PT_CHECK_CUDA(cudaStreamWaitEvent(c.stream2, c.ev_start, 0), "second pipeline start");
+    PT_CHECK_CUDA(cudaMemsetAsync(w_of[1].cnt, 0, kCounters * 4, c.stream2), "reset counters");
+  }
   c.prof_pairs = 0;
   pt_status st = PT_OK;
   // CUDA events around the launches whose device time the stats report (when profiling is on)
@@ -2638,12 +2666,15 @@ pt_status launch_pass(Context& E, const PassLayout& L, const std::vector<SceneDe
     ++c.prof_pairs;
     return PT_OK;
   };
+  // the current chunk's pipeline: its stream, side streams and events (pipeline 0: the context's)
+  cudaStream_t s_main = c.stream;
+  cudaEvent_t e_fork = c.ev_fork, e_join = c.ev_join, e_shade = c.ev_shade, e_shadow = c.ev_shadow;
   auto reset_queues = [&]() -> pt_status {
-    w.q_in = wf.q_a.as<uint32_t>();
-    w.q_out = wf.q_b.as<uint32_t>();
+    w.q_in = wf->q_a.as<uint32_t>();
+    w.q_out = wf->q_b.as<uint32_t>();
     w.in_slot = CNT_ACTIVE_A;
     w.out_slot = CNT_ACTIVE_B;
-    PT_CHECK_CUDA(cudaMemsetAsync(w.cnt, 0, (CNT_FETCH_SH + 1) * 4, c.stream), "reset queues");
+    PT_CHECK_CUDA(cudaMemsetAsync(w.cnt, 0, (CNT_FETCH_SH + 1) * 4, s_main), "reset queues");
     return PT_OK;
   };
   // The overlapped schedule (option "overlap", off while profiling so that the extend events time the
@@ -2655,7 +2686,7 @@ pt_status launch_pass(Context& E, const PassLayout& L, const std::vector<SceneDe
   // so the shadow kernel runs on side[1] beside them, and bounce b + 1's shading, which rewrites the
   // shadow queue and adds to the radiance, waits for it.  Every path's arithmetic is its own, so the
   // images do not depend on the schedule.
-  const bool overlap = c.opt.overlap && !prof && c.side[0] && c.side[1];
+  const bool overlap = c.opt.overlap && !prof && c.side[0] && c.side[1] && (!dual || (c.side2[0] && c.side2[1]));
   cudaStream_t s_small = overlap ? c.side[0] : c.stream;
   cudaStream_t s_shadow = overlap ? c.side[1] : c.stream;
   auto wait_on = [&](cudaStream_t waiter, cudaStream_t from, cudaEvent_t ev) -> pt_status {
@@ -2667,31 +2698,31 @@ pt_status launch_pass(Context& E, const PassLayout& L, const std::vector<SceneDe
   auto bounces = [&](bool adj_pass) -> pt_status {
     const bool adjoint = adj_pass;
     for (int b = 0; b < L.passes; ++b) {
-      PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_Q_MISS, 0, (CNT_FETCH_EXT - CNT_Q_MISS + 1) * 4, c.stream), "reset queues");
-      PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + w.out_slot, 0, 4, c.stream), "reset queues");
+      PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_Q_MISS, 0, (CNT_FETCH_EXT - CNT_Q_MISS + 1) * 4, s_main), "reset queues");
+      PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + w.out_slot, 0, 4, s_main), "reset queues");
       if ((st = prof_begin(PROF_EXTEND)) != PT_OK) return st;
       if (c.opt.extend_mode == 1) {
         if (w4) {
-          if (multi) k_extend_persistent<true, true><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-          else k_extend_persistent<false, true><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          if (multi) k_extend_persistent<true, true><<<grid_persist, kTraceBlock, 0, s_main>>>(S0, w, c.opt.refill);
+          else k_extend_persistent<false, true><<<grid_persist, kTraceBlock, 0, s_main>>>(S0, w, c.opt.refill);
         } else {
-          if (multi) k_extend_persistent<true, false><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
-          else k_extend_persistent<false, false><<<grid_persist, kTraceBlock, 0, c.stream>>>(S0, w, c.opt.refill);
+          if (multi) k_extend_persistent<true, false><<<grid_persist, kTraceBlock, 0, s_main>>>(S0, w, c.opt.refill);
+          else k_extend_persistent<false, false><<<grid_persist, kTraceBlock, 0, s_main>>>(S0, w, c.opt.refill);
         }
       } else {
-        k_extend<<<grid_trace, kBlock, 0, c.stream>>>(w);
+        k_extend<<<grid_trace, kBlock, 0, s_main>>>(w);
       }
       if ((st = prof_end()) != PT_OK) return st;
-      if (c.opt.bin_items == 4) launch_binning<4>(w, grid_bin, c.stream);
-      else if (c.opt.bin_items == 16) launch_binning<16>(w, grid_bin, c.stream);
-      else launch_binning<8>(w, grid_bin, c.stream);
+      if (c.opt.bin_items == 4) launch_binning<4>(w, grid_bin, s_main);
+      else if (c.opt.bin_items == 16) launch_binning<16>(w, grid_bin, s_main);
+      else launch_binning<8>(w, grid_bin, s_main);
       count_launch(3);
       // the previous bounce's shadow rays are done before this bounce's shading refills their queue
-      if (overlap && b > 0 && (st = wait_on(c.stream, s_shadow, c.ev_shadow)) != PT_OK) return st;
-      PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_SHADOW, 0, (CNT_FETCH_SH - CNT_SHADOW + 1) * 4, c.stream), "reset queues");
-      if (overlap && (st = wait_on(s_small, c.stream, c.ev_fork)) != PT_OK) return st;
+      if (overlap && b > 0 && (st = wait_on(s_main, s_shadow, e_shadow)) != PT_OK) return st;
+      PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_SHADOW, 0, (CNT_FETCH_SH - CNT_SHADOW + 1) * 4, s_main), "reset queues");
+      if (overlap && (st = wait_on(s_small, s_main, e_fork)) != PT_OK) return st;
       if (adjoint) {
-        k_shade_diffuse<true><<<full_wave(k_shade_diffuse<true>), kBlock, 0, c.stream>>>(w);
+        k_shade_diffuse<true><<<full_wave(k_shade_diffuse<true>), kBlock, 0, s_main>>>(w);
         k_shade_miss<true><<<full_wave(k_shade_miss<true>), kBlock, 0, s_small>>>(w);
         k_shade_light<true><<<full_wave(k_shade_light<true>), kBlock, 0, s_small>>>(w);
         if (L.ms) {
@@ -2702,7 +2733,7 @@ pt_status launch_pass(Context& E, const PassLayout& L, const std::vector<SceneDe
           k_shade_glass<true, false><<<full_wave(k_shade_glass<true, false>), kBlock, 0, s_small>>>(w);
         }
       } else {
-        k_shade_diffuse<false><<<full_wave(k_shade_diffuse<false>), kBlock, 0, c.stream>>>(w);
+        k_shade_diffuse<false><<<full_wave(k_shade_diffuse<false>), kBlock, 0, s_main>>>(w);
         k_shade_miss<false><<<full_wave(k_shade_miss<false>), kBlock, 0, s_small>>>(w);
         k_shade_light<false><<<full_wave(k_shade_light<false>), kBlock, 0, s_small>>>(w);
         if (L.ms) {
@@ -2715,19 +2746,19 @@ pt_status launch_pass(Context& E, const PassLayout& L, const std::vector<SceneDe
       }
       count_launch(6);
       if (L.layered) {
-        if (adjoint) k_shade_layered<true><<<full_wave(k_shade_layered<true>), kBlock, 0, c.stream>>>(w);
-        else k_shade_layered<false><<<full_wave(k_shade_layered<false>), kBlock, 0, c.stream>>>(w);
+        if (adjoint) k_shade_layered<true><<<full_wave(k_shade_layered<true>), kBlock, 0, s_main>>>(w);
+        else k_shade_layered<false><<<full_wave(k_shade_layered<false>), kBlock, 0, s_main>>>(w);
         count_launch();
       }
       if (L.sss) {
-        if (adjoint) k_shade_translucent<true><<<full_wave(k_shade_translucent<true>), kBlock, 0, c.stream>>>(w);
-        else k_shade_translucent<false><<<full_wave(k_shade_translucent<false>), kBlock, 0, c.stream>>>(w);
+        if (adjoint) k_shade_translucent<true><<<full_wave(k_shade_translucent<true>), kBlock, 0, s_main>>>(w);
+        else k_shade_translucent<false><<<full_wave(k_shade_translucent<false>), kBlock, 0, s_main>>>(w);
         count_launch();
       }
       if (overlap) {
         // join the smaller classes, then fork the shadow rays off the joined stream
-        if ((st = wait_on(c.stream, s_small, c.ev_join)) != PT_OK) return st;
-        if ((st = wait_on(s_shadow, c.stream, c.ev_shade)) != PT_OK) return st;
+        if ((st = wait_on(s_main, s_small, e_join)) != PT_OK) return st;
+        if ((st = wait_on(s_shadow, s_main, e_shade)) != PT_OK) return st;
       }
       if (c.opt.extend_mode == 1) {
         if (w4) {
@@ -2751,12 +2782,21 @@ pt_status launch_pass(Context& E, const PassLayout& L, const std::vector<SceneDe
       std::swap(w.in_slot, w.out_slot);
     }
     // the last bounce's shadow rays join the context stream before anything reads the radiance
-    if (overlap && (st = wait_on(c.stream, s_shadow, c.ev_shadow)) != PT_OK) return st;
+    if (overlap && (st = wait_on(s_main, s_shadow, e_shadow)) != PT_OK) return st;
     return PT_OK;
   };
   const ItemDev* items = c.d_item_tab.as<ItemDev>();
-  const size_t n_chunks = L.chunk_paths.size();
   for (size_t k = 0; k < n_chunks; ++k) {
+    const int pl = dual ? (int)(k & 1) : 0;
+    w = w_of[pl];
+    wf = wf_of[pl];
+    s_main = pl ? c.stream2 : c.stream;
+    s_small = overlap ? (pl ? c.side2[0] : c.side[0]) : s_main;
+    s_shadow = overlap ? (pl ? c.side2[1] : c.side[1]) : s_main;
+    e_fork = pl ? c.ev2_fork : c.ev_fork;
+    e_join = pl ? c.ev2_join : c.ev_join;
+    e_shade = pl ? c.ev2_shade : c.ev_shade;
+    e_shadow = pl ? c.ev2_shadow : c.ev_shadow;
     const uint32_t ib = L.chunk_item_begin[k];
     const uint32_t ie = k + 1 < n_chunks ? L.chunk_item_begin[k + 1] : (uint32_t)L.items.size();
     w.items = items + ib;
@@ -2773,34 +2813,41 @@ pt_status launch_pass(Context& E, const PassLayout& L, const std::vector<SceneDe
       for (uint64_t j0 = 0; j0 < n_probes; j0 += w.cap) {
         uint64_t nj = std::min<uint64_t>(w.cap, n_probes - j0);
         if ((st = reset_queues()) != PT_OK) return st;
-        k_probe_gen<<<grid_for(nj, kBlock, 16), kBlock, 0, c.stream>>>(w, g, j0, nj);
+        k_probe_gen<<<grid_for(nj, kBlock, 16), kBlock, 0, s_main>>>(w, g, j0, nj);
         count_launch();
         if ((st = bounces(false)) != PT_OK) return st;
-        k_probe_finish<<<grid_for(nj, kBlock, 16), kBlock, 0, c.stream>>>(w, g, j0, nj);
+        k_probe_finish<<<grid_for(nj, kBlock, 16), kBlock, 0, s_main>>>(w, g, j0, nj);
         count_launch();
       }
-      k_probe_compact<<<L.chunk_sets[k], 256, 0, c.stream>>>(w, g);
+      k_probe_compact<<<L.chunk_sets[k], 256, 0, s_main>>>(w, g);
       count_launch();
     }
     if ((st = reset_queues()) != PT_OK) return st;
-    if (adjoint) k_raygen<true><<<grid_for(n_paths, kBlock, 16), kBlock, 0, c.stream>>>(w, n_paths);
-    else k_raygen<false><<<grid_for(n_paths, kBlock, 16), kBlock, 0, c.stream>>>(w, n_paths);
+    if (adjoint) k_raygen<true><<<grid_for(n_paths, kBlock, 16), kBlock, 0, s_main>>>(w, n_paths);
+    else k_raygen<false><<<grid_for(n_paths, kBlock, 16), kBlock, 0, s_main>>>(w, n_paths);
     count_launch();
     if ((st = bounces(adjoint)) != PT_OK) return st;
     if (n_probes) {
-      PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_GATHER, 0, 4, c.stream), "reset gather list");
-      uint32_t* list = wf.q_a.as<uint32_t>();
-      k_gather_collect<<<grid_for(n_paths, kBlock, 16), kBlock, 0, c.stream>>>(w, n_paths, list);
+      PT_CHECK_CUDA(cudaMemsetAsync(w.cnt + CNT_GATHER, 0, 4, s_main), "reset gather list");
+      uint32_t* list = wf->q_a.as<uint32_t>();
+      k_gather_collect<<<grid_for(n_paths, kBlock, 16), kBlock, 0, s_main>>>(w, n_paths, list);
       if ((st = prof_begin(PROF_GATHER)) != PT_OK) return st;
-      if (adjoint) k_gather_adjoint<<<grid_shade, kBlock, 0, c.stream>>>(w, g, list);
-      else k_gather<<<grid_shade, kBlock, 0, c.stream>>>(w, g, list);
+      if (adjoint) k_gather_adjoint<<<grid_shade, kBlock, 0, s_main>>>(w, g, list);
+      else k_gather<<<grid_shade, kBlock, 0, s_main>>>(w, g, list);
       if ((st = prof_end()) != PT_OK) return st;
       count_launch(2);
     }
     if (!adjoint) {
-      k_accumulate<<<grid_for(L.chunk_pixels[k], kBlock, 16), kBlock, 0, c.stream>>>(w, L.chunk_pixels[k]);
+      // the running means take the chunks' frames in chunk order
+      if (dual && k > 0) PT_CHECK_CUDA(cudaStreamWaitEvent(s_main, c.ev_acc, 0), "accumulation order");
+      k_accumulate<<<grid_for(L.chunk_pixels[k], kBlock, 16), kBlock, 0, s_main>>>(w, L.chunk_pixels[k]);
       count_launch();
+      if (dual) PT_CHECK_CUDA(cudaEventRecord(c.ev_acc, s_main), "accumulation order");
     }
+  }
+  if (dual) {  // the second pipeline joins the context stream
+    PT_CHECK_CUDA(cudaEventRecord(c.ev_end2, c.stream2), "second pipeline join");
+    PT_CHECK_CUDA(cudaStreamWaitEvent(c.stream, c.ev_end2, 0), "second pipeline join");
   }
   PT_CHECK_CUDA(cudaGetLastError(), "render launch");
   return PT_OK;
@@ -2832,7 +2879,7 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
     c.adj_slots = slots;
     c.adj_valid = true;
   }
-  PassLayout L = plan_pass({f}, {ItemReq{0, first_frame, n_frames}}, c.max_paths);
+  PassLayout L = plan_pass({f}, {ItemReq{0, first_frame, n_frames}}, c.max_paths, c.opt.dual && !c.differentiable);
   std::vector<SceneDev> scenes{c.view()};
   if ((st = pass_resources(c, L, scenes)) != PT_OK) return st;
   uint64_t launches0 = pt_kernel_launch_count();
@@ -2913,9 +2960,16 @@ pt_status pt_get_render_stats(pt_ctx* ctx, pt_render_stats* out)
   PT_CHECK_CUDA(cudaSetDevice(c.device), "cudaSetDevice");
   PT_CHECK_CUDA(cudaStreamSynchronize(c.stream), "pt_get_render_stats");
   if (c.stats_pending && c.wf.counters.p) {
-    uint32_t h[kCounters];
+    uint32_t h[kCounters], h2[kCounters];
     PT_CHECK_CUDA(cudaMemcpy(h, c.wf.counters.p, sizeof(h), cudaMemcpyDeviceToHost), "read counters");
-    auto rd64 = [&](int slot) { unsigned long long v; memcpy(&v, h + slot, 8); return (uint64_t)v; };
+    const bool two = c.pass_dual && c.wf2.counters.p;  // a dual pass counts in both wavefronts
+    if (two) PT_CHECK_CUDA(cudaMemcpy(h2, c.wf2.counters.p, sizeof(h2), cudaMemcpyDeviceToHost), "read counters");
+    auto rd64 = [&](int slot) {
+      unsigned long long v, v2 = 0;
+      memcpy(&v, h + slot, 8);
+      if (two) memcpy(&v2, h2 + slot, 8);
+      return (uint64_t)(v + v2);
+    };
     c.stats.segments = rd64(CNT_SEGMENTS_LO);
     c.stats.shadow_rays = rd64(CNT_SHADOW_TOTAL);
     c.stats.capped_walks = rd64(CNT_CAPPED);

@@ -125,8 +125,10 @@ def test_traversal_variants_leave_identical_images(big):
     data = scenes.single_scene(width=24, height=24) if big else small_scene(24, 24)
     imgs = []
     # the material binning is a stable partition, the same for every chunk size (sort granularity);
-    # every path's arithmetic is its own, so the overlapped and the in-order schedules agree
-    for opts in ({}, {"bvh4": 0}, {"extend_mode": 0}, {"bin_items": 4}, {"bin_items": 16}, {"overlap": 0}):
+    # every path's arithmetic is its own, so the overlapped and the in-order schedules, and one or two
+    # wavefronts in flight, agree
+    for opts in ({}, {"bvh4": 0}, {"extend_mode": 0}, {"bin_items": 4}, {"bin_items": 16}, {"overlap": 0},
+                 {"dual": 0}, {"dual": 0, "overlap": 0}):
         R = sc.Renderer(data)
         for k, v in opts.items():
             nat.call("pt_set_option", R.ctx, k.encode(), v)
@@ -152,6 +154,28 @@ def test_render_frames_in_one_call_equal_frame_by_frame():
     assert np.array_equal(a, b) and np.array_equal(a, c)
     for r in (R1, R2, R3):
         r.close()
+
+
+@pytest.mark.parametrize("w,h,max_paths", [(1, 1, None), (33, 17, None), (7, 1, 1), (33, 17, 100)])
+def test_ragged_sizes_and_tiny_wavefronts_match_oracle(w, h, max_paths):
+    """Images whose pixel count is no multiple of a warp or a block, and wavefronts smaller than a frame
+    (one chunk per frame then), against the CPU restatement; a render of zero frames changes nothing."""
+    data = small_scene(w, h)
+    R = sc.Renderer(data, max_paths_in_flight=max_paths)
+    R.render(3)
+    img = R.readback()
+    R.render(0)
+    assert np.array_equal(img.view(np.uint32), R.readback().view(np.uint32))
+    O = oc.OracleScene(data)
+    ref, _ = O.render(0, 3, accum=np.zeros((h, w, 4), np.float32), threads=4)
+    rel = np.abs(img[..., :3].astype(np.float64) - ref[..., :3]) / np.maximum(np.abs(ref[..., :3]), 1e-3)
+    frac = float(np.mean(np.all(rel <= 1e-3, axis=-1)))
+    err = float(np.mean((img[..., :3] - ref[..., :3]) ** 2 / (ref[..., :3].astype(np.float64) ** 2 + 1e-2)))
+    print("%dx%d, max paths %s: %.4f of pixels within 1e-3, relMSE %.3e" % (w, h, max_paths, frac, err))
+    assert np.all(np.isfinite(img)) and err < 1e-3
+    if w * h >= 64:
+        assert frac >= 0.95
+    R.close()
 
 
 def test_patch_outside_pixels_are_black_with_unit_alpha():
