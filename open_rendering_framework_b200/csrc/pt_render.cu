@@ -2879,7 +2879,8 @@ pt_status pt_render_frames(pt_ctx* ctx, uint32_t first_frame, uint32_t n_frames)
     c.adj_slots = slots;
     c.adj_valid = true;
   }
-  PassLayout L = plan_pass({f}, {ItemReq{0, first_frame, n_frames}}, c.max_paths, c.opt.dual && !c.differentiable);
+  // profiled renders time the kernels of one wavefront (the extend events are on the context stream)
+  PassLayout L = plan_pass({f}, {ItemReq{0, first_frame, n_frames}}, c.max_paths, c.opt.dual && !c.differentiable && !c.profile);
   std::vector<SceneDev> scenes{c.view()};
   if ((st = pass_resources(c, L, scenes)) != PT_OK) return st;
   uint64_t launches0 = pt_kernel_launch_count();
