@@ -39,12 +39,18 @@ void drop_graph(pt_batch* b)
   b->graph_kernels = 0;
 }
 
-// Everything the captured launch sequence depends on: the pass layout (chunks, counts, bounces) and
-// the device buffers and options it was launched with.  Item first frames and the scene table's
-// contents are read from device memory at run time and may change between launches.
-std::vector<uint64_t> graph_key(const Context& E, const PassLayout& L)
+// Everything the captured launch sequence depends on: the pass layout (chunks, counts, bounces), the
+// device buffers and options it was launched with, and the scene records themselves (a chunk that
+// holds one scene passes its record to the traversal kernels by value, so the graph holds a copy).
+// Item first frames are read from device memory at run time and may change between launches.
+std::vector<uint64_t> graph_key(const Context& E, const PassLayout& L, const std::vector<SceneDev>& tab)
 {
   std::vector<uint64_t> k;
+  for (const SceneDev& sd : tab) {  // each record's bytes, word by word (compared exactly)
+    uint64_t words[(sizeof(SceneDev) + 7) / 8] = {};
+    memcpy(words, &sd, sizeof(SceneDev));
+    k.insert(k.end(), words, words + (sizeof(SceneDev) + 7) / 8);
+  }
   k.push_back((uint64_t)L.passes);
   k.push_back(L.sss ? 1 : 0);
   k.push_back(L.layered ? 1 : 0);
@@ -123,7 +129,7 @@ pt_status render(pt_batch* b, bool graph, const std::vector<uint32_t>* frames_ov
   uint64_t launches0 = pt_kernel_launch_count();
   memset(&E.stats, 0, sizeof(E.stats));
   if (graph) {
-    std::vector<uint64_t> key = graph_key(E, L);
+    std::vector<uint64_t> key = graph_key(E, L, tab);
     if (!b->exec || key != b->key) {
       drop_graph(b);
       cudaGraph_t g = nullptr;

@@ -15,6 +15,7 @@ namespace pt {
 SceneDev Context::view() const
 {
   SceneDev s;
+  memset(&s, 0, sizeof(s));  // padding included: captured passes key on the record's bytes
   s.nodes = d_nodes.as<float4>();
   s.nodes4 = has_bvh4 && use_bvh4 ? d_nodes4.as<float4>() : nullptr;
   s.trav_scale = trav_scale;

@@ -60,6 +60,42 @@ def test_batched_render_equals_scene_by_scene(use_graph):
         R.close()
 
 
+def test_graph_replay_follows_changed_scenes():
+    """A scene changed between two batched renders (here its integrator's scene epsilon, which the
+    traversal kernels of a one-scene chunk receive by value) makes the batch capture its graph again, so
+    the second render equals scene-by-scene renders that made the same change."""
+    S = small_batch(3, seed=11)
+    eps2 = 3e-3
+    eps1 = [data.integrator.scene_epsilon for data, _, _ in S]
+
+    def run(batched):
+        for (data, _, _), e in zip(S, eps1):
+            data.integrator.scene_epsilon = e
+        Rs = [sc.Renderer(data) for data, _, _ in S]
+        B = sc.Batch(Rs, [spp for _, spp, _ in S]) if batched else None
+        if B:
+            B.set_option("max_paths_in_flight", 64)  # every chunk one frame of one scene
+        for step in range(2):
+            if step == 1:
+                for R in Rs:
+                    R.data.integrator.scene_epsilon = eps2
+                    R.apply_integrator()
+            if batched:
+                B.render()
+            else:
+                for R, (_, spp, _) in zip(Rs, S):
+                    R.render(spp)
+        imgs = [R.readback() for R in Rs]
+        if B:
+            B.close()
+        for R in Rs:
+            R.close()
+        return imgs
+
+    for a, b, (_, _, info) in zip(run(True), run(False), S):
+        assert np.array_equal(bits(a), bits(b)), info
+
+
 def test_sequential_mode_and_autotune():
     S = small_batch(4, seed=9)
     Rs = [sc.Renderer(data) for data, _, _ in S]
