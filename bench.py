@@ -91,8 +91,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="single_scene", choices=["single_scene", "subsurface", "batched", "adjoint", "bsdf", "ingest", "build"])
-    ap.add_argument("--queries", type=int, default=1 << 22, help="bsdf workload: queries per step")
+    ap.add_argument("--workload", default="single_scene", choices=["single_scene", "subsurface", "batched", "adjoint", "bsdf", "ingest", "build", "queries"])
+    ap.add_argument("--queries", type=int, default=1 << 22, help="bsdf and queries workloads: queries per step / launch")
     ap.add_argument("--scenes", type=int, default=64, help="batched workload: number of scenes")
     ap.add_argument("--spp", type=int, default=None, help="frames per step (default 64, subsurface 256)")
     ap.add_argument("--width", type=int, default=None)
@@ -653,6 +653,174 @@ def run_reference_ingest(args):
     print(json.dumps(line), flush=True)
 
 
+QUERIES = ("per-query entries: %d queries per launch of the dipole BSSRDF of one translucent material (the subsurface "
+           "configuration's seeded coefficients, eta 1.3, scale 100; standard dipole on distances log-uniform over 1e-3..30 mean "
+           "free paths, directional dipole on point pairs of a sphere of 50 mean free paths with random incoming directions; FP32 "
+           "and FP64) and of the multiscattering walks and the conductor Fresnel (GGX and Beckmann, alpha ~ U[0.1, 0.9], upper-"
+           "hemisphere directions, the single-scene conductor's complex IOR)")
+MSQ_OPS = ["dielectric_eval", "dielectric_sample", "conductor_eval", "conductor_sample", "diffuse_eval", "diffuse_sample",
+           "conductor_fresnel", "visible_normal"]
+
+
+def query_inputs(n, seed=0):
+    """Seeded inputs of the per-query workload: the material, the standard dipole's distances, the
+    directional dipole's 15 x n rows, and the microfacet walks' wi, wo, alpha."""
+    import numpy as np
+
+    from open_rendering_framework_b200 import scenes
+
+    rng = np.random.default_rng(seed)
+    sigma_s, sigma_a = scenes.dipole_coefficients(3)
+    params = (np.float32(sigma_a), np.float32(sigma_s), np.zeros(3, np.float32), 1.3, 100.0)
+    mfp = 1.0 / float(params[4] * (np.min(params[1]) + np.min(params[0])))
+    dist = (mfp * np.exp(rng.uniform(np.log(1e-3), np.log(30.0), n))).astype(np.float32)
+
+    def unit(m):
+        v = rng.normal(size=(m, 3))
+        return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+    Rs = 50.0 * mfp
+    ni = unit(n)
+    t = np.cross(ni, unit(n))
+    t /= np.linalg.norm(t, axis=1, keepdims=True)
+    ang = dist / Rs
+    no = ni * np.cos(ang)[:, None] + t * np.sin(ang)[:, None]
+    w12 = unit(n)
+    w12 = np.where((np.sum(w12 * ni, axis=1) > 0)[:, None], -w12, w12)
+    geo = np.concatenate([(Rs * ni).T, ni.T, w12.T, (Rs * no).T, no.T]).astype(np.float32)
+    up = lambda v: np.where(v[:, 2:3] < 0, v * np.array([1, 1, -1]), v)
+    wi = up(unit(n)).T.astype(np.float32)
+    wo = up(unit(n)).T.astype(np.float32)
+    alpha = rng.uniform(0.1, 0.9, n).astype(np.float32)
+    return params, dist, geo, np.ascontiguousarray(wi), np.ascontiguousarray(wo), alpha
+
+
+def run_queries(args, world, rank, local):
+    """Throughput of the per-query entries (pt_bssrdf_queries in FP32 and FP64, pt_microfacet_queries for
+    every operation and both distributions) at a launch size larger than L2, device-resident inputs."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from open_rendering_framework_b200 import _native as nat
+    from open_rendering_framework_b200 import scene as sc
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.queries
+    params, dist, geo, wi, wo, alpha = query_inputs(n)
+    tp = sc.TranslucentParams((ctypes.c_float * 3)(*params[1]), (ctypes.c_float * 3)(*params[0]), (ctypes.c_float * 3)(*params[2]),
+                              params[3], params[4], sc.STANDARD_DIPOLE)
+    d_dist, d_geo = torch.from_numpy(dist).to(dev), torch.from_numpy(geo).to(dev)
+    d_wi, d_wo, d_alpha = torch.from_numpy(wi).to(dev), torch.from_numpy(wo).to(dev), torch.from_numpy(alpha).to(dev)
+    d_seed = torch.arange(n, dtype=torch.int32, device=dev)
+    d_order = torch.zeros(n, dtype=torch.int32, device=dev)
+    out32 = torch.empty((3, n), dtype=torch.float32, device=dev)
+    out64 = torch.empty((3, n), dtype=torch.float64, device=dev)
+    weight = torch.empty((3, n), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    launches = [0]
+
+    def bssrdf(model, precision, d_in):
+        tp.dipole_model = model
+        nat.call("pt_bssrdf_queries", ctypes.byref(tp), precision, d_in.data_ptr(), n, (out64 if precision else out32).data_ptr(), sp)
+        launches[0] += 1
+
+    def walk(op, distn):
+        b = sc.MicrofacetBatch()
+        b.op, b.normal_distribution = op, distn
+        b.normal[:] = [0.0, 0.0, 1.0]
+        b.eta = 1.0 / 1.5
+        b.ior[:] = [0.2, 3.9, 0.55, 3.15, 0.9, 2.4]
+        b.rho[:] = [0.7, 0.7, 0.7]
+        d_order.zero_()
+        nat.call("pt_microfacet_queries", ctypes.byref(b), d_wi.data_ptr(), d_wo.data_ptr(), d_alpha.data_ptr(), d_seed.data_ptr(),
+                 d_order.data_ptr(), n, out32.data_ptr(), weight.data_ptr(), sp)
+        launches[0] += 1
+
+    def timed(fn):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    peak, peak_kind = load_peaks()
+    with ClockSampler(local) as clocks:
+        per_op = {}
+        for model, name, d_in, in_bytes in ((sc.STANDARD_DIPOLE, "standard", d_dist, 4), (sc.DIRECTIONAL_DIPOLE, "directional", d_geo, 60)):
+            for precision, out_bytes in ((0, 12), (1, 24)):
+                ms = timed(lambda: bssrdf(model, precision, d_in))
+                per_op["bssrdf_%s_%s" % (name, "fp64" if precision else "fp32")] = {
+                    "m_queries_per_s": n / (ms * 1e-3) / 1e6, "ms": ms,
+                    "hbm_gb_s": (in_bytes + out_bytes) * n / (ms * 1e-3) / 1e9}
+        for distn, dname in ((sc.GGX_DISTRIBUTION, "ggx"), (sc.BECKMANN_DISTRIBUTION, "beckmann")):
+            for op, oname in enumerate(MSQ_OPS):
+                ms = timed(lambda: walk(op, distn))
+                per_op["%s_%s" % (oname, dname)] = {"m_queries_per_s": n / (ms * 1e-3) / 1e6, "ms": ms}
+        # end to end: the directional dipole from pinned host rows, values read back, every step
+        h_geo = torch.from_numpy(geo).pin_memory()
+        h_out = torch.empty((3, n), dtype=torch.float32).pin_memory()
+
+        def e2e_step():
+            d_geo.copy_(h_geo, non_blocking=True)
+            bssrdf(sc.DIRECTIONAL_DIPOLE, 0, d_geo)
+            h_out.copy_(out32, non_blocking=True)
+
+        e2e_ms = timed(e2e_step)
+    head = per_op["bssrdf_directional_fp32"]
+    rec = ncu_record("k_bssrdf_queries_ncu.csv")
+    sm_mhz = clocks.summary().get("sm_mhz") or 1965.0
+    n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+    issue_peak = n_sm * 4 * sm_mhz * 1e6 / 1e9
+    per_q = rec["totals"]["smsp__inst_executed.sum"] / float(rec["header"]["queries"]) if rec and "queries" in rec["header"] else None
+    issue_achieved = per_q * n / (head["ms"] * 1e-3) / 1e9 if per_q else None
+    issue_roofline = {
+        "bound": "issue", "kernel": "k_bssrdf_directional (FP32)", "achieved": issue_achieved, "peak": issue_peak,
+        "unit": "G warp instructions/s", "frac": issue_achieved / issue_peak if issue_achieved else None,
+        "peak_source": "1 warp instruction / clock / SM sub-partition x 4 x %d SMs x median SM clock %.0f MHz" % (n_sm, sm_mhz),
+        "warp_instructions_per_query": per_q,
+        "traffic": ((rec["totals"]["dram__bytes_read.sum"] + rec["totals"]["dram__bytes_write.sum"]) / float(rec["header"]["queries"]) * n)
+        if per_q else None,
+        "traffic_unit": "DRAM bytes per launch (ncu record of the same launch size, profiles/k_bssrdf_queries_ncu.csv)",
+        "hbm": {"achieved": head["hbm_gb_s"], "peak": peak, "unit": "GB/s", "frac": head["hbm_gb_s"] / peak, "peak_source": peak_kind,
+                "algorithmic_bytes_per_query": 72}}
+    line = {
+        "metric": "M queries/s (per-query BSSRDF and microfacet-walk entries on 1 B200)", "value": head["m_queries_per_s"],
+        "unit": "M queries/s", "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": head["ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": QUERIES % n, "headline": "the directional dipole in FP32 (the per-pair term of the subsurface gathers)",
+                   "l2": "inputs + outputs of %.0f MB per directional launch, larger than L2" % (72 * n / 1e6)},
+        "per_op": per_op,
+        "e2e": {"value": n / (e2e_ms * 1e-3) / 1e6, "unit": "M queries/s", "h2d_bytes_per_step": 60 * n, "d2h_bytes_per_step": 12 * n,
+                "what": "the directional dipole from pinned host rows, values copied back, every step"},
+        "roofline": issue_roofline,
+        "gpu_launches": launches[0],
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle_ctypes as oc
+
+        threads = os.cpu_count() or 1
+        done, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < 3.0:  # whole passes over the batch's rows for about three seconds
+            oc.bssrdf_queries(params, 1, geo, which="ref", threads=threads)
+            done += n
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": done / dt / 1e6, "unit": "M queries/s", "cores": threads, "kind": "reference",
+                                "sample": "%d directional-dipole queries (passes over the %d-query batch), the reference's "
+                                          "dipoles/directional_dipole.h compiled for the host, %d threads, %.1f s" % (done, n, threads, dt)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_reference(args, world, rank):
     from open_rendering_framework_b200 import scenes
 
@@ -664,6 +832,10 @@ def run_reference(args, world, rank):
         return run_reference_bsdf(args)
     if args.workload == "ingest":
         return run_reference_ingest(args)
+    if args.workload == "queries":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference evaluates its dipoles and walks only inside OptiX "
+                                                              "programs; their host compilation is the queries line's cpu_baseline"}), flush=True)
+        return
     if args.workload == "build":
         print(json.dumps({"impl": "reference", "unavailable": "the reference builds its BVH inside OptiX (Trbvh / Sbvh, "
                                                               "OptixSceneLoader.cpp:136), which has no CPU build and is not on this box"}), flush=True)
@@ -1269,6 +1441,8 @@ def main():
         elif args.workload == "build":
             if rank == 0:
                 run_build(args, world, rank, local)
+        elif args.workload == "queries":
+            run_queries(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:
