@@ -821,6 +821,33 @@ def run_queries(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_reference_queries(args):
+    """Reference arm of the queries workload: the reference's directional dipole (dipoles/
+    directional_dipole.h) compiled for the host, all host cores, on the same query rows (each step a
+    pass over a bounded slice of them)."""
+    from oracle import oracle_ctypes as oc
+
+    params, dist, geo, wi, wo, alpha = query_inputs(args.queries)
+    threads = os.cpu_count() or 1
+    m = min(args.queries, 1 << 21)
+    for _ in range(max(0, min(args.warmup, 1))):
+        oc.bssrdf_queries(params, 1, geo[:, :m], which="ref", threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oc.bssrdf_queries(params, 1, geo[:, :m], which="ref", threads=threads)
+    dt = time.perf_counter() - t0
+    value = m * args.steps / dt / 1e6
+    sample = "%d directional-dipole queries per step, the reference's dipoles/directional_dipole.h compiled for the host, %d threads" % (
+        m, threads)
+    print(json.dumps({
+        "impl": "reference", "metric": "M queries/s (per-query BSSRDF and microfacet-walk entries on 1 B200)", "value": value,
+        "unit": "M queries/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / max(1, args.steps),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": QUERIES % args.queries, "sample_per_step": sample},
+        "cpu_baseline": {"value": value, "unit": "M queries/s", "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "M queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+
+
 def run_reference(args, world, rank):
     from open_rendering_framework_b200 import scenes
 
@@ -833,9 +860,7 @@ def run_reference(args, world, rank):
     if args.workload == "ingest":
         return run_reference_ingest(args)
     if args.workload == "queries":
-        print(json.dumps({"impl": "reference", "unavailable": "the reference evaluates its dipoles and walks only inside OptiX "
-                                                              "programs; their host compilation is the queries line's cpu_baseline"}), flush=True)
-        return
+        return run_reference_queries(args)
     if args.workload == "build":
         print(json.dumps({"impl": "reference", "unavailable": "the reference builds its BVH inside OptiX (Trbvh / Sbvh, "
                                                               "OptixSceneLoader.cpp:136), which has no CPU build and is not on this box"}), flush=True)
