@@ -5,7 +5,7 @@
 // query, all coalesced.  The kernel is ALU-bound (16-round TEA, transcendentals, the Beckmann
 // Newton loop in double/float), so it runs a grid-stride loop over a grid sized to a multiple of the
 // SM count; queries are ordered GGX-then-Beckmann and each distribution's range is its own launch of
-// a kernel specialised on it.
+// a kernel specialised on it (Beckmann: two launches, sampling then evaluation).
 #include <mutex>
 #include <vector>
 
@@ -19,7 +19,10 @@ __device__ unsigned long long g_bsdf_capped = 0;
 // One launch per distribution: a kernel instance holds only its own distribution's code, so an SM
 // never runs GGX and Beckmann warps side by side (a single kernel over the mixed batch thrashed the
 // instruction cache: "no instruction" was its top stall).  Queries k in [k_begin, k_end) of the batch.
-template <uint32_t kDist>
+// kPart 0: the whole query.  kPart 1 / 2: the Beckmann launch in two halves with smaller code each --
+// 1 samples the microfacet normal m and the direction wi (m parked in f, pdf, F), 2 evaluates f, pdf
+// and F from wo, wi and m.
+template <uint32_t kDist, int kPart = 0>
 __global__ void __launch_bounds__(256) k_bsdf_queries(const float* __restrict__ wo_soa, const float* __restrict__ alpha, uint64_t n,
                                                       uint64_t k_begin, uint64_t k_end, uint64_t first, float eta,
                                                       float* __restrict__ wi_soa, float* __restrict__ f_out, float* __restrict__ pdf_out,
@@ -27,22 +30,34 @@ __global__ void __launch_bounds__(256) k_bsdf_queries(const float* __restrict__ 
 {
   const float3 nrm = f3(0.0f, 0.0f, 1.0f);
   for (uint64_t k = k_begin + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < k_end; k += (uint64_t)gridDim.x * blockDim.x) {
-    uint64_t i = first + k;
-    uint32_t s = tea16((uint32_t)i, 0u);
-    float u1 = rnd_tea(s);
-    float u2 = rnd_tea(s);
     float3 wo = f3(__ldg(wo_soa + k), __ldg(wo_soa + n + k), __ldg(wo_soa + 2 * n + k));
     float a = __ldg(alpha + k);
-    int capped = 0;
-    float3 m = sample_visible_normal(kDist, wo, nrm, a, a, u1, u2, &capped);
-    float3 wi = reflect(-wo, m);
-    f_out[k] = walter_bsdf(kDist, wo, wi, nrm, a, eta);
-    pdf_out[k] = eval_visible_normal(kDist, wo, m, nrm, a, a) / (4.0f * fabsf(dot(wo, m)));
-    F_out[k] = fresnel_R(wo, m, eta);
-    wi_soa[k] = wi.x;
-    wi_soa[n + k] = wi.y;
-    wi_soa[2 * n + k] = wi.z;
-    if (capped) atomicAdd(&g_bsdf_capped, 1ull);
+    float3 m, wi;
+    if constexpr (kPart != 2) {
+      uint64_t i = first + k;
+      uint32_t s = tea16((uint32_t)i, 0u);
+      float u1 = rnd_tea(s);
+      float u2 = rnd_tea(s);
+      int capped = 0;
+      m = sample_visible_normal(kDist, wo, nrm, a, a, u1, u2, &capped);
+      wi = reflect(-wo, m);
+      wi_soa[k] = wi.x;
+      wi_soa[n + k] = wi.y;
+      wi_soa[2 * n + k] = wi.z;
+      if (capped) atomicAdd(&g_bsdf_capped, 1ull);
+    } else {
+      m = f3(f_out[k], pdf_out[k], F_out[k]);
+      wi = f3(wi_soa[k], wi_soa[n + k], wi_soa[2 * n + k]);
+    }
+    if constexpr (kPart == 1) {
+      f_out[k] = m.x;
+      pdf_out[k] = m.y;
+      F_out[k] = m.z;
+    } else {
+      f_out[k] = walter_bsdf(kDist, wo, wi, nrm, a, eta);
+      pdf_out[k] = eval_visible_normal(kDist, wo, m, nrm, a, a) / (4.0f * fabsf(dot(wo, m)));
+      F_out[k] = fresnel_R(wo, m, eta);
+    }
   }
 }
 
@@ -116,9 +131,13 @@ pt_status pt_bsdf_queries(const float* d_wo_soa, const float* d_alpha, uint64_t 
     PT_CHECK_CUDA(cudaGetLastError(), "pt_bsdf_queries launch (GGX)");
   }
   if (n_ggx < n) {
-    k_bsdf_queries<BECKMANN><<<grid_for(n - n_ggx, block, 8), block, 0, st>>>(d_wo_soa, d_alpha, n, n_ggx, n, first_index, eta, d_wi_soa,
-                                                                              d_f, d_pdf, d_F);
-    count_launch();
+    // the Beckmann queries in two launches (sample, then evaluate): each kernel's code fits the
+    // instruction cache better than the whole query's (+6.6 % on the 2^22-query batch)
+    k_bsdf_queries<BECKMANN, 1><<<grid_for(n - n_ggx, block, 8), block, 0, st>>>(d_wo_soa, d_alpha, n, n_ggx, n, first_index, eta,
+                                                                                 d_wi_soa, d_f, d_pdf, d_F);
+    k_bsdf_queries<BECKMANN, 2><<<grid_for(n - n_ggx, block, 8), block, 0, st>>>(d_wo_soa, d_alpha, n, n_ggx, n, first_index, eta,
+                                                                                 d_wi_soa, d_f, d_pdf, d_F);
+    count_launch(2);
     PT_CHECK_CUDA(cudaGetLastError(), "pt_bsdf_queries launch (Beckmann)");
   }
   return PT_OK;
