@@ -28,6 +28,15 @@ __global__ void __launch_bounds__(256) k_bsdf_queries(const float* __restrict__ 
                                                       float* __restrict__ wi_soa, float* __restrict__ f_out, float* __restrict__ pdf_out,
                                                       float* __restrict__ F_out)
 {
+  // Programmatic dependent launch: the GGX and sampling grids let the next launch of the stream place
+  // its blocks while their own last blocks drain; the evaluation grid reads the sampling grid's
+  // outputs, so it first waits for that grid to complete with its writes visible, and the sampling grid
+  // waits for the GGX grid before it exits, so that the evaluation grid's completion implies all three
+  // (griddepcontrol.wait is a no-op in a grid launched without a programmatic dependency).
+  if constexpr (kPart == 2)
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+  else
+    asm volatile("griddepcontrol.launch_dependents;");
   const float3 nrm = f3(0.0f, 0.0f, 1.0f);
   for (uint64_t k = k_begin + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < k_end; k += (uint64_t)gridDim.x * blockDim.x) {
     float3 wo = f3(__ldg(wo_soa + k), __ldg(wo_soa + n + k), __ldg(wo_soa + 2 * n + k));
@@ -59,6 +68,7 @@ __global__ void __launch_bounds__(256) k_bsdf_queries(const float* __restrict__ 
       F_out[k] = fresnel_R(wo, m, eta);
     }
   }
+  if constexpr (kPart == 1) asm volatile("griddepcontrol.wait;" ::: "memory");
 }
 
 __global__ void k_rng_streams(int kind, uint32_t* seeds, uint64_t n, uint32_t draws, float* out)
@@ -132,13 +142,27 @@ pt_status pt_bsdf_queries(const float* d_wo_soa, const float* d_alpha, uint64_t 
   }
   if (n_ggx < n) {
     // the Beckmann queries in two launches (sample, then evaluate): each kernel's code fits the
-    // instruction cache better than the whole query's (+6.6 % on the 2^22-query batch)
-    k_bsdf_queries<BECKMANN, 1><<<grid_for(n - n_ggx, block, 8), block, 0, st>>>(d_wo_soa, d_alpha, n, n_ggx, n, first_index, eta,
-                                                                                 d_wi_soa, d_f, d_pdf, d_F);
-    k_bsdf_queries<BECKMANN, 2><<<grid_for(n - n_ggx, block, 8), block, 0, st>>>(d_wo_soa, d_alpha, n, n_ggx, n, first_index, eta,
-                                                                                 d_wi_soa, d_f, d_pdf, d_F);
+    // instruction cache better than the whole query's (+6.6 % on the 2^22-query batch).  Each launch
+    // that follows one of this function's own is programmatic: the sampling grid reads only the inputs
+    // (complete before the GGX grid began, which was launched in stream order) and writes outside the
+    // GGX range; the evaluation grid waits in-kernel for the sampling grid.
+    cudaLaunchAttribute pdl[1];
+    pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    pdl[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid_for(n - n_ggx, block, 8));
+    cfg.blockDim = dim3(block);
+    cfg.stream = st;
+    cfg.attrs = pdl;
+    cfg.numAttrs = n_ggx > 0 ? 1 : 0;
+    PT_CHECK_CUDA(cudaLaunchKernelEx(&cfg, k_bsdf_queries<BECKMANN, 1>, d_wo_soa, d_alpha, n, n_ggx, n, first_index, eta, d_wi_soa, d_f,
+                                     d_pdf, d_F),
+                  "pt_bsdf_queries launch (Beckmann sampling)");
+    cfg.numAttrs = 1;
+    PT_CHECK_CUDA(cudaLaunchKernelEx(&cfg, k_bsdf_queries<BECKMANN, 2>, d_wo_soa, d_alpha, n, n_ggx, n, first_index, eta, d_wi_soa, d_f,
+                                     d_pdf, d_F),
+                  "pt_bsdf_queries launch (Beckmann evaluation)");
     count_launch(2);
-    PT_CHECK_CUDA(cudaGetLastError(), "pt_bsdf_queries launch (Beckmann)");
   }
   return PT_OK;
 }
