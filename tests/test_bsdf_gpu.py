@@ -127,6 +127,41 @@ def test_bsdf_queries_host_path_matches_device_path():
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
 
 
+def test_programmatic_launch_chain_on_a_user_stream():
+    # The Beckmann launches are programmatic dependents of the launch before them.  On a stream of the
+    # caller's, between a producer kernel that writes the inputs and a consumer kernel that copies the
+    # outputs, three calls in a row (mixed, all Beckmann, mixed again over rewritten inputs) must give
+    # the bits the default stream gives, the GGX range included.
+    n = 1 << 18
+    eta = np.float32(1 / 1.5)
+    wo0, a0 = oc.c1_inputs(n, 5)
+    wo1, a1 = oc.c1_inputs(n, 9)
+    cases = ((wo0, a0, 5, 5 + n // 2), (wo0, a0, 5, 0), (wo1, a1, 9, 9 + n // 3))
+    want = [run_gpu_queries(wo, a, first, ggx, eta) for wo, a, first, ggx in cases]
+    s = torch.cuda.Stream()
+    h_wo, h_a = dev(wo0), dev(a0)
+    d_wo = torch.empty_like(h_wo)
+    d_a = torch.empty_like(h_a)
+    d_wi = torch.empty((3, n), dtype=torch.float32, device="cuda")
+    outs = [torch.empty(n, dtype=torch.float32, device="cuda") for _ in range(3)]
+    torch.cuda.synchronize()
+    got = []
+    with torch.cuda.stream(s):
+        for wo, a, first, ggx in cases:
+            if wo is wo1:
+                h_wo, h_a = dev(wo1), dev(a1)
+                s.wait_stream(torch.cuda.default_stream())
+            d_wo.copy_(h_wo * 1.0)
+            d_a.copy_(h_a * 1.0)
+            nat.call("pt_bsdf_queries", d_wo.data_ptr(), d_a.data_ptr(), n, first, ggx, eta, d_wi.data_ptr(),
+                     outs[0].data_ptr(), outs[1].data_ptr(), outs[2].data_ptr(), ctypes.c_void_p(s.cuda_stream))
+            got.append([d_wi.clone()] + [o.clone() for o in outs])
+    s.synchronize()
+    for g, w in zip(got, want):
+        for a, b in zip(g, w):
+            assert np.array_equal(a.cpu().numpy().view(np.uint32), b.view(np.uint32))
+
+
 def test_empty_and_edge_inputs():
     # n == 0 is a no-op; grazing and normal-incidence directions stay finite where the oracle is finite.
     nat.call("pt_bsdf_queries", 0, 0, 0, 0, 0, 0.5, 0, 0, 0, 0, None)
