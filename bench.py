@@ -924,6 +924,42 @@ def reference_image(R, spp, factor=16):
     return img * ((spp + n) / n)
 
 
+def batched_roofline(st, clocks, local):
+    """Roofline of the batched pass's dominant kernel from a profiled pass's render stats: the dipole
+    gather against the INT32 issue bound (thread instructions per pair from the gather's ncu capture),
+    or the extend kernel's HBM view (its algorithmic bytes per segment over its live time); the other
+    kernel's figures ride along."""
+    import torch
+
+    sm_mhz = clocks.summary().get("sm_mhz") or 1965.0
+    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+    peak, peak_kind = load_peaks()
+    ext_s, gat_s = st.extend_ms * 1e-3, st.gather_ms * 1e-3
+    hbm = st.segments * EXTEND_BYTES_PER_SEGMENT / ext_s / 1e9 if ext_s > 0 else None
+    extend = {"bound": "hbm", "kernel": "k_extend_persistent (closest-hit traversal + material class record)",
+              "achieved": hbm, "peak": peak, "unit": "GB/s", "frac": hbm / peak if hbm else None, "peak_source": peak_kind,
+              "algorithmic_bytes_per_segment": EXTEND_BYTES_PER_SEGMENT, "traffic": None,
+              "extend_share_of_pass": st.extend_ms / st.gpu_ms if st.gpu_ms else None,
+              "segments_per_path": st.segments / max(1, st.path_samples)}
+    alu_peak = n_sm * 64 * sm_mhz * 1e6 / GATHER_INSTR_PER_PAIR / 1e9
+    pairs = st.dipole_pairs / gat_s / 1e9 if gat_s > 0 else None
+    gather = {"bound": "alu", "kernel": "k_gather (dipole gathers: one MD5 draw per (gather, probe) pair)",
+              "achieved": pairs, "peak": alu_peak, "unit": "Gpair/s", "frac": pairs / alu_peak if pairs else None,
+              "peak_source": "INT32 pipe: 64 lanes/clk/SM x SMs x median SM clock / %d thread instructions per pair "
+                             "(ncu capture of the subsurface configuration's gather)" % GATHER_INSTR_PER_PAIR,
+              "traffic": None, "gather_share_of_pass": st.gather_ms / st.gpu_ms if st.gpu_ms else None,
+              "pairs_per_gather": st.dipole_pairs / max(1, st.dipole_gathers)}
+    if st.gather_ms > st.extend_ms:
+        gather["extend"] = extend
+        out = gather
+    else:
+        extend["gather"] = gather
+        out = extend
+    out["timing"] = ("CUDA events around every extend and gather launch of one profiled batch pass "
+                     "(no graph, in-order schedule); pass time %.1f ms" % st.gpu_ms)
+    return out
+
+
 def measure_batched(args, world, local, relmse=True):
     """The batched configuration (64 seeded scenes in one pass from a CUDA graph): device-timed
     throughput, the same frames scene after scene (plain), the reference's launch pattern, the
@@ -1019,6 +1055,15 @@ def measure_batched(args, world, local, relmse=True):
     t_max = max_over_ranks(f0.elapsed_time(f1), world, "cuda")
     e2e_value = replica_throughput(path_samples, world, args.steps, t_max * 1e-3)
     st = B.stats()
+    # ---- roofline of the batch's dominant kernel, from one more pass without the graph and with CUDA
+    # events around every extend and gather launch (in-order schedule, as the single-scene profile)
+    B.set_option("use_graph", 0)
+    B.set_option("profile", 1)
+    B.render()
+    pst = B.stats()
+    B.set_option("profile", 0)
+    B.set_option("use_graph", 1)
+    roofline = batched_roofline(pst, clocks, local)
     kinds = {}
     for _, p, info in S:
         kinds[info["material"]] = kinds.get(info["material"], 0) + 1
@@ -1035,6 +1080,7 @@ def measure_batched(args, world, local, relmse=True):
         "autotune": {"extend_mode": tune.extend_mode, "refill": tune.refill, "max_paths_in_flight": tune.max_paths_in_flight,
                      "bin_items": tune.bin_items, "trials": tune.trials, "best_calibration_mpaths_per_s": tune.best_mpaths_per_s},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": roofline,
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
         "stats": {"segments_per_path": st.segments / max(1, st.path_samples), "dipole_gathers": st.dipole_gathers,
@@ -1077,7 +1123,6 @@ def measure_batched(args, world, local, relmse=True):
 
 
 def run_batched(args, world, rank, local):
-    peak, peak_kind = load_peaks()
     m = measure_batched(args, world, local)
     line = {
         "metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": m["warmup"],
@@ -1086,10 +1131,7 @@ def run_batched(args, world, rank, local):
         "config": {"workload": m["workload"], "path_samples_per_step": m["path_samples_per_step"], "scenes": m["scenes"],
                    "materials": m["materials"], "parallelism": "replicas (one independent batch per GPU)", "l2": m["l2"]},
         "e2e": m["e2e"], "gpu_launches": m["gpu_launches"], "clocks": m["clocks"],
-        "roofline": {"bound": "issue", "kernel": "k_extend_persistent", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
-                     "peak_source": peak_kind, "traffic": None,
-                     "note": "the batch runs from a CUDA graph without per-kernel events; the extend kernel's roofline is "
-                             "reported by the single-scene workload"},
+        "roofline": m["roofline"],
     }
     for k in ("plain_same_frames", "batched_over_plain_same_frames", "plain_per_frame", "batched_over_plain_per_frame", "autotune", "stats",
               "relmse_vs_16x_spp"):

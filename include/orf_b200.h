@@ -449,7 +449,9 @@ void* pt_batch_stream(pt_batch* batch);
 /* Adds a built scene; each batch render traces frames_per_render frames of it. */
 pt_status pt_batch_add(pt_batch* batch, pt_ctx* scene, uint32_t frames_per_render);
 /* Options of the batch engine: "extend_mode", "refill" (as pt_set_option), "max_paths_in_flight",
- * "use_graph" (1 = capture and replay the launch sequence, the default). */
+ * "use_graph" (1 = capture and replay the launch sequence, the default), "profile" (1 = CUDA events
+ * around every extend and gather launch of a pass without the graph, as pt_set_profiling; their summed
+ * times in pt_batch_get_stats). */
 pt_status pt_batch_set_option(pt_batch* batch, const char* name, int64_t value);
 /* Renders the next frames_per_render frames of every scene (starting at each scene's next frame). */
 pt_status pt_batch_render(pt_batch* batch);

@@ -235,6 +235,7 @@ pt_status pt_batch_set_option(pt_batch* b, const char* name, int64_t value)
     return PT_OK;
   }
   if (k == "max_paths_in_flight") return pt_set_max_paths_in_flight(b->eng, (uint64_t)value);
+  if (k == "profile") return pt_set_profiling(b->eng, (int)value);
   return pt_set_option(b->eng, name, value);
 }
 

@@ -135,3 +135,28 @@ def test_batch_rejects_bad_scenes():
     nat.call("pt_batch_destroy", empty)
     B.close()
     R.close()
+
+
+def test_profiled_batch_pass_times_extend_and_gather_and_keeps_images():
+    # option "profile": events around every extend and gather launch of a pass without the graph; the
+    # pass (in-order schedule) leaves the same images as the graph replay of the same frames
+    S = small_batch()
+    spp = [p for _, p, _ in S]
+    images = []
+    for profile in (0, 1):
+        Rs = [sc.Renderer(data) for data, _, _ in S]
+        B = sc.Batch(Rs, spp)
+        if profile:
+            B.set_option("use_graph", 0)
+            B.set_option("profile", 1)
+        B.render()
+        st = B.stats()
+        if profile:
+            assert st.extend_ms > 0.0 and st.gather_ms > 0.0 and st.dipole_pairs > 0
+            assert st.extend_ms + st.gather_ms <= st.gpu_ms * 1.001
+        images.append([R.readback() for R in Rs])
+        B.close()
+        for R in Rs:
+            R.close()
+    for a, b in zip(*images):
+        assert np.array_equal(bits(a), bits(b))
