@@ -492,7 +492,7 @@ def run_bsdf(args, world, rank, local):
         "config": {"workload": BSDF % n, "queries_per_step": n, "parallelism": "replicas (one independent batch per GPU)",
                    "l2": "inputs + outputs of %.0f MB per step, larger than L2" % (BSDF_BYTES_PER_QUERY * n / 1e6)},
         "e2e": {"value": e2e_value, "unit": "M queries/s", "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 24 * n,
-                "what": "pt_bsdf_queries_host from pinned host buffers (copies in, kernel, copies out, synchronous)",
+                "what": "pt_bsdf_queries_host from pinned host buffers (copies in, kernels, copies out in chunks of 2^19 queries on two streams; synchronous)",
                 "identical_to_device_path": same},
         "roofline": {"bound": "issue", "kernel": "k_bsdf_queries (GGX and Beckmann launches of one step)",
                      "achieved": issue_achieved, "peak": issue_peak, "unit": "G warp instructions/s",

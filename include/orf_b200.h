@@ -59,7 +59,10 @@ pt_status pt_bsdf_queries(const float* d_wo_soa, const float* d_alpha, uint64_t 
                           uint64_t n_ggx_below, float eta, float* d_wi_soa, float* d_f, float* d_pdf, float* d_F,
                           void* stream);
 /* Same query batch through host buffers: copies inputs to the device, runs the kernel, copies the
- * results back and synchronizes.  Device scratch is allocated per call. */
+ * results back and synchronizes.  Device scratch is allocated per call.  The batch moves in chunks of
+ * 2^19 queries on two streams of its own, so that copies in, kernels and copies out of different
+ * chunks overlap (pinned host buffers let the copies run asynchronously); results are identical to
+ * one pt_bsdf_queries over the whole batch. */
 pt_status pt_bsdf_queries_host(const float* wo_soa, const float* alpha, uint64_t n, uint64_t first_index,
                                uint64_t n_ggx_below, float eta, float* wi_soa, float* f, float* pdf, float* F);
 /* Same query batch through host buffers, without allocating any device memory.  This entry point

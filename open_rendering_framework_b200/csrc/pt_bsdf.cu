@@ -91,6 +91,9 @@ __global__ void k_rng_streams(int kind, uint32_t* seeds, uint64_t n, uint32_t dr
   }
 }
 
+// Queries per chunk of pt_bsdf_queries_host's copy / compute pipeline (20 MiB of device staging each).
+constexpr uint64_t kHostChunkQueries = 1ull << 19;
+
 // Staging area of pt_bsdf_queries_host_noalloc: room for kNoAllocMaxQueries queries, laid out as
 // wo (3n) | alpha (n) | wi (3n) | f (n) | pdf (n) | F (n).  Every GPU that loads this library holds
 // it (2.5 MiB) until the process exits.
@@ -172,21 +175,47 @@ pt_status pt_bsdf_queries_host(const float* wo_soa, const float* alpha, uint64_t
 {
   if (n == 0) return PT_OK;
   if (!wo_soa || !alpha || !wi_soa || !f || !pdf || !F) return fail(PT_INVALID_ARG, "pt_bsdf_queries_host: null pointer");
+  // The batch goes through in chunks on two streams, so that one chunk's inputs are copied in while
+  // another's queries run and a third's results are copied out (the copy engines of the two directions
+  // and the SMs work at once).  Chunk c of m queries starts at query k0 and has its own structure-of-
+  // arrays block of 10 m floats on the device: wo (3m) | alpha (m) | wi (3m) | f | pdf | F.  A query's
+  // result does not depend on the chunking (its seed is its global index first_index + k).
   float* d = nullptr;
-  size_t bytes = (size_t)n * 10 * sizeof(float);
-  PT_CHECK_CUDA(cudaMalloc(&d, bytes), "pt_bsdf_queries_host cudaMalloc");
-  float *d_wo = d, *d_a = d + 3 * n, *d_wi = d + 4 * n, *d_f = d + 7 * n, *d_pdf = d + 8 * n, *d_F = d + 9 * n;
+  PT_CHECK_CUDA(cudaMalloc(&d, (size_t)n * 10 * sizeof(float)), "pt_bsdf_queries_host cudaMalloc");
+  cudaStream_t s[2] = {nullptr, nullptr};
   pt_status st = PT_OK;
-  cudaError_t e = cudaMemcpy(d_wo, wo_soa, 3 * n * sizeof(float), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d_a, alpha, n * sizeof(float), cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) st = cuda_status(e, "pt_bsdf_queries_host H2D");
-  if (st == PT_OK) st = pt_bsdf_queries(d_wo, d_a, n, first_index, n_ggx_below, eta, d_wi, d_f, d_pdf, d_F, nullptr);
-  if (st == PT_OK) {
-    e = cudaMemcpy(wi_soa, d_wi, 3 * n * sizeof(float), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemcpy(f, d_f, n * sizeof(float), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemcpy(pdf, d_pdf, n * sizeof(float), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemcpy(F, d_F, n * sizeof(float), cudaMemcpyDeviceToHost);
+  for (int i = 0; i < 2 && st == PT_OK; ++i) {
+    cudaError_t e = cudaStreamCreateWithFlags(&s[i], cudaStreamNonBlocking);
+    if (e != cudaSuccess) st = cuda_status(e, "pt_bsdf_queries_host stream");
+  }
+  const uint64_t chunk = kHostChunkQueries;
+  for (uint64_t k0 = 0, c = 0; k0 < n && st == PT_OK; k0 += chunk, ++c) {
+    const uint64_t m = n - k0 < chunk ? n - k0 : chunk;
+    float* b = d + k0 * 10;
+    float *d_wo = b, *d_a = b + 3 * m, *d_wi = b + 4 * m, *d_f = b + 7 * m, *d_pdf = b + 8 * m, *d_F = b + 9 * m;
+    cudaStream_t cs = s[c & 1];
+    const size_t mb = m * sizeof(float);
+    cudaError_t e = cudaSuccess;
+    for (int j = 0; j < 3 && e == cudaSuccess; ++j) e = cudaMemcpyAsync(d_wo + j * m, wo_soa + j * n + k0, mb, cudaMemcpyHostToDevice, cs);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_a, alpha + k0, mb, cudaMemcpyHostToDevice, cs);
+    if (e != cudaSuccess) {
+      st = cuda_status(e, "pt_bsdf_queries_host H2D");
+      break;
+    }
+    st = pt_bsdf_queries(d_wo, d_a, m, first_index + k0, n_ggx_below, eta, d_wi, d_f, d_pdf, d_F, cs);
+    if (st != PT_OK) break;
+    for (int j = 0; j < 3 && e == cudaSuccess; ++j) e = cudaMemcpyAsync(wi_soa + j * n + k0, d_wi + j * m, mb, cudaMemcpyDeviceToHost, cs);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(f + k0, d_f, mb, cudaMemcpyDeviceToHost, cs);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(pdf + k0, d_pdf, mb, cudaMemcpyDeviceToHost, cs);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(F + k0, d_F, mb, cudaMemcpyDeviceToHost, cs);
     if (e != cudaSuccess) st = cuda_status(e, "pt_bsdf_queries_host D2H");
+  }
+  // wait for both streams whatever happened above, so that no copy still runs into the caller's buffers
+  for (int i = 0; i < 2; ++i) {
+    if (!s[i]) continue;
+    const cudaError_t e = cudaStreamSynchronize(s[i]);
+    if (e != cudaSuccess && st == PT_OK) st = cuda_status(e, "pt_bsdf_queries_host synchronize");
+    cudaStreamDestroy(s[i]);
   }
   cudaFree(d);
   return st;

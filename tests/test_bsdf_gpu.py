@@ -115,13 +115,16 @@ def test_bsdf_queries_match_oracle(first, ggx_fraction, tmp_path):
     print(json.dumps({"first": first, "ggx_fraction": ggx_fraction, "n": n, "report": report, "worst_query_indices": worst}))
 
 
-def test_bsdf_queries_host_path_matches_device_path():
-    n = 4096
+@pytest.mark.parametrize("n, n_ggx", [(4096, 2048), ((1 << 20) + 12345, 700001), ((1 << 19) + 1, 0)])
+def test_bsdf_queries_host_path_matches_device_path(n, n_ggx):
+    # the host entry moves the batch in chunks of 2^19 queries on two streams: one chunk, three chunks
+    # with a ragged last one and the GGX / Beckmann boundary inside the second, two chunks of which
+    # the last holds one query -- every output bit equal to one device call over the whole batch
     wo, alpha = oc.c1_inputs(n, 77)
-    got = run_gpu_queries(wo, alpha, 77, 77 + n // 2, np.float32(1 / 1.5))
+    got = run_gpu_queries(wo, alpha, 77, 77 + n_ggx, np.float32(1 / 1.5))
     wi = np.empty((3, n), np.float32)
     f, pdf, F = (np.empty(n, np.float32) for _ in range(3))
-    nat.call("pt_bsdf_queries_host", oc.fp(wo), oc.fp(alpha), n, 77, 77 + n // 2, np.float32(1 / 1.5),
+    nat.call("pt_bsdf_queries_host", oc.fp(wo), oc.fp(alpha), n, 77, 77 + n_ggx, np.float32(1 / 1.5),
              oc.fp(wi), oc.fp(f), oc.fp(pdf), oc.fp(F))
     for a, b in zip(got, (wi, f, pdf, F)):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
