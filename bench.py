@@ -1147,6 +1147,45 @@ ADJOINT = ("inverse rendering 256x256, 64 spp, depth 6, RR from depth 3: 12-tria
            "1024-spp target from other seeded parameters; forward + path-replay adjoint per step")
 
 
+def adjoint_roofline(fst, ast, clocks, local):
+    """Roofline of the forward + adjoint arm's dominant kernel from one profiled step (the forward
+    pass's and the adjoint pass's render stats): a dipole gather against the INT32 issue bound, or the
+    extend kernel's HBM view.  The bound uses the forward gather's thread instructions per pair (ncu);
+    the adjoint gather adds the derivatives of its accepted pairs, so its fraction is a lower bound."""
+    import torch
+
+    sm_mhz = clocks.summary().get("sm_mhz") or 1965.0
+    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+    peak, peak_kind = load_peaks()
+    total = fst.gpu_ms + ast.gpu_ms
+    parts = {"forward_extend": fst.extend_ms, "forward_gather": fst.gather_ms, "adjoint_extend": ast.extend_ms,
+             "adjoint_gather": ast.gather_ms}
+    shares = {k: (v / total if total else None) for k, v in parts.items()}
+    top = max(parts, key=parts.get)
+    if top.endswith("gather"):
+        s = fst if top.startswith("forward") else ast
+        alu_peak = n_sm * 64 * sm_mhz * 1e6 / GATHER_INSTR_PER_PAIR / 1e9
+        achieved = s.dipole_pairs / (s.gather_ms * 1e-3) / 1e9 if s.gather_ms else None
+        kernel = "k_gather (forward dipole gathers)" if top.startswith("forward") else \
+            "k_gather_adjoint (the adjoint pass's dipole gathers: the MD5 chain replayed, derivatives of accepted pairs)"
+        out = {"bound": "alu", "kernel": kernel, "achieved": achieved, "peak": alu_peak, "unit": "Gpair/s",
+               "frac": achieved / alu_peak if achieved else None,
+               "peak_source": "INT32 pipe: 64 lanes/clk/SM x SMs x median SM clock / %d thread instructions per pair of the "
+                              "forward gather (ncu)%s" % (GATHER_INSTR_PER_PAIR, "" if top.startswith("forward") else
+                                                          "; the adjoint gather does more per pair, so frac is a lower bound"),
+               "traffic": None, "pairs_per_gather": s.dipole_pairs / max(1, s.dipole_gathers)}
+    else:
+        s = fst if top.startswith("forward") else ast
+        hbm = s.segments * EXTEND_BYTES_PER_SEGMENT / (s.extend_ms * 1e-3) / 1e9 if s.extend_ms else None
+        out = {"bound": "hbm", "kernel": "k_extend_persistent (%s pass)" % top.split("_")[0], "achieved": hbm, "peak": peak,
+               "unit": "GB/s", "frac": hbm / peak if hbm else None, "peak_source": peak_kind,
+               "algorithmic_bytes_per_segment": EXTEND_BYTES_PER_SEGMENT, "traffic": None}
+    out["shares_of_forward_plus_adjoint"] = shares
+    out["timing"] = ("CUDA events around every extend and gather launch of one profiled forward + adjoint step (in-order "
+                     "schedule); forward %.2f ms, adjoint %.2f ms" % (fst.gpu_ms, ast.gpu_ms))
+    return out
+
+
 def measure_adjoint(args, local, relmse=True, spp=None, width=None):
     """The differentiable configuration: forward (differentiable) render + path-replay adjoint per
     step, device-timed per phase; the end-to-end figure through the torch.autograd.Function; the
@@ -1222,6 +1261,14 @@ def measure_adjoint(args, local, relmse=True, spp=None, width=None):
         "stats": {"segments_per_path": seg / (args.steps * path_samples), "dipole_gathers_per_step": gathers / args.steps},
         "l2": "per-path forward state of %.2f GB re-read by the adjoint" % (path_samples * 16 * 8 / 1e9),
     }
+    # ---- roofline of the arm's dominant kernel: one more step with CUDA events around every extend and
+    # gather launch of its forward and adjoint passes
+    from open_rendering_framework_b200 import _native as nat
+
+    nat.call("pt_set_profiling", DS.R.ctx, 1)
+    _, pf, pa = step()
+    nat.call("pt_set_profiling", DS.R.ctx, 0)
+    out["roofline"] = adjoint_roofline(pf, pa, clocks, local)
     if relmse:
         img = last["img"].detach().cpu().numpy()
         ref = reference_image(DS.R, spp)
@@ -1238,7 +1285,7 @@ def run_adjoint(args, world, rank, local):
         "data": "synthetic",
         "config": {"workload": m["workload"], "path_samples_per_step": m["path_samples_per_step"], "parameters": m["parameters"],
                    "l2": m["l2"]},
-        "e2e": m["e2e"], "gpu_launches": m["gpu_launches"], "clocks": m["clocks"],
+        "e2e": m["e2e"], "roofline": m["roofline"], "gpu_launches": m["gpu_launches"], "clocks": m["clocks"],
     }
     for k in ("forward", "adjoint_ms_per_step", "fwd_plus_adjoint_over_forward", "target_fwd_plus_adjoint_le_3x_forward", "loss",
               "grad_norms", "stats", "relmse_vs_16x_spp"):
